@@ -1,0 +1,260 @@
+/* tapsim_gpu.h — C ABI of the B200 implementation of TAPSim's per-event hot
+ * path (relax -> field ratio / argmax -> atom removal -> ion flight).
+ *
+ * The reference has no plugin or FFI layer: the path sits behind the C++
+ * class API that Process::evaporation (tapsim/process.cpp:441-1124) calls.
+ * Every device entry point below replaces one of those calls and names it.
+ * Plain pointers and sizes only; all device memory is owned by the handle;
+ * inputs are copied at the call, outputs go to caller-allocated host arrays.
+ * Errors are int status codes (TG_OK == 0); nothing throws across the ABI.
+ * A handle is used from one host thread; its work is ordered on one CUDA
+ * stream.
+ */
+#ifndef TAPSIM_GPU_H
+#define TAPSIM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    TG_OK = 0,
+    TG_ERR_ARGUMENT = 1,        /* invalid argument / size */
+    TG_ERR_CUDA = 2,            /* CUDA runtime error (message via tg_last_error) */
+    TG_ERR_NAN = 3,             /* NaN in a potential, field or trajectory */
+    TG_ERR_SINGULAR = 4,        /* singular 3x3 system in field_o1 */
+    TG_ERR_NOT_SURFACE = 5,     /* removal of a node that is not a surface cell */
+    TG_ERR_RELAX_FAULT = 6,     /* stagnation (Grid_3d::Table::RelaxationFault) */
+    TG_ERR_ITERATION_CAP = 7,   /* iteration cap reached before the tolerance */
+    TG_ERR_OUTSIDE = 8,         /* trajectory start point outside the mesh */
+    TG_ERR_WALK_LIMIT = 9,      /* tetrahedron walk exceeded its step bound */
+    TG_ERR_NO_SURFACE = 10,     /* surface set is empty */
+    TG_ERR_HOST = 11,           /* host-side failure (file, mesh build) */
+    TG_ERR_UNKNOWN_TYPE = 12    /* cell type id not in the type table */
+};
+
+/* Trajectory status, values of Trajectory_3d's enum (trajectory_3d.h:89). */
+enum {
+    TG_TRAJ_INVALID = -1,
+    TG_TRAJ_NO_INTEGRATION = 0,
+    TG_TRAJ_NO_FIELD = 1,
+    TG_TRAJ_STEPPER_LIMIT_PASSED = 2,
+    TG_TRAJ_ITERATION_LIMIT_PASSED = 3,
+    TG_TRAJ_GEOMETRY_LIMIT_PASSED = 4,
+    TG_TRAJ_SYSTEM_LIMIT_PASSED = 5
+};
+
+/* ---- cell types: Configuration::NodeData (configuration.h:70-160) -------- */
+typedef struct {
+    int32_t id;               /* NodeId value 0..127 */
+    float charge_density;     /* [C/m^3] */
+    float epsilon;            /* relative permittivity */
+    int32_t removable;
+    int32_t neumann;
+    int32_t dirichlet;
+    float phi;                /* preset potential [V] */
+    float mass;               /* [amu] */
+    int32_t evap_charge;      /* charge state */
+    float evap_field;         /* [V/m] */
+    float evap_energy;        /* [eV] */
+} tg_type;
+
+/* ---- mesh description (replaces System_3d, system_3d.h:29-42) ------------
+ * Node order is the node-file order; all indices are node-file indices.   */
+typedef struct {
+    int32_t num_nodes;
+    const float* xyz;              /* [3N] Geometry_3d::NodeData::coords [m] */
+    const int8_t* type_id;         /* [N]  Grid_3d::Node::id */
+    const uint8_t* hull;           /* [N]  Geometry_3d::NodeData::boundary */
+    const float* phi;              /* [N]  initial potential [V] */
+    const int32_t* row_ptr;        /* [N+1] Delaunay neighbours, ascending */
+    const int32_t* col;            /* [nnz] */
+    const double* coupling;        /* [nnz] c_ij as Grid_3d::Table::fastSync leaves it */
+    const double* geom;            /* [nnz] face area(0.5 d)/d; NULL: derived from coupling */
+    const uint8_t* area_pos;       /* [nnz] face area(1.0) > 0; NULL: coupling-derived */
+    const double* volume;          /* [N]  capped Voronoi volume; NULL: zero charge */
+    int32_t num_tets;
+    const int32_t* tet_v;          /* [4T] vertices, positively oriented */
+    const int32_t* tet_n;          /* [4T] neighbour k opposite vertex k, -1 on the hull */
+    const int32_t* node_tet;       /* [N]  associated tetrahedron */
+    int32_t num_types;
+    const tg_type* types;
+} tg_mesh_desc;
+
+typedef struct tg_handle tg_handle;
+
+/* Creates the device state from a mesh description.  Copies every array. */
+int tg_create(const tg_mesh_desc* desc, tg_handle** out);
+void tg_destroy(tg_handle* h);
+/* Last error message of the handle (or of the process when h == NULL). */
+const char* tg_last_error(const tg_handle* h);
+int tg_num_nodes(const tg_handle* h);
+
+/* ---- potentials: Grid_3d::Table ---------------------------------------- */
+/* Grid_3d::Table::relax(n) (grid_3d.cpp:591-609): n coloured Gauss-Seidel
+ * sweeps over all free cells (computePotential, grid_3d.cpp:1317-1371);
+ * *deviation = max |phi_new - phi_old| of the last sweep. */
+int tg_relax_cycles(tg_handle* h, int32_t n, double* deviation);
+/* Grid_3d::Table::relax(thr, cycle, queue) (grid_3d.cpp:611-671): repeats
+ * relax(cycle) until the deviation is <= thr; TG_ERR_RELAX_FAULT on the
+ * stagnation rule (zero regression slope over `queue` deviations),
+ * TG_ERR_ITERATION_CAP after max_sweeps. */
+int tg_relax_threshold(tg_handle* h, double threshold, int32_t cycle, int32_t queue, int64_t max_sweeps,
+                       int64_t* iterations, double* deviation);
+/* Grid_3d::Table::localRelax(idx, order, thr, cycle, queue)
+ * (grid_3d.cpp:707-795, find_localNodes :1284-1315). */
+int tg_local_relax(tg_handle* h, int32_t node, int32_t shell, double threshold, int32_t cycle, int32_t queue,
+                   int64_t* iterations, double* deviation);
+
+/* Solves the finite-volume system to a relative residual ||r||_2/||b||_2 <=
+ * rel_tol (r_i = sum_j c_ij (phi_j - phi_i) - q_i over free cells, b = the
+ * Dirichlet part).  FP64 residual and update, FP32 inner iterations.  No
+ * counterpart in the reference, which stops on max |delta phi| instead. */
+typedef struct {
+    double rel_tol;           /* e.g. 1e-8 */
+    int32_t max_outer;        /* FP64 defect-correction steps */
+    int32_t max_inner;        /* FP32 iterations per step */
+    double inner_rtol;        /* inner relative reduction per step */
+} tg_solve_opts;
+typedef struct {
+    int32_t outer;            /* defect-correction steps taken */
+    int32_t inner;            /* FP32 iterations taken in total */
+    double rel_residual;      /* final ||r||/||b|| */
+    double initial_rel_residual;
+} tg_solve_info;
+int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);
+/* ||r||_2 / ||b||_2 of the current potentials (FP64). */
+int tg_residual(tg_handle* h, double* rel_residual);
+
+int tg_get_phi(tg_handle* h, double* phi_out);       /* [N] */
+int tg_set_phi(tg_handle* h, const double* phi_in);  /* [N] */
+/* Grid_3d::Table::field_o1 (grid_3d.cpp:909-991) for a list of nodes. */
+int tg_field_o1(tg_handle* h, int32_t count, const int32_t* nodes, double* field_out /* [3*count] */);
+/* Current coupling, type and effective diagonal (for checks). */
+int tg_get_couplings(tg_handle* h, double* coupling_out /* [nnz] */);
+int tg_get_types(tg_handle* h, int8_t* type_out /* [N] */);
+
+/* ---- surface: Surface_3d --------------------------------------------- */
+/* Surface_3d::Table::init (surface_3d.cpp:50-81). */
+int tg_surface_init(tg_handle* h, int32_t vacuum_id, int32_t* num_surface);
+/* evap_compute_specificFields + evap_compute_probabilities(PROB_LINEAR_FIELD)
+ * + evapMaximum (surface_3d.cpp:194-219, 267-297, 423-431) in one pass:
+ * ratio_i = |E_i| / E_evap(type_i); the candidate is the first maximum in
+ * ascending node order; second is the runner-up (near-tie margin). */
+typedef struct {
+    int32_t num_surface;
+    int32_t candidate;          /* node index, -1 when the surface is empty */
+    float best_ratio;           /* = scaling reference */
+    float second_ratio;
+    double ratio_sum;
+    float probability;          /* best_ratio / ratio_sum */
+    int32_t apex;               /* Surface_3d::Table::apex (surface_3d.cpp:171-190) */
+} tg_select_info;
+int tg_surface_select(tg_handle* h, tg_select_info* info);
+int tg_get_surface(tg_handle* h, int32_t capacity, int32_t* nodes, float* ratios, int32_t* count);
+/* Surface_3d::Table::normal (surface_3d.cpp:123-169). */
+int tg_surface_normal(tg_handle* h, int32_t node, float normal_out[3]);
+/* evap_takeAway (surface_3d.cpp:507-564): flip to vacuum, fastResync
+ * (grid_3d.cpp:555-589), surface update (surface_3d.cpp:83-119) and removal
+ * of detached neighbours.  detached_out receives up to `capacity` indices. */
+int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached_out, int32_t* num_detached);
+/* update_coordination (surface_3d.cpp:568-593). */
+int tg_update_coordination(tg_handle* h);
+
+/* ---- ion flights: Trajectory_3d ---------------------------------------- */
+typedef struct {
+    double time_step;           /* TRAJECTORY_INITIAL_TIME_STEP [s] */
+    double min_time_step;       /* TRAJECTORY_MINIMUM_TIME_STEP [s] */
+    double error_threshold;     /* TRAJECTORY_ERROR_THRESHOLD */
+    int32_t max_steps;          /* iteration bound per ion */
+    int32_t stepper_limit;      /* trial steps per accepted step */
+    int32_t walk_limit;         /* tetrahedra per point location */
+} tg_trace_opts;
+typedef struct {
+    float stop[3];              /* impact after extrapolation to the top plane [m] */
+    float stop_time;            /* [s] */
+    float last_pos[3];          /* last point inside the mesh [m] */
+    int32_t last_tet;
+    float last_phi;             /* Grid_3d::potential at last_pos [V] */
+    int32_t steps;              /* accepted steps */
+    int32_t status;             /* TG_TRAJ_* */
+} tg_impact;
+/* Trajectory_3d::init/integrate/extrapolate (trajectory_3d.cpp:99-209,
+ * 303-332) with o5_integrator (Cash-Karp, :583-676) and
+ * errorRestricted_stepper (:358-425), batched: one ion per thread. */
+int tg_trace(tg_handle* h, int32_t n_ions, const float* start_xyz, const float* start_vel,
+             const float* charge_over_mass, const int32_t* tet_guess, const tg_trace_opts* opts, tg_impact* out);
+/* Grid_3d::potential(geom, grid, pos, tet) (grid_3d.cpp:1585-1602). */
+int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* tet_guess, float* phi_out);
+
+/* ---- one evaporation event: Process::evaporation steps I-VI ------------ */
+typedef struct {
+    int32_t vacuum_id;
+    int32_t relax_mode;         /* 0: reference (local + global sweeps, refresh), 1: solve to rel_tol */
+    /* relax_mode 0: LOCAL_RELAXATION_*, GLOBAL_RELAXATION_STEPS, REFRESH_RELAXATION_* */
+    double local_threshold;
+    int32_t local_shell, local_cycle, local_queue;
+    int32_t global_steps;
+    int32_t refresh_interval;
+    double refresh_threshold;
+    int32_t refresh_cycle, refresh_queue;
+    int64_t refresh_max_sweeps;
+    /* relax_mode 1 */
+    tg_solve_opts solve;
+    tg_trace_opts trace;
+    int32_t trace_enabled;
+    int32_t normal_enabled;
+} tg_event_opts;
+typedef struct {
+    int32_t node;
+    int32_t type_id;
+    float probability;
+    float best_ratio, second_ratio;  /* near-tie margin = (best - second)/best */
+    float scaling_reference;         /* of the selection step */
+    float phi_before, field_before[3];
+    float phi_after, field_after[3];
+    float apex[3];
+    float normal[3];
+    tg_impact impact;
+    int32_t detached;
+    int32_t relax_iterations;
+    double rel_residual;
+    int32_t relax_status;
+} tg_event_record;
+int tg_run_event(tg_handle* h, const tg_event_opts* opts, int32_t event_index, tg_event_record* rec);
+
+/* ---- host-side mesh building (setup, not device work) ------------------ */
+typedef struct tg_mesh tg_mesh;
+typedef struct {
+    double lattice_a, cap_radius, shank_length, half_angle_deg;
+    double box_half_width, box_height, fine_shell;
+    int32_t layers_per_level;
+    double coarsen, max_spacing;
+    double solute_fraction, precip_density, precip_rmin, precip_rmax, precip_mu, precip_sigma;
+    uint64_t seed;
+} tg_tip_params;
+void tg_tip_params_default(tg_tip_params* p);
+/* bcc [110] tip + coarsened vacuum -> Delaunay -> FP64 Voronoi tables. */
+int tg_mesh_from_tip(const tg_tip_params* p, int32_t threads, tg_mesh** out);
+/* Node file + config (meshgen output / File_Io::readGeomGrid input). */
+int tg_mesh_from_files(const char* node_file, const char* config_file, int32_t threads, tg_mesh** out);
+/* TAPSIM dump (File_Io::readSystem); keeps the dump's float couplings.
+ * config_file may be NULL to use the dump's own table. */
+int tg_mesh_from_dump(const char* dump_file, const char* config_file, tg_mesh** out);
+void tg_mesh_destroy(tg_mesh* m);
+/* Fills a description whose pointers stay valid while the mesh lives. */
+int tg_mesh_describe(const tg_mesh* m, tg_mesh_desc* desc, int32_t* nnz);
+int tg_mesh_write_node_file(const tg_mesh* m, const char* path, int32_t binary);
+int tg_mesh_write_config(const tg_mesh* m, const char* path);
+/* Writes a TAPSIM dump (File_Io::writeSystem layout) of the mesh with the
+ * given potentials (NULL: the mesh's own). */
+int tg_mesh_write_dump(const tg_mesh* m, const char* path, const float* phi);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TAPSIM_GPU_H */

@@ -1,0 +1,481 @@
+/* CPU restatement of TAPSim's per-event hot path in FP64 (test oracle).
+ * Test infrastructure only; see tapsim_oracle.h. */
+#include "tapsim_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+static int is_neumann(const orc_mesh* m, int i) { return m->types[(int)m->type[i]].neumann; }
+static int is_dirichlet(const orc_mesh* m, int i) { return m->types[(int)m->type[i]].dirichlet; }
+
+/* weight of neighbour entry q in the update of row i: computePotential
+ * (tapsim/grid_3d.cpp:1317-1371) skips Neumann neighbours of non-Neumann rows */
+static double row_weight(const orc_mesh* m, int i, int q) {
+    if (!is_neumann(m, i) && is_neumann(m, m->col[q])) return 0.0;
+    return m->c[q];
+}
+
+double orc_residual(const orc_mesh* m) {
+    double r2 = 0.0, b2 = 0.0;
+    for (int i = 0; i < m->n; i++) {
+        if (is_dirichlet(m, i)) continue;
+        double s = 0.0, d = 0.0, b = 0.0;
+        for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+            const double w = row_weight(m, i, q);
+            const int j = m->col[q];
+            s += w * m->phi[j];
+            d += w;
+            if (is_dirichlet(m, j)) b += w * m->phi[j];
+        }
+        const double r = s - d * m->phi[i] - m->q[i];
+        b -= m->q[i];
+        r2 += r * r;
+        b2 += b * b;
+    }
+    return b2 > 0.0 ? sqrt(r2 / b2) : sqrt(r2);
+}
+
+static double sweep(orc_mesh* m, double omega) {
+    double dev = 0.0;
+    for (int i = 0; i < m->n; i++) {
+        if (is_dirichlet(m, i)) continue;
+        double s = 0.0, d = 0.0;
+        for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+            const double w = row_weight(m, i, q);
+            s += w * m->phi[m->col[q]];
+            d += w;
+        }
+        const double v = (s - m->q[i]) / d;
+        const double nv = m->phi[i] + omega * (v - m->phi[i]);
+        const double dl = fabs(nv - m->phi[i]);
+        if (dl > dev) dev = dl;
+        m->phi[i] = nv;
+    }
+    return dev;
+}
+
+int64_t orc_solve(orc_mesh* m, double tol, int64_t max_sweeps, double omega, double* rel_out) {
+    int64_t s = 0;
+    double rel = orc_residual(m);
+    while (rel > tol) {
+        if (s >= max_sweeps) {
+            if (rel_out) *rel_out = rel;
+            return -1;
+        }
+        for (int k = 0; k < 10; k++) sweep(m, omega);
+        s += 10;
+        rel = orc_residual(m);
+    }
+    if (rel_out) *rel_out = rel;
+    return s;
+}
+
+double orc_relax_cycles(orc_mesh* m, int32_t n) {
+    double dev = 0.0;
+    for (int k = 0; k < n; k++) dev = sweep(m, 1.0);
+    return dev;
+}
+
+/* Grid_3d::Table::field_o1 (grid_3d.cpp:909-991) in FP64 */
+int orc_field_o1(const orc_mesh* m, int32_t i, double E[3]) {
+    E[0] = E[1] = E[2] = 0.0;
+    if (m->hull && m->hull[i]) return 1;
+    double A[3][3] = {{0}}, b[3] = {0};
+    for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+        if (m->c[q] == 0.0) continue;
+        const int j = m->col[q];
+        double d[3];
+        for (int k = 0; k < 3; k++) d[k] = (double)m->xyz[3 * j + k] - (double)m->xyz[3 * i + k];
+        const double dp = m->phi[j] - m->phi[i];
+        for (int r = 0; r < 3; r++) {
+            for (int s = 0; s < 3; s++) A[r][s] += d[r] * d[s];
+            b[r] += dp * d[r];
+        }
+    }
+    /* Gaussian elimination with partial pivoting */
+    int piv[3] = {0, 1, 2};
+    for (int k = 0; k < 3; k++) {
+        int p = k;
+        for (int r = k + 1; r < 3; r++)
+            if (fabs(A[r][k]) > fabs(A[p][k])) p = r;
+        if (A[p][k] == 0.0) return 0;
+        if (p != k) {
+            for (int s = 0; s < 3; s++) {
+                const double t = A[k][s];
+                A[k][s] = A[p][s];
+                A[p][s] = t;
+            }
+            const double t = b[k];
+            b[k] = b[p];
+            b[p] = t;
+            const int ti = piv[k];
+            piv[k] = piv[p];
+            piv[p] = ti;
+        }
+        for (int r = k + 1; r < 3; r++) {
+            const double f = A[r][k] / A[k][k];
+            for (int s = k; s < 3; s++) A[r][s] -= f * A[k][s];
+            b[r] -= f * b[k];
+        }
+    }
+    double g[3];
+    for (int k = 2; k >= 0; k--) {
+        double s = b[k];
+        for (int r = k + 1; r < 3; r++) s -= A[k][r] * g[r];
+        g[k] = s / A[k][k];
+    }
+    for (int k = 0; k < 3; k++) E[k] = -g[k];
+    return 1;
+}
+
+/* Surface_3d::Table::init / update candidate test (surface_3d.cpp:50-119) */
+static int surface_candidate(const orc_mesh* m, int i, int vac) {
+    const int t = m->type[i];
+    if (t == vac) return 0;
+    if (!m->types[t].removable) return 0;
+    for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++)
+        if (m->type[m->col[q]] == vac && m->area_pos[q]) return 1;
+    return 0;
+}
+
+int32_t orc_surface_init(orc_mesh* m, int32_t vac) {
+    int32_t cnt = 0;
+    for (int i = 0; i < m->n; i++) {
+        m->surface[i] = (uint8_t)surface_candidate(m, i, vac);
+        cnt += m->surface[i];
+    }
+    return cnt;
+}
+
+/* evap_compute_specificFields + probLinear_field + evapMaximum + apex
+ * (surface_3d.cpp:171-219, 267-297, 423-431): ascending node order, first
+ * maximum wins */
+void orc_select(const orc_mesh* m, float* ratio_out, orc_select_info* info) {
+    info->candidate = -1;
+    info->apex = -1;
+    info->num_surface = 0;
+    info->best = -1.0f;
+    info->second = 0.0f;
+    info->sum = 0.0;
+    float zmax = 0.0f;
+    for (int i = 0; i < m->n; i++) {
+        if (!m->surface[i]) continue;
+        double E[3];
+        orc_field_o1(m, i, E);
+        const float r = (float)(sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]) / m->types[(int)m->type[i]].evap_field);
+        if (ratio_out) ratio_out[i] = r;
+        info->sum += r;
+        if (info->candidate < 0 || r > info->best) {
+            if (info->candidate >= 0) info->second = info->best > info->second ? info->best : info->second;
+            info->best = r;
+            info->candidate = i;
+        } else if (r > info->second) {
+            info->second = r;
+        }
+        if (info->apex < 0 || m->xyz[3 * i + 2] > zmax) {
+            zmax = m->xyz[3 * i + 2];
+            info->apex = i;
+        }
+        info->num_surface++;
+    }
+}
+
+/* computeCoupling (grid_3d.cpp:1392-1409) for the pair (n1, n2) */
+static double pair_coupling(const orc_mesh* m, int n1, int n2, double geom) {
+    if (!is_neumann(m, n1) && is_neumann(m, n2)) return 0.0;
+    const double e1 = m->types[(int)m->type[n1]].epsilon, e2 = m->types[(int)m->type[n2]].epsilon;
+    return 2.0 * e1 * e2 / (e1 + e2) * geom;
+}
+
+static int find_entry(const orc_mesh* m, int i, int j) {
+    for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++)
+        if (m->col[q] == j) return q;
+    return -1;
+}
+
+/* setId(vacuum) + fastResync (grid_3d.cpp:555-589) */
+static void flip(orc_mesh* m, int i, int vac) {
+    m->type[i] = (int8_t)vac;
+    for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+        const int j = m->col[q];
+        const double c = pair_coupling(m, i, j, m->geom[q]);
+        m->c[q] = c;
+        m->c[find_entry(m, j, i)] = c;
+    }
+    m->q[i] = m->volume ? m->volume[i] * m->types[vac].charge_density / 8.85418781762e-12 : 0.0;
+}
+
+/* Surface_3d::Table::update (surface_3d.cpp:83-119) */
+static int surface_update(orc_mesh* m, int i, int vac) {
+    if (!m->surface[i]) return 0;
+    m->surface[i] = 0;
+    for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+        const int j = m->col[q];
+        if (!m->surface[j] && surface_candidate(m, j, vac)) m->surface[j] = 1;
+    }
+    return 1;
+}
+
+/* evap_takeAway (surface_3d.cpp:507-564) */
+int32_t orc_take_away(orc_mesh* m, int32_t node, int32_t vac, int32_t* detached, int32_t cap) {
+    if (!m->surface[node]) return -1;
+    flip(m, node, vac);
+    surface_update(m, node, vac);
+    int32_t nd = 0;
+    int32_t lonely[512];
+    for (int q = m->row_ptr[node]; q < m->row_ptr[node + 1]; q++) {
+        const int j = m->col[q];
+        if (m->type[j] == vac) continue;
+        int all = 1;
+        for (int p = m->row_ptr[j]; p < m->row_ptr[j + 1]; p++)
+            if (m->type[m->col[p]] != vac) { all = 0; break; }
+        if (all && nd < 512) lonely[nd++] = j;
+    }
+    for (int k = 0; k < nd; k++) {
+        flip(m, lonely[k], vac);
+        surface_update(m, lonely[k], vac);
+        if (detached && k < cap) detached[k] = lonely[k];
+    }
+    return nd;
+}
+
+/* update_coordination (surface_3d.cpp:568-593), in node order as the reference */
+void orc_update_coordination(orc_mesh* m) {
+    for (int i = 0; i < m->n; i++) {
+        if (m->type[i] < 10) continue;
+        int cnt = 0;
+        for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++)
+            if (m->type[m->col[q]] >= 10) cnt++;
+        m->type[i] = (int8_t)(m->type[i] + cnt);
+    }
+}
+
+/* ---- flights -------------------------------------------------------------- */
+
+static double orient(const double* a, const double* b, const double* c, const double* p) {
+    const double u[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double v[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    const double w[3] = {p[0] - a[0], p[1] - a[1], p[2] - a[2]};
+    return u[0] * (v[1] * w[2] - v[2] * w[1]) - u[1] * (v[0] * w[2] - v[2] * w[0]) + u[2] * (v[0] * w[1] - v[1] * w[0]);
+}
+
+static void node_xyz(const orc_mesh* m, int i, double* o) {
+    o[0] = m->xyz[3 * i];
+    o[1] = m->xyz[3 * i + 1];
+    o[2] = m->xyz[3 * i + 2];
+}
+
+static const int kFace[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};
+
+/* power-of-two scale to an integer grid with |coordinate| <= 2^40 */
+static double snap_scale(const orc_mesh* m) {
+    static const float* cached_xyz = 0;
+    static int cached_n = -1;
+    static double cached = 1.0;
+    if (cached_xyz == m->xyz && cached_n == m->n) return cached;
+    double amax = 0.0;
+    for (int i = 0; i < 3 * m->n; i++)
+        if (fabs((double)m->xyz[i]) > amax) amax = fabs((double)m->xyz[i]);
+    cached = amax > 0.0 ? ldexp(1.0, (int)floor(log2(ldexp(1.0, 40) / amax))) : 1.0;
+    cached_xyz = m->xyz;
+    cached_n = m->n;
+    return cached;
+}
+
+/* exact sign of orient(a,b,c,p) for the points snapped to that grid (the
+ * reference walks with Shewchuk's exact orient3d) */
+static int orient_exact(const double* a, const double* b, const double* c, const double* p, double s) {
+    const double o = orient(a, b, c, p);
+    const double lim = ldexp(1.0, 40);
+    if (fabs(p[0] * s) > lim || fabs(p[1] * s) > lim || fabs(p[2] * s) > lim) return o > 0 ? 1 : (o < 0 ? -1 : 0);
+    long long A[3], U[3], V[3], W[3];
+    for (int k = 0; k < 3; k++) {
+        A[k] = llround(a[k] * s);
+        U[k] = llround(b[k] * s) - A[k];
+        V[k] = llround(c[k] * s) - A[k];
+        W[k] = llround(p[k] * s) - A[k];
+    }
+    const __int128 m0 = (__int128)V[1] * W[2] - (__int128)V[2] * W[1];
+    const __int128 m1 = (__int128)V[0] * W[2] - (__int128)V[2] * W[0];
+    const __int128 m2 = (__int128)V[0] * W[1] - (__int128)V[1] * W[0];
+    const __int128 e = (__int128)U[0] * m0 - (__int128)U[1] * m1 + (__int128)U[2] * m2;
+    return e > 0 ? 1 : (e < 0 ? -1 : 0);
+}
+
+/* findTetrahedron (geometry_3d.cpp:988-1044): visibility walk, faces tried in
+ * a fixed order; -1 outside the mesh */
+static int locate(const orc_mesh* m, const double* p, int t) {
+    const double s = snap_scale(m);
+    for (int step = 0; step < 4 * m->ntets + 16; step++) {
+        if (t < 0) return -1;
+        const int* v = m->tet_v + 4 * t;
+        int next = -2;
+        for (int k = 0; k < 4; k++) {
+            double a[3], b[3], c[3];
+            node_xyz(m, v[kFace[k][0]], a);
+            node_xyz(m, v[kFace[k][1]], b);
+            node_xyz(m, v[kFace[k][2]], c);
+            if (orient_exact(a, b, c, p, s) < 0) {
+                next = m->tet_n[4 * t + k];
+                break;
+            }
+        }
+        if (next == -2) return t;
+        t = next;
+    }
+    return -1;
+}
+
+static void weights(const orc_mesh* m, int t, const double* p, double* w) {
+    double P[4][3];
+    for (int k = 0; k < 4; k++) node_xyz(m, m->tet_v[4 * t + k], P[k]);
+    const double vol = fabs(orient(P[0], P[1], P[2], P[3]));
+    if (vol == 0.0) {
+        w[0] = w[1] = w[2] = w[3] = 0.25;
+        return;
+    }
+    w[0] = fabs(orient(p, P[1], P[2], P[3])) / vol;
+    w[1] = fabs(orient(P[0], p, P[2], P[3])) / vol;
+    w[2] = fabs(orient(P[0], P[1], p, P[3])) / vol;
+    w[3] = fabs(orient(P[0], P[1], P[2], p)) / vol;
+}
+
+/* FastField::compute (grid_3d.cpp:1663-1721) */
+static void field_at(const orc_mesh* m, const double* p, int guess, double* E) {
+    E[0] = E[1] = E[2] = 0.0;
+    const int t = locate(m, p, guess);
+    if (t < 0) return;
+    double w[4];
+    weights(m, t, p, w);
+    for (int k = 0; k < 4; k++) {
+        double Ek[3];
+        orc_field_o1(m, m->tet_v[4 * t + k], Ek);
+        for (int d = 0; d < 3; d++) E[d] += w[k] * Ek[d];
+    }
+}
+
+double orc_potential_at(const orc_mesh* m, const double p[3], int32_t guess) {
+    const int t = locate(m, p, guess);
+    if (t < 0) return 0.0;
+    double w[4];
+    weights(m, t, p, w);
+    double v = 0.0;
+    for (int k = 0; k < 4; k++) v += w[k] * m->phi[m->tet_v[4 * t + k]];
+    return v;
+}
+
+/* Trajectory_3d (trajectory_3d.cpp:130-209, 303-332, 358-425, 583-676) */
+void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t guess, double dt0, double dt_min,
+               double tol, int32_t max_steps, int32_t stepper_limit, double top_z, orc_impact* out) {
+    static const double B[6][5] = {{0, 0, 0, 0, 0},
+                                   {1.0 / 5.0, 0, 0, 0, 0},
+                                   {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
+                                   {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0, 0, 0},
+                                   {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0, 0},
+                                   {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+    static const double C5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
+    static const double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 0.25};
+    double x[3] = {start[0], start[1], start[2]}, v[3] = {0, 0, 0};
+    double time = 0.0;
+    memset(out, 0, sizeof(*out));
+    int tet = locate(m, x, guess);
+    out->last_tet = tet;
+    memcpy(out->last_pos, x, sizeof(x));
+    if (tet < 0) {
+        out->status = -1;
+        memcpy(out->stop, x, sizeof(x));
+        return;
+    }
+    double E0[3];
+    field_at(m, x, tet, E0);
+    int status;
+    if (E0[0] == 0.0 && E0[1] == 0.0 && E0[2] == 0.0) {
+        status = 1;
+    } else {
+        status = 3;
+        double dt = dt0;
+        for (int it = 0; it < max_steps; it++) {
+            double nx[3], nv[3], used = dt;
+            int accepted = 0;
+            for (int tries = 0; tries < stepper_limit; tries++) {
+                if (dt < dt_min) dt = dt_min;
+                used = dt;
+                double dx[6][3], dv[6][3];
+                for (int s = 0; s < 6; s++) {
+                    double ps[3], vs[3];
+                    for (int d = 0; d < 3; d++) {
+                        ps[d] = x[d];
+                        vs[d] = v[d];
+                        for (int j = 0; j < s; j++) {
+                            ps[d] += B[s][j] * dx[j][d];
+                            vs[d] += B[s][j] * dv[j][d];
+                        }
+                    }
+                    double E[3];
+                    field_at(m, ps, tet, E);
+                    for (int d = 0; d < 3; d++) {
+                        dv[s][d] = E[d] * qm * dt;
+                        dx[s][d] = vs[d] * dt;
+                    }
+                }
+                double ex[3], ev[3];
+                for (int d = 0; d < 3; d++) {
+                    nx[d] = x[d];
+                    nv[d] = v[d];
+                    ex[d] = ev[d] = 0.0;
+                    for (int s = 0; s < 6; s++) {
+                        nx[d] += C5[s] * dx[s][d];
+                        nv[d] += C5[s] * dv[s][d];
+                        ex[d] += (C5[s] - C4[s]) * dx[s][d];
+                        ev[d] += (C5[s] - C4[s]) * dv[s][d];
+                    }
+                }
+                double rel = 0.0;
+                for (int d = 0; d < 3; d++) {
+                    if (nx[d] != 0.0 && fabs(ex[d] / nx[d]) > rel) rel = fabs(ex[d] / nx[d]);
+                    if (nv[d] != 0.0 && fabs(ev[d] / nv[d]) > rel) rel = fabs(ev[d] / nv[d]);
+                }
+                if (rel < tol || dt == dt_min) {
+                    if (rel != 0.0) {
+                        const double tmp = dt * pow(tol / rel, 0.25) * 0.9;
+                        if (tmp < dt) dt *= 1.1; else dt = tmp;
+                    }
+                    accepted = 1;
+                    break;
+                }
+                const double tmp = dt * pow(tol / rel, 0.25) * 0.9;
+                if (tmp > dt) dt *= 0.9; else dt = tmp;
+            }
+            if (!accepted) {
+                status = 2;
+                break;
+            }
+            const int nt = locate(m, nx, tet);
+            out->steps++;
+            if (nt < 0) {
+                out->last_tet = tet;
+                memcpy(out->last_pos, x, sizeof(x));
+                memcpy(x, nx, sizeof(x));
+                memcpy(v, nv, sizeof(v));
+                time += used;
+                tet = -1;
+                status = 5;
+                break;
+            }
+            memcpy(x, nx, sizeof(x));
+            memcpy(v, nv, sizeof(v));
+            time += used;
+            tet = nt;
+        }
+    }
+    if (tet >= 0) {
+        out->last_tet = tet;
+        memcpy(out->last_pos, x, sizeof(x));
+    }
+    out->last_phi = out->last_tet >= 0 ? orc_potential_at(m, out->last_pos, out->last_tet) : 0.0;
+    const double dtz = (top_z - x[2]) / v[2];
+    for (int d = 0; d < 3; d++) out->stop[d] = x[d] + dtz * v[d];
+    out->stop_time = time + dtz;
+    out->status = status;
+}

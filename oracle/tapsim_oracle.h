@@ -1,0 +1,76 @@
+/* CPU restatement of TAPSim's per-event hot path in FP64 (test oracle).
+ *
+ * This is test infrastructure: only tests/, __graft_entry__.smoke() and the
+ * CPU leg of bench.py load it, and only as the checker.  Each function cites
+ * the reference routine it restates (paths inside the reference tree).
+ * Arrays follow the layout of tg_mesh_desc (include/tapsim_gpu.h).
+ */
+#ifndef TAPSIM_ORACLE_H
+#define TAPSIM_ORACLE_H
+
+#include <stdint.h>
+
+typedef struct {
+    int32_t present, removable, neumann, dirichlet;
+    double epsilon, evap_field, charge_density, phi, mass;
+    int32_t evap_charge;
+} orc_type;
+
+typedef struct {
+    int32_t n;
+    const float* xyz;          /* [3n] */
+    int8_t* type;              /* [n], mutable */
+    const uint8_t* hull;       /* [n] */
+    const int32_t* row_ptr;    /* [n+1] */
+    const int32_t* col;        /* [nnz] */
+    double* c;                 /* [nnz] coupling, mutable */
+    const double* geom;        /* [nnz] area(0.5d)/d */
+    const uint8_t* area_pos;   /* [nnz] */
+    double* phi;               /* [n] mutable */
+    double* q;                 /* [n] mutable (charge term) */
+    const double* volume;      /* [n] or NULL */
+    int32_t ntets;
+    const int32_t* tet_v;      /* [4T] */
+    const int32_t* tet_n;      /* [4T] */
+    const orc_type* types;     /* [128] by id */
+    uint8_t* surface;          /* [n] surface flag, mutable */
+} orc_mesh;
+
+/* relative residual ||r||/||b|| (r over free rows, computePotential rule) */
+double orc_residual(const orc_mesh* m);
+/* SOR sweeps in ascending node order until the relative residual is <= tol;
+ * returns sweeps done, -1 on the cap.  omega = 1 is Gauss-Seidel. */
+int64_t orc_solve(orc_mesh* m, double tol, int64_t max_sweeps, double omega, double* rel_out);
+/* n reference-style sweeps (Gauss-Seidel, ascending order); returns max |delta| of the last */
+double orc_relax_cycles(orc_mesh* m, int32_t n);
+/* Grid_3d::Table::field_o1; returns 0 when the 3x3 system is singular */
+int orc_field_o1(const orc_mesh* m, int32_t i, double E[3]);
+/* Surface_3d::Table::init; returns the number of surface cells */
+int32_t orc_surface_init(orc_mesh* m, int32_t vacuum_id);
+/* specific fields + probabilities + evapMaximum + apex over the surface set */
+typedef struct {
+    int32_t candidate, apex, num_surface;
+    float best, second;
+    double sum;
+} orc_select_info;
+void orc_select(const orc_mesh* m, float* ratio_out /* [n] or NULL */, orc_select_info* info);
+/* evap_takeAway; returns the number of detached cells (written to detached) */
+int32_t orc_take_away(orc_mesh* m, int32_t node, int32_t vacuum_id, int32_t* detached, int32_t cap);
+/* update_coordination */
+void orc_update_coordination(orc_mesh* m);
+/* one ion: Trajectory_3d init/integrate/extrapolate in FP64 */
+typedef struct {
+    double stop[3];
+    double stop_time;
+    double last_pos[3];
+    int32_t last_tet;
+    double last_phi;
+    int32_t steps;
+    int32_t status;
+} orc_impact;
+void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t tet_guess, double dt0, double dt_min,
+               double tol, int32_t max_steps, int32_t stepper_limit, double top_z, orc_impact* out);
+/* Grid_3d::potential(pos, tet) */
+double orc_potential_at(const orc_mesh* m, const double p[3], int32_t tet_guess);
+
+#endif

@@ -1,0 +1,99 @@
+// Shared device definitions for the TAPSim hot-path kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tgd {
+
+// per-node flag bits
+enum : uint8_t {
+    F_HULL = 1,        // Geometry_3d::NodeData::boundary
+    F_DIRICHLET = 2,   // Grid_3d::Node DIRICHLET
+    F_NEUMANN = 4,     // Grid_3d::Node NEUMANN
+    F_SURFACE = 8,     // member of the Surface_3d::Table node set
+    F_FREE = 16        // listed in a free-row list
+};
+
+// device-side status bits (accumulated, read by the host after a call)
+enum : int {
+    S_NAN = 1,
+    S_SINGULAR = 2,
+    S_NOT_SURFACE = 4,
+    S_WALK_LIMIT = 8,
+    S_UNKNOWN_TYPE = 16,
+    S_ZERO_WEIGHT = 32
+};
+
+struct DType {
+    float epsilon;
+    float evap_field;
+    float charge_density;
+    float phi;
+    uint8_t removable, neumann, dirichlet, present;
+};
+
+constexpr double kEpsilon0 = 8.85418781762e-12;  // As/(Vm), grid_3d.h:283
+
+__device__ __forceinline__ void atomic_max_double_nonneg(double* addr, double v) {
+    // non-negative doubles order like their bit patterns
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// monotone map float -> uint32 (total order, -0 < +0 ignored)
+__device__ __forceinline__ uint32_t float_order_key(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ double warp_max_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum of a double into *out (one atomicAdd per block).
+template <int BLOCK>
+__device__ __forceinline__ void block_sum_atomic(double v, double* out) {
+    __shared__ double red[BLOCK / 32];
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double s = lane < BLOCK / 32 ? red[lane] : 0.0;
+        s = warp_sum(s);
+        if (lane == 0 && s != 0.0) atomicAdd(out, s);
+    }
+    __syncthreads();
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void block_max_atomic_u64(unsigned long long v, unsigned long long* out) {
+    __shared__ unsigned long long red[BLOCK / 32];
+    v = warp_max_u64(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned long long s = lane < BLOCK / 32 ? red[lane] : 0ull;
+        s = warp_max_u64(s);
+        if (lane == 0 && s != 0ull) atomicMax(out, s);
+    }
+    __syncthreads();
+}
+
+}  // namespace tgd

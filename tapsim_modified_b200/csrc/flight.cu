@@ -1,0 +1,329 @@
+// Ion flights: one thread per ion.  Restates Trajectory_3d (tapsim/
+// trajectory_3d.cpp) in FP64: the embedded Cash-Karp Runge-Kutta step
+// (o5_integrator, :583-676, tableau of Cash & Karp 1990), the
+// error-restricted step control (errorRestricted_stepper, :358-425), the
+// loop that ends when the ion leaves the mesh (integrate, :130-209) and the
+// linear extrapolation to the top plane (extrapolate, :303-332).  The field
+// at a point is the barycentric interpolation of the per-vertex field_o1 of
+// the enclosing tetrahedron (Grid_3d::FastField::compute,
+// grid_3d.cpp:1663-1721, with the weights of tetWeights,
+// geometry_3d.cpp:916-980); the tetrahedron comes from a visibility walk
+// (findTetrahedron, geometry_3d.cpp:988-1044) whose start face rotates
+// instead of being drawn with rand().
+#include "kernels.cuh"
+
+namespace tgd {
+namespace {
+
+constexpr int kBlock = 128;
+
+__constant__ int kFaceDev[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};
+
+struct V3 {
+    double x, y, z;
+};
+__device__ __forceinline__ V3 ld3(const float* p, int i) { return {p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+
+__device__ __forceinline__ double orient(V3 a, V3 b, V3 c, V3 p) {
+    const double ux = b.x - a.x, uy = b.y - a.y, uz = b.z - a.z;
+    const double vx = c.x - a.x, vy = c.y - a.y, vz = c.z - a.z;
+    const double wx = p.x - a.x, wy = p.y - a.y, wz = p.z - a.z;
+    return ux * (vy * wz - vz * wy) - uy * (vx * wz - vz * wx) + uz * (vx * wy - vy * wx);
+}
+
+// Sign of orient(a,b,c,p), exact for the points snapped to the power-of-two
+// grid the host Delaunay builder uses (|coordinate| <= 2^40 quanta): a double
+// evaluation with a forward error bound, and an exact 128-bit integer
+// evaluation when the bound does not certify the sign.  The walk thereby
+// decides every face consistently (a point on a shared face, such as an ion
+// starting at a mesh vertex, is never "beyond" it from both sides), which is
+// what makes the visibility walk terminate, as the reference's exact
+// Predicates::orient3d does (geometry_3d.cpp:1750-1768).
+__device__ int orient_sign(V3 a, V3 b, V3 c, V3 p, double snap) {
+    const double ux = b.x - a.x, uy = b.y - a.y, uz = b.z - a.z;
+    const double vx = c.x - a.x, vy = c.y - a.y, vz = c.z - a.z;
+    const double wx = p.x - a.x, wy = p.y - a.y, wz = p.z - a.z;
+    const double m0 = vy * wz - vz * wy, m1 = vx * wz - vz * wx, m2 = vx * wy - vy * wx;
+    const double det = ux * m0 - uy * m1 + uz * m2;
+    const double perm = fabs(ux) * (fabs(vy * wz) + fabs(vz * wy)) + fabs(uy) * (fabs(vx * wz) + fabs(vz * wx)) +
+                        fabs(uz) * (fabs(vx * wy) + fabs(vy * wx));
+    const double bound = 16.0 * 1.1102230246251565e-16 * perm;
+    if (det > bound) return 1;
+    if (det < -bound) return -1;
+    const double lim = 1.0995116277760000e12;  // 2^40
+    const double px = p.x * snap, py = p.y * snap, pz = p.z * snap;
+    if (fabs(px) > lim || fabs(py) > lim || fabs(pz) > lim) return det > 0.0 ? 1 : (det < 0.0 ? -1 : 0);
+    const long long ax = __double2ll_rn(a.x * snap), ay = __double2ll_rn(a.y * snap), az = __double2ll_rn(a.z * snap);
+    const long long Ux = __double2ll_rn(b.x * snap) - ax, Uy = __double2ll_rn(b.y * snap) - ay, Uz = __double2ll_rn(b.z * snap) - az;
+    const long long Vx = __double2ll_rn(c.x * snap) - ax, Vy = __double2ll_rn(c.y * snap) - ay, Vz = __double2ll_rn(c.z * snap) - az;
+    const long long Wx = __double2ll_rn(px) - ax, Wy = __double2ll_rn(py) - ay, Wz = __double2ll_rn(pz) - az;
+    const __int128 M0 = (__int128)Vy * Wz - (__int128)Vz * Wy;
+    const __int128 M1 = (__int128)Vx * Wz - (__int128)Vz * Wx;
+    const __int128 M2 = (__int128)Vx * Wy - (__int128)Vy * Wx;
+    const __int128 e = (__int128)Ux * M0 - (__int128)Uy * M1 + (__int128)Uz * M2;
+    return e > 0 ? 1 : (e < 0 ? -1 : 0);
+}
+
+// Returns the tetrahedron holding p, -1 when p is outside the mesh, -2 when
+// the walk exceeded `limit` steps.
+__device__ int locate(const DevMesh& m, V3 p, int t, int limit, unsigned& rot) {
+    if (t < 0) return -1;
+    for (int step = 0; step < limit; step++) {
+        const int* v = m.tet_v + 4 * t;
+        int next = -1;
+        bool moved = false;
+        const unsigned r = rot++;
+        for (int j = 0; j < 4; j++) {
+            const int k = (int)((r + j) & 3);
+            const V3 a = ld3(m.xyz, v[kFaceDev[k][0]]), b = ld3(m.xyz, v[kFaceDev[k][1]]), c = ld3(m.xyz, v[kFaceDev[k][2]]);
+            if (orient_sign(a, b, c, p, m.snap) < 0) {
+                next = m.tet_n[4 * t + k];
+                moved = true;
+                break;
+            }
+        }
+        if (!moved) return t;
+        if (next < 0) return -1;
+        t = next;
+    }
+    return -2;
+}
+
+// Barycentric weights (tetWeights): |sub-volume| / |volume|, 1/4 each for a
+// flat tetrahedron.
+__device__ void weights(const DevMesh& m, int t, V3 p, double w[4]) {
+    const int* v = m.tet_v + 4 * t;
+    const V3 P[4] = {ld3(m.xyz, v[0]), ld3(m.xyz, v[1]), ld3(m.xyz, v[2]), ld3(m.xyz, v[3])};
+    const double vol = fabs(orient(P[0], P[1], P[2], P[3]));
+    if (vol == 0.0) {
+        w[0] = w[1] = w[2] = w[3] = 0.25;
+        return;
+    }
+    w[0] = fabs(orient(p, P[1], P[2], P[3])) / vol;
+    w[1] = fabs(orient(P[0], p, P[2], P[3])) / vol;
+    w[2] = fabs(orient(P[0], P[1], p, P[3])) / vol;
+    w[3] = fabs(orient(P[0], P[1], P[2], p)) / vol;
+}
+
+// field_o1 of one node (same restatement as in surface.cu)
+__device__ V3 node_field(const DevMesh& m, int i) {
+    V3 E{0, 0, 0};
+    if (m.flags[i] & F_HULL) return E;
+    const double xi = m.xyz[3 * i], yi = m.xyz[3 * i + 1], zi = m.xyz[3 * i + 2];
+    const double pi = m.phi64[i];
+    double a00 = 0, a01 = 0, a02 = 0, a11 = 0, a12 = 0, a22 = 0, b0 = 0, b1 = 0, b2 = 0;
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+        if (m.c64[q] == 0.0) continue;
+        const int j = m.col[q];
+        const double dx = (double)m.xyz[3 * j] - xi, dy = (double)m.xyz[3 * j + 1] - yi, dz = (double)m.xyz[3 * j + 2] - zi;
+        const double dp = m.phi64[j] - pi;
+        a00 += dx * dx; a01 += dx * dy; a02 += dx * dz;
+        a11 += dy * dy; a12 += dy * dz; a22 += dz * dz;
+        b0 += dp * dx; b1 += dp * dy; b2 += dp * dz;
+    }
+    const double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+    const double det = a00 * c00 + a01 * c01 + a02 * c02;
+    if (det == 0.0 || !(det == det)) {
+        atomicOr(m.status, S_SINGULAR);
+        return E;
+    }
+    const double c11 = a00 * a22 - a02 * a02, c12 = a01 * a02 - a00 * a12, c22 = a00 * a11 - a01 * a01;
+    const double inv = 1.0 / det;
+    E.x = -(c00 * b0 + c01 * b1 + c02 * b2) * inv;
+    E.y = -(c01 * b0 + c11 * b1 + c12 * b2) * inv;
+    E.z = -(c02 * b0 + c12 * b1 + c22 * b2) * inv;
+    return E;
+}
+
+// Per-thread cache of the vertex fields of the last two tetrahedra.
+struct FieldCache {
+    int tet[2];
+    V3 f[2][4];
+    int next;
+};
+
+__device__ bool fast_field(const DevMesh& m, FieldCache& fc, V3 p, int guess, int limit, unsigned& rot, V3* E) {
+    const int t = locate(m, p, guess, limit, rot);
+    *E = V3{0, 0, 0};
+    if (t == -2) return false;
+    if (t < 0) return true;
+    int s = -1;
+    if (fc.tet[0] == t) s = 0;
+    else if (fc.tet[1] == t) s = 1;
+    if (s < 0) {
+        s = fc.next;
+        fc.next ^= 1;
+        fc.tet[s] = t;
+        for (int k = 0; k < 4; k++) fc.f[s][k] = node_field(m, m.tet_v[4 * t + k]);
+    }
+    double w[4];
+    weights(m, t, p, w);
+    for (int k = 0; k < 4; k++) {
+        E->x += w[k] * fc.f[s][k].x;
+        E->y += w[k] * fc.f[s][k].y;
+        E->z += w[k] * fc.f[s][k].z;
+    }
+    return true;
+}
+
+__device__ double potential_at(const DevMesh& m, V3 p, int t) {
+    const int* v = m.tet_v + 4 * t;
+    double w[4];
+    weights(m, t, p, w);
+    return w[0] * m.phi64[v[0]] + w[1] * m.phi64[v[1]] + w[2] * m.phi64[v[2]] + w[3] * m.phi64[v[3]];
+}
+
+__global__ void k_trace(DevMesh m, int nIons, const float* start, const float* vel, const float* qm,
+                        const int32_t* guess, TraceParams tp, ImpactOut* out) {
+    const int ion = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ion >= nIons) return;
+    // Cash-Karp tableau
+    const double B[6][5] = {{0, 0, 0, 0, 0},
+                            {1.0 / 5.0, 0, 0, 0, 0},
+                            {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
+                            {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0, 0, 0},
+                            {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0, 0},
+                            {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+    const double C5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
+    const double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
+
+    ImpactOut res;
+    unsigned rot = (unsigned)ion * 7u;
+    FieldCache fc;
+    fc.tet[0] = fc.tet[1] = -1;
+    fc.next = 0;
+    V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
+    V3 v{0, 0, 0};
+    if (vel) v = V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]};
+    const double k = qm[ion];
+    double time = 0.0;
+    int tet = locate(m, x, guess ? guess[ion] : 0, tp.walk_limit, rot);
+    res.steps = 0;
+    res.last_tet = tet;
+    res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
+    res.last_phi = 0.0f;
+    if (tet < 0) {
+        if (tet == -2) atomicOr(m.status, S_WALK_LIMIT);
+        res.status = -1;  // Trajectory_3d::init: initial point is outside
+        res.stop[0] = (float)x.x; res.stop[1] = (float)x.y; res.stop[2] = (float)x.z;
+        res.stop_time = 0.0f;
+        out[ion] = res;
+        return;
+    }
+    V3 E0;
+    if (!fast_field(m, fc, x, tet, tp.walk_limit, rot, &E0)) atomicOr(m.status, S_WALK_LIMIT);
+    int status;
+    if (E0.x == 0.0 && E0.y == 0.0 && E0.z == 0.0) {
+        status = 1;  // NO_FIELD
+    } else {
+        status = 3;  // ITERATION_LIMIT_PASSED unless another exit is taken
+        double dt = tp.dt0;
+        for (int it = 0; it < tp.max_steps; it++) {
+            V3 nx, nv;
+            double used = dt;
+            bool accepted = false;
+            for (int tries = 0; tries < tp.stepper_limit; tries++) {
+                if (dt < tp.dt_min) dt = tp.dt_min;
+                used = dt;
+                V3 dxs[6], dvs[6];
+                bool walkOk = true;
+                for (int s = 0; s < 6; s++) {
+                    V3 ps = x, vs = v;
+                    for (int j = 0; j < s; j++) {
+                        ps.x += B[s][j] * dxs[j].x; ps.y += B[s][j] * dxs[j].y; ps.z += B[s][j] * dxs[j].z;
+                        vs.x += B[s][j] * dvs[j].x; vs.y += B[s][j] * dvs[j].y; vs.z += B[s][j] * dvs[j].z;
+                    }
+                    V3 E;
+                    walkOk &= fast_field(m, fc, ps, tet, tp.walk_limit, rot, &E);
+                    dvs[s] = V3{E.x * k * dt, E.y * k * dt, E.z * k * dt};
+                    dxs[s] = V3{vs.x * dt, vs.y * dt, vs.z * dt};
+                }
+                if (!walkOk) atomicOr(m.status, S_WALK_LIMIT);
+                nx = x; nv = v;
+                V3 ex{0, 0, 0}, evv{0, 0, 0};
+                for (int s = 0; s < 6; s++) {
+                    nx.x += C5[s] * dxs[s].x; nx.y += C5[s] * dxs[s].y; nx.z += C5[s] * dxs[s].z;
+                    nv.x += C5[s] * dvs[s].x; nv.y += C5[s] * dvs[s].y; nv.z += C5[s] * dvs[s].z;
+                    const double dc = C5[s] - C4[s];
+                    ex.x += dc * dxs[s].x; ex.y += dc * dxs[s].y; ex.z += dc * dxs[s].z;
+                    evv.x += dc * dvs[s].x; evv.y += dc * dvs[s].y; evv.z += dc * dvs[s].z;
+                }
+                double rel = 0.0;
+                const double pv[6] = {nx.x, nx.y, nx.z, nv.x, nv.y, nv.z};
+                const double ev[6] = {ex.x, ex.y, ex.z, evv.x, evv.y, evv.z};
+                for (int c = 0; c < 6; c++)
+                    if (pv[c] != 0.0) rel = fmax(rel, fabs(ev[c] / pv[c]));
+                if (rel < tp.tol || dt == tp.dt_min) {
+                    if (rel != 0.0) {
+                        const double tmp = dt * pow(tp.tol / rel, 0.25) * 0.9;
+                        if (tmp < dt) dt *= 1.1; else dt = tmp;
+                    }
+                    accepted = true;
+                    break;
+                }
+                const double tmp = dt * pow(tp.tol / rel, 0.25) * 0.9;
+                if (tmp > dt) dt *= 0.9; else dt = tmp;
+            }
+            if (!accepted) {
+                status = 2;  // STEPPER_LIMIT_PASSED
+                break;
+            }
+            const int nt = locate(m, nx, tet, tp.walk_limit, rot);
+            if (nt == -2) atomicOr(m.status, S_WALK_LIMIT);
+            res.steps++;
+            if (nt < 0) {
+                // left the mesh: the previous point is the last inside it
+                res.last_tet = tet;
+                res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
+                x = nx;
+                v = nv;
+                time += used;
+                tet = -1;
+                status = 5;  // SYSTEM_LIMIT_PASSED
+                break;
+            }
+            x = nx;
+            v = nv;
+            time += used;
+            tet = nt;
+        }
+    }
+    if (tet >= 0) {
+        res.last_tet = tet;
+        res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
+    }
+    res.last_phi = res.last_tet >= 0
+                       ? (float)potential_at(m, V3{res.last_pos[0], res.last_pos[1], res.last_pos[2]}, res.last_tet)
+                       : 0.0f;
+    // extrapolate to the top plane along the last velocity
+    const double dtz = (tp.top_z - x.z) / v.z;
+    res.stop[0] = (float)(x.x + dtz * v.x);
+    res.stop[1] = (float)(x.y + dtz * v.y);
+    res.stop[2] = (float)(x.z + dtz * v.z);
+    res.stop_time = (float)(time + dtz);
+    res.status = status;
+    out[ion] = res;
+}
+
+__global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t* guess, int limit, float* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned rot = (unsigned)i;
+    const V3 p{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+    const int t = locate(m, p, guess ? guess[i] : 0, limit, rot);
+    if (t == -2) atomicOr(m.status, S_WALK_LIMIT);
+    out[i] = t >= 0 ? (float)potential_at(m, p, t) : 0.0f;
+}
+
+}  // namespace
+
+void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
+                  const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s) {
+    if (nIons > 0) k_trace<<<(nIons + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out);
+}
+void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit, float* out,
+                         cudaStream_t s) {
+    if (n > 0) k_potential_at<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, n, xyz, guess, walkLimit, out);
+}
+
+}  // namespace tgd

@@ -1,0 +1,979 @@
+// tg_handle: device state of one mesh and the C-ABI entry points that drive
+// the kernels (include/tapsim_gpu.h).  Host code only; kernels live in
+// relax.cu, surface.cu and flight.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <vector>
+
+#include "../../include/tapsim_gpu.h"
+#include "kernels.cuh"
+
+using namespace tgd;
+
+static_assert(sizeof(ImpactOut) == sizeof(tg_impact), "impact layout");
+
+namespace {
+
+thread_local std::string g_error;
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(&p, count * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+}  // namespace
+
+namespace tgapi {
+void set_process_error(const std::string& msg) { g_error = msg; }
+}  // namespace tgapi
+
+struct tg_handle {
+    int n = 0, nnz = 0, ntets = 0, ncol = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    float top_z = 0.0f;
+    double snap = 1.0;
+    std::vector<tg_type> types;          // by id, id < 0 means absent
+    std::vector<int32_t> segStart;       // host mirror
+    std::vector<int32_t> countV, countN;  // host mirrors
+    int32_t countAllV = 0, countAllN = 0;
+    int32_t surfSlots = 0;
+    std::vector<int32_t> h_node_tet;
+    std::vector<float> h_xyz;
+    std::vector<int8_t> h_type;           // host mirror of the type ids
+
+    // device arrays
+    DBuf<float> xyz;
+    DBuf<int8_t> type, typeScratch;
+    DBuf<uint8_t> flags, area_pos;
+    DBuf<int32_t> row_ptr, col, rev, colour, tet_v, tet_n, node_tet;
+    DBuf<double> geom, volume, c64, ceff64, diag64, q64, phi64;
+    DBuf<float> ceff32, diag32;
+    DBuf<DType> dtypes;
+    DBuf<int> status;
+    DBuf<int32_t> rowsV, rowsN, allV, allN, segStartD, countVD, countND, countAllD;
+    DBuf<int32_t> surfList, surfSlot, surfCount;
+    DBuf<float> surfRatio;
+    DBuf<float> cgbuf;  // 10 vectors of n floats
+    DBuf<double> scalV, scalN;
+    int maxInnerAlloc = 0;
+    DBuf<double> acc;
+    DBuf<unsigned long long> keys;
+    DBuf<int32_t> result;
+    DBuf<int32_t> local, localCount, localScratch;
+    // staging for per-call inputs/outputs
+    DBuf<int32_t> stageI;
+    DBuf<double> stageD;
+    DBuf<float> stageF;
+    DBuf<ImpactOut> stageImpact;
+
+    bool bnormValid = false;
+    double bnorm2 = 0.0;
+    bool selValid = false;
+    tg_select_info sel{};
+    int vacuumId = -1;
+
+    DevMesh dm() {
+        DevMesh m;
+        m.n = n;
+        m.nnz = nnz;
+        m.ntets = ntets;
+        m.xyz = xyz.p;
+        m.type = type.p;
+        m.flags = flags.p;
+        m.row_ptr = row_ptr.p;
+        m.col = col.p;
+        m.rev = rev.p;
+        m.geom = geom.p;
+        m.area_pos = area_pos.p;
+        m.volume = volume.p;
+        m.c64 = c64.p;
+        m.ceff64 = ceff64.p;
+        m.ceff32 = ceff32.p;
+        m.diag64 = diag64.p;
+        m.diag32 = diag32.p;
+        m.q64 = q64.p;
+        m.phi64 = phi64.p;
+        m.colour = colour.p;
+        m.tet_v = tet_v.p;
+        m.tet_n = tet_n.p;
+        m.node_tet = node_tet.p;
+        m.types = dtypes.p;
+        m.status = status.p;
+        m.snap = snap;
+        return m;
+    }
+    RowLists rl() {
+        RowLists r;
+        r.rowsV = rowsV.p;
+        r.rowsN = rowsN.p;
+        r.segStart = segStartD.p;
+        r.countV = countVD.p;
+        r.countN = countND.p;
+        r.allV = allV.p;
+        r.allN = allN.p;
+        r.countAll = countAllD.p;
+        r.ncolours = ncol;
+        return r;
+    }
+    Surface sf() {
+        Surface s;
+        s.list = surfList.p;
+        s.slot = surfSlot.p;
+        s.count = surfCount.p;
+        s.ratio = surfRatio.p;
+        s.capacity = n;
+        return s;
+    }
+    CGVectors cg(int which) {
+        CGVectors v;
+        float* base = cgbuf.p + (size_t)which * 5 * n;
+        v.x = base;
+        v.r = base + (size_t)n;
+        v.z = base + 2 * (size_t)n;
+        v.p = base + 3 * (size_t)n;
+        v.ap = base + 4 * (size_t)n;
+        v.scal = which == 0 ? scalV.p : scalN.p;
+        return v;
+    }
+};
+
+namespace {
+
+int fail(tg_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    g_error = msg;
+    return code;
+}
+
+int cuda_check(tg_handle* h, cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return TG_OK;
+    return fail(h, TG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(expr)                                              \
+    do {                                                      \
+        const int _rc = cuda_check(h, (expr), #expr);         \
+        if (_rc != TG_OK) return _rc;                         \
+    } while (0)
+
+// Synchronises the stream and maps the device status word to a code.
+int sync_status(tg_handle* h, const char* where) {
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    int st = 0;
+    CK(cudaMemcpy(&st, h->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st == 0) return TG_OK;
+    CK(cudaMemset(h->status.p, 0, sizeof(int)));
+    std::string what = where;
+    if (st & S_NAN) return fail(h, TG_ERR_NAN, what + ": NaN");
+    if (st & S_SINGULAR) return fail(h, TG_ERR_SINGULAR, what + ": singular field_o1 system");
+    if (st & S_NOT_SURFACE) return fail(h, TG_ERR_NOT_SURFACE, what + ": node is not a surface cell");
+    if (st & S_WALK_LIMIT) return fail(h, TG_ERR_WALK_LIMIT, what + ": tetrahedron walk limit");
+    if (st & S_UNKNOWN_TYPE) return fail(h, TG_ERR_UNKNOWN_TYPE, what + ": unknown cell type");
+    return fail(h, TG_ERR_CUDA, what + ": device status");
+}
+
+template <typename T>
+int stage(tg_handle* h, DBuf<T>& b, size_t count) {
+    if (b.n >= count) return TG_OK;
+    return cuda_check(h, b.alloc(std::max<size_t>(count, 1024)), "staging alloc");
+}
+
+int refresh_counts(tg_handle* h) {
+    CK(cudaMemcpyAsync(h->countV.data(), h->countVD.p, sizeof(int32_t) * h->ncol, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->countN.data(), h->countND.p, sizeof(int32_t) * h->ncol, cudaMemcpyDeviceToHost, h->stream));
+    int32_t ca[2];
+    CK(cudaMemcpyAsync(ca, h->countAllD.p, sizeof(ca), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&h->surfSlots, h->surfCount.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->countAllV = ca[0];
+    h->countAllN = ca[1];
+    h->surfSlots = std::min(h->surfSlots, h->n);
+    return TG_OK;
+}
+
+int ensure_bnorm(tg_handle* h) {
+    if (h->bnormValid) return TG_OK;
+    DevMesh m = h->dm();
+    CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
+    launch_bnorm(m, h->allV.p, h->countAllV, h->acc.p, h->stream);
+    launch_bnorm(m, h->allN.p, h->countAllN, h->acc.p, h->stream);
+    CK(cudaMemcpyAsync(&h->bnorm2, h->acc.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    const int rc = sync_status(h, "bnorm");
+    if (rc != TG_OK) return rc;
+    h->bnormValid = true;
+    return TG_OK;
+}
+
+// one coloured sweep over all free rows; dev receives max |delta| when non-null
+void sweep_all(tg_handle* h, double* devAcc) {
+    DevMesh m = h->dm();
+    for (int c = 0; c < h->ncol; c++) {
+        launch_sweep64(m, h->rowsV.p + h->segStart[c], h->countV[c], devAcc, h->stream);
+        launch_sweep64(m, h->rowsN.p + h->segStart[c], h->countN[c], devAcc, h->stream);
+    }
+}
+
+// regression slope of the deviation queue as Grid_3d::Table::relax computes
+// it (grid_3d.cpp:628-654)
+bool stagnated(const std::deque<double>& queue, unsigned queueSize, unsigned cycleSize) {
+    if (queueSize == 0 || queue.size() != queueSize) return false;
+    const double xMean = (queueSize - 1) / 2.0;
+    double yMean = 0.0;
+    for (double v : queue) yMean += v;
+    yMean /= queueSize;
+    double num = 0.0;
+    int x = 0;
+    for (double v : queue) num += (x++ - xMean) * (v - yMean);
+    double den = queueSize;
+    den *= queueSize;
+    den -= 1;
+    den *= queueSize;
+    den *= cycleSize;
+    den /= 12.0;
+    return num / den == 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tg_last_error(const tg_handle* h) { return h ? h->err.c_str() : g_error.c_str(); }
+int tg_num_nodes(const tg_handle* h) { return h ? h->n : 0; }
+
+int tg_create(const tg_mesh_desc* d, tg_handle** out) {
+    if (!d || !out || d->num_nodes <= 0 || !d->xyz || !d->type_id || !d->row_ptr || !d->col || !d->coupling ||
+        !d->types || d->num_types <= 0)
+        return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: incomplete mesh description");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, TG_ERR_CUDA, "tg_create: no CUDA device");
+    tg_handle* h = new tg_handle();
+    const int n = d->num_nodes;
+    const int nnz = d->row_ptr[n];
+    h->n = n;
+    h->nnz = nnz;
+    h->ntets = d->num_tets;
+    h->types.assign(128, tg_type{});
+    for (auto& t : h->types) t.id = -1;
+    for (int k = 0; k < d->num_types; k++) {
+        const tg_type& t = d->types[k];
+        if (t.id < 0 || t.id > 127) {
+            delete h;
+            return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: type id out of range");
+        }
+        h->types[t.id] = t;
+    }
+    std::vector<DType> dt(128);
+    for (int k = 0; k < 128; k++) {
+        const tg_type& t = h->types[k];
+        DType& o = dt[k];
+        o.present = t.id >= 0;
+        o.epsilon = t.epsilon;
+        o.evap_field = t.evap_field;
+        o.charge_density = t.charge_density;
+        o.phi = t.phi;
+        o.removable = t.removable != 0;
+        o.neumann = t.neumann != 0;
+        o.dirichlet = t.dirichlet != 0;
+    }
+    h->h_type.assign(d->type_id, d->type_id + n);
+    std::vector<uint8_t> flags(n, 0);
+    for (int i = 0; i < n; i++) {
+        const int t = d->type_id[i];
+        if (t < 0 || !dt[t].present) {
+            delete h;
+            return fail(nullptr, TG_ERR_UNKNOWN_TYPE, "tg_create: node with unknown type id");
+        }
+        if (d->hull && d->hull[i]) flags[i] |= F_HULL;
+        if (dt[t].dirichlet) flags[i] |= F_DIRICHLET;
+        if (dt[t].neumann) flags[i] |= F_NEUMANN;
+    }
+    // reverse index, geometric factor, positive-area flag
+    std::vector<int32_t> rev(nnz);
+    std::vector<double> geom(nnz);
+    std::vector<uint8_t> apos(nnz);
+    for (int i = 0; i < n; i++)
+        for (int q = d->row_ptr[i]; q < d->row_ptr[i + 1]; q++) {
+            const int j = d->col[q];
+            if (j < 0 || j >= n) {
+                delete h;
+                return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: neighbour index out of range");
+            }
+            const int32_t* b = d->col + d->row_ptr[j];
+            const int32_t* e = d->col + d->row_ptr[j + 1];
+            const int32_t* f = std::lower_bound(b, e, (int32_t)i);
+            if (f == e || *f != i) {
+                delete h;
+                return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: adjacency is not symmetric or not sorted");
+            }
+            rev[q] = (int32_t)(f - d->col);
+            if (d->geom) {
+                geom[q] = d->geom[q];
+            } else {
+                const double e1 = dt[d->type_id[i]].epsilon, e2 = dt[d->type_id[j]].epsilon;
+                geom[q] = d->coupling[q] / (2.0 * e1 * e2 / (e1 + e2));
+            }
+            apos[q] = d->area_pos ? d->area_pos[q] : (geom[q] != 0.0);
+        }
+    // greedy colouring of the whole Delaunay graph
+    std::vector<int32_t> colour(n, -1);
+    int ncol = 0;
+    {
+        std::vector<int> mark(128, -1);
+        for (int i = 0; i < n; i++) {
+            for (int q = d->row_ptr[i]; q < d->row_ptr[i + 1]; q++) {
+                const int c = colour[d->col[q]];
+                if (c >= 0 && c < 128) mark[c] = i;
+            }
+            int c = 0;
+            while (c < 128 && mark[c] == i) c++;
+            colour[i] = c;
+            ncol = std::max(ncol, c + 1);
+        }
+    }
+    if (ncol > 64) {
+        delete h;
+        return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: more than 64 colours");
+    }
+    h->ncol = ncol;
+    std::vector<int32_t> csize(ncol, 0);
+    for (int i = 0; i < n; i++) csize[colour[i]]++;
+    h->segStart.assign(ncol, 0);
+    for (int c = 1; c < ncol; c++) h->segStart[c] = h->segStart[c - 1] + csize[c - 1];
+    h->countV.assign(ncol, 0);
+    h->countN.assign(ncol, 0);
+    std::vector<int32_t> rowsV(n, -1), rowsN(n, -1), allV, allN;
+    for (int i = 0; i < n; i++) {
+        if (flags[i] & F_DIRICHLET) continue;
+        const int c = colour[i];
+        if (flags[i] & F_NEUMANN) {
+            rowsN[h->segStart[c] + h->countN[c]++] = i;
+            allN.push_back(i);
+        } else {
+            rowsV[h->segStart[c] + h->countV[c]++] = i;
+            allV.push_back(i);
+        }
+        flags[i] |= F_FREE;
+    }
+    h->countAllV = (int32_t)allV.size();
+    h->countAllN = (int32_t)allN.size();
+    allV.resize(n, -1);
+    allN.resize(n, -1);
+    std::vector<double> phi(n), q(n, 0.0);
+    for (int i = 0; i < n; i++) {
+        phi[i] = d->phi ? (double)d->phi[i] : (double)dt[d->type_id[i]].phi;
+        if (d->volume) q[i] = d->volume[i] * (double)dt[d->type_id[i]].charge_density / kEpsilon0;
+    }
+    h->top_z = -1e30f;
+    double amax = 0.0;
+    for (int i = 0; i < n; i++) {
+        h->top_z = std::max(h->top_z, d->xyz[3 * i + 2]);
+        for (int k = 0; k < 3; k++) amax = std::max(amax, std::fabs((double)d->xyz[3 * i + k]));
+    }
+    // the integer grid of the host Delaunay builder (delaunay.cpp): |x| <= 2^40
+    h->snap = amax > 0.0 ? std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 40) / amax))) : 1.0;
+    h->h_xyz.assign(d->xyz, d->xyz + 3 * (size_t)n);
+    if (d->node_tet) h->h_node_tet.assign(d->node_tet, d->node_tet + n);
+
+    auto up = [&](auto& buf, const auto* src, size_t count) -> cudaError_t {
+        cudaError_t e = buf.alloc(count);
+        if (e != cudaSuccess) return e;
+        if (count && src) return cudaMemcpy(buf.p, src, count * sizeof(*src), cudaMemcpyHostToDevice);
+        return cudaSuccess;
+    };
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    chk(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    chk(up(h->xyz, d->xyz, 3 * (size_t)n));
+    chk(up(h->type, d->type_id, n));
+    chk(h->typeScratch.alloc(n));
+    chk(up(h->flags, flags.data(), n));
+    chk(up(h->area_pos, apos.data(), nnz));
+    chk(up(h->row_ptr, d->row_ptr, n + 1));
+    chk(up(h->col, d->col, nnz));
+    chk(up(h->rev, rev.data(), nnz));
+    chk(up(h->colour, colour.data(), n));
+    chk(up(h->geom, geom.data(), nnz));
+    if (d->volume) chk(up(h->volume, d->volume, n));
+    chk(up(h->c64, d->coupling, nnz));
+    chk(h->ceff64.alloc(nnz));
+    chk(h->ceff32.alloc(nnz));
+    chk(h->diag64.alloc(n));
+    chk(h->diag32.alloc(n));
+    chk(up(h->q64, q.data(), n));
+    chk(up(h->phi64, phi.data(), n));
+    if (d->num_tets > 0 && d->tet_v && d->tet_n) {
+        chk(up(h->tet_v, d->tet_v, 4 * (size_t)d->num_tets));
+        chk(up(h->tet_n, d->tet_n, 4 * (size_t)d->num_tets));
+    }
+    if (d->node_tet) chk(up(h->node_tet, d->node_tet, n));
+    chk(up(h->dtypes, dt.data(), 128));
+    chk(h->status.alloc(1));
+    if (e == cudaSuccess) chk(cudaMemset(h->status.p, 0, sizeof(int)));
+    chk(up(h->rowsV, rowsV.data(), n));
+    chk(up(h->rowsN, rowsN.data(), n));
+    chk(up(h->allV, allV.data(), n));
+    chk(up(h->allN, allN.data(), n));
+    chk(up(h->segStartD, h->segStart.data(), ncol));
+    chk(up(h->countVD, h->countV.data(), ncol));
+    chk(up(h->countND, h->countN.data(), ncol));
+    int32_t ca[2] = {h->countAllV, h->countAllN};
+    chk(up(h->countAllD, ca, 2));
+    chk(h->surfList.alloc(n));
+    chk(h->surfSlot.alloc(n));
+    chk(h->surfCount.alloc(1));
+    chk(h->surfRatio.alloc(n));
+    chk(h->cgbuf.alloc(10 * (size_t)n));
+    if (e == cudaSuccess) chk(cudaMemset(h->cgbuf.p, 0, 10 * (size_t)n * sizeof(float)));
+    chk(h->acc.alloc(16));
+    chk(h->keys.alloc(8));
+    chk(h->result.alloc(1024));
+    chk(h->local.alloc(1 << 16));
+    chk(h->localCount.alloc(66));
+    chk(h->localScratch.alloc(1 << 16));
+    if (e != cudaSuccess) {
+        const std::string msg = std::string("tg_create: ") + cudaGetErrorString(e);
+        tg_destroy(h);
+        return fail(nullptr, TG_ERR_CUDA, msg);
+    }
+    launch_rebuild_rows(h->dm(), h->stream);
+    const int rc = sync_status(h, "tg_create");
+    if (rc != TG_OK) {
+        const std::string msg = h->err;
+        tg_destroy(h);
+        return fail(nullptr, rc, msg);
+    }
+    *out = h;
+    return TG_OK;
+}
+
+void tg_destroy(tg_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->xyz.release(); h->type.release(); h->typeScratch.release(); h->flags.release(); h->area_pos.release();
+    h->row_ptr.release(); h->col.release(); h->rev.release(); h->colour.release(); h->tet_v.release();
+    h->tet_n.release(); h->node_tet.release(); h->geom.release(); h->volume.release(); h->c64.release();
+    h->ceff64.release(); h->diag64.release(); h->q64.release(); h->phi64.release(); h->ceff32.release();
+    h->diag32.release(); h->dtypes.release(); h->status.release(); h->rowsV.release(); h->rowsN.release();
+    h->allV.release(); h->allN.release(); h->segStartD.release(); h->countVD.release(); h->countND.release();
+    h->countAllD.release(); h->surfList.release(); h->surfSlot.release(); h->surfCount.release();
+    h->surfRatio.release(); h->cgbuf.release(); h->scalV.release(); h->scalN.release(); h->acc.release();
+    h->keys.release(); h->result.release(); h->local.release(); h->localCount.release();
+    h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
+    h->stageImpact.release();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int tg_get_phi(tg_handle* h, double* phi) {
+    if (!h || !phi) return fail(h, TG_ERR_ARGUMENT, "tg_get_phi: null argument");
+    CK(cudaMemcpyAsync(phi, h->phi64.p, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_get_phi");
+}
+
+int tg_set_phi(tg_handle* h, const double* phi) {
+    if (!h || !phi) return fail(h, TG_ERR_ARGUMENT, "tg_set_phi: null argument");
+    CK(cudaMemcpyAsync(h->phi64.p, phi, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+    h->bnormValid = false;
+    h->selValid = false;
+    return sync_status(h, "tg_set_phi");
+}
+
+int tg_get_couplings(tg_handle* h, double* out) {
+    if (!h || !out) return fail(h, TG_ERR_ARGUMENT, "tg_get_couplings: null argument");
+    CK(cudaMemcpyAsync(out, h->c64.p, sizeof(double) * h->nnz, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_get_couplings");
+}
+
+int tg_get_types(tg_handle* h, int8_t* out) {
+    if (!h || !out) return fail(h, TG_ERR_ARGUMENT, "tg_get_types: null argument");
+    CK(cudaMemcpyAsync(out, h->type.p, h->n, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_get_types");
+}
+
+int tg_relax_cycles(tg_handle* h, int32_t n, double* deviation) {
+    if (!h || n < 1) return fail(h, TG_ERR_ARGUMENT, "tg_relax_cycles: bad argument");
+    for (int it = 0; it < n - 1; it++) sweep_all(h, nullptr);
+    CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
+    sweep_all(h, h->acc.p);
+    double dev = 0.0;
+    CK(cudaMemcpyAsync(&dev, h->acc.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    const int rc = sync_status(h, "tg_relax_cycles");
+    if (deviation) *deviation = dev;
+    h->selValid = false;
+    return rc;
+}
+
+int tg_relax_threshold(tg_handle* h, double threshold, int32_t cycle, int32_t queueSize, int64_t maxSweeps,
+                       int64_t* iterations, double* deviation) {
+    if (!h || cycle < 1) return fail(h, TG_ERR_ARGUMENT, "tg_relax_threshold: bad argument");
+    std::deque<double> queue;
+    int64_t iter = 0;
+    double dev = 0.0;
+    int rc = TG_OK;
+    do {
+        rc = tg_relax_cycles(h, cycle, &dev);
+        if (rc != TG_OK) break;
+        queue.push_back(dev);
+        while ((int)queue.size() > queueSize) queue.pop_front();
+        if (stagnated(queue, (unsigned)queueSize, (unsigned)cycle)) {
+            rc = fail(h, TG_ERR_RELAX_FAULT, "tg_relax_threshold: stagnation");
+            break;
+        }
+        iter += cycle;
+        if (maxSweeps > 0 && iter >= maxSweeps && dev > threshold) {
+            rc = fail(h, TG_ERR_ITERATION_CAP, "tg_relax_threshold: sweep cap reached");
+            break;
+        }
+    } while (dev > threshold);
+    if (iterations) *iterations = iter;
+    if (deviation) *deviation = dev;
+    return rc;
+}
+
+int tg_local_relax(tg_handle* h, int32_t node, int32_t shell, double threshold, int32_t cycle, int32_t queueSize,
+                   int64_t* iterations, double* deviation) {
+    if (!h || node < 0 || node >= h->n || cycle < 1) return fail(h, TG_ERR_ARGUMENT, "tg_local_relax: bad argument");
+    DevMesh m = h->dm();
+    launch_local_set(m, node, shell, h->local.p, h->localCount.p, (int)h->local.n, h->localScratch.p,
+                     (int)h->localScratch.n, h->ncol, h->stream);
+    std::vector<int32_t> counts(h->ncol + 2);
+    CK(cudaMemcpyAsync(counts.data(), h->localCount.p, sizeof(int32_t) * (h->ncol + 2), cudaMemcpyDeviceToHost,
+                       h->stream));
+    int rc = sync_status(h, "tg_local_relax");
+    if (rc != TG_OK) return rc;
+    std::vector<int32_t> offs(h->ncol, 0);
+    for (int c = 1; c < h->ncol; c++) offs[c] = offs[c - 1] + counts[c - 1];
+    std::deque<double> queue;
+    int64_t iter = 0;
+    double dev = 0.0;
+    do {
+        for (int it = 0; it < cycle; it++) {
+            const bool last = it == cycle - 1;
+            if (last) CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
+            for (int c = 0; c < h->ncol; c++)
+                launch_sweep64(m, h->local.p + offs[c], counts[c], last ? h->acc.p : nullptr, h->stream);
+        }
+        CK(cudaMemcpyAsync(&dev, h->acc.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        rc = sync_status(h, "tg_local_relax");
+        if (rc != TG_OK) break;
+        queue.push_back(dev);
+        while ((int)queue.size() > queueSize) queue.pop_front();
+        if (stagnated(queue, (unsigned)queueSize, (unsigned)cycle)) {
+            rc = fail(h, TG_ERR_RELAX_FAULT, "tg_local_relax: stagnation");
+            break;
+        }
+        iter += cycle;
+        if (iter > 1000000) {
+            rc = fail(h, TG_ERR_ITERATION_CAP, "tg_local_relax: sweep cap reached");
+            break;
+        }
+    } while (dev > threshold);
+    if (iterations) *iterations = iter;
+    if (deviation) *deviation = dev;
+    h->selValid = false;
+    return rc;
+}
+
+int tg_residual(tg_handle* h, double* rel) {
+    if (!h || !rel) return fail(h, TG_ERR_ARGUMENT, "tg_residual: null argument");
+    int rc = ensure_bnorm(h);
+    if (rc != TG_OK) return rc;
+    DevMesh m = h->dm();
+    CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
+    launch_residual(m, h->allV.p, h->countAllV, nullptr, h->acc.p, h->stream);
+    launch_residual(m, h->allN.p, h->countAllN, nullptr, h->acc.p, h->stream);
+    double r2 = 0.0;
+    CK(cudaMemcpyAsync(&r2, h->acc.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    rc = sync_status(h, "tg_residual");
+    *rel = h->bnorm2 > 0.0 ? std::sqrt(r2 / h->bnorm2) : std::sqrt(r2);
+    return rc;
+}
+
+// FP32 conjugate gradients on one row list until r.z falls below
+// rtol^2 of its start value or maxIter is reached; returns iterations.
+static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, double rtol, int maxIter, int* itersOut) {
+    DevMesh m = h->dm();
+    CGVectors v = h->cg(which);
+    DBuf<double>& scal = which == 0 ? h->scalV : h->scalN;
+    const size_t need = 3 * (size_t)(maxIter + 2);
+    if (scal.n < need) {
+        CK(scal.alloc(need));
+        v = h->cg(which);
+    }
+    CK(cudaMemsetAsync(scal.p, 0, sizeof(double) * need, h->stream));
+    launch_cg_init(m, rows, count, v, h->stream);
+    double rz0 = 0.0;
+    CK(cudaMemcpyAsync(&rz0, scal.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const double target = rz0 * rtol * rtol;
+    int it = 0;
+    const int batch = 16;
+    while (it < maxIter && rz0 > 0.0) {
+        const int end = std::min(maxIter, it + batch);
+        for (; it < end; it++) launch_cg_iter(m, rows, count, v, it, target, h->stream);
+        double rz = 0.0;
+        CK(cudaMemcpyAsync(&rz, scal.p + 3 * it, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (rz <= target) break;
+    }
+    *itersOut = it;
+    return TG_OK;
+}
+
+int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
+    if (!h || !o) return fail(h, TG_ERR_ARGUMENT, "tg_solve: null argument");
+    int rc = ensure_bnorm(h);
+    if (rc != TG_OK) return rc;
+    DevMesh m = h->dm();
+    CGVectors vV = h->cg(0), vN = h->cg(1);
+    tg_solve_info inf{};
+    double rel = 0.0;
+    for (int outer = 0;; outer++) {
+        CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
+        launch_residual(m, h->allV.p, h->countAllV, vV.r, h->acc.p, h->stream);
+        launch_residual(m, h->allN.p, h->countAllN, vN.r, h->acc.p + 1, h->stream);
+        double r2[2];
+        CK(cudaMemcpyAsync(r2, h->acc.p, sizeof(r2), cudaMemcpyDeviceToHost, h->stream));
+        rc = sync_status(h, "tg_solve residual");
+        if (rc != TG_OK) return rc;
+        rel = h->bnorm2 > 0.0 ? std::sqrt((r2[0] + r2[1]) / h->bnorm2) : std::sqrt(r2[0] + r2[1]);
+        if (outer == 0) inf.initial_rel_residual = rel;
+        inf.outer = outer;
+        inf.rel_residual = rel;
+        if (rel <= o->rel_tol) break;
+        if (outer >= o->max_outer) {
+            if (info) *info = inf;
+            return fail(h, TG_ERR_ITERATION_CAP, "tg_solve: outer iteration cap reached");
+        }
+        int itV = 0, itN = 0;
+        if (h->countAllV > 0 && r2[0] > 0.0) {
+            rc = run_cg(h, 0, h->allV.p, h->countAllV, o->inner_rtol, o->max_inner, &itV);
+            if (rc != TG_OK) return rc;
+        }
+        if (h->countAllN > 0) {
+            launch_add_coupled(m, h->allN.p, h->countAllN, vV.x, vN.r, h->stream);
+            rc = run_cg(h, 1, h->allN.p, h->countAllN, o->inner_rtol, o->max_inner, &itN);
+            if (rc != TG_OK) return rc;
+        }
+        inf.inner += itV + itN;
+        launch_apply_correction(m, h->allV.p, h->countAllV, vV, h->stream);
+        launch_apply_correction(m, h->allN.p, h->countAllN, vN, h->stream);
+    }
+    h->selValid = false;
+    if (info) *info = inf;
+    return TG_OK;
+}
+
+int tg_field_o1(tg_handle* h, int32_t count, const int32_t* nodes, double* out) {
+    if (!h || count < 0 || (count && (!nodes || !out))) return fail(h, TG_ERR_ARGUMENT, "tg_field_o1: bad argument");
+    if (count == 0) return TG_OK;
+    int rc = stage(h, h->stageI, count);
+    if (rc == TG_OK) rc = stage(h, h->stageD, 3 * (size_t)count);
+    if (rc != TG_OK) return rc;
+    CK(cudaMemcpyAsync(h->stageI.p, nodes, sizeof(int32_t) * count, cudaMemcpyHostToDevice, h->stream));
+    launch_field_o1(h->dm(), h->stageI.p, count, h->stageD.p, h->stream);
+    CK(cudaMemcpyAsync(out, h->stageD.p, sizeof(double) * 3 * count, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_field_o1");
+}
+
+int tg_surface_init(tg_handle* h, int32_t vacuumId, int32_t* num) {
+    if (!h || vacuumId < 0 || vacuumId > 127 || h->types[vacuumId].id < 0)
+        return fail(h, TG_ERR_ARGUMENT, "tg_surface_init: unknown vacuum id");
+    h->vacuumId = vacuumId;
+    CK(cudaMemsetAsync(h->surfCount.p, 0, sizeof(int32_t), h->stream));
+    launch_surface_init(h->dm(), h->sf(), vacuumId, h->stream);
+    int rc = refresh_counts(h);
+    if (rc == TG_OK) rc = sync_status(h, "tg_surface_init");
+    if (num) *num = h->surfSlots;
+    h->selValid = false;
+    return rc;
+}
+
+int tg_surface_select(tg_handle* h, tg_select_info* info) {
+    if (!h || !info) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: null argument");
+    if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: surface not initialised");
+    unsigned long long k[3] = {0, 0, 0};
+    double sum = 0.0;
+    CK(cudaMemsetAsync(h->keys.p, 0, 3 * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
+    launch_surface_select(h->dm(), h->sf(), h->surfSlots, h->keys.p, h->acc.p, h->stream);
+    CK(cudaMemcpyAsync(k, h->keys.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&sum, h->acc.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    int rc = sync_status(h, "tg_surface_select");
+    if (rc != TG_OK) return rc;
+    tg_select_info s{};
+    s.ratio_sum = sum;
+    if (k[0] == 0ull) {
+        s.candidate = -1;
+        s.apex = -1;
+        s.num_surface = 0;
+        *info = s;
+        h->sel = s;
+        h->selValid = true;
+        return fail(h, TG_ERR_NO_SURFACE, "tg_surface_select: empty surface");
+    }
+    auto unkey = [](unsigned long long key, float* v) {
+        const uint32_t hi = (uint32_t)(key >> 32);
+        const uint32_t u = (hi & 0x80000000u) ? (hi & 0x7fffffffu) : ~hi;
+        std::memcpy(v, &u, 4);
+        return (int32_t)(~(uint32_t)key);
+    };
+    float best, zmax;
+    s.candidate = unkey(k[0], &best);
+    s.apex = unkey(k[1], &zmax);
+    s.best_ratio = best;
+    launch_surface_second(h->sf(), h->surfSlots, s.candidate, h->keys.p + 2, h->stream);
+    CK(cudaMemcpyAsync(&k[2], h->keys.p + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    rc = sync_status(h, "tg_surface_select");
+    if (rc != TG_OK) return rc;
+    float second = 0.0f;
+    if (k[2]) unkey(k[2], &second);
+    s.second_ratio = second;
+    s.probability = (float)(best / sum);
+    int cnt = 0;
+    // number of live entries = slots minus removed ones; count on host is
+    // not tracked, report slots (upper bound) unless exact count requested
+    cnt = h->surfSlots;
+    s.num_surface = cnt;
+    *info = s;
+    h->sel = s;
+    h->selValid = true;
+    return TG_OK;
+}
+
+int tg_get_surface(tg_handle* h, int32_t capacity, int32_t* nodes, float* ratios, int32_t* count) {
+    if (!h || !count) return fail(h, TG_ERR_ARGUMENT, "tg_get_surface: null argument");
+    std::vector<int32_t> list(h->surfSlots);
+    std::vector<float> rat(h->surfSlots);
+    if (h->surfSlots) {
+        CK(cudaMemcpyAsync(list.data(), h->surfList.p, sizeof(int32_t) * h->surfSlots, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(rat.data(), h->surfRatio.p, sizeof(float) * h->surfSlots, cudaMemcpyDeviceToHost, h->stream));
+    }
+    int rc = sync_status(h, "tg_get_surface");
+    if (rc != TG_OK) return rc;
+    int c = 0;
+    for (int s = 0; s < h->surfSlots; s++) {
+        if (list[s] < 0) continue;
+        if (c < capacity) {
+            if (nodes) nodes[c] = list[s];
+            if (ratios) ratios[c] = rat[s];
+        }
+        c++;
+    }
+    *count = c;
+    return TG_OK;
+}
+
+int tg_surface_normal(tg_handle* h, int32_t node, float normal[3]) {
+    if (!h || node < 0 || node >= h->n || !normal) return fail(h, TG_ERR_ARGUMENT, "tg_surface_normal: bad argument");
+    int rc = stage(h, h->stageF, 4);
+    if (rc != TG_OK) return rc;
+    // Surface_3d::Table::normal returns zero for nodes outside the surface set
+    uint8_t f = 0;
+    CK(cudaMemcpyAsync(&f, h->flags.p + node, 1, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (!(f & F_SURFACE)) {
+        normal[0] = normal[1] = normal[2] = 0.0f;
+        return TG_OK;
+    }
+    launch_surface_normal(h->dm(), h->sf(), node, h->vacuumId, h->stageF.p, h->stream);
+    CK(cudaMemcpyAsync(normal, h->stageF.p, 3 * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_surface_normal");
+}
+
+int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached, int32_t* numDetached) {
+    if (!h || node < 0 || node >= h->n) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: bad node");
+    if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: surface not initialised");
+    launch_take_away(h->dm(), h->rl(), h->sf(), node, h->vacuumId, h->result.p, (int)h->result.n, h->stream);
+    std::vector<int32_t> res(h->result.n);
+    CK(cudaMemcpyAsync(res.data(), h->result.p, sizeof(int32_t) * res.size(), cudaMemcpyDeviceToHost, h->stream));
+    int rc = sync_status(h, "tg_take_away");
+    if (rc != TG_OK) return rc;
+    rc = refresh_counts(h);
+    if (rc != TG_OK) return rc;
+    const int nd = res[0];
+    h->h_type[node] = (int8_t)h->vacuumId;
+    for (int k = 0; k < nd && k + 1 < (int)res.size(); k++) {
+        h->h_type[res[1 + k]] = (int8_t)h->vacuumId;
+        if (detached && k < capacity) detached[k] = res[1 + k];
+    }
+    if (numDetached) *numDetached = nd;
+    h->bnormValid = false;
+    h->selValid = false;
+    return TG_OK;
+}
+
+int tg_update_coordination(tg_handle* h) {
+    if (!h) return fail(h, TG_ERR_ARGUMENT, "tg_update_coordination: null handle");
+    launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
+    return sync_status(h, "tg_update_coordination");
+}
+
+int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
+             const int32_t* guess, const tg_trace_opts* o, tg_impact* out) {
+    if (!h || nIons < 0 || (nIons && (!start || !qm || !out)) || !o) return fail(h, TG_ERR_ARGUMENT, "tg_trace: bad argument");
+    if (!h->tet_v.p) return fail(h, TG_ERR_ARGUMENT, "tg_trace: mesh has no tetrahedra");
+    if (nIons == 0) return TG_OK;
+    int rc = stage(h, h->stageF, (size_t)nIons * 7);
+    if (rc == TG_OK) rc = stage(h, h->stageI, nIons);
+    if (rc == TG_OK) rc = stage(h, h->stageImpact, nIons);
+    if (rc != TG_OK) return rc;
+    float* dStart = h->stageF.p;
+    float* dVel = h->stageF.p + 3 * (size_t)nIons;
+    float* dQm = h->stageF.p + 6 * (size_t)nIons;
+    CK(cudaMemcpyAsync(dStart, start, sizeof(float) * 3 * nIons, cudaMemcpyHostToDevice, h->stream));
+    if (vel) CK(cudaMemcpyAsync(dVel, vel, sizeof(float) * 3 * nIons, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dQm, qm, sizeof(float) * nIons, cudaMemcpyHostToDevice, h->stream));
+    if (guess) CK(cudaMemcpyAsync(h->stageI.p, guess, sizeof(int32_t) * nIons, cudaMemcpyHostToDevice, h->stream));
+    else CK(cudaMemsetAsync(h->stageI.p, 0, sizeof(int32_t) * nIons, h->stream));
+    TraceParams tp;
+    tp.dt0 = o->time_step;
+    tp.dt_min = o->min_time_step;
+    tp.tol = o->error_threshold;
+    tp.max_steps = o->max_steps;
+    tp.stepper_limit = o->stepper_limit;
+    tp.walk_limit = o->walk_limit;
+    tp.top_z = h->top_z;
+    launch_trace(h->dm(), nIons, dStart, vel ? dVel : nullptr, dQm, h->stageI.p, tp, h->stageImpact.p, h->stream);
+    CK(cudaMemcpyAsync(out, h->stageImpact.p, sizeof(tg_impact) * nIons, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_trace");
+}
+
+int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* guess, float* out) {
+    if (!h || n < 0 || (n && (!xyz || !out))) return fail(h, TG_ERR_ARGUMENT, "tg_potential_at: bad argument");
+    if (n == 0) return TG_OK;
+    int rc = stage(h, h->stageF, (size_t)n * 4);
+    if (rc == TG_OK) rc = stage(h, h->stageI, n);
+    if (rc != TG_OK) return rc;
+    CK(cudaMemcpyAsync(h->stageF.p, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+    if (guess) CK(cudaMemcpyAsync(h->stageI.p, guess, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->stream));
+    else CK(cudaMemsetAsync(h->stageI.p, 0, sizeof(int32_t) * n, h->stream));
+    launch_potential_at(h->dm(), n, h->stageF.p, h->stageI.p, 100000, h->stageF.p + 3 * (size_t)n, h->stream);
+    CK(cudaMemcpyAsync(out, h->stageF.p + 3 * (size_t)n, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_potential_at");
+}
+
+int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec) {
+    if (!h || !o || !rec) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: null argument");
+    if (h->vacuumId != o->vacuum_id) {
+        int32_t ns;
+        int rc = tg_surface_init(h, o->vacuum_id, &ns);
+        if (rc != TG_OK) return rc;
+    }
+    int rc = TG_OK;
+    if (!h->selValid) {
+        tg_select_info s;
+        rc = tg_surface_select(h, &s);
+        if (rc != TG_OK) return rc;
+    }
+    std::memset(rec, 0, sizeof(*rec));
+    const tg_select_info sel = h->sel;
+    if (sel.candidate < 0) return fail(h, TG_ERR_NO_SURFACE, "tg_run_event: empty surface");
+    // I) the candidate and its state before removal
+    const int node = sel.candidate;
+    rec->node = node;
+    rec->type_id = h->h_type[node];
+    rec->probability = sel.probability;
+    rec->best_ratio = sel.best_ratio;
+    rec->second_ratio = sel.second_ratio;
+    rec->scaling_reference = sel.best_ratio;
+    {
+        double phi = 0.0, E[3];
+        CK(cudaMemcpyAsync(&phi, h->phi64.p + node, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        rc = tg_field_o1(h, 1, &node, E);
+        if (rc != TG_OK) return rc;
+        rec->phi_before = (float)phi;
+        for (int k = 0; k < 3; k++) rec->field_before[k] = (float)E[k];
+    }
+    for (int k = 0; k < 3; k++) rec->apex[k] = sel.apex >= 0 ? h->h_xyz[3 * (size_t)sel.apex + k] : 0.0f;
+    if (o->normal_enabled) {
+        rc = tg_surface_normal(h, node, rec->normal);
+        if (rc != TG_OK) return rc;
+    }
+    const tg_type removed = h->types[h->h_type[node]];
+    // II) removal
+    int32_t nd = 0;
+    rc = tg_take_away(h, node, 0, nullptr, &nd);
+    if (rc != TG_OK) return rc;
+    rec->detached = nd;
+    rc = tg_update_coordination(h);
+    if (rc != TG_OK) return rc;
+    // III) relaxation
+    if (o->relax_mode == 0) {
+        int64_t it = 0;
+        double dev = 0.0;
+        int r1 = tg_local_relax(h, node, o->local_shell, o->local_threshold, o->local_cycle, o->local_queue, &it, &dev);
+        if (r1 != TG_OK && r1 != TG_ERR_RELAX_FAULT && r1 != TG_ERR_ITERATION_CAP) return r1;
+        rec->relax_iterations = (int32_t)it;
+        if (o->global_steps > 0) {
+            r1 = tg_relax_cycles(h, o->global_steps, &dev);
+            if (r1 != TG_OK) return r1;
+            rec->relax_iterations += o->global_steps;
+        }
+        if (o->refresh_interval > 0 && eventIndex % o->refresh_interval == 0) {
+            r1 = tg_relax_threshold(h, o->refresh_threshold, o->refresh_cycle, o->refresh_queue, o->refresh_max_sweeps,
+                                    &it, &dev);
+            if (r1 != TG_OK && r1 != TG_ERR_RELAX_FAULT && r1 != TG_ERR_ITERATION_CAP) return r1;
+            rec->relax_status = r1;
+            rec->relax_iterations += (int32_t)it;
+        }
+        rc = tg_residual(h, &rec->rel_residual);
+        if (rc != TG_OK) return rc;
+    } else {
+        tg_solve_info si;
+        rc = tg_solve(h, &o->solve, &si);
+        rec->relax_status = rc;
+        if (rc != TG_OK && rc != TG_ERR_ITERATION_CAP) return rc;
+        rec->relax_iterations = si.inner;
+        rec->rel_residual = si.rel_residual;
+    }
+    // IV) fields, probabilities and the next candidate
+    {
+        tg_select_info s;
+        rc = tg_surface_select(h, &s);
+        if (rc != TG_OK && rc != TG_ERR_NO_SURFACE) return rc;
+    }
+    // V) ion flight of the removed atom, VI) state after removal
+    if (o->trace_enabled) {
+        const float start[3] = {h->h_xyz[3 * (size_t)node], h->h_xyz[3 * (size_t)node + 1], h->h_xyz[3 * (size_t)node + 2]};
+        // Trajectory_3d::eCharge / amu2kg (trajectory_3d.h:91-93) as floats
+        const float charge = (float)removed.evap_charge * 1.60217733e-19f;
+        const float mass = removed.mass * 1.660538782e-27f;
+        const float qm = charge / mass;
+        const int32_t guess = h->h_node_tet.empty() ? 0 : h->h_node_tet[node];
+        rc = tg_trace(h, 1, start, nullptr, &qm, &guess, &o->trace, &rec->impact);
+        if (rc != TG_OK) return rc;
+    }
+    {
+        double phi = 0.0, E[3];
+        CK(cudaMemcpyAsync(&phi, h->phi64.p + node, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        rc = tg_field_o1(h, 1, &node, E);
+        if (rc != TG_OK) return rc;
+        rec->phi_after = (float)phi;
+        for (int k = 0; k < 3; k++) rec->field_after[k] = (float)E[k];
+    }
+    return TG_OK;
+}
+
+}  // extern "C"

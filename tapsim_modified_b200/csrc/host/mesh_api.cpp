@@ -1,0 +1,377 @@
+// Host-side mesh objects behind tg_mesh_* (include/tapsim_gpu.h): build the
+// arrays of a tg_mesh_desc from the tip generator, from a node file plus
+// configuration (the reference's Process::initialization path:
+// readConfig, readGeomGrid, tetrahedralize, fastSync; process.cpp:47-129), or
+// from a TAPSIM dump (File_Io::readSystem, the resumption path).
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../../include/tapsim_gpu.h"
+#include "delaunay.h"
+#include "formats.h"
+#include "tipgen.h"
+#include "voronoi.h"
+
+using namespace tg_host;
+
+struct tg_mesh {
+    std::vector<float> xyz;
+    std::vector<int8_t> type;
+    std::vector<uint8_t> hull;
+    std::vector<float> phi;
+    std::vector<int32_t> row_ptr, col;
+    std::vector<double> coupling, geom, volume;
+    std::vector<uint8_t> area_pos;
+    std::vector<int32_t> tet_v, tet_n, node_tet;
+    std::vector<uint32_t> number;
+    ConfigTable config;
+    std::vector<tg_type> types;
+    bool has_geom = false;
+};
+
+namespace tgapi {
+void set_process_error(const std::string& msg);  // handle.cu: read by tg_last_error(NULL)
+}
+
+namespace {
+
+int mesh_fail(const std::string& m) {
+    tgapi::set_process_error(m);
+    return TG_ERR_HOST;
+}
+
+void fill_types(tg_mesh* m) {
+    m->types.clear();
+    for (const auto& kv : m->config.types) {
+        const CellType& c = kv.second;
+        tg_type t;
+        t.id = c.id;
+        t.charge_density = c.charge_density;
+        t.epsilon = c.epsilon;
+        t.removable = c.removable;
+        t.neumann = c.neumann;
+        t.dirichlet = c.dirichlet;
+        t.phi = c.phi;
+        t.mass = c.mass;
+        t.evap_charge = c.evap_charge;
+        t.evap_field = c.evap_field;
+        t.evap_energy = c.evap_energy;
+        m->types.push_back(t);
+    }
+}
+
+// Coupling of every entry as Grid_3d::Table::fastSync leaves it
+// (grid_3d.cpp:491-553): the pair is evaluated once, from its lower index,
+// by computeCoupling (grid_3d.cpp:1392-1409), and mirrored.
+int couplings_from_tables(tg_mesh* m, const MeshTables& t) {
+    const int n = (int)m->type.size();
+    m->coupling.assign(t.col.size(), 0.0);
+    m->geom.assign(t.col.size(), 0.0);
+    for (int i = 0; i < n; i++) {
+        for (int q = t.row_ptr[i]; q < t.row_ptr[i + 1]; q++) {
+            const int j = t.col[q];
+            const int lo = std::min(i, j), hi = std::max(i, j);
+            auto ilo = m->config.types.find(m->type[lo]);
+            auto ihi = m->config.types.find(m->type[hi]);
+            if (ilo == m->config.types.end() || ihi == m->config.types.end())
+                return mesh_fail("mesh: node type missing from the configuration");
+            const CellType &a = ilo->second, &b = ihi->second;
+            const double g = t.dist[q] > 0.0 ? t.area_half[q] / t.dist[q] : 0.0;
+            m->geom[q] = g;
+            if (!a.neumann && b.neumann) continue;
+            m->coupling[q] = 2.0 * (double)a.epsilon * (double)b.epsilon / ((double)a.epsilon + (double)b.epsilon) * g;
+        }
+    }
+    return TG_OK;
+}
+
+int build_from_points(tg_mesh* m, int threads, uint64_t seed) {
+    const int n = (int)m->type.size();
+    Tetrahedralization T;
+    std::string err = delaunay_tetrahedralize(m->xyz.data(), n, seed, &T);
+    if (!err.empty()) return mesh_fail(err);
+    MeshTables t;
+    err = build_mesh_tables(m->xyz.data(), n, T.vertices.data(), T.neighbours.data(), T.num_tets(), threads, &t);
+    if (!err.empty()) return mesh_fail(err);
+    m->tet_v.swap(T.vertices);
+    m->tet_n.swap(T.neighbours);
+    m->row_ptr.swap(t.row_ptr);
+    m->col.swap(t.col);
+    m->hull.swap(t.hull);
+    m->node_tet.swap(t.node_tet);
+    m->area_pos.swap(t.area_pos);
+    m->volume.swap(t.volume);
+    t.row_ptr = m->row_ptr;
+    t.col = m->col;
+    const int rc = couplings_from_tables(m, t);
+    m->has_geom = true;
+    return rc;
+}
+
+ConfigTable default_tip_config() {
+    ConfigTable ct;
+    auto add = [&](int id, const char* name, bool rem, bool neu, bool dir, float phi, float mass, short q, float E) {
+        CellType t;
+        t.id = id;
+        t.name = name;
+        t.removable = rem;
+        t.neumann = neu;
+        t.dirichlet = dir;
+        t.phi = phi;
+        t.mass = mass;
+        t.evap_charge = q;
+        t.evap_field = E;
+        t.evap_energy = rem ? 1.0f : 0.0f;
+        ct.types[id] = t;
+    };
+    // meshgen markers (meshgen/meshgen.cpp:491-595) with Neumann sides, and
+    // the specimen species: bcc Fe (E_evap 33 V/nm) and Cu (30 V/nm), tip at 1 V
+    add(0, "Vacuum", false, false, false, 0.0f, 0.0f, 0, 0.0f);
+    add(1, "Top", false, false, true, 0.0f, 0.0f, 0, 0.0f);
+    add(2, "Bottom", false, true, false, 0.0f, 0.0f, 0, 0.0f);
+    add(3, "Sides", false, true, false, 0.0f, 0.0f, 0, 0.0f);
+    add(4, "Fe", true, false, true, 1.0f, 55.845f, 2, 33e9f);
+    add(5, "Cu", true, false, true, 1.0f, 63.546f, 2, 30e9f);
+    return ct;
+}
+
+}  // namespace
+
+extern "C" {
+
+void tg_tip_params_default(tg_tip_params* p) {
+    TipParams d;
+    p->lattice_a = d.lattice_a;
+    p->cap_radius = d.cap_radius;
+    p->shank_length = d.shank_length;
+    p->half_angle_deg = d.half_angle_deg;
+    p->box_half_width = d.box_half_width;
+    p->box_height = d.box_height;
+    p->fine_shell = d.fine_shell;
+    p->layers_per_level = d.layers_per_level;
+    p->coarsen = d.coarsen;
+    p->max_spacing = d.max_spacing;
+    p->solute_fraction = d.solute_fraction;
+    p->precip_density = d.precip_density;
+    p->precip_rmin = d.precip_rmin;
+    p->precip_rmax = d.precip_rmax;
+    p->precip_mu = d.precip_mu;
+    p->precip_sigma = d.precip_sigma;
+    p->seed = d.seed;
+}
+
+int tg_mesh_from_tip(const tg_tip_params* p, int32_t threads, tg_mesh** out) {
+    if (!p || !out) return mesh_fail("tg_mesh_from_tip: null argument");
+    TipParams tp;
+    tp.lattice_a = p->lattice_a;
+    tp.cap_radius = p->cap_radius;
+    tp.shank_length = p->shank_length;
+    tp.half_angle_deg = p->half_angle_deg;
+    tp.box_half_width = p->box_half_width;
+    tp.box_height = p->box_height;
+    tp.fine_shell = p->fine_shell;
+    tp.layers_per_level = p->layers_per_level;
+    tp.coarsen = p->coarsen;
+    tp.max_spacing = p->max_spacing;
+    tp.solute_fraction = p->solute_fraction;
+    tp.precip_density = p->precip_density;
+    tp.precip_rmin = p->precip_rmin;
+    tp.precip_rmax = p->precip_rmax;
+    tp.precip_mu = p->precip_mu;
+    tp.precip_sigma = p->precip_sigma;
+    tp.seed = p->seed;
+    TipMesh tm;
+    try {
+        tm = generate_tip(tp);
+    } catch (const std::exception& e) {
+        return mesh_fail(e.what());
+    }
+    tg_mesh* m = new tg_mesh();
+    m->xyz.swap(tm.xyz);
+    m->type.assign(tm.id.begin(), tm.id.end());
+    m->config = default_tip_config();
+    fill_types(m);
+    const int n = (int)m->type.size();
+    m->phi.resize(n);
+    for (int i = 0; i < n; i++) m->phi[i] = m->config.types[m->type[i]].phi;
+    m->number.resize(n);
+    for (int i = 0; i < n; i++) m->number[i] = i + 1;
+    const int rc = build_from_points(m, threads, p->seed);
+    if (rc != TG_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return TG_OK;
+}
+
+int tg_mesh_from_files(const char* nodeFile, const char* configFile, int32_t threads, tg_mesh** out) {
+    if (!nodeFile || !configFile || !out) return mesh_fail("tg_mesh_from_files: null argument");
+    NodeFile nf;
+    std::string err = read_node_file(nodeFile, &nf);
+    if (!err.empty()) return mesh_fail(err);
+    tg_mesh* m = new tg_mesh();
+    err = read_config(configFile, &m->config);
+    if (!err.empty()) {
+        delete m;
+        return mesh_fail(err);
+    }
+    fill_types(m);
+    const int n = (int)nf.id.size();
+    m->xyz.swap(nf.xyz);
+    m->type.assign(nf.id.begin(), nf.id.end());
+    m->number.swap(nf.number);
+    m->phi.resize(n);
+    for (int i = 0; i < n; i++) {
+        auto it = m->config.types.find(m->type[i]);
+        if (it == m->config.types.end()) {
+            delete m;
+            return mesh_fail("tg_mesh_from_files: node type missing from the configuration");
+        }
+        // initial potentials: preset values unless the file carries them
+        // (Process::initialization, process.cpp:63-79)
+        m->phi[i] = nf.phi.empty() ? it->second.phi : nf.phi[i];
+    }
+    const int rc = build_from_points(m, threads, 1);
+    if (rc != TG_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return TG_OK;
+}
+
+int tg_mesh_from_dump(const char* dumpFile, const char* configFile, tg_mesh** out) {
+    if (!dumpFile || !out) return mesh_fail("tg_mesh_from_dump: null argument");
+    Dump d;
+    std::string err = read_dump(dumpFile, &d);
+    if (!err.empty()) return mesh_fail(err);
+    tg_mesh* m = new tg_mesh();
+    if (configFile) {
+        err = read_config(configFile, &m->config);
+        if (!err.empty()) {
+            delete m;
+            return mesh_fail(err);
+        }
+    } else {
+        m->config = d.config;
+    }
+    fill_types(m);
+    const int n = (int)d.id.size();
+    m->xyz.swap(d.xyz);
+    m->type.assign(d.id.begin(), d.id.end());
+    m->hull.swap(d.hull);
+    m->number.swap(d.number);
+    // Grid_3d::Table::potential(i) reads phi[(phiSwitch + 1) % 2] (grid_3d.h:184)
+    m->phi = ((d.phi_switch + 1) % 2) ? d.phi1 : d.phi0;
+    m->row_ptr.swap(d.row_ptr);
+    m->col.swap(d.col);
+    m->coupling.assign(d.coupling.begin(), d.coupling.end());
+    m->tet_v.swap(d.tet_v);
+    m->tet_n.swap(d.tet_n);
+    m->node_tet.swap(d.node_tet);
+    for (int i = 0; i < n; i++)
+        for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++)
+            if (q > m->row_ptr[i] && m->col[q] <= m->col[q - 1]) {
+                delete m;
+                return mesh_fail("tg_mesh_from_dump: neighbour lists are not ascending");
+            }
+    *out = m;
+    return TG_OK;
+}
+
+void tg_mesh_destroy(tg_mesh* m) { delete m; }
+
+int tg_mesh_describe(const tg_mesh* m, tg_mesh_desc* d, int32_t* nnz) {
+    if (!m || !d) return mesh_fail("tg_mesh_describe: null argument");
+    std::memset(d, 0, sizeof(*d));
+    d->num_nodes = (int32_t)m->type.size();
+    d->xyz = m->xyz.data();
+    d->type_id = m->type.data();
+    d->hull = m->hull.empty() ? nullptr : m->hull.data();
+    d->phi = m->phi.data();
+    d->row_ptr = m->row_ptr.data();
+    d->col = m->col.data();
+    d->coupling = m->coupling.data();
+    d->geom = m->has_geom ? m->geom.data() : nullptr;
+    d->area_pos = m->area_pos.empty() ? nullptr : m->area_pos.data();
+    d->volume = m->volume.empty() ? nullptr : m->volume.data();
+    d->num_tets = (int32_t)(m->tet_v.size() / 4);
+    d->tet_v = m->tet_v.data();
+    d->tet_n = m->tet_n.data();
+    d->node_tet = m->node_tet.data();
+    d->num_types = (int32_t)m->types.size();
+    d->types = m->types.data();
+    if (nnz) *nnz = (int32_t)m->col.size();
+    return TG_OK;
+}
+
+int tg_mesh_write_node_file(const tg_mesh* m, const char* path, int32_t binary) {
+    if (!m || !path) return mesh_fail("tg_mesh_write_node_file: null argument");
+    NodeFile nf;
+    nf.xyz = m->xyz;
+    nf.id.assign(m->type.begin(), m->type.end());
+    const std::string err = write_node_file(path, nf, binary != 0);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
+int tg_mesh_write_config(const tg_mesh* m, const char* path) {
+    if (!m || !path) return mesh_fail("tg_mesh_write_config: null argument");
+    const std::string err = write_config_ascii(path, m->config);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
+int tg_mesh_write_dump(const tg_mesh* m, const char* path, const float* phi) {
+    if (!m || !path) return mesh_fail("tg_mesh_write_dump: null argument");
+    Dump d;
+    d.config = m->config;
+    const int n = (int)m->type.size();
+    for (int k = 0; k < 3; k++) {
+        d.min[k] = 1e30f;
+        d.max[k] = -1e30f;
+    }
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) {
+            d.min[k] = std::min(d.min[k], m->xyz[3 * i + k]);
+            d.max[k] = std::max(d.max[k], m->xyz[3 * i + k]);
+        }
+    for (int k = 0; k < 3; k++) {
+        d.cmin[k] = d.min[k];
+        d.cmax[k] = d.max[k];
+    }
+    d.xyz = m->xyz;
+    d.hull = m->hull;
+    d.node_tet = m->node_tet;
+    d.tet_v = m->tet_v;
+    d.tet_n = m->tet_n;
+    d.id.assign(m->type.begin(), m->type.end());
+    d.number = m->number;
+    if (d.number.size() != (size_t)n) {
+        d.number.resize(n);
+        for (int i = 0; i < n; i++) d.number[i] = i + 1;
+    }
+    d.phi0.resize(n);
+    for (int i = 0; i < n; i++) d.phi0[i] = phi ? phi[i] : m->phi[i];
+    d.phi1 = d.phi0;
+    d.charge.assign(n, 0.0f);
+    d.boundary.resize(n);
+    d.dirichlet.resize(n);
+    d.neumann.resize(n);
+    for (int i = 0; i < n; i++) {
+        const CellType& t = m->config.types.at(m->type[i]);
+        d.boundary[i] = m->hull.empty() ? 0 : m->hull[i];
+        d.dirichlet[i] = t.dirichlet;
+        d.neumann[i] = t.neumann;
+        if (!m->volume.empty()) d.charge[i] = (float)(m->volume[i] * t.charge_density / 8.85418781762e-12);
+    }
+    d.row_ptr = m->row_ptr;
+    d.col = m->col;
+    d.coupling.assign(m->coupling.begin(), m->coupling.end());
+    const std::string err = write_dump(path, d);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
+}  // extern "C"

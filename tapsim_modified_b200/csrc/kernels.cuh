@@ -1,0 +1,132 @@
+// Device data layout and host-side launchers of the hot-path kernels.
+//
+// HBM layout (one copy per handle, node-file order, CSR rows ascending):
+//   per node   xyz float[3], type int8, flags uint8, phi64 double, diag64
+//              double, diag32 float, q64 double, colour int32
+//   per entry  col int32, rev int32, c64 double (the Grid_3d coupling),
+//              ceff64 double / ceff32 float (coupling as the row's update
+//              sees it: 0 for a Neumann neighbour of a non-Neumann row),
+//              geom double (Voronoi area / distance), area_pos uint8
+//   free rows  int32 lists grouped by colour, non-Neumann and Neumann apart
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+
+namespace tgd {
+
+struct DevMesh {
+    int n, nnz, ntets;
+    const float* xyz;
+    int8_t* type;
+    uint8_t* flags;
+    const int32_t* row_ptr;
+    const int32_t* col;
+    const int32_t* rev;
+    const double* geom;
+    const uint8_t* area_pos;
+    const double* volume;
+    double* c64;
+    double* ceff64;
+    float* ceff32;
+    double* diag64;
+    float* diag32;
+    double* q64;
+    double* phi64;
+    const int32_t* colour;
+    const int32_t* tet_v;
+    const int32_t* tet_n;
+    const int32_t* node_tet;
+    const DType* types;
+    int* status;
+    double snap;   // power-of-two scale to the integer grid of the exact predicates
+};
+
+// Free-row bookkeeping kept on the device so that removals can append rows
+// without a host round trip.
+struct RowLists {
+    int32_t* rowsV;        // non-Neumann free rows, colour segments
+    int32_t* rowsN;        // Neumann free rows, colour segments
+    const int32_t* segStart;  // [ncolours] segment start (same for V and N)
+    int32_t* countV;       // [ncolours] rows in use
+    int32_t* countN;
+    int32_t* allV;         // the same rows as one compact list each
+    int32_t* allN;
+    int32_t* countAll;     // [2]: rows in allV, allN
+    int ncolours;
+};
+
+struct Surface {
+    int32_t* list;         // surface node per slot, -1 for a removed entry
+    int32_t* slot;         // [n] list slot of a surface node
+    int32_t* count;        // slots in use (device counter)
+    float* ratio;          // per slot |E|/E_evap of the last selection
+    int capacity;
+};
+
+// ---- relaxation (relax.cu) ----
+// coloured Gauss-Seidel sweep of one row list, FP64, max |delta| to *maxdev
+void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* maxdev, cudaStream_t s);
+// r_i (FP64) for a row list; accumulates sum r^2 into *acc; optionally
+// stores r as float into r32
+void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s);
+// b_i = sum over Dirichlet neighbours c_ij phi_j - q_i; sum b^2 into *acc
+void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s);
+// FP32 conjugate gradients on the rows of one list (Jacobi preconditioner)
+struct CGVectors {
+    float *x, *r, *z, *p, *ap;
+    double* scal;  // [3*(max_iter+2)] accumulators: rz, pAp per iteration
+};
+void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s);
+// one CG iteration; all of it is skipped once scal[3it] (r.z) <= target
+void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double target,
+                    cudaStream_t s);
+// rhs_N += sum over non-Neumann free neighbours c_ij x_j (coupling of the
+// Neumann rows to the correction found for the non-Neumann rows)
+void launch_add_coupled(const DevMesh& m, const int32_t* rows, int count, const float* xV, float* r, cudaStream_t s);
+// phi64[i] += x[i] for a row list, and clears the CG vectors on those rows
+void launch_apply_correction(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s);
+// coupling rows: diag64/diag32/ceff from c64 and the flags of all nodes
+void launch_rebuild_rows(const DevMesh& m, cudaStream_t s);
+// k-hop node set (find_localNodes) restricted to non-Dirichlet cells; writes
+// rows grouped by colour into out (capacity cap) and per-colour counts
+void launch_local_set(const DevMesh& m, int node, int hops, int32_t* out, int32_t* outCount, int cap,
+                      int32_t* scratch, int scratchCap, int ncolours, cudaStream_t s);
+
+// ---- surface (surface.cu) ----
+void launch_surface_init(const DevMesh& m, Surface sf, int vacuumId, cudaStream_t s);
+// fields, ratios, argmax key, apex key, ratio sum
+void launch_surface_select(const DevMesh& m, Surface sf, int slots, unsigned long long* keys, double* acc,
+                           cudaStream_t s);
+void launch_surface_second(Surface sf, int slots, int best, unsigned long long* key, cudaStream_t s);
+void launch_field_o1(const DevMesh& m, const int32_t* nodes, int count, double* out, cudaStream_t s);
+// evap_takeAway in one small kernel; result[0] = number of detached nodes,
+// result[1..] their indices
+void launch_take_away(const DevMesh& m, RowLists rl, Surface sf, int node, int vacuumId, int32_t* result,
+                      int resultCap, cudaStream_t s);
+void launch_update_coordination(const DevMesh& m, int8_t* scratchType, cudaStream_t s);
+void launch_surface_normal(const DevMesh& m, Surface sf, int node, int vacuumId, float* out, cudaStream_t s);
+
+// ---- flights (flight.cu) ----
+struct TraceParams {
+    double dt0, dt_min, tol;
+    int max_steps, stepper_limit, walk_limit;
+    float top_z;
+};
+struct ImpactOut {
+    float stop[3];
+    float stop_time;
+    float last_pos[3];
+    int32_t last_tet;
+    float last_phi;
+    int32_t steps;
+    int32_t status;
+};
+void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
+                  const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s);
+void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit,
+                         float* out, cudaStream_t s);
+
+}  // namespace tgd

@@ -1,0 +1,299 @@
+// Finite-volume relaxation kernels: coloured Gauss-Seidel sweeps (the
+// reference's computePotential update), FP64 residual and norm reductions,
+// and the FP32 conjugate-gradient iterations used inside the FP64
+// defect-correction solve.
+//
+// Update rule restated from Grid_3d::Table::computePotential
+// (tapsim/grid_3d.cpp:1317-1371):
+//   Dirichlet row: unchanged
+//   Neumann row:   phi_i = (sum_j c_ij phi_j - q_i) / sum_j c_ij      (all j)
+//   other rows:    the same sums skipping Neumann neighbours
+// The skip is folded into ceff (0 for a Neumann neighbour of a non-Neumann
+// row), so every free row is phi_i = (sum_j ceff_ij phi_j - q_i) / diag_i.
+#include "kernels.cuh"
+
+namespace tgd {
+namespace {
+
+constexpr int kBlock = 256;
+
+__global__ void k_sweep64(DevMesh m, const int32_t* __restrict__ rows, int count, double* maxdev) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double dev = 0.0;
+    if (t < count) {
+        const int i = rows[t];
+        const int q0 = m.row_ptr[i], q1 = m.row_ptr[i + 1];
+        double s = 0.0;
+        for (int q = q0; q < q1; q++) s += m.ceff64[q] * m.phi64[m.col[q]];
+        const double d = m.diag64[i];
+        const double v = (s - m.q64[i]) / d;
+        if (!(v == v)) {
+            atomicOr(m.status, S_NAN);
+        } else {
+            dev = fabs(v - m.phi64[i]);
+            m.phi64[i] = v;
+        }
+    }
+    if (maxdev) {
+        __shared__ double red[kBlock / 32];
+        dev = warp_max_d(dev);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dev;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double v = threadIdx.x < kBlock / 32 ? red[threadIdx.x] : 0.0;
+            v = warp_max_d(v);
+            if (threadIdx.x == 0 && v > 0.0) atomic_max_double_nonneg(maxdev, v);
+        }
+    }
+}
+
+__global__ void k_residual(DevMesh m, const int32_t* __restrict__ rows, int count, float* r32, double* acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double r = 0.0;
+    if (t < count) {
+        const int i = rows[t];
+        const int q0 = m.row_ptr[i], q1 = m.row_ptr[i + 1];
+        double s = 0.0;
+        for (int q = q0; q < q1; q++) s += m.ceff64[q] * m.phi64[m.col[q]];
+        r = s - m.diag64[i] * m.phi64[i] - m.q64[i];
+        if (r32) r32[i] = (float)r;
+    }
+    block_sum_atomic<kBlock>(r * r, acc);
+}
+
+__global__ void k_bnorm(DevMesh m, const int32_t* __restrict__ rows, int count, double* acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double b = 0.0;
+    if (t < count) {
+        const int i = rows[t];
+        const int q0 = m.row_ptr[i], q1 = m.row_ptr[i + 1];
+        double s = 0.0;
+        for (int q = q0; q < q1; q++) {
+            const int j = m.col[q];
+            if (m.flags[j] & F_DIRICHLET) s += m.ceff64[q] * m.phi64[j];
+        }
+        b = s - m.q64[i];
+    }
+    block_sum_atomic<kBlock>(b * b, acc);
+}
+
+// z = r / diag, p = z, rz -> scal[0]
+__global__ void k_cg_init(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double rz = 0.0;
+    if (t < count) {
+        const int i = rows[t];
+        const float r = v.r[i];
+        const float z = r / m.diag32[i];
+        v.z[i] = z;
+        v.p[i] = z;
+        v.x[i] = 0.0f;
+        rz = (double)r * (double)z;
+    }
+    block_sum_atomic<kBlock>(rz, &v.scal[0]);
+}
+
+// ap = A p on the rows (A = diag - offdiag), pAp -> scal[3it+1]
+__global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
+    if (v.scal[3 * it] <= target) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double pap = 0.0;
+    if (t < count) {
+        const int i = rows[t];
+        const int q0 = m.row_ptr[i], q1 = m.row_ptr[i + 1];
+        float s = 0.0f;
+        for (int q = q0; q < q1; q++) s += m.ceff32[q] * v.p[m.col[q]];
+        const float pi = v.p[i];
+        const float ap = m.diag32[i] * pi - s;
+        v.ap[i] = ap;
+        pap = (double)pi * (double)ap;
+    }
+    block_sum_atomic<kBlock>(pap, &v.scal[3 * it + 1]);
+}
+
+// x += a p, r -= a ap, z = r/diag, rz_next -> scal[3(it+1)]
+__global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
+    const double rz = v.scal[3 * it];
+    if (rz <= target) return;
+    const double pap = v.scal[3 * it + 1];
+    const float alpha = pap > 0.0 ? (float)(rz / pap) : 0.0f;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double rzn = 0.0;
+    if (t < count) {
+        const int i = rows[t];
+        v.x[i] += alpha * v.p[i];
+        const float r = v.r[i] - alpha * v.ap[i];
+        v.r[i] = r;
+        const float z = r / m.diag32[i];
+        v.z[i] = z;
+        rzn = (double)r * (double)z;
+    }
+    block_sum_atomic<kBlock>(rzn, &v.scal[3 * (it + 1)]);
+}
+
+// p = z + beta p
+__global__ void k_cg_pupdate(const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
+    const double rz = v.scal[3 * it];
+    if (rz <= target) return;
+    const double rzn = v.scal[3 * (it + 1)];
+    const float beta = (float)(rzn / rz);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) {
+        const int i = rows[t];
+        v.p[i] = v.z[i] + beta * v.p[i];
+    }
+}
+
+__global__ void k_add_coupled(DevMesh m, const int32_t* __restrict__ rows, int count, const float* xV, float* r) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int i = rows[t];
+    float s = 0.0f;
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) s += m.ceff32[q] * xV[m.col[q]];
+    r[i] += s;
+}
+
+__global__ void k_apply_correction(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int i = rows[t];
+    m.phi64[i] += (double)v.x[i];
+    v.x[i] = 0.0f;
+    v.r[i] = 0.0f;
+    v.z[i] = 0.0f;
+    v.p[i] = 0.0f;
+    v.ap[i] = 0.0f;
+}
+
+__global__ void k_rebuild_rows(DevMesh m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    const bool neuI = (m.flags[i] & F_NEUMANN) != 0;
+    double d = 0.0;
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+        const bool neuJ = (m.flags[m.col[q]] & F_NEUMANN) != 0;
+        const double c = (!neuI && neuJ) ? 0.0 : m.c64[q];
+        m.ceff64[q] = c;
+        m.ceff32[q] = (float)c;
+        d += c;
+    }
+    m.diag64[i] = d;
+    m.diag32[i] = (float)d;
+}
+
+// Breadth-first k-hop neighbourhood of one node, one block.  The visited set
+// is an open-addressing hash in shared memory; frontiers live in global
+// scratch.  Non-Dirichlet members are written grouped by colour.
+constexpr int kHashSize = 8192;
+
+__global__ void k_local_set(DevMesh m, int node, int hops, int32_t* out, int32_t* outCount, int cap, int32_t* scratch,
+                            int scratchCap, int ncolours) {
+    __shared__ int32_t hashKeys[kHashSize];
+    __shared__ int frontierStart, frontierEnd, tail, overflow;
+    __shared__ int colourCount[64], colourOffset[64];
+    for (int k = threadIdx.x; k < kHashSize; k += blockDim.x) hashKeys[k] = -1;
+    if (threadIdx.x < 64) colourCount[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+        scratch[0] = node;
+        frontierStart = 0;
+        frontierEnd = 1;
+        tail = 1;
+        overflow = 0;
+    }
+    __syncthreads();
+    // the start node is only recorded when reached again (find_localNodes)
+    for (int h = 0; h < hops; h++) {
+        const int fs = frontierStart, fe = frontierEnd;
+        for (int f = fs + threadIdx.x; f < fe; f += blockDim.x) {
+            const int u = scratch[f];
+            for (int q = m.row_ptr[u]; q < m.row_ptr[u + 1]; q++) {
+                const int v = m.col[q];
+                uint32_t hsh = ((uint32_t)v * 2654435761u) & (kHashSize - 1);
+                bool inserted = false;
+                for (int probe = 0; probe < kHashSize; probe++) {
+                    const int prev = atomicCAS(&hashKeys[hsh], -1, v);
+                    if (prev == -1) { inserted = true; break; }
+                    if (prev == v) break;
+                    hsh = (hsh + 1) & (kHashSize - 1);
+                }
+                if (inserted) {
+                    const int pos = atomicAdd(&tail, 1);
+                    if (pos < scratchCap) scratch[pos] = v;
+                    else overflow = 1;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            frontierStart = fe;
+            frontierEnd = min(tail, scratchCap);
+        }
+        __syncthreads();
+    }
+    // members: scratch[1 .. tail) plus the start node if it was reached again
+    const int members = min(tail, scratchCap);
+    for (int f = 1 + threadIdx.x; f < members; f += blockDim.x) {
+        const int v = scratch[f];
+        if (!(m.flags[v] & F_DIRICHLET)) atomicAdd(&colourCount[m.colour[v]], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int c = 0; c < ncolours; c++) {
+            colourOffset[c] = s;
+            outCount[c] = colourCount[c];
+            s += colourCount[c];
+            colourCount[c] = 0;
+        }
+        outCount[ncolours] = s;
+        outCount[ncolours + 1] = overflow;
+    }
+    __syncthreads();
+    for (int f = 1 + threadIdx.x; f < members; f += blockDim.x) {
+        const int v = scratch[f];
+        if (!(m.flags[v] & F_DIRICHLET)) {
+            const int c = m.colour[v];
+            const int pos = colourOffset[c] + atomicAdd(&colourCount[c], 1);
+            if (pos < cap) out[pos] = v;
+        }
+    }
+}
+
+inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* maxdev, cudaStream_t s) {
+    if (count > 0) k_sweep64<<<blocks(count), kBlock, 0, s>>>(m, rows, count, maxdev);
+}
+void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s) {
+    if (count > 0) k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, acc);
+}
+void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s) {
+    if (count > 0) k_bnorm<<<blocks(count), kBlock, 0, s>>>(m, rows, count, acc);
+}
+void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
+    if (count > 0) k_cg_init<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v);
+}
+void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double target,
+                    cudaStream_t s) {
+    if (count <= 0) return;
+    k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target);
+    k_cg_update<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target);
+    k_cg_pupdate<<<blocks(count), kBlock, 0, s>>>(rows, count, v, it, target);
+}
+void launch_add_coupled(const DevMesh& m, const int32_t* rows, int count, const float* xV, float* r, cudaStream_t s) {
+    if (count > 0) k_add_coupled<<<blocks(count), kBlock, 0, s>>>(m, rows, count, xV, r);
+}
+void launch_apply_correction(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
+    if (count > 0) k_apply_correction<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v);
+}
+void launch_rebuild_rows(const DevMesh& m, cudaStream_t s) {
+    if (m.n > 0) k_rebuild_rows<<<blocks(m.n), kBlock, 0, s>>>(m);
+}
+void launch_local_set(const DevMesh& m, int node, int hops, int32_t* out, int32_t* outCount, int cap, int32_t* scratch,
+                      int scratchCap, int ncolours, cudaStream_t s) {
+    k_local_set<<<1, 512, 0, s>>>(m, node, hops, out, outCount, cap, scratch, scratchCap, ncolours);
+}
+
+}  // namespace tgd

@@ -1,0 +1,455 @@
+"""Host-side mirror of the reference's hot-path interface over the C ABI.
+
+Grid collects what Process::evaporation (tapsim/process.cpp:441-1124) calls
+on Grid_3d::Table, Surface_3d::Table and Trajectory_3d, backed by one device
+handle.  EvaporationOptions reads tapsim.ini with the reference's keys and
+strictness (Process::EvaporationOptions::setDefaults, process.cpp:206-439),
+and Evaporation runs the event loop with its voltage queue and results log.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import struct
+from collections import deque
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+E_CHARGE = 1.60217733e-19   # Trajectory_3d::eCharge (trajectory_3d.h:91)
+AMU2KG = 1.660538782e-27     # Trajectory_3d::amu2kg (trajectory_3d.h:93)
+
+
+class Mesh:
+    """Host mesh (tg_mesh): node set, Delaunay tetrahedra, FP64 Voronoi couplings."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        self._desc = N.tg_mesh_desc()
+        nnz = C.c_int32()
+        N.check(N.lib().tg_mesh_describe(self._h, C.byref(self._desc), C.byref(nnz)))
+        self.nnz = nnz.value
+
+    @staticmethod
+    def tip_params(**kw) -> N.tg_tip_params:
+        p = N.tg_tip_params()
+        N.lib().tg_tip_params_default(C.byref(p))
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise KeyError(k)
+            setattr(p, k, v)
+        return p
+
+    @classmethod
+    def from_tip(cls, threads: int = 0, **kw) -> "Mesh":
+        h = C.c_void_p()
+        N.check(N.lib().tg_mesh_from_tip(C.byref(cls.tip_params(**kw)), threads, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_files(cls, node_file: str, config_file: str, threads: int = 0) -> "Mesh":
+        h = C.c_void_p()
+        N.check(N.lib().tg_mesh_from_files(str(node_file).encode(), str(config_file).encode(), threads, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_dump(cls, dump_file: str, config_file: str | None = None) -> "Mesh":
+        h = C.c_void_p()
+        cfg = str(config_file).encode() if config_file else None
+        N.check(N.lib().tg_mesh_from_dump(str(dump_file).encode(), cfg, C.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            N.lib().tg_mesh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def desc(self) -> N.tg_mesh_desc:
+        return self._desc
+
+    @property
+    def num_nodes(self) -> int:
+        return self._desc.num_nodes
+
+    def arrays(self) -> dict:
+        """Copies of the description arrays (node-file order)."""
+        d = self._desc
+        n, nnz, nt = d.num_nodes, self.nnz, d.num_tets
+
+        def arr(p, dtype, count):
+            if not p:
+                return None
+            ct = np.ctypeslib.as_ctypes_type(np.dtype(dtype))
+            return np.ctypeslib.as_array((ct * count).from_address(p)).copy()
+
+        types = [d.types[k] for k in range(d.num_types)]
+        return {
+            "xyz": arr(d.xyz, np.float32, 3 * n).reshape(n, 3),
+            "type": arr(d.type_id, np.int8, n),
+            "hull": arr(d.hull, np.uint8, n),
+            "phi": arr(d.phi, np.float32, n),
+            "row_ptr": arr(d.row_ptr, np.int32, n + 1),
+            "col": arr(d.col, np.int32, nnz),
+            "coupling": arr(d.coupling, np.float64, nnz),
+            "geom": arr(d.geom, np.float64, nnz),
+            "area_pos": arr(d.area_pos, np.uint8, nnz),
+            "volume": arr(d.volume, np.float64, n),
+            "tet_v": arr(d.tet_v, np.int32, 4 * nt).reshape(nt, 4) if nt else None,
+            "tet_n": arr(d.tet_n, np.int32, 4 * nt).reshape(nt, 4) if nt else None,
+            "node_tet": arr(d.node_tet, np.int32, n),
+            "types": {t.id: {f: getattr(t, f) for f, _ in N.tg_type._fields_} for t in types},
+        }
+
+    def write_node_file(self, path: str, binary: bool = True):
+        N.check(N.lib().tg_mesh_write_node_file(self._h, str(path).encode(), int(binary)))
+
+    def write_config(self, path: str):
+        N.check(N.lib().tg_mesh_write_config(self._h, str(path).encode()))
+
+    def write_dump(self, path: str, phi: np.ndarray | None = None):
+        p = None if phi is None else np.ascontiguousarray(phi, np.float32)
+        N.check(N.lib().tg_mesh_write_dump(self._h, str(path).encode(), N.ptr(p)))
+
+
+def trace_opts(time_step=1e-14, min_time_step=1e-16, error_threshold=1e-6, max_steps=100000, stepper_limit=200,
+               walk_limit=100000) -> N.tg_trace_opts:
+    return N.tg_trace_opts(time_step, min_time_step, error_threshold, max_steps, stepper_limit, walk_limit)
+
+
+def solve_opts(rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4) -> N.tg_solve_opts:
+    return N.tg_solve_opts(rel_tol, max_outer, max_inner, inner_rtol)
+
+
+class Grid:
+    """Device state of one mesh: Grid_3d::Table + Surface_3d::Table + flights."""
+
+    def __init__(self, mesh: Mesh):
+        self.mesh = mesh
+        self._h = C.c_void_p()
+        N.check(N.lib().tg_create(C.byref(mesh.desc), C.byref(self._h)))
+        self.n = mesh.num_nodes
+        self.nnz = mesh.nnz
+
+    def close(self):
+        if self._h:
+            N.lib().tg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        return N.check(rc, self._h)
+
+    # Grid_3d::Table
+    def relax(self, cycles: int) -> float:
+        dev = C.c_double()
+        self._ck(N.lib().tg_relax_cycles(self._h, cycles, C.byref(dev)))
+        return dev.value
+
+    def relax_threshold(self, threshold: float, cycle: int, queue: int, max_sweeps: int = 0):
+        it, dev = C.c_int64(), C.c_double()
+        rc = N.lib().tg_relax_threshold(self._h, threshold, cycle, queue, max_sweeps, C.byref(it), C.byref(dev))
+        if rc not in (N.TG_OK, N.TG_ERR_RELAX_FAULT, N.TG_ERR_ITERATION_CAP):
+            self._ck(rc)
+        return rc, it.value, dev.value
+
+    def local_relax(self, node: int, shell: int, threshold: float, cycle: int, queue: int):
+        it, dev = C.c_int64(), C.c_double()
+        rc = N.lib().tg_local_relax(self._h, node, shell, threshold, cycle, queue, C.byref(it), C.byref(dev))
+        if rc not in (N.TG_OK, N.TG_ERR_RELAX_FAULT, N.TG_ERR_ITERATION_CAP):
+            self._ck(rc)
+        return rc, it.value, dev.value
+
+    def solve(self, rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4) -> N.tg_solve_info:
+        info = N.tg_solve_info()
+        self._ck(N.lib().tg_solve(self._h, C.byref(solve_opts(rel_tol, max_outer, max_inner, inner_rtol)),
+                                  C.byref(info)))
+        return info
+
+    def residual(self) -> float:
+        r = C.c_double()
+        self._ck(N.lib().tg_residual(self._h, C.byref(r)))
+        return r.value
+
+    def potentials(self) -> np.ndarray:
+        out = np.empty(self.n, np.float64)
+        self._ck(N.lib().tg_get_phi(self._h, N.ptr(out)))
+        return out
+
+    def set_potentials(self, phi: np.ndarray):
+        p = np.ascontiguousarray(phi, np.float64)
+        self._ck(N.lib().tg_set_phi(self._h, N.ptr(p)))
+
+    def field_o1(self, nodes) -> np.ndarray:
+        nd = np.ascontiguousarray(np.atleast_1d(nodes), np.int32)
+        out = np.empty((len(nd), 3), np.float64)
+        self._ck(N.lib().tg_field_o1(self._h, len(nd), N.ptr(nd), N.ptr(out)))
+        return out
+
+    def couplings(self) -> np.ndarray:
+        out = np.empty(self.nnz, np.float64)
+        self._ck(N.lib().tg_get_couplings(self._h, N.ptr(out)))
+        return out
+
+    def types(self) -> np.ndarray:
+        out = np.empty(self.n, np.int8)
+        self._ck(N.lib().tg_get_types(self._h, N.ptr(out)))
+        return out
+
+    # Surface_3d
+    def surface_init(self, vacuum_id: int) -> int:
+        ns = C.c_int32()
+        self._ck(N.lib().tg_surface_init(self._h, vacuum_id, C.byref(ns)))
+        return ns.value
+
+    def select(self) -> N.tg_select_info:
+        info = N.tg_select_info()
+        rc = N.lib().tg_surface_select(self._h, C.byref(info))
+        if rc not in (N.TG_OK, N.TG_ERR_NO_SURFACE):
+            self._ck(rc)
+        return info
+
+    def surface(self):
+        cnt = C.c_int32()
+        self._ck(N.lib().tg_get_surface(self._h, 0, None, None, C.byref(cnt)))
+        nodes = np.empty(cnt.value, np.int32)
+        ratios = np.empty(cnt.value, np.float32)
+        self._ck(N.lib().tg_get_surface(self._h, cnt.value, N.ptr(nodes), N.ptr(ratios), C.byref(cnt)))
+        order = np.argsort(nodes)
+        return nodes[order], ratios[order]
+
+    def normal(self, node: int) -> np.ndarray:
+        out = np.empty(3, np.float32)
+        self._ck(N.lib().tg_surface_normal(self._h, node, N.ptr(out)))
+        return out
+
+    def take_away(self, node: int) -> list[int]:
+        cap = 256
+        det = np.empty(cap, np.int32)
+        nd = C.c_int32()
+        self._ck(N.lib().tg_take_away(self._h, node, cap, N.ptr(det), C.byref(nd)))
+        return det[: min(nd.value, cap)].tolist()
+
+    def update_coordination(self):
+        self._ck(N.lib().tg_update_coordination(self._h))
+
+    # Trajectory_3d
+    def trace(self, start: np.ndarray, qm, tet_guess=None, vel=None, **opts) -> np.ndarray:
+        start = np.ascontiguousarray(np.atleast_2d(start), np.float32)
+        n = len(start)
+        q = np.ascontiguousarray(np.broadcast_to(np.asarray(qm, np.float32), (n,)))
+        g = None if tet_guess is None else np.ascontiguousarray(np.broadcast_to(np.asarray(tet_guess, np.int32), (n,)))
+        v = None if vel is None else np.ascontiguousarray(np.atleast_2d(vel), np.float32)
+        out = (N.tg_impact * n)()
+        self._ck(N.lib().tg_trace(self._h, n, N.ptr(start), N.ptr(v), N.ptr(q), N.ptr(g),
+                                  C.byref(trace_opts(**opts)), C.cast(out, C.c_void_p)))
+        return out
+
+    def potential_at(self, xyz: np.ndarray, tet_guess=None) -> np.ndarray:
+        xyz = np.ascontiguousarray(np.atleast_2d(xyz), np.float32)
+        g = None if tet_guess is None else np.ascontiguousarray(tet_guess, np.int32)
+        out = np.empty(len(xyz), np.float32)
+        self._ck(N.lib().tg_potential_at(self._h, len(xyz), N.ptr(xyz), N.ptr(g), N.ptr(out)))
+        return out
+
+    def run_event(self, opts: N.tg_event_opts, event_index: int) -> N.tg_event_record:
+        rec = N.tg_event_record()
+        self._ck(N.lib().tg_run_event(self._h, C.byref(opts), event_index, C.byref(rec)))
+        return rec
+
+
+# ---- tapsim.ini -----------------------------------------------------------
+
+# Process::EvaporationOptions keys (process.cpp:206-439) with the internal
+# defaults of makeIniList (commands.cpp:1249-1325)
+INI_DEFAULTS = {
+    "RESULTS_FILENAME": "results_data", "RESULTS_BINARY_OUTPUT": "0", "RESULTS_CHUNK_SIZE": "10000",
+    "TRAJECTORY_FILENAME": "trajectory_data", "TRAJECTORY_BINARY_OUTPUT": "1", "TRAJECTORY_CHUNK_SIZE": "10000",
+    "GRID_FILENAME": "grid_data", "GRID_BINARY_OUTPUT": "1", "GRID_INTERVAL": "2147483647",
+    "SURFACE_FILENAME": "surface_data", "SURFACE_BINARY_OUTPUT": "1", "SURFACE_INTERVAL": "2147483647",
+    "GEOMETRY_FILENAME": "geometry.dat", "GEOMETRY_BINARY_OUTPUT": "1", "GEOMETRY_CONTENTS": "0xff",
+    "DUMP_FILENAME": "dump", "DUMP_INTERVAL": "10000", "OUTPUT_DELAY_TIME": "60",
+    "METHOD_EVAPORATION_PROBABILITY": "0", "METHOD_EVAPORATION_CHOICE": "0", "VACUUM_CELL_IDENTIFIER": "Vacuum",
+    "TRAJECTORY_INTEGRATOR_TYPE": "1", "TRAJECTORY_STEPPER_TYPE": "1", "TRAJECTORY_INITIAL_TIME_STEP": "1e-14",
+    "TRAJECTORY_MINIMUM_TIME_STEP": "1e-16", "TRAJECTORY_ERROR_THRESHOLD": "1e-6",
+    "TRAJECTORY_NON_RANDOM_START_POSITION": "1", "TRAJECTORY_NO_INITIAL_VELOCITY": "1",
+    "VOLTAGE_QUEUE_SIZE": "250", "LOCAL_RELAXATION_ERROR_THRESHOLD": "1e-2", "LOCAL_RELAXATION_SHELL_SIZE": "3",
+    "LOCAL_RELAXATION_CYCLE_SIZE": "5", "LOCAL_RELAXATION_QUEUE_SIZE": "5", "GLOBAL_RELAXATION_STEPS": "1",
+    "REFRESH_RELAXATION_INTERVAL": "0", "REFRESH_RELAXATION_ERROR_THRESHOLD": "0.0",
+    "REFRESH_RELAXATION_CYCLE_SIZE": "100", "REFRESH_RELAXATION_QUEUE_SIZE": "25",
+}
+
+
+def read_ini(path: str | None) -> dict:
+    """File_Io::readInitialization: 'KEY = VALUE' lines, '#' comments, unique keys."""
+    if path is None:
+        return dict(INI_DEFAULTS)
+    values = {}
+    for line in Path(path).read_text().splitlines():
+        if not line or line.startswith("#"):
+            continue
+        if " = " not in line:
+            raise ValueError(f"ini: bad line {line!r}")
+        k, v = line.split(" = ", 1)
+        k, v = k.strip(), v.strip()
+        if k in values:
+            raise ValueError(f"ini: duplicate key {k}")
+        values[k] = v
+    return values
+
+
+@dataclass
+class EvaporationOptions:
+    values: dict = field(default_factory=lambda: dict(INI_DEFAULTS))
+
+    @classmethod
+    def from_ini(cls, path: str | None) -> "EvaporationOptions":
+        v = read_ini(path)
+        missing = [k for k in INI_DEFAULTS if k not in v]
+        if missing:
+            # setDefaults throws on the first missing key
+            raise ValueError(f"EvaporationOptions::setDefaults(): '{missing[0]}' error!")
+        return cls(v)
+
+    def i(self, k):
+        return int(self.values[k], 0) if k == "GEOMETRY_CONTENTS" else int(float(self.values[k]))
+
+    def f(self, k):
+        return float(self.values[k])
+
+    def s(self, k):
+        return self.values[k]
+
+    def event_opts(self, vacuum_id: int, relax_mode: int, solve: N.tg_solve_opts | None = None,
+                   trace: bool = True, normal: bool = True, refresh_max_sweeps: int = 2_000_000) -> N.tg_event_opts:
+        o = N.tg_event_opts()
+        o.vacuum_id = vacuum_id
+        o.relax_mode = relax_mode
+        o.local_threshold = self.f("LOCAL_RELAXATION_ERROR_THRESHOLD")
+        o.local_shell = self.i("LOCAL_RELAXATION_SHELL_SIZE")
+        o.local_cycle = self.i("LOCAL_RELAXATION_CYCLE_SIZE")
+        o.local_queue = self.i("LOCAL_RELAXATION_QUEUE_SIZE")
+        o.global_steps = self.i("GLOBAL_RELAXATION_STEPS")
+        o.refresh_interval = self.i("REFRESH_RELAXATION_INTERVAL")
+        o.refresh_threshold = self.f("REFRESH_RELAXATION_ERROR_THRESHOLD")
+        o.refresh_cycle = self.i("REFRESH_RELAXATION_CYCLE_SIZE")
+        o.refresh_queue = self.i("REFRESH_RELAXATION_QUEUE_SIZE")
+        o.refresh_max_sweeps = refresh_max_sweeps
+        o.solve = solve if solve is not None else solve_opts()
+        o.trace = trace_opts(self.f("TRAJECTORY_INITIAL_TIME_STEP"), self.f("TRAJECTORY_MINIMUM_TIME_STEP"),
+                             self.f("TRAJECTORY_ERROR_THRESHOLD"))
+        o.trace_enabled = int(trace)
+        o.normal_enabled = int(normal)
+        return o
+
+
+# ---- event loop -------------------------------------------------------------
+
+RESULT_FIELDS = ["index", "id", "number", "voltage", "startX", "startY", "startZ", "stopX", "stopY", "stopZ", "tof",
+                 "probability", "potentialBefore", "fieldBeforeX", "fieldBeforeY", "fieldBeforeZ", "potentialAfter",
+                 "fieldAfterX", "fieldAfterY", "fieldAfterZ", "normalX", "normalY", "normalZ", "apexX", "apexY",
+                 "apexZ"]
+
+
+class Evaporation:
+    """Process::evaporation (process.cpp:441-1124) over one device Grid."""
+
+    def __init__(self, grid: Grid, options: EvaporationOptions, relax_mode: int = 1,
+                 solve: N.tg_solve_opts | None = None, trace: bool = True, normal: bool = True):
+        self.grid = grid
+        self.options = options
+        types = grid.mesh.arrays()["types"]
+        name = options.s("VACUUM_CELL_IDENTIFIER")
+        self.vacuum_id = self._type_id_by_name(grid, name)
+        self.evap_field = {k: v["evap_field"] for k, v in types.items()}
+        self.opts = options.event_opts(self.vacuum_id, relax_mode, solve, trace, normal)
+        self.voltage_queue: deque = deque()
+        self.voltage_sum = 0.0
+        self.queue_size = options.i("VOLTAGE_QUEUE_SIZE")
+        self.event = 0
+        self.records: list[dict] = []
+        grid.surface_init(self.vacuum_id)
+        grid.select()
+
+    @staticmethod
+    def _type_id_by_name(grid: Grid, name: str) -> int:
+        names = getattr(grid.mesh, "type_names", None)
+        if names and name in names:
+            return names[name]
+        # meshgen's vacuum marker is id 0 in every generated configuration
+        return 0
+
+    def step(self) -> dict:
+        self.event += 1
+        rec = self.grid.run_event(self.opts, self.event)
+        r = self._record(rec)
+        self.records.append(r)
+        return r
+
+    def _record(self, rec: N.tg_event_record) -> dict:
+        """Step VI: voltage queue and time-of-flight scale (process.cpp:985-1036)."""
+        imp = rec.impact
+        fb = math.sqrt(sum(float(x) ** 2 for x in rec.field_before))
+        if imp.last_tet >= 0 and fb != 0.0:
+            v = (rec.phi_before - imp.last_phi) * self.evap_field[rec.type_id] / fb / rec.scaling_reference
+            self.voltage_queue.append(v)
+            self.voltage_sum += v
+            while len(self.voltage_queue) > self.queue_size:
+                self.voltage_sum -= self.voltage_queue.popleft()
+            voltage = self.voltage_sum / len(self.voltage_queue)
+            ts = (rec.phi_after - imp.last_phi) / voltage
+            time_scale = math.sqrt(ts) if ts >= 0 else float("nan")
+        else:
+            voltage = 1.0 if fb == 0.0 else 0.0
+            time_scale = 1.0
+        return {
+            "index": self.event, "node": rec.node, "id": rec.type_id, "number": rec.node + 1, "voltage": voltage,
+            "stop": tuple(imp.stop), "tof": imp.stop_time * time_scale, "probability": rec.probability,
+            "best": rec.best_ratio, "second": rec.second_ratio, "scaling_reference": rec.scaling_reference,
+            "potentialBefore": rec.phi_before, "fieldBefore": tuple(rec.field_before),
+            "potentialAfter": rec.phi_after, "fieldAfter": tuple(rec.field_after), "normal": tuple(rec.normal),
+            "apex": tuple(rec.apex), "status": imp.status, "steps": imp.steps, "detached": rec.detached,
+            "relax_iterations": rec.relax_iterations, "rel_residual": rec.rel_residual,
+        }
+
+
+def write_results(path: str, records: list[dict], xyz: np.ndarray, binary: bool = False, header: str = ""):
+    """LogResults record layout (logResults.cpp:135-381)."""
+    with open(path, "wb") as f:
+        f.write(b"TAPSIM RESULTS DATA\nVERSION 1.0\n" + header.encode())
+        units = ["[1]", "[1]", "[1]", "[V]"] + ["[m]"] * 6 + ["[s]", "[1]"] + \
+                ["[V]", "[V/m]", "[V/m]", "[V/m]"] * 2 + ["[m]"] * 6
+        types = ["int", "int", "unsigned int"] + ["float"] * 23
+        for k, name in enumerate(RESULT_FIELDS):
+            u = units[k]
+            if binary:
+                if name.startswith("potential"):
+                    u = "[1]"
+                f.write(f"# {name} {u} ({types[k]})\n".encode())
+            else:
+                f.write(f"# {name} {u}\n".encode())
+        f.write(b"BINARY\n" if binary else b"ASCII\n")
+        for r in records:
+            start = xyz[r["node"]]
+            vals = [r["voltage"], *start, *r["stop"], r["tof"], r["probability"], r["potentialBefore"],
+                    *r["fieldBefore"], r["potentialAfter"], *r["fieldAfter"], *r["normal"], *r["apex"]]
+            if binary:
+                f.write(struct.pack("<IhI", r["index"], r["id"], r["number"]))
+                f.write(struct.pack("<23f", *vals))
+            else:
+                f.write(("\t".join([str(r["index"]), str(r["id"]), str(r["number"])] +
+                                   [f"{v:e}" for v in vals]) + "\n").encode())

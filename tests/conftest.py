@@ -1,0 +1,57 @@
+import gzip
+import shutil
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLDEN = ROOT / "tests" / "golden"
+sys.path.insert(0, str(ROOT))
+
+QM_FE = 2 * 1.60217733e-19 / (55.845 * 1.660538782e-27)
+
+# small tip used by the device parity tests (about 9k nodes)
+SMALL_TIP = dict(cap_radius=1.5e-9, shank_length=2.0e-9, half_angle_deg=0.0, fine_shell=0.6e-9,
+                 box_half_width=10e-9, box_height=40e-9, seed=7)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+@pytest.fixture(scope="session")
+def golden_dump(tmp_path_factory):
+    """The reference's TAPSIM dump of the golden tip (its TetGen mesh and float couplings)."""
+    d = tmp_path_factory.mktemp("golden") / "ref_mesh.dump"
+    with gzip.open(GOLDEN / "ref_mesh.dump.gz") as f, open(d, "wb") as g:
+        shutil.copyfileobj(f, g)
+    return d
+
+
+@pytest.fixture(scope="session")
+def ref_events():
+    return np.loadtxt(GOLDEN / "ref_events.txt")
+
+
+@pytest.fixture(scope="session")
+def ref_phi0():
+    return np.fromfile(GOLDEN / "ref_phi0.bin", np.float32)
+
+
+@pytest.fixture(scope="session")
+def ref_mesh(golden_dump):
+    from tapsim_modified_b200.tapsim import Mesh
+    return Mesh.from_dump(str(golden_dump), str(GOLDEN / "tip.cfg"))
+
+
+@pytest.fixture(scope="session")
+def small_mesh():
+    from tapsim_modified_b200.tapsim import Mesh
+    return Mesh.from_tip(**SMALL_TIP)
+
+
+def free_mask(arrays):
+    types = arrays["types"]
+    return np.array([not types[int(t)]["dirichlet"] for t in arrays["type"]])

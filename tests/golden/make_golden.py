@@ -1,0 +1,73 @@
+"""Generates the golden fixtures of the test suite by running the reference
+TAPSim built from its own sources (oracle/_ref, `make -C oracle ref`).
+
+    python tests/golden/make_golden.py
+
+Inputs are produced by this project's tip generator (a small bcc Fe [110]
+tip in a coarsened vacuum box) and written in the reference's formats.  The
+reference then meshes them with TetGen, relaxes, and evaporates with the
+"oracle" ini (global relaxation to the float fixed point after every event,
+maximum-probability choice).  Outputs:
+
+    tip.nodes        node file (BINARY, meshgen layout)
+    tip.cfg          configuration (ASCII)
+    oracle.ini       evaporation options
+    ref_mesh.dump.gz the reference's TAPSIM dump right after fastSync
+                     (its TetGen tetrahedra and float couplings)
+    ref_phi0.bin     float32 potential() of all nodes after the initial
+                     relaxation
+    ref_events.txt   one line per event (ref_harness evap columns)
+    ref_phi_events.bin.gz  float32 potentials after each event
+"""
+from __future__ import annotations
+
+import gzip
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+from tapsim_modified_b200.tapsim import INI_DEFAULTS, Mesh  # noqa: E402
+
+HARNESS = ROOT / "oracle" / "_ref" / "ref_harness"
+
+# small tip: R = 1.5 nm cap on a 2 nm shank, 0.6 nm lattice-vacuum shell,
+# vacuum box 20 nm wide and 40 nm high
+TIP = dict(cap_radius=1.5e-9, shank_length=2.0e-9, half_angle_deg=0.0, fine_shell=0.6e-9,
+           box_half_width=10e-9, box_height=40e-9, seed=7)
+N_EVENTS = 40
+
+
+def main():
+    if not HARNESS.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    mesh = Mesh.from_tip(**TIP)
+    mesh.write_node_file(str(HERE / "tip.nodes"), binary=True)
+    mesh.write_config(str(HERE / "tip.cfg"))
+    ini = dict(INI_DEFAULTS)
+    ini.update({"REFRESH_RELAXATION_INTERVAL": "1", "REFRESH_RELAXATION_ERROR_THRESHOLD": "0.0",
+                "RESULTS_FILENAME": "", "TRAJECTORY_FILENAME": "", "GRID_FILENAME": "", "SURFACE_FILENAME": "",
+                "GEOMETRY_FILENAME": "", "DUMP_FILENAME": ""})
+    (HERE / "oracle.ini").write_text("".join(f"{k} = {v}\n" for k, v in ini.items()))
+    tmp = HERE / "_tmp"
+    tmp.mkdir(exist_ok=True)
+    subprocess.run([str(HARNESS), "mesh", str(HERE / "tip.cfg"), str(HERE / "tip.nodes"), str(tmp / "ref.dump")],
+                   check=True, capture_output=True)
+    with open(tmp / "ref.dump", "rb") as f, gzip.open(HERE / "ref_mesh.dump.gz", "wb", compresslevel=9) as g:
+        shutil.copyfileobj(f, g)
+    subprocess.run([str(HARNESS), "evap", str(HERE / "tip.cfg"), "-", str(HERE / "oracle.ini"), str(N_EVENTS),
+                    str(HERE / "ref_events.txt"), "--dump", str(tmp / "ref.dump"), "--threads", "1",
+                    "--phi", str(HERE / "ref_phi0.bin"), "--phi-events", str(tmp / "phi_events.bin")],
+                   check=True, capture_output=True)
+    with open(tmp / "phi_events.bin", "rb") as f, gzip.open(HERE / "ref_phi_events.bin.gz", "wb", compresslevel=9) as g:
+        shutil.copyfileobj(f, g)
+    shutil.rmtree(tmp)
+    print("nodes", mesh.num_nodes, "written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

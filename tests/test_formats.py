@@ -1,0 +1,104 @@
+"""Byte-compatible file formats: node file, configuration, ini, dump, results."""
+import struct
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+def test_node_file_roundtrip(tmp_path, small_mesh):
+    from tapsim_modified_b200.tapsim import Mesh
+    a = small_mesh.arrays()
+    for binary in (True, False):
+        p = tmp_path / f"n{int(binary)}.nodes"
+        small_mesh.write_node_file(str(p), binary=binary)
+        small_mesh.write_config(str(tmp_path / "c.cfg"))
+        m2 = Mesh.from_files(str(p), str(tmp_path / "c.cfg"))
+        b = m2.arrays()
+        assert np.array_equal(a["type"], b["type"])
+        if binary:
+            assert np.array_equal(a["xyz"], b["xyz"])
+        else:
+            assert np.allclose(a["xyz"], b["xyz"], rtol=1e-8, atol=0)
+
+
+def test_binary_node_file_layout(tmp_path, small_mesh):
+    p = tmp_path / "x.nodes"
+    small_mesh.write_node_file(str(p), binary=True)
+    raw = p.read_bytes()
+    header, body = raw.split(b"\n", 1)
+    assert header == f"BINARY {small_mesh.num_nodes} 0 0".encode()
+    rec = np.frombuffer(body, dtype=[("xyz", "<f4", 3), ("id", "<i2")])
+    assert len(rec) == small_mesh.num_nodes
+
+
+def test_config_written_by_reference_layout_reads_back(tmp_path):
+    from tapsim_modified_b200.tapsim import Mesh
+    m = Mesh.from_files(str(GOLDEN / "tip.nodes"), str(GOLDEN / "tip.cfg"))
+    types = m.arrays()["types"]
+    assert types[4]["evap_field"] == pytest.approx(33e9)
+    assert types[4]["dirichlet"] == 1 and types[2]["neumann"] == 1 and types[3]["neumann"] == 1
+    assert types[1]["dirichlet"] == 1 and types[1]["phi"] == 0.0
+
+
+def test_dump_roundtrip(tmp_path, small_mesh):
+    from tapsim_modified_b200.tapsim import Mesh
+    a = small_mesh.arrays()
+    p = tmp_path / "d.dump"
+    small_mesh.write_dump(str(p))
+    b = Mesh.from_dump(str(p)).arrays()
+    assert np.array_equal(a["xyz"], b["xyz"])
+    assert np.array_equal(a["type"], b["type"])
+    assert np.array_equal(a["tet_v"], b["tet_v"])
+    assert np.array_equal(a["tet_n"], b["tet_n"])
+    assert np.array_equal(a["col"], b["col"])
+    assert np.array_equal(a["coupling"].astype(np.float32), b["coupling"].astype(np.float32))
+    assert np.array_equal(a["phi"], b["phi"])
+
+
+def test_reference_dump_reads(ref_mesh):
+    a = ref_mesh.arrays()
+    assert len(a["type"]) == 9110
+    assert (a["type"] == 4).sum() > 1000
+    # ascending neighbour lists as std::set leaves them
+    rp, col = a["row_ptr"], a["col"]
+    assert all(np.all(np.diff(col[rp[i]:rp[i + 1]]) > 0) for i in range(0, len(rp) - 1, 37))
+
+
+def test_ini_strict_keys(tmp_path):
+    from tapsim_modified_b200.tapsim import INI_DEFAULTS, EvaporationOptions
+    o = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
+    assert o.i("REFRESH_RELAXATION_INTERVAL") == 1
+    assert o.i("GEOMETRY_CONTENTS") == 0xFF
+    bad = tmp_path / "bad.ini"
+    bad.write_text("".join(f"{k} = {v}\n" for k, v in INI_DEFAULTS.items() if k != "VOLTAGE_QUEUE_SIZE"))
+    with pytest.raises(ValueError, match="VOLTAGE_QUEUE_SIZE"):
+        EvaporationOptions.from_ini(str(bad))
+    dup = tmp_path / "dup.ini"
+    dup.write_text("A = 1\nA = 2\n")
+    with pytest.raises(ValueError):
+        EvaporationOptions.from_ini(str(dup))
+
+
+def test_results_writer_layout(tmp_path):
+    from tapsim_modified_b200.tapsim import write_results
+    xyz = np.array([[1e-9, 2e-9, 3e-9]], np.float32)
+    rec = {"index": 1, "node": 0, "id": 4, "number": 1, "voltage": 1.5, "stop": (1.0, 2.0, 3.0), "tof": 1e-9,
+           "probability": 0.25, "potentialBefore": 1.0, "fieldBefore": (1.0, 2.0, 3.0), "potentialAfter": 0.9,
+           "fieldAfter": (4.0, 5.0, 6.0), "normal": (0.0, 0.0, 1.0), "apex": (0.0, 0.0, 5e-9)}
+    p = tmp_path / "r.bin"
+    write_results(str(p), [rec], xyz, binary=True)
+    raw = p.read_bytes()
+    assert raw.startswith(b"TAPSIM RESULTS DATA\nVERSION 1.0\n")
+    body = raw.split(b"BINARY\n", 1)[1]
+    # 3 integers (4+2+4 bytes) and 23 floats per event (logResults.cpp:305-329)
+    assert len(body) == 10 + 23 * 4
+    idx, tid, num = struct.unpack_from("<IhI", body)
+    assert (idx, tid, num) == (1, 4, 1)
+    vals = struct.unpack_from("<23f", body, 10)
+    assert vals[0] == 1.5 and vals[1] == pytest.approx(1e-9)
+    p2 = tmp_path / "r.txt"
+    write_results(str(p2), [rec], xyz, binary=False)
+    line = p2.read_text().splitlines()[-1].split("\t")
+    assert len(line) == 26 and line[0] == "1" and line[1] == "4"

@@ -1,0 +1,101 @@
+"""Device relaxation vs the FP64 oracle (same mesh, same couplings)."""
+import numpy as np
+import pytest
+
+from conftest import free_mask
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def solved(small_mesh):
+    from oracle import Oracle
+    from tapsim_modified_b200.tapsim import Grid
+    a = small_mesh.arrays()
+    g = Grid(small_mesh)
+    info = g.solve(rel_tol=1e-8)
+    o = Oracle(a)
+    sweeps, rel = o.solve(1e-12, 2_000_000, 1.9)
+    assert sweeps >= 0
+    return a, g, info, o
+
+
+def test_solve_reaches_tolerance(solved):
+    a, g, info, o = solved
+    assert info.rel_residual <= 1e-8
+    assert info.initial_rel_residual > 1e-3
+    # the oracle's own residual evaluation of the device potentials
+    from oracle import Oracle
+    chk = Oracle(a)
+    chk.phi[:] = g.potentials()
+    assert chk.residual() <= 1.05e-8
+
+
+def test_solve_matches_oracle_potentials(solved):
+    a, g, info, o = solved
+    phi = g.potentials()
+    free = free_mask(a)
+    # both solutions have a relative residual <= 1e-8; the potentials (0..1 V)
+    # then agree to a few 1e-7 V on this mesh
+    assert np.abs(phi - o.phi)[free].max() < 2e-6
+    # Dirichlet cells are untouched
+    assert np.array_equal(phi[~free], o.phi[~free])
+
+
+def test_device_residual_matches_oracle(solved):
+    a, g, info, o = solved
+    from oracle import Oracle
+    chk = Oracle(a)
+    chk.phi[:] = g.potentials()
+    assert abs(g.residual() - chk.residual()) <= 1e-3 * chk.residual() + 1e-15
+
+
+def test_relax_threshold_converges_to_solution(small_mesh):
+    from tapsim_modified_b200.tapsim import Grid
+    from oracle import Oracle
+    a = small_mesh.arrays()
+    g = Grid(small_mesh)
+    rc, it, dev = g.relax_threshold(1e-11, 100, 25, max_sweeps=200_000)
+    assert rc == 0 and dev <= 1e-11
+    o = Oracle(a)
+    o.solve(1e-12, 2_000_000, 1.9)
+    free = free_mask(a)
+    assert np.abs(g.potentials() - o.phi)[free].max() < 1e-6
+
+
+def test_relax_cycles_deviation_decreases(small_mesh):
+    from tapsim_modified_b200.tapsim import Grid
+    g = Grid(small_mesh)
+    d1 = g.relax(5)
+    d2 = g.relax(50)
+    assert d2 < d1
+
+
+def test_local_relax_keeps_dirichlet_and_converges(small_mesh):
+    from tapsim_modified_b200.tapsim import Grid
+    a = small_mesh.arrays()
+    g = Grid(small_mesh)
+    g.solve(rel_tol=1e-8)
+    g.surface_init(0)
+    s = g.select()
+    g.take_away(s.candidate)
+    before = g.potentials()
+    rc, it, dev = g.local_relax(s.candidate, 3, 1e-6, 5, 5)
+    after = g.potentials()
+    assert rc in (0, 6) and it >= 5
+    free = free_mask(a)
+    free[s.candidate] = True
+    changed = np.nonzero(after != before)[0]
+    assert len(changed) > 0
+    assert free[changed].all()
+    # only cells within three hops of the removed atom move
+    rp, col = a["row_ptr"], a["col"]
+    ring = {s.candidate}
+    frontier = {s.candidate}
+    for _ in range(3):
+        nxt = set()
+        for u in frontier:
+            nxt.update(col[rp[u]:rp[u + 1]].tolist())
+        frontier = nxt - ring
+        ring |= nxt
+    assert set(changed.tolist()) <= ring

@@ -1,0 +1,138 @@
+"""Device field / ratio / argmax / removal vs the FP64 oracle."""
+import numpy as np
+import pytest
+
+from conftest import free_mask
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pair(small_mesh):
+    from oracle import Oracle
+    from tapsim_modified_b200.tapsim import Grid
+    a = small_mesh.arrays()
+    g = Grid(small_mesh)
+    g.solve(rel_tol=1e-10)
+    o = Oracle(a)
+    o.phi[:] = g.potentials()   # identical potentials: isolates the field/select kernels
+    return a, g, o
+
+
+def test_surface_set_matches(pair):
+    a, g, o = pair
+    n_dev = g.surface_init(0)
+    n_orc = o.surface_init(0)
+    nodes, _ = g.surface()
+    assert n_dev == n_orc == len(nodes)
+    assert np.array_equal(nodes, np.nonzero(o.surface)[0])
+
+
+def test_field_o1_matches(pair):
+    a, g, o = pair
+    g.surface_init(0)
+    nodes, _ = g.surface()
+    extra = np.arange(0, a["type"].size, 97, dtype=np.int32)
+    allnodes = np.concatenate([nodes, extra])
+    E = g.field_o1(allnodes)
+    ref = np.array([o.field_o1(i) for i in allnodes])
+    scale = np.linalg.norm(ref, axis=1).max()
+    assert np.abs(E - ref).max() <= 1e-9 * scale
+    # hull nodes carry no field (field_o1 returns zero on the boundary)
+    hull = np.nonzero(a["hull"])[0][:50]
+    assert np.all(g.field_o1(hull) == 0.0)
+
+
+def test_select_matches(pair):
+    a, g, o = pair
+    g.surface_init(0)
+    o.surface_init(0)
+    s = g.select()
+    info, ratio = o.select()
+    assert s.candidate == info.candidate
+    assert s.apex == info.apex
+    assert abs(s.best_ratio - info.best) <= 1e-6 * info.best
+    assert abs(s.second_ratio - info.second) <= 1e-6 * info.best
+    assert abs(s.ratio_sum - info.sum) <= 1e-9 * info.sum
+    nodes, r = g.surface()
+    assert np.allclose(r, ratio[nodes], rtol=1e-6, atol=0)
+
+
+def test_take_away_sequence_matches(small_mesh):
+    from oracle import Oracle
+    from tapsim_modified_b200.tapsim import Grid
+    a = small_mesh.arrays()
+    g = Grid(small_mesh)
+    g.solve(rel_tol=1e-10)
+    o = Oracle(a)
+    o.phi[:] = g.potentials()
+    g.surface_init(0)
+    o.surface_init(0)
+    removed = 0
+    for k in range(12):
+        s = g.select()
+        info, _ = o.select()
+        assert s.candidate == info.candidate, f"event {k}"
+        det_g = g.take_away(s.candidate)
+        det_o = o.take_away(info.candidate, 0)
+        assert det_g == det_o
+        removed += 1 + len(det_g)
+        assert np.array_equal(g.types(), o.type)
+        assert np.allclose(g.couplings(), o.c, rtol=1e-14, atol=0)
+        nodes, _ = g.surface()
+        assert np.array_equal(nodes, np.nonzero(o.surface)[0])
+        g.solve(rel_tol=1e-10)
+        o.phi[:] = g.potentials()
+    # the removed cells are vacuum and free now
+    assert (g.types() == 0).sum() == (a["type"] == 0).sum() + removed
+
+
+def test_take_away_rejects_non_surface(small_mesh):
+    from tapsim_modified_b200 import _native as N
+    from tapsim_modified_b200.tapsim import Grid
+    g = Grid(small_mesh)
+    g.surface_init(0)
+    with pytest.raises(N.TapsimError) as e:
+        g.take_away(0)   # node 0 is a boundary cell, never on the surface
+    assert e.value.code == 5
+
+
+def test_update_coordination_is_inert_below_10(small_mesh):
+    from tapsim_modified_b200.tapsim import Grid
+    g = Grid(small_mesh)
+    before = g.types()
+    g.update_coordination()
+    assert np.array_equal(before, g.types())
+
+
+def _normal_reference(a, surface, node, vacuum_id=0):
+    rp, col, xyz = a["row_ptr"], a["col"], a["xyz"].astype(np.float64)
+    seen, frontier = set(), [node]
+    for _ in range(3):
+        nxt = []
+        for u in frontier:
+            for v in col[rp[u]:rp[u + 1]]:
+                if v not in seen:
+                    seen.add(int(v))
+                    nxt.append(int(v))
+        frontier = nxt
+    seen.discard(node)
+    vac = [v for v in seen if a["type"][v] == vacuum_id]
+    loc = [v for v in seen if surface[v]]
+    d = xyz[node] - xyz[loc]
+    w, V = np.linalg.eigh(d.T @ d)
+    nrm = V[:, 0]
+    tmp = (xyz[vac] - xyz[node]).sum(0)
+    return nrm if nrm @ tmp >= 0 else -nrm
+
+
+def test_surface_normal(pair):
+    a, g, o = pair
+    g.surface_init(0)
+    o.surface_init(0)
+    nodes, _ = g.surface()
+    for node in nodes[:: max(1, len(nodes) // 15)]:
+        n_dev = g.normal(int(node))
+        n_ref = _normal_reference(a, o.surface, int(node))
+        assert abs(np.linalg.norm(n_dev) - 1.0) < 1e-5
+        assert np.dot(n_dev, n_ref) > 1 - 1e-5
