@@ -226,6 +226,20 @@ typedef struct {
 } tg_event_record;
 int tg_run_event(tg_handle* h, const tg_event_opts* opts, int32_t event_index, tg_event_record* rec);
 
+/* ---- measurement (no counterpart in the reference) ---------------------- */
+/* CUDA events on the handle's stream around a region of calls. */
+int tg_timer_start(tg_handle* h);
+int tg_timer_stop(tg_handle* h, float* elapsed_ms);
+/* Kernels this handle has launched since creation. */
+int64_t tg_launch_count(const tg_handle* h);
+/* Times `iters` back-to-back launches of one hot kernel on the handle's
+ * stream with CUDA events: 0 = FP32 CG SpMV over the non-Neumann free rows,
+ * 1 = FP64 residual over all free rows.  Reports the mean duration of one
+ * launch and the algorithmic bytes one launch moves (CSR rows, coupling and
+ * neighbour-index streams, one compulsory read of every gathered vector
+ * entry, the row outputs). */
+int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, double* algorithmic_bytes);
+
 /* ---- host-side mesh building (setup, not device work) ------------------ */
 typedef struct tg_mesh tg_mesh;
 typedef struct {

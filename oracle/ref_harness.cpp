@@ -25,6 +25,7 @@
 //       --phi <file>         write float32 potential() of all nodes after the
 //                            initial relaxation
 //       --phi-events <file>  append float32 potentials after every event
+//       --no-sync            with --dump: keep the dump's couplings (resumption)
 
 #include <cstdio>
 #include <cstdlib>
@@ -98,6 +99,7 @@ static int cmd_evap(int argc, char** argv)
 	int threads = 1;
 	int initRelax = 1;
 	bool initGiven = false;
+	bool noSync = false;
 	float initThr = 0.0f;
 	unsigned initCycle = 0, initQueue = 0;
 
@@ -116,6 +118,7 @@ static int cmd_evap(int argc, char** argv)
 		else if (!strcmp(argv[a], "--force")) forceName = argv[++a];
 		else if (!strcmp(argv[a], "--phi")) phiName = argv[++a];
 		else if (!strcmp(argv[a], "--phi-events")) phiEventsName = argv[++a];
+		else if (!strcmp(argv[a], "--no-sync")) noSync = true;
 		else { fprintf(stderr, "unknown option %s\n", argv[a]); return 2; }
 	}
 
@@ -132,7 +135,9 @@ static int cmd_evap(int argc, char** argv)
 	{
 		File_Io::readSystem(dumpIn, &system, 0);
 		File_Io::readConfig(cfg, &system.configTable);
-		system.gridTable.fastSync(system.geomTable, system.configTable);
+		// --no-sync keeps the dump's couplings, as `tapsim resumption` does
+		// (tapsim.cpp:195-231); otherwise recompute them (doEvaporation)
+		if (!noSync) system.gridTable.fastSync(system.geomTable, system.configTable);
 	}
 	else
 		Process::initialization(cfg, nodes, &system);

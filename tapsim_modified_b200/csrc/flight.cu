@@ -319,11 +319,11 @@ __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t
 
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s) {
-    if (nIons > 0) k_trace<<<(nIons + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out);
+    if (nIons > 0) { count_launch(); k_trace<<<(nIons + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); }
 }
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit, float* out,
                          cudaStream_t s) {
-    if (n > 0) k_potential_at<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, n, xyz, guess, walkLimit, out);
+    if (n > 0) { count_launch(); k_potential_at<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, n, xyz, guess, walkLimit, out); }
 }
 
 }  // namespace tgd

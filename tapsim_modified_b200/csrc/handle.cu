@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -45,6 +46,12 @@ namespace tgapi {
 void set_process_error(const std::string& msg) { g_error = msg; }
 }  // namespace tgapi
 
+namespace tgd {
+static std::atomic<long long> g_launches(0);
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace tgd
+
 struct tg_handle {
     int n = 0, nnz = 0, ntets = 0, ncol = 0;
     cudaStream_t stream = nullptr;
@@ -84,6 +91,9 @@ struct tg_handle {
     DBuf<double> stageD;
     DBuf<float> stageF;
     DBuf<ImpactOut> stageImpact;
+
+    cudaEvent_t evStart = nullptr, evStop = nullptr;
+    std::vector<int32_t> h_row_ptr;
 
     bool bnormValid = false;
     double bnorm2 = 0.0;
@@ -393,6 +403,7 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     // the integer grid of the host Delaunay builder (delaunay.cpp): |x| <= 2^40
     h->snap = amax > 0.0 ? std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 40) / amax))) : 1.0;
     h->h_xyz.assign(d->xyz, d->xyz + 3 * (size_t)n);
+    h->h_row_ptr.assign(d->row_ptr, d->row_ptr + n + 1);
     if (d->node_tet) h->h_node_tet.assign(d->node_tet, d->node_tet + n);
 
     auto up = [&](auto& buf, const auto* src, size_t count) -> cudaError_t {
@@ -404,6 +415,8 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     cudaError_t e = cudaSuccess;
     auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
     chk(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    chk(cudaEventCreate(&h->evStart));
+    chk(cudaEventCreate(&h->evStop));
     chk(up(h->xyz, d->xyz, 3 * (size_t)n));
     chk(up(h->type, d->type_id, n));
     chk(h->typeScratch.alloc(n));
@@ -481,8 +494,74 @@ void tg_destroy(tg_handle* h) {
     h->keys.release(); h->result.release(); h->local.release(); h->localCount.release();
     h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
     h->stageImpact.release();
+    if (h->evStart) cudaEventDestroy(h->evStart);
+    if (h->evStop) cudaEventDestroy(h->evStop);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
+}
+
+int tg_timer_start(tg_handle* h) {
+    if (!h) return fail(h, TG_ERR_ARGUMENT, "tg_timer_start: null handle");
+    CK(cudaEventRecord(h->evStart, h->stream));
+    return TG_OK;
+}
+
+int tg_timer_stop(tg_handle* h, float* ms) {
+    if (!h || !ms) return fail(h, TG_ERR_ARGUMENT, "tg_timer_stop: null argument");
+    CK(cudaEventRecord(h->evStop, h->stream));
+    CK(cudaEventSynchronize(h->evStop));
+    CK(cudaEventElapsedTime(ms, h->evStart, h->evStop));
+    return TG_OK;
+}
+
+int64_t tg_launch_count(const tg_handle*) { return (int64_t)launches_so_far(); }
+
+int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, double* bytes) {
+    if (!h || iters < 1 || !avg_ms || !bytes) return fail(h, TG_ERR_ARGUMENT, "tg_bench_kernel: bad argument");
+    DevMesh m = h->dm();
+    // rows of the timed kernel and their neighbour entries
+    std::vector<int32_t> rowsV(h->countAllV), rowsN(h->countAllN);
+    if (h->countAllV) CK(cudaMemcpy(rowsV.data(), h->allV.p, sizeof(int32_t) * rowsV.size(), cudaMemcpyDeviceToHost));
+    if (h->countAllN) CK(cudaMemcpy(rowsN.data(), h->allN.p, sizeof(int32_t) * rowsN.size(), cudaMemcpyDeviceToHost));
+    auto entries = [&](const std::vector<int32_t>& rows) {
+        double e = 0.0;
+        for (int32_t i : rows) e += h->h_row_ptr[i + 1] - h->h_row_ptr[i];
+        return e;
+    };
+    if (which == 0) {
+        // k_cg_spmv over the non-Neumann free rows: row index, two row
+        // pointers, col + ceff32 per entry, p (once per row), diag32, ap
+        const double rows = (double)rowsV.size(), nnz = entries(rowsV);
+        *bytes = rows * (4 + 8 + 4 + 4 + 4) + nnz * (4 + 4);
+        CGVectors v = h->cg(0);
+        if (h->scalV.n < 8) CK(h->scalV.alloc(8));
+        v = h->cg(0);
+        const double one = 1.0;
+        CK(cudaMemcpyAsync(h->scalV.p, &one, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        launch_cg_spmv_only(m, h->allV.p, h->countAllV, v, h->stream);  // warm
+        CK(cudaEventRecord(h->evStart, h->stream));
+        for (int k = 0; k < iters; k++) launch_cg_spmv_only(m, h->allV.p, h->countAllV, v, h->stream);
+        CK(cudaEventRecord(h->evStop, h->stream));
+    } else if (which == 1) {
+        // k_residual over all free rows: row index, two row pointers, col +
+        // ceff64 per entry, phi64 (once per row), diag64, q64
+        const double rows = (double)(rowsV.size() + rowsN.size()), nnz = entries(rowsV) + entries(rowsN);
+        *bytes = rows * (4 + 8 + 8 + 8 + 8) + nnz * (4 + 8);
+        launch_residual(m, h->allV.p, h->countAllV, nullptr, h->acc.p, h->stream);
+        CK(cudaEventRecord(h->evStart, h->stream));
+        for (int k = 0; k < iters; k++) {
+            launch_residual(m, h->allV.p, h->countAllV, nullptr, h->acc.p, h->stream);
+            launch_residual(m, h->allN.p, h->countAllN, nullptr, h->acc.p, h->stream);
+        }
+        CK(cudaEventRecord(h->evStop, h->stream));
+    } else {
+        return fail(h, TG_ERR_ARGUMENT, "tg_bench_kernel: unknown kernel");
+    }
+    CK(cudaEventSynchronize(h->evStop));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, h->evStart, h->evStop));
+    *avg_ms = ms / iters;
+    return sync_status(h, "tg_bench_kernel");
 }
 
 int tg_get_phi(tg_handle* h, double* phi) {

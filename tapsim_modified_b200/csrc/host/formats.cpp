@@ -411,8 +411,17 @@ std::string write_dump(const std::string& path, const Dump& d) {
         wr(f, (bool)t.dirichlet);
         wr(f, t.phi);
         wr(f, t.mass);
-        char cs[4] = {0, 0, 0, 0};
+        // The reference writes the 16-bit charge state with sizeof(float)
+        // bytes (configuration.cpp:204) and reads it back the same way
+        // (configuration.cpp:145), so two bytes beyond the short travel with
+        // it.  In the reference as built from its sources, those bytes are
+        // the low half of the type count on the writer's stack, and its
+        // reader stores them back into that count: they must hold the count
+        // for the reference to read the rest of the dump.
+        char cs[4];
+        const uint16_t ntypes = (uint16_t)d.config.types.size();
         std::memcpy(cs, &t.evap_charge, 2);
+        std::memcpy(cs + 2, &ntypes, 2);
         f.write(cs, 4);
         wr(f, t.evap_field);
         wr(f, t.evap_energy);

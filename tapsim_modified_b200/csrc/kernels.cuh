@@ -17,6 +17,10 @@
 
 namespace tgd {
 
+// process-wide count of kernels launched by this library (handle.cu)
+void count_launch();
+long long launches_so_far();
+
 struct DevMesh {
     int n, nnz, ntets;
     const float* xyz;
@@ -83,6 +87,8 @@ void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors 
 // one CG iteration; all of it is skipped once scal[3it] (r.z) <= target
 void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double target,
                     cudaStream_t s);
+// the SpMV kernel of one CG iteration on its own (timing hook)
+void launch_cg_spmv_only(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s);
 // rhs_N += sum over non-Neumann free neighbours c_ij x_j (coupling of the
 // Neumann rows to the correction found for the non-Neumann rows)
 void launch_add_coupled(const DevMesh& m, const int32_t* rows, int count, const float* xV, float* r, cudaStream_t s);

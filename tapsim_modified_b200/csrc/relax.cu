@@ -264,36 +264,39 @@ inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 }  // namespace
 
 void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* maxdev, cudaStream_t s) {
-    if (count > 0) k_sweep64<<<blocks(count), kBlock, 0, s>>>(m, rows, count, maxdev);
+    if (count > 0) { count_launch(); k_sweep64<<<blocks(count), kBlock, 0, s>>>(m, rows, count, maxdev); }
 }
 void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s) {
-    if (count > 0) k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, acc);
+    if (count > 0) { count_launch(); k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, acc); }
 }
 void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s) {
-    if (count > 0) k_bnorm<<<blocks(count), kBlock, 0, s>>>(m, rows, count, acc);
+    if (count > 0) { count_launch(); k_bnorm<<<blocks(count), kBlock, 0, s>>>(m, rows, count, acc); }
 }
 void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
-    if (count > 0) k_cg_init<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v);
+    if (count > 0) { count_launch(); k_cg_init<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v); }
 }
 void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double target,
                     cudaStream_t s) {
     if (count <= 0) return;
-    k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target);
-    k_cg_update<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target);
-    k_cg_pupdate<<<blocks(count), kBlock, 0, s>>>(rows, count, v, it, target);
+    { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target); }
+    { count_launch(); k_cg_update<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target); }
+    { count_launch(); k_cg_pupdate<<<blocks(count), kBlock, 0, s>>>(rows, count, v, it, target); }
+}
+void launch_cg_spmv_only(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
+    if (count > 0) { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, 0, -1.0); }
 }
 void launch_add_coupled(const DevMesh& m, const int32_t* rows, int count, const float* xV, float* r, cudaStream_t s) {
-    if (count > 0) k_add_coupled<<<blocks(count), kBlock, 0, s>>>(m, rows, count, xV, r);
+    if (count > 0) { count_launch(); k_add_coupled<<<blocks(count), kBlock, 0, s>>>(m, rows, count, xV, r); }
 }
 void launch_apply_correction(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
-    if (count > 0) k_apply_correction<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v);
+    if (count > 0) { count_launch(); k_apply_correction<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v); }
 }
 void launch_rebuild_rows(const DevMesh& m, cudaStream_t s) {
-    if (m.n > 0) k_rebuild_rows<<<blocks(m.n), kBlock, 0, s>>>(m);
+    if (m.n > 0) { count_launch(); k_rebuild_rows<<<blocks(m.n), kBlock, 0, s>>>(m); }
 }
 void launch_local_set(const DevMesh& m, int node, int hops, int32_t* out, int32_t* outCount, int cap, int32_t* scratch,
                       int scratchCap, int ncolours, cudaStream_t s) {
-    k_local_set<<<1, 512, 0, s>>>(m, node, hops, out, outCount, cap, scratch, scratchCap, ncolours);
+    { count_launch(); k_local_set<<<1, 512, 0, s>>>(m, node, hops, out, outCount, cap, scratch, scratchCap, ncolours); }
 }
 
 }  // namespace tgd

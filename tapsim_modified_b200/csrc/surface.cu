@@ -401,28 +401,28 @@ inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 }  // namespace
 
 void launch_surface_init(const DevMesh& m, Surface sf, int vacuumId, cudaStream_t s) {
-    k_surface_init<<<blocks(m.n), kBlock, 0, s>>>(m, sf, vacuumId);
+    { count_launch(); k_surface_init<<<blocks(m.n), kBlock, 0, s>>>(m, sf, vacuumId); }
 }
 void launch_surface_select(const DevMesh& m, Surface sf, int slots, unsigned long long* keys, double* acc,
                            cudaStream_t s) {
-    if (slots > 0) k_surface_select<<<blocks(slots), kBlock, 0, s>>>(m, sf, slots, keys, acc);
+    if (slots > 0) { count_launch(); k_surface_select<<<blocks(slots), kBlock, 0, s>>>(m, sf, slots, keys, acc); }
 }
 void launch_surface_second(Surface sf, int slots, int best, unsigned long long* key, cudaStream_t s) {
-    if (slots > 0) k_surface_second<<<blocks(slots), kBlock, 0, s>>>(sf, slots, best, key);
+    if (slots > 0) { count_launch(); k_surface_second<<<blocks(slots), kBlock, 0, s>>>(sf, slots, best, key); }
 }
 void launch_field_o1(const DevMesh& m, const int32_t* nodes, int count, double* out, cudaStream_t s) {
-    if (count > 0) k_field_o1<<<blocks(count), kBlock, 0, s>>>(m, nodes, count, out);
+    if (count > 0) { count_launch(); k_field_o1<<<blocks(count), kBlock, 0, s>>>(m, nodes, count, out); }
 }
 void launch_take_away(const DevMesh& m, RowLists rl, Surface sf, int node, int vacuumId, int32_t* result, int resultCap,
                       cudaStream_t s) {
-    k_take_away<<<1, 32, 0, s>>>(m, rl, sf, node, vacuumId, result, resultCap);
+    { count_launch(); k_take_away<<<1, 32, 0, s>>>(m, rl, sf, node, vacuumId, result, resultCap); }
 }
 void launch_update_coordination(const DevMesh& m, int8_t* scratchType, cudaStream_t s) {
     cudaMemcpyAsync(scratchType, m.type, (size_t)m.n, cudaMemcpyDeviceToDevice, s);
-    k_coordination<<<blocks(m.n), kBlock, 0, s>>>(m, scratchType);
+    { count_launch(); k_coordination<<<blocks(m.n), kBlock, 0, s>>>(m, scratchType); }
 }
 void launch_surface_normal(const DevMesh& m, Surface sf, int node, int vacuumId, float* out, cudaStream_t s) {
-    k_surface_normal<<<1, 256, 0, s>>>(m, sf, node, vacuumId, out);
+    { count_launch(); k_surface_normal<<<1, 256, 0, s>>>(m, sf, node, vacuumId, out); }
 }
 
 }  // namespace tgd
