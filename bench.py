@@ -220,7 +220,7 @@ def run_ours(args, rank: int, world: int, dist):
 
     peak, peak_kind = measured_peak_hbm()
     spmv_rows = int((arrays["type"] == 0).sum())
-    traffic_per_row = ncu_traffic_per_row("cg_spmv")
+    traffic_per_row = ncu_traffic_per_row("vcg_spmv")
     out = {
         "metric": METRIC,
         "value": ev_total / dev_max,
@@ -254,7 +254,7 @@ def run_ours(args, rank: int, world: int, dist):
                         "final potentials download"},
         "gpu_launches": int(launches),
         "roofline": {
-            "kernel": "k_cg_spmv (FP32 CG SpMV over the non-Neumann free rows)",
+            "kernel": "k_vcg_spmv (FP32 SELL-32 SpMV of the single-reduction CG, non-Neumann free rows)",
             "bound": "hbm",
             "achieved": spmv_gbs,
             "peak": peak,

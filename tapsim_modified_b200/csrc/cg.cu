@@ -1,0 +1,237 @@
+// FP32 conjugate gradients on the non-Neumann free rows ("V system"), the
+// inner solver of the FP64 defect-correction solve.
+//
+// Layout.  The V rows get their own dense slot numbering.  Couplings are
+// stored SELL-32: slices of 32 consecutive slots, column-major inside a
+// slice, each slice as wide as its longest row, rows sorted by length
+// within windows of 1024 slots so that slices are nearly full.  One warp
+// handles one slice and every coupling load is a coalesced 128-byte line.
+// A row keeps an entry for every neighbour that is free or may become free
+// (removable Dirichlet atoms); entries of non-free neighbours point at the
+// zero slot, whose vector entries stay 0.  A removal therefore never changes
+// the structure: it appends the new row in a reserve of fixed-width slices
+// and repoints the neighbours' entries (vpos maps a global CSR entry to its
+// SELL position).
+//
+// Iteration.  Chronopoulos-Gear single-reduction PCG with the Jacobi
+// preconditioner: one pointwise kernel (p, s, x, r, u updates and r.u) and
+// one SpMV kernel (w = A u and w.u) per iteration; alpha and beta are
+// computed by every thread from the per-iteration scalars.
+#include "kernels.cuh"
+
+namespace tgd {
+namespace {
+
+constexpr int kBlock = 256;
+
+// s_i = gamma_i, delta_i, alpha_i at scal[3i], scal[3i+1], scal[3i+2]
+__device__ __forceinline__ void cg_coeffs(const double* scal, int it, double* alpha, double* beta) {
+    const double g = scal[3 * it], d = scal[3 * it + 1];
+    if (it == 0) {
+        *beta = 0.0;
+        *alpha = d > 0.0 ? g / d : 0.0;
+    } else {
+        const double gp = scal[3 * (it - 1)], ap = scal[3 * (it - 1) + 2];
+        *beta = gp > 0.0 ? g / gp : 0.0;
+        const double den = d - *beta * g / ap;
+        *alpha = den > 0.0 ? g / den : 0.0;
+    }
+}
+
+// u = r / d, x = 0, gamma_0 = r.u
+__global__ void k_vcg_init(VSys v, int slots) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double g = 0.0;
+    if (s < slots) {
+        const float r = v.r[s];
+        const float u = r / v.d[s];
+        v.u[s] = u;
+        v.x[s] = 0.0f;
+        v.p[s] = 0.0f;
+        v.sv[s] = 0.0f;
+        g = (double)r * (double)u;
+    }
+    block_sum_atomic<kBlock>(g, &v.scal[0]);
+}
+
+// w = A u over SELL-32 slices; delta -> scal[3*it+1] (it = iteration whose
+// u this is); skipped once gamma_it <= target
+__global__ void k_vcg_spmv(VSys v, int slices, int it, double target) {
+    if (it >= 0 && v.scal[3 * it] <= target) return;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    double dl = 0.0;
+    if (warp < slices) {
+        const int base = v.slice_start[warp];
+        const int width = v.slice_width[warp];
+        const int s = warp * 32 + lane;
+        const int* __restrict__ col = v.col + base + lane;
+        const float* __restrict__ val = v.val + base + lane;
+        float acc = 0.0f;
+#pragma unroll 4
+        for (int k = 0; k < width; k++) acc += val[32 * k] * v.u[col[32 * k]];
+        const float u = v.u[s];
+        const float w = v.d[s] * u - acc;
+        v.w[s] = w;
+        dl = (double)w * (double)u;
+    }
+    block_sum_atomic<kBlock>(dl, &v.scal[3 * (it < 0 ? 0 : it) + 1]);
+}
+
+// p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s, u = r / d,
+// gamma_{it+1} = r.u
+__global__ void k_vcg_update(VSys v, int slots, int it, double target) {
+    if (v.scal[3 * it] <= target) return;
+    double alpha, beta;
+    cg_coeffs(v.scal, it, &alpha, &beta);
+    if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[3 * it + 2] = alpha;
+    const float a = (float)alpha, b = (float)beta;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double g = 0.0;
+    if (s < slots) {
+        const float p = v.u[s] + b * v.p[s];
+        const float sv = v.w[s] + b * v.sv[s];
+        v.p[s] = p;
+        v.sv[s] = sv;
+        v.x[s] += a * p;
+        const float r = v.r[s] - a * sv;
+        v.r[s] = r;
+        const float u = r / v.d[s];
+        v.u[s] = u;
+        g = (double)r * (double)u;
+    }
+    block_sum_atomic<kBlock>(g, &v.scal[3 * (it + 1)]);
+}
+
+// phi64[node] += x[slot]; clears the slot's vectors
+__global__ void k_vcg_apply(DevMesh m, VSys v, int slots) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots) return;
+    const int i = v.node_of[s];
+    if (i >= 0) m.phi64[i] += (double)v.x[s];
+    v.x[s] = v.r[s] = v.u[s] = v.w[s] = v.p[s] = v.sv[s] = 0.0f;
+}
+
+// r of the Neumann rows += sum over V neighbours ceff_ij x_j
+__global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int count, float* rN) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int i = rows[t];
+    float s = 0.0f;
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+        const int sl = v.slot_of[m.col[q]];
+        if (sl >= 0) s += m.ceff32[q] * v.x[sl];
+    }
+    rN[i] += s;
+}
+
+// FP64 residual of the V rows written straight into slot order
+__global__ void k_vcg_residual(DevMesh m, VSys v, int slots, double* acc) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double r = 0.0;
+    if (s < slots) {
+        const int i = v.node_of[s];
+        if (i >= 0) {
+            double sum = 0.0;
+            for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) sum += m.ceff64[q] * m.phi64[m.col[q]];
+            r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
+        }
+        v.r[s] = (float)r;
+    }
+    block_sum_atomic<kBlock>(r * r, acc);
+}
+
+// Appends the row of a node that has just become a non-Neumann free cell
+// and repoints its free neighbours' entries at it.  One warp.
+__device__ void vsys_add_row(const DevMesh& m, VSys v, int i) {
+    const int lane = threadIdx.x & 31;
+    int s = -1;
+    if (lane == 0) {
+        s = atomicAdd(v.count, 1);
+        if (s >= v.capacity) {
+            atomicOr(m.status, S_CAPACITY);
+            s = -1;
+        } else {
+            v.slot_of[i] = s;
+            v.node_of[s] = i;
+            v.d[s] = m.diag32[i];
+        }
+    }
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s < 0) return;
+    __syncwarp();
+    const int slice = s >> 5, r = s & 31;
+    const int base = v.slice_start[slice] + r;
+    const int width = v.slice_width[slice];
+    const int q0 = m.row_ptr[i], q1 = m.row_ptr[i + 1];
+    // entries of the new row (sequential positions among kept neighbours)
+    if (lane == 0) {
+        int k = 0;
+        for (int q = q0; q < q1; q++) {
+            const int j = m.col[q];
+            const uint8_t fj = m.flags[j];
+            const bool keep = !(fj & F_NEUMANN) && (!(fj & F_DIRICHLET) || m.types[m.type[j]].removable);
+            if (!keep || k >= width) {
+                v.vpos[q] = -1;
+                continue;
+            }
+            const int sj = v.slot_of[j];
+            v.col[base + 32 * k] = sj >= 0 ? sj : v.capacity;
+            v.val[base + 32 * k] = m.ceff32[q];
+            v.vpos[q] = base + 32 * k;
+            k++;
+        }
+        for (; k < width; k++) {
+            v.col[base + 32 * k] = v.capacity;
+            v.val[base + 32 * k] = 0.0f;
+        }
+    }
+    __syncwarp();
+    // neighbours that are V rows: their entry for i now points at slot s
+    for (int q = q0 + lane; q < q1; q += 32) {
+        const int j = m.col[q];
+        const int sj = v.slot_of[j];
+        if (sj < 0) continue;
+        const int p = v.vpos[m.rev[q]];
+        if (p >= 0) {
+            v.col[p] = s;
+            v.val[p] = m.ceff32[m.rev[q]];
+        }
+        v.d[sj] = m.diag32[j];
+    }
+    __syncwarp();
+}
+
+__global__ void k_vsys_add_rows(DevMesh m, VSys v, const int32_t* nodes, int count) {
+    for (int k = 0; k < count; k++) vsys_add_row(m, v, nodes[k]);
+}
+
+inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+void launch_vcg_init(const VSys& v, int slots, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_init<<<blocks(slots), kBlock, 0, s>>>(v, slots); }
+}
+void launch_vcg_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s) {
+    const int slices = (slots + 31) / 32;
+    if (slices > 0) { count_launch(); k_vcg_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, it, target); }
+}
+void launch_vcg_update(const VSys& v, int slots, int it, double target, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_update<<<blocks(slots), kBlock, 0, s>>>(v, slots, it, target); }
+}
+void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_apply<<<blocks(slots), kBlock, 0, s>>>(m, v, slots); }
+}
+void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
+                               cudaStream_t s) {
+    if (count > 0) { count_launch(); k_vcg_couple_neumann<<<blocks(count), kBlock, 0, s>>>(m, v, rows, count, rN); }
+}
+void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_residual<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, acc); }
+}
+void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
+    if (count > 0) { count_launch(); k_vsys_add_rows<<<1, 32, 0, s>>>(m, v, nodes, count); }
+}
+
+}  // namespace tgd

@@ -22,7 +22,8 @@ enum : int {
     S_NOT_SURFACE = 4,
     S_WALK_LIMIT = 8,
     S_UNKNOWN_TYPE = 16,
-    S_ZERO_WEIGHT = 32
+    S_ZERO_WEIGHT = 32,
+    S_CAPACITY = 64
 };
 
 struct DType {

@@ -105,14 +105,25 @@ __device__ void weights(const DevMesh& m, int t, V3 p, double w[4]) {
     w[3] = fabs(orient(P[0], P[1], P[2], p)) / vol;
 }
 
-// field_o1 of one node (same restatement as in surface.cu)
-__device__ V3 node_field(const DevMesh& m, int i) {
-    V3 E{0, 0, 0};
-    if (m.flags[i] & F_HULL) return E;
-    const double xi = m.xyz[3 * i], yi = m.xyz[3 * i + 1], zi = m.xyz[3 * i + 2];
-    const double pi = m.phi64[i];
+// Vertex fields of one flight call: every node's field_o1 is computed once,
+// in bulk, from the current potentials before the flights start (the
+// FastField buffer of the reference, grid_3d.cpp:1672-1702, filled for all
+// vertices at once instead of on first use).  Four lanes share a row; a
+// singular node stores NaN in x, which the flight reports as S_SINGULAR when
+// it interpolates from that vertex, as the on-demand computation would.
+constexpr int kLanesPerRow = 4;
+__global__ void k_vertex_fields(DevMesh m) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gid / kLanesPerRow;
+    const int lane = gid % kLanesPerRow;
+    const bool live = i < m.n;
+    const int ii = live ? i : m.n - 1;
+    const bool hull = (m.flags[ii] & F_HULL) != 0;
+    const double xi = m.xyz[3 * ii], yi = m.xyz[3 * ii + 1], zi = m.xyz[3 * ii + 2];
+    const double pi = m.phi64[ii];
     double a00 = 0, a01 = 0, a02 = 0, a11 = 0, a12 = 0, a22 = 0, b0 = 0, b1 = 0, b2 = 0;
-    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+    const int q1 = hull ? 0 : m.row_ptr[ii + 1];
+    for (int q = (hull ? 0 : m.row_ptr[ii]) + lane; q < q1; q += kLanesPerRow) {
         if (m.c64[q] == 0.0) continue;
         const int j = m.col[q];
         const double dx = (double)m.xyz[3 * j] - xi, dy = (double)m.xyz[3 * j + 1] - yi, dz = (double)m.xyz[3 * j + 2] - zi;
@@ -121,47 +132,120 @@ __device__ V3 node_field(const DevMesh& m, int i) {
         a11 += dy * dy; a12 += dy * dz; a22 += dz * dz;
         b0 += dp * dx; b1 += dp * dy; b2 += dp * dz;
     }
+    for (int o = kLanesPerRow / 2; o > 0; o >>= 1) {
+        a00 += __shfl_xor_sync(0xffffffffu, a00, o); a01 += __shfl_xor_sync(0xffffffffu, a01, o);
+        a02 += __shfl_xor_sync(0xffffffffu, a02, o); a11 += __shfl_xor_sync(0xffffffffu, a11, o);
+        a12 += __shfl_xor_sync(0xffffffffu, a12, o); a22 += __shfl_xor_sync(0xffffffffu, a22, o);
+        b0 += __shfl_xor_sync(0xffffffffu, b0, o); b1 += __shfl_xor_sync(0xffffffffu, b1, o);
+        b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+    }
+    if (!live || lane != 0) return;
+    double* out = m.vfield + 3 * (size_t)i;
+    if (hull) {
+        out[0] = out[1] = out[2] = 0.0;
+        return;
+    }
     const double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22, c02 = a01 * a12 - a02 * a11;
     const double det = a00 * c00 + a01 * c01 + a02 * c02;
     if (det == 0.0 || !(det == det)) {
-        atomicOr(m.status, S_SINGULAR);
-        return E;
+        out[0] = __longlong_as_double(0x7ff8000000000000ll);
+        out[1] = out[2] = 0.0;
+        return;
     }
     const double c11 = a00 * a22 - a02 * a02, c12 = a01 * a02 - a00 * a12, c22 = a00 * a11 - a01 * a01;
     const double inv = 1.0 / det;
-    E.x = -(c00 * b0 + c01 * b1 + c02 * b2) * inv;
-    E.y = -(c01 * b0 + c11 * b1 + c12 * b2) * inv;
-    E.z = -(c02 * b0 + c12 * b1 + c22 * b2) * inv;
+    out[0] = -(c00 * b0 + c01 * b1 + c02 * b2) * inv;
+    out[1] = -(c01 * b0 + c11 * b1 + c12 * b2) * inv;
+    out[2] = -(c02 * b0 + c12 * b1 + c22 * b2) * inv;
+}
+
+__device__ V3 vertex_field(const DevMesh& m, int i) {
+    const V3 E{m.vfield[3 * i], m.vfield[3 * i + 1], m.vfield[3 * i + 2]};
+    if (E.x != E.x) {
+        atomicOr(m.status, S_SINGULAR);
+        return V3{0, 0, 0};
+    }
     return E;
 }
 
-// Per-thread cache of the vertex fields of the last two tetrahedra.
-struct FieldCache {
-    int tet[2];
-    V3 f[2][4];
-    int next;
+// The last two tetrahedra an ion touched, with vertex coordinates,
+// neighbours and vertex fields in registers: RK stages that stay inside
+// them need no memory traffic.
+struct TetSlot {
+    int t;
+    int nb[4];
+    V3 P[4];
+    V3 F[4];
+};
+struct TetCache {
+    TetSlot s[2];
+    int last;
 };
 
-__device__ bool fast_field(const DevMesh& m, FieldCache& fc, V3 p, int guess, int limit, unsigned& rot, V3* E) {
-    const int t = locate(m, p, guess, limit, rot);
-    *E = V3{0, 0, 0};
-    if (t == -2) return false;
-    if (t < 0) return true;
-    int s = -1;
-    if (fc.tet[0] == t) s = 0;
-    else if (fc.tet[1] == t) s = 1;
-    if (s < 0) {
-        s = fc.next;
-        fc.next ^= 1;
-        fc.tet[s] = t;
-        for (int k = 0; k < 4; k++) fc.f[s][k] = node_field(m, m.tet_v[4 * t + k]);
-    }
-    double w[4];
-    weights(m, t, p, w);
+__device__ void load_slot(const DevMesh& m, TetSlot& s, int t) {
+    s.t = t;
+    int v[4];
     for (int k = 0; k < 4; k++) {
-        E->x += w[k] * fc.f[s][k].x;
-        E->y += w[k] * fc.f[s][k].y;
-        E->z += w[k] * fc.f[s][k].z;
+        v[k] = m.tet_v[4 * t + k];
+        s.nb[k] = m.tet_n[4 * t + k];
+    }
+    for (int k = 0; k < 4; k++) s.P[k] = ld3(m.xyz, v[k]);
+    for (int k = 0; k < 4; k++) s.F[k] = vertex_field(m, v[k]);
+}
+
+__device__ int cache_slot(const DevMesh& m, TetCache& c, int t) {
+    if (c.s[c.last].t == t) return c.last;
+    if (c.s[c.last ^ 1].t == t) return c.last ^= 1;
+    c.last ^= 1;
+    load_slot(m, c.s[c.last], t);
+    return c.last;
+}
+
+// findTetrahedron through the cache; returns the slot holding p, -1 when p
+// is outside the mesh, -2 when the walk exceeded its bound
+__device__ int locate_cached(const DevMesh& m, TetCache& c, V3 p, int t, int limit, unsigned& rot) {
+    if (t < 0) return -1;
+    for (int step = 0; step < limit; step++) {
+        const int sl = cache_slot(m, c, t);
+        const TetSlot& S = c.s[sl];
+        int next = -1;
+        bool moved = false;
+        const unsigned r = rot++;
+        for (int j = 0; j < 4; j++) {
+            const int k = (int)((r + j) & 3);
+            if (orient_sign(S.P[kFaceDev[k][0]], S.P[kFaceDev[k][1]], S.P[kFaceDev[k][2]], p, m.snap) < 0) {
+                next = S.nb[k];
+                moved = true;
+                break;
+            }
+        }
+        if (!moved) return sl;
+        if (next < 0) return -1;
+        t = next;
+    }
+    return -2;
+}
+
+__device__ bool fast_field(const DevMesh& m, TetCache& c, V3 p, int guess, int limit, unsigned& rot, V3* E) {
+    *E = V3{0, 0, 0};
+    const int sl = locate_cached(m, c, p, guess, limit, rot);
+    if (sl == -2) return false;
+    if (sl < 0) return true;
+    const TetSlot& S = c.s[sl];
+    const double vol = fabs(orient(S.P[0], S.P[1], S.P[2], S.P[3]));
+    double w[4];
+    if (vol == 0.0) {
+        w[0] = w[1] = w[2] = w[3] = 0.25;
+    } else {
+        w[0] = fabs(orient(p, S.P[1], S.P[2], S.P[3])) / vol;
+        w[1] = fabs(orient(S.P[0], p, S.P[2], S.P[3])) / vol;
+        w[2] = fabs(orient(S.P[0], S.P[1], p, S.P[3])) / vol;
+        w[3] = fabs(orient(S.P[0], S.P[1], S.P[2], p)) / vol;
+    }
+    for (int k = 0; k < 4; k++) {
+        E->x += w[k] * S.F[k].x;
+        E->y += w[k] * S.F[k].y;
+        E->z += w[k] * S.F[k].z;
     }
     return true;
 }
@@ -189,9 +273,9 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
 
     ImpactOut res;
     unsigned rot = (unsigned)ion * 7u;
-    FieldCache fc;
-    fc.tet[0] = fc.tet[1] = -1;
-    fc.next = 0;
+    TetCache fc;
+    fc.s[0].t = fc.s[1].t = -1;
+    fc.last = 0;
     V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
     V3 v{0, 0, 0};
     if (vel) v = V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]};
@@ -268,7 +352,8 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
                 status = 2;  // STEPPER_LIMIT_PASSED
                 break;
             }
-            const int nt = locate(m, nx, tet, tp.walk_limit, rot);
+            const int nsl = locate_cached(m, fc, nx, tet, tp.walk_limit, rot);
+            const int nt = nsl >= 0 ? fc.s[nsl].t : nsl;
             if (nt == -2) atomicOr(m.status, S_WALK_LIMIT);
             res.steps++;
             if (nt < 0) {
@@ -320,6 +405,13 @@ __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s) {
     if (nIons > 0) { count_launch(); k_trace<<<(nIons + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); }
+}
+void launch_vertex_fields(const DevMesh& m, cudaStream_t s) {
+    if (m.n > 0) {
+        count_launch();
+        const long long threads = (long long)m.n * kLanesPerRow;
+        k_vertex_fields<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m);
+    }
 }
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit, float* out,
                          cudaStream_t s) {

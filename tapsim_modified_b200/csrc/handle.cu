@@ -95,6 +95,38 @@ struct tg_handle {
     cudaEvent_t evStart = nullptr, evStop = nullptr;
     std::vector<int32_t> h_row_ptr;
 
+    // non-Neumann free rows in slot order, SELL-32 (cg.cu)
+    DBuf<int32_t> vSlotOf, vNodeOf, vSliceStart, vSliceWidth, vCol, vPos, vCount;
+    DBuf<float> vVal, vVec;  // vVec: d, x, r, u, w, p, sv, each capacity+1
+    DBuf<double> vScal;
+    DBuf<double> vfield;     // vertex fields of the current flight call
+    int vCapacity = 0;       // slots incl. the append reserve
+    int vActive = 0;         // slots in use (host mirror of vCount)
+    double vEntries = 0.0;   // stored (non-padding) couplings
+
+    VSys vs() {
+        VSys v;
+        v.slot_of = vSlotOf.p;
+        v.node_of = vNodeOf.p;
+        v.slice_start = vSliceStart.p;
+        v.slice_width = vSliceWidth.p;
+        v.col = vCol.p;
+        v.val = vVal.p;
+        v.vpos = vPos.p;
+        const size_t stride = (size_t)vCapacity + 1;
+        v.d = vVec.p;
+        v.x = vVec.p + stride;
+        v.r = vVec.p + 2 * stride;
+        v.u = vVec.p + 3 * stride;
+        v.w = vVec.p + 4 * stride;
+        v.p = vVec.p + 5 * stride;
+        v.sv = vVec.p + 6 * stride;
+        v.scal = vScal.p;
+        v.count = vCount.p;
+        v.capacity = vCapacity;
+        return v;
+    }
+
     bool bnormValid = false;
     double bnorm2 = 0.0;
     bool selValid = false;
@@ -129,6 +161,7 @@ struct tg_handle {
         m.types = dtypes.p;
         m.status = status.p;
         m.snap = snap;
+        m.vfield = vfield.p;
         return m;
     }
     RowLists rl() {
@@ -406,6 +439,74 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     h->h_row_ptr.assign(d->row_ptr, d->row_ptr + n + 1);
     if (d->node_tet) h->h_node_tet.assign(d->node_tet, d->node_tet + n);
 
+    // ---- V system: slots, SELL-32 couplings, append reserve ----
+    auto keepInV = [&](int j) {
+        return !(flags[j] & F_NEUMANN) && (!(flags[j] & F_DIRICHLET) || dt[d->type_id[j]].removable);
+    };
+    const int nV0 = h->countAllV;
+    std::vector<int32_t> vlen(nV0);
+    int maxRow = 1;
+    for (int i = 0; i < n; i++) maxRow = std::max(maxRow, d->row_ptr[i + 1] - d->row_ptr[i]);
+    for (int r = 0; r < nV0; r++) {
+        const int i = allV[r];
+        int c = 0;
+        for (int qq = d->row_ptr[i]; qq < d->row_ptr[i + 1]; qq++) c += keepInV(d->col[qq]);
+        vlen[r] = c;
+    }
+    // rows sorted by stored length within windows of 1024 (locality kept,
+    // slices nearly full)
+    std::vector<int32_t> vorder(nV0);
+    for (int r = 0; r < nV0; r++) vorder[r] = r;
+    for (int w0 = 0; w0 < nV0; w0 += 1024) {
+        const int w1 = std::min(nV0, w0 + 1024);
+        std::stable_sort(vorder.begin() + w0, vorder.begin() + w1,
+                         [&](int a, int b) { return vlen[a] > vlen[b]; });
+    }
+    int removableAtoms = 0;
+    for (int i = 0; i < n; i++) removableAtoms += (flags[i] & F_DIRICHLET) && dt[d->type_id[i]].removable;
+    const int E0 = (nV0 + 31) / 32 * 32;
+    const int reserve = ((std::min(65536, std::max(1024, removableAtoms)) + 31) / 32) * 32;
+    h->vCapacity = E0 + reserve;
+    const int nSlices = h->vCapacity / 32;
+    std::vector<int32_t> sliceStart(nSlices + 1, 0), sliceWidth(nSlices, 0);
+    for (int s = 0; s < E0 / 32; s++) {
+        int wmax = 0;
+        for (int k = 0; k < 32; k++) {
+            const int r = s * 32 + k;
+            if (r < nV0) wmax = std::max(wmax, vlen[vorder[r]]);
+        }
+        sliceWidth[s] = wmax;
+    }
+    for (int s = E0 / 32; s < nSlices; s++) sliceWidth[s] = maxRow;
+    for (int s = 0; s < nSlices; s++) sliceStart[s + 1] = sliceStart[s] + 32 * sliceWidth[s];
+    const size_t vStore = (size_t)sliceStart[nSlices];
+    const int zeroSlot = h->vCapacity;
+    std::vector<int32_t> vSlotOf(n, -1), vNodeOf(h->vCapacity, -1), vCol(vStore, zeroSlot), vPos(nnz, -1);
+    std::vector<float> vVal(vStore, 0.0f), vD(h->vCapacity + 1, 1.0f);
+    for (int s = 0; s < nV0; s++) {
+        vNodeOf[s] = allV[vorder[s]];
+        vSlotOf[vNodeOf[s]] = s;
+    }
+    for (int s = 0; s < nV0; s++) {
+        const int i = vNodeOf[s];
+        const int base = sliceStart[s / 32] + (s & 31);
+        double diag = 0.0;
+        int k = 0;
+        for (int qq = d->row_ptr[i]; qq < d->row_ptr[i + 1]; qq++) {
+            const int j = d->col[qq];
+            const double c = (flags[j] & F_NEUMANN) ? 0.0 : d->coupling[qq];
+            diag += c;
+            if (!keepInV(j)) continue;
+            vCol[base + 32 * k] = vSlotOf[j] >= 0 ? vSlotOf[j] : zeroSlot;
+            vVal[base + 32 * k] = (float)c;
+            vPos[qq] = base + 32 * k;
+            k++;
+        }
+        vD[s] = (float)diag;
+    }
+    h->vActive = E0;
+    for (int r = 0; r < nV0; r++) h->vEntries += vlen[r];
+
     auto up = [&](auto& buf, const auto* src, size_t count) -> cudaError_t {
         cudaError_t e = buf.alloc(count);
         if (e != cudaSuccess) return e;
@@ -464,6 +565,21 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(h->local.alloc(1 << 16));
     chk(h->localCount.alloc(66));
     chk(h->localScratch.alloc(1 << 16));
+    chk(h->vfield.alloc(3 * (size_t)n));
+    chk(up(h->vSlotOf, vSlotOf.data(), n));
+    chk(up(h->vNodeOf, vNodeOf.data(), h->vCapacity));
+    chk(up(h->vSliceStart, sliceStart.data(), nSlices + 1));
+    chk(up(h->vSliceWidth, sliceWidth.data(), nSlices));
+    chk(up(h->vCol, vCol.data(), vStore));
+    chk(up(h->vVal, vVal.data(), vStore));
+    chk(up(h->vPos, vPos.data(), nnz));
+    {
+        const int32_t next = E0;
+        chk(up(h->vCount, &next, 1));
+    }
+    chk(h->vVec.alloc(7 * ((size_t)h->vCapacity + 1)));
+    if (e == cudaSuccess) chk(cudaMemset(h->vVec.p, 0, 7 * ((size_t)h->vCapacity + 1) * sizeof(float)));
+    if (e == cudaSuccess) chk(cudaMemcpy(h->vVec.p, vD.data(), vD.size() * sizeof(float), cudaMemcpyHostToDevice));
     if (e != cudaSuccess) {
         const std::string msg = std::string("tg_create: ") + cudaGetErrorString(e);
         tg_destroy(h);
@@ -494,6 +610,9 @@ void tg_destroy(tg_handle* h) {
     h->keys.release(); h->result.release(); h->local.release(); h->localCount.release();
     h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
     h->stageImpact.release();
+    h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
+    h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
+    h->vScal.release(); h->vfield.release();
     if (h->evStart) cudaEventDestroy(h->evStart);
     if (h->evStop) cudaEventDestroy(h->evStop);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -529,18 +648,17 @@ int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, d
         return e;
     };
     if (which == 0) {
-        // k_cg_spmv over the non-Neumann free rows: row index, two row
-        // pointers, col + ceff32 per entry, p (once per row), diag32, ap
-        const double rows = (double)rowsV.size(), nnz = entries(rowsV);
-        *bytes = rows * (4 + 8 + 4 + 4 + 4) + nnz * (4 + 4);
-        CGVectors v = h->cg(0);
-        if (h->scalV.n < 8) CK(h->scalV.alloc(8));
-        v = h->cg(0);
-        const double one = 1.0;
-        CK(cudaMemcpyAsync(h->scalV.p, &one, sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        launch_cg_spmv_only(m, h->allV.p, h->countAllV, v, h->stream);  // warm
+        // k_vcg_spmv over the V system (SELL-32): col + val per stored entry
+        // (padding excluded), u (one compulsory read per row, the gathers
+        // hit the same vector), d, and the w write per row
+        const double rows = (double)h->vActive, stored = h->vEntries;
+        *bytes = rows * (4 + 4 + 4) + stored * (4 + 4);
+        if (h->vScal.n < 8) CK(h->vScal.alloc(8));
+        VSys v = h->vs();
+        CK(cudaMemsetAsync(h->vScal.p, 0, 8 * sizeof(double), h->stream));
+        launch_vcg_spmv(v, h->vActive, 0, -1.0, h->stream);  // warm
         CK(cudaEventRecord(h->evStart, h->stream));
-        for (int k = 0; k < iters; k++) launch_cg_spmv_only(m, h->allV.p, h->countAllV, v, h->stream);
+        for (int k = 0; k < iters; k++) launch_vcg_spmv(v, h->vActive, 0, -1.0, h->stream);
         CK(cudaEventRecord(h->evStop, h->stream));
     } else if (which == 1) {
         // k_residual over all free rows: row index, two row pointers, col +
@@ -720,17 +838,50 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     return TG_OK;
 }
 
+// Single-reduction PCG on the V system until gamma = r.u falls below
+// rtol^2 of its start value or maxIter is reached.  r (slot order) must hold
+// the right-hand side; x receives the correction.
+static int run_vcg(tg_handle* h, double rtol, int maxIter, int* itersOut) {
+    const size_t need = 3 * (size_t)(maxIter + 2);
+    if (h->vScal.n < need) CK(h->vScal.alloc(need));
+    VSys v = h->vs();
+    const int slots = h->vActive;
+    CK(cudaMemsetAsync(h->vScal.p, 0, sizeof(double) * need, h->stream));
+    launch_vcg_init(v, slots, h->stream);
+    launch_vcg_spmv(v, slots, 0, -1.0, h->stream);
+    double g0 = 0.0;
+    CK(cudaMemcpyAsync(&g0, h->vScal.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const double target = g0 * rtol * rtol;
+    int it = 0;
+    const int batch = 16;
+    while (it < maxIter && g0 > 0.0) {
+        const int end = std::min(maxIter, it + batch);
+        for (; it < end; it++) {
+            launch_vcg_update(v, slots, it, target, h->stream);
+            launch_vcg_spmv(v, slots, it + 1, target, h->stream);
+        }
+        double g = 0.0;
+        CK(cudaMemcpyAsync(&g, h->vScal.p + 3 * it, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (g <= target) break;
+    }
+    *itersOut = it;
+    return TG_OK;
+}
+
 int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     if (!h || !o) return fail(h, TG_ERR_ARGUMENT, "tg_solve: null argument");
     int rc = ensure_bnorm(h);
     if (rc != TG_OK) return rc;
     DevMesh m = h->dm();
-    CGVectors vV = h->cg(0), vN = h->cg(1);
+    VSys vsys = h->vs();
+    CGVectors vN = h->cg(1);
     tg_solve_info inf{};
     double rel = 0.0;
     for (int outer = 0;; outer++) {
         CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
-        launch_residual(m, h->allV.p, h->countAllV, vV.r, h->acc.p, h->stream);
+        launch_vcg_residual(m, vsys, h->vActive, h->acc.p, h->stream);
         launch_residual(m, h->allN.p, h->countAllN, vN.r, h->acc.p + 1, h->stream);
         double r2[2];
         CK(cudaMemcpyAsync(r2, h->acc.p, sizeof(r2), cudaMemcpyDeviceToHost, h->stream));
@@ -745,18 +896,21 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
             if (info) *info = inf;
             return fail(h, TG_ERR_ITERATION_CAP, "tg_solve: outer iteration cap reached");
         }
+        // inner reduction just sufficient for this step (not below the
+        // configured one, which bounds the FP32 work of the first step)
+        const double rtol = std::min(0.5, std::max(o->inner_rtol, 0.3 * o->rel_tol / rel));
         int itV = 0, itN = 0;
-        if (h->countAllV > 0 && r2[0] > 0.0) {
-            rc = run_cg(h, 0, h->allV.p, h->countAllV, o->inner_rtol, o->max_inner, &itV);
+        if (h->vActive > 0 && r2[0] > 0.0) {
+            rc = run_vcg(h, rtol, o->max_inner, &itV);
             if (rc != TG_OK) return rc;
         }
         if (h->countAllN > 0) {
-            launch_add_coupled(m, h->allN.p, h->countAllN, vV.x, vN.r, h->stream);
-            rc = run_cg(h, 1, h->allN.p, h->countAllN, o->inner_rtol, o->max_inner, &itN);
+            launch_vcg_couple_neumann(m, vsys, h->allN.p, h->countAllN, vN.r, h->stream);
+            rc = run_cg(h, 1, h->allN.p, h->countAllN, rtol, o->max_inner, &itN);
             if (rc != TG_OK) return rc;
         }
         inf.inner += itV + itN;
-        launch_apply_correction(m, h->allV.p, h->countAllV, vV, h->stream);
+        launch_vcg_apply(m, vsys, h->vActive, h->stream);
         launch_apply_correction(m, h->allN.p, h->countAllN, vN, h->stream);
     }
     h->selValid = false;
@@ -892,12 +1046,31 @@ int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached
     rc = refresh_counts(h);
     if (rc != TG_OK) return rc;
     const int nd = res[0];
+    std::vector<int32_t> flipped;
+    if (!(h->h_type[node] >= 0 && h->types[h->h_type[node]].dirichlet == 0)) flipped.push_back(node);
     h->h_type[node] = (int8_t)h->vacuumId;
     for (int k = 0; k < nd && k + 1 < (int)res.size(); k++) {
-        h->h_type[res[1 + k]] = (int8_t)h->vacuumId;
-        if (detached && k < capacity) detached[k] = res[1 + k];
+        const int j = res[1 + k];
+        if (h->types[h->h_type[j]].dirichlet) flipped.push_back(j);
+        h->h_type[j] = (int8_t)h->vacuumId;
+        if (detached && k < capacity) detached[k] = j;
     }
     if (numDetached) *numDetached = nd;
+    // cells that became non-Neumann free rows join the V system
+    const tg_type& vt = h->types[h->vacuumId];
+    if (!vt.dirichlet && !vt.neumann && !flipped.empty()) {
+        rc = stage(h, h->stageI, flipped.size());
+        if (rc != TG_OK) return rc;
+        CK(cudaMemcpyAsync(h->stageI.p, flipped.data(), sizeof(int32_t) * flipped.size(), cudaMemcpyHostToDevice,
+                           h->stream));
+        launch_vsys_add_rows(h->dm(), h->vs(), h->stageI.p, (int)flipped.size(), h->stream);
+        int32_t next = 0;
+        CK(cudaMemcpyAsync(&next, h->vCount.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        rc = sync_status(h, "tg_take_away (V rows)");
+        if (rc != TG_OK) return rc;
+        if (next > h->vCapacity) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: V-system reserve exhausted");
+        h->vActive = (next + 31) / 32 * 32;
+    }
     h->bnormValid = false;
     h->selValid = false;
     return TG_OK;
@@ -934,6 +1107,7 @@ int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, 
     tp.stepper_limit = o->stepper_limit;
     tp.walk_limit = o->walk_limit;
     tp.top_z = h->top_z;
+    launch_vertex_fields(h->dm(), h->stream);  // once per call, from the current potentials
     launch_trace(h->dm(), nIons, dStart, vel ? dVel : nullptr, dQm, h->stageI.p, tp, h->stageImpact.p, h->stream);
     CK(cudaMemcpyAsync(out, h->stageImpact.p, sizeof(tg_impact) * nIons, cudaMemcpyDeviceToHost, h->stream));
     return sync_status(h, "tg_trace");

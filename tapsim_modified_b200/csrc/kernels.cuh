@@ -46,6 +46,7 @@ struct DevMesh {
     const DType* types;
     int* status;
     double snap;   // power-of-two scale to the integer grid of the exact predicates
+    double* vfield;  // [3n] vertex fields of the current flight call
 };
 
 // Free-row bookkeeping kept on the device so that removals can append rows
@@ -69,6 +70,31 @@ struct Surface {
     float* ratio;          // per slot |E|/E_evap of the last selection
     int capacity;
 };
+
+// Non-Neumann free rows in their own slot order, couplings in SELL-32
+// (cg.cu).  Vectors hold capacity+1 entries; entry `capacity` is the zero
+// slot that entries of non-free neighbours point at.
+struct VSys {
+    int32_t* slot_of;             // [n] node -> slot, -1
+    int32_t* node_of;             // [capacity] slot -> node, -1 for padding
+    const int32_t* slice_start;   // [slices] first storage index of a slice
+    const int32_t* slice_width;   // [slices] entries per row in the slice
+    int32_t* col;                 // slot of the neighbour (or the zero slot)
+    float* val;                   // coupling as the row sees it
+    int32_t* vpos;                // [nnz] global CSR entry -> storage index, -1
+    float *d, *x, *r, *u, *w, *p, *sv;
+    double* scal;                 // gamma, delta, alpha per iteration
+    int32_t* count;               // next free slot (device counter)
+    int capacity;
+};
+void launch_vcg_init(const VSys& v, int slots, cudaStream_t s);
+void launch_vcg_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s);
+void launch_vcg_update(const VSys& v, int slots, int it, double target, cudaStream_t s);
+void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, cudaStream_t s);
+void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
+                               cudaStream_t s);
+void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, cudaStream_t s);
+void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
 
 // ---- relaxation (relax.cu) ----
 // coloured Gauss-Seidel sweep of one row list, FP64, max |delta| to *maxdev
@@ -130,6 +156,8 @@ struct ImpactOut {
     int32_t steps;
     int32_t status;
 };
+// field_o1 of every node from the current potentials into m.vfield
+void launch_vertex_fields(const DevMesh& m, cudaStream_t s);
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s);
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit,

@@ -41,15 +41,17 @@ def test_impacts_match_oracle(solved):
         assert abs(dev.stop_time - ref.stop_time) <= 1e-3 * abs(ref.stop_time)
         # the last point inside the mesh comes from the final accepted step,
         # which can jump from near the tip out of the box once the ion is
-        # fast: its potential depends on the step sequence
-        if dev.steps == ref.steps:
-            assert abs(dev.last_phi - ref.last_phi) <= 1e-6
+        # fast, so it depends on the step sequence: check the potential the
+        # device reports there against the oracle at the same point
+        lp = np.array(dev.last_pos, dtype=np.float64)
+        assert abs(dev.last_phi - o.potential_at(lp, dev.last_tet)) <= 1e-6
     rel = np.array(rel)
     print("impact radius relative differences", np.sort(rel))
-    # detector impacts relative to the impact radius: typically at rounding
-    # level; a diverged step sequence stays within a few 1e-3 (the per-step
-    # error threshold is 1e-6, magnified by the projection onto the detector)
-    assert np.median(rel) <= 1e-5
+    # detector impacts relative to the impact radius: 1e-6..1e-4 where the
+    # step sequences agree up to rounding-level accept/reject flips; a
+    # diverged sequence stays within a few 1e-3 (the per-step error threshold
+    # is 1e-6, magnified by the projection onto the detector)
+    assert np.median(rel) <= 5e-5
     assert rel.max() <= 1e-2
 
 

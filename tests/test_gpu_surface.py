@@ -85,6 +85,11 @@ def test_take_away_sequence_matches(small_mesh):
         o.phi[:] = g.potentials()
     # the removed cells are vacuum and free now
     assert (g.types() == 0).sum() == (a["type"] == 0).sum() + removed
+    # the solve over the grown system (rows appended by the removals)
+    # matches an independent oracle solve of the same system
+    o.solve(1e-12, 2_000_000, 1.9)
+    free = np.array([not a["types"][int(t)]["dirichlet"] for t in o.type])
+    assert np.abs(g.potentials() - o.phi)[free].max() < 2e-7
 
 
 def test_take_away_rejects_non_surface(small_mesh):
