@@ -133,6 +133,26 @@ int tg_get_phi(tg_handle* h, double* phi_out);       /* [N] */
 int tg_set_phi(tg_handle* h, const double* phi_in);  /* [N] */
 /* Grid_3d::Table::field_o1 (grid_3d.cpp:909-991) for a list of nodes. */
 int tg_field_o1(tg_handle* h, int32_t count, const int32_t* nodes, double* field_out /* [3*count] */);
+/* tg_field_o1 that makes no device allocation; no counterpart in the
+ * reference.  For callers that cannot allocate device memory when they ask
+ * for fields: all device memory already committed to the mesh and to another
+ * allocator's pool, or a real-time loop that must stay off the allocator.
+ * tg_field_o1 grows per-handle staging buffers with cudaMalloc; this call
+ * stages the node list and the results in a fixed scratch array that is part
+ * of the library's device image instead.
+ *   - At most TG_FIELD_O1_NOALLOC_MAX nodes per call; a longer list fails
+ *     with TG_ERR_ARGUMENT before anything runs.  Node indices are checked
+ *     against the mesh (TG_ERR_ARGUMENT when out of range).
+ *   - The first call on a device looks up the scratch's device address
+ *     (which can load the library's device image onto that device); make
+ *     that first call before any stream capture.
+ *   - There is one scratch per device, shared by all handles and threads of
+ *     the process: calls that overlap on the same device (from two threads,
+ *     or two handles) race on it and return each other's results.  Calls
+ *     made one after another are safe.
+ * Results equal tg_field_o1's for the same nodes. */
+#define TG_FIELD_O1_NOALLOC_MAX 65536
+int tg_field_o1_noalloc(tg_handle* h, int32_t count, const int32_t* nodes, double* field_out /* [3*count] */);
 /* Current coupling, type and effective diagonal (for checks). */
 int tg_get_couplings(tg_handle* h, double* coupling_out /* [nnz] */);
 int tg_get_types(tg_handle* h, int8_t* type_out /* [N] */);

@@ -105,6 +105,7 @@ SIGNATURES = {
     "tg_get_phi": (C.c_int, [_P, _P]),
     "tg_set_phi": (C.c_int, [_P, _P]),
     "tg_field_o1": (C.c_int, [_P, _I, _P, _P]),
+    "tg_field_o1_noalloc": (C.c_int, [_P, _I, _P, _P]),
     "tg_get_couplings": (C.c_int, [_P, _P]),
     "tg_get_types": (C.c_int, [_P, _P]),
     "tg_surface_init": (C.c_int, [_P, _I, C.POINTER(_I)]),

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1227,6 +1228,77 @@ int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_ev
         for (int k = 0; k < 3; k++) rec->field_after[k] = (float)E[k];
     }
     return TG_OK;
+}
+
+}  // extern "C"
+
+// ---- field_o1 without allocation ----
+//
+// tg_field_o1 stages its node list and results in per-handle device buffers
+// that grow with cudaMalloc when a call asks for more nodes than any call
+// before it.  Some callers cannot allocate at that point: a host whose
+// device memory is fully committed to the mesh and to another allocator's
+// pool (a caching allocator that already holds the rest of the 180 GB), or a
+// real-time loop that must not take the driver's allocation lock between
+// events.  tg_field_o1_noalloc serves them from a fixed scratch array that
+// is part of this library's device image, so it makes no allocation call.
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+// nodes (int32) first, then the fields (3 doubles per node); both offsets
+// are multiples of 256 bytes
+constexpr size_t kNoAllocNodesBytes = sizeof(int32_t) * (size_t)TG_FIELD_O1_NOALLOC_MAX;
+constexpr size_t kNoAllocBytes = kNoAllocNodesBytes + 3 * sizeof(double) * (size_t)TG_FIELD_O1_NOALLOC_MAX;
+static_assert(kNoAllocNodesBytes % 256 == 0, "field offset must stay 256-byte aligned");
+static __device__ __align__(256) unsigned char g_field_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on the current device, looked up once per
+// device (the lookup may load this library's device image onto the device).
+int noalloc_scratch(tg_handle* h, unsigned char** out) {
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(h, TG_ERR_ARGUMENT, "tg_field_o1_noalloc: device ordinal beyond the 64 the scratch table covers");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_field_scratch));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+    return TG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tg_field_o1_noalloc(tg_handle* h, int32_t count, const int32_t* nodes, double* out) {
+    if (!h || count < 0 || (count && (!nodes || !out)))
+        return fail(h, TG_ERR_ARGUMENT, "tg_field_o1_noalloc: bad argument");
+    if (count > TG_FIELD_O1_NOALLOC_MAX)
+        return fail(h, TG_ERR_ARGUMENT,
+                    "tg_field_o1_noalloc: " + std::to_string(count) + " nodes exceed the fixed scratch of " +
+                        std::to_string(TG_FIELD_O1_NOALLOC_MAX) + " nodes; split the list or call tg_field_o1");
+    for (int32_t k = 0; k < count; k++)
+        if (nodes[k] < 0 || nodes[k] >= h->n)
+            return fail(h, TG_ERR_ARGUMENT, "tg_field_o1_noalloc: node index out of range");
+    unsigned char* base = nullptr;
+    int rc = noalloc_scratch(h, &base);
+    if (rc != TG_OK || count == 0) return rc;
+    int32_t* dNodes = reinterpret_cast<int32_t*>(base);
+    double* dOut = reinterpret_cast<double*>(base + kNoAllocNodesBytes);
+    // Nothing in the scratch has to start at zero: the node list is copied
+    // in and the kernel writes every one of the count results.  The
+    // handle's status word, which the kernel may set, is cleared by
+    // sync_status whenever it is found set.
+    CK(cudaMemcpyAsync(dNodes, nodes, sizeof(int32_t) * count, cudaMemcpyHostToDevice, h->stream));
+    launch_field_o1(h->dm(), dNodes, count, dOut, h->stream);
+    CK(cudaMemcpyAsync(out, dOut, sizeof(double) * 3 * count, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_field_o1_noalloc");
 }
 
 }  // extern "C"
