@@ -124,6 +124,8 @@ typedef struct {
     int32_t inner;            /* FP32 iterations taken in total */
     double rel_residual;      /* final ||r||/||b|| */
     double initial_rel_residual;
+    int32_t inner_neumann;    /* of `inner`, the iterations on the Neumann rows */
+    int32_t reserved;
 } tg_solve_info;
 int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);
 /* ||r||_2 / ||b||_2 of the current potentials (FP64). */

@@ -24,24 +24,25 @@ namespace {
 
 constexpr int kBlock = 256;
 
-// s_i = gamma_i, delta_i, alpha_i at scal[3i], scal[3i+1], scal[3i+2]
+// per iteration i: gamma_i = r.u, delta_i = w.u, alpha_i and rho_i = r.r at
+// scal[4i .. 4i+3]
 __device__ __forceinline__ void cg_coeffs(const double* scal, int it, double* alpha, double* beta) {
-    const double g = scal[3 * it], d = scal[3 * it + 1];
+    const double g = scal[4 * it], d = scal[4 * it + 1];
     if (it == 0) {
         *beta = 0.0;
         *alpha = d > 0.0 ? g / d : 0.0;
     } else {
-        const double gp = scal[3 * (it - 1)], ap = scal[3 * (it - 1) + 2];
+        const double gp = scal[4 * (it - 1)], ap = scal[4 * (it - 1) + 2];
         *beta = gp > 0.0 ? g / gp : 0.0;
         const double den = d - *beta * g / ap;
         *alpha = den > 0.0 ? g / den : 0.0;
     }
 }
 
-// u = r / d, x = 0, gamma_0 = r.u
+// u = r / d, x = 0, gamma_0 = r.u, rho_0 = r.r
 __global__ void k_vcg_init(VSys v, int slots) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    double g = 0.0;
+    double g = 0.0, rr = 0.0;
     if (s < slots) {
         const float r = v.r[s];
         const float u = r / v.d[s];
@@ -50,14 +51,16 @@ __global__ void k_vcg_init(VSys v, int slots) {
         v.p[s] = 0.0f;
         v.sv[s] = 0.0f;
         g = (double)r * (double)u;
+        rr = (double)r * (double)r;
     }
     block_sum_atomic<kBlock>(g, &v.scal[0]);
+    block_sum_atomic<kBlock>(rr, &v.scal[3]);
 }
 
-// w = A u over SELL-32 slices; delta -> scal[3*it+1] (it = iteration whose
-// u this is); skipped once gamma_it <= target
+// w = A u over SELL-32 slices; delta -> scal[4*it+1] (it = iteration whose
+// u this is); skipped once rho_it <= target
 __global__ void k_vcg_spmv(VSys v, int slices, int it, double target) {
-    if (it >= 0 && v.scal[3 * it] <= target) return;
+    if (it >= 0 && v.scal[4 * it + 3] <= target) return;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     double dl = 0.0;
@@ -67,27 +70,42 @@ __global__ void k_vcg_spmv(VSys v, int slices, int it, double target) {
         const int s = warp * 32 + lane;
         const int* __restrict__ col = v.col + base + lane;
         const float* __restrict__ val = v.val + base + lane;
+        const float* __restrict__ uu = v.u;
         float acc = 0.0f;
-#pragma unroll 4
-        for (int k = 0; k < width; k++) acc += val[32 * k] * v.u[col[32 * k]];
+        // eight independent column/value loads ahead of their gathers keep
+        // enough bytes in flight per warp; the matrix is streamed once per
+        // iteration (evict-first), the gathered vector stays cached
+        int k = 0;
+        for (; k + 8 <= width; k += 8) {
+            int c[8];
+            float a[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                c[j] = __ldcs(col + 32 * (k + j));
+                a[j] = __ldcs(val + 32 * (k + j));
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc += a[j] * __ldg(uu + c[j]);
+        }
+        for (; k < width; k++) acc += __ldcs(val + 32 * k) * __ldg(uu + __ldcs(col + 32 * k));
         const float u = v.u[s];
         const float w = v.d[s] * u - acc;
         v.w[s] = w;
         dl = (double)w * (double)u;
     }
-    block_sum_atomic<kBlock>(dl, &v.scal[3 * (it < 0 ? 0 : it) + 1]);
+    block_sum_atomic<kBlock>(dl, &v.scal[4 * (it < 0 ? 0 : it) + 1]);
 }
 
 // p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s, u = r / d,
-// gamma_{it+1} = r.u
+// gamma_{it+1} = r.u, rho_{it+1} = r.r
 __global__ void k_vcg_update(VSys v, int slots, int it, double target) {
-    if (v.scal[3 * it] <= target) return;
+    if (v.scal[4 * it + 3] <= target) return;
     double alpha, beta;
     cg_coeffs(v.scal, it, &alpha, &beta);
-    if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[3 * it + 2] = alpha;
+    if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[4 * it + 2] = alpha;
     const float a = (float)alpha, b = (float)beta;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    double g = 0.0;
+    double g = 0.0, rr = 0.0;
     if (s < slots) {
         const float p = v.u[s] + b * v.p[s];
         const float sv = v.w[s] + b * v.sv[s];
@@ -99,8 +117,10 @@ __global__ void k_vcg_update(VSys v, int slots, int it, double target) {
         const float u = r / v.d[s];
         v.u[s] = u;
         g = (double)r * (double)u;
+        rr = (double)r * (double)r;
     }
-    block_sum_atomic<kBlock>(g, &v.scal[3 * (it + 1)]);
+    block_sum_atomic<kBlock>(g, &v.scal[4 * (it + 1)]);
+    block_sum_atomic<kBlock>(rr, &v.scal[4 * (it + 1) + 3]);
 }
 
 // phi64[node] += x[slot]; clears the slot's vectors

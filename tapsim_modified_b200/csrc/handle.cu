@@ -821,51 +821,76 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     }
     CK(cudaMemsetAsync(scal.p, 0, sizeof(double) * need, h->stream));
     launch_cg_init(m, rows, count, v, h->stream);
-    double rz0 = 0.0;
-    CK(cudaMemcpyAsync(&rz0, scal.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    // stop on the 2-norm of the residual (r.r at scal[3it+2]), the norm the
+    // outer FP64 test uses
+    double rr0 = 0.0;
+    CK(cudaMemcpyAsync(&rr0, scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    const double target = rz0 * rtol * rtol;
+    const double target = rr0 * rtol * rtol;
     int it = 0;
     const int batch = 16;
-    while (it < maxIter && rz0 > 0.0) {
+    double sb[3 * batch];
+    while (it < maxIter && rr0 > 0.0) {
+        const int start = it;
         const int end = std::min(maxIter, it + batch);
         for (; it < end; it++) launch_cg_iter(m, rows, count, v, it, target, h->stream);
-        double rz = 0.0;
-        CK(cudaMemcpyAsync(&rz, scal.p + 3 * it, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        // r.r after j iterations sits at scal[3j+2]; the kernels of later
+        // iterations of the batch returned early once it met the target
+        CK(cudaMemcpyAsync(sb, scal.p + 3 * (size_t)(start + 1), sizeof(double) * 3 * (end - start),
+                           cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        if (rz <= target) break;
+        bool done = false;
+        for (int j = start + 1; j <= end && !done; j++)
+            if (sb[3 * (j - start - 1) + 2] <= target) {
+                it = j;
+                done = true;
+            }
+        if (done) break;
     }
     *itersOut = it;
     return TG_OK;
 }
 
-// Single-reduction PCG on the V system until gamma = r.u falls below
-// rtol^2 of its start value or maxIter is reached.  r (slot order) must hold
+// Single-reduction PCG on the V system until rho = r.r falls below rtol^2
+// of its start value or maxIter is reached.  r (slot order) must hold
 // the right-hand side; x receives the correction.
 static int run_vcg(tg_handle* h, double rtol, int maxIter, int* itersOut) {
-    const size_t need = 3 * (size_t)(maxIter + 2);
+    const size_t need = 4 * (size_t)(maxIter + 2);
     if (h->vScal.n < need) CK(h->vScal.alloc(need));
     VSys v = h->vs();
     const int slots = h->vActive;
     CK(cudaMemsetAsync(h->vScal.p, 0, sizeof(double) * need, h->stream));
     launch_vcg_init(v, slots, h->stream);
     launch_vcg_spmv(v, slots, 0, -1.0, h->stream);
-    double g0 = 0.0;
-    CK(cudaMemcpyAsync(&g0, h->vScal.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    // stop on the 2-norm of the residual (rho = r.r), the norm the outer
+    // FP64 test uses
+    double s0[4];
+    CK(cudaMemcpyAsync(s0, h->vScal.p, sizeof(s0), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    const double target = g0 * rtol * rtol;
+    const double rho0 = s0[3];
+    const double target = rho0 * rtol * rtol;
     int it = 0;
     const int batch = 16;
-    while (it < maxIter && g0 > 0.0) {
+    double sb[4 * batch];
+    while (it < maxIter && rho0 > 0.0) {
+        const int start = it;
         const int end = std::min(maxIter, it + batch);
         for (; it < end; it++) {
             launch_vcg_update(v, slots, it, target, h->stream);
             launch_vcg_spmv(v, slots, it + 1, target, h->stream);
         }
-        double g = 0.0;
-        CK(cudaMemcpyAsync(&g, h->vScal.p + 3 * it, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        // rho after j iterations sits at scal[4j+3]; the kernels of later
+        // iterations of the batch returned early once it met the target
+        CK(cudaMemcpyAsync(sb, h->vScal.p + 4 * (size_t)(start + 1), sizeof(double) * 4 * (end - start),
+                           cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        if (g <= target) break;
+        bool done = false;
+        for (int j = start + 1; j <= end && !done; j++)
+            if (sb[4 * (j - start - 1) + 3] <= target) {
+                it = j;
+                done = true;
+            }
+        if (done) break;
     }
     *itersOut = it;
     return TG_OK;
@@ -911,6 +936,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
             if (rc != TG_OK) return rc;
         }
         inf.inner += itV + itN;
+        inf.inner_neumann += itN;
         launch_vcg_apply(m, vsys, h->vActive, h->stream);
         launch_apply_correction(m, h->allN.p, h->countAllN, vN, h->stream);
     }
@@ -922,6 +948,8 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
 int tg_field_o1(tg_handle* h, int32_t count, const int32_t* nodes, double* out) {
     if (!h || count < 0 || (count && (!nodes || !out))) return fail(h, TG_ERR_ARGUMENT, "tg_field_o1: bad argument");
     if (count == 0) return TG_OK;
+    for (int32_t k = 0; k < count; k++)
+        if (nodes[k] < 0 || nodes[k] >= h->n) return fail(h, TG_ERR_ARGUMENT, "tg_field_o1: node index out of range");
     int rc = stage(h, h->stageI, count);
     if (rc == TG_OK) rc = stage(h, h->stageD, 3 * (size_t)count);
     if (rc != TG_OK) return rc;
@@ -1088,6 +1116,10 @@ int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, 
     if (!h || nIons < 0 || (nIons && (!start || !qm || !out)) || !o) return fail(h, TG_ERR_ARGUMENT, "tg_trace: bad argument");
     if (!h->tet_v.p) return fail(h, TG_ERR_ARGUMENT, "tg_trace: mesh has no tetrahedra");
     if (nIons == 0) return TG_OK;
+    if (guess)
+        for (int32_t k = 0; k < nIons; k++)
+            if (guess[k] < 0 || guess[k] >= h->ntets)
+                return fail(h, TG_ERR_ARGUMENT, "tg_trace: tetrahedron guess out of range");
     int rc = stage(h, h->stageF, (size_t)nIons * 7);
     if (rc == TG_OK) rc = stage(h, h->stageI, nIons);
     if (rc == TG_OK) rc = stage(h, h->stageImpact, nIons);
@@ -1117,6 +1149,11 @@ int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, 
 int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* guess, float* out) {
     if (!h || n < 0 || (n && (!xyz || !out))) return fail(h, TG_ERR_ARGUMENT, "tg_potential_at: bad argument");
     if (n == 0) return TG_OK;
+    if (!h->tet_v.p) return fail(h, TG_ERR_ARGUMENT, "tg_potential_at: mesh has no tetrahedra");
+    if (guess)
+        for (int32_t k = 0; k < n; k++)
+            if (guess[k] < 0 || guess[k] >= h->ntets)
+                return fail(h, TG_ERR_ARGUMENT, "tg_potential_at: tetrahedron guess out of range");
     int rc = stage(h, h->stageF, (size_t)n * 4);
     if (rc == TG_OK) rc = stage(h, h->stageI, n);
     if (rc != TG_OK) return rc;

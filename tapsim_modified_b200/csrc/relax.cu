@@ -80,7 +80,7 @@ __global__ void k_bnorm(DevMesh m, const int32_t* __restrict__ rows, int count, 
 // z = r / diag, p = z, rz -> scal[0]
 __global__ void k_cg_init(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double rz = 0.0;
+    double rz = 0.0, rr = 0.0;
     if (t < count) {
         const int i = rows[t];
         const float r = v.r[i];
@@ -89,13 +89,16 @@ __global__ void k_cg_init(DevMesh m, const int32_t* __restrict__ rows, int count
         v.p[i] = z;
         v.x[i] = 0.0f;
         rz = (double)r * (double)z;
+        rr = (double)r * (double)r;
     }
     block_sum_atomic<kBlock>(rz, &v.scal[0]);
+    block_sum_atomic<kBlock>(rr, &v.scal[2]);
 }
 
-// ap = A p on the rows (A = diag - offdiag), pAp -> scal[3it+1]
+// ap = A p on the rows (A = diag - offdiag), pAp -> scal[3it+1]; all three
+// kernels of an iteration are skipped once r.r (scal[3it+2]) <= target
 __global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
-    if (v.scal[3 * it] <= target) return;
+    if (v.scal[3 * it + 2] <= target) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double pap = 0.0;
     if (t < count) {
@@ -111,14 +114,14 @@ __global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count
     block_sum_atomic<kBlock>(pap, &v.scal[3 * it + 1]);
 }
 
-// x += a p, r -= a ap, z = r/diag, rz_next -> scal[3(it+1)]
+// x += a p, r -= a ap, z = r/diag, rz_next -> scal[3(it+1)], r.r -> scal[3(it+1)+2]
 __global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
     const double rz = v.scal[3 * it];
-    if (rz <= target) return;
+    if (v.scal[3 * it + 2] <= target) return;
     const double pap = v.scal[3 * it + 1];
     const float alpha = pap > 0.0 ? (float)(rz / pap) : 0.0f;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double rzn = 0.0;
+    double rzn = 0.0, rrn = 0.0;
     if (t < count) {
         const int i = rows[t];
         v.x[i] += alpha * v.p[i];
@@ -127,14 +130,16 @@ __global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int cou
         const float z = r / m.diag32[i];
         v.z[i] = z;
         rzn = (double)r * (double)z;
+        rrn = (double)r * (double)r;
     }
     block_sum_atomic<kBlock>(rzn, &v.scal[3 * (it + 1)]);
+    block_sum_atomic<kBlock>(rrn, &v.scal[3 * (it + 1) + 2]);
 }
 
 // p = z + beta p
 __global__ void k_cg_pupdate(const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
     const double rz = v.scal[3 * it];
-    if (rz <= target) return;
+    if (v.scal[3 * it + 2] <= target) return;
     const double rzn = v.scal[3 * (it + 1)];
     const float beta = (float)(rzn / rz);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;

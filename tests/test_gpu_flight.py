@@ -81,3 +81,19 @@ def test_potential_at_matches_oracle(solved):
     dev = g.potential_at(pts, guess)
     ref = np.array([o.potential_at(p, t) for p, t in zip(pts.astype(np.float64), guess)])
     assert np.abs(dev - ref).max() <= 1e-6
+
+
+def test_out_of_range_indices_are_rejected(solved):
+    from tapsim_modified_b200 import _native as N
+    a, g, o = solved
+    ntets = len(a["tet_v"]) // 4 if a["tet_v"].ndim == 1 else len(a["tet_v"])
+    for bad in (-1, ntets):
+        with pytest.raises(N.TapsimError) as e:
+            g.trace(a["xyz"][:1], QM_FE, bad)
+        assert e.value.code == 1
+        with pytest.raises(N.TapsimError) as e:
+            g.potential_at(a["xyz"][:1].astype(np.float32), np.array([bad], np.int32))
+        assert e.value.code == 1
+    with pytest.raises(N.TapsimError) as e:
+        g.field_o1([g.n])
+    assert e.value.code == 1
