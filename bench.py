@@ -166,36 +166,50 @@ def run_ours(args, rank: int, world: int, dist):
     atoms = int((arrays["type"] == 4).sum())
     h2d_bytes = sum(v.nbytes for k, v in arrays.items() if isinstance(v, np.ndarray))
     opts = EvaporationOptions.from_ini(None)
-    sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4)
 
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t_e2e0 = time.perf_counter()
-    grid = Grid(mesh)                       # host -> device upload of the mesh
-    info0 = grid.solve(REL_TOL, 50, 50000, 1e-4)  # initial relaxation
-    ev = Evaporation(grid, opts, relax_mode=1, solve=sopts)
-    for _ in range(args.warmup):
-        ev.step()
-    # timed region: K events, CUDA events on the handle's stream
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = L.tg_launch_count(grid._h)
-    with ClockSampler(local) as clocks:
-        N.check(L.tg_timer_start(grid._h), grid._h)
-        for _ in range(args.steps):
+    def run_arm(warm_start: int):
+        """Mesh upload, initial relaxation, W warm-up and K timed events with
+        the given solve start; returns the timings and the event records."""
+        sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4, warm_start=warm_start)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        grid = Grid(mesh)                       # host -> device upload of the mesh
+        info0 = grid.solve(REL_TOL, 50, 50000, 1e-4)  # initial relaxation
+        ev = Evaporation(grid, opts, relax_mode=1, solve=sopts)
+        for _ in range(args.warmup):
             ev.step()
-        ms = C.c_float()
-        N.check(L.tg_timer_stop(grid._h, C.byref(ms)), grid._h)
-    torch.cuda.synchronize()
-    launches = L.tg_launch_count(grid._h) - launches0
-    phi = grid.potentials()                 # device -> host result
-    t_e2e = time.perf_counter() - t_e2e0
-    dev_s = ms.value / 1e3
-    recs = ev.records[args.warmup:]
+        # timed region: K events, CUDA events on the handle's stream
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = L.tg_launch_count(grid._h)
+        with ClockSampler(local) as clocks:
+            N.check(L.tg_timer_start(grid._h), grid._h)
+            for _ in range(args.steps):
+                ev.step()
+            ms = C.c_float()
+            N.check(L.tg_timer_stop(grid._h, C.byref(ms)), grid._h)
+        torch.cuda.synchronize()
+        launches = L.tg_launch_count(grid._h) - launches0
+        phi = grid.potentials()                 # device -> host result
+        t_e2e = time.perf_counter() - t0
+        return {"grid": grid, "info0": info0, "dev_s": ms.value / 1e3, "t_e2e": t_e2e, "launches": launches,
+                "records": ev.records, "clocks": clocks, "phi": phi}
+
+    plain = run_arm(0)
+    plain["grid"].close()
+    arm = run_arm(1)
+    grid, info0, dev_s, t_e2e, phi, clocks = (arm[k] for k in ("grid", "info0", "dev_s", "t_e2e", "phi", "clocks"))
+    launches = arm["launches"]
+    recs = arm["records"][args.warmup:]
     iters = [r["relax_iterations"] for r in recs]
-    resid = max(r["rel_residual"] for r in recs)
+    iters_plain = [r["relax_iterations"] for r in plain["records"][args.warmup:]]
+    resid = max(r["rel_residual"] for r in recs + plain["records"][args.warmup:])
+    seq_w = [r["node"] for r in arm["records"]]
+    seq_p = [r["node"] for r in plain["records"]]
+    first_diff = next((k for k, (x, y) in enumerate(zip(seq_w, seq_p)) if x != y), None)
     # roofline of the dominant kernel (the FP32 CG SpMV) on this mesh
     avg = C.c_float()
     nbytes = C.c_double()
@@ -206,15 +220,17 @@ def run_ours(args, rank: int, world: int, dist):
     N.check(L.tg_bench_kernel(grid._h, 1, 20, C.byref(r_avg), C.byref(r_bytes)), grid._h)
 
     if dist:
-        t = torch.tensor([dev_s, t_e2e, float(args.steps), float(args.warmup + args.steps)], dtype=torch.float64,
-                         device="cuda")
+        t = torch.tensor([dev_s, t_e2e, plain["dev_s"], float(args.steps), float(args.warmup + args.steps)],
+                         dtype=torch.float64, device="cuda")
         mx = t.clone()
-        dist.all_reduce(mx[:2], op=dist.ReduceOp.MAX)
+        dist.all_reduce(mx[:3], op=dist.ReduceOp.MAX)
         sm = t.clone()
-        dist.all_reduce(sm[2:], op=dist.ReduceOp.SUM)
-        dev_max, e2e_max, ev_total, ev_e2e_total = float(mx[0]), float(mx[1]), float(sm[2]), float(sm[3])
+        dist.all_reduce(sm[3:], op=dist.ReduceOp.SUM)
+        dev_max, e2e_max, plain_max = float(mx[0]), float(mx[1]), float(mx[2])
+        ev_total, ev_e2e_total = float(sm[3]), float(sm[4])
     else:
-        dev_max, e2e_max, ev_total, ev_e2e_total = dev_s, t_e2e, float(args.steps), float(args.warmup + args.steps)
+        dev_max, e2e_max, plain_max = dev_s, t_e2e, plain["dev_s"]
+        ev_total, ev_e2e_total = float(args.steps), float(args.warmup + args.steps)
     if rank != 0:
         return None
 
@@ -239,8 +255,14 @@ def run_ours(args, rank: int, world: int, dist):
                         f"{TIPS[args.tip]['shank_length'] * 1e9:g} nm shank, "
                         f"{TIPS[args.tip]['half_angle_deg']:g} deg, vacuum to 1 um; {atoms} atoms, "
                         f"{mesh.num_nodes} cells per GPU; relax to rel. residual <= {REL_TOL:g} every event; "
-                        "plain relaxation (previous-event warm start)",
+                        "solve started from the previous event's correction (recycled far field)",
             "events_per_gpu": args.steps,
+            "plain": {"value": ev_total / plain_max, "ms_per_step": plain_max * 1e3 / args.steps,
+                      "solver_iterations_median": statistics.median(iters_plain),
+                      "start": "previous event's potentials (plain relaxation)"},
+            "warm_over_plain": plain_max / dev_max,
+            "sequence": {"events": len(seq_w), "first_difference": first_diff,
+                         "note": "removed-node sequences of the warm-start and plain arms"},
             "l2": "inputs larger than L2 (CSR working set ~GB)",
             "parallelism": f"independent tips, one per GPU (x{world})",
             "solver_iterations_median": statistics.median(iters),

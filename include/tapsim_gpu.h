@@ -118,6 +118,14 @@ typedef struct {
     int32_t max_outer;        /* FP64 defect-correction steps */
     int32_t max_inner;        /* FP32 iterations per step */
     double inner_rtol;        /* inner relative reduction per step */
+    /* Start of a solve that follows removals from a converged state:
+     *   0  the current potentials (the previous event's solution; plain),
+     *   1  plus the previous event's correction on the non-Neumann free
+     *      cells (the smooth far field of one removal changes little
+     *      from one site to the next).
+     * The solve always ends at rel_tol, whatever the start. */
+    int32_t warm_start;
+    int32_t reserved;
 } tg_solve_opts;
 typedef struct {
     int32_t outer;            /* defect-correction steps taken */

@@ -39,7 +39,7 @@ class tg_mesh_desc(C.Structure):
 
 class tg_solve_opts(C.Structure):
     _fields_ = [("rel_tol", C.c_double), ("max_outer", C.c_int32), ("max_inner", C.c_int32),
-                ("inner_rtol", C.c_double)]
+                ("inner_rtol", C.c_double), ("warm_start", C.c_int32), ("reserved", C.c_int32)]
 
 
 class tg_solve_info(C.Structure):

@@ -123,13 +123,28 @@ __global__ void k_vcg_update(VSys v, int slots, int it, double target) {
     block_sum_atomic<kBlock>(rr, &v.scal[4 * (it + 1) + 3]);
 }
 
-// phi64[node] += x[slot]; clears the slot's vectors
-__global__ void k_vcg_apply(DevMesh m, VSys v, int slots) {
+// phi64[node] += x[slot] (and hist[slot] += x[slot] when recording);
+// clears the slot's vectors
+__global__ void k_vcg_apply(DevMesh m, VSys v, int slots, int record) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= slots) return;
     const int i = v.node_of[s];
-    if (i >= 0) m.phi64[i] += (double)v.x[s];
+    if (i >= 0) {
+        m.phi64[i] += (double)v.x[s];
+        if (record) v.hist[s] += v.x[s];
+    }
     v.x[s] = v.r[s] = v.u[s] = v.w[s] = v.p[s] = v.sv[s] = 0.0f;
+}
+
+// hist *= alpha; phi64[node] += hist[slot]
+__global__ void k_vcg_warm(DevMesh m, VSys v, int slots, float alpha) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots) return;
+    const int i = v.node_of[s];
+    if (i < 0) return;
+    const float h = alpha * v.hist[s];
+    v.hist[s] = h;
+    m.phi64[i] += (double)h;
 }
 
 // r of the Neumann rows += sum over V neighbours ceff_ij x_j
@@ -240,8 +255,11 @@ void launch_vcg_spmv(const VSys& v, int slots, int it, double target, cudaStream
 void launch_vcg_update(const VSys& v, int slots, int it, double target, cudaStream_t s) {
     if (slots > 0) { count_launch(); k_vcg_update<<<blocks(slots), kBlock, 0, s>>>(v, slots, it, target); }
 }
-void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_apply<<<blocks(slots), kBlock, 0, s>>>(m, v, slots); }
+void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_apply<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, record ? 1 : 0); }
+}
+void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_warm<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, alpha); }
 }
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
                                cudaStream_t s) {

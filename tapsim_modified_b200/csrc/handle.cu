@@ -98,7 +98,7 @@ struct tg_handle {
 
     // non-Neumann free rows in slot order, SELL-32 (cg.cu)
     DBuf<int32_t> vSlotOf, vNodeOf, vSliceStart, vSliceWidth, vCol, vPos, vCount;
-    DBuf<float> vVal, vVec;  // vVec: d, x, r, u, w, p, sv, each capacity+1
+    DBuf<float> vVal, vVec;  // vVec: d, x, r, u, w, p, sv, hist, each capacity+1
     DBuf<double> vScal;
     DBuf<double> vfield;     // vertex fields of the current flight call
     int vCapacity = 0;       // slots incl. the append reserve
@@ -122,6 +122,7 @@ struct tg_handle {
         v.w = vVec.p + 4 * stride;
         v.p = vVec.p + 5 * stride;
         v.sv = vVec.p + 6 * stride;
+        v.hist = vVec.p + 7 * stride;
         v.scal = vScal.p;
         v.count = vCount.p;
         v.capacity = vCapacity;
@@ -130,6 +131,12 @@ struct tg_handle {
 
     bool bnormValid = false;
     double bnorm2 = 0.0;
+    // warm start bookkeeping: the correction of a solve is recorded (VSys
+    // hist) when the solve starts from a converged state changed only by
+    // removals; it seeds the next such solve
+    bool converged = false;
+    int removalsSinceSolve = 0;
+    bool histValid = false;
     bool selValid = false;
     tg_select_info sel{};
     int vacuumId = -1;
@@ -578,8 +585,8 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
         const int32_t next = E0;
         chk(up(h->vCount, &next, 1));
     }
-    chk(h->vVec.alloc(7 * ((size_t)h->vCapacity + 1)));
-    if (e == cudaSuccess) chk(cudaMemset(h->vVec.p, 0, 7 * ((size_t)h->vCapacity + 1) * sizeof(float)));
+    chk(h->vVec.alloc(8 * ((size_t)h->vCapacity + 1)));
+    if (e == cudaSuccess) chk(cudaMemset(h->vVec.p, 0, 8 * ((size_t)h->vCapacity + 1) * sizeof(float)));
     if (e == cudaSuccess) chk(cudaMemcpy(h->vVec.p, vD.data(), vD.size() * sizeof(float), cudaMemcpyHostToDevice));
     if (e != cudaSuccess) {
         const std::string msg = std::string("tg_create: ") + cudaGetErrorString(e);
@@ -694,6 +701,7 @@ int tg_set_phi(tg_handle* h, const double* phi) {
     CK(cudaMemcpyAsync(h->phi64.p, phi, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
     h->bnormValid = false;
     h->selValid = false;
+    h->converged = h->histValid = false;
     return sync_status(h, "tg_set_phi");
 }
 
@@ -719,6 +727,7 @@ int tg_relax_cycles(tg_handle* h, int32_t n, double* deviation) {
     const int rc = sync_status(h, "tg_relax_cycles");
     if (deviation) *deviation = dev;
     h->selValid = false;
+    h->converged = h->histValid = false;
     return rc;
 }
 
@@ -752,6 +761,7 @@ int tg_relax_threshold(tg_handle* h, double threshold, int32_t cycle, int32_t qu
 int tg_local_relax(tg_handle* h, int32_t node, int32_t shell, double threshold, int32_t cycle, int32_t queueSize,
                    int64_t* iterations, double* deviation) {
     if (!h || node < 0 || node >= h->n || cycle < 1) return fail(h, TG_ERR_ARGUMENT, "tg_local_relax: bad argument");
+    h->converged = h->histValid = false;
     DevMesh m = h->dm();
     launch_local_set(m, node, shell, h->local.p, h->localCount.p, (int)h->local.n, h->localScratch.p,
                      (int)h->localScratch.n, h->ncol, h->stream);
@@ -905,6 +915,14 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     CGVectors vN = h->cg(1);
     tg_solve_info inf{};
     double rel = 0.0;
+    // a solve right after removals from a converged state records its
+    // correction; with warm_start it starts from the previous one
+    const bool fromEvent = h->converged && h->removalsSinceSolve > 0;
+    const bool warm = fromEvent && h->histValid && o->warm_start == 1;
+    if (warm) launch_vcg_warm(m, vsys, h->vActive, 1.0f, h->stream);
+    else if (fromEvent) CK(cudaMemsetAsync(vsys.hist, 0, sizeof(float) * ((size_t)h->vCapacity + 1), h->stream));
+    h->converged = h->histValid = false;
+    h->removalsSinceSolve = 0;
     for (int outer = 0;; outer++) {
         CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
         launch_vcg_residual(m, vsys, h->vActive, h->acc.p, h->stream);
@@ -937,10 +955,12 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         }
         inf.inner += itV + itN;
         inf.inner_neumann += itN;
-        launch_vcg_apply(m, vsys, h->vActive, h->stream);
+        launch_vcg_apply(m, vsys, h->vActive, fromEvent, h->stream);
         launch_apply_correction(m, h->allN.p, h->countAllN, vN, h->stream);
     }
     h->selValid = false;
+    h->converged = true;
+    h->histValid = fromEvent;
     if (info) *info = inf;
     return TG_OK;
 }
@@ -1102,6 +1122,7 @@ int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached
     }
     h->bnormValid = false;
     h->selValid = false;
+    h->removalsSinceSolve++;
     return TG_OK;
 }
 

@@ -83,6 +83,7 @@ struct VSys {
     float* val;                   // coupling as the row sees it
     int32_t* vpos;                // [nnz] global CSR entry -> storage index, -1
     float *d, *x, *r, *u, *w, *p, *sv;
+    float* hist;                  // correction of the last event's solve (warm start)
     double* scal;                 // gamma, delta, alpha per iteration
     int32_t* count;               // next free slot (device counter)
     int capacity;
@@ -90,7 +91,10 @@ struct VSys {
 void launch_vcg_init(const VSys& v, int slots, cudaStream_t s);
 void launch_vcg_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s);
 void launch_vcg_update(const VSys& v, int slots, int it, double target, cudaStream_t s);
-void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, cudaStream_t s);
+// phi64 += x on the V rows; with record, hist += x as well
+void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s);
+// warm start: hist *= alpha, phi64 += hist on the V rows
+void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s);
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
                                cudaStream_t s);
 void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, cudaStream_t s);

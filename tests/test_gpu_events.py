@@ -55,3 +55,29 @@ def test_reference_mode_events_run(small_mesh):
         assert r["relax_iterations"] >= 1
     nodes = [r["node"] for r in ev.records]
     assert len(set(nodes)) == len(nodes)
+
+
+def test_warm_start_keeps_sequence_and_saves_iterations(ref_mesh, ref_events):
+    """warm_start 1 (previous event's correction as the start) ends at the
+    same tolerance, so the removed-atom sequence equals the plain solve's
+    and the reference's; it needs fewer iterations once it has a history."""
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
+    opts = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
+    runs = {}
+    for ws in (0, 1):
+        g = Grid(ref_mesh)
+        g.solve(rel_tol=1e-10)
+        ev = Evaporation(g, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, warm_start=ws))
+        runs[ws] = [ev.step() for _ in range(len(ref_events))]
+        g.close()
+    plain, warm = runs[0], runs[1]
+    for k, (p, w) in enumerate(zip(plain, warm)):
+        assert w["rel_residual"] <= 1e-10
+        if p["node"] != w["node"]:
+            assert ref_events[k][6] < NEAR_TIE, f"event {k + 1}"
+            break
+        assert np.allclose(w["fieldBefore"], p["fieldBefore"], rtol=1e-6, atol=0)
+    it_p = np.median([r["relax_iterations"] for r in plain[1:]])
+    it_w = np.median([r["relax_iterations"] for r in warm[1:]])
+    print("median iterations plain", it_p, "warm", it_w)
+    assert it_w < it_p
