@@ -159,6 +159,50 @@ __global__ void k_vertex_fields(DevMesh m) {
     out[2] = -(c02 * b0 + c12 * b1 + c22 * b2) * inv;
 }
 
+// Packed tetrahedron records, 128 bytes each: vertex 0 (3 floats) and the
+// six-fold volume (float), the gradients n1, n2, n3 of the barycentric
+// coordinates of vertices 1..3 (9 doubles: lambda_k(p) = n_k.(p - v0),
+// lambda_0 = 1 - lambda_1 - lambda_2 - lambda_3), the neighbours (4 ints)
+// and the vertex ids (4 ints).  A walk step then tests the four faces with
+// three dot products, and the same lambdas are the interpolation weights
+// |sub-volume| / volume of tetWeights (geometry_3d.cpp:916-980).  A flat
+// tetrahedron stores zero gradients and volume 0.
+constexpr int kTetWords = 32;
+__global__ void k_pack_tets(DevMesh m, float* pack) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.ntets) return;
+    float* o = pack + kTetWords * (size_t)t;
+    int v[4];
+    V3 P[4];
+    for (int k = 0; k < 4; k++) {
+        v[k] = m.tet_v[4 * t + k];
+        P[k] = ld3(m.xyz, v[k]);
+    }
+    const V3 e1{P[1].x - P[0].x, P[1].y - P[0].y, P[1].z - P[0].z};
+    const V3 e2{P[2].x - P[0].x, P[2].y - P[0].y, P[2].z - P[0].z};
+    const V3 e3{P[3].x - P[0].x, P[3].y - P[0].y, P[3].z - P[0].z};
+    const V3 c23{e2.y * e3.z - e2.z * e3.y, e2.z * e3.x - e2.x * e3.z, e2.x * e3.y - e2.y * e3.x};
+    const V3 c31{e3.y * e1.z - e3.z * e1.y, e3.z * e1.x - e3.x * e1.z, e3.x * e1.y - e3.y * e1.x};
+    const V3 c12{e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z, e1.x * e2.y - e1.y * e2.x};
+    const double vol6 = e1.x * c23.x + e1.y * c23.y + e1.z * c23.z;
+    const double inv = vol6 != 0.0 ? 1.0 / vol6 : 0.0;
+    o[0] = m.xyz[3 * v[0]];
+    o[1] = m.xyz[3 * v[0] + 1];
+    o[2] = m.xyz[3 * v[0] + 2];
+    o[3] = (float)vol6;
+    if (vol6 != 0.0 && o[3] == 0.0f) o[3] = 1e-38f;  // keep "not flat" when the float underflows
+    double* g = reinterpret_cast<double*>(o + 4);
+    g[0] = c23.x * inv; g[1] = c23.y * inv; g[2] = c23.z * inv;
+    g[3] = c31.x * inv; g[4] = c31.y * inv; g[5] = c31.z * inv;
+    g[6] = c12.x * inv; g[7] = c12.y * inv; g[8] = c12.z * inv;
+    int* oi = reinterpret_cast<int*>(o);
+    for (int k = 0; k < 4; k++) {
+        oi[22 + k] = m.tet_n[4 * t + k];
+        oi[26 + k] = v[k];
+    }
+    oi[30] = oi[31] = 0;
+}
+
 __device__ V3 vertex_field(const DevMesh& m, int i) {
     const V3 E{m.vfield[3 * i], m.vfield[3 * i + 1], m.vfield[3 * i + 2]};
     if (E.x != E.x) {
@@ -168,85 +212,165 @@ __device__ V3 vertex_field(const DevMesh& m, int i) {
     return E;
 }
 
-// The last two tetrahedra an ion touched, with vertex coordinates,
-// neighbours and vertex fields in registers: RK stages that stay inside
-// them need no memory traffic.
+// The last tetrahedron an ion touched, from its packed record, with the
+// vertex fields once interpolated from: RK stages that stay inside it need
+// no memory traffic.  A record comes in one round trip; the vertex
+// fields of the final tetrahedron of a walk take a second.  Every member is
+// addressed with compile-time indices so that the cache lives in registers.
 struct TetSlot {
     int t;
-    int nb[4];
-    V3 P[4];
-    V3 F[4];
+    int nb0, nb1, nb2, nb3;
+    int v0, v1, v2, v3;
+    V3 P0;
+    V3 G1, G2, G3;
+    float vol6;
+    V3 F0, F1, F2, F3;
+    bool hasF;
 };
+// `a` is the tetrahedron of the last lookup
 struct TetCache {
-    TetSlot s[2];
-    int last;
+    TetSlot a;
 };
+
+__device__ __forceinline__ int pick4(int k, int x0, int x1, int x2, int x3) {
+    return k == 0 ? x0 : (k == 1 ? x1 : (k == 2 ? x2 : x3));
+}
 
 __device__ void load_slot(const DevMesh& m, TetSlot& s, int t) {
+    const float4* p = reinterpret_cast<const float4*>(m.tetpack + kTetWords * (size_t)t);
+    const float4 q0 = __ldg(p);
+    const double2 g0 = __ldg(reinterpret_cast<const double2*>(p + 1));
+    const double2 g1 = __ldg(reinterpret_cast<const double2*>(p + 2));
+    const double2 g2 = __ldg(reinterpret_cast<const double2*>(p + 3));
+    const double2 g3 = __ldg(reinterpret_cast<const double2*>(p + 4));
+    const double2 g4 = __ldg(reinterpret_cast<const double2*>(p + 5));  // g[8], neighbours 0, 1
+    const int4 q6 = __ldg(reinterpret_cast<const int4*>(p + 6));       // neighbours 2, 3, vertices 0, 1
+    const int4 q7 = __ldg(reinterpret_cast<const int4*>(p + 7));       // vertices 2, 3, padding
     s.t = t;
-    int v[4];
-    for (int k = 0; k < 4; k++) {
-        v[k] = m.tet_v[4 * t + k];
-        s.nb[k] = m.tet_n[4 * t + k];
+    s.P0 = V3{q0.x, q0.y, q0.z};
+    s.vol6 = q0.w;
+    s.G1 = V3{g0.x, g0.y, g1.x};
+    s.G2 = V3{g1.y, g2.x, g2.y};
+    s.G3 = V3{g3.x, g3.y, g4.x};
+    const long long nb01 = __double_as_longlong(g4.y);
+    s.nb0 = (int)(unsigned)(nb01 & 0xffffffffll);
+    s.nb1 = (int)(unsigned)((unsigned long long)nb01 >> 32);
+    s.nb2 = q6.x;
+    s.nb3 = q6.y;
+    s.v0 = q6.z;
+    s.v1 = q6.w;
+    s.v2 = q7.x;
+    s.v3 = q7.y;
+    s.hasF = false;
+}
+
+// Barycentric coordinates of p in the slot's tetrahedron and bounds on their
+// rounding error (about a thousand ulps of the terms summed)
+struct Bary {
+    double l0, l1, l2, l3, e0, e1, e2, e3;
+};
+__device__ __forceinline__ Bary lambdas(const TetSlot& S, V3 p) {
+    const double dx = p.x - S.P0.x, dy = p.y - S.P0.y, dz = p.z - S.P0.z;
+    Bary b;
+    b.l1 = S.G1.x * dx + S.G1.y * dy + S.G1.z * dz;
+    b.l2 = S.G2.x * dx + S.G2.y * dy + S.G2.z * dz;
+    b.l3 = S.G3.x * dx + S.G3.y * dy + S.G3.z * dz;
+    const double a1 = fabs(S.G1.x * dx) + fabs(S.G1.y * dy) + fabs(S.G1.z * dz);
+    const double a2 = fabs(S.G2.x * dx) + fabs(S.G2.y * dy) + fabs(S.G2.z * dz);
+    const double a3 = fabs(S.G3.x * dx) + fabs(S.G3.y * dy) + fabs(S.G3.z * dz);
+    b.l0 = 1.0 - b.l1 - b.l2 - b.l3;
+    b.e1 = 1e-13 * a1;
+    b.e2 = 1e-13 * a2;
+    b.e3 = 1e-13 * a3;
+    b.e0 = 1e-13 * (1.0 + a1 + a2 + a3);
+    return b;
+}
+
+// Makes `a` hold tetrahedron t (loading it unless it is already there)
+__device__ __forceinline__ void cache_tet(const DevMesh& m, TetCache& c, int t) {
+    if (c.a.t == t) return;
+    load_slot(m, c.a, t);
+}
+
+// Side of face k (opposite vertex k) that p lies on: -1 beyond it.  The
+// barycentric coordinate decides unless it is within its rounding bound of
+// zero, or the tetrahedron is flat; then the exact predicate on the vertex
+// coordinates decides (as Predicates::orient3d does in the reference).
+__device__ __noinline__ int face_side_exact(const float* xyz, double snap, int i0, int i1, int i2, V3 p) {
+    return orient_sign(ld3(xyz, i0), ld3(xyz, i1), ld3(xyz, i2), p, snap);
+}
+__device__ __forceinline__ bool beyond(const DevMesh& m, const TetSlot& S, int k, V3 p, double lam, double err) {
+    if (S.vol6 != 0.0f) {
+        if (lam < -err) return true;
+        if (lam > err) return false;
     }
-    for (int k = 0; k < 4; k++) s.P[k] = ld3(m.xyz, v[k]);
-    for (int k = 0; k < 4; k++) s.F[k] = vertex_field(m, v[k]);
+    const int i0 = pick4(kFaceDev[k][0], S.v0, S.v1, S.v2, S.v3);
+    const int i1 = pick4(kFaceDev[k][1], S.v0, S.v1, S.v2, S.v3);
+    const int i2 = pick4(kFaceDev[k][2], S.v0, S.v1, S.v2, S.v3);
+    return face_side_exact(m.xyz, m.snap, i0, i1, i2, p) < 0;
 }
 
-__device__ int cache_slot(const DevMesh& m, TetCache& c, int t) {
-    if (c.s[c.last].t == t) return c.last;
-    if (c.s[c.last ^ 1].t == t) return c.last ^= 1;
-    c.last ^= 1;
-    load_slot(m, c.s[c.last], t);
-    return c.last;
-}
-
-// findTetrahedron through the cache; returns the slot holding p, -1 when p
-// is outside the mesh, -2 when the walk exceeded its bound
-__device__ int locate_cached(const DevMesh& m, TetCache& c, V3 p, int t, int limit, unsigned& rot) {
+// findTetrahedron through the cache: on return c.a holds p's tetrahedron
+// (result 0), or -1 when p is outside the mesh, -2 when the walk exceeded
+// its bound.  The faces are tested in an order rotating from walk step to
+// walk step; the walk leaves through the first face p lies beyond.
+__device__ __forceinline__ int locate_cached(const DevMesh& m, TetCache& c, V3 p, int t, int limit, unsigned& rot) {
     if (t < 0) return -1;
     for (int step = 0; step < limit; step++) {
-        const int sl = cache_slot(m, c, t);
-        const TetSlot& S = c.s[sl];
-        int next = -1;
+        cache_tet(m, c, t);
+        const TetSlot& S = c.a;
+        const Bary b = lambdas(S, p);
+        const int r = (int)(rot++ & 3u);
+        int next = 0;
         bool moved = false;
-        const unsigned r = rot++;
+#pragma unroll
         for (int j = 0; j < 4; j++) {
-            const int k = (int)((r + j) & 3);
-            if (orient_sign(S.P[kFaceDev[k][0]], S.P[kFaceDev[k][1]], S.P[kFaceDev[k][2]], p, m.snap) < 0) {
-                next = S.nb[k];
-                moved = true;
-                break;
+            const int k = (r + j) & 3;
+            if (!moved) {
+                const double lam = k == 0 ? b.l0 : (k == 1 ? b.l1 : (k == 2 ? b.l2 : b.l3));
+                const double err = k == 0 ? b.e0 : (k == 1 ? b.e1 : (k == 2 ? b.e2 : b.e3));
+                if (beyond(m, S, k, p, lam, err)) {
+                    next = pick4(k, S.nb0, S.nb1, S.nb2, S.nb3);
+                    moved = true;
+                }
             }
         }
-        if (!moved) return sl;
+        if (!moved) return 0;
         if (next < 0) return -1;
         t = next;
     }
     return -2;
 }
 
-__device__ bool fast_field(const DevMesh& m, TetCache& c, V3 p, int guess, int limit, unsigned& rot, V3* E) {
+// Field at p: walk from `guess`, interpolate the vertex fields with the
+// weights |lambda_k| (1/4 each in a flat tetrahedron).  *located is the
+// tetrahedron holding p (unchanged when p is outside the mesh).
+__device__ __forceinline__ bool fast_field(const DevMesh& m, TetCache& c, V3 p, int guess, int limit, unsigned& rot, V3* E,
+                           int* located) {
     *E = V3{0, 0, 0};
     const int sl = locate_cached(m, c, p, guess, limit, rot);
     if (sl == -2) return false;
     if (sl < 0) return true;
-    const TetSlot& S = c.s[sl];
-    const double vol = fabs(orient(S.P[0], S.P[1], S.P[2], S.P[3]));
-    double w[4];
-    if (vol == 0.0) {
-        w[0] = w[1] = w[2] = w[3] = 0.25;
-    } else {
-        w[0] = fabs(orient(p, S.P[1], S.P[2], S.P[3])) / vol;
-        w[1] = fabs(orient(S.P[0], p, S.P[2], S.P[3])) / vol;
-        w[2] = fabs(orient(S.P[0], S.P[1], p, S.P[3])) / vol;
-        w[3] = fabs(orient(S.P[0], S.P[1], S.P[2], p)) / vol;
+    TetSlot& S = c.a;
+    *located = S.t;
+    if (!S.hasF) {
+        S.F0 = vertex_field(m, S.v0);
+        S.F1 = vertex_field(m, S.v1);
+        S.F2 = vertex_field(m, S.v2);
+        S.F3 = vertex_field(m, S.v3);
+        S.hasF = true;
     }
-    for (int k = 0; k < 4; k++) {
-        E->x += w[k] * S.F[k].x;
-        E->y += w[k] * S.F[k].y;
-        E->z += w[k] * S.F[k].z;
+    double w0 = 0.25, w1 = 0.25, w2 = 0.25, w3 = 0.25;
+    if (S.vol6 != 0.0f) {
+        const Bary b = lambdas(S, p);
+        w0 = fabs(b.l0);
+        w1 = fabs(b.l1);
+        w2 = fabs(b.l2);
+        w3 = fabs(b.l3);
     }
+    E->x = w0 * S.F0.x + w1 * S.F1.x + w2 * S.F2.x + w3 * S.F3.x;
+    E->y = w0 * S.F0.y + w1 * S.F1.y + w2 * S.F2.y + w3 * S.F3.y;
+    E->z = w0 * S.F0.z + w1 * S.F1.z + w2 * S.F2.z + w3 * S.F3.z;
     return true;
 }
 
@@ -261,21 +385,22 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
                         const int32_t* guess, TraceParams tp, ImpactOut* out) {
     const int ion = blockIdx.x * blockDim.x + threadIdx.x;
     if (ion >= nIons) return;
-    // Cash-Karp tableau
-    const double B[6][5] = {{0, 0, 0, 0, 0},
-                            {1.0 / 5.0, 0, 0, 0, 0},
-                            {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
-                            {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0, 0, 0},
-                            {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0, 0},
-                            {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
-    const double C5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
-    const double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
+    // Cash-Karp tableau; the stage loops are unrolled so that every index is
+    // a compile-time constant and the stage vectors stay in registers
+    constexpr double B[6][5] = {{0, 0, 0, 0, 0},
+                                {1.0 / 5.0, 0, 0, 0, 0},
+                                {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
+                                {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0, 0, 0},
+                                {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0, 0},
+                                {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+    constexpr double C5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
+    constexpr double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
 
     ImpactOut res;
     unsigned rot = (unsigned)ion * 7u;
     TetCache fc;
-    fc.s[0].t = fc.s[1].t = -1;
-    fc.last = 0;
+    fc.a.t = -1;
+    fc.a.hasF = false;
     V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
     V3 v{0, 0, 0};
     if (vel) v = V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]};
@@ -295,7 +420,8 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
         return;
     }
     V3 E0;
-    if (!fast_field(m, fc, x, tet, tp.walk_limit, rot, &E0)) atomicOr(m.status, S_WALK_LIMIT);
+    int cur = tet;  // tetrahedron of the last located point: the next walk starts there
+    if (!fast_field(m, fc, x, tet, tp.walk_limit, rot, &E0, &cur)) atomicOr(m.status, S_WALK_LIMIT);
     int status;
     if (E0.x == 0.0 && E0.y == 0.0 && E0.z == 0.0) {
         status = 1;  // NO_FIELD
@@ -311,20 +437,23 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
                 used = dt;
                 V3 dxs[6], dvs[6];
                 bool walkOk = true;
+#pragma unroll
                 for (int s = 0; s < 6; s++) {
                     V3 ps = x, vs = v;
+#pragma unroll
                     for (int j = 0; j < s; j++) {
                         ps.x += B[s][j] * dxs[j].x; ps.y += B[s][j] * dxs[j].y; ps.z += B[s][j] * dxs[j].z;
                         vs.x += B[s][j] * dvs[j].x; vs.y += B[s][j] * dvs[j].y; vs.z += B[s][j] * dvs[j].z;
                     }
                     V3 E;
-                    walkOk &= fast_field(m, fc, ps, tet, tp.walk_limit, rot, &E);
+                    walkOk &= fast_field(m, fc, ps, cur, tp.walk_limit, rot, &E, &cur);
                     dvs[s] = V3{E.x * k * dt, E.y * k * dt, E.z * k * dt};
                     dxs[s] = V3{vs.x * dt, vs.y * dt, vs.z * dt};
                 }
                 if (!walkOk) atomicOr(m.status, S_WALK_LIMIT);
                 nx = x; nv = v;
                 V3 ex{0, 0, 0}, evv{0, 0, 0};
+#pragma unroll
                 for (int s = 0; s < 6; s++) {
                     nx.x += C5[s] * dxs[s].x; nx.y += C5[s] * dxs[s].y; nx.z += C5[s] * dxs[s].z;
                     nv.x += C5[s] * dvs[s].x; nv.y += C5[s] * dvs[s].y; nv.z += C5[s] * dvs[s].z;
@@ -333,10 +462,12 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
                     evv.x += dc * dvs[s].x; evv.y += dc * dvs[s].y; evv.z += dc * dvs[s].z;
                 }
                 double rel = 0.0;
-                const double pv[6] = {nx.x, nx.y, nx.z, nv.x, nv.y, nv.z};
-                const double ev[6] = {ex.x, ex.y, ex.z, evv.x, evv.y, evv.z};
-                for (int c = 0; c < 6; c++)
-                    if (pv[c] != 0.0) rel = fmax(rel, fabs(ev[c] / pv[c]));
+                if (nx.x != 0.0) rel = fmax(rel, fabs(ex.x / nx.x));
+                if (nx.y != 0.0) rel = fmax(rel, fabs(ex.y / nx.y));
+                if (nx.z != 0.0) rel = fmax(rel, fabs(ex.z / nx.z));
+                if (nv.x != 0.0) rel = fmax(rel, fabs(evv.x / nv.x));
+                if (nv.y != 0.0) rel = fmax(rel, fabs(evv.y / nv.y));
+                if (nv.z != 0.0) rel = fmax(rel, fabs(evv.z / nv.z));
                 if (rel < tp.tol || dt == tp.dt_min) {
                     if (rel != 0.0) {
                         const double tmp = dt * pow(tp.tol / rel, 0.25) * 0.9;
@@ -352,8 +483,8 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
                 status = 2;  // STEPPER_LIMIT_PASSED
                 break;
             }
-            const int nsl = locate_cached(m, fc, nx, tet, tp.walk_limit, rot);
-            const int nt = nsl >= 0 ? fc.s[nsl].t : nsl;
+            const int nsl = locate_cached(m, fc, nx, cur, tp.walk_limit, rot);
+            const int nt = nsl >= 0 ? fc.a.t : nsl;
             if (nt == -2) atomicOr(m.status, S_WALK_LIMIT);
             res.steps++;
             if (nt < 0) {
@@ -371,6 +502,7 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
             v = nv;
             time += used;
             tet = nt;
+            cur = nt;
         }
     }
     if (tet >= 0) {
@@ -405,6 +537,9 @@ __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s) {
     if (nIons > 0) { count_launch(); k_trace<<<(nIons + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); }
+}
+void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s) {
+    if (m.ntets > 0) { count_launch(); k_pack_tets<<<(m.ntets + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, pack); }
 }
 void launch_vertex_fields(const DevMesh& m, cudaStream_t s) {
     if (m.n > 0) {

@@ -101,6 +101,7 @@ struct tg_handle {
     DBuf<float> vVal, vVec;  // vVec: d, x, r, u, w, p, sv, hist, each capacity+1
     DBuf<double> vScal;
     DBuf<double> vfield;     // vertex fields of the current flight call
+    DBuf<float> tetpack;     // packed tetrahedra for the flights
     int vCapacity = 0;       // slots incl. the append reserve
     int vActive = 0;         // slots in use (host mirror of vCount)
     double vEntries = 0.0;   // stored (non-padding) couplings
@@ -170,6 +171,7 @@ struct tg_handle {
         m.status = status.p;
         m.snap = snap;
         m.vfield = vfield.p;
+        m.tetpack = tetpack.p;
         return m;
     }
     RowLists rl() {
@@ -334,6 +336,23 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
         }
         h->types[t.id] = t;
     }
+    // every index the device walks and gathers through must stay inside its
+    // array: vertices in [0, N), neighbours and node_tet in [-1, T)
+    if (d->num_tets < 0 || (d->num_tets > 0 && (!d->tet_v || !d->tet_n))) {
+        delete h;
+        return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: tetrahedra arrays missing");
+    }
+    for (size_t k = 0; k < 4 * (size_t)d->num_tets; k++)
+        if (d->tet_v[k] < 0 || d->tet_v[k] >= n || d->tet_n[k] < -1 || d->tet_n[k] >= d->num_tets) {
+            delete h;
+            return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: tetrahedron vertex or neighbour index out of range");
+        }
+    if (d->node_tet && d->num_tets > 0)
+        for (int i = 0; i < n; i++)
+            if (d->node_tet[i] < -1 || d->node_tet[i] >= d->num_tets) {
+                delete h;
+                return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: node_tet index out of range");
+            }
     std::vector<DType> dt(128);
     for (int k = 0; k < 128; k++) {
         const tg_type& t = h->types[k];
@@ -588,12 +607,14 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(h->vVec.alloc(8 * ((size_t)h->vCapacity + 1)));
     if (e == cudaSuccess) chk(cudaMemset(h->vVec.p, 0, 8 * ((size_t)h->vCapacity + 1) * sizeof(float)));
     if (e == cudaSuccess) chk(cudaMemcpy(h->vVec.p, vD.data(), vD.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (h->ntets > 0) chk(h->tetpack.alloc(32 * (size_t)h->ntets));
     if (e != cudaSuccess) {
         const std::string msg = std::string("tg_create: ") + cudaGetErrorString(e);
         tg_destroy(h);
         return fail(nullptr, TG_ERR_CUDA, msg);
     }
     launch_rebuild_rows(h->dm(), h->stream);
+    if (h->ntets > 0) launch_pack_tets(h->dm(), h->tetpack.p, h->stream);
     const int rc = sync_status(h, "tg_create");
     if (rc != TG_OK) {
         const std::string msg = h->err;
@@ -620,7 +641,7 @@ void tg_destroy(tg_handle* h) {
     h->stageImpact.release();
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
-    h->vScal.release(); h->vfield.release();
+    h->vScal.release(); h->vfield.release(); h->tetpack.release();
     if (h->evStart) cudaEventDestroy(h->evStart);
     if (h->evStop) cudaEventDestroy(h->evStop);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1273,7 +1294,7 @@ int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_ev
         const float charge = (float)removed.evap_charge * 1.60217733e-19f;
         const float mass = removed.mass * 1.660538782e-27f;
         const float qm = charge / mass;
-        const int32_t guess = h->h_node_tet.empty() ? 0 : h->h_node_tet[node];
+        const int32_t guess = h->h_node_tet.empty() ? 0 : std::max(0, h->h_node_tet[node]);
         rc = tg_trace(h, 1, start, nullptr, &qm, &guess, &o->trace, &rec->impact);
         if (rc != TG_OK) return rc;
     }

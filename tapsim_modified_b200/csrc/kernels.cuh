@@ -47,6 +47,7 @@ struct DevMesh {
     int* status;
     double snap;   // power-of-two scale to the integer grid of the exact predicates
     double* vfield;  // [3n] vertex fields of the current flight call
+    const float* tetpack;  // [32 ntets] packed tetrahedra (flight.cu)
 };
 
 // Free-row bookkeeping kept on the device so that removals can append rows
@@ -160,6 +161,8 @@ struct ImpactOut {
     int32_t steps;
     int32_t status;
 };
+// packed tetrahedron records (32 words each) from tet_v, tet_n and xyz
+void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s);
 // field_o1 of every node from the current potentials into m.vfield
 void launch_vertex_fields(const DevMesh& m, cudaStream_t s);
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
