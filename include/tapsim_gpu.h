@@ -255,6 +255,14 @@ typedef struct {
     int32_t relax_status;
 } tg_event_record;
 int tg_run_event(tg_handle* h, const tg_event_opts* opts, int32_t event_index, tg_event_record* rec);
+/* `count` events in one call (indices first_index, first_index+1, ...):
+ * the same steps and records as tg_run_event, with each event's ion flight
+ * on a second stream overlapping the next event's removal and relaxation
+ * (the flight reads snapshots of the vertex fields and potentials taken
+ * after its own event's relaxation).  *done = events completed; on an error
+ * the records before it are complete. */
+int tg_run_events(tg_handle* h, const tg_event_opts* opts, int32_t first_index, int32_t count,
+                  tg_event_record* recs, int32_t* done);
 
 /* ---- measurement (no counterpart in the reference) ---------------------- */
 /* CUDA events on the handle's stream around a region of calls. */

@@ -106,7 +106,9 @@ __device__ void weights(const DevMesh& m, int t, V3 p, double w[4]) {
 }
 
 // Vertex fields of one flight call: every node's field_o1 is computed once,
-// in bulk, from the current potentials before the flights start (the
+// in bulk, from the current potentials before the flights start, and the
+// potentials are copied beside them (the flights read only these two
+// snapshots, so a flight may overlap the next event's relaxation) (the
 // FastField buffer of the reference, grid_3d.cpp:1672-1702, filled for all
 // vertices at once instead of on first use).  Four lanes share a row; a
 // singular node stores NaN in x, which the flight reports as S_SINGULAR when
@@ -140,6 +142,7 @@ __global__ void k_vertex_fields(DevMesh m) {
         b2 += __shfl_xor_sync(0xffffffffu, b2, o);
     }
     if (!live || lane != 0) return;
+    m.phiTrace[i] = pi;
     double* out = m.vfield + 3 * (size_t)i;
     if (hull) {
         out[0] = out[1] = out[2] = 0.0;
@@ -374,17 +377,16 @@ __device__ __forceinline__ bool fast_field(const DevMesh& m, TetCache& c, V3 p, 
     return true;
 }
 
-__device__ double potential_at(const DevMesh& m, V3 p, int t) {
+__device__ double potential_at(const DevMesh& m, const double* phi, V3 p, int t) {
     const int* v = m.tet_v + 4 * t;
     double w[4];
     weights(m, t, p, w);
-    return w[0] * m.phi64[v[0]] + w[1] * m.phi64[v[1]] + w[2] * m.phi64[v[2]] + w[3] * m.phi64[v[3]];
+    return w[0] * phi[v[0]] + w[1] * phi[v[1]] + w[2] * phi[v[2]] + w[3] * phi[v[3]];
 }
 
-__global__ void k_trace(DevMesh m, int nIons, const float* start, const float* vel, const float* qm,
-                        const int32_t* guess, TraceParams tp, ImpactOut* out) {
-    const int ion = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ion >= nIons) return;
+// One ion from x0 (velocity v0, charge/mass k) into *out.
+__device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k, int guessTet, const TraceParams& tp,
+                                          unsigned rot, ImpactOut* out) {
     // Cash-Karp tableau; the stage loops are unrolled so that every index is
     // a compile-time constant and the stage vectors stay in registers
     constexpr double B[6][5] = {{0, 0, 0, 0, 0},
@@ -397,16 +399,11 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
     constexpr double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
 
     ImpactOut res;
-    unsigned rot = (unsigned)ion * 7u;
     TetCache fc;
     fc.a.t = -1;
     fc.a.hasF = false;
-    V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
-    V3 v{0, 0, 0};
-    if (vel) v = V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]};
-    const double k = qm[ion];
     double time = 0.0;
-    int tet = locate(m, x, guess ? guess[ion] : 0, tp.walk_limit, rot);
+    int tet = locate(m, x, guessTet, tp.walk_limit, rot);
     res.steps = 0;
     res.last_tet = tet;
     res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
@@ -416,7 +413,7 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
         res.status = -1;  // Trajectory_3d::init: initial point is outside
         res.stop[0] = (float)x.x; res.stop[1] = (float)x.y; res.stop[2] = (float)x.z;
         res.stop_time = 0.0f;
-        out[ion] = res;
+        *out = res;
         return;
     }
     V3 E0;
@@ -509,9 +506,10 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
         res.last_tet = tet;
         res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
     }
-    res.last_phi = res.last_tet >= 0
-                       ? (float)potential_at(m, V3{res.last_pos[0], res.last_pos[1], res.last_pos[2]}, res.last_tet)
-                       : 0.0f;
+    res.last_phi = res.last_tet >= 0 ? (float)potential_at(m, m.phiTrace, V3{res.last_pos[0], res.last_pos[1],
+                                                                              res.last_pos[2]},
+                                                           res.last_tet)
+                                     : 0.0f;
     // extrapolate to the top plane along the last velocity
     const double dtz = (tp.top_z - x.z) / v.z;
     res.stop[0] = (float)(x.x + dtz * v.x);
@@ -519,7 +517,23 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
     res.stop[2] = (float)(x.z + dtz * v.z);
     res.stop_time = (float)(time + dtz);
     res.status = status;
-    out[ion] = res;
+    *out = res;
+}
+
+__global__ void k_trace(DevMesh m, int nIons, const float* start, const float* vel, const float* qm,
+                        const int32_t* guess, TraceParams tp, ImpactOut* out) {
+    const int ion = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ion >= nIons) return;
+    const V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
+    const V3 v = vel ? V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]} : V3{0, 0, 0};
+    trace_ion(m, x, v, qm[ion], guess ? guess[ion] : 0, tp, (unsigned)ion * 7u, out + ion);
+}
+
+// A single ion from rest, its start passed by value (no staging copy)
+__global__ void k_trace_one(DevMesh m, float x, float y, float z, float qm, int guess, TraceParams tp,
+                            ImpactOut* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    trace_ion(m, V3{x, y, z}, V3{0, 0, 0}, qm, guess, tp, 0u, out);
 }
 
 __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t* guess, int limit, float* out) {
@@ -529,7 +543,7 @@ __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t
     const V3 p{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
     const int t = locate(m, p, guess ? guess[i] : 0, limit, rot);
     if (t == -2) atomicOr(m.status, S_WALK_LIMIT);
-    out[i] = t >= 0 ? (float)potential_at(m, p, t) : 0.0f;
+    out[i] = t >= 0 ? (float)potential_at(m, m.phi64, p, t) : 0.0f;
 }
 
 }  // namespace
@@ -547,6 +561,11 @@ void launch_vertex_fields(const DevMesh& m, cudaStream_t s) {
         const long long threads = (long long)m.n * kLanesPerRow;
         k_vertex_fields<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m);
     }
+}
+void launch_trace_one(const DevMesh& m, const float start[3], float qm, int guess, TraceParams tp, ImpactOut* out,
+                      cudaStream_t s) {
+    count_launch();
+    k_trace_one<<<1, 32, 0, s>>>(m, start[0], start[1], start[2], qm, guess, tp, out);
 }
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit, float* out,
                          cudaStream_t s) {

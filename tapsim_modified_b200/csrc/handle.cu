@@ -94,6 +94,12 @@ struct tg_handle {
     DBuf<ImpactOut> stageImpact;
 
     cudaEvent_t evStart = nullptr, evStop = nullptr;
+    // flights of tg_run_events run on their own stream, overlapping the next
+    // event's relaxation; they read only the vfield/phiTrace snapshots
+    cudaStream_t traceStream = nullptr;
+    cudaEvent_t evFields = nullptr, evTraceDone = nullptr;
+    DBuf<int> statusTrace;
+    DBuf<double> phiTrace;
     std::vector<int32_t> h_row_ptr;
 
     // non-Neumann free rows in slot order, SELL-32 (cg.cu)
@@ -171,6 +177,7 @@ struct tg_handle {
         m.status = status.p;
         m.snap = snap;
         m.vfield = vfield.p;
+        m.phiTrace = phiTrace.p;
         m.tetpack = tetpack.p;
         return m;
     }
@@ -229,6 +236,8 @@ int cuda_check(tg_handle* h, cudaError_t e, const char* where) {
     } while (0)
 
 // Synchronises the stream and maps the device status word to a code.
+int status_code(tg_handle* h, int st, const char* where);
+
 int sync_status(tg_handle* h, const char* where) {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
@@ -236,6 +245,11 @@ int sync_status(tg_handle* h, const char* where) {
     CK(cudaMemcpy(&st, h->status.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (st == 0) return TG_OK;
     CK(cudaMemset(h->status.p, 0, sizeof(int)));
+    return status_code(h, st, where);
+}
+
+// Maps a device status word to a code and message.
+int status_code(tg_handle* h, int st, const char* where) {
     std::string what = where;
     if (st & S_NAN) return fail(h, TG_ERR_NAN, what + ": NaN");
     if (st & S_SINGULAR) return fail(h, TG_ERR_SINGULAR, what + ": singular field_o1 system");
@@ -545,6 +559,9 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     chk(cudaEventCreate(&h->evStart));
     chk(cudaEventCreate(&h->evStop));
+    chk(cudaStreamCreateWithFlags(&h->traceStream, cudaStreamNonBlocking));
+    chk(cudaEventCreateWithFlags(&h->evFields, cudaEventDisableTiming));
+    chk(cudaEventCreateWithFlags(&h->evTraceDone, cudaEventDisableTiming));
     chk(up(h->xyz, d->xyz, 3 * (size_t)n));
     chk(up(h->type, d->type_id, n));
     chk(h->typeScratch.alloc(n));
@@ -593,6 +610,9 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(h->localCount.alloc(66));
     chk(h->localScratch.alloc(1 << 16));
     chk(h->vfield.alloc(3 * (size_t)n));
+    chk(h->phiTrace.alloc(n));
+    chk(h->statusTrace.alloc(1));
+    if (e == cudaSuccess) chk(cudaMemset(h->statusTrace.p, 0, sizeof(int)));
     chk(up(h->vSlotOf, vSlotOf.data(), n));
     chk(up(h->vNodeOf, vNodeOf.data(), h->vCapacity));
     chk(up(h->vSliceStart, sliceStart.data(), nSlices + 1));
@@ -642,6 +662,11 @@ void tg_destroy(tg_handle* h) {
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
+    if (h->traceStream) cudaStreamSynchronize(h->traceStream);
+    h->phiTrace.release(); h->statusTrace.release();
+    if (h->evFields) cudaEventDestroy(h->evFields);
+    if (h->evTraceDone) cudaEventDestroy(h->evTraceDone);
+    if (h->traceStream) cudaStreamDestroy(h->traceStream);
     if (h->evStart) cudaEventDestroy(h->evStart);
     if (h->evStop) cudaEventDestroy(h->evStop);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1153,6 +1178,18 @@ int tg_update_coordination(tg_handle* h) {
     return sync_status(h, "tg_update_coordination");
 }
 
+static TraceParams trace_params(const tg_handle* h, const tg_trace_opts* o) {
+    TraceParams tp;
+    tp.dt0 = o->time_step;
+    tp.dt_min = o->min_time_step;
+    tp.tol = o->error_threshold;
+    tp.max_steps = o->max_steps;
+    tp.stepper_limit = o->stepper_limit;
+    tp.walk_limit = o->walk_limit;
+    tp.top_z = h->top_z;
+    return tp;
+}
+
 int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
              const int32_t* guess, const tg_trace_opts* o, tg_impact* out) {
     if (!h || nIons < 0 || (nIons && (!start || !qm || !out)) || !o) return fail(h, TG_ERR_ARGUMENT, "tg_trace: bad argument");
@@ -1174,14 +1211,7 @@ int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, 
     CK(cudaMemcpyAsync(dQm, qm, sizeof(float) * nIons, cudaMemcpyHostToDevice, h->stream));
     if (guess) CK(cudaMemcpyAsync(h->stageI.p, guess, sizeof(int32_t) * nIons, cudaMemcpyHostToDevice, h->stream));
     else CK(cudaMemsetAsync(h->stageI.p, 0, sizeof(int32_t) * nIons, h->stream));
-    TraceParams tp;
-    tp.dt0 = o->time_step;
-    tp.dt_min = o->min_time_step;
-    tp.tol = o->error_threshold;
-    tp.max_steps = o->max_steps;
-    tp.stepper_limit = o->stepper_limit;
-    tp.walk_limit = o->walk_limit;
-    tp.top_z = h->top_z;
+    const TraceParams tp = trace_params(h, o);
     launch_vertex_fields(h->dm(), h->stream);  // once per call, from the current potentials
     launch_trace(h->dm(), nIons, dStart, vel ? dVel : nullptr, dQm, h->stageI.p, tp, h->stageImpact.p, h->stream);
     CK(cudaMemcpyAsync(out, h->stageImpact.p, sizeof(tg_impact) * nIons, cudaMemcpyDeviceToHost, h->stream));
@@ -1207,8 +1237,11 @@ int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* gu
     return sync_status(h, "tg_potential_at");
 }
 
-int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec) {
-    if (!h || !o || !rec) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: null argument");
+// Steps I-VI of one event.  With asyncImpact (a device slot) the flight of
+// step V is queued on the trace stream and its impact left there; without,
+// it runs through tg_trace and lands in rec->impact.
+static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec,
+                     ImpactOut* asyncImpact) {
     if (h->vacuumId != o->vacuum_id) {
         int32_t ns;
         int rc = tg_surface_init(h, o->vacuum_id, &ns);
@@ -1295,8 +1328,23 @@ int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_ev
         const float mass = removed.mass * 1.660538782e-27f;
         const float qm = charge / mass;
         const int32_t guess = h->h_node_tet.empty() ? 0 : std::max(0, h->h_node_tet[node]);
-        rc = tg_trace(h, 1, start, nullptr, &qm, &guess, &o->trace, &rec->impact);
-        if (rc != TG_OK) return rc;
+        if (asyncImpact) {
+            if (guess >= h->ntets || !h->tetpack.p) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: no tetrahedra");
+            // the previous flight must be done with the snapshots before the
+            // vertex fields of this event overwrite them
+            CK(cudaStreamWaitEvent(h->stream, h->evTraceDone, 0));
+            launch_vertex_fields(h->dm(), h->stream);
+            CK(cudaEventRecord(h->evFields, h->stream));
+            CK(cudaStreamWaitEvent(h->traceStream, h->evFields, 0));
+            DevMesh mt = h->dm();
+            mt.status = h->statusTrace.p;
+            launch_trace_one(mt, start, qm, guess, trace_params(h, &o->trace), asyncImpact, h->traceStream);
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(h->evTraceDone, h->traceStream));
+        } else {
+            rc = tg_trace(h, 1, start, nullptr, &qm, &guess, &o->trace, &rec->impact);
+            if (rc != TG_OK) return rc;
+        }
     }
     {
         double phi = 0.0, E[3];
@@ -1307,6 +1355,41 @@ int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_ev
         for (int k = 0; k < 3; k++) rec->field_after[k] = (float)E[k];
     }
     return TG_OK;
+}
+
+int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec) {
+    if (!h || !o || !rec) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: null argument");
+    return run_event(h, o, eventIndex, rec, nullptr);
+}
+
+int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int32_t count, tg_event_record* recs,
+                  int32_t* done) {
+    if (!h || !o || count < 0 || (count && !recs)) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: bad argument");
+    if (done) *done = 0;
+    int rc = stage(h, h->stageImpact, std::max(count, 1));
+    if (rc != TG_OK) return rc;
+    CK(cudaMemsetAsync(h->statusTrace.p, 0, sizeof(int), h->stream));
+    int k = 0;
+    for (; k < count; k++) {
+        rc = run_event(h, o, firstIndex + k, &recs[k], h->stageImpact.p + k);
+        if (rc != TG_OK) break;
+    }
+    // every flight queued so far completes before the impacts are read
+    CK(cudaStreamSynchronize(h->traceStream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (o->trace_enabled && k > 0) {
+        std::vector<ImpactOut> imp(k);
+        CK(cudaMemcpy(imp.data(), h->stageImpact.p, sizeof(ImpactOut) * k, cudaMemcpyDeviceToHost));
+        for (int j = 0; j < k; j++) std::memcpy(&recs[j].impact, &imp[j], sizeof(tg_impact));
+        int st = 0;
+        CK(cudaMemcpy(&st, h->statusTrace.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st != 0) {
+            CK(cudaMemset(h->statusTrace.p, 0, sizeof(int)));
+            if (rc == TG_OK) rc = status_code(h, st, "tg_run_events flights");
+        }
+    }
+    if (done) *done = k;
+    return rc;
 }
 
 }  // extern "C"

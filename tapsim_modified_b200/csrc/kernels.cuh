@@ -46,7 +46,8 @@ struct DevMesh {
     const DType* types;
     int* status;
     double snap;   // power-of-two scale to the integer grid of the exact predicates
-    double* vfield;  // [3n] vertex fields of the current flight call
+    double* vfield;    // [3n] vertex fields of the current flight call
+    double* phiTrace;  // [n] potentials of the current flight call
     const float* tetpack;  // [32 ntets] packed tetrahedra (flight.cu)
 };
 
@@ -167,6 +168,9 @@ void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s);
 void launch_vertex_fields(const DevMesh& m, cudaStream_t s);
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s);
+// one ion from rest at start (values passed to the kernel)
+void launch_trace_one(const DevMesh& m, const float start[3], float qm, int guess, TraceParams tp, ImpactOut* out,
+                      cudaStream_t s);
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit,
                          float* out, cudaStream_t s);
 

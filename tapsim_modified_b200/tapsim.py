@@ -271,6 +271,16 @@ class Grid:
         self._ck(N.lib().tg_run_event(self._h, C.byref(opts), event_index, C.byref(rec)))
         return rec
 
+    def run_events(self, opts: N.tg_event_opts, first_index: int, count: int) -> list:
+        """`count` events in one call, flights overlapping the next event's
+        relaxation (tg_run_events); returns the records."""
+        recs = (N.tg_event_record * count)()
+        done = C.c_int32()
+        rc = N.lib().tg_run_events(self._h, C.byref(opts), first_index, count, C.cast(recs, C.c_void_p),
+                                   C.byref(done))
+        self._ck(rc)
+        return list(recs)[:done.value]
+
 
 # ---- tapsim.ini -----------------------------------------------------------
 
@@ -399,6 +409,18 @@ class Evaporation:
         r = self._record(rec)
         self.records.append(r)
         return r
+
+    def run(self, count: int) -> list[dict]:
+        """`count` events in one library call: each ion flight overlaps the
+        next event's removal and relaxation.  Same records as `step`."""
+        recs = self.grid.run_events(self.opts, self.event + 1, count)
+        out = []
+        for rec in recs:
+            self.event += 1
+            r = self._record(rec)
+            self.records.append(r)
+            out.append(r)
+        return out
 
     def _record(self, rec: N.tg_event_record) -> dict:
         """Step VI: voltage queue and time-of-flight scale (process.cpp:985-1036)."""

@@ -81,3 +81,27 @@ def test_warm_start_keeps_sequence_and_saves_iterations(ref_mesh, ref_events):
     it_w = np.median([r["relax_iterations"] for r in warm[1:]])
     print("median iterations plain", it_p, "warm", it_w)
     assert it_w < it_p
+
+
+def test_batched_events_match_single_events(ref_mesh):
+    """tg_run_events (flights overlapping the next event's relaxation on a
+    second stream) returns the records tg_run_event returns one by one."""
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
+    opts = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
+    out = {}
+    for batched in (False, True):
+        g = Grid(ref_mesh)
+        g.solve(rel_tol=1e-10)
+        ev = Evaporation(g, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, warm_start=1))
+        if batched:
+            out[batched] = ev.run(7) + ev.run(8)
+        else:
+            out[batched] = [ev.step() for _ in range(15)]
+        g.close()
+    for a, b in zip(out[False], out[True]):
+        assert a["node"] == b["node"]
+        assert a["status"] == b["status"] == 5
+        sa, sb = np.array(a["stop"]), np.array(b["stop"])
+        assert np.linalg.norm(sa - sb) <= 1e-5 * np.linalg.norm(sa)
+        assert abs(a["tof"] - b["tof"]) <= 1e-5 * abs(a["tof"])
+        assert abs(a["voltage"] - b["voltage"]) <= 1e-5 * abs(a["voltage"])
