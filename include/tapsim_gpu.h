@@ -33,7 +33,8 @@ enum {
     TG_ERR_WALK_LIMIT = 9,      /* tetrahedron walk exceeded its step bound */
     TG_ERR_NO_SURFACE = 10,     /* surface set is empty */
     TG_ERR_HOST = 11,           /* host-side failure (file, mesh build) */
-    TG_ERR_UNKNOWN_TYPE = 12    /* cell type id not in the type table */
+    TG_ERR_UNKNOWN_TYPE = 12,   /* cell type id not in the type table */
+    TG_ERR_TIMEOUT = 13         /* a bounded wait inside a kernel ran out */
 };
 
 /* Trajectory status, values of Trajectory_3d's enum (trajectory_3d.h:89). */
@@ -277,6 +278,11 @@ int64_t tg_launch_count(const tg_handle* h);
  * neighbour-index streams, one compulsory read of every gathered vector
  * entry, the row outputs). */
 int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, double* algorithmic_bytes);
+/* The tensor-core GEMM of the learned warm start on host arrays (a check
+ * hook; no counterpart in the reference): C[M x N] (FP32) = A[M x K] *
+ * B[N x K]^T with A, B BF16 bit patterns, row-major; M % 128 == 0,
+ * N in {64, 128}, K % 64 == 0. */
+int tg_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, int32_t M, int32_t N, int32_t K);
 
 /* ---- host-side mesh building (setup, not device work) ------------------ */
 typedef struct tg_mesh tg_mesh;

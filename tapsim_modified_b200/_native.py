@@ -122,6 +122,7 @@ SIGNATURES = {
     "tg_timer_stop": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "tg_launch_count": (C.c_int64, [_P]),
     "tg_bench_kernel": (C.c_int, [_P, _I, _I, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
+    "tg_gemm_bf16": (C.c_int, [_P, _P, _P, _I, _I, _I]),
     "tg_tip_params_default": (None, [C.POINTER(tg_tip_params)]),
     "tg_mesh_from_tip": (C.c_int, [C.POINTER(tg_tip_params), _I, C.POINTER(_P)]),
     "tg_mesh_from_files": (C.c_int, [C.c_char_p, C.c_char_p, _I, C.POINTER(_P)]),

@@ -23,7 +23,8 @@ enum : int {
     S_WALK_LIMIT = 8,
     S_UNKNOWN_TYPE = 16,
     S_ZERO_WEIGHT = 32,
-    S_CAPACITY = 64
+    S_CAPACITY = 64,
+    S_TIMEOUT = 128    // a bounded wait inside a kernel ran out
 };
 
 struct DType {

@@ -256,6 +256,7 @@ int status_code(tg_handle* h, int st, const char* where) {
     if (st & S_NOT_SURFACE) return fail(h, TG_ERR_NOT_SURFACE, what + ": node is not a surface cell");
     if (st & S_WALK_LIMIT) return fail(h, TG_ERR_WALK_LIMIT, what + ": tetrahedron walk limit");
     if (st & S_UNKNOWN_TYPE) return fail(h, TG_ERR_UNKNOWN_TYPE, what + ": unknown cell type");
+    if (st & S_TIMEOUT) return fail(h, TG_ERR_TIMEOUT, what + ": a bounded device wait ran out");
     return fail(h, TG_ERR_CUDA, what + ": device status");
 }
 
@@ -1354,6 +1355,35 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
         rec->phi_after = (float)phi;
         for (int k = 0; k < 3; k++) rec->field_after[k] = (float)E[k];
     }
+    return TG_OK;
+}
+
+int tg_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, int32_t M, int32_t N, int32_t K) {
+    if (!A || !B || !C || !gemm_shape_ok(M, N, K))
+        return fail(nullptr, TG_ERR_ARGUMENT, "tg_gemm_bf16: M % 128, N in {64, 128}, K % 64 required");
+    void *dA = nullptr, *dB = nullptr;
+    float* dC = nullptr;
+    int* dSt = nullptr;
+    const size_t bytesA = sizeof(uint16_t) * (size_t)M * K, bytesB = sizeof(uint16_t) * (size_t)N * K;
+    const size_t bytesC = sizeof(float) * (size_t)M * N;
+    cudaError_t e = cudaMalloc(&dA, bytesA);
+    if (e == cudaSuccess) e = cudaMalloc(&dB, bytesB);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&dC), bytesC);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&dSt), sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(dA, A, bytesA, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dB, B, bytesB, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(dSt, 0, sizeof(int));
+    if (e == cudaSuccess) e = launch_gemm_bf16(dA, dB, dC, M, N, K, dSt, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int st = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&st, dSt, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(C, dC, bytesC, cudaMemcpyDeviceToHost);
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+    cudaFree(dSt);
+    if (e != cudaSuccess) return fail(nullptr, TG_ERR_CUDA, std::string("tg_gemm_bf16: ") + cudaGetErrorString(e));
+    if (st != 0) return status_code(nullptr, st, "tg_gemm_bf16");
     return TG_OK;
 }
 

@@ -174,4 +174,36 @@ void launch_trace_one(const DevMesh& m, const float start[3], float qm, int gues
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit,
                          float* out, cudaStream_t s);
 
+// ---- learned warm start (mpnn.cu) ----
+// C[M x N] (FP32) = A[M x K] * B[N x K]^T, A and B BF16 row-major, on the
+// tensor cores; M % 128 == 0, N in {64, 128}, K % 64 == 0
+bool gemm_shape_ok(int M, int N, int K);
+cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int* status,
+                             cudaStream_t s);
+void launch_ball_bfs(const DevMesh& m, int site, int hops, int cap, int32_t* nodes, int8_t* level, int32_t* count,
+                     int32_t* localOf, cudaStream_t s);
+void launch_ball_reset(const int32_t* nodes, const int32_t* count, int32_t* localOf, int cap, cudaStream_t s);
+void launch_ball_features(const DevMesh& m, int site, int hops, int D, const int32_t* nodes, const int8_t* level,
+                          const int32_t* count, const int32_t* localOf, float* scale, float* X, int32_t* ellCol,
+                          float* ellW, double* phiStart, int cap, cudaStream_t s);
+void launch_input_bf16(const float* X, int n, int npad, void* Z, void* ZT, cudaStream_t s);
+void launch_bias_act(const float* C, const float* b, const float* hPrev, float* u, float* h, int npad, cudaStream_t s);
+void launch_message_concat(const float* h, const int32_t* ellCol, const float* ellW, int D, int n, int npad, void* Z,
+                           void* ZT, cudaStream_t s);
+void launch_readout(const float* h, const float* w, const float* b, int n, float* y, cudaStream_t s);
+void launch_loss(const float* y, const float* tgt, int n, float invCount, float* dy, float* loss, cudaStream_t s);
+void launch_readout_back(const float* h, const float* dy, const float* w, int n, int npad, float* gw, float* gb,
+                         float* dh, cudaStream_t s);
+void launch_act_back(const float* dh, const float* u, int npad, void* DU, void* DUT, float* gb, cudaStream_t s);
+void launch_message_back(const float* dh, const float* dz, const int32_t* ellCol, const float* ellW, int D, int n,
+                         int npad, float* dhPrev, cudaStream_t s);
+void launch_adam(float* p, const float* g, float* m1, float* m2, int count, float lr, float b1, float b2, float eps,
+                 float c1, float c2, cudaStream_t s);
+void launch_weights_bf16(const float* W, void* Wb, void* WTb, cudaStream_t s);
+void launch_apply_prediction(const DevMesh& m, const int32_t* nodes, const int32_t* count, const float* y,
+                             const float* scale, const int32_t* slotOf, float* hist, int cap, cudaStream_t s);
+void launch_collect_target(const DevMesh& m, const int32_t* nodes, const int32_t* count, const double* phiStart,
+                           const float* scale, float* tgt, int cap, cudaStream_t s);
+void launch_shift_cols(int32_t* col, int count, int shift, cudaStream_t s);
+
 }  // namespace tgd
