@@ -123,7 +123,9 @@ typedef struct {
      *   0  the current potentials (the previous event's solution; plain),
      *   1  plus the previous event's correction on the non-Neumann free
      *      cells (the smooth far field of one removal changes little
-     *      from one site to the next).
+     *      from one site to the next),
+     *   2  as 1, plus the prediction of an attached learner on the cells
+     *      around the removed atom (tg_learner_attach, mode bit 1).
      * The solve always ends at rel_tol, whatever the start. */
     int32_t warm_start;
     int32_t reserved;
@@ -264,6 +266,40 @@ int tg_run_event(tg_handle* h, const tg_event_opts* opts, int32_t event_index, t
  * the records before it are complete. */
 int tg_run_events(tg_handle* h, const tg_event_opts* opts, int32_t first_index, int32_t count,
                   tg_event_record* recs, int32_t* done);
+
+/* ---- learned near-field warm start (no counterpart in the reference) -----
+ * A message-passing network (an input layer and four message layers of
+ * width 64, BF16 tensor-core GEMMs with FP32 accumulation) on the free cells
+ * within `hops` steps of a removed atom predicts the part of the event's
+ * correction that the recycled far field (warm_start 1) misses.  Samples are
+ * (features right after the far-field start, converged correction) pairs
+ * that tg_solve collects while a learner is attached in collect mode; the
+ * network is trained on them on the device; tg_solve with warm_start 2 adds
+ * its prediction before the CG.  The solve still ends at rel_tol. */
+typedef struct tg_learner tg_learner;
+int tg_learner_create(int32_t hops, int32_t max_cells, int32_t ell_width, uint64_t seed, tg_learner** out);
+void tg_learner_destroy(tg_learner* L);
+const char* tg_learner_last_error(const tg_learner* L);
+int32_t tg_learner_num_params(void);
+/* mode: 0 detach, bit 0 collect samples, bit 1 predict (for warm_start 2).
+ * The learner's graph width must hold the mesh's longest row. */
+int tg_learner_attach(tg_handle* h, tg_learner* L, int32_t mode);
+int tg_learner_samples(const tg_learner* L, int32_t* count, int64_t* cells);
+int tg_learner_get_params(tg_learner* L, float* params /* [num_params] */);
+int tg_learner_set_params(tg_learner* L, const float* params);
+/* sample idx to host: *n cells, features [n*16], ELL columns / weights
+ * [n*ell_width] (graph-local indices, -1 padding), target [n]; any output
+ * may be NULL */
+int tg_learner_get_sample(tg_learner* L, int32_t idx, int32_t* n, float* features, int32_t* ell_col, float* ell_w,
+                          float* target);
+/* loss, gradient [num_params] and outputs [cells] over samples
+ * first..first+count-1 taken as one batch (no update) */
+int tg_learner_gradients(tg_learner* L, int32_t first, int32_t count, float* loss, float* grads, float* outputs);
+/* `steps` Adam steps on random batches of `batch` samples drawn from
+ * first..first+count-1 (count <= 0: to the end); *mean_loss over the last
+ * tenth of the steps */
+int tg_learner_train(tg_learner* L, int32_t steps, int32_t batch, float lr, uint64_t seed, int32_t first,
+                     int32_t count, float* mean_loss);
 
 /* ---- measurement (no counterpart in the reference) ---------------------- */
 /* CUDA events on the handle's stream around a region of calls. */

@@ -123,6 +123,17 @@ SIGNATURES = {
     "tg_launch_count": (C.c_int64, [_P]),
     "tg_bench_kernel": (C.c_int, [_P, _I, _I, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
     "tg_gemm_bf16": (C.c_int, [_P, _P, _P, _I, _I, _I]),
+    "tg_learner_create": (C.c_int, [_I, _I, _I, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "tg_learner_destroy": (None, [_P]),
+    "tg_learner_last_error": (C.c_char_p, [_P]),
+    "tg_learner_num_params": (C.c_int32, []),
+    "tg_learner_attach": (C.c_int, [_P, _P, _I]),
+    "tg_learner_samples": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "tg_learner_get_params": (C.c_int, [_P, _P]),
+    "tg_learner_set_params": (C.c_int, [_P, _P]),
+    "tg_learner_get_sample": (C.c_int, [_P, _I, C.POINTER(C.c_int32), _P, _P, _P, _P]),
+    "tg_learner_gradients": (C.c_int, [_P, _I, _I, C.POINTER(C.c_float), _P, _P]),
+    "tg_learner_train": (C.c_int, [_P, _I, _I, C.c_float, C.c_uint64, _I, _I, C.POINTER(C.c_float)]),
     "tg_tip_params_default": (None, [C.POINTER(tg_tip_params)]),
     "tg_mesh_from_tip": (C.c_int, [C.POINTER(tg_tip_params), _I, C.POINTER(_P)]),
     "tg_mesh_from_files": (C.c_int, [C.c_char_p, C.c_char_p, _I, C.POINTER(_P)]),

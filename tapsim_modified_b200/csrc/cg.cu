@@ -41,30 +41,28 @@ __device__ __forceinline__ void cg_coeffs(const double* scal, int it, double* al
 
 // u = r / d, x = 0, gamma_0 = r.u, rho_0 = r.r
 __global__ void k_vcg_init(VSys v, int slots) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double g = 0.0, rr = 0.0;
-    if (s < slots) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
         const float r = v.r[s];
         const float u = r / v.d[s];
         v.u[s] = u;
         v.x[s] = 0.0f;
         v.p[s] = 0.0f;
         v.sv[s] = 0.0f;
-        g = (double)r * (double)u;
-        rr = (double)r * (double)r;
+        g += (double)r * (double)u;
+        rr += (double)r * (double)r;
     }
-    block_sum_atomic<kBlock>(g, &v.scal[0]);
-    block_sum_atomic<kBlock>(rr, &v.scal[3]);
+    block_sum2_atomic<kBlock>(g, rr, &v.scal[0], &v.scal[3]);
 }
 
 // w = A u over SELL-32 slices; delta -> scal[4*it+1] (it = iteration whose
 // u this is); skipped once rho_it <= target
 __global__ void k_vcg_spmv(VSys v, int slices, int it, double target) {
     if (it >= 0 && v.scal[4 * it + 3] <= target) return;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
     double dl = 0.0;
-    if (warp < slices) {
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
         const int base = v.slice_start[warp];
         const int width = v.slice_width[warp];
         const int s = warp * 32 + lane;
@@ -91,7 +89,7 @@ __global__ void k_vcg_spmv(VSys v, int slices, int it, double target) {
         const float u = v.u[s];
         const float w = v.d[s] * u - acc;
         v.w[s] = w;
-        dl = (double)w * (double)u;
+        dl += (double)w * (double)u;
     }
     block_sum_atomic<kBlock>(dl, &v.scal[4 * (it < 0 ? 0 : it) + 1]);
 }
@@ -104,9 +102,8 @@ __global__ void k_vcg_update(VSys v, int slots, int it, double target) {
     cg_coeffs(v.scal, it, &alpha, &beta);
     if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[4 * it + 2] = alpha;
     const float a = (float)alpha, b = (float)beta;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double g = 0.0, rr = 0.0;
-    if (s < slots) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
         const float p = v.u[s] + b * v.p[s];
         const float sv = v.w[s] + b * v.sv[s];
         v.p[s] = p;
@@ -116,11 +113,10 @@ __global__ void k_vcg_update(VSys v, int slots, int it, double target) {
         v.r[s] = r;
         const float u = r / v.d[s];
         v.u[s] = u;
-        g = (double)r * (double)u;
-        rr = (double)r * (double)r;
+        g += (double)r * (double)u;
+        rr += (double)r * (double)r;
     }
-    block_sum_atomic<kBlock>(g, &v.scal[4 * (it + 1)]);
-    block_sum_atomic<kBlock>(rr, &v.scal[4 * (it + 1) + 3]);
+    block_sum2_atomic<kBlock>(g, rr, &v.scal[4 * (it + 1)], &v.scal[4 * (it + 1) + 3]);
 }
 
 // phi64[node] += x[slot] (and hist[slot] += x[slot] when recording);
@@ -162,18 +158,19 @@ __global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int
 
 // FP64 residual of the V rows written straight into slot order
 __global__ void k_vcg_residual(DevMesh m, VSys v, int slots, double* acc) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    double r = 0.0;
-    if (s < slots) {
+    double r2 = 0.0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
         const int i = v.node_of[s];
+        double r = 0.0;
         if (i >= 0) {
             double sum = 0.0;
             for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) sum += m.ceff64[q] * m.phi64[m.col[q]];
             r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
         }
         v.r[s] = (float)r;
+        r2 += r * r;
     }
-    block_sum_atomic<kBlock>(r * r, acc);
+    block_sum_atomic<kBlock>(r2, acc);
 }
 
 // Appends the row of a node that has just become a non-Neumann free cell
@@ -243,17 +240,33 @@ __global__ void k_vsys_add_rows(DevMesh m, VSys v, const int32_t* nodes, int cou
 
 inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 
+// Pointwise kernels that end in a global reduction loop over their rows
+// with a grid of at most eight blocks per SM (full occupancy at 256
+// threads), so that the reduction costs ~1.2K same-address atomics instead
+// of one per 256 rows.  The SpMV keeps one warp per slice over the full
+// grid: slices differ in width, and many small blocks balance them.
+inline int reduce_blocks(int n) {
+    static int cap = 0;
+    if (cap == 0) {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cap = 8 * (sms > 0 ? sms : 148);
+    }
+    const int b = blocks(n);
+    return b < cap ? b : cap;
+}
+
 }  // namespace
 
 void launch_vcg_init(const VSys& v, int slots, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_init<<<blocks(slots), kBlock, 0, s>>>(v, slots); }
+    if (slots > 0) { count_launch(); k_vcg_init<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots); }
 }
 void launch_vcg_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s) {
     const int slices = (slots + 31) / 32;
     if (slices > 0) { count_launch(); k_vcg_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, it, target); }
 }
 void launch_vcg_update(const VSys& v, int slots, int it, double target, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_update<<<blocks(slots), kBlock, 0, s>>>(v, slots, it, target); }
+    if (slots > 0) { count_launch(); k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, it, target); }
 }
 void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s) {
     if (slots > 0) { count_launch(); k_vcg_apply<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, record ? 1 : 0); }
@@ -266,7 +279,7 @@ void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* r
     if (count > 0) { count_launch(); k_vcg_couple_neumann<<<blocks(count), kBlock, 0, s>>>(m, v, rows, count, rN); }
 }
 void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_residual<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, acc); }
+    if (slots > 0) { count_launch(); k_vcg_residual<<<reduce_blocks(slots), kBlock, 0, s>>>(m, v, slots, acc); }
 }
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
     if (count > 0) { count_launch(); k_vsys_add_rows<<<1, 32, 0, s>>>(m, v, nodes, count); }

