@@ -48,6 +48,10 @@ TIPS = {
     # about 3 GB on the device
     "prof": dict(cap_radius=12e-9, shank_length=30e-9, half_angle_deg=8.0, fine_shell=4e-9,
                  box_half_width=0.5e-6, box_height=1.0e-6),
+    # training tip of the learned warm start: another shape and seed than the
+    # timed tip (the network sees only neighbourhoods of removed atoms)
+    "train": dict(cap_radius=10e-9, shank_length=20e-9, half_angle_deg=8.0, fine_shell=4e-9,
+                  box_half_width=0.5e-6, box_height=1.0e-6),
 }
 REL_TOL = 1e-8
 
@@ -151,7 +155,7 @@ def run_ours(args, rank: int, world: int, dist):
     import torch
 
     from tapsim_modified_b200 import _native as N
-    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, Mesh, solve_opts
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, Learner, Mesh, solve_opts
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -168,7 +172,35 @@ def run_ours(args, rank: int, world: int, dist):
     h2d_bytes = sum(v.nbytes for k, v in arrays.items() if isinstance(v, np.ndarray))
     opts = EvaporationOptions.from_ini(None)
 
-    def run_arm(warm_start: int):
+    def train_learner():
+        """Learned near field: samples from events on a training tip of
+        another shape and seed (plain solver with the recycled far field),
+        trained on the device; the last tenth of the samples is held out."""
+        t0 = time.perf_counter()
+        tmesh = Mesh.from_tip(seed=101 + rank, **TIPS["train"])
+        tgrid = Grid(tmesh)
+        tgrid.solve(REL_TOL, 50, 50000, 1e-4)
+        learner = Learner(hops=6, max_cells=8192, ell_width=64, seed=7 + rank)
+        learner.attach(tgrid, collect=True)
+        tev = Evaporation(tgrid, opts, relax_mode=1,
+                          solve=solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, warm_start=1))
+        tev.run(args.train_events)
+        learner.attach(tgrid)
+        tgrid.close()
+        n, cells = learner.samples()
+        hold = max(1, n // 10)
+        train_n = n - hold
+        before = learner.gradients(train_n, hold)[0]
+        last = learner.train(args.train_steps, batch=8, lr=1e-3, seed=rank, first=0, count=train_n)
+        after = learner.gradients(train_n, hold)[0]
+        return learner, {"train_tip": f"train: r={TIPS['train']['cap_radius'] * 1e9:g} nm cap, "
+                                      f"{TIPS['train']['shank_length'] * 1e9:g} nm shank, seed {101 + rank}, "
+                                      f"{tmesh.num_nodes} cells",
+                         "samples": n, "cells_per_sample": cells / max(n, 1), "train_steps": args.train_steps,
+                         "train_loss_last": last, "heldout_loss_untrained": before, "heldout_loss_trained": after,
+                         "setup_s": time.perf_counter() - t0}
+
+    def run_arm(warm_start: int, learner=None):
         """Mesh upload, initial relaxation, W warm-up and K timed events with
         the given solve start; returns the timings and the event records."""
         sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4, warm_start=warm_start)
@@ -178,6 +210,8 @@ def run_ours(args, rank: int, world: int, dist):
         t0 = time.perf_counter()
         grid = Grid(mesh)                       # host -> device upload of the mesh
         info0 = grid.solve(REL_TOL, 50, 50000, 1e-4)  # initial relaxation
+        if learner is not None:
+            learner.attach(grid, predict=True)
         ev = Evaporation(grid, opts, relax_mode=1, solve=sopts)
         ev.run(args.warmup)
         # timed region: K events in one call (flights overlap the next
@@ -186,7 +220,7 @@ def run_ours(args, rank: int, world: int, dist):
             dist.barrier()
         torch.cuda.synchronize()
         launches0 = L.tg_launch_count(grid._h)
-        torch.cuda.nvtx.range_push(f"timed_{'warm' if warm_start else 'plain'}")
+        torch.cuda.nvtx.range_push(f"timed_{('plain', 'warm', 'learned')[warm_start]}")
         with ClockSampler(local) as clocks:
             N.check(L.tg_timer_start(grid._h), grid._h)
             ev.run(args.steps)
@@ -200,8 +234,15 @@ def run_ours(args, rank: int, world: int, dist):
         return {"grid": grid, "info0": info0, "dev_s": ms.value / 1e3, "t_e2e": t_e2e, "launches": launches,
                 "records": ev.records, "clocks": clocks, "phi": phi}
 
+    learner, learn_info = (None, None) if args.no_learned else train_learner()
     plain = run_arm(0)
     plain["grid"].close()
+    learned = None
+    if learner is not None:
+        learned = run_arm(2, learner)
+        learned["grid"].close()
+        learner.close()
+    # the headline arm: the fastest start measured, the recycled far field
     arm = run_arm(1)
     grid, info0, dev_s, t_e2e, phi, clocks = (arm[k] for k in ("grid", "info0", "dev_s", "t_e2e", "phi", "clocks"))
     launches = arm["launches"]
@@ -222,16 +263,18 @@ def run_ours(args, rank: int, world: int, dist):
     N.check(L.tg_bench_kernel(grid._h, 1, 20, C.byref(r_avg), C.byref(r_bytes)), grid._h)
 
     if dist:
-        t = torch.tensor([dev_s, t_e2e, plain["dev_s"], float(args.steps), float(args.warmup + args.steps)],
+        lrn_s = learned["dev_s"] if learned else 0.0
+        t = torch.tensor([dev_s, t_e2e, plain["dev_s"], lrn_s, float(args.steps), float(args.warmup + args.steps)],
                          dtype=torch.float64, device="cuda")
         mx = t.clone()
-        dist.all_reduce(mx[:3], op=dist.ReduceOp.MAX)
+        dist.all_reduce(mx[:4], op=dist.ReduceOp.MAX)
         sm = t.clone()
-        dist.all_reduce(sm[3:], op=dist.ReduceOp.SUM)
-        dev_max, e2e_max, plain_max = float(mx[0]), float(mx[1]), float(mx[2])
-        ev_total, ev_e2e_total = float(sm[3]), float(sm[4])
+        dist.all_reduce(sm[4:], op=dist.ReduceOp.SUM)
+        dev_max, e2e_max, plain_max, lrn_max = float(mx[0]), float(mx[1]), float(mx[2]), float(mx[3])
+        ev_total, ev_e2e_total = float(sm[4]), float(sm[5])
     else:
         dev_max, e2e_max, plain_max = dev_s, t_e2e, plain["dev_s"]
+        lrn_max = learned["dev_s"] if learned else 0.0
         ev_total, ev_e2e_total = float(args.steps), float(args.warmup + args.steps)
     if rank != 0:
         return None
@@ -256,11 +299,21 @@ def run_ours(args, rank: int, world: int, dist):
                         f"{TIPS[args.tip]['shank_length'] * 1e9:g} nm shank, "
                         f"{TIPS[args.tip]['half_angle_deg']:g} deg, vacuum to 1 um; {atoms} atoms, "
                         f"{mesh.num_nodes} cells per GPU; relax to rel. residual <= {REL_TOL:g} every event; "
-                        "solve started from the previous event's correction (recycled far field)",
+                        "solve started from the previous event's correction (recycled far field, warm_start 1)",
+            "value_arm": "recycled far field (warm_start 1): the fastest start measured; the learned arm "
+                         "(warm_start 2) is in config.learned",
             "events_per_gpu": args.steps,
             "plain": {"value": ev_total / plain_max, "ms_per_step": plain_max * 1e3 / args.steps,
                       "solver_iterations_median": statistics.median(iters_plain),
                       "start": "previous event's potentials (plain relaxation)"},
+            "learned": None if learned is None else dict(learn_info, **{
+                "value": ev_total / lrn_max, "ms_per_step": lrn_max * 1e3 / args.steps,
+                "solver_iterations_median": statistics.median(
+                    [r["relax_iterations"] for r in learned["records"][args.warmup:]]),
+                "sequence_first_difference": next((k for k, (x, y) in enumerate(zip(
+                    [r["node"] for r in learned["records"]], [r["node"] for r in plain["records"]])) if x != y), None),
+                "start": "recycled far field plus the network's near-field prediction (warm_start 2); training "
+                         "on the device outside the timed region"}),
             "warm_over_plain": plain_max / dev_max,
             "sequence": {"events": len(seq_w), "first_difference": first_diff,
                          "note": "removed-node sequences of the warm-start and plain arms"},
@@ -361,6 +414,9 @@ def main():
     ap.add_argument("--tip", default="config2", choices=sorted(TIPS))
     ap.add_argument("--cpu-events", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
+    ap.add_argument("--train-steps", type=int, default=600, help="Adam steps of the learned warm start")
+    ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -201,7 +201,8 @@ void launch_adam(float* p, const float* g, float* m1, float* m2, int count, floa
                  float c1, float c2, cudaStream_t s);
 void launch_weights_bf16(const float* W, void* Wb, void* WTb, cudaStream_t s);
 void launch_apply_prediction(const DevMesh& m, const int32_t* nodes, const int32_t* count, const float* y,
-                             const float* scale, const int32_t* slotOf, float* hist, int cap, cudaStream_t s);
+                             const float* scale, float gain, const int32_t* slotOf, float* hist, int cap,
+                             cudaStream_t s);
 void launch_collect_target(const DevMesh& m, const int32_t* nodes, const int32_t* count, const double* phiStart,
                            const float* scale, float* tgt, int cap, cudaStream_t s);
 void launch_shift_cols(int32_t* col, int count, int shift, cudaStream_t s);

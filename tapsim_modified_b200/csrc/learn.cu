@@ -72,6 +72,7 @@ inline int roundup128(int n) { return (n + 127) / 128 * 128; }
 
 struct tg_learner {
     int hops = 6, cap = 4096, D = 32;
+    float gain = 1.0f;  // multiplier of the prediction added in tg_solve
     std::string err;
     cudaStream_t stream = nullptr;
     // parameters, gradients, Adam moments (FP32), BF16 weight copies
@@ -295,7 +296,8 @@ int learner_predict(tg_learner* L, const DevMesh& m, int site, const int32_t* sl
     }
     if (rc == TG_OK && hist != nullptr) {
         rc = forward(L, L->X.p, L->ellCol.p, L->ellW.p, n);
-        if (rc == TG_OK) launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, slotOf, hist, L->cap, s);
+        if (rc == TG_OK)
+            launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, slotOf, hist, L->cap, s);
     }
     L->stream = own;
     if (rc == TG_OK && cudaGetLastError() != cudaSuccess) rc = lfail(L, TG_ERR_CUDA, "learner: launch");
@@ -401,6 +403,12 @@ void tg_learner_destroy(tg_learner* L) {
 const char* tg_learner_last_error(const tg_learner* L) { return L ? L->err.c_str() : ""; }
 
 int32_t tg_learner_num_params(void) { return kParams; }
+
+int tg_learner_set_gain(tg_learner* L, float gain) {
+    if (!L || !(gain >= 0.0f) || gain > 4.0f) return lfail(L, TG_ERR_ARGUMENT, "tg_learner_set_gain: gain in [0, 4]");
+    L->gain = gain;
+    return TG_OK;
+}
 
 int tg_learner_samples(const tg_learner* L, int32_t* count, int64_t* cells) {
     if (!L) return lfail(nullptr, TG_ERR_ARGUMENT, "tg_learner_samples: null learner");

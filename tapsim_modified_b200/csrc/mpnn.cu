@@ -430,12 +430,12 @@ __global__ void k_weights_bf16(const float* W, __nv_bfloat16* Wb, __nv_bfloat16*
 // phi += sigma y on the graph's cells (and on the recorded correction of the
 // V rows, so that the next event recycles the whole correction)
 __global__ void k_apply_prediction(DevMesh m, const int32_t* nodes, const int32_t* count, const float* y,
-                                   const float* scale, const int32_t* slotOf, float* hist) {
+                                   const float* scale, float gain, const int32_t* slotOf, float* hist) {
     const int n = *count;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int g = nodes[t];
-    const float d = scale[0] * y[t];
+    const float d = gain * scale[0] * y[t];
     m.phi64[g] += (double)d;
     if (hist) {
         const int s = slotOf[g];
@@ -553,9 +553,10 @@ void launch_weights_bf16(const float* W, void* Wb, void* WTb, cudaStream_t s) {
                                                      static_cast<__nv_bfloat16*>(WTb));
 }
 void launch_apply_prediction(const DevMesh& m, const int32_t* nodes, const int32_t* count, const float* y,
-                             const float* scale, const int32_t* slotOf, float* hist, int cap, cudaStream_t s) {
+                             const float* scale, float gain, const int32_t* slotOf, float* hist, int cap,
+                             cudaStream_t s) {
     count_launch();
-    k_apply_prediction<<<nblk(cap), 256, 0, s>>>(m, nodes, count, y, scale, slotOf, hist);
+    k_apply_prediction<<<nblk(cap), 256, 0, s>>>(m, nodes, count, y, scale, gain, slotOf, hist);
 }
 void launch_collect_target(const DevMesh& m, const int32_t* nodes, const int32_t* count, const double* phiStart,
                            const float* scale, float* tgt, int cap, cudaStream_t s) {

@@ -316,6 +316,10 @@ class Learner:
         mode = (1 if collect else 0) | (2 if predict else 0)
         grid._ck(N.lib().tg_learner_attach(grid._h, self._h if mode else None, mode))
 
+    def set_gain(self, gain: float):
+        """Multiplier of the prediction that warm_start=2 adds (default 1)."""
+        self._ck(N.lib().tg_learner_set_gain(self._h, gain))
+
     def samples(self) -> tuple[int, int]:
         n, cells = C.c_int32(), C.c_int64()
         self._ck(N.lib().tg_learner_samples(self._h, C.byref(n), C.byref(cells)))
