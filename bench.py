@@ -140,6 +140,26 @@ def reference_run(dump: Path, cfg: Path, n_events: int, threads: int) -> tuple[l
     return walls, "reference TAPSim default ini: localRelax(shell 3) + 1 global sweep per event"
 
 
+def reduce_over_ranks(dist, maxed: list, summed: list, device: str):
+    """Max over ranks of the times, sum over ranks of the event counts (the
+    whole-job throughput is the events of all ranks over the slowest rank's
+    time).  Without a process group the values pass through."""
+    if not dist:
+        return [float(x) for x in maxed], [float(x) for x in summed]
+    import torch
+    t = torch.tensor([*maxed, *summed], dtype=torch.float64, device=device)
+    mx = t[:len(maxed)].clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t[len(maxed):].clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return [float(x) for x in mx], [float(x) for x in sm]
+
+
+def tip_seed(rank: int) -> int:
+    """Each rank evaporates its own tip (independent units, weak scaling)."""
+    return 1 + rank
+
+
 def build_mesh(tip: str, seed: int):
     from tapsim_modified_b200.tapsim import Mesh
     t = time.time()
@@ -166,7 +186,7 @@ def run_ours(args, rank: int, world: int, dist):
     warm.solve()
     warm.close()
 
-    mesh = build_mesh(args.tip, seed=1 + rank)
+    mesh = build_mesh(args.tip, seed=tip_seed(rank))
     arrays = mesh.arrays()
     atoms = int((arrays["type"] == 4).sum())
     h2d_bytes = sum(v.nbytes for k, v in arrays.items() if isinstance(v, np.ndarray))
@@ -262,20 +282,9 @@ def run_ours(args, rank: int, world: int, dist):
     r_bytes = C.c_double()
     N.check(L.tg_bench_kernel(grid._h, 1, 20, C.byref(r_avg), C.byref(r_bytes)), grid._h)
 
-    if dist:
-        lrn_s = learned["dev_s"] if learned else 0.0
-        t = torch.tensor([dev_s, t_e2e, plain["dev_s"], lrn_s, float(args.steps), float(args.warmup + args.steps)],
-                         dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx[:4], op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm[4:], op=dist.ReduceOp.SUM)
-        dev_max, e2e_max, plain_max, lrn_max = float(mx[0]), float(mx[1]), float(mx[2]), float(mx[3])
-        ev_total, ev_e2e_total = float(sm[4]), float(sm[5])
-    else:
-        dev_max, e2e_max, plain_max = dev_s, t_e2e, plain["dev_s"]
-        lrn_max = learned["dev_s"] if learned else 0.0
-        ev_total, ev_e2e_total = float(args.steps), float(args.warmup + args.steps)
+    (dev_max, e2e_max, plain_max, lrn_max), (ev_total, ev_e2e_total) = reduce_over_ranks(
+        dist, [dev_s, t_e2e, plain["dev_s"], learned["dev_s"] if learned else 0.0],
+        [args.steps, args.warmup + args.steps], "cuda")
     if rank != 0:
         return None
 
