@@ -183,10 +183,24 @@ typedef struct {
     float best_ratio;           /* = scaling reference */
     float second_ratio;
     double ratio_sum;
-    float probability;          /* best_ratio / ratio_sum */
+    float probability;          /* the candidate's normalised probability */
     int32_t apex;               /* Surface_3d::Table::apex (surface_3d.cpp:171-190) */
+    int32_t prob_mode;          /* probability mode of this selection */
+    float best_probability;     /* the two largest normalised probabilities */
+    float second_probability;   /* (near-tie margin = (best - second) / best) */
+    double score_sum;           /* sum of the scores before normalisation */
 } tg_select_info;
 int tg_surface_select(tg_handle* h, tg_select_info* info);
+/* The same with Surface_3d::evap_compute_probabilities' mode
+ * (surface_3d.cpp:220-399): 0 linear field, 1 Boltzmann at `temperature`
+ * [K] (> 0), 2 linear force (field_o2, grid_3d.cpp:993-1199), 3 Voronoi
+ * flux force.  The candidate is evapMaximum's: the first maximum of the
+ * normalised probabilities in ascending node order. */
+int tg_surface_select_mode(tg_handle* h, int32_t prob_mode, float temperature, tg_select_info* info);
+/* evapMonteCarlo (surface_3d.cpp:433-449) on the last selection: the first
+ * surface cell, in ascending node order, whose cumulative probability
+ * reaches u in [0, 1] (the last cell when none does). */
+int tg_surface_pick(tg_handle* h, double u, int32_t* node, float* probability);
 int tg_get_surface(tg_handle* h, int32_t capacity, int32_t* nodes, float* ratios, int32_t* count);
 /* Surface_3d::Table::normal (surface_3d.cpp:123-169). */
 int tg_surface_normal(tg_handle* h, int32_t node, float normal_out[3]);
@@ -240,6 +254,16 @@ typedef struct {
     tg_trace_opts trace;
     int32_t trace_enabled;
     int32_t normal_enabled;
+    /* METHOD_EVAPORATION_PROBABILITY (0 linear field, 1 Boltzmann, 2 linear
+     * force, 3 Voronoi flux force) and METHOD_EVAPORATION_CHOICE (0
+     * maximum, 1 Monte-Carlo); the configuration's TEMPERATURE [K] for
+     * Boltzmann; the seed of the handle's Monte-Carlo stream, which draws
+     * like rand() after srand(seed) (the reference seeds 99, tapsim.cpp:235),
+     * seeded at the first Monte-Carlo choice of the handle */
+    int32_t prob_mode;
+    int32_t choice_mode;
+    float temperature;
+    uint32_t rng_seed;
 } tg_event_opts;
 typedef struct {
     int32_t node;
@@ -256,6 +280,7 @@ typedef struct {
     int32_t relax_iterations;
     double rel_residual;
     int32_t relax_status;
+    float best_probability, second_probability;  /* of the selection that chose node */
 } tg_event_record;
 int tg_run_event(tg_handle* h, const tg_event_opts* opts, int32_t event_index, tg_event_record* rec);
 /* `count` events in one call (indices first_index, first_index+1, ...):
@@ -341,6 +366,8 @@ int tg_mesh_from_files(const char* node_file, const char* config_file, int32_t t
  * config_file may be NULL to use the dump's own table. */
 int tg_mesh_from_dump(const char* dump_file, const char* config_file, tg_mesh** out);
 void tg_mesh_destroy(tg_mesh* m);
+/* Configuration::Table::temperature of the mesh's configuration [K] */
+float tg_mesh_temperature(const tg_mesh* m);
 /* Fills a description whose pointers stay valid while the mesh lives. */
 int tg_mesh_describe(const tg_mesh* m, tg_mesh_desc* desc, int32_t* nnz);
 int tg_mesh_write_node_file(const tg_mesh* m, const char* path, int32_t binary);

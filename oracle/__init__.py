@@ -26,7 +26,8 @@ def build():
 class orc_type(C.Structure):
     _fields_ = [("present", C.c_int32), ("removable", C.c_int32), ("neumann", C.c_int32), ("dirichlet", C.c_int32),
                 ("epsilon", C.c_double), ("evap_field", C.c_double), ("charge_density", C.c_double),
-                ("phi", C.c_double), ("mass", C.c_double), ("evap_charge", C.c_int32)]
+                ("phi", C.c_double), ("mass", C.c_double), ("evap_charge", C.c_int32),
+                ("evap_energy", C.c_double)]
 
 
 class orc_mesh(C.Structure):
@@ -69,6 +70,14 @@ def lib():
         L.orc_surface_init.argtypes = [P, C.c_int32]
         L.orc_select.restype = None
         L.orc_select.argtypes = [P, C.c_void_p, C.POINTER(orc_select_info)]
+        L.orc_select_mode.restype = None
+        L.orc_select_mode.argtypes = [P, C.c_int32, C.c_double, C.c_void_p, C.POINTER(orc_select_info)]
+        L.orc_field_o2.restype = C.c_int
+        L.orc_field_o2.argtypes = [P, C.c_int32, C.c_void_p, C.POINTER(C.c_double)]
+        L.orc_score.restype = C.c_double
+        L.orc_score.argtypes = [P, C.c_int32, C.c_int32, C.c_double]
+        L.orc_pick.restype = C.c_int32
+        L.orc_pick.argtypes = [P, C.c_void_p, C.c_double, C.c_double]
         L.orc_take_away.restype = C.c_int32
         L.orc_take_away.argtypes = [P, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
         L.orc_update_coordination.restype = None
@@ -123,6 +132,7 @@ class Oracle:
             o.dirichlet = t["dirichlet"]
             o.epsilon = t["epsilon"]
             o.evap_field = t["evap_field"]
+            o.evap_energy = t["evap_energy"]
             o.charge_density = t["charge_density"]
             o.phi = t["phi"]
             o.mass = t["mass"]
@@ -163,6 +173,22 @@ class Oracle:
         ratio = np.zeros(self.n, np.float32)
         self.L.orc_select(C.byref(self.m), _p(ratio), C.byref(info))
         return info, ratio
+
+    def select_mode(self, mode: int, temperature: float = 0.0):
+        """(info, score) for probability mode 0..3 (surface_3d.cpp:220-399)."""
+        info = orc_select_info()
+        score = np.zeros(self.n, np.float32)
+        self.L.orc_select_mode(C.byref(self.m), int(mode), float(temperature), _p(score), C.byref(info))
+        return info, score
+
+    def field_o2(self, i: int):
+        E = np.zeros(3)
+        q = C.c_double()
+        ok = self.L.orc_field_o2(C.byref(self.m), int(i), _p(E), C.byref(q))
+        return E, q.value, bool(ok)
+
+    def pick(self, score: np.ndarray, total: float, u: float) -> int:
+        return int(self.L.orc_pick(C.byref(self.m), _p(np.ascontiguousarray(score, np.float32)), float(total), float(u)))
 
     def take_away(self, node: int, vacuum_id: int) -> list[int]:
         det = np.zeros(512, np.int32)

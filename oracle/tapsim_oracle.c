@@ -181,6 +181,157 @@ void orc_select(const orc_mesh* m, float* ratio_out, orc_select_info* info) {
     }
 }
 
+/* Gaussian elimination with partial pivoting on a 9x9 system (the
+ * reference uses LU with partial pivoting, utils.h:52-210); returns 0 when
+ * a pivot vanishes */
+static int solve9(double a[81], double b[9]) {
+    for (int k = 0; k < 9; k++) {
+        int p = k;
+        for (int r = k + 1; r < 9; r++)
+            if (fabs(a[r * 9 + k]) > fabs(a[p * 9 + k])) p = r;
+        if (a[p * 9 + k] == 0.0) return 0;
+        if (p != k) {
+            for (int j = 0; j < 9; j++) {
+                const double t = a[k * 9 + j];
+                a[k * 9 + j] = a[p * 9 + j];
+                a[p * 9 + j] = t;
+            }
+            const double t = b[k];
+            b[k] = b[p];
+            b[p] = t;
+        }
+        for (int r = k + 1; r < 9; r++) {
+            const double f = a[r * 9 + k] / a[k * 9 + k];
+            for (int j = k; j < 9; j++) a[r * 9 + j] -= f * a[k * 9 + j];
+            b[r] -= f * b[k];
+        }
+    }
+    for (int k = 8; k >= 0; k--) {
+        double s = b[k];
+        for (int j = k + 1; j < 9; j++) s -= a[k * 9 + j] * b[j];
+        b[k] = s / a[k * 9 + k];
+    }
+    return 1;
+}
+
+/* basis of the second-order fit: x, y, z, x^2/2, xy, xz, y^2/2, yz, z^2/2 */
+static void basis9(double x, double y, double z, double f[9]) {
+    f[0] = x; f[1] = y; f[2] = z;
+    f[3] = 0.5 * x * x; f[4] = x * y; f[5] = x * z;
+    f[6] = 0.5 * y * y; f[7] = y * z; f[8] = 0.5 * z * z;
+}
+
+int orc_field_o2(const orc_mesh* m, int32_t i, double E[3], double* charge) {
+    E[0] = E[1] = E[2] = 0.0;
+    *charge = 0.0;
+    if (m->hull[i]) return 1;
+    double a[81] = {0}, b[9] = {0};
+    for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+        const int j = m->col[q];
+        double f[9];
+        basis9((double)m->xyz[3 * j] - m->xyz[3 * i], (double)m->xyz[3 * j + 1] - m->xyz[3 * i + 1],
+               (double)m->xyz[3 * j + 2] - m->xyz[3 * i + 2], f);
+        const double dp = m->phi[j] - m->phi[i];
+        for (int r = 0; r < 9; r++) {
+            b[r] += dp * f[r];
+            for (int s = 0; s < 9; s++) a[r * 9 + s] += f[r] * f[s];
+        }
+    }
+    if (!solve9(a, b)) return 0;
+    E[0] = -b[0];
+    E[1] = -b[1];
+    E[2] = -b[2];
+    *charge = -(b[3] + b[6] + b[8]) * 8.85418781762e-12;
+    return 1;
+}
+
+double orc_score(const orc_mesh* m, int32_t i, int32_t mode, double temperature) {
+    const orc_type* t = &m->types[(int)m->type[i]];
+    if (mode == 1 || mode == 0) {
+        double E[3];
+        orc_field_o1(m, i, E);
+        const double ratio = sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]) / t->evap_field;
+        if (mode == 0) return ratio;
+        /* probBoltzmann (surface_3d.cpp:222-264) */
+        return exp(-(1.0 - ratio) * t->evap_energy / (temperature * 8.6173431e-5) / 2.0);
+    }
+    if (mode == 2) {
+        /* probLinear_force (surface_3d.cpp:299-330) */
+        double E[3], q;
+        orc_field_o2(m, i, E, &q);
+        return q * sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]) / (t->evap_field * t->evap_field);
+    }
+    /* probVoronoiFluxForce (surface_3d.cpp:332-399) */
+    const double eps0 = 8.85418781762e-12;
+    double F[3] = {0, 0, 0}, area = 0.0;
+    const double ei = 1.0 / t->epsilon;
+    for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+        const int j = m->col[q];
+        const double ej = 1.0 / m->types[(int)m->type[j]].epsilon;
+        const double dp = m->phi[j] - m->phi[i];
+        const double v = -eps0 * dp * dp * m->c[q] * (ej - ei);
+        const double dx = (double)m->xyz[3 * j] - m->xyz[3 * i], dy = (double)m->xyz[3 * j + 1] - m->xyz[3 * i + 1],
+                     dz = (double)m->xyz[3 * j + 2] - m->xyz[3 * i + 2];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        area += m->c[q] * sqrt(d2) / 2.0 * (ei + ej);
+        F[0] += dx / d2 * v;
+        F[1] += dy / d2 * v;
+        F[2] += dz / d2 * v;
+    }
+    return sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]) / area / (t->evap_field * t->evap_field);
+}
+
+void orc_select_mode(const orc_mesh* m, int32_t mode, double temperature, float* score_out, orc_select_info* info) {
+    info->candidate = -1;
+    info->apex = -1;
+    info->num_surface = 0;
+    info->best = -1.0f;
+    info->second = 0.0f;
+    info->sum = 0.0;
+    float zmax = 0.0f;
+    for (int i = 0; i < m->n; i++) {
+        if (!m->surface[i]) continue;
+        const float s = (float)orc_score(m, i, mode, temperature);
+        score_out[i] = s;
+        info->sum += s;
+        if (info->apex < 0 || m->xyz[3 * i + 2] > zmax) {
+            zmax = m->xyz[3 * i + 2];
+            info->apex = i;
+        }
+        info->num_surface++;
+    }
+    /* evapMaximum on the normalised probabilities: the first maximum (a NaN
+     * probability, as from a zero sum, never replaces the first cell) */
+    const float sum = (float)info->sum;
+    for (int i = 0; i < m->n; i++) {
+        if (!m->surface[i]) continue;
+        const float p = score_out[i] / sum;
+        if (info->candidate < 0) {
+            info->candidate = i;
+            info->best = p;
+        } else if (info->best < p) {
+            if (info->best > info->second) info->second = info->best;
+            info->best = p;
+            info->candidate = i;
+        } else if (p > info->second) {
+            info->second = p;
+        }
+    }
+}
+
+int32_t orc_pick(const orc_mesh* m, const float* score, double sum, double u) {
+    const float fs = (float)sum;
+    double cum = 0.0;
+    int32_t last = -1;
+    for (int i = 0; i < m->n; i++) {
+        if (!m->surface[i]) continue;
+        cum += (double)(score[i] / fs);
+        last = i;
+        if (!(u > cum)) return i;
+    }
+    return last;
+}
+
 /* computeCoupling (grid_3d.cpp:1392-1409) for the pair (n1, n2) */
 static double pair_coupling(const orc_mesh* m, int n1, int n2, double geom) {
     if (!is_neumann(m, n1) && is_neumann(m, n2)) return 0.0;

@@ -14,6 +14,7 @@ typedef struct {
     int32_t present, removable, neumann, dirichlet;
     double epsilon, evap_field, charge_density, phi, mass;
     int32_t evap_charge;
+    double evap_energy;        /* [eV] */
 } orc_type;
 
 typedef struct {
@@ -54,6 +55,21 @@ typedef struct {
     double sum;
 } orc_select_info;
 void orc_select(const orc_mesh* m, float* ratio_out /* [n] or NULL */, orc_select_info* info);
+/* Grid_3d::Table::field_o2 (grid_3d.cpp:993-1199): second-order fit over all
+ * neighbours; field and charge (0 on hull cells); returns 0 when singular */
+int orc_field_o2(const orc_mesh* m, int32_t i, double E[3], double* charge);
+/* score of one surface cell before normalisation (surface_3d.cpp:222-399):
+ * mode 0 |E|/E_evap, 1 Boltzmann, 2 linear force (field_o2), 3 Voronoi flux
+ * force; temperature [K] for mode 1 */
+double orc_score(const orc_mesh* m, int32_t i, int32_t mode, double temperature);
+/* evap_compute_probabilities + evapMaximum over the surface set in
+ * ascending order: score_out[i] = score (float), info->candidate = first
+ * maximum of score / sum, best / second = the two largest normalised
+ * probabilities, sum = the score sum */
+void orc_select_mode(const orc_mesh* m, int32_t mode, double temperature, float* score_out, orc_select_info* info);
+/* evapMonteCarlo (surface_3d.cpp:433-449): the first surface cell (ascending)
+ * whose cumulative probability score/sum reaches u; the last one if none */
+int32_t orc_pick(const orc_mesh* m, const float* score, double sum, double u);
 /* evap_takeAway; returns the number of detached cells (written to detached) */
 int32_t orc_take_away(orc_mesh* m, int32_t node, int32_t vacuum_id, int32_t* detached, int32_t cap);
 /* update_coordination */

@@ -50,7 +50,8 @@ class tg_solve_info(C.Structure):
 class tg_select_info(C.Structure):
     _fields_ = [("num_surface", C.c_int32), ("candidate", C.c_int32), ("best_ratio", C.c_float),
                 ("second_ratio", C.c_float), ("ratio_sum", C.c_double), ("probability", C.c_float),
-                ("apex", C.c_int32)]
+                ("apex", C.c_int32), ("prob_mode", C.c_int32), ("best_probability", C.c_float),
+                ("second_probability", C.c_float), ("score_sum", C.c_double)]
 
 
 class tg_trace_opts(C.Structure):
@@ -69,7 +70,8 @@ class tg_event_opts(C.Structure):
                 ("global_steps", C.c_int32), ("refresh_interval", C.c_int32), ("refresh_threshold", C.c_double),
                 ("refresh_cycle", C.c_int32), ("refresh_queue", C.c_int32), ("refresh_max_sweeps", C.c_int64),
                 ("solve", tg_solve_opts), ("trace", tg_trace_opts), ("trace_enabled", C.c_int32),
-                ("normal_enabled", C.c_int32)]
+                ("normal_enabled", C.c_int32), ("prob_mode", C.c_int32), ("choice_mode", C.c_int32),
+                ("temperature", C.c_float), ("rng_seed", C.c_uint32)]
 
 
 class tg_event_record(C.Structure):
@@ -77,7 +79,8 @@ class tg_event_record(C.Structure):
                 ("second_ratio", C.c_float), ("scaling_reference", C.c_float), ("phi_before", C.c_float),
                 ("field_before", C.c_float * 3), ("phi_after", C.c_float), ("field_after", C.c_float * 3),
                 ("apex", C.c_float * 3), ("normal", C.c_float * 3), ("impact", tg_impact), ("detached", C.c_int32),
-                ("relax_iterations", C.c_int32), ("rel_residual", C.c_double), ("relax_status", C.c_int32)]
+                ("relax_iterations", C.c_int32), ("rel_residual", C.c_double), ("relax_status", C.c_int32), ("best_probability", C.c_float),
+                ("second_probability", C.c_float)]
 
 
 class tg_tip_params(C.Structure):
@@ -110,6 +113,8 @@ SIGNATURES = {
     "tg_get_types": (C.c_int, [_P, _P]),
     "tg_surface_init": (C.c_int, [_P, _I, C.POINTER(_I)]),
     "tg_surface_select": (C.c_int, [_P, C.POINTER(tg_select_info)]),
+    "tg_surface_select_mode": (C.c_int, [_P, _I, C.c_float, C.POINTER(tg_select_info)]),
+    "tg_surface_pick": (C.c_int, [_P, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "tg_get_surface": (C.c_int, [_P, _I, _P, _P, C.POINTER(_I)]),
     "tg_surface_normal": (C.c_int, [_P, _I, _P]),
     "tg_take_away": (C.c_int, [_P, _I, _I, _P, C.POINTER(_I)]),
@@ -140,6 +145,7 @@ SIGNATURES = {
     "tg_mesh_from_files": (C.c_int, [C.c_char_p, C.c_char_p, _I, C.POINTER(_P)]),
     "tg_mesh_from_dump": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_P)]),
     "tg_mesh_destroy": (None, [_P]),
+    "tg_mesh_temperature": (C.c_float, [_P]),
     "tg_mesh_describe": (C.c_int, [_P, C.POINTER(tg_mesh_desc), C.POINTER(_I)]),
     "tg_mesh_write_node_file": (C.c_int, [_P, C.c_char_p, _I]),
     "tg_mesh_write_config": (C.c_int, [_P, C.c_char_p]),

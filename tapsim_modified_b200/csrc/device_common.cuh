@@ -30,6 +30,7 @@ enum : int {
 struct DType {
     float epsilon;
     float evap_field;
+    float evap_energy;  // [eV], EVAPORATION_ACTIVATION_ENERGY
     float charge_density;
     float phi;
     uint8_t removable, neumann, dirichlet, present;

@@ -9,7 +9,10 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <limits>
 #include <mutex>
+
+#include <stdlib.h>
 #include <string>
 #include <vector>
 
@@ -65,6 +68,7 @@ struct tg_handle {
     std::vector<int32_t> countV, countN;  // host mirrors
     int32_t countAllV = 0, countAllN = 0;
     int32_t surfSlots = 0;
+    int32_t surfMinNode = 0, surfMaxNode = -1;  // surface node range of the last selection
     std::vector<int32_t> h_node_tet;
     std::vector<float> h_xyz;
     std::vector<int8_t> h_type;           // host mirror of the type ids
@@ -80,7 +84,7 @@ struct tg_handle {
     DBuf<int> status;
     DBuf<int32_t> rowsV, rowsN, allV, allN, segStartD, countVD, countND, countAllD;
     DBuf<int32_t> surfList, surfSlot, surfCount;
-    DBuf<float> surfRatio;
+    DBuf<float> surfRatio, surfScore;
     DBuf<float> cgbuf;  // 10 vectors of n floats
     DBuf<double> scalV, scalN;
     int maxInnerAlloc = 0;
@@ -146,6 +150,10 @@ struct tg_handle {
     int removalsSinceSolve = 0;
     bool histValid = false;
     int lastSite = -1;                 // cell of the last removal
+    // Monte-Carlo choice: a stream drawing like rand() after srand(seed)
+    struct random_data rng {};
+    char rngState[128] = {};
+    bool rngSeeded = false;
     tg_learner* learner = nullptr;     // learned near-field start (learn.cu)
     int learnMode = 0;                 // bit 0 collect samples, bit 1 predict
     bool selValid = false;
@@ -204,6 +212,7 @@ struct tg_handle {
         s.slot = surfSlot.p;
         s.count = surfCount.p;
         s.ratio = surfRatio.p;
+        s.score = surfScore.p;
         s.capacity = n;
         return s;
     }
@@ -379,6 +388,7 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
         o.present = t.id >= 0;
         o.epsilon = t.epsilon;
         o.evap_field = t.evap_field;
+        o.evap_energy = t.evap_energy;
         o.charge_density = t.charge_density;
         o.phi = t.phi;
         o.removable = t.removable != 0;
@@ -606,6 +616,7 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(h->surfSlot.alloc(n));
     chk(h->surfCount.alloc(1));
     chk(h->surfRatio.alloc(n));
+    chk(h->surfScore.alloc(n));
     chk(h->cgbuf.alloc(10 * (size_t)n));
     if (e == cudaSuccess) chk(cudaMemset(h->cgbuf.p, 0, 10 * (size_t)n * sizeof(float)));
     chk(h->acc.alloc(16));
@@ -660,7 +671,7 @@ void tg_destroy(tg_handle* h) {
     h->diag32.release(); h->dtypes.release(); h->status.release(); h->rowsV.release(); h->rowsN.release();
     h->allV.release(); h->allN.release(); h->segStartD.release(); h->countVD.release(); h->countND.release();
     h->countAllD.release(); h->surfList.release(); h->surfSlot.release(); h->surfCount.release();
-    h->surfRatio.release(); h->cgbuf.release(); h->scalV.release(); h->scalN.release(); h->acc.release();
+    h->surfRatio.release(); h->surfScore.release(); h->cgbuf.release(); h->scalV.release(); h->scalN.release(); h->acc.release();
     h->keys.release(); h->result.release(); h->local.release(); h->localCount.release();
     h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
     h->stageImpact.release();
@@ -1072,20 +1083,27 @@ int tg_surface_init(tg_handle* h, int32_t vacuumId, int32_t* num) {
     return rc;
 }
 
-int tg_surface_select(tg_handle* h, tg_select_info* info) {
+int tg_surface_select(tg_handle* h, tg_select_info* info) { return tg_surface_select_mode(h, 0, 0.0f, info); }
+
+int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_select_info* info) {
     if (!h || !info) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: null argument");
     if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: surface not initialised");
-    unsigned long long k[3] = {0, 0, 0};
-    double sum = 0.0;
-    CK(cudaMemsetAsync(h->keys.p, 0, 3 * sizeof(unsigned long long), h->stream));
-    CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
-    launch_surface_select(h->dm(), h->sf(), h->surfSlots, h->keys.p, h->acc.p, h->stream);
-    CK(cudaMemcpyAsync(k, h->keys.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(&sum, h->acc.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (mode < 0 || mode > 3) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: probability mode 0..3");
+    if (mode == 1 && !(temperature > 0.0f))
+        return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: Boltzmann probabilities need a temperature > 0");
+    unsigned long long k[7] = {0, 0, 0, 0, 0, 0, 0};
+    double sums[2] = {0.0, 0.0};
+    CK(cudaMemsetAsync(h->keys.p, 0, 7 * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
+    launch_surface_select(h->dm(), h->sf(), h->surfSlots, mode, temperature, h->keys.p, h->acc.p, h->stream);
+    CK(cudaMemcpyAsync(k, h->keys.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(sums, h->acc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     int rc = sync_status(h, "tg_surface_select");
     if (rc != TG_OK) return rc;
     tg_select_info s{};
-    s.ratio_sum = sum;
+    s.prob_mode = mode;
+    s.ratio_sum = sums[0];
+    s.score_sum = sums[1];
     if (k[0] == 0ull) {
         s.candidate = -1;
         s.apex = -1;
@@ -1101,26 +1119,76 @@ int tg_surface_select(tg_handle* h, tg_select_info* info) {
         std::memcpy(v, &u, 4);
         return (int32_t)(~(uint32_t)key);
     };
-    float best, zmax;
-    s.candidate = unkey(k[0], &best);
+    float bestRatio, zmax;
+    const int bestRatioNode = unkey(k[0], &bestRatio);
     s.apex = unkey(k[1], &zmax);
-    s.best_ratio = best;
-    launch_surface_second(h->sf(), h->surfSlots, s.candidate, h->keys.p + 2, h->stream);
-    CK(cudaMemcpyAsync(&k[2], h->keys.p + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    s.best_ratio = bestRatio;
+    h->surfMinNode = (int32_t)(~(uint32_t)k[2]);
+    h->surfMaxNode = (int32_t)k[3] - 1;
+    // the probabilities are score / sum in float, as the reference normalises
+    const float fsum = (float)s.score_sum;
+    launch_surface_best(h->sf(), h->surfSlots, fsum, bestRatioNode, h->keys.p, h->stream);
+    CK(cudaMemcpyAsync(&k[4], h->keys.p + 4, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
     rc = sync_status(h, "tg_surface_select");
     if (rc != TG_OK) return rc;
-    float second = 0.0f;
-    if (k[2]) unkey(k[2], &second);
-    s.second_ratio = second;
-    s.probability = (float)(best / sum);
-    int cnt = 0;
-    // number of live entries = slots minus removed ones; count on host is
-    // not tracked, report slots (upper bound) unless exact count requested
-    cnt = h->surfSlots;
-    s.num_surface = cnt;
+    float bestP = 0.0f;
+    s.candidate = unkey(k[4], &bestP);
+    if ((uint32_t)(k[4] >> 32) == 0u) bestP = std::numeric_limits<float>::quiet_NaN();
+    launch_surface_second(h->sf(), h->surfSlots, fsum, s.candidate, bestRatioNode, h->keys.p, h->stream);
+    CK(cudaMemcpyAsync(&k[5], h->keys.p + 5, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    rc = sync_status(h, "tg_surface_select");
+    if (rc != TG_OK) return rc;
+    float secondP = 0.0f, secondRatio = 0.0f;
+    if (k[5]) unkey(k[5], &secondP);
+    if (k[6]) unkey(k[6], &secondRatio);
+    s.second_ratio = secondRatio;
+    s.best_probability = bestP;
+    s.second_probability = secondP;
+    s.probability = bestP;
+    s.num_surface = h->surfSlots;
     *info = s;
     h->sel = s;
     h->selValid = true;
+    return TG_OK;
+}
+
+int tg_surface_pick(tg_handle* h, double u, int32_t* node, float* probability) {
+    if (!h || !node) return fail(h, TG_ERR_ARGUMENT, "tg_surface_pick: null argument");
+    if (!h->selValid || h->sel.candidate < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_pick: no selection");
+    // the smallest node T with sum_{surface i <= T} p_i >= u, by bisection
+    // over node indices (the cumulative sum only grows at surface nodes)
+    const float fsum = (float)h->sel.score_sum;
+    auto prefix = [&](int upTo, double* out) -> int {
+        CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
+        launch_surface_prefix(h->sf(), h->surfSlots, fsum, upTo, h->acc.p, h->stream);
+        CK(cudaMemcpyAsync(out, h->acc.p, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        return sync_status(h, "tg_surface_pick");
+    };
+    int lo = h->surfMinNode, hi = h->surfMaxNode;
+    double cum = 0.0;
+    int rc = prefix(hi, &cum);
+    if (rc != TG_OK) return rc;
+    if (u > cum) {
+        lo = hi;  // past the end: the last cell
+    } else {
+        while (lo < hi) {
+            const int mid = lo + (hi - lo) / 2;
+            if ((rc = prefix(mid, &cum)) != TG_OK) return rc;
+            if (u > cum) lo = mid + 1;
+            else hi = mid;
+        }
+    }
+    *node = lo;
+    if (probability) {
+        int32_t slot = -1;
+        CK(cudaMemcpyAsync(&slot, h->surfSlot.p + lo, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        float sc = 0.0f;
+        CK(cudaStreamSynchronize(h->stream));
+        if (slot >= 0 && slot < h->surfSlots) {
+            CK(cudaMemcpy(&sc, h->surfScore.p + slot, sizeof(float), cudaMemcpyDeviceToHost));
+        }
+        *probability = sc / fsum;
+    }
     return TG_OK;
 }
 
@@ -1282,20 +1350,37 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
         int rc = tg_surface_init(h, o->vacuum_id, &ns);
         if (rc != TG_OK) return rc;
     }
+    if (o->prob_mode < 0 || o->prob_mode > 3 || o->choice_mode < 0 || o->choice_mode > 1)
+        return fail(h, TG_ERR_ARGUMENT, "tg_run_event: probability mode 0..3, choice mode 0..1");
     int rc = TG_OK;
-    if (!h->selValid) {
+    if (!h->selValid || h->sel.prob_mode != o->prob_mode) {
         tg_select_info s;
-        rc = tg_surface_select(h, &s);
+        rc = tg_surface_select_mode(h, o->prob_mode, o->temperature, &s);
         if (rc != TG_OK) return rc;
     }
     std::memset(rec, 0, sizeof(*rec));
     const tg_select_info sel = h->sel;
     if (sel.candidate < 0) return fail(h, TG_ERR_NO_SURFACE, "tg_run_event: empty surface");
-    // I) the candidate and its state before removal
-    const int node = sel.candidate;
+    // I) the candidate (evapMaximum, or evapMonteCarlo with the handle's
+    // stream) and its state before removal
+    int node = sel.candidate;
+    float probability = sel.probability;
+    if (o->choice_mode == 1) {
+        if (!h->rngSeeded) {
+            if (initstate_r(o->rng_seed, h->rngState, sizeof(h->rngState), &h->rng) != 0)
+                return fail(h, TG_ERR_HOST, "tg_run_event: random stream");
+            h->rngSeeded = true;
+        }
+        int32_t r = 0;
+        random_r(&h->rng, &r);
+        rc = tg_surface_pick(h, (double)r / (double)RAND_MAX, &node, &probability);
+        if (rc != TG_OK) return rc;
+    }
     rec->node = node;
     rec->type_id = h->h_type[node];
-    rec->probability = sel.probability;
+    rec->probability = probability;
+    rec->best_probability = sel.best_probability;
+    rec->second_probability = sel.second_probability;
     rec->best_ratio = sel.best_ratio;
     rec->second_ratio = sel.second_ratio;
     rec->scaling_reference = sel.best_ratio;
@@ -1352,7 +1437,7 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
     // IV) fields, probabilities and the next candidate
     {
         tg_select_info s;
-        rc = tg_surface_select(h, &s);
+        rc = tg_surface_select_mode(h, o->prob_mode, o->temperature, &s);
         if (rc != TG_OK && rc != TG_ERR_NO_SURFACE) return rc;
     }
     // V) ion flight of the removed atom, VI) state after removal

@@ -285,6 +285,8 @@ int tg_mesh_from_dump(const char* dumpFile, const char* configFile, tg_mesh** ou
 
 void tg_mesh_destroy(tg_mesh* m) { delete m; }
 
+float tg_mesh_temperature(const tg_mesh* m) { return m ? m->config.temperature : 0.0f; }
+
 int tg_mesh_describe(const tg_mesh* m, tg_mesh_desc* d, int32_t* nnz) {
     if (!m || !d) return mesh_fail("tg_mesh_describe: null argument");
     std::memset(d, 0, sizeof(*d));

@@ -70,6 +70,7 @@ struct Surface {
     int32_t* slot;         // [n] list slot of a surface node
     int32_t* count;        // slots in use (device counter)
     float* ratio;          // per slot |E|/E_evap of the last selection
+    float* score;          // per slot score of the probability mode (before normalisation)
     int capacity;
 };
 
@@ -135,10 +136,21 @@ void launch_local_set(const DevMesh& m, int node, int hops, int32_t* out, int32_
 
 // ---- surface (surface.cu) ----
 void launch_surface_init(const DevMesh& m, Surface sf, int vacuumId, cudaStream_t s);
-// fields, ratios, argmax key, apex key, ratio sum
-void launch_surface_select(const DevMesh& m, Surface sf, int slots, unsigned long long* keys, double* acc,
-                           cudaStream_t s);
-void launch_surface_second(Surface sf, int slots, int best, unsigned long long* key, cudaStream_t s);
+// fields, ratios and scores of probability mode `mode` (0 linear field,
+// 1 Boltzmann at `temperature`, 2 linear force, 3 Voronoi flux force);
+// keys[0] max ratio, keys[1] apex, keys[2] min / keys[3] max surface node;
+// acc[0] sum of ratios, acc[1] sum of scores
+void launch_surface_select(const DevMesh& m, Surface sf, int slots, int mode, float temperature,
+                           unsigned long long* keys, double* acc, cudaStream_t s);
+// keys[4] candidate (first maximum of score / sum), keys[5] runner-up
+// probability (excluding the candidate), keys[6] runner-up ratio
+// (excluding bestRatioNode)
+void launch_surface_best(Surface sf, int slots, float sum, int bestRatioNode, unsigned long long* keys,
+                         cudaStream_t s);
+void launch_surface_second(Surface sf, int slots, float sum, int candidate, int bestRatioNode,
+                           unsigned long long* keys, cudaStream_t s);
+// *acc = sum of score / sum over surface nodes <= upTo (Monte-Carlo choice)
+void launch_surface_prefix(Surface sf, int slots, float sum, int upTo, double* acc, cudaStream_t s);
 void launch_field_o1(const DevMesh& m, const int32_t* nodes, int count, double* out, cudaStream_t s);
 // evap_takeAway in one small kernel; result[0] = number of detached nodes,
 // result[1..] their indices

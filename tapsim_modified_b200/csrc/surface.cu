@@ -97,10 +97,103 @@ __global__ void k_surface_init(DevMesh m, Surface sf, int vacuumId) {
 // index order (evapMaximum's strict '<', surface_3d.cpp:427-428; apex,
 // surface_3d.cpp:171-190): the low word holds ~index so that ties resolve to
 // the smallest index.
-__global__ void k_surface_select(DevMesh m, Surface sf, int slots, unsigned long long* keys, double* acc) {
+// Grid_3d::Table::field_o2 (tapsim/grid_3d.cpp:993-1199): least-squares fit
+// of the second-order Taylor model (basis x, y, z, x^2/2, xy, xz, y^2/2, yz,
+// z^2/2) over all neighbours, solved by Gaussian elimination with partial
+// pivoting in FP64; E = -gradient, charge = -eps0 * Laplacian; zeros on hull
+// nodes.  Returns false when the system is singular.
+__device__ bool field_o2(const DevMesh& m, int i, double E[3], double* charge) {
+    E[0] = E[1] = E[2] = 0.0;
+    *charge = 0.0;
+    if (m.flags[i] & F_HULL) return true;
+    double a[81], b[9];
+    for (int k = 0; k < 81; k++) a[k] = 0.0;
+    for (int k = 0; k < 9; k++) b[k] = 0.0;
+    const double xi = m.xyz[3 * i], yi = m.xyz[3 * i + 1], zi = m.xyz[3 * i + 2];
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+        const int j = m.col[q];
+        const double x = (double)m.xyz[3 * j] - xi, y = (double)m.xyz[3 * j + 1] - yi, z = (double)m.xyz[3 * j + 2] - zi;
+        const double f[9] = {x, y, z, 0.5 * x * x, x * y, x * z, 0.5 * y * y, y * z, 0.5 * z * z};
+        const double dp = m.phi64[j] - m.phi64[i];
+        for (int r = 0; r < 9; r++) {
+            b[r] += dp * f[r];
+            for (int c = r; c < 9; c++) a[r * 9 + c] += f[r] * f[c];
+        }
+    }
+    for (int r = 0; r < 9; r++)
+        for (int c = 0; c < r; c++) a[r * 9 + c] = a[c * 9 + r];
+    for (int k = 0; k < 9; k++) {
+        int p = k;
+        for (int r = k + 1; r < 9; r++)
+            if (fabs(a[r * 9 + k]) > fabs(a[p * 9 + k])) p = r;
+        if (a[p * 9 + k] == 0.0) return false;
+        if (p != k) {
+            for (int c = 0; c < 9; c++) {
+                const double t = a[k * 9 + c];
+                a[k * 9 + c] = a[p * 9 + c];
+                a[p * 9 + c] = t;
+            }
+            const double t = b[k];
+            b[k] = b[p];
+            b[p] = t;
+        }
+        for (int r = k + 1; r < 9; r++) {
+            const double f = a[r * 9 + k] / a[k * 9 + k];
+            for (int c = k; c < 9; c++) a[r * 9 + c] -= f * a[k * 9 + c];
+            b[r] -= f * b[k];
+        }
+    }
+    for (int k = 8; k >= 0; k--) {
+        double acc = b[k];
+        for (int c = k + 1; c < 9; c++) acc -= a[k * 9 + c] * b[c];
+        b[k] = acc / a[k * 9 + k];
+    }
+    E[0] = -b[0];
+    E[1] = -b[1];
+    E[2] = -b[2];
+    *charge = -(b[3] + b[6] + b[8]) * kEpsilon0;
+    return b[0] == b[0] && b[1] == b[1] && b[2] == b[2];
+}
+
+// Score of a surface cell before normalisation, by probability mode
+// (Surface_3d::evap_compute_probabilities, surface_3d.cpp:222-399):
+// 0 |E|/E_evap; 1 Boltzmann exp(-(1 - |E|/E_evap) Q / (2 kB T)); 2 linear
+// force q |E| / E_evap^2 from field_o2; 3 Voronoi flux force |F| / A / E_evap^2
+// with F = sum_j -eps0 (phi_j - phi_i)^2 c_ij (1/eps_j - 1/eps_i) d_ij / |d_ij|^2
+// and A = sum_j c_ij |d_ij| (1/eps_i + 1/eps_j) / 2 (the capped face areas).
+__device__ double select_score(const DevMesh& m, int i, int mode, float temperature, double ratio) {
+    const DType& t = m.types[m.type[i]];
+    if (mode == 0) return ratio;
+    if (mode == 1) return exp(-(1.0 - ratio) * (double)t.evap_energy / ((double)temperature * 8.6173431e-5) / 2.0);
+    const double ef = (double)t.evap_field;
+    if (mode == 2) {
+        double E[3], q;
+        if (!field_o2(m, i, E, &q)) atomicOr(m.status, S_SINGULAR);
+        return q * sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]) / (ef * ef);
+    }
+    const double ei = 1.0 / (double)t.epsilon;
+    const double xi = m.xyz[3 * i], yi = m.xyz[3 * i + 1], zi = m.xyz[3 * i + 2];
+    double F0 = 0.0, F1 = 0.0, F2 = 0.0, area = 0.0;
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+        const int j = m.col[q];
+        const double ej = 1.0 / (double)m.types[m.type[j]].epsilon;
+        const double dp = m.phi64[j] - m.phi64[i];
+        const double v = -kEpsilon0 * dp * dp * m.c64[q] * (ej - ei);
+        const double dx = (double)m.xyz[3 * j] - xi, dy = (double)m.xyz[3 * j + 1] - yi, dz = (double)m.xyz[3 * j + 2] - zi;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        area += m.c64[q] * sqrt(d2) / 2.0 * (ei + ej);
+        F0 += dx / d2 * v;
+        F1 += dy / d2 * v;
+        F2 += dz / d2 * v;
+    }
+    return sqrt(F0 * F0 + F1 * F1 + F2 * F2) / area / (ef * ef);
+}
+
+__global__ void k_surface_select(DevMesh m, Surface sf, int slots, int mode, float temperature,
+                                 unsigned long long* keys, double* acc) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long kr = 0ull, kz = 0ull;
-    double r = 0.0;
+    unsigned long long kr = 0ull, kz = 0ull, kmin = 0ull, kmax = 0ull;
+    double r = 0.0, sc = 0.0;
     if (t < slots) {
         const int i = sf.list[t];
         if (i >= 0) {
@@ -111,26 +204,66 @@ __global__ void k_surface_select(DevMesh m, Surface sf, int slots, unsigned long
             sf.ratio[t] = ratio;
             if (!(ratio == ratio)) atomicOr(m.status, S_NAN);
             r = (double)ratio;
+            const float score = (float)select_score(m, i, mode, temperature, (double)ratio);
+            sf.score[t] = score;
+            sc = (double)score;
             const uint32_t low = ~(uint32_t)i;
             kr = ((unsigned long long)float_order_key(ratio) << 32) | low;
             kz = ((unsigned long long)float_order_key(m.xyz[3 * i + 2]) << 32) | low;
+            kmin = (unsigned long long)low;   // max of ~i = smallest node
+            kmax = (unsigned long long)(uint32_t)i + 1ull;
         } else {
             sf.ratio[t] = -1.0f;
+            sf.score[t] = 0.0f;
         }
     }
     block_max_atomic_u64<kBlock>(kr, &keys[0]);
     block_max_atomic_u64<kBlock>(kz, &keys[1]);
-    block_sum_atomic<kBlock>(r, &acc[0]);
+    block_max_atomic_u64<kBlock>(kmin, &keys[2]);
+    block_max_atomic_u64<kBlock>(kmax, &keys[3]);
+    block_sum2_atomic<kBlock>(r, sc, &acc[0], &acc[1]);
 }
 
-__global__ void k_surface_second(Surface sf, int slots, int best, unsigned long long* key) {
+// probability key: (p, ~node) so that the maximum is the first maximum in
+// ascending node order; a NaN probability (zero or NaN sum) keys as 0, so
+// the first surface cell wins, as evapMaximum keeps it (surface_3d.cpp:423-431)
+__device__ __forceinline__ unsigned long long prob_key(float p, int i) {
+    const uint32_t hi = (p == p) ? float_order_key(p) : 0u;
+    return ((unsigned long long)hi << 32) | (~(uint32_t)i);
+}
+
+__global__ void k_surface_best(Surface sf, int slots, float sum, unsigned long long* key) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long k = 0ull;
     if (t < slots) {
         const int i = sf.list[t];
-        if (i >= 0 && i != best) k = ((unsigned long long)float_order_key(sf.ratio[t]) << 32) | (~(uint32_t)i);
+        if (i >= 0) k = prob_key(sf.score[t] / sum, i);
     }
     block_max_atomic_u64<kBlock>(k, key);
+}
+
+__global__ void k_surface_second(Surface sf, int slots, float sum, int candidate, int bestRatioNode,
+                                 unsigned long long* keys) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long kp = 0ull, kr = 0ull;
+    if (t < slots) {
+        const int i = sf.list[t];
+        if (i >= 0 && i != candidate) kp = prob_key(sf.score[t] / sum, i);
+        if (i >= 0 && i != bestRatioNode) kr = ((unsigned long long)float_order_key(sf.ratio[t]) << 32) | (~(uint32_t)i);
+    }
+    block_max_atomic_u64<kBlock>(kp, &keys[0]);
+    block_max_atomic_u64<kBlock>(kr, &keys[1]);
+}
+
+// sum of the normalised probabilities of the surface nodes <= upTo
+__global__ void k_surface_prefix(Surface sf, int slots, float sum, int upTo, double* acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double p = 0.0;
+    if (t < slots) {
+        const int i = sf.list[t];
+        if (i >= 0 && i <= upTo) p = (double)(sf.score[t] / sum);
+    }
+    block_sum_atomic<kBlock>(p, acc);
 }
 
 // Coupling of the pair (n1, n2) as Grid_3d::Table::computeCoupling
@@ -403,12 +536,27 @@ inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 void launch_surface_init(const DevMesh& m, Surface sf, int vacuumId, cudaStream_t s) {
     { count_launch(); k_surface_init<<<blocks(m.n), kBlock, 0, s>>>(m, sf, vacuumId); }
 }
-void launch_surface_select(const DevMesh& m, Surface sf, int slots, unsigned long long* keys, double* acc,
-                           cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_surface_select<<<blocks(slots), kBlock, 0, s>>>(m, sf, slots, keys, acc); }
+void launch_surface_select(const DevMesh& m, Surface sf, int slots, int mode, float temperature,
+                           unsigned long long* keys, double* acc, cudaStream_t s) {
+    if (slots > 0) {
+        count_launch();
+        k_surface_select<<<blocks(slots), kBlock, 0, s>>>(m, sf, slots, mode, temperature, keys, acc);
+    }
 }
-void launch_surface_second(Surface sf, int slots, int best, unsigned long long* key, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_surface_second<<<blocks(slots), kBlock, 0, s>>>(sf, slots, best, key); }
+void launch_surface_best(Surface sf, int slots, float sum, int bestRatioNode, unsigned long long* keys,
+                         cudaStream_t s) {
+    (void)bestRatioNode;
+    if (slots > 0) { count_launch(); k_surface_best<<<blocks(slots), kBlock, 0, s>>>(sf, slots, sum, keys + 4); }
+}
+void launch_surface_second(Surface sf, int slots, float sum, int candidate, int bestRatioNode,
+                           unsigned long long* keys, cudaStream_t s) {
+    if (slots > 0) {
+        count_launch();
+        k_surface_second<<<blocks(slots), kBlock, 0, s>>>(sf, slots, sum, candidate, bestRatioNode, keys + 5);
+    }
+}
+void launch_surface_prefix(Surface sf, int slots, float sum, int upTo, double* acc, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_surface_prefix<<<blocks(slots), kBlock, 0, s>>>(sf, slots, sum, upTo, acc); }
 }
 void launch_field_o1(const DevMesh& m, const int32_t* nodes, int count, double* out, cudaStream_t s) {
     if (count > 0) { count_launch(); k_field_o1<<<blocks(count), kBlock, 0, s>>>(m, nodes, count, out); }

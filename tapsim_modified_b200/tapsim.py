@@ -81,6 +81,11 @@ class Mesh:
     def num_nodes(self) -> int:
         return self._desc.num_nodes
 
+    @property
+    def temperature(self) -> float:
+        """TEMPERATURE of the mesh's configuration [K]."""
+        return float(N.lib().tg_mesh_temperature(self._h))
+
     def arrays(self) -> dict:
         """Copies of the description arrays (node-file order)."""
         d = self._desc
@@ -216,12 +221,21 @@ class Grid:
         self._ck(N.lib().tg_surface_init(self._h, vacuum_id, C.byref(ns)))
         return ns.value
 
-    def select(self) -> N.tg_select_info:
+    def select(self, mode: int = 0, temperature: float = 0.0) -> N.tg_select_info:
+        """Probabilities of probability mode `mode` (0 linear field, 1
+        Boltzmann, 2 linear force, 3 Voronoi flux force) and evapMaximum's
+        candidate."""
         info = N.tg_select_info()
-        rc = N.lib().tg_surface_select(self._h, C.byref(info))
+        rc = N.lib().tg_surface_select_mode(self._h, mode, temperature, C.byref(info))
         if rc not in (N.TG_OK, N.TG_ERR_NO_SURFACE):
             self._ck(rc)
         return info
+
+    def pick(self, u: float) -> tuple[int, float]:
+        """evapMonteCarlo on the last selection for a uniform draw u."""
+        node, p = C.c_int32(), C.c_float()
+        self._ck(N.lib().tg_surface_pick(self._h, u, C.byref(node), C.byref(p)))
+        return node.value, p.value
 
     def surface(self):
         cnt = C.c_int32()
@@ -425,8 +439,13 @@ class EvaporationOptions:
         return self.values[k]
 
     def event_opts(self, vacuum_id: int, relax_mode: int, solve: N.tg_solve_opts | None = None,
-                   trace: bool = True, normal: bool = True, refresh_max_sweeps: int = 2_000_000) -> N.tg_event_opts:
+                   trace: bool = True, normal: bool = True, refresh_max_sweeps: int = 2_000_000,
+                   temperature: float = 0.0, rng_seed: int = 99) -> N.tg_event_opts:
         o = N.tg_event_opts()
+        o.prob_mode = self.i("METHOD_EVAPORATION_PROBABILITY")
+        o.choice_mode = self.i("METHOD_EVAPORATION_CHOICE")
+        o.temperature = temperature
+        o.rng_seed = rng_seed
         o.vacuum_id = vacuum_id
         o.relax_mode = relax_mode
         o.local_threshold = self.f("LOCAL_RELAXATION_ERROR_THRESHOLD")
@@ -466,7 +485,8 @@ class Evaporation:
         name = options.s("VACUUM_CELL_IDENTIFIER")
         self.vacuum_id = self._type_id_by_name(grid, name)
         self.evap_field = {k: v["evap_field"] for k, v in types.items()}
-        self.opts = options.event_opts(self.vacuum_id, relax_mode, solve, trace, normal)
+        self.opts = options.event_opts(self.vacuum_id, relax_mode, solve, trace, normal,
+                                       temperature=grid.mesh.temperature)
         self.voltage_queue: deque = deque()
         self.voltage_sum = 0.0
         self.queue_size = options.i("VOLTAGE_QUEUE_SIZE")
@@ -526,6 +546,7 @@ class Evaporation:
             "potentialAfter": rec.phi_after, "fieldAfter": tuple(rec.field_after), "normal": tuple(rec.normal),
             "apex": tuple(rec.apex), "status": imp.status, "steps": imp.steps, "detached": rec.detached,
             "relax_iterations": rec.relax_iterations, "rel_residual": rec.rel_residual,
+            "best_probability": rec.best_probability, "second_probability": rec.second_probability,
         }
 
 

@@ -18,6 +18,16 @@ maximum-probability choice).  Outputs:
                      relaxation
     ref_events.txt   one line per event (ref_harness evap columns)
     ref_phi_events.bin.gz  float32 potentials after each event
+
+With `--modes` it adds, from the same dump, 15 events of each other
+probability / choice mode of the reference (surface_3d.cpp:220-449):
+
+    tip_t300.cfg                       tip.cfg with TEMPERATURE = 300 (Boltzmann; at
+                                       1 V the field ratios are ~3e-3, and below ~70 K
+                                       the reference's float exponentials underflow)
+    ref_events_prob{P}_choice{C}.txt   ref_harness evap lines, P in 1..3 with
+                                       choice 0, and P = 0 with choice 1
+                                       (Monte-Carlo, rand() seeded 99)
 """
 from __future__ import annotations
 
@@ -40,6 +50,8 @@ HARNESS = ROOT / "oracle" / "_ref" / "ref_harness"
 TIP = dict(cap_radius=1.5e-9, shank_length=2.0e-9, half_angle_deg=0.0, fine_shell=0.6e-9,
            box_half_width=10e-9, box_height=40e-9, seed=7)
 N_EVENTS = 40
+MODE_EVENTS = 15
+MODES = [(1, 0), (2, 0), (3, 0), (0, 1)]
 
 
 def main():
@@ -69,5 +81,28 @@ def main():
     print("nodes", mesh.num_nodes, "written to", HERE)
 
 
+def modes():
+    if not HARNESS.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    cfg = (HERE / "tip.cfg").read_text().replace("TEMPERATURE = 0\n", "TEMPERATURE = 300\n", 1)
+    assert "TEMPERATURE = 300" in cfg
+    (HERE / "tip_t300.cfg").write_text(cfg)
+    tmp = HERE / "_tmp"
+    tmp.mkdir(exist_ok=True)
+    with gzip.open(HERE / "ref_mesh.dump.gz", "rb") as f, open(tmp / "ref.dump", "wb") as g:
+        shutil.copyfileobj(f, g)
+    base = (HERE / "oracle.ini").read_text()
+    for prob, choice in MODES:
+        ini = base.replace("METHOD_EVAPORATION_PROBABILITY = 0", f"METHOD_EVAPORATION_PROBABILITY = {prob}")
+        ini = ini.replace("METHOD_EVAPORATION_CHOICE = 0", f"METHOD_EVAPORATION_CHOICE = {choice}")
+        (tmp / "mode.ini").write_text(ini)
+        out = HERE / f"ref_events_prob{prob}_choice{choice}.txt"
+        subprocess.run([str(HARNESS), "evap", str(HERE / "tip_t300.cfg"), "-", str(tmp / "mode.ini"),
+                        str(MODE_EVENTS), str(out), "--dump", str(tmp / "ref.dump"), "--threads", "1"],
+                       check=True, capture_output=True)
+        print("mode", prob, choice, "->", out.name)
+    shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
-    main()
+    modes() if "--modes" in sys.argv else main()
