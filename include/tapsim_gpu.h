@@ -219,6 +219,9 @@ typedef struct {
     int32_t max_steps;          /* iteration bound per ion */
     int32_t stepper_limit;      /* trial steps per accepted step */
     int32_t walk_limit;         /* tetrahedra per point location */
+    int32_t integrator;         /* TRAJECTORY_INTEGRATOR_TYPE: 0 Euler, 1 Cash-Karp (the reference's default) */
+    int32_t stepper;            /* TRAJECTORY_STEPPER_TYPE: 0 none, 1 error-restricted (default),
+                                   2 geometry-restricted, 3 adaptive (trajectory_3d.cpp:358-532) */
 } tg_trace_opts;
 typedef struct {
     float stop[3];              /* impact after extrapolation to the top plane [m] */
@@ -264,6 +267,10 @@ typedef struct {
     int32_t choice_mode;
     float temperature;
     uint32_t rng_seed;
+    /* !TRAJECTORY_NO_INITIAL_VELOCITY: draw the ion's initial velocity as
+     * evap_initialVelocity does (surface_3d.cpp:472-503) from the same
+     * stream; 0 starts it at rest (the reference's default) */
+    int32_t initial_velocity;
 } tg_event_opts;
 typedef struct {
     int32_t node;

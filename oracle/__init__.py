@@ -85,6 +85,10 @@ def lib():
         L.orc_trace.restype = None
         L.orc_trace.argtypes = [P, C.c_void_p, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32,
                                 C.c_int32, C.c_double, C.POINTER(orc_impact)]
+        L.orc_trace_ext.restype = None
+        L.orc_trace_ext.argtypes = [P, C.c_void_p, C.c_void_p, C.c_double, C.c_int32, C.c_double, C.c_double,
+                                    C.c_double, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
+                                    C.POINTER(orc_impact)]
         L.orc_potential_at.restype = C.c_double
         L.orc_potential_at.argtypes = [P, C.c_void_p, C.c_int32]
         _lib = L
@@ -206,6 +210,15 @@ class Oracle:
         out = orc_impact()
         self.L.orc_trace(C.byref(self.m), _p(s), qm, int(tet_guess), dt0, dt_min, tol, max_steps, stepper_limit,
                          self.top_z, C.byref(out))
+        return out
+
+    def trace_ext(self, start, vel, qm, tet_guess, integrator=1, stepper=1, dt0=1e-14, dt_min=1e-16, tol=1e-6,
+                  max_steps=200000, stepper_limit=1000) -> orc_impact:
+        s = np.ascontiguousarray(start, np.float64)
+        v = np.ascontiguousarray(vel, np.float64)
+        out = orc_impact()
+        self.L.orc_trace_ext(C.byref(self.m), _p(s), _p(v), qm, int(tet_guess), dt0, dt_min, tol, max_steps,
+                             stepper_limit, self.top_z, int(integrator), int(stepper), C.byref(out))
         return out
 
     def potential_at(self, p, tet_guess) -> float:

@@ -517,8 +517,33 @@ double orc_potential_at(const orc_mesh* m, const double p[3], int32_t guess) {
 }
 
 /* Trajectory_3d (trajectory_3d.cpp:130-209, 303-332, 358-425, 583-676) */
+/* tetrahedron t2 shares a vertex with t1 (t1's entry in the set that
+ * Geometry_3d::Table::adjacentTetrahedra, geometry_3d.cpp:1046-1096, builds
+ * by a walk over face neighbours; t1 itself is excluded) */
+static int shares_vertex(const orc_mesh* m, int t1, int t2) {
+    if (t2 < 0 || t2 == t1) return 0;
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++)
+            if (m->tet_v[4 * t1 + a] == m->tet_v[4 * t2 + b]) return 1;
+    return 0;
+}
+
+/* Geometry_3d::Table::isBoundaryTetrahedron (geometry_3d.cpp:819-828) */
+static int boundary_tet(const orc_mesh* m, int t) {
+    for (int a = 0; a < 4; a++)
+        if (m->hull[m->tet_v[4 * t + a]]) return 1;
+    return 0;
+}
+
 void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t guess, double dt0, double dt_min,
                double tol, int32_t max_steps, int32_t stepper_limit, double top_z, orc_impact* out) {
+    const double v0[3] = {0.0, 0.0, 0.0};
+    orc_trace_ext(m, start, v0, qm, guess, dt0, dt_min, tol, max_steps, stepper_limit, top_z, 1, 1, out);
+}
+
+void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t guess,
+                   double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
+                   int32_t integrator, int32_t stepper, orc_impact* out) {
     static const double B[6][5] = {{0, 0, 0, 0, 0},
                                    {1.0 / 5.0, 0, 0, 0, 0},
                                    {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
@@ -527,7 +552,7 @@ void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t gues
                                    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
     static const double C5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
     static const double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 0.25};
-    double x[3] = {start[0], start[1], start[2]}, v[3] = {0, 0, 0};
+    double x[3] = {start[0], start[1], start[2]}, v[3] = {vel[0], vel[1], vel[2]};
     double time = 0.0;
     memset(out, 0, sizeof(*out));
     int tet = locate(m, x, guess);
@@ -548,45 +573,82 @@ void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t gues
         double dt = dt0;
         for (int it = 0; it < max_steps; it++) {
             double nx[3], nv[3], used = dt;
-            int accepted = 0;
+            int accepted = 0, nt = -1;
             for (int tries = 0; tries < stepper_limit; tries++) {
                 if (dt < dt_min) dt = dt_min;
                 used = dt;
-                double dx[6][3], dv[6][3];
-                for (int s = 0; s < 6; s++) {
-                    double ps[3], vs[3];
+                double rel = 0.0;
+                if (integrator == 0) {
+                    /* o1_integrator (trajectory_3d.cpp:560-581): Euler step;
+                     * error = next state times dt^2 */
+                    double E[3];
+                    field_at(m, x, tet, E);
                     for (int d = 0; d < 3; d++) {
-                        ps[d] = x[d];
-                        vs[d] = v[d];
-                        for (int j = 0; j < s; j++) {
-                            ps[d] += B[s][j] * dx[j][d];
-                            vs[d] += B[s][j] * dv[j][d];
+                        nv[d] = v[d] + dt * E[d] * qm;
+                        nx[d] = x[d] + dt * v[d];
+                    }
+                    for (int d = 0; d < 3; d++) {
+                        if (nx[d] != 0.0 && dt * dt > rel) rel = dt * dt;
+                        if (nv[d] != 0.0 && dt * dt > rel) rel = dt * dt;
+                    }
+                } else {
+                    double dx[6][3], dv[6][3];
+                    for (int s = 0; s < 6; s++) {
+                        double ps[3], vs[3];
+                        for (int d = 0; d < 3; d++) {
+                            ps[d] = x[d];
+                            vs[d] = v[d];
+                            for (int j = 0; j < s; j++) {
+                                ps[d] += B[s][j] * dx[j][d];
+                                vs[d] += B[s][j] * dv[j][d];
+                            }
+                        }
+                        double E[3];
+                        field_at(m, ps, tet, E);
+                        for (int d = 0; d < 3; d++) {
+                            dv[s][d] = E[d] * qm * dt;
+                            dx[s][d] = vs[d] * dt;
                         }
                     }
-                    double E[3];
-                    field_at(m, ps, tet, E);
+                    double ex[3], ev[3];
                     for (int d = 0; d < 3; d++) {
-                        dv[s][d] = E[d] * qm * dt;
-                        dx[s][d] = vs[d] * dt;
+                        nx[d] = x[d];
+                        nv[d] = v[d];
+                        ex[d] = ev[d] = 0.0;
+                        for (int s = 0; s < 6; s++) {
+                            nx[d] += C5[s] * dx[s][d];
+                            nv[d] += C5[s] * dv[s][d];
+                            ex[d] += (C5[s] - C4[s]) * dx[s][d];
+                            ev[d] += (C5[s] - C4[s]) * dv[s][d];
+                        }
+                    }
+                    for (int d = 0; d < 3; d++) {
+                        if (nx[d] != 0.0 && fabs(ex[d] / nx[d]) > rel) rel = fabs(ex[d] / nx[d]);
+                        if (nv[d] != 0.0 && fabs(ev[d] / nv[d]) > rel) rel = fabs(ev[d] / nv[d]);
                     }
                 }
-                double ex[3], ev[3];
-                for (int d = 0; d < 3; d++) {
-                    nx[d] = x[d];
-                    nv[d] = v[d];
-                    ex[d] = ev[d] = 0.0;
-                    for (int s = 0; s < 6; s++) {
-                        nx[d] += C5[s] * dx[s][d];
-                        nv[d] += C5[s] * dv[s][d];
-                        ex[d] += (C5[s] - C4[s]) * dx[s][d];
-                        ev[d] += (C5[s] - C4[s]) * dv[s][d];
+                nt = locate(m, nx, tet);
+                if (stepper == 0) { /* NONE: every step is taken */
+                    accepted = 1;
+                    break;
+                }
+                if (stepper == 2) { /* geometryRestricted_stepper (trajectory_3d.cpp:427-452) */
+                    if (nt < 0 && boundary_tet(m, tet)) { accepted = 1; break; }
+                    if (shares_vertex(m, tet, nt)) { accepted = 1; break; }
+                    if (nt == tet) {
+                        dt *= 1.1;
+                    } else {
+                        if (dt == dt_min) { accepted = 1; break; }
+                        dt *= 0.9;
                     }
+                    continue;
                 }
-                double rel = 0.0;
-                for (int d = 0; d < 3; d++) {
-                    if (nx[d] != 0.0 && fabs(ex[d] / nx[d]) > rel) rel = fabs(ex[d] / nx[d]);
-                    if (nv[d] != 0.0 && fabs(ev[d] / nv[d]) > rel) rel = fabs(ev[d] / nv[d]);
+                if (stepper == 3 && nt >= 0 && nt != tet && !shares_vertex(m, tet, nt)) {
+                    /* adaptive_stepper (trajectory_3d.cpp:454-532): leaving the star */
+                    dt *= 0.1;
+                    continue;
                 }
+                /* errorRestricted_stepper (trajectory_3d.cpp:358-425) */
                 if (rel < tol || dt == dt_min) {
                     if (rel != 0.0) {
                         const double tmp = dt * pow(tol / rel, 0.25) * 0.9;
@@ -602,7 +664,6 @@ void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t gues
                 status = 2;
                 break;
             }
-            const int nt = locate(m, nx, tet);
             out->steps++;
             if (nt < 0) {
                 out->last_tet = tet;

@@ -86,6 +86,12 @@ typedef struct {
 } orc_impact;
 void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t tet_guess, double dt0, double dt_min,
                double tol, int32_t max_steps, int32_t stepper_limit, double top_z, orc_impact* out);
+/* the same with an initial velocity, TRAJECTORY_INTEGRATOR_TYPE (0 Euler,
+ * 1 Cash-Karp) and TRAJECTORY_STEPPER_TYPE (0 none, 1 error-restricted,
+ * 2 geometry-restricted, 3 adaptive) */
+void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t tet_guess,
+                   double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
+                   int32_t integrator, int32_t stepper, orc_impact* out);
 /* Grid_3d::potential(pos, tet) */
 double orc_potential_at(const orc_mesh* m, const double p[3], int32_t tet_guess);
 

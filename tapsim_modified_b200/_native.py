@@ -56,7 +56,7 @@ class tg_select_info(C.Structure):
 
 class tg_trace_opts(C.Structure):
     _fields_ = [("time_step", C.c_double), ("min_time_step", C.c_double), ("error_threshold", C.c_double),
-                ("max_steps", C.c_int32), ("stepper_limit", C.c_int32), ("walk_limit", C.c_int32)]
+                ("max_steps", C.c_int32), ("stepper_limit", C.c_int32), ("walk_limit", C.c_int32), ("integrator", C.c_int32), ("stepper", C.c_int32)]
 
 
 class tg_impact(C.Structure):
@@ -71,7 +71,7 @@ class tg_event_opts(C.Structure):
                 ("refresh_cycle", C.c_int32), ("refresh_queue", C.c_int32), ("refresh_max_sweeps", C.c_int64),
                 ("solve", tg_solve_opts), ("trace", tg_trace_opts), ("trace_enabled", C.c_int32),
                 ("normal_enabled", C.c_int32), ("prob_mode", C.c_int32), ("choice_mode", C.c_int32),
-                ("temperature", C.c_float), ("rng_seed", C.c_uint32)]
+                ("temperature", C.c_float), ("rng_seed", C.c_uint32), ("initial_velocity", C.c_int32)]
 
 
 class tg_event_record(C.Structure):

@@ -384,6 +384,76 @@ __device__ double potential_at(const DevMesh& m, const double* phi, V3 p, int t)
     return w[0] * phi[v[0]] + w[1] * phi[v[1]] + w[2] * phi[v[2]] + w[3] * phi[v[3]];
 }
 
+// Tetrahedron t2 shares a vertex with t1 and is not t1: membership of the
+// set Geometry_3d::Table::adjacentTetrahedra (geometry_3d.cpp:1046-1096)
+// builds for t1 by a walk over face neighbours.
+__device__ bool shares_vertex(const DevMesh& m, int t1, int t2) {
+    if (t2 < 0 || t2 == t1) return false;
+    for (int a = 0; a < 4; a++) {
+        const int va = m.tet_v[4 * t1 + a];
+        for (int b = 0; b < 4; b++)
+            if (va == m.tet_v[4 * t2 + b]) return true;
+    }
+    return false;
+}
+
+// Geometry_3d::Table::isBoundaryTetrahedron (geometry_3d.cpp:819-828)
+__device__ bool boundary_tet(const DevMesh& m, int t) {
+    for (int a = 0; a < 4; a++)
+        if (m.flags[m.tet_v[4 * t + a]] & F_HULL) return true;
+    return false;
+}
+
+// The accept / retry rule of the steppers other than the error-restricted
+// one of the main path: 0 NONE takes every step; 2 geometryRestricted_stepper
+// (trajectory_3d.cpp:427-452) accepts a point in a tetrahedron sharing a
+// vertex with the current one (or outside the mesh from a boundary
+// tetrahedron), grows dt by 1.1 while the point stays in the current
+// tetrahedron and shrinks it by 0.9 otherwise; 3 adaptive_stepper
+// (:454-532) shrinks dt by 0.1 when the point leaves that set, then applies
+// the error rule.  Returns 1 to accept, 0 to retry with the updated dt; *nt
+// is the located tetrahedron when *located.
+__device__ __forceinline__ int stepper_verdict(const DevMesh& m, TetCache& fc, const TraceParams& tp, V3 nx, int tet,
+                                            int& cur, unsigned& rot, double rel, double* dt, int* nt, bool* located) {
+    *located = false;
+    if (tp.stepper == 0) return 1;
+    if (tp.stepper == 2 || tp.stepper == 3) {
+        const int nsl = locate_cached(m, fc, nx, cur, tp.walk_limit, rot);
+        *nt = nsl >= 0 ? fc.a.t : nsl;
+        if (*nt == -2) atomicOr(m.status, S_WALK_LIMIT);
+        if (*nt >= 0) cur = *nt;
+        *located = true;
+        if (tp.stepper == 2) {
+            if (*nt < 0 && boundary_tet(m, tet)) return 1;
+            if (shares_vertex(m, tet, *nt)) return 1;
+            if (*nt == tet) {
+                *dt *= 1.1;
+            } else {
+                if (*dt == tp.dt_min) return 1;
+                *dt *= 0.9;
+            }
+            *located = false;
+            return 0;
+        }
+        if (*nt >= 0 && *nt != tet && !shares_vertex(m, tet, *nt)) {
+            *dt *= 0.1;
+            *located = false;
+            return 0;
+        }
+    }
+    if (rel < tp.tol || *dt == tp.dt_min) {
+        if (rel != 0.0) {
+            const double tmp = *dt * pow(tp.tol / rel, 0.25) * 0.9;
+            if (tmp < *dt) *dt *= 1.1; else *dt = tmp;
+        }
+        return 1;
+    }
+    const double tmp = *dt * pow(tp.tol / rel, 0.25) * 0.9;
+    if (tmp > *dt) *dt *= 0.9; else *dt = tmp;
+    *located = false;
+    return 0;
+}
+
 // One ion from x0 (velocity v0, charge/mass k) into *out.
 __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k, int guessTet, const TraceParams& tp,
                                           unsigned rot, ImpactOut* out) {
@@ -429,9 +499,28 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
             V3 nx, nv;
             double used = dt;
             bool accepted = false;
+            bool located = false;  // the accepted trial point is already located (steppers 2, 3)
+            int nt = -1;
             for (int tries = 0; tries < tp.stepper_limit; tries++) {
                 if (dt < tp.dt_min) dt = tp.dt_min;
                 used = dt;
+                if (tp.integrator == 0) {
+                    // o1_integrator (trajectory_3d.cpp:560-581): Euler; the
+                    // error estimate is the next state times dt^2
+                    V3 E;
+                    if (!fast_field(m, fc, x, cur, tp.walk_limit, rot, &E, &cur)) atomicOr(m.status, S_WALK_LIMIT);
+                    nv = V3{v.x + dt * E.x * k, v.y + dt * E.y * k, v.z + dt * E.z * k};
+                    nx = V3{x.x + dt * v.x, x.y + dt * v.y, x.z + dt * v.z};
+                    const bool any = nx.x != 0.0 || nx.y != 0.0 || nx.z != 0.0 || nv.x != 0.0 || nv.y != 0.0 ||
+                                     nv.z != 0.0;
+                    const double rel = any ? dt * dt : 0.0;
+                    const int verdict = stepper_verdict(m, fc, tp, nx, tet, cur, rot, rel, &dt, &nt, &located);
+                    if (verdict > 0) {
+                        accepted = true;
+                        break;
+                    }
+                    continue;
+                }
                 V3 dxs[6], dvs[6];
                 bool walkOk = true;
 #pragma unroll
@@ -465,6 +554,14 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                 if (nv.x != 0.0) rel = fmax(rel, fabs(evv.x / nv.x));
                 if (nv.y != 0.0) rel = fmax(rel, fabs(evv.y / nv.y));
                 if (nv.z != 0.0) rel = fmax(rel, fabs(evv.z / nv.z));
+                if (tp.stepper != 1) {
+                    const int verdict = stepper_verdict(m, fc, tp, nx, tet, cur, rot, rel, &dt, &nt, &located);
+                    if (verdict > 0) {
+                        accepted = true;
+                        break;
+                    }
+                    continue;
+                }
                 if (rel < tp.tol || dt == tp.dt_min) {
                     if (rel != 0.0) {
                         const double tmp = dt * pow(tp.tol / rel, 0.25) * 0.9;
@@ -480,9 +577,11 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                 status = 2;  // STEPPER_LIMIT_PASSED
                 break;
             }
-            const int nsl = locate_cached(m, fc, nx, cur, tp.walk_limit, rot);
-            const int nt = nsl >= 0 ? fc.a.t : nsl;
-            if (nt == -2) atomicOr(m.status, S_WALK_LIMIT);
+            if (!located) {
+                const int nsl = locate_cached(m, fc, nx, cur, tp.walk_limit, rot);
+                nt = nsl >= 0 ? fc.a.t : nsl;
+                if (nt == -2) atomicOr(m.status, S_WALK_LIMIT);
+            }
             res.steps++;
             if (nt < 0) {
                 // left the mesh: the previous point is the last inside it
@@ -530,10 +629,10 @@ __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* v
 }
 
 // A single ion from rest, its start passed by value (no staging copy)
-__global__ void k_trace_one(DevMesh m, float x, float y, float z, float qm, int guess, TraceParams tp,
-                            ImpactOut* out) {
+__global__ void k_trace_one(DevMesh m, float x, float y, float z, float vx, float vy, float vz, float qm, int guess,
+                            TraceParams tp, ImpactOut* out) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    trace_ion(m, V3{x, y, z}, V3{0, 0, 0}, qm, guess, tp, 0u, out);
+    trace_ion(m, V3{x, y, z}, V3{vx, vy, vz}, qm, guess, tp, 0u, out);
 }
 
 __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t* guess, int limit, float* out) {
@@ -562,10 +661,10 @@ void launch_vertex_fields(const DevMesh& m, cudaStream_t s) {
         k_vertex_fields<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m);
     }
 }
-void launch_trace_one(const DevMesh& m, const float start[3], float qm, int guess, TraceParams tp, ImpactOut* out,
-                      cudaStream_t s) {
+void launch_trace_one(const DevMesh& m, const float start[3], const float vel[3], float qm, int guess, TraceParams tp,
+                      ImpactOut* out, cudaStream_t s) {
     count_launch();
-    k_trace_one<<<1, 32, 0, s>>>(m, start[0], start[1], start[2], qm, guess, tp, out);
+    k_trace_one<<<1, 32, 0, s>>>(m, start[0], start[1], start[2], vel[0], vel[1], vel[2], qm, guess, tp, out);
 }
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit, float* out,
                          cudaStream_t s) {

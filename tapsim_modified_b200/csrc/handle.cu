@@ -1290,6 +1290,8 @@ static TraceParams trace_params(const tg_handle* h, const tg_trace_opts* o) {
     tp.stepper_limit = o->stepper_limit;
     tp.walk_limit = o->walk_limit;
     tp.top_z = h->top_z;
+    tp.integrator = o->integrator;
+    tp.stepper = o->stepper;
     return tp;
 }
 
@@ -1448,6 +1450,30 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
         const float mass = removed.mass * 1.660538782e-27f;
         const float qm = charge / mass;
         const int32_t guess = h->h_node_tet.empty() ? 0 : std::max(0, h->h_node_tet[node]);
+        float vel[3] = {0.0f, 0.0f, 0.0f};
+        if (o->initial_velocity) {
+            // evap_initialVelocity (surface_3d.cpp:472-503): kinetic energies
+            // split by two uniform draws, a random sign per component
+            if (!h->rngSeeded) {
+                if (initstate_r(o->rng_seed, h->rngState, sizeof(h->rngState), &h->rng) != 0)
+                    return fail(h, TG_ERR_HOST, "tg_run_event: random stream");
+                h->rngSeeded = true;
+            }
+            auto draw = [&]() {
+                int32_t r = 0;
+                random_r(&h->rng, &r);
+                return r;
+            };
+            const double vmax = 2.0 * 1.3806504e-23 * (double)o->temperature / (double)removed.mass / 1.660538782e-27;
+            float e2[3];
+            e2[0] = (float)((double)draw() / RAND_MAX) * (float)vmax;
+            e2[1] = (float)((double)draw() / RAND_MAX) * ((float)vmax - e2[0]);
+            e2[2] = (float)vmax - e2[0] - e2[1];
+            for (int c = 0; c < 3; c++) {
+                vel[c] = std::sqrt(std::max(e2[c], 0.0f));
+                if (draw() % 2) vel[c] = -vel[c];
+            }
+        }
         if (asyncImpact) {
             if (guess >= h->ntets || !h->tetpack.p) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: no tetrahedra");
             // the previous flight must be done with the snapshots before the
@@ -1458,11 +1484,11 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
             CK(cudaStreamWaitEvent(h->traceStream, h->evFields, 0));
             DevMesh mt = h->dm();
             mt.status = h->statusTrace.p;
-            launch_trace_one(mt, start, qm, guess, trace_params(h, &o->trace), asyncImpact, h->traceStream);
+            launch_trace_one(mt, start, vel, qm, guess, trace_params(h, &o->trace), asyncImpact, h->traceStream);
             CK(cudaGetLastError());
             CK(cudaEventRecord(h->evTraceDone, h->traceStream));
         } else {
-            rc = tg_trace(h, 1, start, nullptr, &qm, &guess, &o->trace, &rec->impact);
+            rc = tg_trace(h, 1, start, o->initial_velocity ? vel : nullptr, &qm, &guess, &o->trace, &rec->impact);
             if (rc != TG_OK) return rc;
         }
     }

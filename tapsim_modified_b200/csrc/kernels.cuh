@@ -164,6 +164,8 @@ struct TraceParams {
     double dt0, dt_min, tol;
     int max_steps, stepper_limit, walk_limit;
     float top_z;
+    int integrator;  // 0 Euler, 1 Cash-Karp (TRAJECTORY_INTEGRATOR_TYPE)
+    int stepper;     // 0 none, 1 error-restricted, 2 geometry-restricted, 3 adaptive
 };
 struct ImpactOut {
     float stop[3];
@@ -181,8 +183,8 @@ void launch_vertex_fields(const DevMesh& m, cudaStream_t s);
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s);
 // one ion from rest at start (values passed to the kernel)
-void launch_trace_one(const DevMesh& m, const float start[3], float qm, int guess, TraceParams tp, ImpactOut* out,
-                      cudaStream_t s);
+void launch_trace_one(const DevMesh& m, const float start[3], const float vel[3], float qm, int guess, TraceParams tp,
+                      ImpactOut* out, cudaStream_t s);
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit,
                          float* out, cudaStream_t s);
 

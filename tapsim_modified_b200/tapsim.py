@@ -127,8 +127,12 @@ class Mesh:
 
 
 def trace_opts(time_step=1e-14, min_time_step=1e-16, error_threshold=1e-6, max_steps=100000, stepper_limit=200,
-               walk_limit=100000) -> N.tg_trace_opts:
-    return N.tg_trace_opts(time_step, min_time_step, error_threshold, max_steps, stepper_limit, walk_limit)
+               walk_limit=100000, integrator=1, stepper=1) -> N.tg_trace_opts:
+    """Trajectory options; integrator / stepper are TRAJECTORY_INTEGRATOR_TYPE
+    (0 Euler, 1 Cash-Karp) and TRAJECTORY_STEPPER_TYPE (0 none, 1 error-
+    restricted, 2 geometry-restricted, 3 adaptive)."""
+    return N.tg_trace_opts(time_step, min_time_step, error_threshold, max_steps, stepper_limit, walk_limit,
+                           integrator, stepper)
 
 
 def solve_opts(rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4, warm_start=0) -> N.tg_solve_opts:
@@ -460,7 +464,9 @@ class EvaporationOptions:
         o.refresh_max_sweeps = refresh_max_sweeps
         o.solve = solve if solve is not None else solve_opts()
         o.trace = trace_opts(self.f("TRAJECTORY_INITIAL_TIME_STEP"), self.f("TRAJECTORY_MINIMUM_TIME_STEP"),
-                             self.f("TRAJECTORY_ERROR_THRESHOLD"))
+                             self.f("TRAJECTORY_ERROR_THRESHOLD"), integrator=self.i("TRAJECTORY_INTEGRATOR_TYPE"),
+                             stepper=self.i("TRAJECTORY_STEPPER_TYPE"))
+        o.initial_velocity = 0 if self.i("TRAJECTORY_NO_INITIAL_VELOCITY") else 1
         o.trace_enabled = int(trace)
         o.normal_enabled = int(normal)
         return o

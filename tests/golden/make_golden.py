@@ -28,6 +28,8 @@ probability / choice mode of the reference (surface_3d.cpp:220-449):
     ref_events_prob{P}_choice{C}.txt   ref_harness evap lines, P in 1..3 with
                                        choice 0, and P = 0 with choice 1
                                        (Monte-Carlo, rand() seeded 99)
+    ref_events_int{I}_step{S}.txt      8 events with TRAJECTORY_INTEGRATOR_TYPE I and
+                                       TRAJECTORY_STEPPER_TYPE S: (1, 2), (1, 3), (0, 1)
 """
 from __future__ import annotations
 
@@ -52,6 +54,8 @@ TIP = dict(cap_radius=1.5e-9, shank_length=2.0e-9, half_angle_deg=0.0, fine_shel
 N_EVENTS = 40
 MODE_EVENTS = 15
 MODES = [(1, 0), (2, 0), (3, 0), (0, 1)]
+TRAJECTORY_MODES = [(1, 2), (1, 3), (0, 1)]
+TRAJECTORY_EVENTS = 8
 
 
 def main():
@@ -101,6 +105,15 @@ def modes():
                         str(MODE_EVENTS), str(out), "--dump", str(tmp / "ref.dump"), "--threads", "1"],
                        check=True, capture_output=True)
         print("mode", prob, choice, "->", out.name)
+    for integ, step in TRAJECTORY_MODES:
+        ini = base.replace("TRAJECTORY_INTEGRATOR_TYPE = 1", f"TRAJECTORY_INTEGRATOR_TYPE = {integ}")
+        ini = ini.replace("TRAJECTORY_STEPPER_TYPE = 1", f"TRAJECTORY_STEPPER_TYPE = {step}")
+        (tmp / "traj.ini").write_text(ini)
+        out = HERE / f"ref_events_int{integ}_step{step}.txt"
+        subprocess.run([str(HARNESS), "evap", str(HERE / "tip.cfg"), "-", str(tmp / "traj.ini"),
+                        str(TRAJECTORY_EVENTS), str(out), "--dump", str(tmp / "ref.dump"), "--threads", "1"],
+                       check=True, capture_output=True)
+        print("trajectory", integ, step, "->", out.name)
     shutil.rmtree(tmp)
 
 

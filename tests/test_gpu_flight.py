@@ -97,3 +97,41 @@ def test_out_of_range_indices_are_rejected(solved):
     with pytest.raises(N.TapsimError) as e:
         g.field_o1([g.n])
     assert e.value.code == 1
+
+
+@pytest.mark.parametrize("integrator,stepper", [(1, 0), (0, 1), (1, 2), (1, 3), (0, 2)])
+def test_other_integrators_and_steppers_match_oracle(solved, integrator, stepper):
+    """Euler / Cash-Karp with the none, error-restricted, geometry-restricted
+    and adaptive steppers (trajectory_3d.cpp:358-581) against the oracle."""
+    a, g, o = solved
+    nodes, _ = g.surface()
+    starts = nodes[:: max(1, len(nodes) // 8)][:8]
+    kw = dict(integrator=integrator, stepper=stepper, max_steps=20000)
+    out = g.trace(a["xyz"][starts], QM_FE, a["node_tet"][starts], **kw)
+    H = float(a["xyz"][:, 2].max())
+    for k, node in enumerate(starts):
+        ref = o.trace_ext(a["xyz"][node], np.zeros(3), QM_FE, a["node_tet"][node], integrator, stepper,
+                          max_steps=20000, stepper_limit=200)
+        dev = out[k]
+        assert dev.status == ref.status
+        assert abs(dev.steps - ref.steps) <= max(2, 0.25 * ref.steps)
+        if dev.status == 5 and dev.steps == ref.steps and integrator == 1:
+            d = np.hypot(dev.stop[0] - ref.stop[0], dev.stop[1] - ref.stop[1])
+            assert d <= 1e-2 * np.hypot(ref.stop[0], ref.stop[1]) + 1e-12
+            assert abs(dev.stop[2] - H) <= 1e-6 * H
+
+
+def test_initial_velocity_matches_oracle(solved):
+    a, g, o = solved
+    nodes, _ = g.surface()
+    starts = nodes[:: max(1, len(nodes) // 6)][:6]
+    rng = np.random.default_rng(11)
+    vel = (rng.standard_normal((len(starts), 3)) * 2e3).astype(np.float32)
+    out = g.trace(a["xyz"][starts], QM_FE, a["node_tet"][starts], vel=vel)
+    for k, node in enumerate(starts):
+        ref = o.trace_ext(a["xyz"][node], vel[k].astype(np.float64), QM_FE, a["node_tet"][node], 1, 1,
+                          stepper_limit=200)
+        dev = out[k]
+        assert dev.status == ref.status == 5
+        d = np.hypot(dev.stop[0] - ref.stop[0], dev.stop[1] - ref.stop[1])
+        assert d <= 1e-2 * np.hypot(ref.stop[0], ref.stop[1])
