@@ -556,29 +556,100 @@ class Evaporation:
         }
 
 
-def write_results(path: str, records: list[dict], xyz: np.ndarray, binary: bool = False, header: str = ""):
-    """LogResults record layout (logResults.cpp:135-381)."""
-    with open(path, "wb") as f:
-        f.write(b"TAPSIM RESULTS DATA\nVERSION 1.0\n" + header.encode())
-        units = ["[1]", "[1]", "[1]", "[V]"] + ["[m]"] * 6 + ["[s]", "[1]"] + \
-                ["[V]", "[V/m]", "[V/m]", "[V/m]"] * 2 + ["[m]"] * 6
-        types = ["int", "int", "unsigned int"] + ["float"] * 23
-        for k, name in enumerate(RESULT_FIELDS):
-            u = units[k]
+_RESULT_UNITS = ["[1]", "[1]", "[1]", "[V]"] + ["[m]"] * 6 + ["[s]", "[1]"] + \
+    ["[V]", "[V/m]", "[V/m]", "[V/m]"] * 2 + ["[m]"] * 6
+_RESULT_TYPES = ["int", "int", "unsigned int"] + ["float"] * 23
+
+
+def _results_header(binary: bool, header: str) -> bytes:
+    """LogResults::writeHeader (logResults.cpp:135-225)."""
+    out = ["TAPSIM RESULTS DATA\nVERSION 1.0\n", header]
+    for k, name in enumerate(RESULT_FIELDS):
+        u = _RESULT_UNITS[k]
+        if binary:
+            if name.startswith("potential"):
+                u = "[1]"
+            out.append(f"# {name} {u} ({_RESULT_TYPES[k]})\n")
+        else:
+            out.append(f"# {name} {u}\n")
+    out.append("BINARY\n" if binary else "ASCII\n")
+    return "".join(out).encode()
+
+
+def write_results_rows(path: str, rows: list, binary: bool = False, header: str = "", chunk_size: int = 0) -> list:
+    """Results files in LogResults' layout (logResults.cpp:135-381) from rows
+    of the 26 RESULT_FIELDS values.  With chunk_size > 0 the rows go to
+    files named path.%08u after the index of the event opening each chunk
+    (a new chunk when index % chunk_size == 0), the header only in the
+    first, as the reference's writer thread does.  Returns the file names."""
+    names, f = [], None
+    try:
+        for r in rows:
+            index = int(r[0])
+            if f is None or (chunk_size > 0 and index % chunk_size == 0):
+                first = f is None
+                if f is not None:
+                    f.close()
+                name = f"{path}.{index:08d}" if chunk_size > 0 else path
+                f = open(name, "wb")
+                names.append(name)
+                f.write(_results_header(binary, header if first else ""))
             if binary:
-                if name.startswith("potential"):
-                    u = "[1]"
-                f.write(f"# {name} {u} ({types[k]})\n".encode())
+                f.write(struct.pack("<IhI", index, int(r[1]), int(r[2])))
+                f.write(struct.pack("<23f", *[float(v) for v in r[3:]]))
             else:
-                f.write(f"# {name} {u}\n".encode())
-        f.write(b"BINARY\n" if binary else b"ASCII\n")
-        for r in records:
-            start = xyz[r["node"]]
-            vals = [r["voltage"], *start, *r["stop"], r["tof"], r["probability"], r["potentialBefore"],
-                    *r["fieldBefore"], r["potentialAfter"], *r["fieldAfter"], *r["normal"], *r["apex"]]
-            if binary:
-                f.write(struct.pack("<IhI", r["index"], r["id"], r["number"]))
-                f.write(struct.pack("<23f", *vals))
-            else:
-                f.write(("\t".join([str(r["index"]), str(r["id"]), str(r["number"])] +
-                                   [f"{v:e}" for v in vals]) + "\n").encode())
+                f.write(("\t".join([str(int(r[0])), str(int(r[1])), str(int(r[2]))] +
+                                   [_c_scientific(v) for v in r[3:]]) + "\n").encode())
+        if f is None:
+            f = open(path, "wb")
+            names.append(path)
+            f.write(_results_header(binary, header))
+    finally:
+        if f is not None:
+            f.close()
+    return names
+
+
+def _c_scientific(v: float) -> str:
+    """A float as C++ iostream prints it with std::ios::scientific."""
+    if v != v:
+        return "nan" if math.copysign(1.0, v) > 0 else "-nan"
+    return f"{float(np.float32(v)):e}"
+
+
+def read_results(path: str) -> tuple[str, list]:
+    """(header, rows) of one results file, ASCII or binary."""
+    data = open(path, "rb").read()
+    lines = data.split(b"\n")
+    head, k = [], 2
+    while not lines[k].startswith(b"# index"):
+        head.append(lines[k].decode() + "\n")
+        k += 1
+    k += len(RESULT_FIELDS)
+    mode = lines[k]
+    body_start = sum(len(l) + 1 for l in lines[:k + 1])
+    rows = []
+    if mode == b"BINARY":
+        rec = struct.Struct("<IhI23f")
+        body = data[body_start:]
+        for o in range(0, len(body) - len(body) % rec.size, rec.size):
+            rows.append(list(rec.unpack_from(body, o)))
+    else:
+        for l in lines[k + 1:]:
+            if l.strip():
+                t = l.decode().split("\t")
+                rows.append([int(t[0]), int(t[1]), int(t[2])] + [float(x) for x in t[3:]])
+    return "".join(head), rows
+
+
+def write_results(path: str, records: list[dict], xyz: np.ndarray, binary: bool = False, header: str = "",
+                  chunk_size: int = 0) -> list:
+    """Results files of Evaporation records (LogResults::Dataset,
+    logResults.h:41-66)."""
+    rows = []
+    for r in records:
+        start = xyz[r["node"]]
+        rows.append([r["index"], r["id"], r["number"], r["voltage"], *start, *r["stop"], r["tof"],
+                     r["probability"], r["potentialBefore"], *r["fieldBefore"], r["potentialAfter"],
+                     *r["fieldAfter"], *r["normal"], *r["apex"]])
+    return write_results_rows(path, rows, binary, header, chunk_size)

@@ -30,6 +30,11 @@ probability / choice mode of the reference (surface_3d.cpp:220-449):
                                        (Monte-Carlo, rand() seeded 99)
     ref_events_int{I}_step{S}.txt      8 events with TRAJECTORY_INTEGRATOR_TYPE I and
                                        TRAJECTORY_STEPPER_TYPE S: (1, 2), (1, 3), (0, 1)
+
+With `--results` it runs the reference's own `tapsim resumption` on the
+dump for 6 events and keeps the results files its LogResults writes
+(logResults.cpp:135-381): ref_results_ascii.txt (one file) and
+ref_results_bin.00000001 / .00000004 (binary, chunk size 4).
 """
 from __future__ import annotations
 
@@ -117,5 +122,31 @@ def modes():
     shutil.rmtree(tmp)
 
 
+def results():
+    tapsim = ROOT / "oracle" / "_ref" / "tapsim"
+    if not tapsim.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    tmp = HERE / "_tmp"
+    tmp.mkdir(exist_ok=True)
+    with gzip.open(HERE / "ref_mesh.dump.gz", "rb") as f, open(tmp / "ref.dump", "wb") as g:
+        shutil.copyfileobj(f, g)
+    shutil.copy(HERE / "oracle.ini", tmp / "oracle.ini")
+    common = ["resumption", "ref.dump", "--ini-file=oracle.ini", "--event-limit=6", "--no-trajectories",
+              "--no-grids", "--no-surfaces", "--no-dump", "--threads=1"]
+    subprocess.run([str(tapsim), *common, "--write-ascii", "--no-chunks", "ref_results_ascii.txt"], cwd=tmp,
+                   check=True, capture_output=True)
+    subprocess.run([str(tapsim), *common, "--write-binary", "--chunk-size=4", "ref_results_bin"], cwd=tmp,
+                   check=True, capture_output=True)
+    for name in ("ref_results_ascii.txt", "ref_results_bin.00000001", "ref_results_bin.00000004"):
+        shutil.copy(tmp / name, HERE / name)
+        print("results ->", name)
+    shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
-    modes() if "--modes" in sys.argv else main()
+    if "--modes" in sys.argv:
+        modes()
+    elif "--results" in sys.argv:
+        results()
+    else:
+        main()

@@ -102,3 +102,28 @@ def test_results_writer_layout(tmp_path):
     write_results(str(p2), [rec], xyz, binary=False)
     line = p2.read_text().splitlines()[-1].split("\t")
     assert len(line) == 26 and line[0] == "1" and line[1] == "4"
+
+
+def test_results_files_round_trip_the_reference_bytes():
+    """Results written by the reference's own LogResults (tapsim resumption,
+    ASCII in one file and binary in chunks of 4 events) are read and written
+    back byte for byte, chunk file names included."""
+    import os
+    import tempfile
+    from tapsim_modified_b200.tapsim import read_results, write_results_rows
+    from conftest import GOLDEN
+    header, rows = read_results(str(GOLDEN / "ref_results_ascii.txt"))
+    assert len(rows) == 6 and rows[0][0] == 1 and header.startswith("# Generated by TAPSim")
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "r.txt")
+        names = write_results_rows(out, rows, binary=False, header=header)
+        assert open(names[0], "rb").read() == (GOLDEN / "ref_results_ascii.txt").read_bytes()
+        h1, rows1 = read_results(str(GOLDEN / "ref_results_bin.00000001"))
+        h2, rows2 = read_results(str(GOLDEN / "ref_results_bin.00000004"))
+        assert [r[0] for r in rows1 + rows2] == [1, 2, 3, 4, 5, 6] and h2 == ""
+        names = write_results_rows(os.path.join(td, "b"), rows1 + rows2, binary=True, header=h1, chunk_size=4)
+        assert [os.path.basename(n) for n in names] == ["b.00000001", "b.00000004"]
+        assert open(names[0], "rb").read() == (GOLDEN / "ref_results_bin.00000001").read_bytes()
+        assert open(names[1], "rb").read() == (GOLDEN / "ref_results_bin.00000004").read_bytes()
+    # the ASCII and binary runs are the same events
+    assert [r[2] for r in rows] == [r[2] for r in rows1 + rows2]
