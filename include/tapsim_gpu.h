@@ -237,6 +237,28 @@ typedef struct {
  * errorRestricted_stepper (:358-425), batched: one ion per thread. */
 int tg_trace(tg_handle* h, int32_t n_ions, const float* start_xyz, const float* start_vel,
              const float* charge_over_mass, const int32_t* tet_guess, const tg_trace_opts* opts, tg_impact* out);
+/* One phase-space point of a flight, Trajectory_3d::phaseVector
+ * (trajectory_3d.h:40-80): time [s] from the start, position [m], velocity
+ * [m/s], tetrahedron (-1 outside the mesh). */
+typedef struct {
+    float time;
+    float position[3];
+    float velocity[3];
+    int32_t tet;
+} tg_path_point;
+/* tg_trace that also keeps each flight's path as Trajectory_3d::data()
+ * holds it: the start, one point per accepted step (the one that leaves the
+ * mesh with tet -1) and the point extrapolated to the top plane
+ * (trajectory_3d.cpp:99-209, 303-332), plus error_estimate(): the
+ * component-wise root sum of squares of the accepted steps' error vectors
+ * (cumulative_error, :683-700), the position part grown by the extrapolation
+ * time times the velocity part (:329).  Ion k's path fills
+ * points[k*cap .. k*cap + cap-1]; it has impact.steps + 2 points (0 when the
+ * start is outside the mesh), and a path longer than cap keeps its first cap
+ * points.  errors[6k .. 6k+5] = position x, y, z, velocity x, y, z. */
+int tg_trace_path(tg_handle* h, int32_t n_ions, const float* start_xyz, const float* start_vel,
+                  const float* charge_over_mass, const int32_t* tet_guess, const tg_trace_opts* opts, int32_t cap,
+                  tg_impact* out, tg_path_point* points, float* errors);
 /* Grid_3d::potential(geom, grid, pos, tet) (grid_3d.cpp:1585-1602). */
 int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* tet_guess, float* phi_out);
 
@@ -271,6 +293,13 @@ typedef struct {
      * evap_initialVelocity does (surface_3d.cpp:472-503) from the same
      * stream; 0 starts it at rest (the reference's default) */
     int32_t initial_velocity;
+    /* path_cap > 0 keeps each event's flight path for the trajectory log
+     * (LogTrajectory, logTrajectory.cpp:137-300) as tg_trace_path does: the
+     * k-th event of a call writes path_points[k*path_cap ..] (host memory,
+     * count*path_cap points) and path_errors[6k .. 6k+5] */
+    int32_t path_cap;
+    tg_path_point* path_points;
+    float* path_errors;
 } tg_event_opts;
 typedef struct {
     int32_t node;

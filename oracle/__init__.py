@@ -89,6 +89,10 @@ def lib():
         L.orc_trace_ext.argtypes = [P, C.c_void_p, C.c_void_p, C.c_double, C.c_int32, C.c_double, C.c_double,
                                     C.c_double, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                     C.POINTER(orc_impact)]
+        L.orc_trace_path.restype = None
+        L.orc_trace_path.argtypes = [P, C.c_void_p, C.c_void_p, C.c_double, C.c_int32, C.c_double, C.c_double,
+                                     C.c_double, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
+                                     C.POINTER(orc_impact), C.c_int32, C.c_void_p, C.c_void_p]
         L.orc_potential_at.restype = C.c_double
         L.orc_potential_at.argtypes = [P, C.c_void_p, C.c_int32]
         _lib = L
@@ -220,6 +224,21 @@ class Oracle:
         self.L.orc_trace_ext(C.byref(self.m), _p(s), _p(v), qm, int(tet_guess), dt0, dt_min, tol, max_steps,
                              stepper_limit, self.top_z, int(integrator), int(stepper), C.byref(out))
         return out
+
+    def trace_path(self, start, vel, qm, tet_guess, integrator=1, stepper=1, dt0=1e-14, dt_min=1e-16, tol=1e-6,
+                   max_steps=200000, stepper_limit=1000, cap=100000):
+        """(impact, points [k, 8]: time, position, velocity, tetrahedron;
+        error estimate [6]) of one flight."""
+        s = np.ascontiguousarray(start, np.float64)
+        v = np.ascontiguousarray(vel, np.float64)
+        out = orc_impact()
+        path = np.zeros((cap, 8), np.float64)
+        err = np.zeros(6, np.float64)
+        self.L.orc_trace_path(C.byref(self.m), _p(s), _p(v), qm, int(tet_guess), dt0, dt_min, tol, max_steps,
+                              stepper_limit, self.top_z, int(integrator), int(stepper), C.byref(out), cap, _p(path),
+                              _p(err))
+        n = 0 if out.status == -1 else min(out.steps + 2, cap)
+        return out, path[:n], err
 
     def potential_at(self, p, tet_guess) -> float:
         s = np.ascontiguousarray(p, np.float64)

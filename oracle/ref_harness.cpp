@@ -26,6 +26,10 @@
 //                            initial relaxation
 //       --phi-events <file>  append float32 potentials after every event
 //       --no-sync            with --dump: keep the dump's couplings (resumption)
+//       --trajectories <file> <ascii|binary> <chunk>
+//                            write every event's trajectory with the
+//                            reference's own File_Io::LogTrajectory, as
+//                            process.cpp:1048-1049 pushes it
 
 #include <cstdio>
 #include <cstdlib>
@@ -45,6 +49,7 @@
 #include "trajectory_3d.h"
 #include "process.h"
 #include "file_io.h"
+#include "logTrajectory.h"
 
 // commands.cpp (linked for makeIniList) refers to these globals, which the
 // reference defines next to main() in tapsim.cpp.
@@ -97,6 +102,9 @@ static int cmd_evap(int argc, char** argv)
 	const char* phiName = 0;
 	const char* phiEventsName = 0;
 	int threads = 1;
+	const char* trajName = 0;
+	int trajMode = File_Io::ASCII;
+	unsigned trajChunk = 0;
 	int initRelax = 1;
 	bool initGiven = false;
 	bool noSync = false;
@@ -119,8 +127,15 @@ static int cmd_evap(int argc, char** argv)
 		else if (!strcmp(argv[a], "--phi")) phiName = argv[++a];
 		else if (!strcmp(argv[a], "--phi-events")) phiEventsName = argv[++a];
 		else if (!strcmp(argv[a], "--no-sync")) noSync = true;
+		else if (!strcmp(argv[a], "--trajectories") && a + 3 < argc)
+		{
+			trajName = argv[++a];
+			trajMode = strcmp(argv[++a], "binary") ? File_Io::ASCII : File_Io::BINARY;
+			trajChunk = atoi(argv[++a]);
+		}
 		else { fprintf(stderr, "unknown option %s\n", argv[a]); return 2; }
 	}
+	File_Io::LogTrajectory* trajLog = trajName ? new File_Io::LogTrajectory(trajName, trajMode, 0, trajChunk) : 0;
 
 	std::srand(99); // as main() does (tapsim.cpp:235)
 
@@ -305,7 +320,9 @@ static int cmd_evap(int argc, char** argv)
 			lastPhi, apex[0], apex[1], apex[2], normal[0], normal[1], normal[2], t1 - t0);
 		fflush(out);
 		if (phiEvents) write_phi(phiEvents, system);
+		if (trajLog) trajLog->push(ev + 1, system.gridTable.number(nodeIndex).toValue(), timeScale, trajectory);
 	}
+	delete trajLog;  // joins the writer thread after it has written the queue
 	fclose(out);
 	if (phiEvents) fclose(phiEvents);
 	return 0;

@@ -541,9 +541,50 @@ void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t gues
     orc_trace_ext(m, start, v0, qm, guess, dt0, dt_min, tol, max_steps, stepper_limit, top_z, 1, 1, out);
 }
 
+/* point k of a recorded path: time, position, velocity, tetrahedron */
+static void put_point(double* path, int32_t cap, int32_t k, double t, const double* x, const double* v, int tet) {
+    if (!path || k >= cap) return;
+    double* p = path + 8 * (size_t)k;
+    p[0] = t;
+    for (int d = 0; d < 3; d++) {
+        p[1 + d] = x[d];
+        p[4 + d] = v[d];
+    }
+    p[7] = tet < 0 ? -1.0 : (double)tet;
+}
+
+/* Trajectory_3d::cumulative_error (trajectory_3d.cpp:683-700) */
+static void add_error(double* err, const double* ex, const double* ev) {
+    if (!err) return;
+    for (int d = 0; d < 3; d++) {
+        err[d] = sqrt(err[d] * err[d] + ex[d] * ex[d]);
+        err[3 + d] = sqrt(err[3 + d] * err[3 + d] + ev[d] * ev[d]);
+    }
+}
+
+static void trace_core(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t guess,
+                       double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
+                       int32_t integrator, int32_t stepper, orc_impact* out, int32_t cap, double* path,
+                       double* err);
+
 void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t guess,
                    double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
                    int32_t integrator, int32_t stepper, orc_impact* out) {
+    trace_core(m, start, vel, qm, guess, dt0, dt_min, tol, max_steps, stepper_limit, top_z, integrator, stepper, out,
+               0, NULL, NULL);
+}
+
+void orc_trace_path(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t guess,
+                    double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
+                    int32_t integrator, int32_t stepper, orc_impact* out, int32_t cap, double* path, double* err) {
+    trace_core(m, start, vel, qm, guess, dt0, dt_min, tol, max_steps, stepper_limit, top_z, integrator, stepper, out,
+               cap, path, err);
+}
+
+static void trace_core(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t guess,
+                       double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
+                       int32_t integrator, int32_t stepper, orc_impact* out, int32_t cap, double* path,
+                       double* err) {
     static const double B[6][5] = {{0, 0, 0, 0, 0},
                                    {1.0 / 5.0, 0, 0, 0, 0},
                                    {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
@@ -555,9 +596,11 @@ void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3]
     double x[3] = {start[0], start[1], start[2]}, v[3] = {vel[0], vel[1], vel[2]};
     double time = 0.0;
     memset(out, 0, sizeof(*out));
+    if (err) memset(err, 0, 6 * sizeof(double));
     int tet = locate(m, x, guess);
     out->last_tet = tet;
     memcpy(out->last_pos, x, sizeof(x));
+    if (tet >= 0) put_point(path, cap, 0, 0.0, x, v, tet); /* Trajectory_3d::init (trajectory_3d.cpp:99-123) */
     if (tet < 0) {
         out->status = -1;
         memcpy(out->stop, x, sizeof(x));
@@ -573,6 +616,7 @@ void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3]
         double dt = dt0;
         for (int it = 0; it < max_steps; it++) {
             double nx[3], nv[3], used = dt;
+            double ex[3] = {0, 0, 0}, ev[3] = {0, 0, 0}; /* error vector of the trial step */
             int accepted = 0, nt = -1;
             for (int tries = 0; tries < stepper_limit; tries++) {
                 if (dt < dt_min) dt = dt_min;
@@ -590,6 +634,8 @@ void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3]
                     for (int d = 0; d < 3; d++) {
                         if (nx[d] != 0.0 && dt * dt > rel) rel = dt * dt;
                         if (nv[d] != 0.0 && dt * dt > rel) rel = dt * dt;
+                        ex[d] = nx[d] * dt * dt;
+                        ev[d] = nv[d] * dt * dt;
                     }
                 } else {
                     double dx[6][3], dv[6][3];
@@ -610,7 +656,6 @@ void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3]
                             dx[s][d] = vs[d] * dt;
                         }
                     }
-                    double ex[3], ev[3];
                     for (int d = 0; d < 3; d++) {
                         nx[d] = x[d];
                         nv[d] = v[d];
@@ -665,6 +710,8 @@ void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3]
                 break;
             }
             out->steps++;
+            add_error(err, ex, ev);
+            put_point(path, cap, out->steps, time + used, nx, nv, nt);
             if (nt < 0) {
                 out->last_tet = tet;
                 memcpy(out->last_pos, x, sizeof(x));
@@ -690,4 +737,9 @@ void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3]
     for (int d = 0; d < 3; d++) out->stop[d] = x[d] + dtz * v[d];
     out->stop_time = time + dtz;
     out->status = status;
+    /* Trajectory_3d::extrapolate (trajectory_3d.cpp:303-332) */
+    const int finite = isfinite(out->stop[0]) && isfinite(out->stop[1]) && isfinite(out->stop[2]);
+    put_point(path, cap, out->steps + 1, time + dtz, out->stop, v, tet >= 0 && finite ? locate(m, out->stop, tet) : -1);
+    if (err && dtz > 0.0)
+        for (int d = 0; d < 3; d++) err[d] += dtz * err[3 + d];
 }

@@ -92,6 +92,13 @@ void orc_trace(const orc_mesh* m, const double start[3], double qm, int32_t tet_
 void orc_trace_ext(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t tet_guess,
                    double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
                    int32_t integrator, int32_t stepper, orc_impact* out);
+/* orc_trace_ext keeping the path as Trajectory_3d::data() holds it (start,
+ * each accepted step, the extrapolated point; at most cap points of 8
+ * doubles: time, position, velocity, tetrahedron) and the cumulative error
+ * estimate err[6] (position, velocity) */
+void orc_trace_path(const orc_mesh* m, const double start[3], const double vel[3], double qm, int32_t tet_guess,
+                    double dt0, double dt_min, double tol, int32_t max_steps, int32_t stepper_limit, double top_z,
+                    int32_t integrator, int32_t stepper, orc_impact* out, int32_t cap, double* path, double* err);
 /* Grid_3d::potential(pos, tet) */
 double orc_potential_at(const orc_mesh* m, const double p[3], int32_t tet_guess);
 

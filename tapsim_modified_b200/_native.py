@@ -64,6 +64,14 @@ class tg_impact(C.Structure):
                 ("last_tet", C.c_int32), ("last_phi", C.c_float), ("steps", C.c_int32), ("status", C.c_int32)]
 
 
+class tg_path_point(C.Structure):
+    _fields_ = [("time", C.c_float), ("position", C.c_float * 3), ("velocity", C.c_float * 3), ("tet", C.c_int32)]
+
+
+# tg_path_point as a numpy record (the same 32 bytes)
+PATH_POINT = np.dtype([("time", "<f4"), ("position", "<f4", 3), ("velocity", "<f4", 3), ("tet", "<i4")])
+
+
 class tg_event_opts(C.Structure):
     _fields_ = [("vacuum_id", C.c_int32), ("relax_mode", C.c_int32), ("local_threshold", C.c_double),
                 ("local_shell", C.c_int32), ("local_cycle", C.c_int32), ("local_queue", C.c_int32),
@@ -71,7 +79,8 @@ class tg_event_opts(C.Structure):
                 ("refresh_cycle", C.c_int32), ("refresh_queue", C.c_int32), ("refresh_max_sweeps", C.c_int64),
                 ("solve", tg_solve_opts), ("trace", tg_trace_opts), ("trace_enabled", C.c_int32),
                 ("normal_enabled", C.c_int32), ("prob_mode", C.c_int32), ("choice_mode", C.c_int32),
-                ("temperature", C.c_float), ("rng_seed", C.c_uint32), ("initial_velocity", C.c_int32)]
+                ("temperature", C.c_float), ("rng_seed", C.c_uint32), ("initial_velocity", C.c_int32),
+                ("path_cap", C.c_int32), ("path_points", C.c_void_p), ("path_errors", C.c_void_p)]
 
 
 class tg_event_record(C.Structure):
@@ -120,6 +129,7 @@ SIGNATURES = {
     "tg_take_away": (C.c_int, [_P, _I, _I, _P, C.POINTER(_I)]),
     "tg_update_coordination": (C.c_int, [_P]),
     "tg_trace": (C.c_int, [_P, _I, _P, _P, _P, _P, C.POINTER(tg_trace_opts), _P]),
+    "tg_trace_path": (C.c_int, [_P, _I, _P, _P, _P, _P, C.POINTER(tg_trace_opts), _I, _P, _P, _P]),
     "tg_potential_at": (C.c_int, [_P, _I, _P, _P, _P]),
     "tg_run_event": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, C.POINTER(tg_event_record)]),
     "tg_run_events": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, _I, _P, C.POINTER(C.c_int32)]),

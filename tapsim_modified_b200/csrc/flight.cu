@@ -454,9 +454,40 @@ __device__ __forceinline__ int stepper_verdict(const DevMesh& m, TetCache& fc, c
     return 0;
 }
 
-// One ion from x0 (velocity v0, charge/mass k) into *out.
+// Point idx of the path of ion `slot` (Trajectory_3d::phaseVector,
+// trajectory_3d.h:40-80), dropped beyond the path's capacity.
+__device__ __forceinline__ void path_point(const TraceParams& tp, int slot, int idx, double t, V3 x, V3 v, int tet) {
+    if (idx >= tp.path_cap) return;
+    float4* p = reinterpret_cast<float4*>(tp.path + ((size_t)slot * tp.path_cap + idx) * 8);
+    p[0] = make_float4((float)t, (float)x.x, (float)x.y, (float)x.z);
+    p[1] = make_float4((float)v.x, (float)v.y, (float)v.z, __int_as_float(tet < 0 ? -1 : tet));
+}
+
+// The error vector of the latest trial step, parked in words 6..11 of the
+// ion's error record so that it holds no registers across the stepper's
+// point location.
+__device__ __forceinline__ void path_trial_error(const TraceParams& tp, int slot, V3 ex, V3 ev) {
+    float* e = tp.path_err + 12 * (size_t)slot + 6;
+    e[0] = (float)ex.x; e[1] = (float)ex.y; e[2] = (float)ex.z;
+    e[3] = (float)ev.x; e[4] = (float)ev.y; e[5] = (float)ev.z;
+}
+
+// Trajectory_3d::cumulative_error (trajectory_3d.cpp:683-700) with the
+// accepted step's error: each of the six components becomes
+// sqrt(current^2 + step^2), in float as the reference keeps it.
+__device__ __forceinline__ void path_error(const TraceParams& tp, int slot) {
+    float* e = tp.path_err + 12 * (size_t)slot;
+#pragma unroll
+    for (int j = 0; j < 6; j++) e[j] = sqrtf(e[j] * e[j] + e[6 + j] * e[6 + j]);
+}
+
+// One ion from x0 (velocity v0, charge/mass k) into *out; with kPath its
+// path and error estimate go to slot `slot` of tp's path buffers (a
+// separate instantiation, so that the flights without a path keep their
+// registers).
+template <bool kPath>
 __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k, int guessTet, const TraceParams& tp,
-                                          unsigned rot, ImpactOut* out) {
+                                          unsigned rot, int slot, ImpactOut* out) {
     // Cash-Karp tableau; the stage loops are unrolled so that every index is
     // a compile-time constant and the stage vectors stay in registers
     constexpr double B[6][5] = {{0, 0, 0, 0, 0},
@@ -478,6 +509,12 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
     res.last_tet = tet;
     res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
     res.last_phi = 0.0f;
+    if (kPath) {
+        float* e = tp.path_err + 12 * (size_t)slot;
+#pragma unroll
+        for (int j = 0; j < 12; j++) e[j] = 0.0f;
+        if (tet >= 0) path_point(tp, slot, 0, 0.0, x, v, tet);  // Trajectory_3d::init (:99-123)
+    }
     if (tet < 0) {
         if (tet == -2) atomicOr(m.status, S_WALK_LIMIT);
         res.status = -1;  // Trajectory_3d::init: initial point is outside
@@ -554,6 +591,7 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                 if (nv.x != 0.0) rel = fmax(rel, fabs(evv.x / nv.x));
                 if (nv.y != 0.0) rel = fmax(rel, fabs(evv.y / nv.y));
                 if (nv.z != 0.0) rel = fmax(rel, fabs(evv.z / nv.z));
+                if (kPath) path_trial_error(tp, slot, ex, evv);
                 if (tp.stepper != 1) {
                     const int verdict = stepper_verdict(m, fc, tp, nx, tet, cur, rot, rel, &dt, &nt, &located);
                     if (verdict > 0) {
@@ -583,6 +621,16 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                 if (nt == -2) atomicOr(m.status, S_WALK_LIMIT);
             }
             res.steps++;
+            if (kPath) {
+                // the error of the accepted step: o1_integrator's is the new
+                // state times dt^2 (trajectory_3d.cpp:568-576)
+                if (tp.integrator == 0) {
+                    const double d2 = used * used;
+                    path_trial_error(tp, slot, V3{nx.x * d2, nx.y * d2, nx.z * d2}, V3{nv.x * d2, nv.y * d2, nv.z * d2});
+                }
+                path_error(tp, slot);
+                path_point(tp, slot, res.steps, time + used, nx, nv, nt);
+            }
             if (nt < 0) {
                 // left the mesh: the previous point is the last inside it
                 res.last_tet = tet;
@@ -616,23 +664,43 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
     res.stop[2] = (float)(x.z + dtz * v.z);
     res.stop_time = (float)(time + dtz);
     res.status = status;
+    if (kPath) {
+        // Trajectory_3d::extrapolate (trajectory_3d.cpp:303-332): the last
+        // point, located from the last tetrahedron (outside stays outside;
+        // a flight at rest, NO_FIELD, extrapolates to a non-finite point)
+        const V3 p{x.x + dtz * v.x, x.y + dtz * v.y, x.z + dtz * v.z};
+        int pt = -1;
+        if (tet >= 0 && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
+            pt = locate(m, p, tet, tp.walk_limit, rot);
+            if (pt == -2) atomicOr(m.status, S_WALK_LIMIT);
+        }
+        path_point(tp, slot, res.steps + 1, time + dtz, p, v, pt);
+        const float fdt = (float)dtz;
+        if (fdt > 0.0f) {
+            float* e = tp.path_err + 12 * (size_t)slot;
+#pragma unroll
+            for (int j = 0; j < 3; j++) e[j] += fdt * e[3 + j];
+        }
+    }
     *out = res;
 }
 
+template <bool kPath>
 __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* vel, const float* qm,
                         const int32_t* guess, TraceParams tp, ImpactOut* out) {
     const int ion = blockIdx.x * blockDim.x + threadIdx.x;
     if (ion >= nIons) return;
     const V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
     const V3 v = vel ? V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]} : V3{0, 0, 0};
-    trace_ion(m, x, v, qm[ion], guess ? guess[ion] : 0, tp, (unsigned)ion * 7u, out + ion);
+    trace_ion<kPath>(m, x, v, qm[ion], guess ? guess[ion] : 0, tp, (unsigned)ion * 7u, ion, out + ion);
 }
 
 // A single ion from rest, its start passed by value (no staging copy)
+template <bool kPath>
 __global__ void k_trace_one(DevMesh m, float x, float y, float z, float vx, float vy, float vz, float qm, int guess,
                             TraceParams tp, ImpactOut* out) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    trace_ion(m, V3{x, y, z}, V3{vx, vy, vz}, qm, guess, tp, 0u, out);
+    trace_ion<kPath>(m, V3{x, y, z}, V3{vx, vy, vz}, qm, guess, tp, 0u, 0, out);
 }
 
 __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t* guess, int limit, float* out) {
@@ -649,7 +717,11 @@ __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t
 
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s) {
-    if (nIons > 0) { count_launch(); k_trace<<<(nIons + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); }
+    if (nIons <= 0) return;
+    count_launch();
+    const int blocks = (nIons + kBlock - 1) / kBlock;
+    if (tp.path) k_trace<true><<<blocks, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out);
+    else k_trace<false><<<blocks, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out);
 }
 void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s) {
     if (m.ntets > 0) { count_launch(); k_pack_tets<<<(m.ntets + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, pack); }
@@ -664,7 +736,8 @@ void launch_vertex_fields(const DevMesh& m, cudaStream_t s) {
 void launch_trace_one(const DevMesh& m, const float start[3], const float vel[3], float qm, int guess, TraceParams tp,
                       ImpactOut* out, cudaStream_t s) {
     count_launch();
-    k_trace_one<<<1, 32, 0, s>>>(m, start[0], start[1], start[2], vel[0], vel[1], vel[2], qm, guess, tp, out);
+    if (tp.path) k_trace_one<true><<<1, 32, 0, s>>>(m, start[0], start[1], start[2], vel[0], vel[1], vel[2], qm, guess, tp, out);
+    else k_trace_one<false><<<1, 32, 0, s>>>(m, start[0], start[1], start[2], vel[0], vel[1], vel[2], qm, guess, tp, out);
 }
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit, float* out,
                          cudaStream_t s) {

@@ -23,6 +23,7 @@
 using namespace tgd;
 
 static_assert(sizeof(ImpactOut) == sizeof(tg_impact), "impact layout");
+static_assert(sizeof(tg_path_point) == 8 * sizeof(float), "path point layout");
 
 namespace {
 
@@ -97,6 +98,8 @@ struct tg_handle {
     DBuf<double> stageD;
     DBuf<float> stageF;
     DBuf<ImpactOut> stageImpact;
+    // flight paths (tg_trace_path, tg_event_opts.path_cap): 8 words a point
+    DBuf<float> pathBuf, pathErr;
 
     cudaEvent_t evStart = nullptr, evStop = nullptr;
     // flights of tg_run_events run on their own stream, overlapping the next
@@ -674,7 +677,7 @@ void tg_destroy(tg_handle* h) {
     h->surfRatio.release(); h->surfScore.release(); h->cgbuf.release(); h->scalV.release(); h->scalN.release(); h->acc.release();
     h->keys.release(); h->result.release(); h->local.release(); h->localCount.release();
     h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
-    h->stageImpact.release();
+    h->stageImpact.release(); h->pathBuf.release(); h->pathErr.release();
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
@@ -1283,6 +1286,9 @@ int tg_update_coordination(tg_handle* h) {
 
 static TraceParams trace_params(const tg_handle* h, const tg_trace_opts* o) {
     TraceParams tp;
+    tp.path = nullptr;
+    tp.path_err = nullptr;
+    tp.path_cap = 0;
     tp.dt0 = o->time_step;
     tp.dt_min = o->min_time_step;
     tp.tol = o->error_threshold;
@@ -1295,18 +1301,30 @@ static TraceParams trace_params(const tg_handle* h, const tg_trace_opts* o) {
     return tp;
 }
 
-int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
-             const int32_t* guess, const tg_trace_opts* o, tg_impact* out) {
-    if (!h || nIons < 0 || (nIons && (!start || !qm || !out)) || !o) return fail(h, TG_ERR_ARGUMENT, "tg_trace: bad argument");
-    if (!h->tet_v.p) return fail(h, TG_ERR_ARGUMENT, "tg_trace: mesh has no tetrahedra");
+// Device path buffers for `slots` flights of `cap` points each.
+static int stage_paths(tg_handle* h, size_t slots, int32_t cap) {
+    int rc = stage(h, h->pathBuf, slots * (size_t)cap * 8);
+    if (rc == TG_OK) rc = stage(h, h->pathErr, slots * 12);
+    return rc;
+}
+
+// tg_trace, and tg_trace_path when cap > 0 (paths to host points/errors).
+static int trace_impl(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
+                      const int32_t* guess, const tg_trace_opts* o, tg_impact* out, int32_t cap,
+                      tg_path_point* points, float* errors, const char* what) {
+    if (!h || nIons < 0 || (nIons && (!start || !qm || !out)) || !o || cap < 0 ||
+        (cap > 0 && nIons && (!points || !errors)))
+        return fail(h, TG_ERR_ARGUMENT, std::string(what) + ": bad argument");
+    if (!h->tet_v.p) return fail(h, TG_ERR_ARGUMENT, std::string(what) + ": mesh has no tetrahedra");
     if (nIons == 0) return TG_OK;
     if (guess)
         for (int32_t k = 0; k < nIons; k++)
             if (guess[k] < 0 || guess[k] >= h->ntets)
-                return fail(h, TG_ERR_ARGUMENT, "tg_trace: tetrahedron guess out of range");
+                return fail(h, TG_ERR_ARGUMENT, std::string(what) + ": tetrahedron guess out of range");
     int rc = stage(h, h->stageF, (size_t)nIons * 7);
     if (rc == TG_OK) rc = stage(h, h->stageI, nIons);
     if (rc == TG_OK) rc = stage(h, h->stageImpact, nIons);
+    if (rc == TG_OK && cap > 0) rc = stage_paths(h, nIons, cap);
     if (rc != TG_OK) return rc;
     float* dStart = h->stageF.p;
     float* dVel = h->stageF.p + 3 * (size_t)nIons;
@@ -1316,11 +1334,34 @@ int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, 
     CK(cudaMemcpyAsync(dQm, qm, sizeof(float) * nIons, cudaMemcpyHostToDevice, h->stream));
     if (guess) CK(cudaMemcpyAsync(h->stageI.p, guess, sizeof(int32_t) * nIons, cudaMemcpyHostToDevice, h->stream));
     else CK(cudaMemsetAsync(h->stageI.p, 0, sizeof(int32_t) * nIons, h->stream));
-    const TraceParams tp = trace_params(h, o);
+    TraceParams tp = trace_params(h, o);
+    if (cap > 0) {
+        tp.path = h->pathBuf.p;
+        tp.path_err = h->pathErr.p;
+        tp.path_cap = cap;
+    }
     launch_vertex_fields(h->dm(), h->stream);  // once per call, from the current potentials
     launch_trace(h->dm(), nIons, dStart, vel ? dVel : nullptr, dQm, h->stageI.p, tp, h->stageImpact.p, h->stream);
     CK(cudaMemcpyAsync(out, h->stageImpact.p, sizeof(tg_impact) * nIons, cudaMemcpyDeviceToHost, h->stream));
-    return sync_status(h, "tg_trace");
+    if (cap > 0) {
+        CK(cudaMemcpyAsync(points, h->pathBuf.p, sizeof(tg_path_point) * (size_t)nIons * cap, cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaMemcpy2DAsync(errors, 6 * sizeof(float), h->pathErr.p, 12 * sizeof(float), 6 * sizeof(float), nIons,
+                             cudaMemcpyDeviceToHost, h->stream));
+    }
+    return sync_status(h, what);
+}
+
+int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
+             const int32_t* guess, const tg_trace_opts* o, tg_impact* out) {
+    return trace_impl(h, nIons, start, vel, qm, guess, o, out, 0, nullptr, nullptr, "tg_trace");
+}
+
+int tg_trace_path(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
+                  const int32_t* guess, const tg_trace_opts* o, int32_t cap, tg_impact* out, tg_path_point* points,
+                  float* errors) {
+    if (cap <= 0) return fail(h, TG_ERR_ARGUMENT, "tg_trace_path: cap must be positive");
+    return trace_impl(h, nIons, start, vel, qm, guess, o, out, cap, points, errors, "tg_trace_path");
 }
 
 int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* guess, float* out) {
@@ -1484,11 +1525,20 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
             CK(cudaStreamWaitEvent(h->traceStream, h->evFields, 0));
             DevMesh mt = h->dm();
             mt.status = h->statusTrace.p;
-            launch_trace_one(mt, start, vel, qm, guess, trace_params(h, &o->trace), asyncImpact, h->traceStream);
+            TraceParams tp = trace_params(h, &o->trace);
+            if (o->path_cap > 0) {
+                // this event's slot of the batch
+                const size_t slot = (size_t)(asyncImpact - h->stageImpact.p);
+                tp.path = h->pathBuf.p + slot * (size_t)o->path_cap * 8;
+                tp.path_err = h->pathErr.p + 12 * slot;
+                tp.path_cap = o->path_cap;
+            }
+            launch_trace_one(mt, start, vel, qm, guess, tp, asyncImpact, h->traceStream);
             CK(cudaGetLastError());
             CK(cudaEventRecord(h->evTraceDone, h->traceStream));
         } else {
-            rc = tg_trace(h, 1, start, o->initial_velocity ? vel : nullptr, &qm, &guess, &o->trace, &rec->impact);
+            rc = trace_impl(h, 1, start, o->initial_velocity ? vel : nullptr, &qm, &guess, &o->trace, &rec->impact,
+                            o->path_cap, o->path_points, o->path_errors, "tg_run_event");
             if (rc != TG_OK) return rc;
         }
     }
@@ -1532,16 +1582,23 @@ int tg_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, int32_t M, int3
     return TG_OK;
 }
 
+static bool path_opts_ok(const tg_event_opts* o) {
+    return o->path_cap >= 0 && (o->path_cap == 0 || (o->path_points && o->path_errors));
+}
+
 int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec) {
     if (!h || !o || !rec) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: null argument");
+    if (!path_opts_ok(o)) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: path_cap < 0 or path buffers missing");
     return run_event(h, o, eventIndex, rec, nullptr);
 }
 
 int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int32_t count, tg_event_record* recs,
                   int32_t* done) {
     if (!h || !o || count < 0 || (count && !recs)) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: bad argument");
+    if (!path_opts_ok(o)) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: path_cap < 0 or path buffers missing");
     if (done) *done = 0;
     int rc = stage(h, h->stageImpact, std::max(count, 1));
+    if (rc == TG_OK && o->path_cap > 0 && o->trace_enabled) rc = stage_paths(h, std::max(count, 1), o->path_cap);
     if (rc != TG_OK) return rc;
     CK(cudaMemsetAsync(h->statusTrace.p, 0, sizeof(int), h->stream));
     int k = 0;
@@ -1556,6 +1613,12 @@ int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int3
         std::vector<ImpactOut> imp(k);
         CK(cudaMemcpy(imp.data(), h->stageImpact.p, sizeof(ImpactOut) * k, cudaMemcpyDeviceToHost));
         for (int j = 0; j < k; j++) std::memcpy(&recs[j].impact, &imp[j], sizeof(tg_impact));
+        if (o->path_cap > 0) {
+            CK(cudaMemcpy(o->path_points, h->pathBuf.p, sizeof(tg_path_point) * (size_t)k * o->path_cap,
+                          cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy2D(o->path_errors, 6 * sizeof(float), h->pathErr.p, 12 * sizeof(float), 6 * sizeof(float), k,
+                            cudaMemcpyDeviceToHost));
+        }
         int st = 0;
         CK(cudaMemcpy(&st, h->statusTrace.p, sizeof(int), cudaMemcpyDeviceToHost));
         if (st != 0) {

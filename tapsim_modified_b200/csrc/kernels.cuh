@@ -166,6 +166,14 @@ struct TraceParams {
     float top_z;
     int integrator;  // 0 Euler, 1 Cash-Karp (TRAJECTORY_INTEGRATOR_TYPE)
     int stepper;     // 0 none, 1 error-restricted, 2 geometry-restricted, 3 adaptive
+    // optional path recording (null path: none): ion k keeps up to path_cap
+    // points of 8 words (time, position, velocity, tetrahedron bits) at
+    // path + k * path_cap * 8, and 12 words at path_err + 12k: its
+    // cumulative error estimate (position, velocity), then the latest trial
+    // step's error
+    float* path;
+    float* path_err;
+    int path_cap;
 };
 struct ImpactOut {
     float stop[3];

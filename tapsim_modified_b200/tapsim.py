@@ -126,6 +126,12 @@ class Mesh:
         N.check(N.lib().tg_mesh_write_dump(self._h, str(path).encode(), N.ptr(p)))
 
 
+def path_length(impact: N.tg_impact, cap: int) -> int:
+    """Points a flight's path holds: start, accepted steps, extrapolated
+    point; none when the start is outside the mesh; at most cap kept."""
+    return 0 if impact.status == -1 else min(impact.steps + 2, cap)
+
+
 def trace_opts(time_step=1e-14, min_time_step=1e-16, error_threshold=1e-6, max_steps=100000, stepper_limit=200,
                walk_limit=100000, integrator=1, stepper=1) -> N.tg_trace_opts:
     """Trajectory options; integrator / stepper are TRAJECTORY_INTEGRATOR_TYPE
@@ -276,6 +282,24 @@ class Grid:
         self._ck(N.lib().tg_trace(self._h, n, N.ptr(start), N.ptr(v), N.ptr(q), N.ptr(g),
                                   C.byref(trace_opts(**opts)), C.cast(out, C.c_void_p)))
         return out
+
+    def trace_path(self, start: np.ndarray, qm, tet_guess=None, vel=None, cap: int = 4096, **opts):
+        """tg_trace_path: (impacts, paths, errors).  paths[k] is ion k's
+        Trajectory_3d::data() as PATH_POINT records (start, accepted steps,
+        extrapolated point; at most cap), errors[k] its error estimate
+        (position x, y, z, velocity x, y, z)."""
+        start = np.ascontiguousarray(np.atleast_2d(start), np.float32)
+        n = len(start)
+        q = np.ascontiguousarray(np.broadcast_to(np.asarray(qm, np.float32), (n,)))
+        g = None if tet_guess is None else np.ascontiguousarray(np.broadcast_to(np.asarray(tet_guess, np.int32), (n,)))
+        v = None if vel is None else np.ascontiguousarray(np.atleast_2d(vel), np.float32)
+        out = (N.tg_impact * n)()
+        pts = np.zeros((n, cap), N.PATH_POINT)
+        err = np.zeros((n, 6), np.float32)
+        self._ck(N.lib().tg_trace_path(self._h, n, N.ptr(start), N.ptr(v), N.ptr(q), N.ptr(g),
+                                       C.byref(trace_opts(**opts)), cap, C.cast(out, C.c_void_p), N.ptr(pts),
+                                       N.ptr(err)))
+        return out, [pts[k, :path_length(out[k], cap)] for k in range(n)], err
 
     def potential_at(self, xyz: np.ndarray, tet_guess=None) -> np.ndarray:
         xyz = np.ascontiguousarray(np.atleast_2d(xyz), np.float32)
@@ -484,13 +508,20 @@ class Evaporation:
     """Process::evaporation (process.cpp:441-1124) over one device Grid."""
 
     def __init__(self, grid: Grid, options: EvaporationOptions, relax_mode: int = 1,
-                 solve: N.tg_solve_opts | None = None, trace: bool = True, normal: bool = True):
+                 solve: N.tg_solve_opts | None = None, trace: bool = True, normal: bool = True, path_cap: int = 0):
+        """path_cap > 0 keeps each event's flight path (up to path_cap points)
+        in its record for write_trajectories."""
         self.grid = grid
         self.options = options
         types = grid.mesh.arrays()["types"]
         name = options.s("VACUUM_CELL_IDENTIFIER")
         self.vacuum_id = self._type_id_by_name(grid, name)
         self.evap_field = {k: v["evap_field"] for k, v in types.items()}
+        # the ion's charge [C] and mass [kg] as Process::evaporation forms
+        # them in float (process.cpp:929-933)
+        self.charge_mass = {k: (float(np.float32(v["evap_charge"]) * np.float32(1.60217733e-19)),
+                                float(np.float32(v["mass"]) * np.float32(1.660538782e-27))) for k, v in types.items()}
+        self.path_cap = int(path_cap)
         self.opts = options.event_opts(self.vacuum_id, relax_mode, solve, trace, normal,
                                        temperature=grid.mesh.temperature)
         self.voltage_queue: deque = deque()
@@ -509,26 +540,41 @@ class Evaporation:
         # meshgen's vacuum marker is id 0 in every generated configuration
         return 0
 
+    def _path_buffers(self, count: int):
+        if self.path_cap <= 0:
+            self.opts.path_cap = 0
+            self.opts.path_points = None
+            self.opts.path_errors = None
+            return None, None
+        pts = np.zeros((count, self.path_cap), N.PATH_POINT)
+        err = np.zeros((count, 6), np.float32)
+        self.opts.path_cap = self.path_cap
+        self.opts.path_points = pts.ctypes.data
+        self.opts.path_errors = err.ctypes.data
+        return pts, err
+
     def step(self) -> dict:
         self.event += 1
+        pts, err = self._path_buffers(1)
         rec = self.grid.run_event(self.opts, self.event)
-        r = self._record(rec)
+        r = self._record(rec, None if pts is None else (pts[0], err[0]))
         self.records.append(r)
         return r
 
     def run(self, count: int) -> list[dict]:
         """`count` events in one library call: each ion flight overlaps the
         next event's removal and relaxation.  Same records as `step`."""
+        pts, err = self._path_buffers(count)
         recs = self.grid.run_events(self.opts, self.event + 1, count)
         out = []
-        for rec in recs:
+        for k, rec in enumerate(recs):
             self.event += 1
-            r = self._record(rec)
+            r = self._record(rec, None if pts is None else (pts[k], err[k]))
             self.records.append(r)
             out.append(r)
         return out
 
-    def _record(self, rec: N.tg_event_record) -> dict:
+    def _record(self, rec: N.tg_event_record, path=None) -> dict:
         """Step VI: voltage queue and time-of-flight scale (process.cpp:985-1036)."""
         imp = rec.impact
         fb = math.sqrt(sum(float(x) ** 2 for x in rec.field_before))
@@ -553,7 +599,10 @@ class Evaporation:
             "apex": tuple(rec.apex), "status": imp.status, "steps": imp.steps, "detached": rec.detached,
             "relax_iterations": rec.relax_iterations, "rel_residual": rec.rel_residual,
             "best_probability": rec.best_probability, "second_probability": rec.second_probability,
-        }
+            "time_scale": time_scale, "charge": self.charge_mass[rec.type_id][0],
+            "mass": self.charge_mass[rec.type_id][1],
+        } | ({} if path is None else {"path": path[0][:path_length(imp, self.path_cap)].copy(),
+                                      "path_error": path[1].copy()})
 
 
 _RESULT_UNITS = ["[1]", "[1]", "[1]", "[V]"] + ["[m]"] * 6 + ["[s]", "[1]"] + \
@@ -653,3 +702,129 @@ def write_results(path: str, records: list[dict], xyz: np.ndarray, binary: bool 
                      r["probability"], r["potentialBefore"], *r["fieldBefore"], r["potentialAfter"],
                      *r["fieldAfter"], *r["normal"], *r["apex"]])
     return write_results_rows(path, rows, binary, header, chunk_size)
+
+# ---- trajectory files (LogTrajectory) -----------------------------------------
+
+_TRAJ_STATUS = {0: "NO_INTEGRATION", 1: "NO_FIELD", 2: "STEPPER_LIMIT_PASSED", 3: "ITERATION_LIMIT_PASSED",
+                4: "GEOMETRY_LIMIT_PASSED", 5: "SYSTEM_LIMIT_PASSED"}
+_TRAJ_COLUMNS = [("time", "[s]", "float"), ("positionX", "[m]", "float"), ("positionY", "[m]", "float"),
+                 ("positionZ", "[m]", "float"), ("velocityX", "[m/s]", "float"), ("velocityY", "[m/s]", "float"),
+                 ("velocityZ", "[m/s]", "float"), ("tetrahedron", "[1]", "int")]
+
+
+def _trajectory_header(binary: bool) -> bytes:
+    """LogTrajectory::writeHeader (logTrajectory.cpp:137-168)."""
+    out = ["TAPSIM TRAJECTORY DATA\nVERSION 1.0\n"]
+    for name, unit, kind in _TRAJ_COLUMNS:
+        out.append(f"# {name} {unit} ({kind})\n" if binary else f"# {name} {unit}\n")
+    out.append("\n")
+    return "".join(out).encode()
+
+
+def write_trajectory_items(path: str, items: list, binary: bool = False, chunk_size: int = 0) -> list:
+    """Trajectory files in LogTrajectory's layout (logTrajectory.cpp:170-300).
+    Each item holds index, number, time_scale, status, charge, mass, points
+    (PATH_POINT records whose time column is written as it is) and error
+    (6 floats).  With chunk_size > 0 the items go to files named
+    path.%08u after the index opening each chunk (a new chunk when
+    index % chunk_size == 0), each file with the header.  Returns the file
+    names."""
+    names, f = [], None
+    try:
+        for it in items:
+            index = int(it["index"])
+            if f is None or (chunk_size > 0 and index % chunk_size == 0):
+                if f is not None:
+                    f.close()
+                name = f"{path}.{index:08d}" if chunk_size > 0 else path
+                f = open(name, "wb")
+                names.append(name)
+                f.write(_trajectory_header(binary))
+            status = int(it["status"])
+            pts = np.asarray(it["points"], N.PATH_POINT)
+            head = (f"# index = {index}\n# unique number = {int(it['number'])}\n"
+                    f"# time scale = {_c_scientific(it['time_scale'])}\n"
+                    f"# integrator status = {status} => {_TRAJ_STATUS.get(status, 'INVALID')}\n"
+                    f"# charge [C] / mass [kg] = {_c_scientific(it['charge'])} / {_c_scientific(it['mass'])}\n")
+            f.write(head.encode())
+            if binary:
+                f.write(f"BINARY {len(pts)}\n".encode())
+                f.write(pts.tobytes())
+                f.write(b"\n")
+            else:
+                f.write(f"ASCII {len(pts)}\n".encode())
+                lines = []
+                for p in pts:
+                    vals = [p["time"], *p["position"], *p["velocity"]]
+                    lines.append("\t".join(_c_scientific(v) for v in vals) + f"\t{int(p['tet'])}\n")
+                f.write("".join(lines).encode())
+            e = [_c_scientific(v) for v in it["error"]]
+            f.write((f"# final error estimate (position) = ({e[0]}/{e[1]}/{e[2]})\n"
+                     f"# final error estimate (velocity) = ({e[3]}/{e[4]}/{e[5]})\n\n").encode())
+        if f is None:
+            f = open(path, "wb")
+            names.append(path)
+            f.write(_trajectory_header(binary))
+    finally:
+        if f is not None:
+            f.close()
+    return names
+
+
+def write_trajectories(path: str, records: list[dict], binary: bool = False, chunk_size: int = 0) -> list:
+    """Trajectory files of Evaporation records kept with path_cap > 0
+    (Process::evaporation step VII, process.cpp:1048-1049): each point's
+    time is written times the event's time scale, in float."""
+    items = []
+    for r in records:
+        if "path" not in r:
+            raise ValueError("write_trajectories: records carry no path (Evaporation(..., path_cap=...))")
+        pts = r["path"].copy()
+        pts["time"] = pts["time"] * np.float32(r["time_scale"])
+        items.append({"index": r["index"], "number": r["number"], "time_scale": r["time_scale"],
+                      "status": r["status"], "charge": r["charge"], "mass": r["mass"], "points": pts,
+                      "error": r["path_error"]})
+    return write_trajectory_items(path, items, binary, chunk_size)
+
+
+def read_trajectories(path: str) -> tuple[bool, list]:
+    """(binary, items) of one trajectory file, items as
+    write_trajectory_items takes them."""
+    data = open(path, "rb").read()
+    pos = data.index(b"\n\n") + 2  # header ends with an empty line
+    binary = b"(float)" in data[:pos]
+    items = []
+
+    def line():
+        nonlocal pos
+        end = data.index(b"\n", pos)
+        out = data[pos:end].decode()
+        pos = end + 1
+        return out
+
+    def value(text):
+        return text.split(" = ", 1)[1]
+
+    while pos < len(data):
+        index = int(value(line()))
+        number = int(value(line()))
+        ts = float(value(line()))
+        status = int(value(line()).split(" => ")[0])
+        charge, mass = (float(x) for x in value(line()).split(" / "))
+        mode, count = line().split(" ")
+        count = int(count)
+        if mode == "BINARY":
+            pts = np.frombuffer(data, N.PATH_POINT, count, pos).copy()
+            pos += count * N.PATH_POINT.itemsize + 1
+        else:
+            pts = np.zeros(count, N.PATH_POINT)
+            for k in range(count):
+                t = line().split("\t")
+                pts[k] = (float(t[0]), [float(x) for x in t[1:4]], [float(x) for x in t[4:7]], int(t[7]))
+        err = []
+        for _ in range(2):
+            err += [float(x) for x in value(line()).strip("()").split("/")]
+        line()  # the empty line after each trajectory
+        items.append({"index": index, "number": number, "time_scale": ts, "status": status, "charge": charge,
+                      "mass": mass, "points": pts, "error": np.array(err, np.float32)})
+    return binary, items

@@ -55,3 +55,18 @@ def small_mesh():
 def free_mask(arrays):
     types = arrays["types"]
     return np.array([not types[int(t)]["dirichlet"] for t in arrays["type"]])
+
+
+def path_deviation(times, xyz, ref_points, time_scale):
+    """Largest distance between a flight path (times [s], positions [m])
+    and the in-mesh points of a reference trajectory read from a LogTrajectory
+    file (times there are multiplied by the event's time scale), the path
+    interpolated linearly at the reference's times; and the reference path's
+    largest displacement from its start, to scale it by."""
+    rt = ref_points["time"].astype(np.float64) / float(np.float32(time_scale))
+    inside = ref_points["tet"] >= 0
+    rp = ref_points["position"][inside].astype(np.float64)
+    ip = np.stack([np.interp(rt[inside], times, xyz[:, c]) for c in range(3)], axis=1)
+    dev = np.linalg.norm(ip - rp, axis=1).max()
+    disp = np.linalg.norm(rp - rp[0], axis=1).max()
+    return dev, disp

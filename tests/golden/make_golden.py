@@ -35,6 +35,12 @@ With `--results` it runs the reference's own `tapsim resumption` on the
 dump for 6 events and keeps the results files its LogResults writes
 (logResults.cpp:135-381): ref_results_ascii.txt (one file) and
 ref_results_bin.00000001 / .00000004 (binary, chunk size 4).
+
+With `--trajectories` it repeats the first 3 events of ref_events.txt and
+keeps the trajectory files that the reference's own LogTrajectory writes
+for them (logTrajectory.cpp:137-300, pushed as process.cpp:1048-1049 does):
+ref_traj_ascii.txt (one file) and ref_traj_bin.00000001 / .00000002
+(binary, chunk size 2).
 """
 from __future__ import annotations
 
@@ -143,10 +149,29 @@ def results():
     shutil.rmtree(tmp)
 
 
+def trajectories():
+    if not HARNESS.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    tmp = HERE / "_tmp"
+    tmp.mkdir(exist_ok=True)
+    with gzip.open(HERE / "ref_mesh.dump.gz", "rb") as f, open(tmp / "ref.dump", "wb") as g:
+        shutil.copyfileobj(f, g)
+    for mode, name, chunk in (("ascii", "ref_traj_ascii.txt", "0"), ("binary", "ref_traj_bin", "2")):
+        subprocess.run([str(HARNESS), "evap", str(HERE / "tip.cfg"), "-", str(HERE / "oracle.ini"), "3",
+                        str(tmp / "events.txt"), "--dump", str(tmp / "ref.dump"), "--threads", "1",
+                        "--trajectories", str(tmp / name), mode, chunk], check=True, capture_output=True)
+    for name in ("ref_traj_ascii.txt", "ref_traj_bin.00000001", "ref_traj_bin.00000002"):
+        shutil.copy(tmp / name, HERE / name)
+        print("trajectories ->", name)
+    shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
     if "--modes" in sys.argv:
         modes()
     elif "--results" in sys.argv:
         results()
+    elif "--trajectories" in sys.argv:
+        trajectories()
     else:
         main()

@@ -127,3 +127,44 @@ def test_results_files_round_trip_the_reference_bytes():
         assert open(names[1], "rb").read() == (GOLDEN / "ref_results_bin.00000004").read_bytes()
     # the ASCII and binary runs are the same events
     assert [r[2] for r in rows] == [r[2] for r in rows1 + rows2]
+
+
+def test_trajectory_files_round_trip_the_reference_bytes(tmp_path):
+    """The reference's own LogTrajectory output (logTrajectory.cpp:137-300),
+    ASCII in one file and binary in chunks of 2, read and written back byte
+    for byte."""
+    from tapsim_modified_b200.tapsim import read_trajectories, write_trajectory_items
+    binary, items = read_trajectories(str(GOLDEN / "ref_traj_ascii.txt"))
+    assert not binary and [it["index"] for it in items] == [1, 2, 3]
+    assert [len(it["points"]) for it in items] == [273, 115, 120]
+    names = write_trajectory_items(str(tmp_path / "a.txt"), items)
+    assert open(names[0], "rb").read() == (GOLDEN / "ref_traj_ascii.txt").read_bytes()
+    b1, items1 = read_trajectories(str(GOLDEN / "ref_traj_bin.00000001"))
+    b2, items2 = read_trajectories(str(GOLDEN / "ref_traj_bin.00000002"))
+    assert b1 and b2 and [it["index"] for it in items1 + items2] == [1, 2, 3]
+    names = write_trajectory_items(str(tmp_path / "b"), items1 + items2, binary=True, chunk_size=2)
+    assert [n.rsplit(".", 1)[1] for n in names] == ["00000001", "00000002"]
+    assert open(names[0], "rb").read() == (GOLDEN / "ref_traj_bin.00000001").read_bytes()
+    assert open(names[1], "rb").read() == (GOLDEN / "ref_traj_bin.00000002").read_bytes()
+    # the binary points are the ASCII ones at full float precision
+    for a, b in zip(items, items1 + items2):
+        assert a["status"] == b["status"] and a["number"] == b["number"]
+        np.testing.assert_array_equal(a["points"]["tet"], b["points"]["tet"])
+        np.testing.assert_allclose(a["points"]["position"], b["points"]["position"], rtol=1e-6)
+
+
+def test_reference_trajectory_structure():
+    """Trajectory_3d's data in the reference's files: the start point at
+    time 0 and rest, steps inside the mesh, the step that leaves it with
+    tetrahedron -1, then the point extrapolated to the top of the box."""
+    from tapsim_modified_b200.tapsim import read_trajectories
+    _, items = read_trajectories(str(GOLDEN / "ref_traj_ascii.txt"))
+    for it in items:
+        p = it["points"]
+        assert it["status"] == 5
+        assert p["time"][0] == 0.0 and np.all(p["velocity"][0] == 0.0)
+        assert np.all(p["tet"][1:-2] >= 0) and p["tet"][-2] == -1 and p["tet"][-1] == -1
+        assert np.all(np.diff(p["time"]) > 0)
+        # the extrapolated point keeps the last velocity and reaches the top
+        np.testing.assert_array_equal(p["velocity"][-1], p["velocity"][-2])
+        assert abs(p["position"][-1][2] - 4.0e-8) <= 1e-14

@@ -135,3 +135,54 @@ def test_initial_velocity_matches_oracle(solved):
         assert dev.status == ref.status == 5
         d = np.hypot(dev.stop[0] - ref.stop[0], dev.stop[1] - ref.stop[1])
         assert d <= 1e-2 * np.hypot(ref.stop[0], ref.stop[1])
+
+
+def test_paths_match_oracle(solved):
+    """tg_trace_path: the recorded path (Trajectory_3d::data) and error
+    estimate against the oracle's, and the impacts of the recording kernel
+    against tg_trace's."""
+    from conftest import path_deviation
+    a, g, o = solved
+    nodes, _ = g.surface()
+    starts = nodes[:: max(1, len(nodes) // 8)][:8]
+    imps, paths, errs = g.trace_path(a["xyz"][starts], QM_FE, a["node_tet"][starts], cap=8192)
+    plain = g.trace(a["xyz"][starts], QM_FE, a["node_tet"][starts])
+    for k, node in enumerate(starts):
+        dev_imp, p, e = imps[k], paths[k], errs[k]
+        assert tuple(dev_imp.stop) == tuple(plain[k].stop) and dev_imp.steps == plain[k].steps
+        ref, rp, re = o.trace_path(a["xyz"][node], np.zeros(3), QM_FE, a["node_tet"][node], stepper_limit=200)
+        assert dev_imp.status == ref.status == 5
+        assert len(p) == dev_imp.steps + 2
+        assert abs(len(p) - len(rp)) <= 0.25 * len(rp)
+        np.testing.assert_array_equal(p["position"][0], a["xyz"][node].astype(np.float32))
+        assert p["tet"][0] == rp[0, 7] and p["time"][0] == 0.0
+        assert p["tet"][-1] == p["tet"][-2] == -1 and np.all(p["tet"][1:-2] >= 0)
+        # the oracle's path as a curve through the device's points
+        t = rp[:, 0]
+        inside = p["tet"] >= 0
+        ip = np.stack([np.interp(p["time"][inside].astype(np.float64), t, rp[:, 1 + c]) for c in range(3)], axis=1)
+        disp = np.linalg.norm(rp[:-1, 1:4] - rp[0, 1:4], axis=1).max()
+        assert np.linalg.norm(ip - p["position"][inside], axis=1).max() <= 1e-3 * disp
+        # the extrapolated point is the impact
+        np.testing.assert_array_equal(p["position"][-1], np.array(dev_imp.stop, np.float32))
+        if dev_imp.steps == ref.steps:
+            np.testing.assert_allclose(e, re, rtol=1e-3, atol=0)
+        else:
+            assert np.all((e / re > 0.1) & (e / re < 10.0))
+
+
+def test_path_cap_keeps_the_first_points(solved):
+    a, g, o = solved
+    nodes, _ = g.surface()
+    node = nodes[len(nodes) // 3]
+    _, (full,), (ef,) = g.trace_path(a["xyz"][node], QM_FE, a["node_tet"][node], cap=8192)
+    (imp,), (part,), (ep,) = g.trace_path(a["xyz"][node], QM_FE, a["node_tet"][node], cap=12)
+    assert imp.steps + 2 > 12 and len(part) == 12
+    assert part.tobytes() == full[:12].tobytes()
+    np.testing.assert_array_equal(ef, ep)
+
+
+def test_path_of_a_start_outside_is_empty(solved):
+    a, g, o = solved
+    imps, paths, errs = g.trace_path(np.array([[0.0, 0.0, 10.0]]), QM_FE, 0, cap=16)
+    assert imps[0].status == -1 and len(paths[0]) == 0 and np.all(errs[0] == 0.0)
