@@ -211,6 +211,29 @@ int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached
 /* update_coordination (surface_3d.cpp:568-593). */
 int tg_update_coordination(tg_handle* h);
 
+/* Potential, field_o1 and Grid_3d::Table::force (grid_3d.cpp:1201-1236) of
+ * cells nodes[0..count), as float (the values LogGrid::push and
+ * LogSurface::prepare collect, logGrid.cpp:119-143, logSurface.cpp:159-201);
+ * nodes NULL: every cell (count = N).  Any output may be NULL. */
+int tg_cell_values(tg_handle* h, int32_t count, const int32_t* nodes, float* phi_out, float* field_out /* [3*count] */,
+                   float* force_out /* [3*count] */);
+/* Surface_3d::Table::normal of each listed cell, one block per cell. */
+int tg_surface_normals(tg_handle* h, int32_t count, const int32_t* nodes, float* normals_out /* [3*count] */);
+/* The surface set in ascending index order with the probabilities of
+ * METHOD_EVAPORATION_PROBABILITY prob_mode, normalised as
+ * evap_compute_probabilities leaves them (surface_3d.cpp:220-420).  *count
+ * is the set's size; at most capacity cells are written. */
+int tg_surface_cells(tg_handle* h, int32_t prob_mode, float temperature, int32_t capacity, int32_t* count,
+                     int32_t* cells, float* probability);
+/* LogGrid::push + its writer thread (logGrid.cpp:119-245) for the handle's
+ * current state: writes path.%08u (index) in ASCII or binary.  numbers:
+ * the cells' unique numbers (tg_mesh_numbers), NULL for index + 1. */
+int tg_log_grid(tg_handle* h, const char* path, int32_t index, int32_t binary, const uint32_t* numbers);
+/* LogSurface::push + writer (logSurface.cpp:130-293) for the handle's
+ * current state and probability mode: writes path.%08u (index). */
+int tg_log_surface(tg_handle* h, const char* path, int32_t index, int32_t binary, int32_t with_neighbours,
+                   int32_t prob_mode, float temperature, const uint32_t* numbers);
+
 /* ---- ion flights: Trajectory_3d ---------------------------------------- */
 typedef struct {
     double time_step;           /* TRAJECTORY_INITIAL_TIME_STEP [s] */
@@ -411,6 +434,26 @@ int tg_mesh_write_config(const tg_mesh* m, const char* path);
 /* Writes a TAPSIM dump (File_Io::writeSystem layout) of the mesh with the
  * given potentials (NULL: the mesh's own). */
 int tg_mesh_write_dump(const tg_mesh* m, const char* path, const float* phi);
+/* Grid_3d::Node::number of every node: the unique numbers of the node file
+ * or dump (File_Io::readGeomGrid numbering, file_io.cpp:975-1000), index + 1
+ * for a generated tip.  numbers_out: [N]. */
+int tg_mesh_numbers(const tg_mesh* m, uint32_t* numbers_out);
+
+/* ---- grid and surface snapshots: File_Io::LogGrid / LogSurface ---------- */
+/* Writes one grid snapshot file in LogGrid's layout (logGrid.cpp:197-245):
+ * for each of n cells the type id, unique number, potential, field [3] and
+ * force [3]. */
+int tg_grid_log_write(const char* path, int32_t binary, int32_t n, const int32_t* id, const uint32_t* number,
+                      const float* phi, const float* field, const float* force);
+/* Writes one surface snapshot file in LogSurface's layout
+ * (logSurface.cpp:203-293): n_cells surface cells (ascending) with type,
+ * unique number, probability and, when neighbour_ptr is not NULL, their
+ * neighbour lists neighbours[neighbour_ptr[c] .. neighbour_ptr[c+1]); then
+ * n_nodes cells (ascending) with potential, field [3] and normal [3]. */
+int tg_surface_log_write(const char* path, int32_t binary, int32_t n_cells, const int32_t* cells, const int32_t* type,
+                         const uint32_t* number, const float* probability, const int32_t* neighbour_ptr,
+                         const int32_t* neighbours, int32_t n_nodes, const int32_t* nodes, const float* phi,
+                         const float* field, const float* normal);
 
 #ifdef __cplusplus
 }

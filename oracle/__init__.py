@@ -66,6 +66,8 @@ def lib():
         L.orc_relax_cycles.argtypes = [P, C.c_int32]
         L.orc_field_o1.restype = C.c_int
         L.orc_field_o1.argtypes = [P, C.c_int32, C.c_void_p]
+        L.orc_force.restype = None
+        L.orc_force.argtypes = [P, C.c_int32, C.c_void_p]
         L.orc_surface_init.restype = C.c_int32
         L.orc_surface_init.argtypes = [P, C.c_int32]
         L.orc_select.restype = None
@@ -171,6 +173,11 @@ class Oracle:
     def field_o1(self, node: int) -> np.ndarray:
         out = np.zeros(3, np.float64)
         self.L.orc_field_o1(C.byref(self.m), int(node), _p(out))
+        return out
+
+    def force(self, node: int) -> np.ndarray:
+        out = np.zeros(3, np.float64)
+        self.L.orc_force(C.byref(self.m), int(node), _p(out))
         return out
 
     def surface_init(self, vacuum_id: int) -> int:

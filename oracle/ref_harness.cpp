@@ -30,6 +30,11 @@
 //                            write every event's trajectory with the
 //                            reference's own File_Io::LogTrajectory, as
 //                            process.cpp:1048-1049 pushes it
+//       --grids <file> <ascii|binary>
+//       --surfaces <file> <ascii|binary> <neighbours 0|1>
+//                            snapshots after every event with the reference's
+//                            own File_Io::LogGrid / LogSurface
+//                            (process.cpp:1068-1072 with interval 1)
 
 #include <cstdio>
 #include <cstdlib>
@@ -50,6 +55,8 @@
 #include "process.h"
 #include "file_io.h"
 #include "logTrajectory.h"
+#include "logGrid.h"
+#include "logSurface.h"
 
 // commands.cpp (linked for makeIniList) refers to these globals, which the
 // reference defines next to main() in tapsim.cpp.
@@ -105,6 +112,11 @@ static int cmd_evap(int argc, char** argv)
 	const char* trajName = 0;
 	int trajMode = File_Io::ASCII;
 	unsigned trajChunk = 0;
+	const char* gridName = 0;
+	int gridMode = File_Io::ASCII;
+	const char* surfName = 0;
+	int surfMode = File_Io::ASCII;
+	bool surfNeighbours = false;
 	int initRelax = 1;
 	bool initGiven = false;
 	bool noSync = false;
@@ -133,9 +145,22 @@ static int cmd_evap(int argc, char** argv)
 			trajMode = strcmp(argv[++a], "binary") ? File_Io::ASCII : File_Io::BINARY;
 			trajChunk = atoi(argv[++a]);
 		}
+		else if (!strcmp(argv[a], "--grids") && a + 2 < argc)
+		{
+			gridName = argv[++a];
+			gridMode = strcmp(argv[++a], "binary") ? File_Io::ASCII : File_Io::BINARY;
+		}
+		else if (!strcmp(argv[a], "--surfaces") && a + 3 < argc)
+		{
+			surfName = argv[++a];
+			surfMode = strcmp(argv[++a], "binary") ? File_Io::ASCII : File_Io::BINARY;
+			surfNeighbours = atoi(argv[++a]) != 0;
+		}
 		else { fprintf(stderr, "unknown option %s\n", argv[a]); return 2; }
 	}
 	File_Io::LogTrajectory* trajLog = trajName ? new File_Io::LogTrajectory(trajName, trajMode, 0, trajChunk) : 0;
+	File_Io::LogGrid* gridLog = 0;  // created once the system is loaded
+	File_Io::LogSurface* surfLog = 0;
 
 	std::srand(99); // as main() does (tapsim.cpp:235)
 
@@ -321,8 +346,21 @@ static int cmd_evap(int argc, char** argv)
 		fflush(out);
 		if (phiEvents) write_phi(phiEvents, system);
 		if (trajLog) trajLog->push(ev + 1, system.gridTable.number(nodeIndex).toValue(), timeScale, trajectory);
+		if (gridName)
+		{
+			if (!gridLog) gridLog = new File_Io::LogGrid(gridName, &system.geomTable, &system.configTable, gridMode);
+			gridLog->push(ev + 1, system.gridTable);
+		}
+		if (surfName)
+		{
+			if (!surfLog) surfLog = new File_Io::LogSurface(surfName, &system, surfMode, 0, 0, surfNeighbours);
+			surfLog->push(ev + 1, surfaceTable);
+		}
 	}
-	delete trajLog;  // joins the writer thread after it has written the queue
+	// the destructors join the writer threads after they have written their queues
+	delete trajLog;
+	delete gridLog;
+	delete surfLog;
 	fclose(out);
 	if (phiEvents) fclose(phiEvents);
 	return 0;

@@ -77,6 +77,26 @@ double orc_relax_cycles(orc_mesh* m, int32_t n) {
     return dev;
 }
 
+/* Grid_3d::Table::force (grid_3d.cpp:1201-1236) in FP64: sum over the
+ * neighbours of eps0 c_ij (phi_j - phi_i)^2 (1/eps_j - 1/eps_i) d / |d|^2,
+ * d = x_j - x_i */
+void orc_force(const orc_mesh* m, int32_t i, double F[3]) {
+    const double eps0 = 8.85418781762e-12;
+    const double ei = 1.0 / m->types[m->type[i]].epsilon;
+    F[0] = F[1] = F[2] = 0.0;
+    for (int32_t q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+        const int32_t j = m->col[q];
+        const double dp = m->phi[j] - m->phi[i];
+        const double mag = eps0 * m->c[q] * dp * dp * (1.0 / m->types[m->type[j]].epsilon - ei);
+        double d[3], d2 = 0.0;
+        for (int k = 0; k < 3; k++) {
+            d[k] = (double)m->xyz[3 * j + k] - (double)m->xyz[3 * i + k];
+            d2 += d[k] * d[k];
+        }
+        for (int k = 0; k < 3; k++) F[k] += d[k] * mag / d2;
+    }
+}
+
 /* Grid_3d::Table::field_o1 (grid_3d.cpp:909-991) in FP64 */
 int orc_field_o1(const orc_mesh* m, int32_t i, double E[3]) {
     E[0] = E[1] = E[2] = 0.0;

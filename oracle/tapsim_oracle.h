@@ -46,6 +46,8 @@ int64_t orc_solve(orc_mesh* m, double tol, int64_t max_sweeps, double omega, dou
 double orc_relax_cycles(orc_mesh* m, int32_t n);
 /* Grid_3d::Table::field_o1; returns 0 when the 3x3 system is singular */
 int orc_field_o1(const orc_mesh* m, int32_t i, double E[3]);
+/* Grid_3d::Table::force (grid_3d.cpp:1201-1236) */
+void orc_force(const orc_mesh* m, int32_t i, double F[3]);
 /* Surface_3d::Table::init; returns the number of surface cells */
 int32_t orc_surface_init(orc_mesh* m, int32_t vacuum_id);
 /* specific fields + probabilities + evapMaximum + apex over the surface set */

@@ -130,6 +130,14 @@ SIGNATURES = {
     "tg_update_coordination": (C.c_int, [_P]),
     "tg_trace": (C.c_int, [_P, _I, _P, _P, _P, _P, C.POINTER(tg_trace_opts), _P]),
     "tg_trace_path": (C.c_int, [_P, _I, _P, _P, _P, _P, C.POINTER(tg_trace_opts), _I, _P, _P, _P]),
+    "tg_cell_values": (C.c_int, [_P, _I, _P, _P, _P, _P]),
+    "tg_surface_normals": (C.c_int, [_P, _I, _P, _P]),
+    "tg_surface_cells": (C.c_int, [_P, _I, C.c_float, _I, C.POINTER(_I), _P, _P]),
+    "tg_log_grid": (C.c_int, [_P, C.c_char_p, _I, _I, _P]),
+    "tg_log_surface": (C.c_int, [_P, C.c_char_p, _I, _I, _I, _I, C.c_float, _P]),
+    "tg_mesh_numbers": (C.c_int, [_P, _P]),
+    "tg_grid_log_write": (C.c_int, [C.c_char_p, _I, _I, _P, _P, _P, _P, _P]),
+    "tg_surface_log_write": (C.c_int, [C.c_char_p, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P]),
     "tg_potential_at": (C.c_int, [_P, _I, _P, _P, _P]),
     "tg_run_event": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, C.POINTER(tg_event_record)]),
     "tg_run_events": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, _I, _P, C.POINTER(C.c_int32)]),

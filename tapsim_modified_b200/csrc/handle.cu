@@ -109,6 +109,7 @@ struct tg_handle {
     DBuf<int> statusTrace;
     DBuf<double> phiTrace;
     std::vector<int32_t> h_row_ptr;
+    std::vector<int32_t> h_col;  // the Delaunay neighbours never change
 
     // non-Neumann free rows in slot order, SELL-32 (cg.cu)
     DBuf<int32_t> vSlotOf, vNodeOf, vSliceStart, vSliceWidth, vCol, vPos, vCount;
@@ -496,6 +497,7 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     h->snap = amax > 0.0 ? std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 40) / amax))) : 1.0;
     h->h_xyz.assign(d->xyz, d->xyz + 3 * (size_t)n);
     h->h_row_ptr.assign(d->row_ptr, d->row_ptr + n + 1);
+    h->h_col.assign(d->col, d->col + d->row_ptr[n]);
     if (d->node_tet) h->h_node_tet.assign(d->node_tet, d->node_tet + n);
 
     // ---- V system: slots, SELL-32 couplings, append reserve ----
@@ -1192,6 +1194,143 @@ int tg_surface_pick(tg_handle* h, double u, int32_t* node, float* probability) {
         }
         *probability = sc / fsum;
     }
+    return TG_OK;
+}
+
+int tg_cell_values(tg_handle* h, int32_t count, const int32_t* nodes, float* phi, float* field, float* force) {
+    if (!h || count < 0 || (!nodes && count != h->n))
+        return fail(h, TG_ERR_ARGUMENT, "tg_cell_values: bad argument (nodes NULL needs count = N)");
+    if (nodes)
+        for (int32_t k = 0; k < count; k++)
+            if (nodes[k] < 0 || nodes[k] >= h->n) return fail(h, TG_ERR_ARGUMENT, "tg_cell_values: node out of range");
+    if (count == 0 || (!phi && !field && !force)) return TG_OK;
+    int rc = stage(h, h->stageF, 7 * (size_t)count);
+    if (rc == TG_OK && nodes) rc = stage(h, h->stageI, count);
+    if (rc != TG_OK) return rc;
+    float* dPhi = h->stageF.p;
+    float* dField = dPhi + count;
+    float* dForce = dField + 3 * (size_t)count;
+    if (nodes) CK(cudaMemcpyAsync(h->stageI.p, nodes, sizeof(int32_t) * count, cudaMemcpyHostToDevice, h->stream));
+    launch_cell_values(h->dm(), nodes ? h->stageI.p : nullptr, count, phi ? dPhi : nullptr, field ? dField : nullptr,
+                       force ? dForce : nullptr, h->stream);
+    if (phi) CK(cudaMemcpyAsync(phi, dPhi, sizeof(float) * count, cudaMemcpyDeviceToHost, h->stream));
+    if (field) CK(cudaMemcpyAsync(field, dField, sizeof(float) * 3 * count, cudaMemcpyDeviceToHost, h->stream));
+    if (force) CK(cudaMemcpyAsync(force, dForce, sizeof(float) * 3 * count, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_cell_values");
+}
+
+int tg_surface_normals(tg_handle* h, int32_t count, const int32_t* nodes, float* normals) {
+    if (!h || count < 0 || (count && (!nodes || !normals))) return fail(h, TG_ERR_ARGUMENT, "tg_surface_normals: bad argument");
+    if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_normals: surface not initialised");
+    for (int32_t k = 0; k < count; k++)
+        if (nodes[k] < 0 || nodes[k] >= h->n) return fail(h, TG_ERR_ARGUMENT, "tg_surface_normals: node out of range");
+    if (count == 0) return TG_OK;
+    int rc = stage(h, h->stageF, 3 * (size_t)count);
+    if (rc == TG_OK) rc = stage(h, h->stageI, count);
+    if (rc != TG_OK) return rc;
+    CK(cudaMemcpyAsync(h->stageI.p, nodes, sizeof(int32_t) * count, cudaMemcpyHostToDevice, h->stream));
+    launch_surface_normals(h->dm(), h->stageI.p, count, h->vacuumId, h->stageF.p, h->stream);
+    CK(cudaMemcpyAsync(normals, h->stageF.p, sizeof(float) * 3 * count, cudaMemcpyDeviceToHost, h->stream));
+    return sync_status(h, "tg_surface_normals");
+}
+
+int tg_surface_cells(tg_handle* h, int32_t mode, float temperature, int32_t capacity, int32_t* count, int32_t* cells,
+                     float* probability) {
+    if (!h || !count || capacity < 0 || (capacity && (!cells || !probability)))
+        return fail(h, TG_ERR_ARGUMENT, "tg_surface_cells: bad argument");
+    *count = 0;
+    tg_select_info info;
+    int rc = tg_surface_select_mode(h, mode, temperature, &info);
+    if (rc == TG_ERR_NO_SURFACE) return TG_OK;
+    if (rc != TG_OK) return rc;
+    std::vector<int32_t> list(h->surfSlots);
+    std::vector<float> score(h->surfSlots);
+    CK(cudaMemcpyAsync(list.data(), h->surfList.p, sizeof(int32_t) * h->surfSlots, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(score.data(), h->surfScore.p, sizeof(float) * h->surfSlots, cudaMemcpyDeviceToHost, h->stream));
+    rc = sync_status(h, "tg_surface_cells");
+    if (rc != TG_OK) return rc;
+    std::vector<std::pair<int32_t, float>> set;
+    set.reserve(h->surfSlots);
+    for (int s = 0; s < h->surfSlots; s++)
+        if (list[s] >= 0) set.emplace_back(list[s], score[s]);
+    std::sort(set.begin(), set.end());
+    // evap_compute_probabilities normalises each cell's value by the sum
+    // over the set, in float
+    const float fsum = (float)info.score_sum;
+    for (size_t k = 0; k < set.size() && (int32_t)k < capacity; k++) {
+        cells[k] = set[k].first;
+        probability[k] = set[k].second / fsum;
+    }
+    *count = (int32_t)set.size();
+    return TG_OK;
+}
+
+static std::string snapshot_name(const char* path, int32_t index) {
+    char suffix[16];
+    snprintf(suffix, sizeof(suffix), ".%08u", (unsigned)index);
+    return std::string(path) + suffix;
+}
+
+int tg_log_grid(tg_handle* h, const char* path, int32_t index, int32_t binary, const uint32_t* numbers) {
+    if (!h || !path) return fail(h, TG_ERR_ARGUMENT, "tg_log_grid: null argument");
+    const int n = h->n;
+    std::vector<float> phi(n), field(3 * (size_t)n), force(3 * (size_t)n);
+    int rc = tg_cell_values(h, n, nullptr, phi.data(), field.data(), force.data());
+    if (rc != TG_OK) return rc;
+    std::vector<int8_t> t8(n);
+    if ((rc = tg_get_types(h, t8.data())) != TG_OK) return rc;
+    std::vector<int32_t> id(t8.begin(), t8.end());
+    std::vector<uint32_t> num(n);
+    for (int i = 0; i < n; i++) num[i] = numbers ? numbers[i] : (uint32_t)(i + 1);
+    rc = tg_grid_log_write(snapshot_name(path, index).c_str(), binary, n, id.data(), num.data(), phi.data(),
+                           field.data(), force.data());
+    if (rc != TG_OK) return fail(h, rc, tg_last_error(nullptr));
+    return TG_OK;
+}
+
+int tg_log_surface(tg_handle* h, const char* path, int32_t index, int32_t binary, int32_t withNeighbours,
+                   int32_t mode, float temperature, const uint32_t* numbers) {
+    if (!h || !path) return fail(h, TG_ERR_ARGUMENT, "tg_log_surface: null argument");
+    const int n = h->n;
+    int32_t nc = 0;
+    int rc = tg_surface_cells(h, mode, temperature, 0, &nc, nullptr, nullptr);
+    if (rc != TG_OK) return rc;
+    std::vector<int32_t> cells(nc);
+    std::vector<float> prob(nc);
+    if (nc && (rc = tg_surface_cells(h, mode, temperature, nc, &nc, cells.data(), prob.data())) != TG_OK) return rc;
+    std::vector<int8_t> t8(n);
+    if ((rc = tg_get_types(h, t8.data())) != TG_OK) return rc;
+    // LogSurface::prepare (logSurface.cpp:159-201): the cells, their
+    // neighbour lists, and every cell and neighbour once, ascending
+    std::vector<int32_t> type(nc), nptr(nc + 1, 0), nb;
+    std::vector<uint32_t> num(nc);
+    std::vector<char> mark(n, 0);
+    for (int c = 0; c < nc; c++) {
+        const int i = cells[c];
+        type[c] = t8[i];
+        num[c] = numbers ? numbers[i] : (uint32_t)(i + 1);
+        mark[i] = 1;
+        for (int q = h->h_row_ptr[i]; q < h->h_row_ptr[i + 1]; q++) {
+            nb.push_back(h->h_col[q]);
+            mark[h->h_col[q]] = 1;
+        }
+        nptr[c + 1] = (int32_t)nb.size();
+    }
+    std::vector<int32_t> nodes;
+    for (int i = 0; i < n; i++)
+        if (mark[i]) nodes.push_back(i);
+    const int nn = (int)nodes.size();
+    std::vector<float> phi(nn), field(3 * (size_t)nn), normal(3 * (size_t)nn, 0.0f), cellNormal(3 * (size_t)nc);
+    if (nn && (rc = tg_cell_values(h, nn, nodes.data(), phi.data(), field.data(), nullptr)) != TG_OK) return rc;
+    if (nc && (rc = tg_surface_normals(h, nc, cells.data(), cellNormal.data())) != TG_OK) return rc;
+    for (int c = 0; c < nc; c++) {
+        const size_t k = std::lower_bound(nodes.begin(), nodes.end(), cells[c]) - nodes.begin();
+        for (int j = 0; j < 3; j++) normal[3 * k + j] = cellNormal[3 * (size_t)c + j];
+    }
+    rc = tg_surface_log_write(snapshot_name(path, index).c_str(), binary, nc, cells.data(), type.data(), num.data(),
+                              prob.data(), withNeighbours ? nptr.data() : nullptr, nb.data(), nn, nodes.data(),
+                              phi.data(), field.data(), normal.data());
+    if (rc != TG_OK) return fail(h, rc, tg_last_error(nullptr));
     return TG_OK;
 }
 

@@ -526,4 +526,81 @@ std::string write_results(const std::string& path, const std::vector<ResultRecor
     return f.good() ? std::string() : "results: write error";
 }
 
+std::string write_grid_log(const std::string& path, bool binary, const GridLog& g) {
+    std::ofstream f(path, std::ios::binary | std::ios::trunc);
+    if (!f.good()) return "grid log: cannot write " + path;
+    f << "TAPSIM GRID DATA\nVERSION 1.0\n" << (binary ? "BINARY " : "ASCII ") << g.n << '\n';
+    std::string buf;
+    for (int i = 0; i < g.n; i++) {
+        const float* E = g.field + 3 * (size_t)i;
+        const float* F = g.force + 3 * (size_t)i;
+        if (binary) {
+            wr(f, (short)g.id[i]);
+            wr(f, g.number[i]);
+            wr(f, g.phi[i]);
+            for (int k = 0; k < 3; k++) wr(f, E[k]);
+            for (int k = 0; k < 3; k++) wr(f, F[k]);
+        } else {
+            char line[512];
+            const int len = snprintf(line, sizeof(line), "%d\t%u\t%e\t%e\t%e\t%e\t%e\t%e\t%e\n", (int)(short)g.id[i],
+                                     g.number[i], g.phi[i], E[0], E[1], E[2], F[0], F[1], F[2]);
+            buf.append(line, len);
+            if (buf.size() > (1u << 20)) {
+                f.write(buf.data(), buf.size());
+                buf.clear();
+            }
+        }
+    }
+    f.write(buf.data(), buf.size());
+    return f.good() ? std::string() : "grid log: write error";
+}
+
+std::string write_surface_log(const std::string& path, bool binary, const SurfaceLog& s) {
+    std::ofstream f(path, std::ios::binary | std::ios::trunc);
+    if (!f.good()) return "surface log: cannot write " + path;
+    f << "TAPSIM SURFACE DATA\nVERSION 1.0\n" << (binary ? "BINARY" : "ASCII") << "\n\n";
+    f << "CELLS " << s.cells << '\n';
+    char line[512];
+    for (int c = 0; c < s.cells; c++) {
+        const int q0 = s.neighbour_ptr ? s.neighbour_ptr[c] : 0, q1 = s.neighbour_ptr ? s.neighbour_ptr[c + 1] : 0;
+        if (binary) {
+            wr(f, s.cell[c]);
+            wr(f, (short)s.type[c]);
+            wr(f, s.number[c]);
+            wr(f, s.probability[c]);
+            wr(f, (uint32_t)(q1 - q0));
+            for (int q = q0; q < q1; q++) wr(f, s.neighbours[q]);
+        } else {
+            int len = snprintf(line, sizeof(line), "%d\t%d\t%u\t%e", s.cell[c], (int)(short)s.type[c], s.number[c],
+                               s.probability[c]);
+            f.write(line, len);
+            if (s.neighbour_ptr) {
+                len = snprintf(line, sizeof(line), "\t%d", q1 - q0);
+                f.write(line, len);
+                for (int q = q0; q < q1; q++) {
+                    len = snprintf(line, sizeof(line), "\t%d", s.neighbours[q]);
+                    f.write(line, len);
+                }
+            }
+            f << '\n';
+        }
+    }
+    f << '\n' << "NODES " << s.nodes << '\n';
+    for (int k = 0; k < s.nodes; k++) {
+        const float* E = s.field + 3 * (size_t)k;
+        const float* N = s.normal + 3 * (size_t)k;
+        if (binary) {
+            wr(f, s.node[k]);
+            wr(f, s.phi[k]);
+            for (int j = 0; j < 3; j++) wr(f, E[j]);
+            for (int j = 0; j < 3; j++) wr(f, N[j]);
+        } else {
+            const int len = snprintf(line, sizeof(line), "%d\t%e\t%e\t%e\t%e\t%e\t%e\t%e\n", s.node[k], s.phi[k], E[0],
+                                     E[1], E[2], N[0], N[1], N[2]);
+            f.write(line, len);
+        }
+    }
+    return f.good() ? std::string() : "surface log: write error";
+}
+
 }  // namespace tg_host

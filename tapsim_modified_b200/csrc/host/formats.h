@@ -95,4 +95,39 @@ struct ResultRecord {
 std::string write_results(const std::string& path, const std::vector<ResultRecord>& recs, bool binary,
                           const std::string& header);
 
+// One grid snapshot as File_Io::LogGrid writes it (logGrid.cpp:197-245):
+// per cell the type id, unique number, potential, field_o1 [3] and
+// force [3].
+struct GridLog {
+    int n;
+    const int32_t* id;
+    const uint32_t* number;
+    const float* phi;
+    const float* field;
+    const float* force;
+};
+std::string write_grid_log(const std::string& path, bool binary, const GridLog& g);
+
+// One surface snapshot as File_Io::LogSurface::writer writes it
+// (logSurface.cpp:203-293): the surface cells in ascending index order with
+// type, unique number, probability and optionally their neighbour lists
+// (neighbour_ptr null: none), then the cells and all their neighbours in
+// ascending order with potential, field_o1 [3] and normal [3] (zero for
+// cells off the surface).
+struct SurfaceLog {
+    int cells;
+    const int32_t* cell;
+    const int32_t* type;
+    const uint32_t* number;
+    const float* probability;
+    const int32_t* neighbour_ptr;  // [cells + 1]
+    const int32_t* neighbours;
+    int nodes;
+    const int32_t* node;
+    const float* phi;
+    const float* field;
+    const float* normal;
+};
+std::string write_surface_log(const std::string& path, bool binary, const SurfaceLog& s);
+
 }  // namespace tg_host

@@ -279,6 +279,27 @@ int tg_mesh_from_dump(const char* dumpFile, const char* configFile, tg_mesh** ou
                 delete m;
                 return mesh_fail("tg_mesh_from_dump: neighbour lists are not ascending");
             }
+    for (int32_t c : m->col)
+        if (c < 0 || c >= n) {
+            delete m;
+            return mesh_fail("tg_mesh_from_dump: neighbour index out of range");
+        }
+    // The dump's couplings were computed with the dump's own type table
+    // (computeCoupling, grid_3d.cpp:1392-1409: 2 e1 e2 / (e1 + e2) times
+    // area / distance).  Dividing that table's permittivity factor out gives
+    // each entry's geometric factor, so that a removal resynced under another
+    // configuration sees the true geometry, as the reference's does.
+    auto eps = [&](int id) {
+        const auto it = d.config.types.find(id);
+        return it == d.config.types.end() ? 1.0 : (double)it->second.epsilon;
+    };
+    m->geom.resize(m->coupling.size());
+    for (int i = 0; i < n; i++)
+        for (int q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+            const double e1 = eps(m->type[i]), e2 = eps(m->type[m->col[q]]);
+            m->geom[q] = m->coupling[q] / (2.0 * e1 * e2 / (e1 + e2));
+        }
+    m->has_geom = true;
     *out = m;
     return TG_OK;
 }
@@ -323,6 +344,35 @@ int tg_mesh_write_node_file(const tg_mesh* m, const char* path, int32_t binary) 
 int tg_mesh_write_config(const tg_mesh* m, const char* path) {
     if (!m || !path) return mesh_fail("tg_mesh_write_config: null argument");
     const std::string err = write_config_ascii(path, m->config);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
+int tg_mesh_numbers(const tg_mesh* m, uint32_t* out) {
+    if (!m || !out) return mesh_fail("tg_mesh_numbers: null argument");
+    const size_t n = m->type.size();
+    for (size_t i = 0; i < n; i++) out[i] = m->number.size() == n ? m->number[i] : (uint32_t)(i + 1);
+    return TG_OK;
+}
+
+int tg_grid_log_write(const char* path, int32_t binary, int32_t n, const int32_t* id, const uint32_t* number,
+                      const float* phi, const float* field, const float* force) {
+    if (!path || n < 0 || (n && (!id || !number || !phi || !field || !force)))
+        return mesh_fail("tg_grid_log_write: bad argument");
+    GridLog g{n, id, number, phi, field, force};
+    const std::string err = write_grid_log(path, binary != 0, g);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
+int tg_surface_log_write(const char* path, int32_t binary, int32_t nCells, const int32_t* cells, const int32_t* type,
+                         const uint32_t* number, const float* probability, const int32_t* neighbourPtr,
+                         const int32_t* neighbours, int32_t nNodes, const int32_t* nodes, const float* phi,
+                         const float* field, const float* normal) {
+    if (!path || nCells < 0 || nNodes < 0 || (nCells && (!cells || !type || !number || !probability)) ||
+        (nNodes && (!nodes || !phi || !field || !normal)) || (neighbourPtr && nCells && !neighbours &&
+                                                               neighbourPtr[nCells] > 0))
+        return mesh_fail("tg_surface_log_write: bad argument");
+    SurfaceLog sl{nCells, cells, type, number, probability, neighbourPtr, neighbours, nNodes, nodes, phi, field, normal};
+    const std::string err = write_surface_log(path, binary != 0, sl);
     return err.empty() ? TG_OK : mesh_fail(err);
 }
 

@@ -158,6 +158,13 @@ void launch_take_away(const DevMesh& m, RowLists rl, Surface sf, int node, int v
                       int resultCap, cudaStream_t s);
 void launch_update_coordination(const DevMesh& m, int8_t* scratchType, cudaStream_t s);
 void launch_surface_normal(const DevMesh& m, Surface sf, int node, int vacuumId, float* out, cudaStream_t s);
+// the normals of a list of cells, one block each
+void launch_surface_normals(const DevMesh& m, const int32_t* nodes, int count, int vacuumId, float* out,
+                            cudaStream_t s);
+// potential, field_o1 and Grid_3d force (float) of a list of cells, or of
+// every cell when nodes is null; outputs may be null
+void launch_cell_values(const DevMesh& m, const int32_t* nodes, int count, float* phi, float* field, float* force,
+                        cudaStream_t s);
 
 // ---- flights (flight.cu) ----
 struct TraceParams {

@@ -53,6 +53,51 @@ __global__ void k_field_o1(DevMesh m, const int32_t* nodes, int count, double* o
     out[3 * t + 2] = E[2];
 }
 
+// Grid_3d::Table::force (grid_3d.cpp:1201-1236) in FP64: the dielectric
+// force on cell i, sum over its neighbours j of
+// eps0 c_ij (phi_j - phi_i)^2 (1/eps_j - 1/eps_i) (x_j - x_i) / |x_j - x_i|^2.
+__device__ void cell_force(const DevMesh& m, int i, double F[3]) {
+    F[0] = F[1] = F[2] = 0.0;
+    const double xi = m.xyz[3 * i], yi = m.xyz[3 * i + 1], zi = m.xyz[3 * i + 2];
+    const double pi = m.phi64[i];
+    const double ei = 1.0 / (double)m.types[m.type[i]].epsilon;
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+        const int j = m.col[q];
+        const double dp = m.phi64[j] - pi;
+        const double mag = dp * dp * kEpsilon0 * m.c64[q] * (1.0 / (double)m.types[m.type[j]].epsilon - ei);
+        const double dx = (double)m.xyz[3 * j] - xi, dy = (double)m.xyz[3 * j + 1] - yi, dz = (double)m.xyz[3 * j + 2] - zi;
+        const double s = mag / (dx * dx + dy * dy + dz * dz);
+        F[0] += dx * s;
+        F[1] += dy * s;
+        F[2] += dz * s;
+    }
+}
+
+// Potential, field_o1 and force of cells nodes[0..count) (all cells when
+// nodes is null), as float: the values File_Io::LogGrid::push
+// (logGrid.cpp:119-143) and LogSurface::prepare (logSurface.cpp:159-201)
+// collect.  Any output may be null.
+__global__ void k_cell_values(DevMesh m, const int32_t* nodes, int count, float* phi, float* field, float* force) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int i = nodes ? nodes[k] : k;
+    if (phi) phi[k] = (float)m.phi64[i];
+    if (field) {
+        double E[3];
+        if (!field_o1(m, i, E)) atomicOr(m.status, S_SINGULAR);
+        field[3 * (size_t)k] = (float)E[0];
+        field[3 * (size_t)k + 1] = (float)E[1];
+        field[3 * (size_t)k + 2] = (float)E[2];
+    }
+    if (force) {
+        double F[3];
+        cell_force(m, i, F);
+        force[3 * (size_t)k] = (float)F[0];
+        force[3 * (size_t)k + 1] = (float)F[1];
+        force[3 * (size_t)k + 2] = (float)F[2];
+    }
+}
+
 // A removable, non-vacuum cell with a vacuum neighbour across a face of
 // positive area (Surface_3d::Table::init/update, surface_3d.cpp:50-119).
 __device__ bool is_surface_candidate(const DevMesh& m, int i, int vacuumId) {
@@ -426,7 +471,7 @@ __global__ void k_coordination(DevMesh m, const int8_t* before) {
 // geometry_3d.cpp:1806-1870), oriented towards the vacuum cells of the
 // neighbourhood.  One block; Jacobi eigen-iteration in FP64.
 constexpr int kNHash = 4096;
-__global__ void k_surface_normal(DevMesh m, Surface sf, int node, int vacuumId, float* out) {
+__device__ void surface_normal(const DevMesh& m, int node, int vacuumId, float* out) {
     __shared__ int32_t keys[kNHash];
     __shared__ int32_t frontier[kNHash];
     __shared__ int fs, fe, tail;
@@ -529,6 +574,15 @@ __global__ void k_surface_normal(DevMesh m, Surface sf, int node, int vacuumId, 
     out[2] = (float)n2;
 }
 
+__global__ void k_surface_normal(DevMesh m, int node, int vacuumId, float* out) {
+    surface_normal(m, node, vacuumId, out);
+}
+
+// The normals of cells nodes[0..count), one block each.
+__global__ void k_surface_normals(DevMesh m, const int32_t* nodes, int vacuumId, float* out) {
+    surface_normal(m, nodes[blockIdx.x], vacuumId, out + 3 * (size_t)blockIdx.x);
+}
+
 inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 
 }  // namespace
@@ -570,7 +624,16 @@ void launch_update_coordination(const DevMesh& m, int8_t* scratchType, cudaStrea
     { count_launch(); k_coordination<<<blocks(m.n), kBlock, 0, s>>>(m, scratchType); }
 }
 void launch_surface_normal(const DevMesh& m, Surface sf, int node, int vacuumId, float* out, cudaStream_t s) {
-    { count_launch(); k_surface_normal<<<1, 256, 0, s>>>(m, sf, node, vacuumId, out); }
+    (void)sf;
+    { count_launch(); k_surface_normal<<<1, 256, 0, s>>>(m, node, vacuumId, out); }
+}
+void launch_surface_normals(const DevMesh& m, const int32_t* nodes, int count, int vacuumId, float* out,
+                            cudaStream_t s) {
+    if (count > 0) { count_launch(); k_surface_normals<<<count, 256, 0, s>>>(m, nodes, vacuumId, out); }
+}
+void launch_cell_values(const DevMesh& m, const int32_t* nodes, int count, float* phi, float* field, float* force,
+                        cudaStream_t s) {
+    if (count > 0) { count_launch(); k_cell_values<<<blocks(count), kBlock, 0, s>>>(m, nodes, count, phi, field, force); }
 }
 
 }  // namespace tgd

@@ -115,6 +115,13 @@ class Mesh:
             "types": {t.id: {f: getattr(t, f) for f, _ in N.tg_type._fields_} for t in types},
         }
 
+    def numbers(self) -> np.ndarray:
+        """Grid_3d::Node::number of every node (the node file's or dump's
+        unique numbers; index + 1 for a generated tip)."""
+        out = np.empty(self._desc.num_nodes, np.uint32)
+        N.check(N.lib().tg_mesh_numbers(self._h, N.ptr(out)))
+        return out
+
     def write_node_file(self, path: str, binary: bool = True):
         N.check(N.lib().tg_mesh_write_node_file(self._h, str(path).encode(), int(binary)))
 
@@ -255,6 +262,47 @@ class Grid:
         self._ck(N.lib().tg_get_surface(self._h, cnt.value, N.ptr(nodes), N.ptr(ratios), C.byref(cnt)))
         order = np.argsort(nodes)
         return nodes[order], ratios[order]
+
+    def cell_values(self, nodes=None, force: bool = True):
+        """(phi, field [n, 3], force [n, 3] or None) as float of the listed
+        cells, or of every cell (tg_cell_values)."""
+        idx = None if nodes is None else np.ascontiguousarray(nodes, np.int32)
+        n = self.n if idx is None else len(idx)
+        phi = np.empty(n, np.float32)
+        field = np.empty((n, 3), np.float32)
+        frc = np.empty((n, 3), np.float32) if force else None
+        self._ck(N.lib().tg_cell_values(self._h, n, N.ptr(idx), N.ptr(phi), N.ptr(field), N.ptr(frc)))
+        return phi, field, frc
+
+    def surface_normals(self, nodes) -> np.ndarray:
+        idx = np.ascontiguousarray(nodes, np.int32)
+        out = np.empty((len(idx), 3), np.float32)
+        self._ck(N.lib().tg_surface_normals(self._h, len(idx), N.ptr(idx), N.ptr(out)))
+        return out
+
+    def surface_cells(self, mode: int = 0, temperature: float = 0.0):
+        """(cells ascending, probabilities) of probability mode `mode`."""
+        cnt = C.c_int32()
+        self._ck(N.lib().tg_surface_cells(self._h, mode, temperature, 0, C.byref(cnt), None, None))
+        cells = np.empty(cnt.value, np.int32)
+        prob = np.empty(cnt.value, np.float32)
+        self._ck(N.lib().tg_surface_cells(self._h, mode, temperature, cnt.value, C.byref(cnt), N.ptr(cells),
+                                          N.ptr(prob)))
+        return cells, prob
+
+    def log_grid(self, path: str, index: int, binary: bool = False, numbers=None) -> str:
+        """LogGrid snapshot of the current state into path.%08u; returns the name."""
+        num = None if numbers is None else np.ascontiguousarray(numbers, np.uint32)
+        self._ck(N.lib().tg_log_grid(self._h, str(path).encode(), index, int(binary), N.ptr(num)))
+        return f"{path}.{index:08d}"
+
+    def log_surface(self, path: str, index: int, binary: bool = False, with_neighbours: bool = False,
+                    mode: int = 0, temperature: float = 0.0, numbers=None) -> str:
+        """LogSurface snapshot of the current state into path.%08u."""
+        num = None if numbers is None else np.ascontiguousarray(numbers, np.uint32)
+        self._ck(N.lib().tg_log_surface(self._h, str(path).encode(), index, int(binary), int(with_neighbours), mode,
+                                        temperature, N.ptr(num)))
+        return f"{path}.{index:08d}"
 
     def normal(self, node: int) -> np.ndarray:
         out = np.empty(3, np.float32)
@@ -508,9 +556,14 @@ class Evaporation:
     """Process::evaporation (process.cpp:441-1124) over one device Grid."""
 
     def __init__(self, grid: Grid, options: EvaporationOptions, relax_mode: int = 1,
-                 solve: N.tg_solve_opts | None = None, trace: bool = True, normal: bool = True, path_cap: int = 0):
+                 solve: N.tg_solve_opts | None = None, trace: bool = True, normal: bool = True, path_cap: int = 0,
+                 snapshots: bool = False):
         """path_cap > 0 keeps each event's flight path (up to path_cap points)
-        in its record for write_trajectories."""
+        in its record for write_trajectories.  snapshots writes the grid and
+        surface snapshots that GRID_FILENAME / SURFACE_FILENAME, *_INTERVAL
+        and *_BINARY_OUTPUT ask for (process.cpp:641-643, 1068-1072): once
+        before the first event and after every event whose index is a
+        multiple of the interval."""
         self.grid = grid
         self.options = options
         types = grid.mesh.arrays()["types"]
@@ -522,6 +575,8 @@ class Evaporation:
         self.charge_mass = {k: (float(np.float32(v["evap_charge"]) * np.float32(1.60217733e-19)),
                                 float(np.float32(v["mass"]) * np.float32(1.660538782e-27))) for k, v in types.items()}
         self.path_cap = int(path_cap)
+        self.numbers = grid.mesh.numbers()
+        self.snapshots = bool(snapshots)
         self.opts = options.event_opts(self.vacuum_id, relax_mode, solve, trace, normal,
                                        temperature=grid.mesh.temperature)
         self.voltage_queue: deque = deque()
@@ -531,6 +586,34 @@ class Evaporation:
         self.records: list[dict] = []
         grid.surface_init(self.vacuum_id)
         grid.select()
+        if self.snapshots:
+            self._snapshot(force=True)
+
+    def _snapshot_logs(self):
+        for key in ("GRID", "SURFACE"):
+            name = self.options.s(f"{key}_FILENAME")
+            if name:
+                yield key, name, self.options.i(f"{key}_INTERVAL"), self.options.i(f"{key}_BINARY_OUTPUT") != 0
+
+    def _snapshot(self, force: bool = False):
+        """Step VII's snapshots (process.cpp:1068-1072) after event self.event."""
+        for key, name, interval, binary in self._snapshot_logs():
+            if not force and (interval <= 0 or self.event % interval != 0):
+                continue
+            if key == "GRID":
+                self.grid.log_grid(name, self.event, binary, self.numbers)
+            else:
+                self.grid.log_surface(name, self.event, binary, False, self.opts.prob_mode, self.opts.temperature,
+                                      self.numbers)
+
+    def _events_to_snapshot(self) -> int:
+        """Events until the next one after which a snapshot is due."""
+        k = 1 << 62
+        if self.snapshots:
+            for _, _, interval, _ in self._snapshot_logs():
+                if interval > 0:
+                    k = min(k, interval - self.event % interval)
+        return k
 
     @staticmethod
     def _type_id_by_name(grid: Grid, name: str) -> int:
@@ -559,19 +642,27 @@ class Evaporation:
         rec = self.grid.run_event(self.opts, self.event)
         r = self._record(rec, None if pts is None else (pts[0], err[0]))
         self.records.append(r)
+        if self.snapshots:
+            self._snapshot()
         return r
 
     def run(self, count: int) -> list[dict]:
         """`count` events in one library call: each ion flight overlaps the
         next event's removal and relaxation.  Same records as `step`."""
-        pts, err = self._path_buffers(count)
-        recs = self.grid.run_events(self.opts, self.event + 1, count)
         out = []
-        for k, rec in enumerate(recs):
-            self.event += 1
-            r = self._record(rec, None if pts is None else (pts[k], err[k]))
-            self.records.append(r)
-            out.append(r)
+        while count > 0:
+            # a batch ends where a snapshot is due
+            k = min(count, self._events_to_snapshot())
+            pts, err = self._path_buffers(k)
+            recs = self.grid.run_events(self.opts, self.event + 1, k)
+            for j, rec in enumerate(recs):
+                self.event += 1
+                r = self._record(rec, None if pts is None else (pts[j], err[j]))
+                self.records.append(r)
+                out.append(r)
+            if self.snapshots:
+                self._snapshot()
+            count -= k
         return out
 
     def _record(self, rec: N.tg_event_record, path=None) -> dict:
@@ -591,7 +682,8 @@ class Evaporation:
             voltage = 1.0 if fb == 0.0 else 0.0
             time_scale = 1.0
         return {
-            "index": self.event, "node": rec.node, "id": rec.type_id, "number": rec.node + 1, "voltage": voltage,
+            "index": self.event, "node": rec.node, "id": rec.type_id, "number": int(self.numbers[rec.node]),
+            "voltage": voltage,
             "stop": tuple(imp.stop), "tof": imp.stop_time * time_scale, "probability": rec.probability,
             "best": rec.best_ratio, "second": rec.second_ratio, "scaling_reference": rec.scaling_reference,
             "potentialBefore": rec.phi_before, "fieldBefore": tuple(rec.field_before),
@@ -828,3 +920,113 @@ def read_trajectories(path: str) -> tuple[bool, list]:
         items.append({"index": index, "number": number, "time_scale": ts, "status": status, "charge": charge,
                       "mass": mass, "points": pts, "error": np.array(err, np.float32)})
     return binary, items
+
+
+# ---- grid and surface snapshots (LogGrid, LogSurface) --------------------------
+
+GRID_RECORD = np.dtype([("id", "<i2"), ("number", "<u4"), ("phi", "<f4"), ("field", "<f4", 3), ("force", "<f4", 3)],
+                       align=False)
+
+
+def write_grid_log(path: str, id, number, phi, field, force, binary: bool = False):
+    """One grid snapshot file in LogGrid's layout (logGrid.cpp:197-245),
+    written by the library's native writer."""
+    id = np.ascontiguousarray(id, np.int32)
+    n = len(id)
+    arrs = [np.ascontiguousarray(number, np.uint32), np.ascontiguousarray(phi, np.float32),
+            np.ascontiguousarray(np.reshape(field, (n, 3)), np.float32),
+            np.ascontiguousarray(np.reshape(force, (n, 3)), np.float32)]
+    N.check(N.lib().tg_grid_log_write(str(path).encode(), int(binary), n, N.ptr(id), *[N.ptr(a) for a in arrs]))
+
+
+def read_grid_log(path: str) -> tuple[bool, np.ndarray]:
+    """(binary, records GRID_RECORD) of one grid snapshot file."""
+    data = open(path, "rb").read()
+    head = data.split(b"\n", 3)
+    mode, count = head[2].decode().split(" ")
+    count = int(count)
+    body = head[3]
+    if mode == "BINARY":
+        return True, np.frombuffer(body, GRID_RECORD, count).copy()
+    out = np.zeros(count, GRID_RECORD)
+    rows = [l.split(b"\t") for l in body.split(b"\n")[:count]]
+    out["id"] = [int(r[0]) for r in rows]
+    out["number"] = [int(r[1]) for r in rows]
+    vals = np.array([[float(x) for x in r[2:9]] for r in rows], np.float32).reshape(count, 7)
+    out["phi"] = vals[:, 0]
+    out["field"] = vals[:, 1:4]
+    out["force"] = vals[:, 4:7]
+    return False, out
+
+
+def write_surface_log(path: str, cells: dict, nodes: dict, binary: bool = False):
+    """One surface snapshot file in LogSurface's layout
+    (logSurface.cpp:203-293), written by the library's native writer.
+    cells: index, type, number, probability and optionally neighbours (a
+    list of arrays); nodes: index, phi, field [n, 3], normal [n, 3]."""
+    ci = np.ascontiguousarray(cells["index"], np.int32)
+    ct = np.ascontiguousarray(cells["type"], np.int32)
+    cn = np.ascontiguousarray(cells["number"], np.uint32)
+    cp = np.ascontiguousarray(cells["probability"], np.float32)
+    nptr = nb = None
+    if cells.get("neighbours") is not None:
+        lens = [len(x) for x in cells["neighbours"]]
+        nptr = np.ascontiguousarray(np.concatenate([[0], np.cumsum(lens)]), np.int32)
+        nb = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in cells["neighbours"]] or
+                                                 [np.zeros(0, np.int32)]), np.int32)
+    ni = np.ascontiguousarray(nodes["index"], np.int32)
+    nphi = np.ascontiguousarray(nodes["phi"], np.float32)
+    nf = np.ascontiguousarray(np.reshape(nodes["field"], (len(ni), 3)), np.float32)
+    nn = np.ascontiguousarray(np.reshape(nodes["normal"], (len(ni), 3)), np.float32)
+    N.check(N.lib().tg_surface_log_write(str(path).encode(), int(binary), len(ci), N.ptr(ci), N.ptr(ct), N.ptr(cn),
+                                         N.ptr(cp), N.ptr(nptr), N.ptr(nb), len(ni), N.ptr(ni), N.ptr(nphi),
+                                         N.ptr(nf), N.ptr(nn)))
+
+
+def read_surface_log(path: str) -> tuple[bool, dict, dict]:
+    """(binary, cells, nodes) of one surface snapshot file; cells carry
+    "neighbours" (list of arrays, empty when the file has none)."""
+    data = open(path, "rb").read()
+    binary = data.split(b"\n")[2] == b"BINARY"
+    pos = data.index(b"CELLS ")
+    end = data.index(b"\n", pos)
+    nc = int(data[pos + 6:end])
+    pos = end + 1
+    cells = {"index": np.zeros(nc, np.int32), "type": np.zeros(nc, np.int32), "number": np.zeros(nc, np.uint32),
+             "probability": np.zeros(nc, np.float32), "neighbours": []}
+    if binary:
+        for c in range(nc):
+            idx, typ, num, prob, cnt = struct.unpack_from("<ihIfI", data, pos)
+            pos += 18
+            nbrs = np.frombuffer(data, "<i4", cnt, pos).copy()
+            pos += 4 * cnt
+            cells["index"][c], cells["type"][c], cells["number"][c], cells["probability"][c] = idx, typ, num, prob
+            cells["neighbours"].append(nbrs)
+        pos += 1  # the newline after the cells
+    else:
+        for c in range(nc):
+            end = data.index(b"\n", pos)
+            t = data[pos:end].split(b"\t")
+            pos = end + 1
+            cells["index"][c], cells["type"][c], cells["number"][c] = int(t[0]), int(t[1]), int(t[2])
+            cells["probability"][c] = float(t[3])
+            cells["neighbours"].append(np.array([int(x) for x in t[5:]], np.int32) if len(t) > 4 else
+                                       np.zeros(0, np.int32))
+        pos += 1  # the empty line
+    end = data.index(b"\n", pos)
+    assert data[pos:pos + 6] == b"NODES "
+    nn = int(data[pos + 6:end])
+    pos = end + 1
+    if binary:
+        rec = np.dtype([("index", "<i4"), ("phi", "<f4"), ("field", "<f4", 3), ("normal", "<f4", 3)])
+        arr = np.frombuffer(data, rec, nn, pos)
+        nodes = {"index": arr["index"].copy(), "phi": arr["phi"].copy(), "field": arr["field"].copy(),
+                 "normal": arr["normal"].copy()}
+    else:
+        rows = [l.split(b"\t") for l in data[pos:].split(b"\n")[:nn]]
+        vals = np.array([[float(x) for x in r[1:8]] for r in rows], np.float32).reshape(nn, 7)
+        nodes = {"index": np.array([int(r[0]) for r in rows], np.int32), "phi": vals[:, 0], "field": vals[:, 1:4],
+                 "normal": vals[:, 4:7]}
+    if not any(len(x) for x in cells["neighbours"]) and not binary:
+        cells["neighbours"] = None
+    return binary, cells, nodes

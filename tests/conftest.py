@@ -70,3 +70,24 @@ def path_deviation(times, xyz, ref_points, time_scale):
     dev = np.linalg.norm(ip - rp, axis=1).max()
     disp = np.linalg.norm(rp - rp[0], axis=1).max()
     return dev, disp
+
+
+@pytest.fixture(scope="session")
+def snapshot_files(tmp_path_factory):
+    """The reference's grid and surface snapshots after the first event with
+    Fe's permittivity 5 (tests/golden/ref_{grid,surf}_*.00000001.gz),
+    unpacked: {name: path}."""
+    d = tmp_path_factory.mktemp("snapshots")
+    out = {}
+    for name in ("ref_grid_ascii", "ref_grid_bin", "ref_surf_ascii", "ref_surf_bin"):
+        with gzip.open(GOLDEN / f"{name}.00000001.gz") as f, open(d / name, "wb") as g:
+            shutil.copyfileobj(f, g)
+        out[name] = str(d / name)
+    return out
+
+
+@pytest.fixture(scope="session")
+def ref_mesh_eps5(golden_dump):
+    """The golden dump under tip_eps5.cfg (Fe permittivity 5)."""
+    from tapsim_modified_b200.tapsim import Mesh
+    return Mesh.from_dump(str(golden_dump), str(GOLDEN / "tip_eps5.cfg"))

@@ -41,6 +41,14 @@ keeps the trajectory files that the reference's own LogTrajectory writes
 for them (logTrajectory.cpp:137-300, pushed as process.cpp:1048-1049 does):
 ref_traj_ascii.txt (one file) and ref_traj_bin.00000001 / .00000002
 (binary, chunk size 2).
+
+With `--snapshots` it repeats the first event with Fe's DIELECTRICITY set
+to 5 (tip_eps5.cfg; --no-sync keeps the dump's couplings, so only the
+dielectric force changes) and keeps the snapshots that the reference's own
+LogGrid and LogSurface write after it (logGrid.cpp:119-245,
+logSurface.cpp:130-293), gzipped: ref_grid_ascii.00000001.gz,
+ref_grid_bin.00000001.gz, ref_surf_ascii.00000001.gz (no neighbour lists)
+and ref_surf_bin.00000001.gz (with neighbour lists).
 """
 from __future__ import annotations
 
@@ -166,6 +174,32 @@ def trajectories():
     shutil.rmtree(tmp)
 
 
+def snapshots():
+    if not HARNESS.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    cfg = (HERE / "tip.cfg").read_text()
+    head, fe = cfg.split("NAME = Fe\n", 1)
+    assert fe.startswith("CHARGE_DENSITY = 0\nDIELECTRICITY = 1\n")
+    fe = fe.replace("DIELECTRICITY = 1\n", "DIELECTRICITY = 5\n", 1)
+    (HERE / "tip_eps5.cfg").write_text(head + "NAME = Fe\n" + fe)
+    tmp = HERE / "_tmp"
+    tmp.mkdir(exist_ok=True)
+    with gzip.open(HERE / "ref_mesh.dump.gz", "rb") as f, open(tmp / "ref.dump", "wb") as g:
+        shutil.copyfileobj(f, g)
+    for mode, grid, surf, nb in (("ascii", "ref_grid_ascii", "ref_surf_ascii", "0"),
+                                 ("binary", "ref_grid_bin", "ref_surf_bin", "1")):
+        subprocess.run([str(HARNESS), "evap", str(HERE / "tip_eps5.cfg"), "-", str(HERE / "oracle.ini"), "1",
+                        str(tmp / "events.txt"), "--dump", str(tmp / "ref.dump"), "--threads", "1", "--no-sync",
+                        "--grids", str(tmp / grid), mode, "--surfaces", str(tmp / surf), mode, nb],
+                       check=True, capture_output=True)
+        for name in (grid, surf):
+            with open(tmp / f"{name}.00000001", "rb") as f, \
+                    gzip.open(HERE / f"{name}.00000001.gz", "wb", compresslevel=9) as g:
+                shutil.copyfileobj(f, g)
+            print("snapshot ->", f"{name}.00000001.gz")
+    shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
     if "--modes" in sys.argv:
         modes()
@@ -173,5 +207,7 @@ if __name__ == "__main__":
         results()
     elif "--trajectories" in sys.argv:
         trajectories()
+    elif "--snapshots" in sys.argv:
+        snapshots()
     else:
         main()

@@ -168,3 +168,26 @@ def test_reference_trajectory_structure():
         # the extrapolated point keeps the last velocity and reaches the top
         np.testing.assert_array_equal(p["velocity"][-1], p["velocity"][-2])
         assert abs(p["position"][-1][2] - 4.0e-8) <= 1e-14
+
+
+def test_snapshot_files_round_trip_the_reference_bytes(tmp_path, snapshot_files):
+    """The reference's LogGrid and LogSurface output (ASCII, binary, with and
+    without neighbour lists) read and written back by the library's native
+    writers byte for byte."""
+    from tapsim_modified_b200.tapsim import read_grid_log, read_surface_log, write_grid_log, write_surface_log
+    for name in ("ref_grid_ascii", "ref_grid_bin"):
+        binary, g = read_grid_log(snapshot_files[name])
+        assert binary == name.endswith("bin") and len(g) == 9110
+        write_grid_log(str(tmp_path / name), g["id"], g["number"], g["phi"], g["field"], g["force"], binary)
+        assert (tmp_path / name).read_bytes() == open(snapshot_files[name], "rb").read()
+    for name in ("ref_surf_ascii", "ref_surf_bin"):
+        binary, cells, nodes = read_surface_log(snapshot_files[name])
+        assert binary == name.endswith("bin") and len(cells["index"]) == 617 and len(nodes["index"]) == 1960
+        assert (cells["neighbours"] is None) == (not binary)
+        write_surface_log(str(tmp_path / name), cells, nodes, binary)
+        assert (tmp_path / name).read_bytes() == open(snapshot_files[name], "rb").read()
+    # the ASCII files carry the binary ones' values at 7 digits
+    _, ga = read_grid_log(snapshot_files["ref_grid_ascii"])
+    _, gb = read_grid_log(snapshot_files["ref_grid_bin"])
+    np.testing.assert_array_equal(ga["number"], gb["number"])
+    np.testing.assert_allclose(ga["force"], gb["force"], rtol=1e-6, atol=0)
