@@ -142,7 +142,7 @@ __global__ void k_vertex_fields(DevMesh m) {
         b2 += __shfl_xor_sync(0xffffffffu, b2, o);
     }
     if (!live || lane != 0) return;
-    m.phiTrace[i] = pi;
+    if (m.phiTrace != m.phi64) m.phiTrace[i] = pi;
     double* out = m.vfield + 3 * (size_t)i;
     if (hull) {
         out[0] = out[1] = out[2] = 0.0;

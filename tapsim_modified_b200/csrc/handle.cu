@@ -102,12 +102,20 @@ struct tg_handle {
     DBuf<float> pathBuf, pathErr;
 
     cudaEvent_t evStart = nullptr, evStop = nullptr;
-    // flights of tg_run_events run on their own stream, overlapping the next
-    // event's relaxation; they read only the vfield/phiTrace snapshots
-    cudaStream_t traceStream = nullptr;
-    cudaEvent_t evFields = nullptr, evTraceDone = nullptr;
+    // error flags of the flights of tg_run_events; potentials of the
+    // flights of tg_trace
     DBuf<int> statusTrace;
     DBuf<double> phiTrace;
+    // tg_run_events: a ring of flight slots, each with its own stream and
+    // snapshots (potentials, vertex fields), so that the flights of
+    // successive events run side by side and overlap the relaxations; the
+    // main stream only copies the potentials into the next free slot
+    static constexpr int kRing = 4;
+    cudaStream_t ringStream[kRing] = {};
+    cudaEvent_t ringPhi[kRing] = {}, ringDone[kRing] = {};
+    DBuf<double> ringPhiBuf[kRing], ringField[kRing];
+    int ringNext = 0;
+    bool ringReady = false;
     std::vector<int32_t> h_row_ptr;
     std::vector<int32_t> h_col;  // the Delaunay neighbours never change
 
@@ -576,12 +584,13 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     };
     cudaError_t e = cudaSuccess;
     auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
-    chk(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    // the event's own work runs at the highest stream priority, so that its
+    // kernels take SMs ahead of the blocks of the flight slots
+    int leastPriority = 0, greatestPriority = 0;
+    chk(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+    chk(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatestPriority));
     chk(cudaEventCreate(&h->evStart));
     chk(cudaEventCreate(&h->evStop));
-    chk(cudaStreamCreateWithFlags(&h->traceStream, cudaStreamNonBlocking));
-    chk(cudaEventCreateWithFlags(&h->evFields, cudaEventDisableTiming));
-    chk(cudaEventCreateWithFlags(&h->evTraceDone, cudaEventDisableTiming));
     chk(up(h->xyz, d->xyz, 3 * (size_t)n));
     chk(up(h->type, d->type_id, n));
     chk(h->typeScratch.alloc(n));
@@ -683,11 +692,17 @@ void tg_destroy(tg_handle* h) {
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
-    if (h->traceStream) cudaStreamSynchronize(h->traceStream);
+    for (int r = 0; r < tg_handle::kRing; r++) {
+        if (h->ringStream[r]) {
+            cudaStreamSynchronize(h->ringStream[r]);
+            cudaStreamDestroy(h->ringStream[r]);
+        }
+        if (h->ringPhi[r]) cudaEventDestroy(h->ringPhi[r]);
+        if (h->ringDone[r]) cudaEventDestroy(h->ringDone[r]);
+        h->ringPhiBuf[r].release();
+        h->ringField[r].release();
+    }
     h->phiTrace.release(); h->statusTrace.release();
-    if (h->evFields) cudaEventDestroy(h->evFields);
-    if (h->evTraceDone) cudaEventDestroy(h->evTraceDone);
-    if (h->traceStream) cudaStreamDestroy(h->traceStream);
     if (h->evStart) cudaEventDestroy(h->evStart);
     if (h->evStop) cudaEventDestroy(h->evStop);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1525,6 +1540,23 @@ int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* gu
 // Steps I-VI of one event.  With asyncImpact (a device slot) the flight of
 // step V is queued on the trace stream and its impact left there; without,
 // it runs through tg_trace and lands in rec->impact.
+// The flight ring of tg_run_events, allocated at its first use.
+static int ring_ready(tg_handle* h) {
+    if (h->ringReady) return TG_OK;
+    for (int r = 0; r < tg_handle::kRing; r++) {
+        int leastPriority = 0, greatestPriority = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+        CK(cudaStreamCreateWithPriority(&h->ringStream[r], cudaStreamNonBlocking, leastPriority));
+        CK(cudaEventCreateWithFlags(&h->ringPhi[r], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->ringDone[r], cudaEventDisableTiming));
+        CK(cudaEventRecord(h->ringDone[r], h->ringStream[r]));
+        CK(h->ringPhiBuf[r].alloc(h->n));
+        CK(h->ringField[r].alloc(3 * (size_t)h->n));
+    }
+    h->ringReady = true;
+    return TG_OK;
+}
+
 static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec,
                      ImpactOut* asyncImpact) {
     if (h->vacuumId != o->vacuum_id) {
@@ -1656,14 +1688,27 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
         }
         if (asyncImpact) {
             if (guess >= h->ntets || !h->tetpack.p) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: no tetrahedra");
-            // the previous flight must be done with the snapshots before the
-            // vertex fields of this event overwrite them
-            CK(cudaStreamWaitEvent(h->stream, h->evTraceDone, 0));
-            launch_vertex_fields(h->dm(), h->stream);
-            CK(cudaEventRecord(h->evFields, h->stream));
-            CK(cudaStreamWaitEvent(h->traceStream, h->evFields, 0));
+            rc = ring_ready(h);
+            if (rc != TG_OK) return rc;
+            const int r = h->ringNext;
+            h->ringNext = (r + 1) % tg_handle::kRing;
+            // the flight that used this slot (kRing events ago) is done with
+            // its snapshots before this event's potentials replace them
+            CK(cudaStreamWaitEvent(h->stream, h->ringDone[r], 0));
+            CK(cudaMemcpyAsync(h->ringPhiBuf[r].p, h->phi64.p, sizeof(double) * h->n, cudaMemcpyDeviceToDevice,
+                               h->stream));
+            CK(cudaEventRecord(h->ringPhi[r], h->stream));
+            CK(cudaStreamWaitEvent(h->ringStream[r], h->ringPhi[r], 0));
+            // vertex fields from the snapshot on the slot's stream: they read
+            // the couplings only through their zero pattern, which a flip to
+            // the vacuum type never changes, so the next event's removal may
+            // run meanwhile
             DevMesh mt = h->dm();
+            mt.phi64 = h->ringPhiBuf[r].p;
+            mt.phiTrace = h->ringPhiBuf[r].p;
+            mt.vfield = h->ringField[r].p;
             mt.status = h->statusTrace.p;
+            launch_vertex_fields(mt, h->ringStream[r]);
             TraceParams tp = trace_params(h, &o->trace);
             if (o->path_cap > 0) {
                 // this event's slot of the batch
@@ -1672,9 +1717,9 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
                 tp.path_err = h->pathErr.p + 12 * slot;
                 tp.path_cap = o->path_cap;
             }
-            launch_trace_one(mt, start, vel, qm, guess, tp, asyncImpact, h->traceStream);
+            launch_trace_one(mt, start, vel, qm, guess, tp, asyncImpact, h->ringStream[r]);
             CK(cudaGetLastError());
-            CK(cudaEventRecord(h->evTraceDone, h->traceStream));
+            CK(cudaEventRecord(h->ringDone[r], h->ringStream[r]));
         } else {
             rc = trace_impl(h, 1, start, o->initial_velocity ? vel : nullptr, &qm, &guess, &o->trace, &rec->impact,
                             o->path_cap, o->path_points, o->path_errors, "tg_run_event");
@@ -1746,7 +1791,8 @@ int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int3
         if (rc != TG_OK) break;
     }
     // every flight queued so far completes before the impacts are read
-    CK(cudaStreamSynchronize(h->traceStream));
+    if (h->ringReady)
+        for (int r = 0; r < tg_handle::kRing; r++) CK(cudaStreamSynchronize(h->ringStream[r]));
     CK(cudaStreamSynchronize(h->stream));
     if (o->trace_enabled && k > 0) {
         std::vector<ImpactOut> imp(k);
