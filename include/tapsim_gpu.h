@@ -128,7 +128,12 @@ typedef struct {
      *      around the removed atom (tg_learner_attach, mode bit 1).
      * The solve always ends at rel_tol, whatever the start. */
     int32_t warm_start;
-    int32_t reserved;
+    /* Preconditioner of the inner iterations on the non-Neumann free cells:
+     *   0  Jacobi (the diagonal),
+     *   1  a smoothed-aggregation multigrid V(1,1)-cycle, its hierarchy
+     *      built on the host at the first solve that asks for it and again
+     *      once removals have added 2% more cells to the system. */
+    int32_t preconditioner;
 } tg_solve_opts;
 typedef struct {
     int32_t outer;            /* defect-correction steps taken */
@@ -137,6 +142,7 @@ typedef struct {
     double initial_rel_residual;
     int32_t inner_neumann;    /* of `inner`, the iterations on the Neumann rows */
     int32_t reserved;
+    double setup_seconds;     /* multigrid hierarchy built during this solve [s], 0 if none */
 } tg_solve_info;
 int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);
 /* ||r||_2 / ||b||_2 of the current potentials (FP64). */

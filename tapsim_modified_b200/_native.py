@@ -39,12 +39,13 @@ class tg_mesh_desc(C.Structure):
 
 class tg_solve_opts(C.Structure):
     _fields_ = [("rel_tol", C.c_double), ("max_outer", C.c_int32), ("max_inner", C.c_int32),
-                ("inner_rtol", C.c_double), ("warm_start", C.c_int32), ("reserved", C.c_int32)]
+                ("inner_rtol", C.c_double), ("warm_start", C.c_int32), ("preconditioner", C.c_int32)]
 
 
 class tg_solve_info(C.Structure):
     _fields_ = [("outer", C.c_int32), ("inner", C.c_int32), ("rel_residual", C.c_double),
-                ("initial_rel_residual", C.c_double), ("inner_neumann", C.c_int32), ("reserved", C.c_int32)]
+                ("initial_rel_residual", C.c_double), ("inner_neumann", C.c_int32), ("reserved", C.c_int32),
+                ("setup_seconds", C.c_double)]
 
 
 class tg_select_info(C.Structure):

@@ -1,0 +1,209 @@
+// Smoothed-aggregation multigrid V-cycle as the preconditioner of the V
+// system's conjugate gradients: u = M^-1 r.
+//
+// Level 0 is the live V system (SELL-32, cg.cu), so the fine operator is
+// always the current one; the prolongator P_0 covers the slots that existed
+// when the hierarchy was built, and slots appended later by removals are
+// only smoothed.  Levels 1.. hold their Galerkin operators R A P in CSR
+// (FP32), and the coarsest level is solved with a dense inverse.  The cycle
+// is V(1,1) with damped Jacobi (weight 2/3) before and after the coarse
+// correction, which keeps the preconditioner symmetric:
+//     y = w D^-1 b;  t = b - A y;  b' = R t;  x' = cycle(b');  y += P x';
+//     x = y + w D^-1 (b - A y)
+// Every kernel returns at once when the CG iteration it belongs to has
+// already met its target, as the CG kernels do.
+#include "kernels.cuh"
+
+namespace tgd {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr float kSmooth = 2.0f / 3.0f;
+
+__device__ __forceinline__ bool done(const double* scal, int it, double target) {
+    return scal[4 * it + 3] <= target;
+}
+
+// y = w b / d
+__global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, const double* scal, int it,
+                             double target) {
+    if (done(scal, it, target)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        y[i] = kSmooth * b[i] / d[i];
+}
+
+// Level 0 over SELL-32 slices: mode 0: t = b - A y; mode 1: x = y + w (b - A y) / d
+__global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, float* out, int mode,
+                           const double* scal, int it, double target) {
+    if (done(scal, it, target)) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
+        const int base = v.slice_start[warp];
+        const int width = v.slice_width[warp];
+        const int s = warp * 32 + lane;
+        const int* __restrict__ col = v.col + base + lane;
+        const float* __restrict__ val = v.val + base + lane;
+        float acc = 0.0f;
+        int k = 0;
+        for (; k + 8 <= width; k += 8) {
+            int c[8];
+            float a[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                c[j] = __ldcs(col + 32 * (k + j));
+                a[j] = __ldcs(val + 32 * (k + j));
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc += a[j] * __ldg(y + c[j]);
+        }
+        for (; k < width; k++) acc += __ldcs(val + 32 * k) * __ldg(y + __ldcs(col + 32 * k));
+        const float d = v.d[s], ys = y[s];
+        const float t = b[s] - (d * ys - acc);
+        out[s] = mode == 0 ? t : ys + kSmooth * t / d;
+    }
+}
+
+// Rows of the coarse operators and of the restriction hold tens to a few
+// hundred entries: a group of kRowLanes lanes per row, one row per group,
+// a grid with a group for every row (no grid-stride loop, so that every row's
+// loads are in flight at once).
+constexpr int kRowLanes = 16;
+
+__device__ __forceinline__ float row_dot(const int32_t* ptr, const int32_t* col, const float* val, const float* y,
+                                         int row, int lane) {
+    float acc = 0.0f;
+    const int q1 = ptr[row + 1];
+    for (int q = ptr[row] + lane; q < q1; q += kRowLanes) acc += __ldcs(val + q) * __ldg(y + __ldcs(col + q));
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+// Rows of a CSR operator A (with its diagonal):
+// mode 0: t = b - A y; mode 1: x = y + w (b - A y) / diag
+__global__ void k_amg_csr(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* diag,
+                          const float* b, const float* y, float* out, int mode, const double* scal, int it,
+                          double target) {
+    if (done(scal, it, target)) return;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = gid % kRowLanes;
+    const int row = min(gid / kRowLanes, n - 1);  // whole groups stay active for the shuffles
+    const float acc = row_dot(ptr, col, val, y, row, lane);
+    if (lane == 0 && gid / kRowLanes < n) {
+        const float t = b[row] - acc;
+        out[row] = mode == 0 ? t : y[row] + kSmooth * t / diag[row];
+    }
+}
+
+// out = M y for a CSR matrix (restriction R t)
+__global__ void k_amg_mv(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* y, float* out,
+                         const double* scal, int it, double target) {
+    if (done(scal, it, target)) return;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = gid % kRowLanes;
+    const int row = min(gid / kRowLanes, n - 1);
+    const float acc = row_dot(ptr, col, val, y, row, lane);
+    if (lane == 0 && gid / kRowLanes < n) out[row] = acc;
+}
+
+// y += P x' (prolongation, a few entries per row), one thread per row
+__global__ void k_amg_prolong(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* xc,
+                              float* y, const double* scal, int it, double target) {
+    if (done(scal, it, target)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (int q = ptr[i]; q < ptr[i + 1]; q++) acc += val[q] * __ldg(xc + col[q]);
+        y[i] += acc;
+    }
+}
+
+// x = C^-1 b with the coarsest level's dense inverse (row-major), one warp per row
+__global__ void k_amg_dense(int n, const float* inv, const float* b, float* x, const double* scal, int it,
+                            double target) {
+    if (done(scal, it, target)) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
+        float acc = 0.0f;
+        for (int k = lane; k < n; k += 32) acc += inv[(size_t)row * n + k] * b[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) x[row] = acc;
+    }
+}
+
+// a thread for every lane of every slice (the SELL kernels' grid-stride
+// loop then makes one pass)
+inline unsigned grid_full(long long threads) { return (unsigned)((threads + kBlock - 1) / kBlock); }
+
+// a group of kRowLanes threads for every row
+inline unsigned grid_rows(int n) { return (unsigned)(((long long)n * kRowLanes + kBlock - 1) / kBlock); }
+
+inline int grid_for(long long threads) {
+    static int cap = 0;
+    if (cap == 0) {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cap = 16 * (sms > 0 ? sms : 148);
+    }
+    const long long b = (threads + kBlock - 1) / kBlock;
+    return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+}  // namespace
+
+void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s) {
+    const double* scal = v.scal;
+    // level 0: b = r, output u
+    const int slices = (slots + 31) / 32;
+    count_launch();
+    k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.r, v.d, g.y0, scal, it, target);
+    if (g.levels > 1) {
+        count_launch();
+        k_amg_fine<<<grid_full(slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, g.t0, 0, scal, it,
+                                                                         target);
+        // down: restrict, smooth, residual
+        for (int l = 0; l + 1 < g.levels; l++) {
+            const AmgDevLevel& L = g.lev[l];
+            const AmgDevLevel& C = g.lev[l + 1];
+            const float* t = l == 0 ? g.t0 : L.t;
+            count_launch();
+            k_amg_mv<<<grid_rows(C.n), kBlock, 0, s>>>(C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, scal, it, target);
+            if (l + 1 == g.levels - 1) {
+                count_launch();
+                k_amg_dense<<<grid_for((long long)C.n * 32), kBlock, 0, s>>>(C.n, g.coarse_inv, C.b, C.x, scal, it,
+                                                                             target);
+            } else {
+                count_launch();
+                k_amg_jacobi<<<grid_for(C.n), kBlock, 0, s>>>(C.n, C.b, C.diag, C.y, scal, it, target);
+                count_launch();
+                k_amg_csr<<<grid_rows(C.n), kBlock, 0, s>>>(C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0,
+                                                            scal, it, target);
+            }
+        }
+        // up: prolong, post-smooth
+        for (int l = g.levels - 2; l >= 0; l--) {
+            const AmgDevLevel& L = g.lev[l];
+            const AmgDevLevel& C = g.lev[l + 1];
+            float* y = l == 0 ? g.y0 : L.y;
+            count_launch();
+            k_amg_prolong<<<grid_for(L.n), kBlock, 0, s>>>(L.n, L.p_ptr, L.p_col, L.p_val, C.x, y, scal, it, target);
+            count_launch();
+            if (l == 0) {
+                k_amg_fine<<<grid_full(slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, v.u, 1, scal, it,
+                                                                                 target);
+            } else {
+                k_amg_csr<<<grid_rows(L.n), kBlock, 0, s>>>(L.n, L.a_ptr, L.a_col, L.a_val, L.diag, L.b, L.y, L.x, 1,
+                                                            scal, it, target);
+            }
+        }
+    } else {
+        // a single level: Jacobi twice (y, then the post-smoothing step)
+        count_launch();
+        k_amg_fine<<<grid_full(slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, v.u, 1, scal, it,
+                                                                         target);
+    }
+}
+
+}  // namespace tgd

@@ -39,29 +39,34 @@ __device__ __forceinline__ void cg_coeffs(const double* scal, int it, double* al
     }
 }
 
-// u = r / d, x = 0, gamma_0 = r.u, rho_0 = r.r
-__global__ void k_vcg_init(VSys v, int slots) {
+// x = 0, rho_0 = r.r; with the Jacobi preconditioner also u = r / d and
+// gamma_0 = r.u (with the multigrid one the V-cycle makes u and the SpMV
+// gamma)
+__global__ void k_vcg_init(VSys v, int slots, int jacobi) {
     double g = 0.0, rr = 0.0;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
         const float r = v.r[s];
-        const float u = r / v.d[s];
-        v.u[s] = u;
+        if (jacobi) {
+            const float u = r / v.d[s];
+            v.u[s] = u;
+            g += (double)r * (double)u;
+        }
         v.x[s] = 0.0f;
         v.p[s] = 0.0f;
         v.sv[s] = 0.0f;
-        g += (double)r * (double)u;
         rr += (double)r * (double)r;
     }
     block_sum2_atomic<kBlock>(g, rr, &v.scal[0], &v.scal[3]);
 }
 
 // w = A u over SELL-32 slices; delta -> scal[4*it+1] (it = iteration whose
-// u this is); skipped once rho_it <= target
-__global__ void k_vcg_spmv(VSys v, int slices, int it, double target) {
+// u this is), and with withGamma gamma = r.u -> scal[4*it]; skipped once
+// rho_it <= target
+__global__ void k_vcg_spmv(VSys v, int slices, int it, double target, int withGamma) {
     if (it >= 0 && v.scal[4 * it + 3] <= target) return;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    double dl = 0.0;
+    double dl = 0.0, gl = 0.0;
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
         const int base = v.slice_start[warp];
         const int width = v.slice_width[warp];
@@ -90,13 +95,17 @@ __global__ void k_vcg_spmv(VSys v, int slices, int it, double target) {
         const float w = v.d[s] * u - acc;
         v.w[s] = w;
         dl += (double)w * (double)u;
+        if (withGamma) gl += (double)v.r[s] * (double)u;
     }
-    block_sum_atomic<kBlock>(dl, &v.scal[4 * (it < 0 ? 0 : it) + 1]);
+    const int at = 4 * (it < 0 ? 0 : it);
+    if (withGamma) block_sum2_atomic<kBlock>(dl, gl, &v.scal[at + 1], &v.scal[at]);
+    else block_sum_atomic<kBlock>(dl, &v.scal[at + 1]);
 }
 
-// p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s, u = r / d,
-// gamma_{it+1} = r.u, rho_{it+1} = r.r
-__global__ void k_vcg_update(VSys v, int slots, int it, double target) {
+// p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s,
+// rho_{it+1} = r.r; with the Jacobi preconditioner also u = r / d and
+// gamma_{it+1} = r.u
+__global__ void k_vcg_update(VSys v, int slots, int it, double target, int jacobi) {
     if (v.scal[4 * it + 3] <= target) return;
     double alpha, beta;
     cg_coeffs(v.scal, it, &alpha, &beta);
@@ -111,9 +120,11 @@ __global__ void k_vcg_update(VSys v, int slots, int it, double target) {
         v.x[s] += a * p;
         const float r = v.r[s] - a * sv;
         v.r[s] = r;
-        const float u = r / v.d[s];
-        v.u[s] = u;
-        g += (double)r * (double)u;
+        if (jacobi) {
+            const float u = r / v.d[s];
+            v.u[s] = u;
+            g += (double)r * (double)u;
+        }
         rr += (double)r * (double)r;
     }
     block_sum2_atomic<kBlock>(g, rr, &v.scal[4 * (it + 1)], &v.scal[4 * (it + 1) + 3]);
@@ -258,15 +269,21 @@ inline int reduce_blocks(int n) {
 
 }  // namespace
 
-void launch_vcg_init(const VSys& v, int slots, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_init<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots); }
+void launch_vcg_init(const VSys& v, int slots, bool jacobi, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_init<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, jacobi ? 1 : 0); }
 }
-void launch_vcg_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s) {
+void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withGamma, cudaStream_t s) {
     const int slices = (slots + 31) / 32;
-    if (slices > 0) { count_launch(); k_vcg_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, it, target); }
+    if (slices > 0) {
+        count_launch();
+        k_vcg_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, it, target, withGamma ? 1 : 0);
+    }
 }
-void launch_vcg_update(const VSys& v, int slots, int it, double target, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, it, target); }
+void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s) {
+    if (slots > 0) {
+        count_launch();
+        k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, it, target, jacobi ? 1 : 0);
+    }
 }
 void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s) {
     if (slots > 0) { count_launch(); k_vcg_apply<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, record ? 1 : 0); }

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -17,6 +18,7 @@
 #include <vector>
 
 #include "../../include/tapsim_gpu.h"
+#include "host/amg.h"
 #include "kernels.cuh"
 #include "learn.h"
 
@@ -128,6 +130,22 @@ struct tg_handle {
     int vCapacity = 0;       // slots incl. the append reserve
     int vActive = 0;         // slots in use (host mirror of vCount)
     double vEntries = 0.0;   // stored (non-padding) couplings
+
+    // multigrid preconditioner of the V system (amg.cu): hierarchy built on
+    // the host from the V system as it is, uploaded as CSR levels
+    bool amgReady = false;
+    int amgSlots = 0;                       // V slots its prolongator covers
+    tgd::AmgDev amg{};
+    std::vector<DBuf<int32_t>> amgI;
+    std::vector<DBuf<float>> amgF;
+    void amg_release() {
+        for (auto& b : amgI) b.release();
+        for (auto& b : amgF) b.release();
+        amgI.clear();
+        amgF.clear();
+        amgReady = false;
+        amgSlots = 0;
+    }
 
     VSys vs() {
         VSys v;
@@ -689,6 +707,7 @@ void tg_destroy(tg_handle* h) {
     h->keys.release(); h->result.release(); h->local.release(); h->localCount.release();
     h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
     h->stageImpact.release(); h->pathBuf.release(); h->pathErr.release();
+    h->amg_release();
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
@@ -746,9 +765,9 @@ int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, d
         if (h->vScal.n < 8) CK(h->vScal.alloc(8));
         VSys v = h->vs();
         CK(cudaMemsetAsync(h->vScal.p, 0, 8 * sizeof(double), h->stream));
-        launch_vcg_spmv(v, h->vActive, 0, -1.0, h->stream);  // warm
+        launch_vcg_spmv(v, h->vActive, 0, -1.0, false, h->stream);  // warm
         CK(cudaEventRecord(h->evStart, h->stream));
-        for (int k = 0; k < iters; k++) launch_vcg_spmv(v, h->vActive, 0, -1.0, h->stream);
+        for (int k = 0; k < iters; k++) launch_vcg_spmv(v, h->vActive, 0, -1.0, false, h->stream);
         CK(cudaEventRecord(h->evStop, h->stream));
     } else if (which == 1) {
         // k_residual over all free rows: row index, two row pointers, col +
@@ -943,17 +962,131 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     return TG_OK;
 }
 
+// Builds the multigrid hierarchy of the V system as it is now (its slots in
+// use, their couplings and diagonals read back from the device) and
+// uploads it.
+static int amg_setup(tg_handle* h, double* seconds) {
+    const auto t0 = std::chrono::steady_clock::now();
+    h->amg_release();
+    const int slots = h->vActive;
+    const int slices = (slots + 31) / 32;
+    std::vector<int32_t> sliceStart(slices + 1), sliceWidth(slices);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(sliceStart.data(), h->vSliceStart.p, sizeof(int32_t) * (slices + 1), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sliceWidth.data(), h->vSliceWidth.p, sizeof(int32_t) * slices, cudaMemcpyDeviceToHost));
+    const size_t used = (size_t)sliceStart[slices];
+    std::vector<int32_t> col(used);
+    std::vector<float> val(used), d(slots);
+    CK(cudaMemcpy(col.data(), h->vCol.p, sizeof(int32_t) * used, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(val.data(), h->vVal.p, sizeof(float) * used, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(d.data(), h->vs().d, sizeof(float) * slots, cudaMemcpyDeviceToHost));
+    // A = D - C in CSR, slot order
+    tg_host::AmgCsr A;
+    A.rows = A.cols = slots;
+    A.ptr.reserve(slots + 1);
+    A.col.reserve(used + slots);
+    A.val.reserve(used + slots);
+    A.ptr.push_back(0);
+    for (int s = 0; s < slots; s++) {
+        const int base = sliceStart[s / 32] + (s & 31), width = sliceWidth[s / 32];
+        A.col.push_back(s);
+        A.val.push_back(d[s]);
+        for (int k = 0; k < width; k++) {
+            const int c = col[base + 32 * (size_t)k];
+            const float a = val[base + 32 * (size_t)k];
+            if (c >= slots || a == 0.0f) continue;
+            A.col.push_back(c);
+            A.val.push_back(-(double)a);
+        }
+        A.ptr.push_back((int32_t)A.col.size());
+    }
+    tg_host::AmgHierarchy H;
+    const std::string err = tg_host::amg_build(std::move(A), tg_host::AmgOptions(), &H);
+    if (!err.empty()) return fail(h, TG_ERR_HOST, "tg_solve: " + err);
+    if ((int)H.levels.size() > tgd::kAmgMaxLevels) return fail(h, TG_ERR_HOST, "tg_solve: too many multigrid levels");
+    cudaError_t e = cudaSuccess;
+    auto upI = [&](const std::vector<int32_t>& src) -> int32_t* {
+        h->amgI.emplace_back();
+        DBuf<int32_t>& b = h->amgI.back();
+        if (e == cudaSuccess) e = b.alloc(std::max<size_t>(src.size(), 1));
+        if (e == cudaSuccess && !src.empty())
+            e = cudaMemcpy(b.p, src.data(), sizeof(int32_t) * src.size(), cudaMemcpyHostToDevice);
+        return b.p;
+    };
+    auto upF = [&](const std::vector<double>& src) -> float* {
+        std::vector<float> f(src.begin(), src.end());
+        h->amgF.emplace_back();
+        DBuf<float>& b = h->amgF.back();
+        if (e == cudaSuccess) e = b.alloc(std::max<size_t>(f.size(), 1));
+        if (e == cudaSuccess && !f.empty()) e = cudaMemcpy(b.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice);
+        return b.p;
+    };
+    auto vec = [&](size_t n) -> float* {
+        h->amgF.emplace_back();
+        DBuf<float>& b = h->amgF.back();
+        if (e == cudaSuccess) e = b.alloc(std::max<size_t>(n, 1));
+        if (e == cudaSuccess) e = cudaMemset(b.p, 0, sizeof(float) * std::max<size_t>(n, 1));
+        return b.p;
+    };
+    // the DBuf vectors must not reallocate while pointers into them are live
+    h->amgI.reserve(8 * H.levels.size() + 4);
+    h->amgF.reserve(8 * H.levels.size() + 4);
+    tgd::AmgDev g{};
+    g.levels = (int)H.levels.size();
+    for (int l = 0; l < g.levels; l++) {
+        const tg_host::AmgLevel& L = H.levels[l];
+        tgd::AmgDevLevel& D = g.lev[l];
+        D.n = L.A.rows;
+        if (l > 0) {
+            D.a_ptr = upI(L.A.ptr);
+            D.a_col = upI(L.A.col);
+            D.a_val = upF(L.A.val);
+            std::vector<double> diag(L.A.rows, 1.0);
+            for (int i = 0; i < L.A.rows; i++)
+                for (int q = L.A.ptr[i]; q < L.A.ptr[i + 1]; q++)
+                    if (L.A.col[q] == i && L.A.val[q] > 0.0) diag[i] = L.A.val[q];
+            D.diag = upF(diag);
+            D.b = vec(D.n);
+            D.y = vec(D.n);
+            D.x = vec(D.n);
+            D.t = vec(D.n);
+        }
+        if (l + 1 < g.levels) {
+            D.p_ptr = upI(L.P.ptr);
+            D.p_col = upI(L.P.col);
+            D.p_val = upF(L.P.val);
+            D.r_ptr = upI(L.R.ptr);
+            D.r_col = upI(L.R.col);
+            D.r_val = upF(L.R.val);
+        }
+    }
+    g.y0 = vec((size_t)h->vCapacity + 1);
+    g.t0 = vec((size_t)h->vCapacity + 1);
+    g.coarse_inv = upF(H.coarse_inv);
+    if (e != cudaSuccess) {
+        h->amg_release();
+        return cuda_check(h, e, "multigrid upload");
+    }
+    h->amg = g;
+    h->amgReady = true;
+    h->amgSlots = slots;
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return TG_OK;
+}
+
 // Single-reduction PCG on the V system until rho = r.r falls below rtol^2
 // of its start value or maxIter is reached.  r (slot order) must hold
-// the right-hand side; x receives the correction.
-static int run_vcg(tg_handle* h, double rtol, int maxIter, int* itersOut) {
+// the right-hand side; x receives the correction.  amg: the multigrid
+// V-cycle as the preconditioner instead of the diagonal.
+static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersOut) {
     const size_t need = 4 * (size_t)(maxIter + 2);
     if (h->vScal.n < need) CK(h->vScal.alloc(need));
     VSys v = h->vs();
     const int slots = h->vActive;
     CK(cudaMemsetAsync(h->vScal.p, 0, sizeof(double) * need, h->stream));
-    launch_vcg_init(v, slots, h->stream);
-    launch_vcg_spmv(v, slots, 0, -1.0, h->stream);
+    launch_vcg_init(v, slots, !amg, h->stream);
+    if (amg) launch_amg_vcycle(v, slots, h->amg, 0, -1.0, h->stream);
+    launch_vcg_spmv(v, slots, 0, -1.0, amg, h->stream);
     // stop on the 2-norm of the residual (rho = r.r), the norm the outer
     // FP64 test uses
     double s0[4];
@@ -962,14 +1095,17 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, int* itersOut) {
     const double rho0 = s0[3];
     const double target = rho0 * rtol * rtol;
     int it = 0;
-    const int batch = 16;
-    double sb[4 * batch];
+    // iterations queued between two reads of the residual norms; the
+    // multigrid ones are fewer and launch more kernels each
+    const int batch = amg ? 4 : 16;
+    double sb[4 * 16];
     while (it < maxIter && rho0 > 0.0) {
         const int start = it;
         const int end = std::min(maxIter, it + batch);
         for (; it < end; it++) {
-            launch_vcg_update(v, slots, it, target, h->stream);
-            launch_vcg_spmv(v, slots, it + 1, target, h->stream);
+            launch_vcg_update(v, slots, it, target, !amg, h->stream);
+            if (amg) launch_amg_vcycle(v, slots, h->amg, it + 1, target, h->stream);
+            launch_vcg_spmv(v, slots, it + 1, target, amg, h->stream);
         }
         // rho after j iterations sits at scal[4j+3]; the kernels of later
         // iterations of the batch returned early once it met the target
@@ -1013,6 +1149,15 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     }
     h->converged = h->histValid = false;
     h->removalsSinceSolve = 0;
+    const bool amg = o->preconditioner == 1;
+    if (o->preconditioner < 0 || o->preconditioner > 1)
+        return fail(h, TG_ERR_ARGUMENT, "tg_solve: preconditioner 0 (Jacobi) or 1 (multigrid)");
+    // (re)build the hierarchy when there is none or removals have grown the
+    // system by 2% since
+    if (amg && (!h->amgReady || h->vActive > h->amgSlots + h->amgSlots / 50)) {
+        rc = amg_setup(h, &inf.setup_seconds);
+        if (rc != TG_OK) return rc;
+    }
     for (int outer = 0;; outer++) {
         CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
         launch_vcg_residual(m, vsys, h->vActive, h->acc.p, h->stream);
@@ -1036,7 +1181,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         const double rtol = std::min(0.5, std::max(o->inner_rtol, 0.3 * o->rel_tol / rel));
         int itV = 0, itN = 0;
         if (h->vActive > 0 && r2[0] > 0.0) {
-            rc = run_vcg(h, rtol, o->max_inner, &itV);
+            rc = run_vcg(h, rtol, o->max_inner, amg, &itV);
             if (rc != TG_OK) return rc;
         }
         if (h->countAllN > 0) {

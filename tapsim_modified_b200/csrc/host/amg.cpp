@@ -1,0 +1,316 @@
+#include "amg.h"
+
+#include <algorithm>
+#include <cmath>
+#include <thread>
+
+namespace tg_host {
+namespace {
+
+template <class F>
+void parallel_rows(int n, int threads, F f) {
+    if (threads <= 1 || n < 256) {
+        f(0, n, 0);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const int chunk = (n + threads - 1) / threads;
+    for (int t = 0; t < threads; t++) {
+        const int b = t * chunk, e = std::min(n, b + chunk);
+        if (b >= e) break;
+        pool.emplace_back(f, b, e, t);
+    }
+    for (auto& th : pool) th.join();
+}
+
+AmgCsr transpose(const AmgCsr& P) {
+    AmgCsr R;
+    R.rows = P.cols;
+    R.cols = P.rows;
+    R.ptr.assign(R.rows + 1, 0);
+    for (int32_t c : P.col) R.ptr[c + 1]++;
+    for (int c = 0; c < R.rows; c++) R.ptr[c + 1] += R.ptr[c];
+    R.col.resize(P.col.size());
+    R.val.resize(P.val.size());
+    std::vector<int32_t> next(R.ptr.begin(), R.ptr.end() - 1);
+    for (int i = 0; i < P.rows; i++)
+        for (int q = P.ptr[i]; q < P.ptr[i + 1]; q++) {
+            const int k = next[P.col[q]]++;
+            R.col[k] = i;
+            R.val[k] = P.val[q];
+        }
+    return R;
+}
+
+// Strong off-diagonal entries: |a_ij| >= theta sqrt(a_ii a_jj).
+std::vector<char> strength(const AmgCsr& A, const std::vector<double>& diag, double theta, int threads) {
+    std::vector<char> s(A.col.size(), 0);
+    parallel_rows(A.rows, threads, [&](int b, int e, int) {
+        for (int i = b; i < e; i++)
+            for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) {
+                const int j = A.col[q];
+                if (j == i) continue;
+                s[q] = std::fabs(A.val[q]) >= theta * std::sqrt(std::fabs(diag[i] * diag[j]));
+            }
+    });
+    return s;
+}
+
+// Greedy aggregation (Vanek et al. 1996, section 5): whole strong
+// neighbourhoods first, then the left-over rows join the aggregate they are
+// most strongly connected to, then what remains forms aggregates of its own.
+// Rows without any off-diagonal entry stay out (-2).
+std::vector<int32_t> aggregate(const AmgCsr& A, const std::vector<char>& strong, int* count) {
+    const int n = A.rows;
+    std::vector<int32_t> agg(n, -1);
+    for (int i = 0; i < n; i++) {
+        bool any = false;
+        for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) any |= A.col[q] != i;
+        if (!any) agg[i] = -2;
+    }
+    int nc = 0;
+    for (int i = 0; i < n; i++) {
+        if (agg[i] != -1) continue;
+        bool free = true, hasStrong = false;
+        for (int q = A.ptr[i]; q < A.ptr[i + 1] && free; q++)
+            if (strong[q]) {
+                hasStrong = true;
+                free = agg[A.col[q]] == -1;
+            }
+        if (!free || !hasStrong) continue;
+        agg[i] = nc;
+        for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++)
+            if (strong[q]) agg[A.col[q]] = nc;
+        nc++;
+    }
+    const std::vector<int32_t> first = agg;
+    for (int i = 0; i < n; i++) {
+        if (agg[i] != -1) continue;
+        double best = 0.0;
+        for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) {
+            const int j = A.col[q];
+            if (strong[q] && first[j] >= 0 && std::fabs(A.val[q]) > best) {
+                best = std::fabs(A.val[q]);
+                agg[i] = first[j];
+            }
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        if (agg[i] != -1) continue;
+        agg[i] = nc;
+        for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++)
+            if (strong[q] && agg[A.col[q]] == -1) agg[A.col[q]] = nc;
+        nc++;
+    }
+    *count = nc;
+    return agg;
+}
+
+// P = (I - omega D_F^-1 A_F) P0 with the filtered matrix A_F (weak entries
+// lumped into the diagonal) and the tentative P0 (one per row, its aggregate).
+AmgCsr smoothed_prolongator(const AmgCsr& A, const std::vector<char>& strong, const std::vector<int32_t>& agg,
+                            int nc, double omega, int threads) {
+    const int n = A.rows;
+    // each row's entries (merged by aggregate) go to its slot of an
+    // upper-bound layout (1 + its strong entries), then are compacted
+    std::vector<int64_t> bound(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        int k = agg[i] < 0 ? 0 : 1;
+        if (agg[i] >= 0)
+            for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) k += strong[q] && A.col[q] != i;
+        bound[i + 1] = bound[i] + k;
+    }
+    std::vector<int32_t> tcol(bound[n]), cnt(n, 0);
+    std::vector<double> tval(bound[n]);
+    parallel_rows(n, threads, [&](int b, int e, int) {
+        std::vector<std::pair<int32_t, double>> tmp;
+        for (int i = b; i < e; i++) {
+            if (agg[i] < 0) continue;
+            double dF = 0.0;
+            for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++)
+                if (A.col[q] == i || !strong[q]) dF += A.val[q];
+            tmp.clear();
+            tmp.emplace_back(agg[i], 1.0 - omega);
+            for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) {
+                const int j = A.col[q];
+                if (j == i || !strong[q] || agg[j] < 0) continue;
+                tmp.emplace_back(agg[j], -omega * A.val[q] / dF);
+            }
+            std::sort(tmp.begin(), tmp.end());
+            int k = 0;
+            const int64_t base = bound[i];
+            for (const auto& e2 : tmp) {
+                if (k > 0 && tcol[base + k - 1] == e2.first) {
+                    tval[base + k - 1] += e2.second;
+                } else {
+                    tcol[base + k] = e2.first;
+                    tval[base + k] = e2.second;
+                    k++;
+                }
+            }
+            cnt[i] = k;
+        }
+    });
+    AmgCsr P;
+    P.rows = n;
+    P.cols = nc;
+    P.ptr.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) P.ptr[i + 1] = P.ptr[i] + cnt[i];
+    P.col.resize(P.ptr[n]);
+    P.val.resize(P.ptr[n]);
+    parallel_rows(n, threads, [&](int b, int e, int) {
+        for (int i = b; i < e; i++)
+            for (int k = 0; k < cnt[i]; k++) {
+                P.col[P.ptr[i] + k] = tcol[bound[i] + k];
+                P.val[P.ptr[i] + k] = tval[bound[i] + k];
+            }
+    });
+    return P;
+}
+
+// A_c = R A P, one coarse row per step, dense accumulator per thread.
+AmgCsr galerkin(const AmgCsr& R, const AmgCsr& A, const AmgCsr& P, int threads) {
+    const int nc = R.rows;
+    std::vector<std::vector<std::pair<int32_t, double>>> rows(nc);
+    parallel_rows(nc, threads, [&](int b, int e, int) {
+        std::vector<double> acc(nc, 0.0);
+        std::vector<char> used(nc, 0);
+        std::vector<int32_t> touched;
+        for (int c = b; c < e; c++) {
+            touched.clear();
+            for (int qr = R.ptr[c]; qr < R.ptr[c + 1]; qr++) {
+                const int i = R.col[qr];
+                const double rci = R.val[qr];
+                for (int qa = A.ptr[i]; qa < A.ptr[i + 1]; qa++) {
+                    const int k = A.col[qa];
+                    const double w = rci * A.val[qa];
+                    for (int qp = P.ptr[k]; qp < P.ptr[k + 1]; qp++) {
+                        const int cc = P.col[qp];
+                        if (!used[cc]) {
+                            used[cc] = 1;
+                            touched.push_back(cc);
+                        }
+                        acc[cc] += w * P.val[qp];
+                    }
+                }
+            }
+            std::sort(touched.begin(), touched.end());
+            auto& out = rows[c];
+            out.reserve(touched.size());
+            for (int32_t cc : touched) {
+                out.emplace_back(cc, acc[cc]);
+                acc[cc] = 0.0;
+                used[cc] = 0;
+            }
+        }
+    });
+    AmgCsr Ac;
+    Ac.rows = Ac.cols = nc;
+    Ac.ptr.assign(nc + 1, 0);
+    for (int c = 0; c < nc; c++) Ac.ptr[c + 1] = Ac.ptr[c] + (int32_t)rows[c].size();
+    Ac.col.resize(Ac.ptr[nc]);
+    Ac.val.resize(Ac.ptr[nc]);
+    for (int c = 0; c < nc; c++) {
+        int k = Ac.ptr[c];
+        for (const auto& e2 : rows[c]) {
+            Ac.col[k] = e2.first;
+            Ac.val[k] = e2.second;
+            k++;
+        }
+    }
+    return Ac;
+}
+
+// Gauss-Jordan inverse with partial pivoting (row-major, in place).
+bool dense_inverse(int n, std::vector<double>& a, std::vector<double>* inv) {
+    inv->assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) (*inv)[(size_t)i * n + i] = 1.0;
+    for (int c = 0; c < n; c++) {
+        int p = c;
+        for (int r = c + 1; r < n; r++)
+            if (std::fabs(a[(size_t)r * n + c]) > std::fabs(a[(size_t)p * n + c])) p = r;
+        const double piv = a[(size_t)p * n + c];
+        if (piv == 0.0 || !std::isfinite(piv)) return false;
+        if (p != c)
+            for (int k = 0; k < n; k++) {
+                std::swap(a[(size_t)p * n + k], a[(size_t)c * n + k]);
+                std::swap((*inv)[(size_t)p * n + k], (*inv)[(size_t)c * n + k]);
+            }
+        const double s = 1.0 / piv;
+        for (int k = 0; k < n; k++) {
+            a[(size_t)c * n + k] *= s;
+            (*inv)[(size_t)c * n + k] *= s;
+        }
+        for (int r = 0; r < n; r++) {
+            if (r == c) continue;
+            const double f = a[(size_t)r * n + c];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; k++) {
+                a[(size_t)r * n + k] -= f * a[(size_t)c * n + k];
+                (*inv)[(size_t)r * n + k] -= f * (*inv)[(size_t)c * n + k];
+            }
+        }
+    }
+    return true;
+}
+
+}  // namespace
+
+std::string amg_build(AmgCsr&& A0, const AmgOptions& opt, AmgHierarchy* out) {
+    const int threads = opt.threads > 0 ? opt.threads : std::max(1u, std::thread::hardware_concurrency());
+    out->levels.clear();
+    out->coarse_inv.clear();
+    AmgCsr A = std::move(A0);
+    for (int lev = 0;; lev++) {
+        std::vector<double> diag(A.rows, 0.0);
+        for (int i = 0; i < A.rows; i++)
+            for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++)
+                if (A.col[q] == i) diag[i] = A.val[q];
+        for (int i = 0; i < A.rows; i++)
+            if (!(diag[i] > 0.0)) {
+                // rows without an entry (padding) keep a unit diagonal
+                bool any = false;
+                for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) any |= A.col[q] != i;
+                if (any) return "amg: non-positive diagonal";
+                diag[i] = 1.0;
+            }
+        AmgLevel L;
+        const bool last = A.rows <= opt.max_coarse || lev + 1 >= opt.max_levels;
+        if (!last) {
+            const std::vector<char> strong = strength(A, diag, lev == 0 ? opt.theta : opt.theta_coarse, threads);
+            int nc = 0;
+            const std::vector<int32_t> agg = aggregate(A, strong, &nc);
+            if (nc == 0 || nc > (int)(0.8 * A.rows)) {
+                L.A = std::move(A);
+                out->levels.push_back(std::move(L));
+                break;
+            }
+            L.P = smoothed_prolongator(A, strong, agg, nc, opt.omega, threads);
+            L.R = transpose(L.P);
+            AmgCsr Ac = galerkin(L.R, A, L.P, threads);
+            L.A = std::move(A);
+            out->levels.push_back(std::move(L));
+            A = std::move(Ac);
+            continue;
+        }
+        L.A = std::move(A);
+        out->levels.push_back(std::move(L));
+        break;
+    }
+    // coarsest level: dense inverse
+    const AmgCsr& C = out->levels.back().A;
+    if (C.rows > 4096) return "amg: coarsest level too large for a dense inverse";
+    std::vector<double> dense((size_t)C.rows * C.rows, 0.0);
+    for (int i = 0; i < C.rows; i++) {
+        bool any = false;
+        for (int q = C.ptr[i]; q < C.ptr[i + 1]; q++) {
+            dense[(size_t)i * C.rows + C.col[q]] = C.val[q];
+            any = true;
+        }
+        if (!any) dense[(size_t)i * C.rows + i] = 1.0;
+    }
+    if (!dense_inverse(C.rows, dense, &out->coarse_inv)) return "amg: singular coarsest operator";
+    return std::string();
+}
+
+}  // namespace tg_host

@@ -91,9 +91,32 @@ struct VSys {
     int32_t* count;               // next free slot (device counter)
     int capacity;
 };
-void launch_vcg_init(const VSys& v, int slots, cudaStream_t s);
-void launch_vcg_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s);
-void launch_vcg_update(const VSys& v, int slots, int it, double target, cudaStream_t s);
+// jacobi: the Jacobi preconditioner (u = r / d inside init / update);
+// otherwise u comes from launch_amg_vcycle and the SpMV adds gamma = r.u
+void launch_vcg_init(const VSys& v, int slots, bool jacobi, cudaStream_t s);
+void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withGamma, cudaStream_t s);
+void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s);
+
+// ---- multigrid preconditioner (amg.cu) ----
+constexpr int kAmgMaxLevels = 12;
+struct AmgDevLevel {
+    int n;                                  // rows (level 0: slots covered by its prolongator)
+    const int32_t *a_ptr, *a_col;           // operator, levels >= 1 (CSR with diagonal)
+    const float *a_val, *diag;
+    const int32_t *p_ptr, *p_col;           // prolongator: n rows
+    const float* p_val;
+    const int32_t *r_ptr, *r_col;           // restriction: the next level's rows
+    const float* r_val;
+    float *b, *y, *x, *t;                   // right-hand side, work, result, residual (levels >= 1)
+};
+struct AmgDev {
+    int levels;                             // including level 0 (the V system) and the coarsest
+    AmgDevLevel lev[kAmgMaxLevels];
+    float *y0, *t0;                         // level-0 work vectors (capacity + 1)
+    const float* coarse_inv;                // dense inverse of the coarsest operator, row-major
+};
+// u = M^-1 r, one V(1,1)-cycle, for CG iteration `it`
+void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s);
 // phi64 += x on the V rows; with record, hist += x as well
 void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s);
 // warm start: hist *= alpha, phi64 += hist on the V rows

@@ -148,8 +148,10 @@ def trace_opts(time_step=1e-14, min_time_step=1e-16, error_threshold=1e-6, max_s
                            integrator, stepper)
 
 
-def solve_opts(rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4, warm_start=0) -> N.tg_solve_opts:
-    return N.tg_solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, 0)
+def solve_opts(rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4, warm_start=0,
+               preconditioner=0) -> N.tg_solve_opts:
+    """preconditioner: 0 Jacobi, 1 multigrid (tg_solve_opts)."""
+    return N.tg_solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, preconditioner)
 
 
 class Grid:
@@ -196,10 +198,11 @@ class Grid:
             self._ck(rc)
         return rc, it.value, dev.value
 
-    def solve(self, rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4, warm_start=0) -> N.tg_solve_info:
+    def solve(self, rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4, warm_start=0,
+              preconditioner=0) -> N.tg_solve_info:
         info = N.tg_solve_info()
-        self._ck(N.lib().tg_solve(self._h, C.byref(solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start)),
-                                  C.byref(info)))
+        o = solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, preconditioner)
+        self._ck(N.lib().tg_solve(self._h, C.byref(o), C.byref(info)))
         return info
 
     def residual(self) -> float:

@@ -165,7 +165,9 @@ def test_paths_match_oracle(solved):
         assert np.linalg.norm(ip - p["position"][inside], axis=1).max() <= 1e-3 * disp
         # the extrapolated point is the impact
         np.testing.assert_array_equal(p["position"][-1], np.array(dev_imp.stop, np.float32))
-        if dev_imp.steps == ref.steps:
+        # the same step sequence (not only the same count: a rounding-level
+        # accept/reject flip changes the step sizes) gives the same estimate
+        if len(p) == len(rp) and np.allclose(p["time"][:-1], rp[:-1, 0], rtol=1e-5, atol=0):
             np.testing.assert_allclose(e, re, rtol=1e-3, atol=0)
         else:
             assert np.all((e / re > 0.1) & (e / re < 10.0))
