@@ -20,8 +20,9 @@ namespace {
 constexpr int kBlock = 256;
 constexpr float kSmooth = 2.0f / 3.0f;
 
-__device__ __forceinline__ bool done(const double* scal, int it, double target) {
-    return scal[4 * it + 3] <= target;
+// the CG iteration has converged: rho_it <= rel2 * rho_0 (rel2 < 0: never)
+__device__ __forceinline__ bool done(const double* scal, int it, double rel2) {
+    return rel2 >= 0.0 && scal[4 * it + 3] <= rel2 * scal[3];
 }
 
 // y = w b / d

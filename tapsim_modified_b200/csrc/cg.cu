@@ -25,7 +25,13 @@ namespace {
 constexpr int kBlock = 256;
 
 // per iteration i: gamma_i = r.u, delta_i = w.u, alpha_i and rho_i = r.r at
-// scal[4i .. 4i+3]
+// scal[4i .. 4i+3].  A kernel of iteration it does nothing once rho_it <=
+// rel2 * rho_0 (rel2 < 0: never), so that iterations can be queued before
+// the host has seen rho_0.
+__device__ __forceinline__ bool cg_done(const double* scal, int it, double rel2) {
+    return rel2 >= 0.0 && scal[4 * it + 3] <= rel2 * scal[3];
+}
+
 __device__ __forceinline__ void cg_coeffs(const double* scal, int it, double* alpha, double* beta) {
     const double g = scal[4 * it], d = scal[4 * it + 1];
     if (it == 0) {
@@ -61,9 +67,9 @@ __global__ void k_vcg_init(VSys v, int slots, int jacobi) {
 
 // w = A u over SELL-32 slices; delta -> scal[4*it+1] (it = iteration whose
 // u this is), and with withGamma gamma = r.u -> scal[4*it]; skipped once
-// rho_it <= target
+// iteration it has converged (cg_done)
 __global__ void k_vcg_spmv(VSys v, int slices, int it, double target, int withGamma) {
-    if (it >= 0 && v.scal[4 * it + 3] <= target) return;
+    if (it >= 0 && cg_done(v.scal, it, target)) return;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     double dl = 0.0, gl = 0.0;
@@ -106,7 +112,7 @@ __global__ void k_vcg_spmv(VSys v, int slices, int it, double target, int withGa
 // rho_{it+1} = r.r; with the Jacobi preconditioner also u = r / d and
 // gamma_{it+1} = r.u
 __global__ void k_vcg_update(VSys v, int slots, int it, double target, int jacobi) {
-    if (v.scal[4 * it + 3] <= target) return;
+    if (cg_done(v.scal, it, target)) return;
     double alpha, beta;
     cg_coeffs(v.scal, it, &alpha, &beta);
     if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[4 * it + 2] = alpha;

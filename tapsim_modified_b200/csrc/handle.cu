@@ -131,6 +131,27 @@ struct tg_handle {
     int vActive = 0;         // slots in use (host mirror of vCount)
     double vEntries = 0.0;   // stored (non-padding) couplings
 
+    // pinned host staging of the event loop's small copies, so that they
+    // queue without blocking and a sync only waits for the device
+    static constexpr int kMaxColours = 4096;
+    struct Pinned {
+        unsigned long long keys[8];
+        double sums[4];
+        double r2[4];
+        double sb[4 * 17];
+        double before[4];     // phi and field_o1 of the removed cell before removal
+        double after[4];      // and after
+        float normal[4];
+        int32_t node[4];
+        int32_t misc[4];      // V and N row counts, surface slots
+        int32_t result[1024];
+        int32_t flipped[1024];
+        int32_t counts[2 * kMaxColours];
+    };
+    Pinned* pin = nullptr;
+    int vNext = 0;            // host mirror of the V system's slot counter
+    int lastItersJacobi = 16, lastItersAmg = 4;  // iterations of the last inner solves
+
     // multigrid preconditioner of the V system (amg.cu): hierarchy built on
     // the host from the V system as it is, uploaded as CSR levels
     bool amgReady = false;
@@ -671,7 +692,12 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     {
         const int32_t next = E0;
         chk(up(h->vCount, &next, 1));
+        h->vNext = E0;
     }
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->pin), sizeof(tg_handle::Pinned));
+    chk(h->stageI.alloc(1024));
+    chk(h->stageD.alloc(1024));
+    chk(h->stageF.alloc(1024));
     chk(h->vVec.alloc(8 * ((size_t)h->vCapacity + 1)));
     if (e == cudaSuccess) chk(cudaMemset(h->vVec.p, 0, 8 * ((size_t)h->vCapacity + 1) * sizeof(float)));
     if (e == cudaSuccess) chk(cudaMemcpy(h->vVec.p, vD.data(), vD.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -708,6 +734,8 @@ void tg_destroy(tg_handle* h) {
     h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
     h->stageImpact.release(); h->pathBuf.release(); h->pathErr.release();
     h->amg_release();
+    if (h->pin) cudaFreeHost(h->pin);
+    h->pin = nullptr;
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
@@ -1088,47 +1116,59 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
     if (amg) launch_amg_vcycle(v, slots, h->amg, 0, -1.0, h->stream);
     launch_vcg_spmv(v, slots, 0, -1.0, amg, h->stream);
     // stop on the 2-norm of the residual (rho = r.r), the norm the outer
-    // FP64 test uses
-    double s0[4];
-    CK(cudaMemcpyAsync(s0, h->vScal.p, sizeof(s0), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    const double rho0 = s0[3];
-    const double target = rho0 * rtol * rtol;
+    // FP64 test uses: rho_it <= rtol^2 rho_0, tested by the kernels
+    // themselves, so the iterations queue before rho_0 is read back
+    const double rel2 = rtol * rtol;
     int it = 0;
-    // iterations queued between two reads of the residual norms; the
-    // multigrid ones are fewer and launch more kernels each
-    const int batch = amg ? 4 : 16;
-    double sb[4 * 16];
-    while (it < maxIter && rho0 > 0.0) {
+    // iterations queued before the first read: about as many as the last
+    // solve took; then small batches
+    int& last = amg ? h->lastItersAmg : h->lastItersJacobi;
+    int batch = std::min(16, std::max(amg ? 2 : 8, last - (amg ? 1 : 4)));
+    double* sb = h->pin->sb;  // scal[0..3], then the batch's iterations
+    while (it < maxIter) {
         const int start = it;
         const int end = std::min(maxIter, it + batch);
         for (; it < end; it++) {
-            launch_vcg_update(v, slots, it, target, !amg, h->stream);
-            if (amg) launch_amg_vcycle(v, slots, h->amg, it + 1, target, h->stream);
-            launch_vcg_spmv(v, slots, it + 1, target, amg, h->stream);
+            launch_vcg_update(v, slots, it, rel2, !amg, h->stream);
+            if (amg) launch_amg_vcycle(v, slots, h->amg, it + 1, rel2, h->stream);
+            launch_vcg_spmv(v, slots, it + 1, rel2, amg, h->stream);
         }
         // rho after j iterations sits at scal[4j+3]; the kernels of later
         // iterations of the batch returned early once it met the target
-        CK(cudaMemcpyAsync(sb, h->vScal.p + 4 * (size_t)(start + 1), sizeof(double) * 4 * (end - start),
+        CK(cudaMemcpyAsync(sb, h->vScal.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(sb + 4, h->vScal.p + 4 * (size_t)(start + 1), sizeof(double) * 4 * (end - start),
                            cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
+        const double rho0 = sb[3];
+        if (!(rho0 > 0.0)) {
+            it = 0;
+            break;
+        }
         bool done = false;
         for (int j = start + 1; j <= end && !done; j++)
-            if (sb[4 * (j - start - 1) + 3] <= target) {
+            if (sb[4 + 4 * (j - start - 1) + 3] <= rel2 * rho0) {
                 it = j;
                 done = true;
             }
         if (done) break;
+        batch = amg ? 2 : 4;
     }
+    last = it;
     *itersOut = it;
     return TG_OK;
 }
 
 int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     if (!h || !o) return fail(h, TG_ERR_ARGUMENT, "tg_solve: null argument");
-    int rc = ensure_bnorm(h);
-    if (rc != TG_OK) return rc;
+    int rc = TG_OK;
     DevMesh m = h->dm();
+    // ||b||^2 (after removals it changes) is read with the first residual
+    bool needB = !h->bnormValid;
+    if (needB) {
+        CK(cudaMemsetAsync(h->acc.p + 2, 0, sizeof(double), h->stream));
+        launch_bnorm(m, h->allV.p, h->countAllV, h->acc.p + 2, h->stream);
+        launch_bnorm(m, h->allN.p, h->countAllN, h->acc.p + 2, h->stream);
+    }
     VSys vsys = h->vs();
     CGVectors vN = h->cg(1);
     tg_solve_info inf{};
@@ -1162,10 +1202,15 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
         launch_vcg_residual(m, vsys, h->vActive, h->acc.p, h->stream);
         launch_residual(m, h->allN.p, h->countAllN, vN.r, h->acc.p + 1, h->stream);
-        double r2[2];
-        CK(cudaMemcpyAsync(r2, h->acc.p, sizeof(r2), cudaMemcpyDeviceToHost, h->stream));
+        double* r2 = h->pin->r2;
+        CK(cudaMemcpyAsync(r2, h->acc.p, sizeof(double) * (needB ? 3 : 2), cudaMemcpyDeviceToHost, h->stream));
         rc = sync_status(h, "tg_solve residual");
         if (rc != TG_OK) return rc;
+        if (needB) {
+            h->bnorm2 = r2[2];
+            h->bnormValid = true;
+            needB = false;
+        }
         rel = h->bnorm2 > 0.0 ? std::sqrt((r2[0] + r2[1]) / h->bnorm2) : std::sqrt(r2[0] + r2[1]);
         if (outer == 0) inf.initial_rel_residual = rel;
         inf.outer = outer;
@@ -1256,15 +1301,20 @@ int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_sel
     if (mode < 0 || mode > 3) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: probability mode 0..3");
     if (mode == 1 && !(temperature > 0.0f))
         return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: Boltzmann probabilities need a temperature > 0");
-    unsigned long long k[7] = {0, 0, 0, 0, 0, 0, 0};
-    double sums[2] = {0.0, 0.0};
+    // ratios, scores and keys, then the candidate and the runner-ups, all
+    // decoded on the device; one read at the end
     CK(cudaMemsetAsync(h->keys.p, 0, 7 * sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
     launch_surface_select(h->dm(), h->sf(), h->surfSlots, mode, temperature, h->keys.p, h->acc.p, h->stream);
-    CK(cudaMemcpyAsync(k, h->keys.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(sums, h->acc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    launch_surface_best(h->sf(), h->surfSlots, h->acc.p, h->keys.p, h->stream);
+    launch_surface_second(h->sf(), h->surfSlots, h->acc.p, h->keys.p, h->stream);
+    CK(cudaMemcpyAsync(h->pin->keys, h->keys.p, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->pin->sums, h->acc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     int rc = sync_status(h, "tg_surface_select");
     if (rc != TG_OK) return rc;
+    unsigned long long k[7];
+    std::memcpy(k, h->pin->keys, sizeof(k));
+    const double sums[2] = {h->pin->sums[0], h->pin->sums[1]};
     tg_select_info s{};
     s.prob_mode = mode;
     s.ratio_sum = sums[0];
@@ -1288,21 +1338,13 @@ int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_sel
     const int bestRatioNode = unkey(k[0], &bestRatio);
     s.apex = unkey(k[1], &zmax);
     s.best_ratio = bestRatio;
+    (void)bestRatioNode;
     h->surfMinNode = (int32_t)(~(uint32_t)k[2]);
     h->surfMaxNode = (int32_t)k[3] - 1;
     // the probabilities are score / sum in float, as the reference normalises
-    const float fsum = (float)s.score_sum;
-    launch_surface_best(h->sf(), h->surfSlots, fsum, bestRatioNode, h->keys.p, h->stream);
-    CK(cudaMemcpyAsync(&k[4], h->keys.p + 4, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
-    rc = sync_status(h, "tg_surface_select");
-    if (rc != TG_OK) return rc;
     float bestP = 0.0f;
     s.candidate = unkey(k[4], &bestP);
     if ((uint32_t)(k[4] >> 32) == 0u) bestP = std::numeric_limits<float>::quiet_NaN();
-    launch_surface_second(h->sf(), h->surfSlots, fsum, s.candidate, bestRatioNode, h->keys.p, h->stream);
-    CK(cudaMemcpyAsync(&k[5], h->keys.p + 5, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
-    rc = sync_status(h, "tg_surface_select");
-    if (rc != TG_OK) return rc;
     float secondP = 0.0f, secondRatio = 0.0f;
     if (k[5]) unkey(k[5], &secondP);
     if (k[6]) unkey(k[6], &secondRatio);
@@ -1534,47 +1576,61 @@ int tg_surface_normal(tg_handle* h, int32_t node, float normal[3]) {
     return sync_status(h, "tg_surface_normal");
 }
 
-int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached, int32_t* numDetached) {
-    if (!h || node < 0 || node >= h->n) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: bad node");
-    if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: surface not initialised");
-    launch_take_away(h->dm(), h->rl(), h->sf(), node, h->vacuumId, h->result.p, (int)h->result.n, h->stream);
-    std::vector<int32_t> res(h->result.n);
-    CK(cudaMemcpyAsync(res.data(), h->result.p, sizeof(int32_t) * res.size(), cudaMemcpyDeviceToHost, h->stream));
+// evap_takeAway on the device with one read back: the removal's result
+// and the row and surface counts come back together; the cells that become
+// free non-Neumann rows are appended to the V system, whose slot counter
+// the host mirrors (an overflow raises S_CAPACITY at the next status read).
+static int take_away_impl(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached, int32_t* numDetached) {
+    if (h->ncol > tg_handle::kMaxColours) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: too many colours");
+    tg_handle::Pinned* pin = h->pin;
+    const int cap = (int)std::min<size_t>(h->result.n, 1024);
+    launch_take_away(h->dm(), h->rl(), h->sf(), node, h->vacuumId, h->result.p, cap, h->stream);
+    CK(cudaMemcpyAsync(pin->result, h->result.p, sizeof(int32_t) * cap, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(pin->counts, h->countVD.p, sizeof(int32_t) * h->ncol, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(pin->counts + h->ncol, h->countND.p, sizeof(int32_t) * h->ncol, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaMemcpyAsync(pin->misc, h->countAllD.p, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(pin->misc + 2, h->surfCount.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     int rc = sync_status(h, "tg_take_away");
     if (rc != TG_OK) return rc;
-    rc = refresh_counts(h);
-    if (rc != TG_OK) return rc;
-    const int nd = res[0];
-    std::vector<int32_t> flipped;
-    if (!(h->h_type[node] >= 0 && h->types[h->h_type[node]].dirichlet == 0)) flipped.push_back(node);
+    std::memcpy(h->countV.data(), pin->counts, sizeof(int32_t) * h->ncol);
+    std::memcpy(h->countN.data(), pin->counts + h->ncol, sizeof(int32_t) * h->ncol);
+    h->countAllV = pin->misc[0];
+    h->countAllN = pin->misc[1];
+    h->surfSlots = std::min(pin->misc[2], h->n);
+    const int nd = pin->result[0];
+    int nf = 0;
+    if (!(h->h_type[node] >= 0 && h->types[h->h_type[node]].dirichlet == 0)) pin->flipped[nf++] = node;
     h->h_type[node] = (int8_t)h->vacuumId;
-    for (int k = 0; k < nd && k + 1 < (int)res.size(); k++) {
-        const int j = res[1 + k];
-        if (h->types[h->h_type[j]].dirichlet) flipped.push_back(j);
+    for (int k = 0; k < nd && k + 1 < cap; k++) {
+        const int j = pin->result[1 + k];
+        if (h->types[h->h_type[j]].dirichlet) pin->flipped[nf++] = j;
         h->h_type[j] = (int8_t)h->vacuumId;
         if (detached && k < capacity) detached[k] = j;
     }
     if (numDetached) *numDetached = nd;
     // cells that became non-Neumann free rows join the V system
     const tg_type& vt = h->types[h->vacuumId];
-    if (!vt.dirichlet && !vt.neumann && !flipped.empty()) {
-        rc = stage(h, h->stageI, flipped.size());
-        if (rc != TG_OK) return rc;
-        CK(cudaMemcpyAsync(h->stageI.p, flipped.data(), sizeof(int32_t) * flipped.size(), cudaMemcpyHostToDevice,
-                           h->stream));
-        launch_vsys_add_rows(h->dm(), h->vs(), h->stageI.p, (int)flipped.size(), h->stream);
-        int32_t next = 0;
-        CK(cudaMemcpyAsync(&next, h->vCount.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-        rc = sync_status(h, "tg_take_away (V rows)");
-        if (rc != TG_OK) return rc;
-        if (next > h->vCapacity) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: V-system reserve exhausted");
-        h->vActive = (next + 31) / 32 * 32;
+    if (!vt.dirichlet && !vt.neumann && nf > 0) {
+        if (h->vNext + nf > h->vCapacity) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: V-system reserve exhausted");
+        CK(cudaMemcpyAsync(h->stageI.p, pin->flipped, sizeof(int32_t) * nf, cudaMemcpyHostToDevice, h->stream));
+        launch_vsys_add_rows(h->dm(), h->vs(), h->stageI.p, nf, h->stream);
+        h->vNext += nf;
+        h->vActive = (h->vNext + 31) / 32 * 32;
     }
     h->bnormValid = false;
     h->selValid = false;
     h->removalsSinceSolve++;
     h->lastSite = node;
     return TG_OK;
+}
+
+int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached, int32_t* numDetached) {
+    if (!h || node < 0 || node >= h->n) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: bad node");
+    if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: surface not initialised");
+    const int rc = take_away_impl(h, node, capacity, detached, numDetached);
+    if (rc != TG_OK) return rc;
+    return sync_status(h, "tg_take_away (V rows)");
 }
 
 int tg_update_coordination(tg_handle* h) {
@@ -1743,27 +1799,28 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
     rec->best_ratio = sel.best_ratio;
     rec->second_ratio = sel.second_ratio;
     rec->scaling_reference = sel.best_ratio;
-    {
-        double phi = 0.0, E[3];
-        CK(cudaMemcpyAsync(&phi, h->phi64.p + node, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        rc = tg_field_o1(h, 1, &node, E);
-        if (rc != TG_OK) return rc;
-        rec->phi_before = (float)phi;
-        for (int k = 0; k < 3; k++) rec->field_before[k] = (float)E[k];
-    }
+    // the state before removal (potential, field_o1, surface normal of the
+    // candidate) is copied into pinned memory and read with the record at
+    // the end of the event
+    tg_handle::Pinned* pin = h->pin;
+    pin->node[0] = node;
+    CK(cudaMemcpyAsync(h->stageI.p + 512, &pin->node[0], sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    launch_field_o1(h->dm(), h->stageI.p + 512, 1, h->stageD.p, h->stream);
+    CK(cudaMemcpyAsync(&pin->before[0], h->phi64.p + node, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&pin->before[1], h->stageD.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     for (int k = 0; k < 3; k++) rec->apex[k] = sel.apex >= 0 ? h->h_xyz[3 * (size_t)sel.apex + k] : 0.0f;
     if (o->normal_enabled) {
-        rc = tg_surface_normal(h, node, rec->normal);
-        if (rc != TG_OK) return rc;
+        // the candidate is a surface cell by construction
+        launch_surface_normal(h->dm(), h->sf(), node, h->vacuumId, h->stageF.p, h->stream);
+        CK(cudaMemcpyAsync(pin->normal, h->stageF.p, 3 * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     }
     const tg_type removed = h->types[h->h_type[node]];
     // II) removal
     int32_t nd = 0;
-    rc = tg_take_away(h, node, 0, nullptr, &nd);
+    rc = take_away_impl(h, node, 0, nullptr, &nd);
     if (rc != TG_OK) return rc;
     rec->detached = nd;
-    rc = tg_update_coordination(h);
-    if (rc != TG_OK) return rc;
+    launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
     // III) relaxation
     if (o->relax_mode == 0) {
         int64_t it = 0;
@@ -1871,13 +1928,18 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
             if (rc != TG_OK) return rc;
         }
     }
-    {
-        double phi = 0.0, E[3];
-        CK(cudaMemcpyAsync(&phi, h->phi64.p + node, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        rc = tg_field_o1(h, 1, &node, E);
-        if (rc != TG_OK) return rc;
-        rec->phi_after = (float)phi;
-        for (int k = 0; k < 3; k++) rec->field_after[k] = (float)E[k];
+    // the state after removal, and one read of both
+    launch_field_o1(h->dm(), h->stageI.p + 512, 1, h->stageD.p + 4, h->stream);
+    CK(cudaMemcpyAsync(&pin->after[0], h->phi64.p + node, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&pin->after[1], h->stageD.p + 4, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    rc = sync_status(h, "tg_run_event");
+    if (rc != TG_OK) return rc;
+    rec->phi_before = (float)pin->before[0];
+    rec->phi_after = (float)pin->after[0];
+    for (int k = 0; k < 3; k++) {
+        rec->field_before[k] = (float)pin->before[1 + k];
+        rec->field_after[k] = (float)pin->after[1 + k];
+        if (o->normal_enabled) rec->normal[k] = pin->normal[k];
     }
     return TG_OK;
 }

@@ -92,7 +92,9 @@ struct VSys {
     int capacity;
 };
 // jacobi: the Jacobi preconditioner (u = r / d inside init / update);
-// otherwise u comes from launch_amg_vcycle and the SpMV adds gamma = r.u
+// otherwise u comes from launch_amg_vcycle and the SpMV adds gamma = r.u.
+// `target` of the iteration kernels (and of the V-cycle) is relative: they
+// do nothing once rho_it <= target * rho_0; a negative target never skips
 void launch_vcg_init(const VSys& v, int slots, bool jacobi, cudaStream_t s);
 void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withGamma, cudaStream_t s);
 void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s);
@@ -165,14 +167,12 @@ void launch_surface_init(const DevMesh& m, Surface sf, int vacuumId, cudaStream_
 // acc[0] sum of ratios, acc[1] sum of scores
 void launch_surface_select(const DevMesh& m, Surface sf, int slots, int mode, float temperature,
                            unsigned long long* keys, double* acc, cudaStream_t s);
-// keys[4] candidate (first maximum of score / sum), keys[5] runner-up
-// probability (excluding the candidate), keys[6] runner-up ratio
-// (excluding bestRatioNode)
-void launch_surface_best(Surface sf, int slots, float sum, int bestRatioNode, unsigned long long* keys,
-                         cudaStream_t s);
-void launch_surface_second(Surface sf, int slots, float sum, int candidate, int bestRatioNode,
-                           unsigned long long* keys, cudaStream_t s);
-// *acc = sum of score / sum over surface nodes <= upTo (Monte-Carlo choice)
+// keys[4] candidate (first maximum of score / sum, sum = acc[1]), then
+// keys[5] runner-up probability (excluding the candidate) and keys[6]
+// runner-up ratio (excluding the best-ratio node of keys[0]); both read what
+// they need from device memory, so the selection needs one read at its end
+void launch_surface_best(Surface sf, int slots, const double* acc, unsigned long long* keys, cudaStream_t s);
+void launch_surface_second(Surface sf, int slots, const double* acc, unsigned long long* keys, cudaStream_t s);
 void launch_surface_prefix(Surface sf, int slots, float sum, int upTo, double* acc, cudaStream_t s);
 void launch_field_o1(const DevMesh& m, const int32_t* nodes, int count, double* out, cudaStream_t s);
 // evap_takeAway in one small kernel; result[0] = number of detached nodes,

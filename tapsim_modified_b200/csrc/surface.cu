@@ -277,18 +277,29 @@ __device__ __forceinline__ unsigned long long prob_key(float p, int i) {
     return ((unsigned long long)hi << 32) | (~(uint32_t)i);
 }
 
-__global__ void k_surface_best(Surface sf, int slots, float sum, unsigned long long* key) {
+// The node of a (value, node) key: the low word holds ~node.
+__device__ __forceinline__ int key_node(unsigned long long key) { return (int)(~(uint32_t)key); }
+
+// keys[4]: the first maximum of score / sum, sum = acc[1] as float (the
+// reference normalises in float); nothing on an empty surface (keys[0] == 0)
+__global__ void k_surface_best(Surface sf, int slots, const double* acc, unsigned long long* keys) {
+    if (keys[0] == 0ull) return;
+    const float sum = (float)acc[1];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long k = 0ull;
     if (t < slots) {
         const int i = sf.list[t];
         if (i >= 0) k = prob_key(sf.score[t] / sum, i);
     }
-    block_max_atomic_u64<kBlock>(k, key);
+    block_max_atomic_u64<kBlock>(k, &keys[4]);
 }
 
-__global__ void k_surface_second(Surface sf, int slots, float sum, int candidate, int bestRatioNode,
-                                 unsigned long long* keys) {
+// keys[5]: the runner-up probability (the candidate of keys[4] left out),
+// keys[6]: the runner-up ratio (the best-ratio node of keys[0] left out)
+__global__ void k_surface_second(Surface sf, int slots, const double* acc, unsigned long long* keys) {
+    if (keys[0] == 0ull) return;
+    const float sum = (float)acc[1];
+    const int candidate = key_node(keys[4]), bestRatioNode = key_node(keys[0]);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long kp = 0ull, kr = 0ull;
     if (t < slots) {
@@ -296,8 +307,8 @@ __global__ void k_surface_second(Surface sf, int slots, float sum, int candidate
         if (i >= 0 && i != candidate) kp = prob_key(sf.score[t] / sum, i);
         if (i >= 0 && i != bestRatioNode) kr = ((unsigned long long)float_order_key(sf.ratio[t]) << 32) | (~(uint32_t)i);
     }
-    block_max_atomic_u64<kBlock>(kp, &keys[0]);
-    block_max_atomic_u64<kBlock>(kr, &keys[1]);
+    block_max_atomic_u64<kBlock>(kp, &keys[5]);
+    block_max_atomic_u64<kBlock>(kr, &keys[6]);
 }
 
 // sum of the normalised probabilities of the surface nodes <= upTo
@@ -597,17 +608,11 @@ void launch_surface_select(const DevMesh& m, Surface sf, int slots, int mode, fl
         k_surface_select<<<blocks(slots), kBlock, 0, s>>>(m, sf, slots, mode, temperature, keys, acc);
     }
 }
-void launch_surface_best(Surface sf, int slots, float sum, int bestRatioNode, unsigned long long* keys,
-                         cudaStream_t s) {
-    (void)bestRatioNode;
-    if (slots > 0) { count_launch(); k_surface_best<<<blocks(slots), kBlock, 0, s>>>(sf, slots, sum, keys + 4); }
+void launch_surface_best(Surface sf, int slots, const double* acc, unsigned long long* keys, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_surface_best<<<blocks(slots), kBlock, 0, s>>>(sf, slots, acc, keys); }
 }
-void launch_surface_second(Surface sf, int slots, float sum, int candidate, int bestRatioNode,
-                           unsigned long long* keys, cudaStream_t s) {
-    if (slots > 0) {
-        count_launch();
-        k_surface_second<<<blocks(slots), kBlock, 0, s>>>(sf, slots, sum, candidate, bestRatioNode, keys + 5);
-    }
+void launch_surface_second(Surface sf, int slots, const double* acc, unsigned long long* keys, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_surface_second<<<blocks(slots), kBlock, 0, s>>>(sf, slots, acc, keys); }
 }
 void launch_surface_prefix(Surface sf, int slots, float sum, int upTo, double* acc, cudaStream_t s) {
     if (slots > 0) { count_launch(); k_surface_prefix<<<blocks(slots), kBlock, 0, s>>>(sf, slots, sum, upTo, acc); }
