@@ -173,21 +173,32 @@ __global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int
     rN[i] += s;
 }
 
-// FP64 residual of the V rows written straight into slot order
-__global__ void k_vcg_residual(DevMesh m, VSys v, int slots, double* acc) {
-    double r2 = 0.0;
+// FP64 residual of the V rows written straight into slot order, sum r^2
+// into *acc; with bacc also the squared norm of the Dirichlet part
+// b_i = sum over Dirichlet neighbours c_ij phi_j - q_i into *bacc (k_bnorm's
+// value, from the same pass over the row)
+__global__ void k_vcg_residual(DevMesh m, VSys v, int slots, double* acc, double* bacc) {
+    double r2 = 0.0, b2 = 0.0;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
         const int i = v.node_of[s];
         double r = 0.0;
         if (i >= 0) {
-            double sum = 0.0;
-            for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) sum += m.ceff64[q] * m.phi64[m.col[q]];
+            double sum = 0.0, sb = 0.0;
+            for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+                const int j = m.col[q];
+                const double c = m.ceff64[q] * m.phi64[j];
+                sum += c;
+                if (bacc && (m.flags[j] & F_DIRICHLET)) sb += c;
+            }
             r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
+            const double b = sb - m.q64[i];
+            b2 += b * b;
         }
         v.r[s] = (float)r;
         r2 += r * r;
     }
-    block_sum_atomic<kBlock>(r2, acc);
+    if (bacc) block_sum2_atomic<kBlock>(r2, b2, acc, bacc);
+    else block_sum_atomic<kBlock>(r2, acc);
 }
 
 // Appends the row of a node that has just become a non-Neumann free cell
@@ -301,8 +312,8 @@ void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* r
                                cudaStream_t s) {
     if (count > 0) { count_launch(); k_vcg_couple_neumann<<<blocks(count), kBlock, 0, s>>>(m, v, rows, count, rN); }
 }
-void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_residual<<<reduce_blocks(slots), kBlock, 0, s>>>(m, v, slots, acc); }
+void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, double* bacc, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_residual<<<reduce_blocks(slots), kBlock, 0, s>>>(m, v, slots, acc, bacc); }
 }
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
     if (count > 0) { count_launch(); k_vsys_add_rows<<<1, 32, 0, s>>>(m, v, nodes, count); }

@@ -150,6 +150,13 @@ struct tg_handle {
     };
     Pinned* pin = nullptr;
     int vNext = 0;            // host mirror of the V system's slot counter
+    // the surface normal of an event's candidate runs on its own stream from
+    // snapshots of the cell flags and types, beside the removal and solve
+    cudaStream_t auxStream = nullptr;
+    cudaEvent_t evSnap = nullptr, evNormal = nullptr;
+    DBuf<uint8_t> snapFlags;
+    DBuf<int8_t> snapType;
+    DBuf<float> normalBuf;
     int lastItersJacobi = 16, lastItersAmg = 4;  // iterations of the last inner solves
 
     // multigrid preconditioner of the V system (amg.cu): hierarchy built on
@@ -628,6 +635,9 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     int leastPriority = 0, greatestPriority = 0;
     chk(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
     chk(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatestPriority));
+    chk(cudaStreamCreateWithPriority(&h->auxStream, cudaStreamNonBlocking, greatestPriority));
+    chk(cudaEventCreateWithFlags(&h->evSnap, cudaEventDisableTiming));
+    chk(cudaEventCreateWithFlags(&h->evNormal, cudaEventDisableTiming));
     chk(cudaEventCreate(&h->evStart));
     chk(cudaEventCreate(&h->evStop));
     chk(up(h->xyz, d->xyz, 3 * (size_t)n));
@@ -695,6 +705,9 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
         h->vNext = E0;
     }
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->pin), sizeof(tg_handle::Pinned));
+    chk(h->snapFlags.alloc(n));
+    chk(h->snapType.alloc(n));
+    chk(h->normalBuf.alloc(4));
     chk(h->stageI.alloc(1024));
     chk(h->stageD.alloc(1024));
     chk(h->stageF.alloc(1024));
@@ -736,6 +749,15 @@ void tg_destroy(tg_handle* h) {
     h->amg_release();
     if (h->pin) cudaFreeHost(h->pin);
     h->pin = nullptr;
+    if (h->auxStream) {
+        cudaStreamSynchronize(h->auxStream);
+        cudaStreamDestroy(h->auxStream);
+    }
+    if (h->evSnap) cudaEventDestroy(h->evSnap);
+    if (h->evNormal) cudaEventDestroy(h->evNormal);
+    h->snapFlags.release();
+    h->snapType.release();
+    h->normalBuf.release();
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
@@ -1162,13 +1184,8 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     if (!h || !o) return fail(h, TG_ERR_ARGUMENT, "tg_solve: null argument");
     int rc = TG_OK;
     DevMesh m = h->dm();
-    // ||b||^2 (after removals it changes) is read with the first residual
+    // ||b||^2 (after removals it changes) comes with the first residual
     bool needB = !h->bnormValid;
-    if (needB) {
-        CK(cudaMemsetAsync(h->acc.p + 2, 0, sizeof(double), h->stream));
-        launch_bnorm(m, h->allV.p, h->countAllV, h->acc.p + 2, h->stream);
-        launch_bnorm(m, h->allN.p, h->countAllN, h->acc.p + 2, h->stream);
-    }
     VSys vsys = h->vs();
     CGVectors vN = h->cg(1);
     tg_solve_info inf{};
@@ -1199,9 +1216,9 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         if (rc != TG_OK) return rc;
     }
     for (int outer = 0;; outer++) {
-        CK(cudaMemsetAsync(h->acc.p, 0, 2 * sizeof(double), h->stream));
-        launch_vcg_residual(m, vsys, h->vActive, h->acc.p, h->stream);
-        launch_residual(m, h->allN.p, h->countAllN, vN.r, h->acc.p + 1, h->stream);
+        CK(cudaMemsetAsync(h->acc.p, 0, 3 * sizeof(double), h->stream));
+        launch_vcg_residual(m, vsys, h->vActive, h->acc.p, needB ? h->acc.p + 2 : nullptr, h->stream);
+        launch_residual(m, h->allN.p, h->countAllN, vN.r, h->acc.p + 1, h->stream, needB ? h->acc.p + 2 : nullptr);
         double* r2 = h->pin->r2;
         CK(cudaMemcpyAsync(r2, h->acc.p, sizeof(double) * (needB ? 3 : 2), cudaMemcpyDeviceToHost, h->stream));
         rc = sync_status(h, "tg_solve residual");
@@ -1810,9 +1827,19 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
     CK(cudaMemcpyAsync(&pin->before[1], h->stageD.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     for (int k = 0; k < 3; k++) rec->apex[k] = sel.apex >= 0 ? h->h_xyz[3 * (size_t)sel.apex + k] : 0.0f;
     if (o->normal_enabled) {
-        // the candidate is a surface cell by construction
-        launch_surface_normal(h->dm(), h->sf(), node, h->vacuumId, h->stageF.p, h->stream);
-        CK(cudaMemcpyAsync(pin->normal, h->stageF.p, 3 * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        // the candidate is a surface cell by construction; the normal reads
+        // the flags and types as they are before the removal, from copies,
+        // on the auxiliary stream while the removal and the solve go on
+        CK(cudaMemcpyAsync(h->snapFlags.p, h->flags.p, h->n, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->snapType.p, h->type.p, h->n, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaEventRecord(h->evSnap, h->stream));
+        CK(cudaStreamWaitEvent(h->auxStream, h->evSnap, 0));
+        DevMesh ms = h->dm();
+        ms.flags = h->snapFlags.p;
+        ms.type = h->snapType.p;
+        launch_surface_normal(ms, h->sf(), node, h->vacuumId, h->normalBuf.p, h->auxStream);
+        CK(cudaMemcpyAsync(pin->normal, h->normalBuf.p, 3 * sizeof(float), cudaMemcpyDeviceToHost, h->auxStream));
+        CK(cudaEventRecord(h->evNormal, h->auxStream));
     }
     const tg_type removed = h->types[h->h_type[node]];
     // II) removal
@@ -1932,6 +1959,7 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
     launch_field_o1(h->dm(), h->stageI.p + 512, 1, h->stageD.p + 4, h->stream);
     CK(cudaMemcpyAsync(&pin->after[0], h->phi64.p + node, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(&pin->after[1], h->stageD.p + 4, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (o->normal_enabled) CK(cudaStreamWaitEvent(h->stream, h->evNormal, 0));
     rc = sync_status(h, "tg_run_event");
     if (rc != TG_OK) return rc;
     rec->phi_before = (float)pin->before[0];

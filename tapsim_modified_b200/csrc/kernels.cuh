@@ -125,7 +125,8 @@ void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, c
 void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s);
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
                                cudaStream_t s);
-void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, cudaStream_t s);
+// FP64 residual of the V rows; with bacc, also ||b||^2 of those rows
+void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, double* bacc, cudaStream_t s);
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
 
 // ---- relaxation (relax.cu) ----
@@ -133,7 +134,10 @@ void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes,
 void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* maxdev, cudaStream_t s);
 // r_i (FP64) for a row list; accumulates sum r^2 into *acc; optionally
 // stores r as float into r32
-void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s);
+// with bacc, also the squared norm of the rows' Dirichlet part (as
+// launch_bnorm) into *bacc
+void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s,
+                     double* bacc = nullptr);
 // b_i = sum over Dirichlet neighbours c_ij phi_j - q_i; sum b^2 into *acc
 void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s);
 // FP32 conjugate gradients on the rows of one list (Jacobi preconditioner)

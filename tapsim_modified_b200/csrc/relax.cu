@@ -47,18 +47,28 @@ __global__ void k_sweep64(DevMesh m, const int32_t* __restrict__ rows, int count
     }
 }
 
-__global__ void k_residual(DevMesh m, const int32_t* __restrict__ rows, int count, float* r32, double* acc) {
+// with bacc, also the squared norm of the rows' Dirichlet part (k_bnorm's
+// value) from the same pass
+__global__ void k_residual(DevMesh m, const int32_t* __restrict__ rows, int count, float* r32, double* acc,
+                           double* bacc) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double r = 0.0;
+    double r = 0.0, b = 0.0;
     if (t < count) {
         const int i = rows[t];
         const int q0 = m.row_ptr[i], q1 = m.row_ptr[i + 1];
-        double s = 0.0;
-        for (int q = q0; q < q1; q++) s += m.ceff64[q] * m.phi64[m.col[q]];
+        double s = 0.0, sb = 0.0;
+        for (int q = q0; q < q1; q++) {
+            const int j = m.col[q];
+            const double c = m.ceff64[q] * m.phi64[j];
+            s += c;
+            if (bacc && (m.flags[j] & F_DIRICHLET)) sb += c;
+        }
         r = s - m.diag64[i] * m.phi64[i] - m.q64[i];
+        b = sb - m.q64[i];
         if (r32) r32[i] = (float)r;
     }
-    block_sum_atomic<kBlock>(r * r, acc);
+    if (bacc) block_sum2_atomic<kBlock>(r * r, b * b, acc, bacc);
+    else block_sum_atomic<kBlock>(r * r, acc);
 }
 
 __global__ void k_bnorm(DevMesh m, const int32_t* __restrict__ rows, int count, double* acc) {
@@ -271,8 +281,9 @@ inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* maxdev, cudaStream_t s) {
     if (count > 0) { count_launch(); k_sweep64<<<blocks(count), kBlock, 0, s>>>(m, rows, count, maxdev); }
 }
-void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s) {
-    if (count > 0) { count_launch(); k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, acc); }
+void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s,
+                     double* bacc) {
+    if (count > 0) { count_launch(); k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, acc, bacc); }
 }
 void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s) {
     if (count > 0) { count_launch(); k_bnorm<<<blocks(count), kBlock, 0, s>>>(m, rows, count, acc); }
