@@ -401,7 +401,9 @@ int tg_timer_stop(tg_handle* h, float* elapsed_ms);
 int64_t tg_launch_count(const tg_handle* h);
 /* Times `iters` back-to-back launches of one hot kernel on the handle's
  * stream with CUDA events: 0 = FP32 CG SpMV over the non-Neumann free rows,
- * 1 = FP64 residual over all free rows.  Reports the mean duration of one
+ * 1 = FP64 residual over all free rows, 2 = the multigrid's level-0
+ * smoothing pass t = b - A y (after a multigrid solve has built the
+ * hierarchy).  Reports the mean duration of one
  * launch and the algorithmic bytes one launch moves (CSR rows, coupling and
  * neighbour-index streams, one compulsory read of every gathered vector
  * entry, the row outputs). */

@@ -154,6 +154,12 @@ inline int grid_for(long long threads) {
 
 }  // namespace
 
+void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s) {
+    const int slices = (slots + 31) / 32;
+    count_launch();
+    k_amg_fine<<<grid_full((long long)slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, g.t0, 0, v.scal, 0, -1.0);
+}
+
 void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s) {
     const double* scal = v.scal;
     // level 0: b = r, output u

@@ -266,6 +266,29 @@ __global__ void k_vsys_add_rows(DevMesh m, VSys v, const int32_t* nodes, int cou
     for (int k = 0; k < count; k++) vsys_add_row(m, v, nodes[k]);
 }
 
+// After a flip has resynced the couplings of cell i (flip_and_resync), the
+// V system's copies of them: i's own row when it has one, the entries of
+// its V neighbours that point at it, and those rows' diagonals.  One warp
+// per cell.
+__global__ void k_vsys_refresh(DevMesh m, VSys v, const int32_t* nodes, int count) {
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k < count; k++) {
+        const int i = nodes[k];
+        const int si = v.slot_of[i];
+        if (si >= 0 && lane == 0) v.d[si] = m.diag32[i];
+        for (int q = m.row_ptr[i] + lane; q < m.row_ptr[i + 1]; q += 32) {
+            if (si >= 0 && v.vpos[q] >= 0) v.val[v.vpos[q]] = m.ceff32[q];
+            const int j = m.col[q];
+            const int sj = v.slot_of[j];
+            if (sj < 0) continue;
+            const int p = v.vpos[m.rev[q]];
+            if (p >= 0) v.val[p] = m.ceff32[m.rev[q]];
+            v.d[sj] = m.diag32[j];
+        }
+        __syncwarp();
+    }
+}
+
 inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 
 // Pointwise kernels that end in a global reduction loop over their rows
@@ -317,6 +340,9 @@ void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc
 }
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
     if (count > 0) { count_launch(); k_vsys_add_rows<<<1, 32, 0, s>>>(m, v, nodes, count); }
+}
+void launch_vsys_refresh(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
+    if (count > 0) { count_launch(); k_vsys_refresh<<<1, 32, 0, s>>>(m, v, nodes, count); }
 }
 
 }  // namespace tgd

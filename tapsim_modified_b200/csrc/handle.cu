@@ -831,6 +831,19 @@ int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, d
             launch_residual(m, h->allN.p, h->countAllN, nullptr, h->acc.p, h->stream);
         }
         CK(cudaEventRecord(h->evStop, h->stream));
+    } else if (which == 2) {
+        // k_amg_fine (the multigrid's level-0 smoothing pass, t = b - A y
+        // over SELL-32): col + val per stored entry, and per row b, y (the
+        // gathers hit the same vector), d and the t write
+        if (!h->amgReady) return fail(h, TG_ERR_ARGUMENT, "tg_bench_kernel: no multigrid hierarchy yet");
+        const double rows = (double)h->vActive, stored = h->vEntries;
+        *bytes = rows * (4 + 4 + 4 + 4) + stored * (4 + 4);
+        if (h->vScal.n < 8) CK(h->vScal.alloc(8));
+        VSys v = h->vs();
+        launch_amg_fine_residual(v, h->vActive, h->amg, h->stream);  // warm
+        CK(cudaEventRecord(h->evStart, h->stream));
+        for (int k = 0; k < iters; k++) launch_amg_fine_residual(v, h->vActive, h->amg, h->stream);
+        CK(cudaEventRecord(h->evStop, h->stream));
     } else {
         return fail(h, TG_ERR_ARGUMENT, "tg_bench_kernel: unknown kernel");
     }
@@ -1634,6 +1647,16 @@ static int take_away_impl(tg_handle* h, int32_t node, int32_t capacity, int32_t*
         launch_vsys_add_rows(h->dm(), h->vs(), h->stageI.p, nf, h->stream);
         h->vNext += nf;
         h->vActive = (h->vNext + 31) / 32 * 32;
+    }
+    // cells that were free already (a removed non-Dirichlet species) keep
+    // their rows, whose couplings the flip has changed
+    if (nf < 1 + nd) {
+        pin->flipped[512] = node;
+        for (int k = 0; k < nd && k + 1 < cap; k++) pin->flipped[513 + k] = pin->result[1 + k];
+        const int nr = 1 + std::min(nd, cap - 1);
+        CK(cudaMemcpyAsync(h->stageI.p + 256, pin->flipped + 512, sizeof(int32_t) * nr, cudaMemcpyHostToDevice,
+                           h->stream));
+        launch_vsys_refresh(h->dm(), h->vs(), h->stageI.p + 256, nr, h->stream);
     }
     h->bnormValid = false;
     h->selValid = false;

@@ -117,6 +117,8 @@ struct AmgDev {
     float *y0, *t0;                         // level-0 work vectors (capacity + 1)
     const float* coarse_inv;                // dense inverse of the coarsest operator, row-major
 };
+// the level-0 smoothing pass t = b - A y alone (timing hook)
+void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s);
 // u = M^-1 r, one V(1,1)-cycle, for CG iteration `it`
 void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s);
 // phi64 += x on the V rows; with record, hist += x as well
@@ -128,6 +130,9 @@ void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* r
 // FP64 residual of the V rows; with bacc, also ||b||^2 of those rows
 void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, double* bacc, cudaStream_t s);
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
+// re-copies the couplings and diagonals that flips of the listed cells
+// changed into the V system (rows that existed before the flips)
+void launch_vsys_refresh(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
 
 // ---- relaxation (relax.cu) ----
 // coloured Gauss-Seidel sweep of one row list, FP64, max |delta| to *maxdev
