@@ -37,7 +37,7 @@ struct AmgHierarchy {
 struct AmgOptions {
     double theta = 0.08;       // strength threshold on the finest level
     double theta_coarse = 0.0; // and on the coarser ones, whose Galerkin rows spread over more entries
-    double omega = 2.0 / 3.0;  // prolongator smoothing weight (4/3 over rho(D^-1 A) <= 2)
+    double omega = 0.8;        // prolongator smoothing weight, 4/3 over rho(D_F^-1 A_F) for rho ~ 1.7
     int max_coarse = 1000;     // rows at which coarsening stops
     int max_levels = 12;
     int threads = 0;           // 0: hardware concurrency
