@@ -158,6 +158,7 @@ struct tg_handle {
     DBuf<int8_t> snapType;
     DBuf<float> normalBuf;
     int lastItersJacobi = 16, lastItersAmg = 4;  // iterations of the last inner solves
+    int lastItersCgV = 16, lastItersCgN = 16;
 
     // multigrid preconditioner of the V system (amg.cu): hierarchy built on
     // the host from the V system as it is, uploaded as CSR levels
@@ -984,7 +985,11 @@ int tg_residual(tg_handle* h, double* rel) {
 
 // FP32 conjugate gradients on one row list until r.z falls below
 // rtol^2 of its start value or maxIter is reached; returns iterations.
-static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, double rtol, int maxIter, int* itersOut) {
+// absTarget2: a floor under the target of r.r (0: none), for a system whose
+// part of the global residual only has to fall below a share of the outer
+// tolerance
+static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, double rtol, int maxIter, int* itersOut,
+                  double absTarget2 = 0.0) {
     DevMesh m = h->dm();
     CGVectors v = h->cg(which);
     DBuf<double>& scal = which == 0 ? h->scalV : h->scalN;
@@ -1000,11 +1005,14 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     double rr0 = 0.0;
     CK(cudaMemcpyAsync(&rr0, scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    const double target = rr0 * rtol * rtol;
+    const double target = std::max(rr0 * rtol * rtol, absTarget2);
     int it = 0;
-    const int batch = 16;
-    double sb[3 * batch];
-    while (it < maxIter && rr0 > 0.0) {
+    // iterations queued before the first read: one more than the last solve
+    // of this system took, then small batches
+    int& last = which == 0 ? h->lastItersCgV : h->lastItersCgN;
+    int batch = std::min(16, std::max(2, last + 1));
+    double sb[3 * 16];
+    while (it < maxIter && rr0 > target) {
         const int start = it;
         const int end = std::min(maxIter, it + batch);
         for (; it < end; it++) launch_cg_iter(m, rows, count, v, it, target, h->stream);
@@ -1020,7 +1028,9 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
                 done = true;
             }
         if (done) break;
+        batch = 4;
     }
+    last = it;
     *itersOut = it;
     return TG_OK;
 }
@@ -1261,7 +1271,11 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         }
         if (h->countAllN > 0) {
             launch_vcg_couple_neumann(m, vsys, h->allN.p, h->countAllN, vN.r, h->stream);
-            rc = run_cg(h, 1, h->allN.p, h->countAllN, rtol, o->max_inner, &itN);
+            // the Neumann rows' share of the global residual only has to fall
+            // below 0.3 of the outer tolerance (the V rows' solve brings
+            // theirs to about the same), whatever their own start
+            const double floorN = 0.3 * o->rel_tol;
+            rc = run_cg(h, 1, h->allN.p, h->countAllN, rtol, o->max_inner, &itN, floorN * floorN * h->bnorm2);
             if (rc != TG_OK) return rc;
         }
         inf.inner += itV + itN;
