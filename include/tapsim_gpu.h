@@ -447,6 +447,47 @@ int tg_mesh_write_dump(const tg_mesh* m, const char* path, const float* phi);
  * for a generated tip.  numbers_out: [N]. */
 int tg_mesh_numbers(const tg_mesh* m, uint32_t* numbers_out);
 
+/* ---- results and trajectory files: File_Io::LogResults / LogTrajectory -- */
+/* One results row, LogResults::Dataset (logResults.h:41-66). */
+typedef struct {
+    uint32_t index;
+    int32_t id;                 /* written as short */
+    uint32_t number;
+    float voltage;
+    float start[3], stop[3];
+    float tof;
+    float probability;
+    float potential_before, field_before[3];
+    float potential_after, field_after[3];
+    float normal[3], apex[3];
+} tg_result_row;
+/* Writes results files in LogResults' layout (logResults.cpp:135-381), ASCII
+ * or binary.  With chunk_size > 0 the rows go to files path.%08u named after
+ * the index of the row opening each chunk (a new chunk when index %
+ * chunk_size == 0), the header text only in the first, as the reference's
+ * writer thread does; otherwise to path.  header: extra header lines (may
+ * be NULL). */
+int tg_results_write(const char* path, int32_t binary, const char* header, int32_t count, const tg_result_row* rows,
+                     int32_t chunk_size);
+/* One trajectory, as LogTrajectory::push receives it
+ * (logTrajectory.cpp:104-135): the points' times are written as given
+ * (the caller multiplies by the time scale, as the writer thread does). */
+typedef struct {
+    uint32_t index;
+    uint32_t number;
+    float time_scale;
+    int32_t status;             /* TG_TRAJ_* */
+    float charge, mass;         /* [C], [kg] */
+    int32_t num_points;
+    const tg_path_point* points;
+    float error[6];             /* error estimate: position x, y, z, velocity x, y, z */
+} tg_trajectory_item;
+/* Writes trajectory files in LogTrajectory's layout
+ * (logTrajectory.cpp:137-300), chunked as tg_results_write with the header
+ * in every file. */
+int tg_trajectory_write(const char* path, int32_t binary, int32_t count, const tg_trajectory_item* items,
+                        int32_t chunk_size);
+
 /* ---- grid and surface snapshots: File_Io::LogGrid / LogSurface ---------- */
 /* Writes one grid snapshot file in LogGrid's layout (logGrid.cpp:197-245):
  * for each of n cells the type id, unique number, potential, field [3] and

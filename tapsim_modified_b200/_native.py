@@ -69,6 +69,19 @@ class tg_path_point(C.Structure):
     _fields_ = [("time", C.c_float), ("position", C.c_float * 3), ("velocity", C.c_float * 3), ("tet", C.c_int32)]
 
 
+class tg_result_row(C.Structure):
+    _fields_ = [("index", C.c_uint32), ("id", C.c_int32), ("number", C.c_uint32), ("voltage", C.c_float),
+                ("start", C.c_float * 3), ("stop", C.c_float * 3), ("tof", C.c_float), ("probability", C.c_float),
+                ("potential_before", C.c_float), ("field_before", C.c_float * 3), ("potential_after", C.c_float),
+                ("field_after", C.c_float * 3), ("normal", C.c_float * 3), ("apex", C.c_float * 3)]
+
+
+class tg_trajectory_item(C.Structure):
+    _fields_ = [("index", C.c_uint32), ("number", C.c_uint32), ("time_scale", C.c_float), ("status", C.c_int32),
+                ("charge", C.c_float), ("mass", C.c_float), ("num_points", C.c_int32), ("points", C.c_void_p),
+                ("error", C.c_float * 6)]
+
+
 # tg_path_point as a numpy record (the same 32 bytes)
 PATH_POINT = np.dtype([("time", "<f4"), ("position", "<f4", 3), ("velocity", "<f4", 3), ("tet", "<i4")])
 
@@ -138,6 +151,8 @@ SIGNATURES = {
     "tg_log_surface": (C.c_int, [_P, C.c_char_p, _I, _I, _I, _I, C.c_float, _P]),
     "tg_mesh_numbers": (C.c_int, [_P, _P]),
     "tg_grid_log_write": (C.c_int, [C.c_char_p, _I, _I, _P, _P, _P, _P, _P]),
+    "tg_results_write": (C.c_int, [C.c_char_p, _I, C.c_char_p, _I, _P, _I]),
+    "tg_trajectory_write": (C.c_int, [C.c_char_p, _I, _I, _P, _I]),
     "tg_surface_log_write": (C.c_int, [C.c_char_p, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P]),
     "tg_potential_at": (C.c_int, [_P, _I, _P, _P, _P]),
     "tg_run_event": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, C.POINTER(tg_event_record)]),

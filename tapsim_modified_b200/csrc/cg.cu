@@ -173,28 +173,28 @@ __global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int
     rN[i] += s;
 }
 
-// FP64 residual of the V rows written straight into slot order, sum r^2
-// into *acc; with bacc also the squared norm of the Dirichlet part
-// b_i = sum over Dirichlet neighbours c_ij phi_j - q_i into *bacc (k_bnorm's
-// value, from the same pass over the row)
-__global__ void k_vcg_residual(DevMesh m, VSys v, int slots, double* acc, double* bacc) {
+// FP64 residual of the V rows, sum r^2 into *acc; with bacc also the
+// squared norm of the Dirichlet part b_i = sum over Dirichlet neighbours
+// c_ij phi_j - q_i into *bacc (k_bnorm's value, from the same pass over the
+// row).  The rows are walked in node order (the compact list, whose CSR rows
+// neighbouring threads then read from neighbouring memory) and each result
+// is written to its slot; padding slots keep r = 0.
+__global__ void k_vcg_residual(DevMesh m, VSys v, const int32_t* __restrict__ rows, int count, double* acc,
+                               double* bacc) {
     double r2 = 0.0, b2 = 0.0;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
-        const int i = v.node_of[s];
-        double r = 0.0;
-        if (i >= 0) {
-            double sum = 0.0, sb = 0.0;
-            for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
-                const int j = m.col[q];
-                const double c = m.ceff64[q] * m.phi64[j];
-                sum += c;
-                if (bacc && (m.flags[j] & F_DIRICHLET)) sb += c;
-            }
-            r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
-            const double b = sb - m.q64[i];
-            b2 += b * b;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const int i = rows[t];
+        double sum = 0.0, sb = 0.0;
+        for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+            const int j = m.col[q];
+            const double c = m.ceff64[q] * m.phi64[j];
+            sum += c;
+            if (bacc && (m.flags[j] & F_DIRICHLET)) sb += c;
         }
-        v.r[s] = (float)r;
+        const double r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
+        const double b = sb - m.q64[i];
+        b2 += b * b;
+        v.r[v.slot_of[i]] = (float)r;
         r2 += r * r;
     }
     if (bacc) block_sum2_atomic<kBlock>(r2, b2, acc, bacc);
@@ -335,8 +335,12 @@ void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* r
                                cudaStream_t s) {
     if (count > 0) { count_launch(); k_vcg_couple_neumann<<<blocks(count), kBlock, 0, s>>>(m, v, rows, count, rN); }
 }
-void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, double* bacc, cudaStream_t s) {
-    if (slots > 0) { count_launch(); k_vcg_residual<<<reduce_blocks(slots), kBlock, 0, s>>>(m, v, slots, acc, bacc); }
+void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, int count, double* acc, double* bacc,
+                         cudaStream_t s) {
+    if (count > 0) {
+        count_launch();
+        k_vcg_residual<<<reduce_blocks(count), kBlock, 0, s>>>(m, v, rows, count, acc, bacc);
+    }
 }
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
     if (count > 0) { count_launch(); k_vsys_add_rows<<<1, 32, 0, s>>>(m, v, nodes, count); }

@@ -67,6 +67,9 @@ struct tg_handle {
     float top_z = 0.0f;
     double snap = 1.0;
     std::vector<tg_type> types;          // by id, id < 0 means absent
+    // update_coordination only changes cells whose id is >= 10; without such
+    // a type in the table no cell ever has one
+    bool coordinationActive = false;
     std::vector<int32_t> segStart;       // host mirror
     std::vector<int32_t> countV, countN;  // host mirrors
     int32_t countAllV = 0, countAllN = 0;
@@ -422,6 +425,7 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
             return fail(nullptr, TG_ERR_ARGUMENT, "tg_create: type id out of range");
         }
         h->types[t.id] = t;
+        if (t.id >= 10) h->coordinationActive = true;
     }
     // every index the device walks and gathers through must stay inside its
     // array: vertices in [0, N), neighbours and node_tet in [-1, T)
@@ -1240,7 +1244,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     }
     for (int outer = 0;; outer++) {
         CK(cudaMemsetAsync(h->acc.p, 0, 3 * sizeof(double), h->stream));
-        launch_vcg_residual(m, vsys, h->vActive, h->acc.p, needB ? h->acc.p + 2 : nullptr, h->stream);
+        launch_vcg_residual(m, vsys, h->allV.p, h->countAllV, h->acc.p, needB ? h->acc.p + 2 : nullptr, h->stream);
         launch_residual(m, h->allN.p, h->countAllN, vN.r, h->acc.p + 1, h->stream, needB ? h->acc.p + 2 : nullptr);
         double* r2 = h->pin->r2;
         CK(cudaMemcpyAsync(r2, h->acc.p, sizeof(double) * (needB ? 3 : 2), cudaMemcpyDeviceToHost, h->stream));
@@ -1884,7 +1888,7 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
     rc = take_away_impl(h, node, 0, nullptr, &nd);
     if (rc != TG_OK) return rc;
     rec->detached = nd;
-    launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
+    if (h->coordinationActive) launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
     // III) relaxation
     if (o->relax_mode == 0) {
         int64_t it = 0;

@@ -470,10 +470,16 @@ std::string write_dump(const std::string& path, const Dump& d) {
     return f.good() ? std::string() : "dump: write error";
 }
 
-std::string write_results(const std::string& path, const std::vector<ResultRecord>& recs, bool binary,
-                          const std::string& header) {
-    std::ofstream f(path, std::ios::binary | std::ios::trunc);
-    if (!f.good()) return "results: cannot write " + path;
+namespace {
+
+// File name of a chunk: path.%08u after the index that opens it.
+std::string chunk_name(const std::string& path, uint32_t index) {
+    char suffix[16];
+    snprintf(suffix, sizeof(suffix), ".%08u", index);
+    return path + suffix;
+}
+
+void results_header(std::ostream& f, bool binary, const std::string& header) {
     static const char* fields[] = {"index [1]", "id [1]", "number [1]", "voltage [V]", "startX [m]", "startY [m]",
                                    "startZ [m]", "stopX [m]", "stopY [m]", "stopZ [m]", "tof [s]",
                                    "probability [1]", "potentialBefore [V]", "fieldBeforeX [V/m]",
@@ -496,22 +502,41 @@ std::string write_results(const std::string& path, const std::vector<ResultRecor
         }
     }
     f << (binary ? "BINARY\n" : "ASCII\n");
-    for (const ResultRecord& r : recs) {
+}
+
+}  // namespace
+
+std::string write_results(const std::string& path, const std::vector<ResultRecord>& recs, bool binary,
+                          const std::string& header, int chunk) {
+    std::ofstream f;
+    auto open = [&](const std::string& name, bool first) {
+        if (f.is_open()) f.close();
+        f.open(name, std::ios::binary | std::ios::trunc);
+        if (f.good()) results_header(f, binary, first ? header : std::string());
+        return f.good();
+    };
+    if (recs.empty() && !open(path, true)) return "results: cannot write " + path;
+    for (size_t k = 0; k < recs.size(); k++) {
+        const ResultRecord& r = recs[k];
+        if (k == 0 || (chunk > 0 && r.index % (uint32_t)chunk == 0)) {
+            const std::string name = chunk > 0 ? chunk_name(path, r.index) : path;
+            if (!open(name, k == 0)) return "results: cannot write " + name;
+        }
         if (binary) {
             wr(f, r.index);
             wr(f, r.id);
             wr(f, r.number);
             wr(f, r.voltage);
-            for (int k = 0; k < 3; k++) wr(f, r.start[k]);
-            for (int k = 0; k < 3; k++) wr(f, r.stop[k]);
+            for (int j = 0; j < 3; j++) wr(f, r.start[j]);
+            for (int j = 0; j < 3; j++) wr(f, r.stop[j]);
             wr(f, r.tof);
             wr(f, r.probability);
             wr(f, r.phi_before);
-            for (int k = 0; k < 3; k++) wr(f, r.field_before[k]);
+            for (int j = 0; j < 3; j++) wr(f, r.field_before[j]);
             wr(f, r.phi_after);
-            for (int k = 0; k < 3; k++) wr(f, r.field_after[k]);
-            for (int k = 0; k < 3; k++) wr(f, r.normal[k]);
-            for (int k = 0; k < 3; k++) wr(f, r.apex[k]);
+            for (int j = 0; j < 3; j++) wr(f, r.field_after[j]);
+            for (int j = 0; j < 3; j++) wr(f, r.normal[j]);
+            for (int j = 0; j < 3; j++) wr(f, r.apex[j]);
         } else {
             char buf[1024];
             int len = snprintf(buf, sizeof(buf),
@@ -524,6 +549,78 @@ std::string write_results(const std::string& path, const std::vector<ResultRecor
         }
     }
     return f.good() ? std::string() : "results: write error";
+}
+
+namespace {
+
+void trajectory_header(std::ostream& f, bool binary) {
+    static const char* cols[] = {"time [s]", "positionX [m]", "positionY [m]", "positionZ [m]", "velocityX [m/s]",
+                                 "velocityY [m/s]", "velocityZ [m/s]", "tetrahedron [1]"};
+    f << "TAPSIM TRAJECTORY DATA\nVERSION 1.0\n";
+    for (int k = 0; k < 8; k++) {
+        f << "# " << cols[k];
+        if (binary) f << (k == 7 ? " (int)" : " (float)");
+        f << '\n';
+    }
+    f << '\n';
+}
+
+const char* status_name(int s) {
+    switch (s) {
+        case 0: return "NO_INTEGRATION";
+        case 1: return "NO_FIELD";
+        case 2: return "STEPPER_LIMIT_PASSED";
+        case 3: return "ITERATION_LIMIT_PASSED";
+        case 4: return "GEOMETRY_LIMIT_PASSED";
+        case 5: return "SYSTEM_LIMIT_PASSED";
+        default: return "INVALID";
+    }
+}
+
+}  // namespace
+
+std::string write_trajectories(const std::string& path, const std::vector<TrajectoryRecord>& recs, bool binary,
+                               int chunk) {
+    std::ofstream f;
+    auto open = [&](const std::string& name) {
+        if (f.is_open()) f.close();
+        f.open(name, std::ios::binary | std::ios::trunc);
+        if (f.good()) trajectory_header(f, binary);
+        return f.good();
+    };
+    if (recs.empty() && !open(path)) return "trajectories: cannot write " + path;
+    char line[512];
+    for (size_t k = 0; k < recs.size(); k++) {
+        const TrajectoryRecord& t = recs[k];
+        if (k == 0 || (chunk > 0 && t.index % (uint32_t)chunk == 0)) {
+            const std::string name = chunk > 0 ? chunk_name(path, t.index) : path;
+            if (!open(name)) return "trajectories: cannot write " + name;
+        }
+        int len = snprintf(line, sizeof(line),
+                           "# index = %u\n# unique number = %u\n# time scale = %e\n# integrator status = %d => %s\n"
+                           "# charge [C] / mass [kg] = %e / %e\n%s %d\n",
+                           t.index, t.number, t.time_scale, t.status, status_name(t.status), t.charge, t.mass,
+                           binary ? "BINARY" : "ASCII", t.num_points);
+        f.write(line, len);
+        if (binary) {
+            f.write(reinterpret_cast<const char*>(t.points), 32 * (std::streamsize)t.num_points);
+            f << '\n';
+        } else {
+            for (int p = 0; p < t.num_points; p++) {
+                const float* q = t.points + 8 * (size_t)p;
+                int32_t tet;
+                std::memcpy(&tet, q + 7, sizeof(tet));
+                len = snprintf(line, sizeof(line), "%e\t%e\t%e\t%e\t%e\t%e\t%e\t%d\n", q[0], q[1], q[2], q[3], q[4],
+                               q[5], q[6], tet);
+                f.write(line, len);
+            }
+        }
+        len = snprintf(line, sizeof(line),
+                       "# final error estimate (position) = (%e/%e/%e)\n# final error estimate (velocity) = (%e/%e/%e)\n\n",
+                       t.error[0], t.error[1], t.error[2], t.error[3], t.error[4], t.error[5]);
+        f.write(line, len);
+    }
+    return f.good() ? std::string() : "trajectories: write error";
 }
 
 std::string write_grid_log(const std::string& path, bool binary, const GridLog& g) {

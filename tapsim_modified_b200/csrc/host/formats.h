@@ -92,8 +92,24 @@ struct ResultRecord {
     float normal[3], apex[3];
 };
 
+// Results files; with chunk > 0 split as LogResults' writer thread does
+// (path.%08u after the index opening each chunk, the header text in the
+// first file only).
 std::string write_results(const std::string& path, const std::vector<ResultRecord>& recs, bool binary,
-                          const std::string& header);
+                          const std::string& header, int chunk = 0);
+
+// One trajectory of the trajectory log (LogTrajectory::Dataset).
+struct TrajectoryRecord {
+    uint32_t index, number;
+    float time_scale;
+    int32_t status;
+    float charge, mass;
+    int32_t num_points;
+    const float* points;  // 8 words a point: time, position, velocity, tetrahedron bits
+    float error[6];
+};
+std::string write_trajectories(const std::string& path, const std::vector<TrajectoryRecord>& recs, bool binary,
+                               int chunk = 0);
 
 // One grid snapshot as File_Io::LogGrid writes it (logGrid.cpp:197-245):
 // per cell the type id, unique number, potential, field_o1 [3] and

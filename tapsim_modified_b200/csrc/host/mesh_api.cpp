@@ -354,6 +354,56 @@ int tg_mesh_numbers(const tg_mesh* m, uint32_t* out) {
     return TG_OK;
 }
 
+int tg_results_write(const char* path, int32_t binary, const char* header, int32_t count, const tg_result_row* rows,
+                     int32_t chunk) {
+    if (!path || count < 0 || (count && !rows) || chunk < 0) return mesh_fail("tg_results_write: bad argument");
+    std::vector<ResultRecord> recs(count);
+    for (int32_t k = 0; k < count; k++) {
+        const tg_result_row& a = rows[k];
+        ResultRecord& r = recs[k];
+        r.index = a.index;
+        r.id = (short)a.id;
+        r.number = a.number;
+        r.voltage = a.voltage;
+        for (int j = 0; j < 3; j++) {
+            r.start[j] = a.start[j];
+            r.stop[j] = a.stop[j];
+            r.field_before[j] = a.field_before[j];
+            r.field_after[j] = a.field_after[j];
+            r.normal[j] = a.normal[j];
+            r.apex[j] = a.apex[j];
+        }
+        r.tof = a.tof;
+        r.probability = a.probability;
+        r.phi_before = a.potential_before;
+        r.phi_after = a.potential_after;
+    }
+    const std::string err = write_results(path, recs, binary != 0, header ? header : "", chunk);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
+int tg_trajectory_write(const char* path, int32_t binary, int32_t count, const tg_trajectory_item* items,
+                        int32_t chunk) {
+    if (!path || count < 0 || (count && !items) || chunk < 0) return mesh_fail("tg_trajectory_write: bad argument");
+    std::vector<TrajectoryRecord> recs(count);
+    for (int32_t k = 0; k < count; k++) {
+        const tg_trajectory_item& a = items[k];
+        if (a.num_points < 0 || (a.num_points && !a.points)) return mesh_fail("tg_trajectory_write: bad points");
+        TrajectoryRecord& t = recs[k];
+        t.index = a.index;
+        t.number = a.number;
+        t.time_scale = a.time_scale;
+        t.status = a.status;
+        t.charge = a.charge;
+        t.mass = a.mass;
+        t.num_points = a.num_points;
+        t.points = reinterpret_cast<const float*>(a.points);
+        for (int j = 0; j < 6; j++) t.error[j] = a.error[j];
+    }
+    const std::string err = write_trajectories(path, recs, binary != 0, chunk);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
 int tg_grid_log_write(const char* path, int32_t binary, int32_t n, const int32_t* id, const uint32_t* number,
                       const float* phi, const float* field, const float* force) {
     if (!path || n < 0 || (n && (!id || !number || !phi || !field || !force)))

@@ -127,8 +127,10 @@ void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, c
 void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s);
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
                                cudaStream_t s);
-// FP64 residual of the V rows; with bacc, also ||b||^2 of those rows
-void launch_vcg_residual(const DevMesh& m, const VSys& v, int slots, double* acc, double* bacc, cudaStream_t s);
+// FP64 residual of the V rows (rows: their compact list, in node order)
+// into the V system's r; with bacc, also ||b||^2 of those rows
+void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, int count, double* acc, double* bacc,
+                         cudaStream_t s);
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
 // re-copies the couplings and diagonals that flips of the listed cells
 // changed into the V system (rows that existed before the flips)

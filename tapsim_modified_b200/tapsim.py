@@ -700,65 +700,36 @@ class Evaporation:
                                       "path_error": path[1].copy()})
 
 
-_RESULT_UNITS = ["[1]", "[1]", "[1]", "[V]"] + ["[m]"] * 6 + ["[s]", "[1]"] + \
-    ["[V]", "[V/m]", "[V/m]", "[V/m]"] * 2 + ["[m]"] * 6
-_RESULT_TYPES = ["int", "int", "unsigned int"] + ["float"] * 23
-
-
-def _results_header(binary: bool, header: str) -> bytes:
-    """LogResults::writeHeader (logResults.cpp:135-225)."""
-    out = ["TAPSIM RESULTS DATA\nVERSION 1.0\n", header]
-    for k, name in enumerate(RESULT_FIELDS):
-        u = _RESULT_UNITS[k]
-        if binary:
-            if name.startswith("potential"):
-                u = "[1]"
-            out.append(f"# {name} {u} ({_RESULT_TYPES[k]})\n")
-        else:
-            out.append(f"# {name} {u}\n")
-    out.append("BINARY\n" if binary else "ASCII\n")
-    return "".join(out).encode()
+def _chunk_names(path: str, indices: list, chunk_size: int) -> list:
+    """The files a chunked log writes: path.%08u after the index opening
+    each chunk (a new chunk when index % chunk_size == 0), else path."""
+    if chunk_size <= 0 or not indices:
+        return [path]
+    return [f"{path}.{i:08d}" for k, i in enumerate(indices) if k == 0 or i % chunk_size == 0]
 
 
 def write_results_rows(path: str, rows: list, binary: bool = False, header: str = "", chunk_size: int = 0) -> list:
     """Results files in LogResults' layout (logResults.cpp:135-381) from rows
-    of the 26 RESULT_FIELDS values.  With chunk_size > 0 the rows go to
-    files named path.%08u after the index of the event opening each chunk
-    (a new chunk when index % chunk_size == 0), the header only in the
-    first, as the reference's writer thread does.  Returns the file names."""
-    names, f = [], None
-    try:
-        for r in rows:
-            index = int(r[0])
-            if f is None or (chunk_size > 0 and index % chunk_size == 0):
-                first = f is None
-                if f is not None:
-                    f.close()
-                name = f"{path}.{index:08d}" if chunk_size > 0 else path
-                f = open(name, "wb")
-                names.append(name)
-                f.write(_results_header(binary, header if first else ""))
-            if binary:
-                f.write(struct.pack("<IhI", index, int(r[1]), int(r[2])))
-                f.write(struct.pack("<23f", *[float(v) for v in r[3:]]))
-            else:
-                f.write(("\t".join([str(int(r[0])), str(int(r[1])), str(int(r[2]))] +
-                                   [_c_scientific(v) for v in r[3:]]) + "\n").encode())
-        if f is None:
-            f = open(path, "wb")
-            names.append(path)
-            f.write(_results_header(binary, header))
-    finally:
-        if f is not None:
-            f.close()
-    return names
-
-
-def _c_scientific(v: float) -> str:
-    """A float as C++ iostream prints it with std::ios::scientific."""
-    if v != v:
-        return "nan" if math.copysign(1.0, v) > 0 else "-nan"
-    return f"{float(np.float32(v)):e}"
+    of the 26 RESULT_FIELDS values, by the library's native writer
+    (tg_results_write).  With chunk_size > 0 the rows go to files named
+    path.%08u after the index of the event opening each chunk, the header
+    only in the first, as the reference's writer thread does.  Returns the
+    file names."""
+    arr = (N.tg_result_row * len(rows))()
+    for k, r in enumerate(rows):
+        a = arr[k]
+        a.index, a.id, a.number, a.voltage = int(r[0]), int(r[1]), int(r[2]), float(r[3])
+        a.start[:] = [float(v) for v in r[4:7]]
+        a.stop[:] = [float(v) for v in r[7:10]]
+        a.tof, a.probability, a.potential_before = float(r[10]), float(r[11]), float(r[12])
+        a.field_before[:] = [float(v) for v in r[13:16]]
+        a.potential_after = float(r[16])
+        a.field_after[:] = [float(v) for v in r[17:20]]
+        a.normal[:] = [float(v) for v in r[20:23]]
+        a.apex[:] = [float(v) for v in r[23:26]]
+    N.check(N.lib().tg_results_write(str(path).encode(), int(binary), header.encode(), len(rows),
+                                     C.cast(arr, C.c_void_p), int(chunk_size)))
+    return _chunk_names(str(path), [int(r[0]) for r in rows], chunk_size)
 
 
 def read_results(path: str) -> tuple[str, list]:
@@ -800,70 +771,27 @@ def write_results(path: str, records: list[dict], xyz: np.ndarray, binary: bool 
 
 # ---- trajectory files (LogTrajectory) -----------------------------------------
 
-_TRAJ_STATUS = {0: "NO_INTEGRATION", 1: "NO_FIELD", 2: "STEPPER_LIMIT_PASSED", 3: "ITERATION_LIMIT_PASSED",
-                4: "GEOMETRY_LIMIT_PASSED", 5: "SYSTEM_LIMIT_PASSED"}
-_TRAJ_COLUMNS = [("time", "[s]", "float"), ("positionX", "[m]", "float"), ("positionY", "[m]", "float"),
-                 ("positionZ", "[m]", "float"), ("velocityX", "[m/s]", "float"), ("velocityY", "[m/s]", "float"),
-                 ("velocityZ", "[m/s]", "float"), ("tetrahedron", "[1]", "int")]
-
-
-def _trajectory_header(binary: bool) -> bytes:
-    """LogTrajectory::writeHeader (logTrajectory.cpp:137-168)."""
-    out = ["TAPSIM TRAJECTORY DATA\nVERSION 1.0\n"]
-    for name, unit, kind in _TRAJ_COLUMNS:
-        out.append(f"# {name} {unit} ({kind})\n" if binary else f"# {name} {unit}\n")
-    out.append("\n")
-    return "".join(out).encode()
-
-
 def write_trajectory_items(path: str, items: list, binary: bool = False, chunk_size: int = 0) -> list:
-    """Trajectory files in LogTrajectory's layout (logTrajectory.cpp:170-300).
-    Each item holds index, number, time_scale, status, charge, mass, points
-    (PATH_POINT records whose time column is written as it is) and error
-    (6 floats).  With chunk_size > 0 the items go to files named
-    path.%08u after the index opening each chunk (a new chunk when
-    index % chunk_size == 0), each file with the header.  Returns the file
-    names."""
-    names, f = [], None
-    try:
-        for it in items:
-            index = int(it["index"])
-            if f is None or (chunk_size > 0 and index % chunk_size == 0):
-                if f is not None:
-                    f.close()
-                name = f"{path}.{index:08d}" if chunk_size > 0 else path
-                f = open(name, "wb")
-                names.append(name)
-                f.write(_trajectory_header(binary))
-            status = int(it["status"])
-            pts = np.asarray(it["points"], N.PATH_POINT)
-            head = (f"# index = {index}\n# unique number = {int(it['number'])}\n"
-                    f"# time scale = {_c_scientific(it['time_scale'])}\n"
-                    f"# integrator status = {status} => {_TRAJ_STATUS.get(status, 'INVALID')}\n"
-                    f"# charge [C] / mass [kg] = {_c_scientific(it['charge'])} / {_c_scientific(it['mass'])}\n")
-            f.write(head.encode())
-            if binary:
-                f.write(f"BINARY {len(pts)}\n".encode())
-                f.write(pts.tobytes())
-                f.write(b"\n")
-            else:
-                f.write(f"ASCII {len(pts)}\n".encode())
-                lines = []
-                for p in pts:
-                    vals = [p["time"], *p["position"], *p["velocity"]]
-                    lines.append("\t".join(_c_scientific(v) for v in vals) + f"\t{int(p['tet'])}\n")
-                f.write("".join(lines).encode())
-            e = [_c_scientific(v) for v in it["error"]]
-            f.write((f"# final error estimate (position) = ({e[0]}/{e[1]}/{e[2]})\n"
-                     f"# final error estimate (velocity) = ({e[3]}/{e[4]}/{e[5]})\n\n").encode())
-        if f is None:
-            f = open(path, "wb")
-            names.append(path)
-            f.write(_trajectory_header(binary))
-    finally:
-        if f is not None:
-            f.close()
-    return names
+    """Trajectory files in LogTrajectory's layout (logTrajectory.cpp:170-300)
+    by the library's native writer (tg_trajectory_write).  Each item holds
+    index, number, time_scale, status, charge, mass, points (PATH_POINT
+    records whose time column is written as it is) and error (6 floats).
+    With chunk_size > 0 the items go to files named path.%08u after the index
+    opening each chunk, each file with the header.  Returns the file names."""
+    arr = (N.tg_trajectory_item * len(items))()
+    keep = []
+    for k, it in enumerate(items):
+        pts = np.ascontiguousarray(np.asarray(it["points"], N.PATH_POINT))
+        keep.append(pts)
+        a = arr[k]
+        a.index, a.number, a.time_scale, a.status = int(it["index"]), int(it["number"]), float(it["time_scale"]), \
+            int(it["status"])
+        a.charge, a.mass, a.num_points = float(it["charge"]), float(it["mass"]), len(pts)
+        a.points = pts.ctypes.data if len(pts) else None
+        a.error[:] = [float(v) for v in it["error"]]
+    N.check(N.lib().tg_trajectory_write(str(path).encode(), int(binary), len(items), C.cast(arr, C.c_void_p),
+                                        int(chunk_size)))
+    return _chunk_names(str(path), [int(it["index"]) for it in items], chunk_size)
 
 
 def write_trajectories(path: str, records: list[dict], binary: bool = False, chunk_size: int = 0) -> list:
