@@ -221,6 +221,43 @@ AmgCsr galerkin(const AmgCsr& R, const AmgCsr& A, const AmgCsr& P, int threads) 
     return Ac;
 }
 
+// Drops the entries |a_ij| < drop sqrt(a_ii a_jj) of a coarse operator and
+// adds them to a_ii, which keeps every row sum (and so the constants in the
+// near null space) as it was.  Rows without a positive diagonal are kept whole.
+void drop_weak(AmgCsr* A, double drop) {
+    const int n = A->rows;
+    std::vector<double> diag(n, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++)
+            if (A->col[q] == i) diag[i] = A->val[q];
+    std::vector<int32_t> ptr(n + 1, 0), col;
+    std::vector<double> val;
+    col.reserve(A->col.size());
+    val.reserve(A->val.size());
+    for (int i = 0; i < n; i++) {
+        int dpos = -1;
+        double lump = 0.0;
+        for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++) {
+            const int j = A->col[q];
+            const double a = A->val[q];
+            const bool keep = j == i || !(diag[i] > 0.0) || !(diag[j] > 0.0) ||
+                              std::fabs(a) >= drop * std::sqrt(diag[i] * diag[j]);
+            if (!keep) {
+                lump += a;
+                continue;
+            }
+            if (j == i) dpos = (int)col.size();
+            col.push_back(j);
+            val.push_back(a);
+        }
+        if (dpos >= 0) val[dpos] += lump;
+        ptr[i + 1] = (int32_t)col.size();
+    }
+    A->ptr.swap(ptr);
+    A->col.swap(col);
+    A->val.swap(val);
+}
+
 // Gauss-Jordan inverse with partial pivoting (row-major, in place).
 bool dense_inverse(int n, std::vector<double>& a, std::vector<double>* inv) {
     inv->assign((size_t)n * n, 0.0);
@@ -288,6 +325,7 @@ std::string amg_build(AmgCsr&& A0, const AmgOptions& opt, AmgHierarchy* out) {
             L.P = smoothed_prolongator(A, strong, agg, nc, opt.omega, threads);
             L.R = transpose(L.P);
             AmgCsr Ac = galerkin(L.R, A, L.P, threads);
+            if (opt.coarse_drop > 0.0) drop_weak(&Ac, opt.coarse_drop);
             L.A = std::move(A);
             out->levels.push_back(std::move(L));
             A = std::move(Ac);

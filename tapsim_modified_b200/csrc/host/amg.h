@@ -7,8 +7,9 @@
 // construction is Vanek, Mandel and Brezina's (Computing 56, 1996): strength
 // of connection |a_ij| >= theta sqrt(a_ii a_jj), greedy aggregation,
 // piecewise-constant tentative prolongator smoothed by one damped Jacobi
-// step on the filtered matrix, Galerkin coarse operators R A P with R = P^T,
-// down to a coarsest level solved with a dense inverse.
+// step on the filtered matrix, Galerkin coarse operators R A P with R = P^T
+// whose weakest entries are lumped into the diagonal, down to a coarsest
+// level solved with a dense inverse.
 #pragma once
 
 #include <cstdint>
@@ -38,6 +39,11 @@ struct AmgOptions {
     double theta = 0.08;       // strength threshold on the finest level
     double theta_coarse = 0.0; // and on the coarser ones, whose Galerkin rows spread over more entries
     double omega = 0.8;        // prolongator smoothing weight, 4/3 over rho(D_F^-1 A_F) for rho ~ 1.7
+    // coarse-operator entries |a_ij| < coarse_drop sqrt(a_ii a_jj) are dropped
+    // and lumped into a_ii: on the 3.2M-row system of the 7.3M-cell tip 0.01
+    // halves level 1's entries per row (50 -> 24) and lowers the CG
+    // iterations to 1e-8 from 21 to 16
+    double coarse_drop = 0.01;
     int max_coarse = 1000;     // rows at which coarsening stops
     int max_levels = 12;
     int threads = 0;           // 0: hardware concurrency
