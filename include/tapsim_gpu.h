@@ -141,7 +141,9 @@ typedef struct {
     double rel_residual;      /* final ||r||/||b|| */
     double initial_rel_residual;
     int32_t inner_neumann;    /* of `inner`, the iterations on the Neumann rows */
-    int32_t reserved;
+    int32_t residual_cells;   /* cells flipped since the last converged solve whose rows, and their
+                                 neighbours', the first residual recomputed from the kept residuals;
+                                 0 when the first residual was a pass over every row */
     double setup_seconds;     /* multigrid hierarchy built during this solve [s], 0 if none */
 } tg_solve_info;
 int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);

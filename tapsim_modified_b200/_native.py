@@ -44,7 +44,7 @@ class tg_solve_opts(C.Structure):
 
 class tg_solve_info(C.Structure):
     _fields_ = [("outer", C.c_int32), ("inner", C.c_int32), ("rel_residual", C.c_double),
-                ("initial_rel_residual", C.c_double), ("inner_neumann", C.c_int32), ("reserved", C.c_int32),
+                ("initial_rel_residual", C.c_double), ("inner_neumann", C.c_int32), ("residual_cells", C.c_int32),
                 ("setup_seconds", C.c_double)]
 
 

@@ -70,47 +70,62 @@ __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, f
     }
 }
 
-// Rows of the coarse operators and of the restriction hold tens to a few
-// hundred entries: a group of kRowLanes lanes per row, one row per group,
-// a grid with a group for every row (no grid-stride loop, so that every row's
-// loads are in flight at once).
-constexpr int kRowLanes = 16;
-
+// Rows of the coarse operators and of the restrictions hold tens to a few
+// hundred entries: a group of L lanes per row (L from the matrix's mean row
+// length, AmgDevLevel::a_lanes / r_lanes), one row per group, a grid with a
+// group for every row (no grid-stride loop, so that every row's loads are in
+// flight at once).  Each lane loads four of its entries before it gathers
+// their y, so that a row of up to 4 L entries costs one round trip.
+template <int L>
 __device__ __forceinline__ float row_dot(const int32_t* ptr, const int32_t* col, const float* val, const float* y,
                                          int row, int lane) {
     float acc = 0.0f;
     const int q1 = ptr[row + 1];
-    for (int q = ptr[row] + lane; q < q1; q += kRowLanes) acc += __ldcs(val + q) * __ldg(y + __ldcs(col + q));
+    for (int q = ptr[row] + lane; q < q1; q += 4 * L) {
+        int c[4];
+        float a[4];
 #pragma unroll
-    for (int o = kRowLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        for (int j = 0; j < 4; j++) {
+            const bool in = q + j * L < q1;
+            c[j] = in ? __ldcs(col + q + j * L) : -1;
+            a[j] = in ? __ldcs(val + q + j * L) : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (c[j] >= 0) acc += a[j] * __ldg(y + c[j]);
+    }
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return acc;
 }
 
 // Rows of a CSR operator A (with its diagonal):
 // mode 0: t = b - A y; mode 1: x = y + w (b - A y) / diag
+template <int L>
 __global__ void k_amg_csr(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* diag,
                           const float* b, const float* y, float* out, int mode, const double* scal, int it,
                           double target) {
     if (done(scal, it, target)) return;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = gid % kRowLanes;
-    const int row = min(gid / kRowLanes, n - 1);  // whole groups stay active for the shuffles
-    const float acc = row_dot(ptr, col, val, y, row, lane);
-    if (lane == 0 && gid / kRowLanes < n) {
+    const int lane = gid % L;
+    const int row = min(gid / L, n - 1);  // whole groups stay active for the shuffles
+    const float acc = row_dot<L>(ptr, col, val, y, row, lane);
+    if (lane == 0 && gid / L < n) {
         const float t = b[row] - acc;
         out[row] = mode == 0 ? t : y[row] + kSmooth * t / diag[row];
     }
 }
 
 // out = M y for a CSR matrix (restriction R t)
+template <int L>
 __global__ void k_amg_mv(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* y, float* out,
                          const double* scal, int it, double target) {
     if (done(scal, it, target)) return;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = gid % kRowLanes;
-    const int row = min(gid / kRowLanes, n - 1);
-    const float acc = row_dot(ptr, col, val, y, row, lane);
-    if (lane == 0 && gid / kRowLanes < n) out[row] = acc;
+    const int lane = gid % L;
+    const int row = min(gid / L, n - 1);
+    const float acc = row_dot<L>(ptr, col, val, y, row, lane);
+    if (lane == 0 && gid / L < n) out[row] = acc;
 }
 
 // y += P x' (prolongation, a few entries per row), one thread per row
@@ -143,8 +158,33 @@ __global__ void k_amg_dense(int n, const float* inv, const float* b, float* x, c
 // loop then makes one pass)
 inline unsigned grid_full(long long threads) { return (unsigned)((threads + kBlock - 1) / kBlock); }
 
-// a group of kRowLanes threads for every row
-inline unsigned grid_rows(int n) { return (unsigned)(((long long)n * kRowLanes + kBlock - 1) / kBlock); }
+// a group of L threads for every row
+inline unsigned grid_rows(int n, int L) { return (unsigned)(((long long)n * L + kBlock - 1) / kBlock); }
+
+// the lane-group kernels for L = 2 .. 32
+void launch_csr(int L, int n, const int32_t* ptr, const int32_t* col, const float* val, const float* diag,
+                const float* b, const float* y, float* out, int mode, const double* scal, int it, double target,
+                cudaStream_t s) {
+    count_launch();
+    switch (L) {
+        case 2: k_amg_csr<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
+        case 4: k_amg_csr<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
+        case 8: k_amg_csr<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
+        case 16: k_amg_csr<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
+        default: k_amg_csr<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
+    }
+}
+void launch_mv(int L, int n, const int32_t* ptr, const int32_t* col, const float* val, const float* y, float* out,
+               const double* scal, int it, double target, cudaStream_t s) {
+    count_launch();
+    switch (L) {
+        case 2: k_amg_mv<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
+        case 4: k_amg_mv<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
+        case 8: k_amg_mv<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
+        case 16: k_amg_mv<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
+        default: k_amg_mv<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
+    }
+}
 
 inline int grid_for(long long threads) {
     static int cap = 0;
@@ -180,8 +220,7 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
             const AmgDevLevel& L = g.lev[l];
             const AmgDevLevel& C = g.lev[l + 1];
             const float* t = l == 0 ? g.t0 : L.t;
-            count_launch();
-            k_amg_mv<<<grid_rows(C.n), kBlock, 0, s>>>(C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, scal, it, target);
+            launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, scal, it, target, s);
             if (l + 1 == g.levels - 1) {
                 count_launch();
                 k_amg_dense<<<grid_for((long long)C.n * 32), kBlock, 0, s>>>(C.n, g.coarse_inv, C.b, C.x, scal, it,
@@ -189,9 +228,7 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
             } else {
                 count_launch();
                 k_amg_jacobi<<<grid_for(C.n), kBlock, 0, s>>>(C.n, C.b, C.diag, C.y, scal, it, target);
-                count_launch();
-                k_amg_csr<<<grid_rows(C.n), kBlock, 0, s>>>(C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0,
-                                                            scal, it, target);
+                launch_csr(C.a_lanes, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, scal, it, target, s);
             }
         }
         // up: prolong, post-smooth
@@ -201,13 +238,12 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
             float* y = l == 0 ? g.y0 : L.y;
             count_launch();
             k_amg_prolong<<<grid_for(L.n), kBlock, 0, s>>>(L.n, L.p_ptr, L.p_col, L.p_val, C.x, y, scal, it, target);
-            count_launch();
             if (l == 0) {
+                count_launch();
                 k_amg_fine<<<grid_full(slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, v.u, 1, scal, it,
                                                                                  target);
             } else {
-                k_amg_csr<<<grid_rows(L.n), kBlock, 0, s>>>(L.n, L.a_ptr, L.a_col, L.a_val, L.diag, L.b, L.y, L.x, 1,
-                                                            scal, it, target);
+                launch_csr(L.a_lanes, L.n, L.a_ptr, L.a_col, L.a_val, L.diag, L.b, L.y, L.x, 1, scal, it, target, s);
             }
         }
     } else {

@@ -160,6 +160,43 @@ __global__ void k_vcg_warm(DevMesh m, VSys v, int slots, float alpha) {
     m.phi64[i] += (double)h;
 }
 
+// The first residual of a warm solve: after the warm start has added hist to
+// the V rows' potentials, r -= A hist on the V system (FP32 operator, as the
+// inner solve applies it) and sum r^2 into *acc.  The residual it starts
+// from is the one of the potentials before the start, kept from the last
+// full pass and updated on the rows that removals touched.
+__global__ void k_vcg_warm_residual(VSys v, int slices, double* acc) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    double r2 = 0.0;
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
+        const int base = v.slice_start[warp];
+        const int width = v.slice_width[warp];
+        const int s = warp * 32 + lane;
+        const int* __restrict__ col = v.col + base + lane;
+        const float* __restrict__ val = v.val + base + lane;
+        const float* __restrict__ hh = v.hist;
+        float acc_ = 0.0f;
+        int k = 0;
+        for (; k + 8 <= width; k += 8) {
+            int c[8];
+            float a[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                c[j] = __ldcs(col + 32 * (k + j));
+                a[j] = __ldcs(val + 32 * (k + j));
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc_ += a[j] * __ldg(hh + c[j]);
+        }
+        for (; k < width; k++) acc_ += __ldcs(val + 32 * k) * __ldg(hh + __ldcs(col + 32 * k));
+        const float r = v.r[s] - (v.d[s] * hh[s] - acc_);
+        v.r[s] = r;
+        r2 += (double)r * (double)r;
+    }
+    block_sum_atomic<kBlock>(r2, acc);
+}
+
 // r of the Neumann rows += sum over V neighbours ceff_ij x_j
 __global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int count, float* rN) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -180,7 +217,7 @@ __global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int
 // neighbouring threads then read from neighbouring memory) and each result
 // is written to its slot; padding slots keep r = 0.
 __global__ void k_vcg_residual(DevMesh m, VSys v, const int32_t* __restrict__ rows, int count, double* acc,
-                               double* bacc) {
+                               double* bacc, double* r64, double* b64) {
     double r2 = 0.0, b2 = 0.0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
         const int i = rows[t];
@@ -195,10 +232,51 @@ __global__ void k_vcg_residual(DevMesh m, VSys v, const int32_t* __restrict__ ro
         const double b = sb - m.q64[i];
         b2 += b * b;
         v.r[v.slot_of[i]] = (float)r;
+        if (r64) r64[i] = r;
+        if (b64) b64[i] = b;
         r2 += r * r;
     }
     if (bacc) block_sum2_atomic<kBlock>(r2, b2, acc, bacc);
     else block_sum_atomic<kBlock>(r2, acc);
+}
+
+// Residuals of the rows that removals have changed since the last full
+// pass: the flipped cells and their neighbours, the only rows whose
+// couplings, class or neighbour potentials a flip touches.  One warp per
+// flipped cell; a row shared by several is taken by the first warp to stamp
+// it.  Each row's residual and Dirichlet part are recomputed as the full
+// passes compute them; the differences of their squares to the stored
+// values go into rsum (V rows, Neumann rows, b), and the FP32 right-hand
+// sides of the inner solves get the new values.
+__global__ void k_residual_rows(DevMesh m, VSys v, float* rN, const int32_t* __restrict__ flips, int count,
+                                int32_t* stamp, int epoch, double* r64, double* b64, double* rsum) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= count) return;
+    const int f = flips[warp];
+    const int q0 = m.row_ptr[f], q1 = m.row_ptr[f + 1];
+    for (int k = lane - 1; k < q1 - q0; k += 32) {
+        const int i = k < 0 ? f : m.col[q0 + k];
+        if (m.flags[i] & F_DIRICHLET) continue;
+        if (atomicExch(stamp + i, epoch) == epoch) continue;
+        double sum = 0.0, sb = 0.0;
+        for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+            const int j = m.col[q];
+            const double c = m.ceff64[q] * m.phi64[j];
+            sum += c;
+            if (m.flags[j] & F_DIRICHLET) sb += c;
+        }
+        const double r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
+        const double b = sb - m.q64[i];
+        const double r0 = r64[i], b0 = b64[i];
+        r64[i] = r;
+        b64[i] = b;
+        const bool neumann = (m.flags[i] & F_NEUMANN) != 0;
+        if (neumann) rN[i] = (float)r;
+        else v.r[v.slot_of[i]] = (float)r;
+        atomicAdd(rsum + (neumann ? 1 : 0), r * r - r0 * r0);
+        atomicAdd(rsum + 2, b * b - b0 * b0);
+    }
 }
 
 // Appends the row of a node that has just become a non-Neumann free cell
@@ -331,15 +409,30 @@ void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, c
 void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s) {
     if (slots > 0) { count_launch(); k_vcg_warm<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, alpha); }
 }
+void launch_vcg_warm_residual(const VSys& v, int slots, double* acc, cudaStream_t s) {
+    const int slices = (slots + 31) / 32;
+    if (slices > 0) {
+        count_launch();
+        k_vcg_warm_residual<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, acc);
+    }
+}
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
                                cudaStream_t s) {
     if (count > 0) { count_launch(); k_vcg_couple_neumann<<<blocks(count), kBlock, 0, s>>>(m, v, rows, count, rN); }
 }
 void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, int count, double* acc, double* bacc,
-                         cudaStream_t s) {
+                         cudaStream_t s, double* r64, double* b64) {
     if (count > 0) {
         count_launch();
-        k_vcg_residual<<<reduce_blocks(count), kBlock, 0, s>>>(m, v, rows, count, acc, bacc);
+        k_vcg_residual<<<reduce_blocks(count), kBlock, 0, s>>>(m, v, rows, count, acc, bacc, r64, bacc ? b64 : nullptr);
+    }
+}
+void launch_residual_rows(const DevMesh& m, const VSys& v, float* rN, const int32_t* flips, int count, int32_t* stamp,
+                          int epoch, double* r64, double* b64, double* rsum, cudaStream_t s) {
+    if (count > 0) {
+        count_launch();
+        k_residual_rows<<<(count + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, s>>>(m, v, rN, flips, count, stamp,
+                                                                                     epoch, r64, b64, rsum);
     }
 }
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {

@@ -150,6 +150,7 @@ struct tg_handle {
         int32_t result[1024];
         int32_t flipped[1024];
         int32_t counts[2 * kMaxColours];
+        int32_t pending[4096];  // cells flipped since the last solve
     };
     Pinned* pin = nullptr;
     int vNext = 0;            // host mirror of the V system's slot counter
@@ -205,6 +206,21 @@ struct tg_handle {
 
     bool bnormValid = false;
     double bnorm2 = 0.0;
+    // residuals kept between solves: the last full pass of a converged solve
+    // leaves every free row's FP64 residual and Dirichlet part (resid, by
+    // node: r, then b) and their sums of squares (rsum: V rows, Neumann rows,
+    // b).  Removals list the cells they flip, and the next solve's first
+    // residual recomputes only those cells' rows and their neighbours'
+    // (launch_residual_rows) instead of every row.  Anything else that
+    // changes potentials, couplings or types clears residValid.
+    DBuf<double> resid;
+    DBuf<double> rsum;
+    DBuf<int32_t> resStamp;
+    DBuf<int32_t> pendingDev;
+    int resEpoch = 0;
+    bool residValid = false;
+    int nPending = 0;
+    bool pendingOverflow = false;
     // warm start bookkeeping: the correction of a solve is recorded (VSys
     // hist) when the solve starts from a converged state changed only by
     // removals; it seeds the next such solve
@@ -688,6 +704,13 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(h->cgbuf.alloc(10 * (size_t)n));
     if (e == cudaSuccess) chk(cudaMemset(h->cgbuf.p, 0, 10 * (size_t)n * sizeof(float)));
     chk(h->acc.alloc(16));
+    chk(h->resid.alloc(2 * (size_t)n));
+    if (e == cudaSuccess) chk(cudaMemset(h->resid.p, 0, 2 * (size_t)n * sizeof(double)));
+    chk(h->rsum.alloc(4));
+    if (e == cudaSuccess) chk(cudaMemset(h->rsum.p, 0, 4 * sizeof(double)));
+    chk(h->resStamp.alloc(n));
+    if (e == cudaSuccess) chk(cudaMemset(h->resStamp.p, 0, (size_t)n * sizeof(int32_t)));
+    chk(h->pendingDev.alloc(4096));
     chk(h->keys.alloc(8));
     chk(h->result.alloc(1024));
     chk(h->local.alloc(1 << 16));
@@ -748,6 +771,7 @@ void tg_destroy(tg_handle* h) {
     h->allV.release(); h->allN.release(); h->segStartD.release(); h->countVD.release(); h->countND.release();
     h->countAllD.release(); h->surfList.release(); h->surfSlot.release(); h->surfCount.release();
     h->surfRatio.release(); h->surfScore.release(); h->cgbuf.release(); h->scalV.release(); h->scalN.release(); h->acc.release();
+    h->resid.release(); h->rsum.release(); h->resStamp.release(); h->pendingDev.release();
     h->keys.release(); h->result.release(); h->local.release(); h->localCount.release();
     h->localScratch.release(); h->stageI.release(); h->stageD.release(); h->stageF.release();
     h->stageImpact.release(); h->pathBuf.release(); h->pathErr.release();
@@ -870,7 +894,7 @@ int tg_set_phi(tg_handle* h, const double* phi) {
     CK(cudaMemcpyAsync(h->phi64.p, phi, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
     h->bnormValid = false;
     h->selValid = false;
-    h->converged = h->histValid = false;
+    h->converged = h->histValid = h->residValid = false;
     return sync_status(h, "tg_set_phi");
 }
 
@@ -896,7 +920,7 @@ int tg_relax_cycles(tg_handle* h, int32_t n, double* deviation) {
     const int rc = sync_status(h, "tg_relax_cycles");
     if (deviation) *deviation = dev;
     h->selValid = false;
-    h->converged = h->histValid = false;
+    h->converged = h->histValid = h->residValid = false;
     return rc;
 }
 
@@ -930,7 +954,7 @@ int tg_relax_threshold(tg_handle* h, double threshold, int32_t cycle, int32_t qu
 int tg_local_relax(tg_handle* h, int32_t node, int32_t shell, double threshold, int32_t cycle, int32_t queueSize,
                    int64_t* iterations, double* deviation) {
     if (!h || node < 0 || node >= h->n || cycle < 1) return fail(h, TG_ERR_ARGUMENT, "tg_local_relax: bad argument");
-    h->converged = h->histValid = false;
+    h->converged = h->histValid = h->residValid = false;
     DevMesh m = h->dm();
     launch_local_set(m, node, shell, h->local.p, h->localCount.p, (int)h->local.n, h->localScratch.p,
                      (int)h->localScratch.n, h->ncol, h->stream);
@@ -1108,6 +1132,14 @@ static int amg_setup(tg_handle* h, double* seconds) {
     // the DBuf vectors must not reallocate while pointers into them are live
     h->amgI.reserve(8 * H.levels.size() + 4);
     h->amgF.reserve(8 * H.levels.size() + 4);
+    // lanes per CSR row: the power of two nearest a quarter of the mean row
+    // length, so that a lane's entries take about one round of loads
+    auto lanes = [](const tg_host::AmgCsr& M) {
+        const double per = M.rows > 0 ? (double)M.val.size() / M.rows / 4.0 : 1.0;
+        int L = 2;
+        while (L < 32 && per > L * 1.4142135623730951) L *= 2;
+        return L;
+    };
     tgd::AmgDev g{};
     g.levels = (int)H.levels.size();
     for (int l = 0; l < g.levels; l++) {
@@ -1118,6 +1150,7 @@ static int amg_setup(tg_handle* h, double* seconds) {
             D.a_ptr = upI(L.A.ptr);
             D.a_col = upI(L.A.col);
             D.a_val = upF(L.A.val);
+            D.a_lanes = lanes(L.A);
             std::vector<double> diag(L.A.rows, 1.0);
             for (int i = 0; i < L.A.rows; i++)
                 for (int q = L.A.ptr[i]; q < L.A.ptr[i + 1]; q++)
@@ -1135,6 +1168,7 @@ static int amg_setup(tg_handle* h, double* seconds) {
             D.r_ptr = upI(L.R.ptr);
             D.r_col = upI(L.R.col);
             D.r_val = upF(L.R.val);
+            D.r_lanes = lanes(L.R);
         }
     }
     g.y0 = vec((size_t)h->vCapacity + 1);
@@ -1221,10 +1255,32 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     // correction; with warm_start it starts from the previous one
     const bool fromEvent = h->converged && h->removalsSinceSolve > 0;
     const bool warm = fromEvent && h->histValid && (o->warm_start == 1 || o->warm_start == 2);
+    const bool learnPredict = fromEvent && h->learner && (h->learnMode & 2) && o->warm_start == 2 && h->lastSite >= 0;
+    // the first residual after removals from a converged state: the rows the
+    // removals touched, from the kept residuals of the potentials as they
+    // are; a warm start then takes A hist off the V rows (FP32) and the
+    // Neumann rows are recomputed.  The learned start changes potentials
+    // around the site as well and takes the full pass.
+    const bool incremental = h->residValid && fromEvent && !h->pendingOverflow && h->nPending > 0 && !learnPredict;
+    const int nPending = h->nPending;
+    h->residValid = h->pendingOverflow = false;
+    h->nPending = 0;
+    double* rv = h->resid.p;
+    double* bv = h->resid.p + h->n;
+    if (incremental) {
+        CK(cudaMemcpyAsync(h->pendingDev.p, h->pin->pending, sizeof(int32_t) * nPending, cudaMemcpyHostToDevice,
+                           h->stream));
+        if (++h->resEpoch == INT32_MAX) {
+            CK(cudaMemsetAsync(h->resStamp.p, 0, sizeof(int32_t) * (size_t)h->n, h->stream));
+            h->resEpoch = 1;
+        }
+        launch_residual_rows(m, vsys, vN.r, h->pendingDev.p, nPending, h->resStamp.p, h->resEpoch, rv, bv, h->rsum.p,
+                             h->stream);
+        inf.residual_cells = nPending;
+    }
     if (warm) launch_vcg_warm(m, vsys, h->vActive, 1.0f, h->stream);
     else if (fromEvent) CK(cudaMemsetAsync(vsys.hist, 0, sizeof(float) * ((size_t)h->vCapacity + 1), h->stream));
     // learned near field on top of the recycled far field; sample collection
-    const bool learnPredict = fromEvent && h->learner && (h->learnMode & 2) && o->warm_start == 2 && h->lastSite >= 0;
     const bool learnCollect = fromEvent && h->learner && (h->learnMode & 1) && h->lastSite >= 0;
     if (learnPredict || learnCollect) {
         rc = learner_predict(h->learner, m, h->lastSite, vsys.slot_of, learnPredict ? vsys.hist : nullptr, h->stream,
@@ -1243,15 +1299,32 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         if (rc != TG_OK) return rc;
     }
     for (int outer = 0;; outer++) {
-        CK(cudaMemsetAsync(h->acc.p, 0, 3 * sizeof(double), h->stream));
-        launch_vcg_residual(m, vsys, h->allV.p, h->countAllV, h->acc.p, needB ? h->acc.p + 2 : nullptr, h->stream);
-        launch_residual(m, h->allN.p, h->countAllN, vN.r, h->acc.p + 1, h->stream, needB ? h->acc.p + 2 : nullptr);
+        if (outer == 0 && incremental) {
+            if (warm) {
+                CK(cudaMemsetAsync(h->rsum.p, 0, 2 * sizeof(double), h->stream));
+                launch_vcg_warm_residual(vsys, h->vActive, h->rsum.p, h->stream);
+                launch_residual(m, h->allN.p, h->countAllN, vN.r, h->rsum.p + 1, h->stream, nullptr, rv, nullptr);
+            }
+            needB = true;
+        } else {
+            // a full pass; the first one also takes the Dirichlet parts, so
+            // that the kept values describe the rows as they are
+            if (outer == 0) needB = true;
+            CK(cudaMemsetAsync(h->rsum.p, 0, (needB ? 3 : 2) * sizeof(double), h->stream));
+            launch_vcg_residual(m, vsys, h->allV.p, h->countAllV, h->rsum.p, needB ? h->rsum.p + 2 : nullptr,
+                                h->stream, rv, bv);
+            launch_residual(m, h->allN.p, h->countAllN, vN.r, h->rsum.p + 1, h->stream,
+                            needB ? h->rsum.p + 2 : nullptr, rv, bv);
+        }
         double* r2 = h->pin->r2;
-        CK(cudaMemcpyAsync(r2, h->acc.p, sizeof(double) * (needB ? 3 : 2), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(r2, h->rsum.p, sizeof(double) * (needB ? 3 : 2), cudaMemcpyDeviceToHost, h->stream));
         rc = sync_status(h, "tg_solve residual");
         if (rc != TG_OK) return rc;
+        // sums kept across removals can round to a little below zero
+        r2[0] = std::max(r2[0], 0.0);
+        r2[1] = std::max(r2[1], 0.0);
         if (needB) {
-            h->bnorm2 = r2[2];
+            h->bnorm2 = std::max(r2[2], 0.0);
             h->bnormValid = true;
             needB = false;
         }
@@ -1290,6 +1363,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     h->selValid = false;
     h->converged = true;
     h->histValid = fromEvent;
+    h->residValid = true;
     if (learnCollect) {
         rc = learner_collect_end(h->learner, m, h->stream);
         if (rc != TG_OK) return fail(h, rc, std::string("tg_solve: ") + tg_learner_last_error(h->learner));
@@ -1647,6 +1721,25 @@ static int take_away_impl(tg_handle* h, int32_t node, int32_t capacity, int32_t*
     h->countAllN = pin->misc[1];
     h->surfSlots = std::min(pin->misc[2], h->n);
     const int nd = pin->result[0];
+    // the flipped cells for the next solve's first residual; rows that move
+    // between the V and Neumann classes, or out of the free rows, and lists
+    // cut short by the result capacity take the full pass instead
+    {
+        const tg_type& vt0 = h->types[h->vacuumId];
+        bool ok = nd + 1 < cap && h->nPending + 1 + nd <= (int)(sizeof(pin->pending) / sizeof(int32_t)) &&
+                  !vt0.dirichlet;
+        for (int k = -1; ok && k < nd; k++) {
+            const int j = k < 0 ? node : pin->result[1 + k];
+            const int t = h->h_type[j];
+            if (t >= 0 && !h->types[t].dirichlet && h->types[t].neumann != vt0.neumann) ok = false;
+        }
+        if (ok) {
+            pin->pending[h->nPending++] = node;
+            for (int k = 0; k < nd; k++) pin->pending[h->nPending++] = pin->result[1 + k];
+        } else {
+            h->pendingOverflow = true;
+        }
+    }
     int nf = 0;
     if (!(h->h_type[node] >= 0 && h->types[h->h_type[node]].dirichlet == 0)) pin->flipped[nf++] = node;
     h->h_type[node] = (int8_t)h->vacuumId;
@@ -1693,6 +1786,7 @@ int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached
 
 int tg_update_coordination(tg_handle* h) {
     if (!h) return fail(h, TG_ERR_ARGUMENT, "tg_update_coordination: null handle");
+    h->residValid = false;
     launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
     return sync_status(h, "tg_update_coordination");
 }
@@ -1888,7 +1982,10 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
     rc = take_away_impl(h, node, 0, nullptr, &nd);
     if (rc != TG_OK) return rc;
     rec->detached = nd;
-    if (h->coordinationActive) launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
+    if (h->coordinationActive) {
+        h->residValid = false;
+        launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
+    }
     // III) relaxation
     if (o->relax_mode == 0) {
         int64_t it = 0;

@@ -110,6 +110,7 @@ struct AmgDevLevel {
     const int32_t *r_ptr, *r_col;           // restriction: the next level's rows
     const float* r_val;
     float *b, *y, *x, *t;                   // right-hand side, work, result, residual (levels >= 1)
+    int a_lanes, r_lanes;                   // lanes per row of the operator and of the restriction (2..32)
 };
 struct AmgDev {
     int levels;                             // including level 0 (the V system) and the coarsest
@@ -125,12 +126,23 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
 void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s);
 // warm start: hist *= alpha, phi64 += hist on the V rows
 void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s);
+// r -= A hist on the V system (FP32), sum r^2 into *acc
+void launch_vcg_warm_residual(const VSys& v, int slots, double* acc, cudaStream_t s);
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
                                cudaStream_t s);
 // FP64 residual of the V rows (rows: their compact list, in node order)
-// into the V system's r; with bacc, also ||b||^2 of those rows
+// into the V system's r; with bacc, also ||b||^2 of those rows.  With r64
+// (by node) each row's FP64 residual is kept, and with bacc and b64 its
+// Dirichlet part
 void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, int count, double* acc, double* bacc,
-                         cudaStream_t s);
+                         cudaStream_t s, double* r64 = nullptr, double* b64 = nullptr);
+// the residuals of the flipped cells and their neighbours after removals,
+// from the values the last full passes kept in r64 / b64: rsum[0..2] (the V
+// rows' r^2, the Neumann rows' r^2, ||b||^2) take the differences, the V
+// system's r and rN the new values.  stamp (by node) holds a value other
+// than epoch for every row
+void launch_residual_rows(const DevMesh& m, const VSys& v, float* rN, const int32_t* flips, int count, int32_t* stamp,
+                          int epoch, double* r64, double* b64, double* rsum, cudaStream_t s);
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
 // re-copies the couplings and diagonals that flips of the listed cells
 // changed into the V system (rows that existed before the flips)
@@ -144,7 +156,7 @@ void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* ma
 // with bacc, also the squared norm of the rows' Dirichlet part (as
 // launch_bnorm) into *bacc
 void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s,
-                     double* bacc = nullptr);
+                     double* bacc = nullptr, double* r64 = nullptr, double* b64 = nullptr);
 // b_i = sum over Dirichlet neighbours c_ij phi_j - q_i; sum b^2 into *acc
 void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s);
 // FP32 conjugate gradients on the rows of one list (Jacobi preconditioner)

@@ -50,7 +50,7 @@ __global__ void k_sweep64(DevMesh m, const int32_t* __restrict__ rows, int count
 // with bacc, also the squared norm of the rows' Dirichlet part (k_bnorm's
 // value) from the same pass
 __global__ void k_residual(DevMesh m, const int32_t* __restrict__ rows, int count, float* r32, double* acc,
-                           double* bacc) {
+                           double* bacc, double* r64, double* b64) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double r = 0.0, b = 0.0;
     if (t < count) {
@@ -66,6 +66,8 @@ __global__ void k_residual(DevMesh m, const int32_t* __restrict__ rows, int coun
         r = s - m.diag64[i] * m.phi64[i] - m.q64[i];
         b = sb - m.q64[i];
         if (r32) r32[i] = (float)r;
+        if (r64) r64[i] = r;
+        if (b64) b64[i] = b;
     }
     if (bacc) block_sum2_atomic<kBlock>(r * r, b * b, acc, bacc);
     else block_sum_atomic<kBlock>(r * r, acc);
@@ -282,8 +284,11 @@ void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* ma
     if (count > 0) { count_launch(); k_sweep64<<<blocks(count), kBlock, 0, s>>>(m, rows, count, maxdev); }
 }
 void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s,
-                     double* bacc) {
-    if (count > 0) { count_launch(); k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, acc, bacc); }
+                     double* bacc, double* r64, double* b64) {
+    if (count > 0) {
+        count_launch();
+        k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, acc, bacc, r64, bacc ? b64 : nullptr);
+    }
 }
 void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s) {
     if (count > 0) { count_launch(); k_bnorm<<<blocks(count), kBlock, 0, s>>>(m, rows, count, acc); }
