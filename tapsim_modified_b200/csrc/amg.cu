@@ -38,7 +38,13 @@ __global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, co
         y[i] = kSmooth * b[i] / d[i];
 }
 
-// Level 0 over SELL-32 slices: mode 0: t = b - A y; mode 1: x = y + w (b - A y) / d
+// Level 0 over SELL-32 slices: mode 0: t = b - A y; mode 1: x = y + w (b - A y) / d.
+// A is applied from the bf16 couplings and the FP32 row sums g:
+// (A y)_s = (g_s + sum a16) y_s - sum a16 y_col.  Its entries differ from
+// the CG's FP32 operator by at most 2^-9 relative and its row sums not at
+// all, so it is spectrally within a fraction of a percent of it; the
+// smoothing steps divide by the FP32 diagonal d on both sides of the cycle,
+// which keeps the preconditioner symmetric.
 __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, float* out, int mode,
                            const double* scal, int it, double target) {
     if (done(scal, it, target)) return;
@@ -49,8 +55,8 @@ __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, f
         const int width = v.slice_width[warp];
         const int s = warp * 32 + lane;
         const int* __restrict__ col = v.col + base + lane;
-        const float* __restrict__ val = v.val + base + lane;
-        float acc = 0.0f;
+        const __nv_bfloat16* __restrict__ val = v.val16 + base + lane;
+        float acc = 0.0f, sum = 0.0f;
         int k = 0;
         for (; k + 8 <= width; k += 8) {
             int c[8];
@@ -58,15 +64,22 @@ __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, f
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 c[j] = __ldcs(col + 32 * (k + j));
-                a[j] = __ldcs(val + 32 * (k + j));
+                a[j] = __bfloat162float(__ldcs(val + 32 * (k + j)));
             }
 #pragma unroll
-            for (int j = 0; j < 8; j++) acc += a[j] * __ldg(y + c[j]);
+            for (int j = 0; j < 8; j++) {
+                acc += a[j] * __ldg(y + c[j]);
+                sum += a[j];
+            }
         }
-        for (; k < width; k++) acc += __ldcs(val + 32 * k) * __ldg(y + __ldcs(col + 32 * k));
-        const float d = v.d[s], ys = y[s];
-        const float t = b[s] - (d * ys - acc);
-        out[s] = mode == 0 ? t : ys + kSmooth * t / d;
+        for (; k < width; k++) {
+            const float a = __bfloat162float(__ldcs(val + 32 * k));
+            acc += a * __ldg(y + __ldcs(col + 32 * k));
+            sum += a;
+        }
+        const float ys = y[s];
+        const float t = b[s] - ((v.g[s] + sum) * ys - acc);
+        out[s] = mode == 0 ? t : ys + kSmooth * t / v.d[s];
     }
 }
 

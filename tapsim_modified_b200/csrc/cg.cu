@@ -279,6 +279,24 @@ __global__ void k_residual_rows(DevMesh m, VSys v, float* rN, const int32_t* __r
     }
 }
 
+// Row sum of a V row: d minus its stored couplings, summed in FP64 and
+// rounded once.  With it the multigrid's smoothing pass applies the
+// operator from bf16 couplings as (g + sum a16) y_s - sum a16 y_col, which
+// keeps every row sum of the FP32 operator (constants stay in its near
+// null space) and its symmetry.
+__device__ __forceinline__ void vsys_set_row_sum(VSys v, int s) {
+    const int base = v.slice_start[s >> 5] + (s & 31);
+    const int width = v.slice_width[s >> 5];
+    double sum = 0.0;
+    for (int k = 0; k < width; k++) sum += v.val[base + 32 * k];
+    v.g[s] = (float)((double)v.d[s] - sum);
+}
+
+__device__ __forceinline__ void vsys_set_val(VSys v, int p, float a) {
+    v.val[p] = a;
+    v.val16[p] = __float2bfloat16_rn(a);
+}
+
 // Appends the row of a node that has just become a non-Neumann free cell
 // and repoints its free neighbours' entries at it.  One warp.
 __device__ void vsys_add_row(const DevMesh& m, VSys v, int i) {
@@ -315,14 +333,15 @@ __device__ void vsys_add_row(const DevMesh& m, VSys v, int i) {
             }
             const int sj = v.slot_of[j];
             v.col[base + 32 * k] = sj >= 0 ? sj : v.capacity;
-            v.val[base + 32 * k] = m.ceff32[q];
+            vsys_set_val(v, base + 32 * k, m.ceff32[q]);
             v.vpos[q] = base + 32 * k;
             k++;
         }
         for (; k < width; k++) {
             v.col[base + 32 * k] = v.capacity;
-            v.val[base + 32 * k] = 0.0f;
+            vsys_set_val(v, base + 32 * k, 0.0f);
         }
+        vsys_set_row_sum(v, s);
     }
     __syncwarp();
     // neighbours that are V rows: their entry for i now points at slot s
@@ -333,9 +352,10 @@ __device__ void vsys_add_row(const DevMesh& m, VSys v, int i) {
         const int p = v.vpos[m.rev[q]];
         if (p >= 0) {
             v.col[p] = s;
-            v.val[p] = m.ceff32[m.rev[q]];
+            vsys_set_val(v, p, m.ceff32[m.rev[q]]);
         }
         v.d[sj] = m.diag32[j];
+        vsys_set_row_sum(v, sj);
     }
     __syncwarp();
 }
@@ -355,16 +375,28 @@ __global__ void k_vsys_refresh(DevMesh m, VSys v, const int32_t* nodes, int coun
         const int si = v.slot_of[i];
         if (si >= 0 && lane == 0) v.d[si] = m.diag32[i];
         for (int q = m.row_ptr[i] + lane; q < m.row_ptr[i + 1]; q += 32) {
-            if (si >= 0 && v.vpos[q] >= 0) v.val[v.vpos[q]] = m.ceff32[q];
+            if (si >= 0 && v.vpos[q] >= 0) vsys_set_val(v, v.vpos[q], m.ceff32[q]);
             const int j = m.col[q];
             const int sj = v.slot_of[j];
             if (sj < 0) continue;
             const int p = v.vpos[m.rev[q]];
-            if (p >= 0) v.val[p] = m.ceff32[m.rev[q]];
+            if (p >= 0) vsys_set_val(v, p, m.ceff32[m.rev[q]]);
             v.d[sj] = m.diag32[j];
+            vsys_set_row_sum(v, sj);
         }
         __syncwarp();
+        if (si >= 0 && lane == 0) vsys_set_row_sum(v, si);
+        __syncwarp();
     }
+}
+
+__global__ void k_vsys_derive(VSys v, size_t stored) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < stored; e += stride)
+        v.val16[e] = __float2bfloat16_rn(v.val[e]);
+    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < (size_t)v.capacity; s += stride)
+        vsys_set_row_sum(v, (int)s);
+    if (blockIdx.x == 0 && threadIdx.x == 0) v.g[v.capacity] = 0.0f;
 }
 
 inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
@@ -437,6 +469,10 @@ void launch_residual_rows(const DevMesh& m, const VSys& v, float* rN, const int3
 }
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
     if (count > 0) { count_launch(); k_vsys_add_rows<<<1, 32, 0, s>>>(m, v, nodes, count); }
+}
+void launch_vsys_derive(const VSys& v, size_t stored, cudaStream_t s) {
+    count_launch();
+    k_vsys_derive<<<4096, kBlock, 0, s>>>(v, stored);
 }
 void launch_vsys_refresh(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {
     if (count > 0) { count_launch(); k_vsys_refresh<<<1, 32, 0, s>>>(m, v, nodes, count); }

@@ -114,8 +114,11 @@ struct tg_handle {
     // tg_run_events: a ring of flight slots, each with its own stream and
     // snapshots (potentials, vertex fields), so that the flights of
     // successive events run side by side and overlap the relaxations; the
-    // main stream only copies the potentials into the next free slot
-    static constexpr int kRing = 4;
+    // main stream only copies the potentials into the next free slot.  A
+    // flight takes 9-13 ms beside the relaxations on the 7.3M-cell tip
+    // (vertex fields at low priority, then the walk), so eight slots keep
+    // the event's stream from waiting for a slot at 4-5 ms per event
+    static constexpr int kRing = 8;
     cudaStream_t ringStream[kRing] = {};
     cudaEvent_t ringPhi[kRing] = {}, ringDone[kRing] = {};
     DBuf<double> ringPhiBuf[kRing], ringField[kRing];
@@ -127,6 +130,8 @@ struct tg_handle {
     // non-Neumann free rows in slot order, SELL-32 (cg.cu)
     DBuf<int32_t> vSlotOf, vNodeOf, vSliceStart, vSliceWidth, vCol, vPos, vCount;
     DBuf<float> vVal, vVec;  // vVec: d, x, r, u, w, p, sv, hist, each capacity+1
+    DBuf<__nv_bfloat16> vVal16;  // vVal rounded to bf16 (multigrid smoothing pass)
+    DBuf<float> vG;              // row sums of the V rows (capacity+1)
     DBuf<double> vScal;
     DBuf<double> vfield;     // vertex fields of the current flight call
     DBuf<float> tetpack;     // packed tetrahedra for the flights
@@ -188,6 +193,8 @@ struct tg_handle {
         v.slice_width = vSliceWidth.p;
         v.col = vCol.p;
         v.val = vVal.p;
+        v.val16 = vVal16.p;
+        v.g = vG.p;
         v.vpos = vPos.p;
         const size_t stride = (size_t)vCapacity + 1;
         v.d = vVec.p;
@@ -726,6 +733,8 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(up(h->vSliceWidth, sliceWidth.data(), nSlices));
     chk(up(h->vCol, vCol.data(), vStore));
     chk(up(h->vVal, vVal.data(), vStore));
+    chk(h->vVal16.alloc(vStore));
+    chk(h->vG.alloc((size_t)h->vCapacity + 1));
     chk(up(h->vPos, vPos.data(), nnz));
     {
         const int32_t next = E0;
@@ -749,6 +758,7 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
         return fail(nullptr, TG_ERR_CUDA, msg);
     }
     launch_rebuild_rows(h->dm(), h->stream);
+    launch_vsys_derive(h->vs(), h->vVal.n, h->stream);
     if (h->ntets > 0) launch_pack_tets(h->dm(), h->tetpack.p, h->stream);
     const int rc = sync_status(h, "tg_create");
     if (rc != TG_OK) {
@@ -789,6 +799,7 @@ void tg_destroy(tg_handle* h) {
     h->normalBuf.release();
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
+    h->vVal16.release(); h->vG.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
     for (int r = 0; r < tg_handle::kRing; r++) {
         if (h->ringStream[r]) {
@@ -862,11 +873,11 @@ int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, d
         CK(cudaEventRecord(h->evStop, h->stream));
     } else if (which == 2) {
         // k_amg_fine (the multigrid's level-0 smoothing pass, t = b - A y
-        // over SELL-32): col + val per stored entry, and per row b, y (the
-        // gathers hit the same vector), d and the t write
+        // over SELL-32): col + bf16 val per stored entry, and per row b, y
+        // (the gathers hit the same vector), the row sum g and the t write
         if (!h->amgReady) return fail(h, TG_ERR_ARGUMENT, "tg_bench_kernel: no multigrid hierarchy yet");
         const double rows = (double)h->vActive, stored = h->vEntries;
-        *bytes = rows * (4 + 4 + 4 + 4) + stored * (4 + 4);
+        *bytes = rows * (4 + 4 + 4 + 4) + stored * (4 + 2);
         if (h->vScal.n < 8) CK(h->vScal.alloc(8));
         VSys v = h->vs();
         launch_amg_fine_residual(v, h->vActive, h->amg, h->stream);  // warm

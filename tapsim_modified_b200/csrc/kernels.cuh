@@ -10,6 +10,7 @@
 //   free rows  int32 lists grouped by colour, non-Neumann and Neumann apart
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -84,6 +85,8 @@ struct VSys {
     const int32_t* slice_width;   // [slices] entries per row in the slice
     int32_t* col;                 // slot of the neighbour (or the zero slot)
     float* val;                   // coupling as the row sees it
+    __nv_bfloat16* val16;         // the same rounded to bf16, for the multigrid's smoothing pass
+    float* g;                     // [capacity + 1] row sum: d minus the row's stored val
     int32_t* vpos;                // [nnz] global CSR entry -> storage index, -1
     float *d, *x, *r, *u, *w, *p, *sv;
     float* hist;                  // correction of the last event's solve (warm start)
@@ -147,6 +150,8 @@ void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes,
 // re-copies the couplings and diagonals that flips of the listed cells
 // changed into the V system (rows that existed before the flips)
 void launch_vsys_refresh(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
+// val16 and g of every slot from val and d (after the upload)
+void launch_vsys_derive(const VSys& v, size_t stored, cudaStream_t s);
 
 // ---- relaxation (relax.cu) ----
 // coloured Gauss-Seidel sweep of one row list, FP64, max |delta| to *maxdev
