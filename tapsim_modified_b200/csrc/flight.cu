@@ -113,20 +113,25 @@ __device__ void weights(const DevMesh& m, int t, V3 p, double w[4]) {
 // vertices at once instead of on first use).  Four lanes share a row; a
 // singular node stores NaN in x, which the flight reports as S_SINGULAR when
 // it interpolates from that vertex, as the on-demand computation would.
+// With a cell list, only the listed cells are computed: the event loop lists
+// the cells that are free or have a free neighbour, since the field of a
+// Dirichlet cell among Dirichlet cells depends only on potentials and
+// couplings that never change.
 constexpr int kLanesPerRow = 4;
-__global__ void k_vertex_fields(DevMesh m) {
+__global__ void k_vertex_fields(DevMesh m, const int32_t* __restrict__ cells, int count) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gid / kLanesPerRow;
+    const int t = gid / kLanesPerRow;
     const int lane = gid % kLanesPerRow;
-    const bool live = i < m.n;
-    const int ii = live ? i : m.n - 1;
+    const bool live = t < (cells ? count : m.n);
+    const int ii = live ? (cells ? cells[t] : t) : m.n - 1;
+    const int i = ii;
     const bool hull = (m.flags[ii] & F_HULL) != 0;
     const double xi = m.xyz[3 * ii], yi = m.xyz[3 * ii + 1], zi = m.xyz[3 * ii + 2];
     const double pi = m.phi64[ii];
     double a00 = 0, a01 = 0, a02 = 0, a11 = 0, a12 = 0, a22 = 0, b0 = 0, b1 = 0, b2 = 0;
     const int q1 = hull ? 0 : m.row_ptr[ii + 1];
     for (int q = (hull ? 0 : m.row_ptr[ii]) + lane; q < q1; q += kLanesPerRow) {
-        if (m.c64[q] == 0.0) continue;
+        if (m.cnz[q] == 0) continue;
         const int j = m.col[q];
         const double dx = (double)m.xyz[3 * j] - xi, dy = (double)m.xyz[3 * j + 1] - yi, dz = (double)m.xyz[3 * j + 2] - zi;
         const double dp = m.phi64[j] - pi;
@@ -726,11 +731,12 @@ void launch_trace(const DevMesh& m, int nIons, const float* start, const float* 
 void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s) {
     if (m.ntets > 0) { count_launch(); k_pack_tets<<<(m.ntets + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, pack); }
 }
-void launch_vertex_fields(const DevMesh& m, cudaStream_t s) {
-    if (m.n > 0) {
+void launch_vertex_fields(const DevMesh& m, cudaStream_t s, const int32_t* cells, int count) {
+    const long long items = cells ? count : m.n;
+    if (m.n > 0 && items > 0) {
         count_launch();
-        const long long threads = (long long)m.n * kLanesPerRow;
-        k_vertex_fields<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m);
+        const long long threads = items * kLanesPerRow;
+        k_vertex_fields<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m, cells, (int)items);
     }
 }
 void launch_trace_one(const DevMesh& m, const float start[3], const float vel[3], float qm, int guess, TraceParams tp,

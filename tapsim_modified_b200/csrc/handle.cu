@@ -124,6 +124,16 @@ struct tg_handle {
     DBuf<double> ringPhiBuf[kRing], ringField[kRing];
     int ringNext = 0;
     bool ringReady = false;
+    // the flights' vertex fields are recomputed only for the cells that are
+    // free or have a free neighbour (fieldCells, grown by removals on the
+    // host); a slot whose field array has not been filled for every cell
+    // since the potentials were last written takes the full pass
+    bool ringFull[kRing] = {};
+    DBuf<int32_t> fieldCells;
+    int fieldCount = 0;
+    bool fieldAll = false;             // a removal's list was cut short: all cells from then on
+    std::vector<uint8_t> h_fieldActive;
+    DBuf<uint8_t> cnz;
     std::vector<int32_t> h_row_ptr;
     std::vector<int32_t> h_col;  // the Delaunay neighbours never change
 
@@ -156,6 +166,7 @@ struct tg_handle {
         int32_t flipped[1024];
         int32_t counts[2 * kMaxColours];
         int32_t pending[4096];  // cells flipped since the last solve
+        int32_t activated[4096];  // cells a removal adds to fieldCells
     };
     Pinned* pin = nullptr;
     int vNext = 0;            // host mirror of the V system's slot counter
@@ -260,6 +271,7 @@ struct tg_handle {
         m.area_pos = area_pos.p;
         m.volume = volume.p;
         m.c64 = c64.p;
+        m.cnz = cnz.p;
         m.ceff64 = ceff64.p;
         m.ceff32 = ceff32.p;
         m.diag64 = diag64.p;
@@ -680,6 +692,26 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     chk(up(h->geom, geom.data(), nnz));
     if (d->volume) chk(up(h->volume, d->volume, n));
     chk(up(h->c64, d->coupling, nnz));
+    {
+        std::vector<uint8_t> nzv(nnz);
+        for (size_t q = 0; q < (size_t)nnz; q++) nzv[q] = d->coupling[q] != 0.0;
+        chk(up(h->cnz, nzv.data(), nnz));
+        // cells whose vertex field can change: free, or with a free neighbour
+        h->h_fieldActive.assign(n, 0);
+        std::vector<int32_t> cells;
+        for (int i = 0; i < n; i++) {
+            bool act = !(flags[i] & F_DIRICHLET);
+            for (int q = d->row_ptr[i]; q < d->row_ptr[i + 1] && !act; q++) act = !(flags[d->col[q]] & F_DIRICHLET);
+            if (act) {
+                h->h_fieldActive[i] = 1;
+                cells.push_back(i);
+            }
+        }
+        chk(h->fieldCells.alloc(n));
+        if (e == cudaSuccess && !cells.empty())
+            chk(cudaMemcpy(h->fieldCells.p, cells.data(), sizeof(int32_t) * cells.size(), cudaMemcpyHostToDevice));
+        h->fieldCount = (int)cells.size();
+    }
     chk(h->ceff64.alloc(nnz));
     chk(h->ceff32.alloc(nnz));
     chk(h->diag64.alloc(n));
@@ -776,6 +808,7 @@ void tg_destroy(tg_handle* h) {
     h->xyz.release(); h->type.release(); h->typeScratch.release(); h->flags.release(); h->area_pos.release();
     h->row_ptr.release(); h->col.release(); h->rev.release(); h->colour.release(); h->tet_v.release();
     h->tet_n.release(); h->node_tet.release(); h->geom.release(); h->volume.release(); h->c64.release();
+    h->cnz.release(); h->fieldCells.release();
     h->ceff64.release(); h->diag64.release(); h->q64.release(); h->phi64.release(); h->ceff32.release();
     h->diag32.release(); h->dtypes.release(); h->status.release(); h->rowsV.release(); h->rowsN.release();
     h->allV.release(); h->allN.release(); h->segStartD.release(); h->countVD.release(); h->countND.release();
@@ -903,6 +936,7 @@ int tg_get_phi(tg_handle* h, double* phi) {
 int tg_set_phi(tg_handle* h, const double* phi) {
     if (!h || !phi) return fail(h, TG_ERR_ARGUMENT, "tg_set_phi: null argument");
     CK(cudaMemcpyAsync(h->phi64.p, phi, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+    for (int r = 0; r < tg_handle::kRing; r++) h->ringFull[r] = true;  // Dirichlet potentials may have changed
     h->bnormValid = false;
     h->selValid = false;
     h->converged = h->histValid = h->residValid = false;
@@ -1751,6 +1785,34 @@ static int take_away_impl(tg_handle* h, int32_t node, int32_t capacity, int32_t*
             h->pendingOverflow = true;
         }
     }
+    // the flipped cells and their neighbours join the vertex-field cells
+    if (nd + 1 >= cap) {
+        h->fieldAll = true;
+    } else if (!h->fieldAll) {
+        std::vector<int32_t> act;
+        for (int k = -1; k < nd; k++) {
+            const int f = k < 0 ? node : pin->result[1 + k];
+            for (int q = h->h_row_ptr[f] - 1; q < h->h_row_ptr[f + 1]; q++) {
+                const int j = q < h->h_row_ptr[f] ? f : h->h_col[q];
+                if (!h->h_fieldActive[j]) {
+                    h->h_fieldActive[j] = 1;
+                    act.push_back(j);
+                }
+            }
+        }
+        if (!act.empty()) {
+            const size_t na = act.size();
+            if (na <= sizeof(pin->activated) / sizeof(int32_t)) {
+                std::memcpy(pin->activated, act.data(), sizeof(int32_t) * na);
+                CK(cudaMemcpyAsync(h->fieldCells.p + h->fieldCount, pin->activated, sizeof(int32_t) * na,
+                                   cudaMemcpyHostToDevice, h->stream));
+            } else {
+                CK(cudaMemcpy(h->fieldCells.p + h->fieldCount, act.data(), sizeof(int32_t) * na,
+                              cudaMemcpyHostToDevice));
+            }
+            h->fieldCount += (int)na;
+        }
+    }
     int nf = 0;
     if (!(h->h_type[node] >= 0 && h->types[h->h_type[node]].dirichlet == 0)) pin->flipped[nf++] = node;
     h->h_type[node] = (int8_t)h->vacuumId;
@@ -1916,6 +1978,7 @@ static int ring_ready(tg_handle* h) {
         CK(cudaEventRecord(h->ringDone[r], h->ringStream[r]));
         CK(h->ringPhiBuf[r].alloc(h->n));
         CK(h->ringField[r].alloc(3 * (size_t)h->n));
+        h->ringFull[r] = true;
     }
     h->ringReady = true;
     return TG_OK;
@@ -2086,7 +2149,12 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
             mt.phiTrace = h->ringPhiBuf[r].p;
             mt.vfield = h->ringField[r].p;
             mt.status = h->statusTrace.p;
-            launch_vertex_fields(mt, h->ringStream[r]);
+            if (h->ringFull[r] || h->fieldAll) {
+                launch_vertex_fields(mt, h->ringStream[r]);
+                h->ringFull[r] = false;
+            } else {
+                launch_vertex_fields(mt, h->ringStream[r], h->fieldCells.p, h->fieldCount);
+            }
             TraceParams tp = trace_params(h, &o->trace);
             if (o->path_cap > 0) {
                 // this event's slot of the batch

@@ -34,6 +34,7 @@ struct DevMesh {
     const uint8_t* area_pos;
     const double* volume;
     double* c64;
+    const uint8_t* cnz;           // [nnz] 1 where c64 != 0 (a flip never changes it)
     double* ceff64;
     float* ceff32;
     double* diag64;
@@ -245,7 +246,9 @@ struct ImpactOut {
 // packed tetrahedron records (32 words each) from tet_v, tet_n and xyz
 void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s);
 // field_o1 of every node from the current potentials into m.vfield
-void launch_vertex_fields(const DevMesh& m, cudaStream_t s);
+// vertex fields (field_o1 of every cell) into m.vfield; with cells, only the
+// listed cells (the others keep their values)
+void launch_vertex_fields(const DevMesh& m, cudaStream_t s, const int32_t* cells = nullptr, int count = 0);
 void launch_trace(const DevMesh& m, int nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s);
 // one ion from rest at start (values passed to the kernel)

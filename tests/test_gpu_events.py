@@ -107,6 +107,34 @@ def test_batched_events_match_single_events(ref_mesh):
         assert abs(a["voltage"] - b["voltage"]) <= 1e-5 * abs(a["voltage"])
 
 
+def test_batched_events_after_a_potential_write(ref_mesh):
+    """Event batches recompute their flights' vertex fields only for the cells
+    that are free or have a free neighbour; writing the potentials (Dirichlet
+    cells included) makes every flight slot refill all cells first.  The
+    records must equal those of single events, whose flights compute every
+    cell's field."""
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
+    opts = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
+    out = {}
+    for batched in (False, True):
+        g = Grid(ref_mesh)
+        g.solve(rel_tol=1e-10)
+        ev = Evaporation(g, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, warm_start=1))
+        recs = ev.run(5) if batched else [ev.step() for _ in range(5)]
+        g.set_potentials(g.potentials() * 1.25)
+        g.solve(rel_tol=1e-10)
+        recs += ev.run(10) if batched else [ev.step() for _ in range(10)]
+        out[batched] = recs
+        g.close()
+    assert len(out[False]) == len(out[True]) == 15
+    for a, b in zip(out[False], out[True]):
+        assert a["node"] == b["node"]
+        assert a["status"] == b["status"] == 5
+        sa, sb = np.array(a["stop"]), np.array(b["stop"])
+        assert np.linalg.norm(sa - sb) <= 1e-5 * np.linalg.norm(sa)
+        assert abs(a["tof"] - b["tof"]) <= 1e-5 * abs(a["tof"])
+
+
 @pytest.mark.parametrize("integrator,stepper", [(1, 2), (1, 3), (0, 1)])
 def test_trajectory_modes_match_reference(ref_mesh, integrator, stepper):
     """Events with TRAJECTORY_INTEGRATOR_TYPE / TRAJECTORY_STEPPER_TYPE set,
