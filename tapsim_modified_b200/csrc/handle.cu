@@ -167,6 +167,7 @@ struct tg_handle {
         int32_t counts[2 * kMaxColours];
         int32_t pending[4096];  // cells flipped since the last solve
         int32_t activated[4096];  // cells a removal adds to fieldCells
+        int32_t status[4];        // the device status word, read with each sync
     };
     Pinned* pin = nullptr;
     int vNext = 0;            // host mirror of the V system's slot counter
@@ -348,13 +349,22 @@ int cuda_check(tg_handle* h, cudaError_t e, const char* where) {
 // Synchronises the stream and maps the device status word to a code.
 int status_code(tg_handle* h, int st, const char* where);
 
+// The status word comes back in the same stream-ordered copy as the
+// sync, into pinned memory: one round trip per check.
 int sync_status(tg_handle* h, const char* where) {
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(h->stream));
     int st = 0;
-    CK(cudaMemcpy(&st, h->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h->pin) {
+        CK(cudaMemcpyAsync(&h->pin->status[0], h->status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        st = h->pin->status[0];
+    } else {
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaMemcpy(&st, h->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    }
     if (st == 0) return TG_OK;
-    CK(cudaMemset(h->status.p, 0, sizeof(int)));
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return status_code(h, st, where);
 }
 
