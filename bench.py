@@ -273,7 +273,8 @@ def run_ours(args, rank: int, world: int, dist):
         learned = run_arm(2, learner)
         learned["grid"].close()
         learner.close()
-    # the headline arm: the fastest start measured, the recycled far field
+    # the headline arm: the recycled far field (warm_start 1); the plain and
+    # learned starts are timed on the same tip beside it
     arm = run_arm(1)
     grid, info0, dev_s, t_e2e, phi, clocks = (arm[k] for k in ("grid", "info0", "dev_s", "t_e2e", "phi", "clocks"))
     launches = arm["launches"]
@@ -326,8 +327,8 @@ def run_ours(args, rank: int, world: int, dist):
                         f"{TIPS[args.tip]['half_angle_deg']:g} deg, vacuum to 1 um; {atoms} atoms, "
                         f"{mesh.num_nodes} cells per GPU; relax to rel. residual <= {REL_TOL:g} every event; "
                         "solve started from the previous event's correction (recycled far field, warm_start 1)",
-            "value_arm": "recycled far field (warm_start 1): the fastest start measured; the learned arm "
-                         "(warm_start 2) is in config.learned",
+            "value_arm": "recycled far field (warm_start 1); the plain start (warm_start 0) is in "
+                         "config.plain and the learned start (warm_start 2) in config.learned, timed on the same tip",
             "events_per_gpu": args.steps,
             "plain": {"value": ev_total / plain_max, "ms_per_step": plain_max * 1e3 / args.steps,
                       "solver_iterations_median": statistics.median(iters_plain),
