@@ -1,6 +1,6 @@
 """Evaporation-event throughput of the device hot path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--tip config2|config1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--tip tip15|tip5]
 
 A step is one evaporation event of the reference's loop (Process::evaporation
 steps I-VI): field ratio + argmax over the surface, removal of the chosen
@@ -35,11 +35,13 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "events/s at 3M-atom tip: learned warm-start vs plain relax, same GPU, resid<=1e-8"
 TIPS = {
-    # r=15 nm cap, 40 nm shank, 10 deg half angle, vacuum to 1 um
-    "config2": dict(cap_radius=15e-9, shank_length=40e-9, half_angle_deg=10.0, fine_shell=5e-9,
+    # the timed tip: r=15 nm cap, 40 nm shank, 10 deg half angle, vacuum to
+    # 1 um (4.06M atoms, 7.3M cells)
+    "tip15": dict(cap_radius=15e-9, shank_length=40e-9, half_angle_deg=10.0, fine_shell=5e-9,
                     box_half_width=0.5e-6, box_height=1.0e-6),
-    # r=5 nm cap on a 10 nm cylinder
-    "config1": dict(cap_radius=5e-9, shank_length=10e-9, half_angle_deg=0.0, fine_shell=3e-9,
+    # r=5 nm cap on a 10 nm cylinder, the size the reference's CPU path
+    # relaxes in minutes
+    "tip5": dict(cap_radius=5e-9, shank_length=10e-9, half_angle_deg=0.0, fine_shell=3e-9,
                     box_half_width=0.5e-6, box_height=1.0e-6),
     # small tip (1.06M cells): SpMV stream about 75 MB, inside L2
     "mid": dict(cap_radius=8e-9, shank_length=20e-9, half_angle_deg=5.0, fine_shell=3e-9,
@@ -384,8 +386,8 @@ def run_ours(args, rank: int, world: int, dist):
     }
     if not args.no_cpu_baseline and world == 1:
         try:
-            with tempfile.TemporaryDirectory(dir=str(ROOT / "gpurun_out") if (ROOT / "gpurun_out").exists()
-                                             else None) as td:
+            # beside the repository: the dump of the timed tip is a few hundred MB
+            with tempfile.TemporaryDirectory(prefix=".bench-", dir=str(ROOT)) as td:
                 dump = Path(td) / "bench.dump"
                 cfg = Path(td) / "bench.cfg"
                 mesh.write_dump(str(dump), phi.astype(np.float32))
@@ -409,7 +411,7 @@ def run_reference(args, rank: int, world: int):
 
     mesh = build_mesh(args.tip, seed=1)
     from tapsim_modified_b200.tapsim import Grid  # noqa: F401  (potentials come from the mesh presets)
-    with tempfile.TemporaryDirectory() as td:
+    with tempfile.TemporaryDirectory(prefix=".bench-", dir=str(ROOT)) as td:
         dump = Path(td) / "ref.dump"
         cfg = Path(td) / "ref.cfg"
         mesh.write_dump(str(dump))
@@ -447,7 +449,7 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--tip", default="config2", choices=sorted(TIPS))
+    ap.add_argument("--tip", default="tip15", choices=sorted(TIPS))
     ap.add_argument("--cpu-events", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
