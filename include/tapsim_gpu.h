@@ -415,6 +415,21 @@ int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, d
  * B[N x K]^T with A, B BF16 bit patterns, row-major; M % 128 == 0,
  * N in {64, 128}, K % 64 == 0. */
 int tg_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, int32_t M, int32_t N, int32_t K);
+/* The multigrid hierarchy that tg_solve builds for preconditioner 1, built on
+ * the host from a matrix the caller gives (a check hook; no counterpart in
+ * the reference, no device work): row_ptr / col / val hold a symmetric
+ * n x n M-matrix in CSR with its diagonal. */
+typedef struct tg_amg_host tg_amg_host;
+int tg_amg_host_build(int32_t n, const int32_t* row_ptr, const int32_t* col, const double* val, tg_amg_host** out);
+/* Levels, the finest (the matrix given) and the coarsest included. */
+int32_t tg_amg_host_levels(const tg_amg_host* a);
+/* One matrix of a level in CSR: which 0 = the level's operator A, 1 = its
+ * prolongator P (rows x the next level's rows), 2 = its restriction R = P^T
+ * (the coarsest level has only A).  Null arrays are skipped, so a first call
+ * with rows / cols / nnz alone sizes the second. */
+int tg_amg_host_matrix(const tg_amg_host* a, int32_t level, int32_t which, int32_t* rows, int32_t* cols, int64_t* nnz,
+                       int32_t* ptr, int32_t* col, double* val);
+void tg_amg_host_destroy(tg_amg_host* a);
 
 /* ---- host-side mesh building (setup, not device work) ------------------ */
 typedef struct tg_mesh tg_mesh;

@@ -18,6 +18,7 @@ ERRORS = {
     6: "TG_ERR_RELAX_FAULT", 7: "TG_ERR_ITERATION_CAP", 8: "TG_ERR_OUTSIDE", 9: "TG_ERR_WALK_LIMIT",
     10: "TG_ERR_NO_SURFACE", 11: "TG_ERR_HOST", 12: "TG_ERR_UNKNOWN_TYPE",
 }
+TG_ERR_ARGUMENT = 1
 TG_ERR_RELAX_FAULT = 6
 TG_ERR_ITERATION_CAP = 7
 TG_ERR_NO_SURFACE = 10
@@ -162,6 +163,11 @@ SIGNATURES = {
     "tg_launch_count": (C.c_int64, [_P]),
     "tg_bench_kernel": (C.c_int, [_P, _I, _I, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
     "tg_gemm_bf16": (C.c_int, [_P, _P, _P, _I, _I, _I]),
+    "tg_amg_host_build": (C.c_int, [_I, _P, _P, _P, C.POINTER(C.c_void_p)]),
+    "tg_amg_host_levels": (C.c_int32, [_P]),
+    "tg_amg_host_matrix": (C.c_int, [_P, _I, _I, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                     _P, _P, _P]),
+    "tg_amg_host_destroy": (None, [_P]),
     "tg_learner_create": (C.c_int, [_I, _I, _I, C.c_uint64, C.POINTER(C.c_void_p)]),
     "tg_learner_destroy": (None, [_P]),
     "tg_learner_last_error": (C.c_char_p, [_P]),

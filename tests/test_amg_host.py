@@ -1,0 +1,171 @@
+"""The multigrid hierarchy of the inner solve's preconditioner, built on the
+host (csrc/host/amg.cpp through tg_amg_host_build) from a seeded 3D
+finite-volume M-matrix, checked without a device:
+
+- level 0 is the matrix given, and every restriction is the transpose of its
+  prolongator;
+- every coarse operator is the Galerkin product R A P with its weak entries
+  (|g_ij| < 0.01 sqrt(g_ii g_jj)) lumped into the diagonal: kept entries are
+  the product's, row sums are the product's, and the operator is symmetric;
+- coarsening stops at 1,000 rows or fewer;
+- the V(1,1)-cycle the device runs (damped Jacobi 0.9 on both sides, a dense
+  solve on the coarsest level), restated here in numpy, preconditions CG to
+  a relative residual of 1e-8 in a small fraction of the Jacobi-CG
+  iterations."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from tapsim_modified_b200 import _native as N
+
+DROP = 0.01       # AmgOptions::coarse_drop
+SMOOTH = 0.9      # the device cycle's damped-Jacobi weight
+
+
+def _poisson(m=32, seed=5):
+    """7-point finite-volume operator on an m^3 grid: seeded couplings in
+    [0.5, 2] and a Dirichlet coupling to the outside on boundary faces."""
+    rng = np.random.default_rng(seed)
+    n = m ** 3
+    idx = np.arange(n).reshape(m, m, m)
+    rows, cols, vals = [], [], []
+    diag = np.zeros(n)
+    for axis in range(3):
+        a = np.moveaxis(idx, axis, 0)
+        i, j = a[:-1].ravel(), a[1:].ravel()
+        c = rng.uniform(0.5, 2.0, i.size)
+        rows += [i, j]
+        cols += [j, i]
+        vals += [-c, -c]
+        np.add.at(diag, i, c)
+        np.add.at(diag, j, c)
+        for face in (a[0].ravel(), a[-1].ravel()):
+            np.add.at(diag, face, rng.uniform(0.5, 2.0, face.size))
+    rows.append(np.arange(n))
+    cols.append(np.arange(n))
+    vals.append(diag)
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    A.sort_indices()
+    return A
+
+
+def _matrix(h, level, which):
+    rows, cols, nnz = C.c_int32(), C.c_int32(), C.c_int64()
+    L = N.lib()
+    assert L.tg_amg_host_matrix(h, level, which, C.byref(rows), C.byref(cols), C.byref(nnz), None, None, None) == 0
+    ptr = np.empty(rows.value + 1, np.int32)
+    col = np.empty(nnz.value, np.int32)
+    val = np.empty(nnz.value, np.float64)
+    assert L.tg_amg_host_matrix(h, level, which, C.byref(rows), C.byref(cols), C.byref(nnz), N.ptr(ptr), N.ptr(col),
+                                N.ptr(val)) == 0
+    return sp.csr_matrix((val, col, ptr), shape=(rows.value, cols.value))
+
+
+@pytest.fixture(scope="module")
+def hierarchy():
+    A = _poisson()
+    ptr, col, val = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64)
+    h = C.c_void_p()
+    L = N.lib()
+    assert L.tg_amg_host_build(A.shape[0], N.ptr(ptr), N.ptr(col), N.ptr(val), C.byref(h)) == 0
+    levels = L.tg_amg_host_levels(h)
+    As = [_matrix(h, l, 0) for l in range(levels)]
+    Ps = [_matrix(h, l, 1) for l in range(levels - 1)]
+    Rs = [_matrix(h, l, 2) for l in range(levels - 1)]
+    with pytest.raises(AssertionError):
+        _matrix(h, levels - 1, 1)  # the coarsest level has no prolongator
+    L.tg_amg_host_destroy(h)
+    return A, As, Ps, Rs
+
+
+def test_levels_and_transfer_operators(hierarchy):
+    A, As, Ps, Rs = hierarchy
+    assert len(As) >= 3
+    assert (As[0] != A).nnz == 0
+    assert As[-1].shape[0] <= 1000
+    for l, (P, R) in enumerate(zip(Ps, Rs)):
+        assert P.shape == (As[l].shape[0], As[l + 1].shape[0])
+        assert (R != P.T.tocsr()).nnz == 0, l
+
+
+def test_coarse_operators_are_truncated_galerkin_products(hierarchy):
+    _, As, Ps, Rs = hierarchy
+    dropped = 0
+    for l in range(len(Ps)):
+        G = (Rs[l] @ As[l] @ Ps[l]).tocsr()
+        Ac = As[l + 1].tocsr()
+        scale = np.abs(G).max()
+        assert abs(Ac - Ac.T).max() <= 1e-12 * scale, l
+        g = G.diagonal()
+        # kept off-diagonal entries are the product's
+        coo = Ac.tocoo()
+        off = coo.row != coo.col
+        gk = np.asarray(G[coo.row[off], coo.col[off]]).ravel()
+        assert np.abs(coo.data[off] - gk).max() <= 1e-12 * scale, l
+        # the product's entries that are missing are the weak ones
+        D = (G - Ac).tocoo()
+        miss = (D.row != D.col) & (np.abs(D.data) > 1e-12 * scale)
+        assert np.all(np.abs(D.data[miss]) < DROP * np.sqrt(g[D.row[miss]] * g[D.col[miss]])), l
+        dropped += int(miss.sum())
+        # lumping keeps every row sum
+        rs_g = np.asarray(G.sum(axis=1)).ravel()
+        rs_a = np.asarray(Ac.sum(axis=1)).ravel()
+        assert np.abs(rs_a - rs_g).max() <= 1e-10 * np.abs(G).sum(axis=1).max(), l
+    assert dropped > 0
+
+
+def _pcg(A, b, prec, tol=1e-8, maxit=2000):
+    x = np.zeros_like(b)
+    r = b.copy()
+    z = prec(r)
+    p = z.copy()
+    rz = r @ z
+    b2 = b @ b
+    for it in range(1, maxit + 1):
+        q = A @ p
+        alpha = rz / (p @ q)
+        x += alpha * p
+        r -= alpha * q
+        if r @ r <= tol * tol * b2:
+            return it, x
+        z = prec(r)
+        rz_new = r @ z
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+    return maxit, x
+
+
+def test_v_cycle_preconditions_cg(hierarchy):
+    A, As, Ps, Rs = hierarchy
+    coarse_inv = np.linalg.inv(As[-1].toarray())
+    diags = [M.diagonal() for M in As]
+
+    def cycle(l, b):
+        if l == len(As) - 1:
+            return coarse_inv @ b
+        y = SMOOTH * b / diags[l]
+        t = b - As[l] @ y
+        y = y + Ps[l] @ cycle(l + 1, Rs[l] @ t)
+        return y + SMOOTH * (b - As[l] @ y) / diags[l]
+
+    b = np.random.default_rng(11).standard_normal(A.shape[0])
+    it_mg, x = _pcg(A, b, lambda r: cycle(0, r))
+    assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+    d = A.diagonal()
+    it_j, _ = _pcg(A, b, lambda r: r / d)
+    print("CG iterations to 1e-8: multigrid", it_mg, "Jacobi", it_j)
+    assert it_mg <= 25
+    assert it_mg <= 0.25 * it_j
+
+
+def test_bad_input_is_rejected():
+    L = N.lib()
+    h = C.c_void_p()
+    ptr = np.array([0, 1, 2], np.int32)
+    col = np.array([0, 5], np.int32)  # column out of range
+    val = np.array([1.0, 1.0])
+    assert L.tg_amg_host_build(2, N.ptr(ptr), N.ptr(col), N.ptr(val), C.byref(h)) == N.TG_ERR_ARGUMENT
+    assert not h.value
+    assert L.tg_amg_host_levels(None) == 0
