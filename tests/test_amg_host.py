@@ -11,7 +11,8 @@ finite-volume M-matrix, checked without a device:
 - the V(1,1)-cycle the device runs (damped Jacobi 0.9 on both sides, a dense
   solve on the coarsest level), restated here in numpy, preconditions CG to
   a relative residual of 1e-8 in a small fraction of the Jacobi-CG
-  iterations."""
+  iterations, with the exact level-0 operator and with the one the device's
+  smoothing pass applies (bf16 couplings, FP32 row sums)."""
 import ctypes as C
 
 import numpy as np
@@ -137,25 +138,60 @@ def _pcg(A, b, prec, tol=1e-8, maxit=2000):
     return maxit, x
 
 
-def test_v_cycle_preconditions_cg(hierarchy):
+def _bf16(x):
+    """Round to the nearest bf16 (ties to even), returned as float32."""
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def _level0_bf16(A):
+    """The operator the device's level-0 smoothing pass applies: FP32
+    couplings rounded to bf16, and the diagonal g + sum of the rounded
+    couplings, g being the FP32 operator's row sum."""
+    A32 = A.astype(np.float32).tocsr()
+    d = A32.diagonal().astype(np.float64)
+    off = A32 - sp.diags(A32.diagonal())
+    off.eliminate_zeros()
+    a = -off.data                                    # couplings, positive
+    g = d - np.asarray(sp.csr_matrix((a.astype(np.float64), off.indices, off.indptr), shape=A.shape).sum(axis=1)).ravel()
+    ah = _bf16(a).astype(np.float64)
+    Oh = sp.csr_matrix((ah, off.indices, off.indptr), shape=A.shape)
+    return (sp.diags(g + np.asarray(Oh.sum(axis=1)).ravel()) - Oh).tocsr()
+
+
+@pytest.mark.parametrize("level0", ["fp64", "bf16"])
+def test_v_cycle_preconditions_cg(hierarchy, level0):
     A, As, Ps, Rs = hierarchy
     coarse_inv = np.linalg.inv(As[-1].toarray())
     diags = [M.diagonal() for M in As]
+    ops = list(As)
+    if level0 == "bf16":
+        ops[0] = _level0_bf16(A)
+        # symmetric, with the FP32 operator's row sums, and within 2^-8 of it
+        # in every Rayleigh quotient
+        assert abs(ops[0] - ops[0].T).max() == 0.0
+        A32 = A.astype(np.float32).astype(np.float64)
+        assert np.abs(np.asarray(ops[0].sum(axis=1)).ravel() - np.asarray(A32.sum(axis=1)).ravel()).max() <= \
+            1e-6 * np.abs(A).sum(axis=1).max()
+        v = np.random.default_rng(3).standard_normal((A.shape[0], 8))
+        q = np.einsum("ij,ij->j", v, ops[0] @ v) / np.einsum("ij,ij->j", v, A @ v)
+        assert np.all(np.abs(q - 1.0) <= 2.0 ** -8), q
 
     def cycle(l, b):
         if l == len(As) - 1:
             return coarse_inv @ b
         y = SMOOTH * b / diags[l]
-        t = b - As[l] @ y
+        t = b - ops[l] @ y
         y = y + Ps[l] @ cycle(l + 1, Rs[l] @ t)
-        return y + SMOOTH * (b - As[l] @ y) / diags[l]
+        return y + SMOOTH * (b - ops[l] @ y) / diags[l]
 
     b = np.random.default_rng(11).standard_normal(A.shape[0])
     it_mg, x = _pcg(A, b, lambda r: cycle(0, r))
     assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
     d = A.diagonal()
     it_j, _ = _pcg(A, b, lambda r: r / d)
-    print("CG iterations to 1e-8: multigrid", it_mg, "Jacobi", it_j)
+    print("CG iterations to 1e-8 with the", level0, "level-0 operator: multigrid", it_mg, "Jacobi", it_j)
     assert it_mg <= 25
     assert it_mg <= 0.25 * it_j
 
