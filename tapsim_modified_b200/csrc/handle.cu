@@ -1300,7 +1300,8 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     if (!h || !o) return fail(h, TG_ERR_ARGUMENT, "tg_solve: null argument");
     int rc = TG_OK;
     DevMesh m = h->dm();
-    // ||b||^2 (after removals it changes) comes with the first residual
+    // ||b||^2 comes with the first residual of every solve (from a full pass
+    // or from the kept values) and holds until the next removal
     bool needB = !h->bnormValid;
     VSys vsys = h->vs();
     CGVectors vN = h->cg(1);
@@ -1387,7 +1388,10 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         if (outer == 0) inf.initial_rel_residual = rel;
         inf.outer = outer;
         inf.rel_residual = rel;
-        if (rel <= o->rel_tol) break;
+        // the first residual of a warm start taken from the kept values holds
+        // A hist in FP32 only: it is not the FP64 test and never ends the
+        // solve (the kept V-row values are also those before the start)
+        if (rel <= o->rel_tol && !(outer == 0 && incremental && warm)) break;
         if (outer >= o->max_outer) {
             if (info) *info = inf;
             if (learnCollect) learner_collect_cancel(h->learner);
