@@ -12,7 +12,9 @@ finite-volume M-matrix, checked without a device:
   solve on the coarsest level), restated here in numpy, preconditions CG to
   a relative residual of 1e-8 in a small fraction of the Jacobi-CG
   iterations, with the exact level-0 operator and with the one the device's
-  smoothing pass applies (bf16 couplings, FP32 row sums)."""
+  smoothing pass applies (bf16 couplings, FP32 row sums);
+- the same cycle on the inner system of a generated tip (an irregular
+  Voronoi graph), assembled from the mesh arrays as the device assembles it."""
 import ctypes as C
 
 import numpy as np
@@ -205,3 +207,68 @@ def test_bad_input_is_rejected():
     assert L.tg_amg_host_build(2, N.ptr(ptr), N.ptr(col), N.ptr(val), C.byref(h)) == N.TG_ERR_ARGUMENT
     assert not h.value
     assert L.tg_amg_host_levels(None) == 0
+
+
+def _tip_v_system():
+    """The inner system of a generated tip, as the device assembles it: rows
+    of the free non-Neumann cells, off-diagonals -c_ij to free non-Neumann
+    neighbours, and the diagonal sum c_ij over all non-Neumann neighbours
+    (Dirichlet ones included)."""
+    from conftest import SMALL_TIP
+    from tapsim_modified_b200.tapsim import Mesh
+    m = Mesh.from_tip(**dict(SMALL_TIP, cap_radius=4e-9, shank_length=6e-9, fine_shell=2e-9))
+    a = m.arrays()
+    n = m.num_nodes
+    dirichlet = np.array([a["types"][int(t)]["dirichlet"] for t in a["type"]], bool)
+    neumann = np.array([a["types"][int(t)]["neumann"] for t in a["type"]], bool)
+    rp, col, c = a["row_ptr"], a["col"], a["coupling"]
+    row = np.repeat(np.arange(n), np.diff(rp))
+    live = ~neumann[col]
+    diag = np.bincount(row[live], weights=c[live], minlength=n)
+    free = ~dirichlet & ~neumann
+    slot = np.full(n, -1)
+    slot[free] = np.arange(free.sum())
+    e = free[row] & free[col]
+    nv = int(free.sum())
+    A = sp.csr_matrix((np.concatenate([-c[e], diag[free]]),
+                       (np.concatenate([slot[row[e]], np.arange(nv)]), np.concatenate([slot[col[e]], np.arange(nv)]))),
+                      shape=(nv, nv))
+    A.sort_indices()
+    return A
+
+
+def test_tip_v_system_hierarchy_preconditions_cg():
+    """The same checks on the operator class the device solves: the V system
+    of a 116k-cell generated tip (irregular Voronoi graph, graded cells)."""
+    A = _tip_v_system()
+    assert abs(A - A.T).max() <= 1e-12 * abs(A).max()
+    ptr, col, val = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64)
+    h = C.c_void_p()
+    L = N.lib()
+    assert L.tg_amg_host_build(A.shape[0], N.ptr(ptr), N.ptr(col), N.ptr(val), C.byref(h)) == 0
+    levels = L.tg_amg_host_levels(h)
+    As = [_matrix(h, l, 0) for l in range(levels)]
+    Ps = [_matrix(h, l, 1) for l in range(levels - 1)]
+    L.tg_amg_host_destroy(h)
+    assert levels >= 3 and As[-1].shape[0] <= 1000
+    coarse_inv = np.linalg.inv(As[-1].toarray())
+    diags = [M.diagonal() for M in As]
+    ops = [_level0_bf16(A)] + As[1:]
+
+    def cycle(l, b):
+        if l == len(As) - 1:
+            return coarse_inv @ b
+        y = SMOOTH * b / diags[l]
+        t = b - ops[l] @ y
+        y = y + Ps[l] @ cycle(l + 1, Ps[l].T @ t)
+        return y + SMOOTH * (b - ops[l] @ y) / diags[l]
+
+    b = np.random.default_rng(13).standard_normal(A.shape[0])
+    it_mg, x = _pcg(A, b, lambda r: cycle(0, r))
+    assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+    d = A.diagonal()
+    it_j, _ = _pcg(A, b, lambda r: r / d)
+    print("tip V system", A.shape[0], "rows,", levels, "levels; CG iterations to 1e-8: multigrid", it_mg,
+          "Jacobi", it_j)
+    assert it_mg <= 30
+    assert it_mg <= 0.2 * it_j
