@@ -4,7 +4,11 @@ neighbours' and keeps every other row's residual and Dirichlet part from the
 last full pass.  Here the FP64 oracle removes atoms (with detachment, on the
 plain Fe tip and on one whose Cu solute is a free dielectric species), and
 the per-row residual and Dirichlet part before and after each removal may
-differ only on those rows."""
+differ only on those rows.
+
+The flights' vertex fields in event batches rest on a second premise, checked
+the same way: the field of a Dirichlet cell among Dirichlet cells never
+changes, and neither does the zero pattern of the couplings."""
 import numpy as np
 import pytest
 
@@ -66,3 +70,36 @@ def test_removals_change_only_flipped_rows_and_neighbours(kind, tmp_path):
         # relax so that the next removal starts from a converged state again
         o.solve(1e-10, 2_000_000, 1.9)
     assert changed_total > 12
+
+
+@pytest.mark.parametrize("kind", ["fe", "dielectric"])
+def test_fields_outside_the_listed_cells_never_change(kind, tmp_path):
+    """The flights' vertex fields in event batches are recomputed only for the
+    cells that are free or have a free neighbour, a list that removals grow
+    by the flipped cells and their neighbours.  The field of every cell left
+    off the list must keep its first value, and the zero pattern of the
+    couplings (all the fields read of them) must not change."""
+    from oracle import Oracle
+    o = Oracle(_mesh(kind, tmp_path).arrays())
+    o.solve(1e-10, 2_000_000, 1.9)
+    o.surface_init(0)
+    n = o.n
+    row = np.repeat(np.arange(n), np.diff(o.row_ptr))
+    free = ~np.array([o.types[int(t)].dirichlet for t in o.type], bool)
+    active = free | (np.bincount(row, weights=free[o.col].astype(float), minlength=n) > 0)
+    off = np.nonzero(~active)[0]
+    assert off.size > 0
+    first = {int(i): o.field_o1(int(i)).copy() for i in off}
+    pattern = o.c == 0.0
+    for k in range(12):
+        info, _ = o.select()
+        flipped = [info.candidate] + list(o.take_away(info.candidate, 0))
+        for f in flipped:
+            active[f] = True
+            active[o.col[o.row_ptr[f]:o.row_ptr[f + 1]]] = True
+        o.solve(1e-10, 2_000_000, 1.9)
+        assert np.array_equal(o.c == 0.0, pattern), k
+    still = [i for i in first if not active[i]]
+    assert len(still) > 0.5 * len(first)
+    for i in still:
+        assert np.array_equal(o.field_o1(i), first[i]), i
