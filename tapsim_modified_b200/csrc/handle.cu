@@ -14,6 +14,7 @@
 #include <mutex>
 
 #include <stdlib.h>
+#include <exception>
 #include <string>
 #include <vector>
 
@@ -1121,7 +1122,7 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
 // Builds the multigrid hierarchy of the V system as it is now (its slots in
 // use, their couplings and diagonals read back from the device) and
 // uploads it.
-static int amg_setup(tg_handle* h, double* seconds) {
+static int amg_setup_impl(tg_handle* h, double* seconds) {
     const auto t0 = std::chrono::steady_clock::now();
     h->amg_release();
     const int slots = h->vActive;
@@ -1238,6 +1239,16 @@ static int amg_setup(tg_handle* h, double* seconds) {
     h->amgSlots = slots;
     *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return TG_OK;
+}
+
+// the hierarchy build allocates on the host: no exception crosses the C ABI
+static int amg_setup(tg_handle* h, double* seconds) {
+    try {
+        return amg_setup_impl(h, seconds);
+    } catch (const std::exception& e) {
+        h->amg_release();
+        return fail(h, TG_ERR_HOST, std::string("tg_solve: multigrid setup: ") + e.what());
+    }
 }
 
 // Single-reduction PCG on the V system until rho = r.r falls below rtol^2

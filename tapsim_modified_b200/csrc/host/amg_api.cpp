@@ -3,6 +3,8 @@
 // the caller gives, so that its construction can be checked without a
 // device.  No counterpart in the reference.
 #include <cstring>
+#include <exception>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -37,18 +39,20 @@ int tg_amg_host_build(int32_t n, const int32_t* row_ptr, const int32_t* col, con
     const int32_t nnz = row_ptr[n];
     for (int32_t q = 0; q < nnz; q++)
         if (col[q] < 0 || col[q] >= n) return amg_fail("tg_amg_host_build: column out of range", TG_ERR_ARGUMENT);
-    tg_host::AmgCsr A;
-    A.rows = A.cols = n;
-    A.ptr.assign(row_ptr, row_ptr + n + 1);
-    A.col.assign(col, col + nnz);
-    A.val.assign(val, val + nnz);
-    auto* a = new tg_amg_host;
-    const std::string err = tg_host::amg_build(std::move(A), tg_host::AmgOptions(), &a->h);
-    if (!err.empty()) {
-        delete a;
-        return amg_fail("tg_amg_host_build: " + err, TG_ERR_HOST);
+    // no exception crosses the C ABI: an allocation failure is a host error
+    try {
+        tg_host::AmgCsr A;
+        A.rows = A.cols = n;
+        A.ptr.assign(row_ptr, row_ptr + n + 1);
+        A.col.assign(col, col + nnz);
+        A.val.assign(val, val + nnz);
+        std::unique_ptr<tg_amg_host> a(new tg_amg_host);
+        const std::string err = tg_host::amg_build(std::move(A), tg_host::AmgOptions(), &a->h);
+        if (!err.empty()) return amg_fail("tg_amg_host_build: " + err, TG_ERR_HOST);
+        *out = a.release();
+    } catch (const std::exception& e) {
+        return amg_fail(std::string("tg_amg_host_build: ") + e.what(), TG_ERR_HOST);
     }
-    *out = a;
     return TG_OK;
 }
 
