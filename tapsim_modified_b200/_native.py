@@ -22,6 +22,7 @@ TG_ERR_ARGUMENT = 1
 TG_ERR_RELAX_FAULT = 6
 TG_ERR_ITERATION_CAP = 7
 TG_ERR_NO_SURFACE = 10
+TG_ERR_HOST = 11
 
 
 class tg_type(C.Structure):

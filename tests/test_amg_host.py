@@ -272,3 +272,73 @@ def test_tip_v_system_hierarchy_preconditions_cg():
           "Jacobi", it_j)
     assert it_mg <= 30
     assert it_mg <= 0.2 * it_j
+
+
+def _build(A):
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    ptr, col, val = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64)
+    h = C.c_void_p()
+    rc = N.lib().tg_amg_host_build(A.shape[0], N.ptr(ptr), N.ptr(col), N.ptr(val), C.byref(h))
+    return rc, h
+
+
+def test_small_matrix_is_one_level():
+    """At most 1,000 rows: no coarsening, the matrix itself is the coarsest
+    level (inverted densely on the device), with no transfer operators."""
+    A = _poisson(m=8)  # 512 rows
+    rc, h = _build(A)
+    assert rc == 0
+    L = N.lib()
+    assert L.tg_amg_host_levels(h) == 1
+    assert (_matrix(h, 0, 0) != A).nnz == 0
+    rows = C.c_int32()
+    assert L.tg_amg_host_matrix(h, 0, 1, C.byref(rows), None, None, None, None, None) == N.TG_ERR_ARGUMENT
+    L.tg_amg_host_destroy(h)
+
+
+def test_rows_without_neighbours_and_disconnected_blocks():
+    """Rows without off-diagonal entries (cells whose neighbours are all
+    Dirichlet) stay out of the coarse levels, and two disconnected blocks are
+    coarsened apart: the prolongator has no entry that couples them, and the
+    hierarchy still preconditions CG."""
+    B = _poisson(m=14, seed=9)                       # 2,744 rows
+    iso = sp.diags(np.full(300, 3.0))                # isolated rows
+    A = sp.block_diag([B, iso, _poisson(m=14, seed=21)]).tocsr()
+    rc, h = _build(A)
+    assert rc == 0
+    L = N.lib()
+    levels = L.tg_amg_host_levels(h)
+    assert levels >= 2
+    As = [_matrix(h, l, 0) for l in range(levels)]
+    Ps = [_matrix(h, l, 1) for l in range(levels - 1)]
+    L.tg_amg_host_destroy(h)
+    nb = B.shape[0]
+    P = Ps[0].tocoo()
+    assert not np.any((P.row >= nb) & (P.row < nb + 300)), "isolated rows enter the coarse space"
+    first = set(P.col[P.row < nb].tolist())
+    second = set(P.col[P.row >= nb + 300].tolist())
+    assert first and second and not (first & second)
+    coarse_inv = np.linalg.inv(As[-1].toarray())
+    diags = [M.diagonal() for M in As]
+
+    def cycle(l, b):
+        if l == len(As) - 1:
+            return coarse_inv @ b
+        y = SMOOTH * b / diags[l]
+        t = b - As[l] @ y
+        y = y + Ps[l] @ cycle(l + 1, Ps[l].T @ t)
+        return y + SMOOTH * (b - As[l] @ y) / diags[l]
+
+    b = np.random.default_rng(2).standard_normal(A.shape[0])
+    it, x = _pcg(A, b, lambda r: cycle(0, r))
+    assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+    assert it <= 25
+
+
+def test_non_positive_diagonal_is_a_host_error():
+    A = _poisson(m=12).tolil()
+    A[5, 5] = -1.0
+    rc, h = _build(A)
+    assert rc == N.TG_ERR_HOST
+    assert not h.value
