@@ -1,6 +1,7 @@
 #include "amg.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <thread>
 
@@ -23,22 +24,41 @@ void parallel_rows(int n, int threads, F f) {
     for (auto& th : pool) th.join();
 }
 
-AmgCsr transpose(const AmgCsr& P) {
+// R = P^T.  Each thread takes a contiguous block of P's rows and writes its
+// entries after those of the blocks before it, so that every row of R lists
+// P's rows in ascending order, as a serial pass would.
+AmgCsr transpose(const AmgCsr& P, int threads) {
     AmgCsr R;
     R.rows = P.cols;
     R.cols = P.rows;
+    const int T = std::max(1, threads);
+    std::vector<std::vector<int32_t>> count(T);
+    parallel_rows(P.rows, T, [&](int b, int e, int t) {
+        count[t].assign(R.rows, 0);
+        for (int q = P.ptr[b]; q < P.ptr[e]; q++) count[t][P.col[q]]++;
+    });
     R.ptr.assign(R.rows + 1, 0);
-    for (int32_t c : P.col) R.ptr[c + 1]++;
-    for (int c = 0; c < R.rows; c++) R.ptr[c + 1] += R.ptr[c];
+    for (int c = 0; c < R.rows; c++) {
+        int32_t at = R.ptr[c];
+        for (int t = 0; t < T; t++) {
+            if (count[t].empty()) continue;
+            const int32_t k = count[t][c];
+            count[t][c] = at;  // becomes the block's next position in row c
+            at += k;
+        }
+        R.ptr[c + 1] = at;
+    }
     R.col.resize(P.col.size());
     R.val.resize(P.val.size());
-    std::vector<int32_t> next(R.ptr.begin(), R.ptr.end() - 1);
-    for (int i = 0; i < P.rows; i++)
-        for (int q = P.ptr[i]; q < P.ptr[i + 1]; q++) {
-            const int k = next[P.col[q]]++;
-            R.col[k] = i;
-            R.val[k] = P.val[q];
-        }
+    parallel_rows(P.rows, T, [&](int b, int e, int t) {
+        std::vector<int32_t>& next = count[t];
+        for (int i = b; i < e; i++)
+            for (int q = P.ptr[i]; q < P.ptr[i + 1]; q++) {
+                const int k = next[P.col[q]]++;
+                R.col[k] = i;
+                R.val[k] = P.val[q];
+            }
+    });
     return R;
 }
 
@@ -114,12 +134,15 @@ AmgCsr smoothed_prolongator(const AmgCsr& A, const std::vector<char>& strong, co
     // each row's entries (merged by aggregate) go to its slot of an
     // upper-bound layout (1 + its strong entries), then are compacted
     std::vector<int64_t> bound(n + 1, 0);
-    for (int i = 0; i < n; i++) {
-        int k = agg[i] < 0 ? 0 : 1;
-        if (agg[i] >= 0)
-            for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) k += strong[q] && A.col[q] != i;
-        bound[i + 1] = bound[i] + k;
-    }
+    parallel_rows(n, threads, [&](int b, int e, int) {
+        for (int i = b; i < e; i++) {
+            int k = agg[i] < 0 ? 0 : 1;
+            if (agg[i] >= 0)
+                for (int q = A.ptr[i]; q < A.ptr[i + 1]; q++) k += strong[q] && A.col[q] != i;
+            bound[i + 1] = k;
+        }
+    });
+    for (int i = 0; i < n; i++) bound[i + 1] += bound[i];
     std::vector<int32_t> tcol(bound[n]), cnt(n, 0);
     std::vector<double> tval(bound[n]);
     parallel_rows(n, threads, [&](int b, int e, int) {
@@ -168,91 +191,131 @@ AmgCsr smoothed_prolongator(const AmgCsr& A, const std::vector<char>& strong, co
     return P;
 }
 
-// A_c = R A P, one coarse row per step, dense accumulator per thread.
+// A_c = R A P, one coarse row per step, dense accumulator per thread.  The
+// rows go to the threads in blocks of 64 as they free up (row costs vary
+// with the aggregates' sizes), each thread appends its rows to a buffer of
+// its own, and the rows are then copied into place; every row is summed in
+// the same order whichever thread takes it.
 AmgCsr galerkin(const AmgCsr& R, const AmgCsr& A, const AmgCsr& P, int threads) {
     const int nc = R.rows;
-    std::vector<std::vector<std::pair<int32_t, double>>> rows(nc);
-    parallel_rows(nc, threads, [&](int b, int e, int) {
+    const int T = nc < 256 ? 1 : std::max(1, threads);
+    std::vector<int32_t> cnt(nc), owner(nc);
+    std::vector<int64_t> off(nc);
+    std::vector<std::vector<int32_t>> bufc(T);
+    std::vector<std::vector<double>> bufv(T);
+    std::atomic<int> next(0);
+    constexpr int kRowsPerTake = 64;
+    auto work = [&](int t) {
         std::vector<double> acc(nc, 0.0);
         std::vector<char> used(nc, 0);
         std::vector<int32_t> touched;
-        for (int c = b; c < e; c++) {
-            touched.clear();
-            for (int qr = R.ptr[c]; qr < R.ptr[c + 1]; qr++) {
-                const int i = R.col[qr];
-                const double rci = R.val[qr];
-                for (int qa = A.ptr[i]; qa < A.ptr[i + 1]; qa++) {
-                    const int k = A.col[qa];
-                    const double w = rci * A.val[qa];
-                    for (int qp = P.ptr[k]; qp < P.ptr[k + 1]; qp++) {
-                        const int cc = P.col[qp];
-                        if (!used[cc]) {
-                            used[cc] = 1;
-                            touched.push_back(cc);
+        std::vector<int32_t>& bc = bufc[t];
+        std::vector<double>& bv = bufv[t];
+        for (;;) {
+            const int b = next.fetch_add(kRowsPerTake);
+            if (b >= nc) break;
+            const int e = std::min(nc, b + kRowsPerTake);
+            for (int c = b; c < e; c++) {
+                touched.clear();
+                for (int qr = R.ptr[c]; qr < R.ptr[c + 1]; qr++) {
+                    const int i = R.col[qr];
+                    const double rci = R.val[qr];
+                    for (int qa = A.ptr[i]; qa < A.ptr[i + 1]; qa++) {
+                        const int k = A.col[qa];
+                        const double w = rci * A.val[qa];
+                        for (int qp = P.ptr[k]; qp < P.ptr[k + 1]; qp++) {
+                            const int cc = P.col[qp];
+                            if (!used[cc]) {
+                                used[cc] = 1;
+                                touched.push_back(cc);
+                            }
+                            acc[cc] += w * P.val[qp];
                         }
-                        acc[cc] += w * P.val[qp];
                     }
                 }
-            }
-            std::sort(touched.begin(), touched.end());
-            auto& out = rows[c];
-            out.reserve(touched.size());
-            for (int32_t cc : touched) {
-                out.emplace_back(cc, acc[cc]);
-                acc[cc] = 0.0;
-                used[cc] = 0;
+                std::sort(touched.begin(), touched.end());
+                owner[c] = t;
+                off[c] = (int64_t)bc.size();
+                cnt[c] = (int32_t)touched.size();
+                for (int32_t cc : touched) {
+                    bc.push_back(cc);
+                    bv.push_back(acc[cc]);
+                    acc[cc] = 0.0;
+                    used[cc] = 0;
+                }
             }
         }
-    });
+    };
+    if (T == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; t++) pool.emplace_back(work, t);
+        for (auto& th : pool) th.join();
+    }
     AmgCsr Ac;
     Ac.rows = Ac.cols = nc;
     Ac.ptr.assign(nc + 1, 0);
-    for (int c = 0; c < nc; c++) Ac.ptr[c + 1] = Ac.ptr[c] + (int32_t)rows[c].size();
+    for (int c = 0; c < nc; c++) Ac.ptr[c + 1] = Ac.ptr[c] + cnt[c];
     Ac.col.resize(Ac.ptr[nc]);
     Ac.val.resize(Ac.ptr[nc]);
-    for (int c = 0; c < nc; c++) {
-        int k = Ac.ptr[c];
-        for (const auto& e2 : rows[c]) {
-            Ac.col[k] = e2.first;
-            Ac.val[k] = e2.second;
-            k++;
+    parallel_rows(nc, threads, [&](int b, int e, int) {
+        for (int c = b; c < e; c++) {
+            const int32_t* sc = bufc[owner[c]].data() + off[c];
+            const double* sv = bufv[owner[c]].data() + off[c];
+            std::copy(sc, sc + cnt[c], Ac.col.begin() + Ac.ptr[c]);
+            std::copy(sv, sv + cnt[c], Ac.val.begin() + Ac.ptr[c]);
         }
-    }
+    });
     return Ac;
 }
 
 // Drops the entries |a_ij| < drop sqrt(a_ii a_jj) of a coarse operator and
 // adds them to a_ii, which keeps every row sum (and so the constants in the
 // near null space) as it was.  Rows without a positive diagonal are kept whole.
-void drop_weak(AmgCsr* A, double drop) {
+// Two passes over the rows in parallel: count the kept entries, then write
+// them (the dropped ones summed in row order, as one pass would).
+void drop_weak(AmgCsr* A, double drop, int threads) {
     const int n = A->rows;
     std::vector<double> diag(n, 0.0);
-    for (int i = 0; i < n; i++)
-        for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++)
-            if (A->col[q] == i) diag[i] = A->val[q];
-    std::vector<int32_t> ptr(n + 1, 0), col;
-    std::vector<double> val;
-    col.reserve(A->col.size());
-    val.reserve(A->val.size());
-    for (int i = 0; i < n; i++) {
-        int dpos = -1;
-        double lump = 0.0;
-        for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++) {
-            const int j = A->col[q];
-            const double a = A->val[q];
-            const bool keep = j == i || !(diag[i] > 0.0) || !(diag[j] > 0.0) ||
-                              std::fabs(a) >= drop * std::sqrt(diag[i] * diag[j]);
-            if (!keep) {
-                lump += a;
-                continue;
-            }
-            if (j == i) dpos = (int)col.size();
-            col.push_back(j);
-            val.push_back(a);
+    parallel_rows(n, threads, [&](int b, int e, int) {
+        for (int i = b; i < e; i++)
+            for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++)
+                if (A->col[q] == i) diag[i] = A->val[q];
+    });
+    auto keep = [&](int i, int q) {
+        const int j = A->col[q];
+        return j == i || !(diag[i] > 0.0) || !(diag[j] > 0.0) ||
+               std::fabs(A->val[q]) >= drop * std::sqrt(diag[i] * diag[j]);
+    };
+    std::vector<int32_t> ptr(n + 1, 0);
+    parallel_rows(n, threads, [&](int b, int e, int) {
+        for (int i = b; i < e; i++) {
+            int32_t k = 0;
+            for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++) k += keep(i, q);
+            ptr[i + 1] = k;
         }
-        if (dpos >= 0) val[dpos] += lump;
-        ptr[i + 1] = (int32_t)col.size();
-    }
+    });
+    for (int i = 0; i < n; i++) ptr[i + 1] += ptr[i];
+    std::vector<int32_t> col(ptr[n]);
+    std::vector<double> val(ptr[n]);
+    parallel_rows(n, threads, [&](int b, int e, int) {
+        for (int i = b; i < e; i++) {
+            int32_t k = ptr[i], dpos = -1;
+            double lump = 0.0;
+            for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++) {
+                if (!keep(i, q)) {
+                    lump += A->val[q];
+                    continue;
+                }
+                if (A->col[q] == i) dpos = k;
+                col[k] = A->col[q];
+                val[k] = A->val[q];
+                k++;
+            }
+            if (dpos >= 0) val[dpos] += lump;
+        }
+    });
     A->ptr.swap(ptr);
     A->col.swap(col);
     A->val.swap(val);
@@ -323,9 +386,9 @@ std::string amg_build(AmgCsr&& A0, const AmgOptions& opt, AmgHierarchy* out) {
                 break;
             }
             L.P = smoothed_prolongator(A, strong, agg, nc, opt.omega, threads);
-            L.R = transpose(L.P);
+            L.R = transpose(L.P, threads);
             AmgCsr Ac = galerkin(L.R, A, L.P, threads);
-            if (opt.coarse_drop > 0.0) drop_weak(&Ac, opt.coarse_drop);
+            if (opt.coarse_drop > 0.0) drop_weak(&Ac, opt.coarse_drop, threads);
             L.A = std::move(A);
             out->levels.push_back(std::move(L));
             A = std::move(Ac);
