@@ -450,7 +450,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tip", default="tip15", choices=sorted(TIPS))
-    ap.add_argument("--cpu-events", type=int, default=6)
+    # about 10 s of the reference's per-event work on the 16 host cores (the
+    # median event time of the sample gives the rate)
+    ap.add_argument("--cpu-events", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
     ap.add_argument("--train-steps", type=int, default=600, help="Adam steps of the learned warm start")
