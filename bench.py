@@ -404,6 +404,101 @@ def run_ours(args, rank: int, world: int, dist):
     return out
 
 
+def hop_ball(row_ptr, col, site: int, hops: int):
+    """Cells within `hops` steps of `site` in the cell graph (site included)."""
+    import numpy as np
+    seen = np.zeros(len(row_ptr) - 1, bool)
+    seen[site] = True
+    front = np.array([site], np.int64)
+    for _ in range(hops):
+        nb = np.concatenate([col[row_ptr[i]:row_ptr[i + 1]] for i in front]) if len(front) else front
+        nb = np.unique(nb)
+        nb = nb[~seen[nb]]
+        seen[nb] = True
+        front = nb
+    return seen
+
+
+def run_warm_bounds(args):
+    """Upper bounds of warm starts under the solver the events use (multigrid
+    PCG to a relative residual of 1e-8).  Two grids of the same tip run the
+    same events in lockstep: grid A takes the plain path, which gives each
+    event's exact correction d_k = phi_post - phi_pre; grid B, after the same
+    removal, is set to a constructed start and re-solved, once per start:
+
+      plain          phi_pre
+      recycled       phi_pre + d_{k-1}            (previous event's correction)
+      exact_ball6    phi_pre + d_k on the 6-hop ball of the removed atom
+      exact_ball12   phi_pre + d_k on the 12-hop ball
+      ball6+recycled phi_pre + d_k on the 6-hop ball, d_{k-1} elsewhere
+      exact          phi_pre + d_k everywhere      (ceiling of any warm start)
+
+    Every start's solve takes the full FP64 first residual (the potentials
+    were written), so the starts differ only in where they begin.  Prints one
+    JSON line: per start, the median inner iterations and the median solve
+    time on the host clock (the call synchronises)."""
+    import numpy as np
+    import torch
+
+    from tapsim_modified_b200.tapsim import Grid
+
+    torch.cuda.set_device(0)
+    mesh = build_mesh(args.tip, seed=tip_seed(0))
+    arr = mesh.arrays()
+    row_ptr, col = arr["row_ptr"], arr["col"]
+    A, B = Grid(mesh), Grid(mesh)
+    for g in (A, B):
+        g.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
+        g.surface_init(0)
+    starts = ["plain", "recycled", "exact_ball6", "exact_ball12", "ball6+recycled", "exact"]
+    rows = {s: [] for s in starts}
+    plain_path = []
+    d_prev = None
+    for k in range(args.warmup + args.steps):
+        phi_pre = A.potentials()
+        sa, sb = A.select(), B.select()
+        if sa.candidate != sb.candidate:
+            raise RuntimeError(f"grids diverged at event {k}: {sa.candidate} vs {sb.candidate}")
+        c = sa.candidate
+        A.take_away(c)
+        B.take_away(c)
+        t0 = time.perf_counter()
+        info = A.solve(REL_TOL, 50, 20000, 1e-4, warm_start=0, preconditioner=PRECOND)
+        t_plain = time.perf_counter() - t0
+        phi_post = A.potentials()
+        d = phi_post - phi_pre
+        if k >= args.warmup and d_prev is not None:
+            plain_path.append((info.inner, t_plain))
+            b6 = hop_ball(row_ptr, col, c, 6)
+            b12 = hop_ball(row_ptr, col, c, 12)
+            cand = {"plain": phi_pre, "recycled": phi_pre + d_prev, "exact_ball6": phi_pre + np.where(b6, d, 0.0),
+                    "exact_ball12": phi_pre + np.where(b12, d, 0.0),
+                    "ball6+recycled": phi_pre + np.where(b6, d, d_prev), "exact": phi_post}
+            for s in starts:
+                B.set_potentials(cand[s])
+                t0 = time.perf_counter()
+                bi = B.solve(REL_TOL, 50, 20000, 1e-4, warm_start=0, preconditioner=PRECOND)
+                rows[s].append((bi.inner, time.perf_counter() - t0, bi.initial_rel_residual, int(b6.sum()),
+                                int(b12.sum())))
+        B.set_potentials(phi_post)
+        d_prev = d
+    out = {"impl": "warm_bounds", "workload": args.tip, "cells": mesh.num_nodes, "events": len(plain_path),
+           "rel_tol": REL_TOL, "preconditioner": "multigrid V(1,1)" if PRECOND == 1 else "Jacobi",
+           "plain_event_path": {"inner_median": statistics.median(x[0] for x in plain_path),
+                                "solve_ms_median": 1e3 * statistics.median(x[1] for x in plain_path)},
+           "starts": {s: {"inner_median": statistics.median(r[0] for r in v),
+                          "inner_mean": statistics.mean(r[0] for r in v),
+                          "solve_ms_median": 1e3 * statistics.median(r[1] for r in v),
+                          "initial_rel_residual_median": statistics.median(r[2] for r in v)}
+                      for s, v in rows.items()},
+           "ball_cells_median": {"6": statistics.median(r[3] for r in rows["plain"]),
+                                 "12": statistics.median(r[4] for r in rows["plain"])},
+           "note": "each start's solve includes a full FP64 residual pass (the potentials were written)"}
+    A.close()
+    B.close()
+    return out
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return None
@@ -457,6 +552,8 @@ def main():
     ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
     ap.add_argument("--train-steps", type=int, default=600, help="Adam steps of the learned warm start")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
+    ap.add_argument("--warm-bounds", action="store_true",
+                    help="measure the iterations of exact and recycled starts instead of the events/s line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -468,7 +565,9 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(minutes=20))
-    if args.impl == "reference":
+    if args.warm_bounds:
+        out = run_warm_bounds(args) if rank == 0 else None
+    elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:
         out = run_ours(args, rank, world, dist)

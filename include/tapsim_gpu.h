@@ -430,6 +430,11 @@ int32_t tg_amg_host_levels(const tg_amg_host* a);
 int tg_amg_host_matrix(const tg_amg_host* a, int32_t level, int32_t which, int32_t* rows, int32_t* cols, int64_t* nnz,
                        int32_t* ptr, int32_t* col, double* val);
 void tg_amg_host_destroy(tg_amg_host* a);
+/* Test hook, no counterpart in the reference: while on is non-zero, one
+ * worker thread of every threaded pass of tg_amg_host_build (and of the
+ * hierarchy tg_solve builds) throws std::bad_alloc, as an allocation failure
+ * in that thread would.  The build must report TG_ERR_HOST, not terminate. */
+void tg_amg_host_inject_worker_failure(int32_t on);
 
 /* ---- host-side mesh building (setup, not device work) ------------------ */
 typedef struct tg_mesh tg_mesh;

@@ -169,6 +169,7 @@ SIGNATURES = {
     "tg_amg_host_matrix": (C.c_int, [_P, _I, _I, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                      _P, _P, _P]),
     "tg_amg_host_destroy": (None, [_P]),
+    "tg_amg_host_inject_worker_failure": (None, [_I]),
     "tg_learner_create": (C.c_int, [_I, _I, _I, C.c_uint64, C.POINTER(C.c_void_p)]),
     "tg_learner_destroy": (None, [_P]),
     "tg_learner_last_error": (C.c_char_p, [_P]),

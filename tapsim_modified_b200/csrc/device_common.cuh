@@ -6,6 +6,27 @@
 
 namespace tgd {
 
+// Makes device dev current for a scope (dev < 0: leaves the current device
+// alone) and gives the caller's current device back at the scope's end.  A
+// handle's buffers, streams and events live on the device that was current
+// when it was created; the entry points run under one of these, so a caller
+// whose current device is another one still reaches the handle's memory.
+struct ScopedDevice {
+    int prev = -1;
+    explicit ScopedDevice(int dev) {
+        if (dev < 0 || cudaGetDevice(&prev) != cudaSuccess || prev == dev) {
+            prev = -1;
+            return;
+        }
+        if (cudaSetDevice(dev) != cudaSuccess) prev = -1;
+    }
+    ~ScopedDevice() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    ScopedDevice(const ScopedDevice&) = delete;
+    ScopedDevice& operator=(const ScopedDevice&) = delete;
+};
+
 // per-node flag bits
 enum : uint8_t {
     F_HULL = 1,        // Geometry_3d::NodeData::boundary

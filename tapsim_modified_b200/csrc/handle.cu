@@ -63,6 +63,9 @@ long long launches_so_far() { return g_launches.load(std::memory_order_relaxed);
 
 struct tg_handle {
     int n = 0, nnz = 0, ntets = 0, ncol = 0;
+    // the device that was current at tg_create: the handle's buffers,
+    // streams and events live there, and every entry point makes it current
+    int device = -1;
     cudaStream_t stream = nullptr;
     std::string err;
     float top_z = 0.0f;
@@ -330,6 +333,11 @@ struct tg_handle {
 
 namespace {
 
+// The handle's device, current for the length of an entry point.
+struct DeviceScope : ScopedDevice {
+    explicit DeviceScope(const tg_handle* h) : ScopedDevice(h ? h->device : -1) {}
+};
+
 int fail(tg_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
     g_error = msg;
@@ -457,6 +465,10 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(nullptr, TG_ERR_CUDA, "tg_create: no CUDA device");
     tg_handle* h = new tg_handle();
+    if (cudaGetDevice(&h->device) != cudaSuccess) {
+        delete h;
+        return fail(nullptr, TG_ERR_CUDA, "tg_create: no current CUDA device");
+    }
     const int n = d->num_nodes;
     const int nnz = d->row_ptr[n];
     h->n = n;
@@ -814,6 +826,7 @@ int tg_create(const tg_mesh_desc* d, tg_handle** out) {
 }
 
 void tg_destroy(tg_handle* h) {
+    DeviceScope dev_scope(h);
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->xyz.release(); h->type.release(); h->typeScratch.release(); h->flags.release(); h->area_pos.release();
@@ -863,12 +876,14 @@ void tg_destroy(tg_handle* h) {
 }
 
 int tg_timer_start(tg_handle* h) {
+    DeviceScope dev_scope(h);
     if (!h) return fail(h, TG_ERR_ARGUMENT, "tg_timer_start: null handle");
     CK(cudaEventRecord(h->evStart, h->stream));
     return TG_OK;
 }
 
 int tg_timer_stop(tg_handle* h, float* ms) {
+    DeviceScope dev_scope(h);
     if (!h || !ms) return fail(h, TG_ERR_ARGUMENT, "tg_timer_stop: null argument");
     CK(cudaEventRecord(h->evStop, h->stream));
     CK(cudaEventSynchronize(h->evStop));
@@ -879,6 +894,7 @@ int tg_timer_stop(tg_handle* h, float* ms) {
 int64_t tg_launch_count(const tg_handle*) { return (int64_t)launches_so_far(); }
 
 int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, double* bytes) {
+    DeviceScope dev_scope(h);
     if (!h || iters < 1 || !avg_ms || !bytes) return fail(h, TG_ERR_ARGUMENT, "tg_bench_kernel: bad argument");
     DevMesh m = h->dm();
     // rows of the timed kernel and their neighbour entries
@@ -939,12 +955,14 @@ int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, d
 }
 
 int tg_get_phi(tg_handle* h, double* phi) {
+    DeviceScope dev_scope(h);
     if (!h || !phi) return fail(h, TG_ERR_ARGUMENT, "tg_get_phi: null argument");
     CK(cudaMemcpyAsync(phi, h->phi64.p, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
     return sync_status(h, "tg_get_phi");
 }
 
 int tg_set_phi(tg_handle* h, const double* phi) {
+    DeviceScope dev_scope(h);
     if (!h || !phi) return fail(h, TG_ERR_ARGUMENT, "tg_set_phi: null argument");
     CK(cudaMemcpyAsync(h->phi64.p, phi, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
     for (int r = 0; r < tg_handle::kRing; r++) h->ringFull[r] = true;  // Dirichlet potentials may have changed
@@ -955,18 +973,21 @@ int tg_set_phi(tg_handle* h, const double* phi) {
 }
 
 int tg_get_couplings(tg_handle* h, double* out) {
+    DeviceScope dev_scope(h);
     if (!h || !out) return fail(h, TG_ERR_ARGUMENT, "tg_get_couplings: null argument");
     CK(cudaMemcpyAsync(out, h->c64.p, sizeof(double) * h->nnz, cudaMemcpyDeviceToHost, h->stream));
     return sync_status(h, "tg_get_couplings");
 }
 
 int tg_get_types(tg_handle* h, int8_t* out) {
+    DeviceScope dev_scope(h);
     if (!h || !out) return fail(h, TG_ERR_ARGUMENT, "tg_get_types: null argument");
     CK(cudaMemcpyAsync(out, h->type.p, h->n, cudaMemcpyDeviceToHost, h->stream));
     return sync_status(h, "tg_get_types");
 }
 
 int tg_relax_cycles(tg_handle* h, int32_t n, double* deviation) {
+    DeviceScope dev_scope(h);
     if (!h || n < 1) return fail(h, TG_ERR_ARGUMENT, "tg_relax_cycles: bad argument");
     for (int it = 0; it < n - 1; it++) sweep_all(h, nullptr);
     CK(cudaMemsetAsync(h->acc.p, 0, sizeof(double), h->stream));
@@ -982,6 +1003,7 @@ int tg_relax_cycles(tg_handle* h, int32_t n, double* deviation) {
 
 int tg_relax_threshold(tg_handle* h, double threshold, int32_t cycle, int32_t queueSize, int64_t maxSweeps,
                        int64_t* iterations, double* deviation) {
+    DeviceScope dev_scope(h);
     if (!h || cycle < 1) return fail(h, TG_ERR_ARGUMENT, "tg_relax_threshold: bad argument");
     std::deque<double> queue;
     int64_t iter = 0;
@@ -1009,6 +1031,7 @@ int tg_relax_threshold(tg_handle* h, double threshold, int32_t cycle, int32_t qu
 
 int tg_local_relax(tg_handle* h, int32_t node, int32_t shell, double threshold, int32_t cycle, int32_t queueSize,
                    int64_t* iterations, double* deviation) {
+    DeviceScope dev_scope(h);
     if (!h || node < 0 || node >= h->n || cycle < 1) return fail(h, TG_ERR_ARGUMENT, "tg_local_relax: bad argument");
     h->converged = h->histValid = h->residValid = false;
     DevMesh m = h->dm();
@@ -1053,6 +1076,7 @@ int tg_local_relax(tg_handle* h, int32_t node, int32_t shell, double threshold, 
 }
 
 int tg_residual(tg_handle* h, double* rel) {
+    DeviceScope dev_scope(h);
     if (!h || !rel) return fail(h, TG_ERR_ARGUMENT, "tg_residual: null argument");
     int rc = ensure_bnorm(h);
     if (rc != TG_OK) return rc;
@@ -1308,6 +1332,7 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
 }
 
 int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
+    DeviceScope dev_scope(h);
     if (!h || !o) return fail(h, TG_ERR_ARGUMENT, "tg_solve: null argument");
     int rc = TG_OK;
     DevMesh m = h->dm();
@@ -1443,12 +1468,15 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
 }
 
 int tg_learner_attach(tg_handle* h, tg_learner* L, int32_t mode) {
+    DeviceScope dev_scope(h);
     if (!h || mode < 0 || mode > 3 || (mode && !L)) return fail(h, TG_ERR_ARGUMENT, "tg_learner_attach: bad argument");
     if (mode == 0) {
         h->learner = nullptr;
         h->learnMode = 0;
         return TG_OK;
     }
+    if (learner_device(L) != h->device)
+        return fail(h, TG_ERR_ARGUMENT, "tg_learner_attach: the learner and the grid live on different devices");
     int maxRow = 0;
     for (int i = 0; i < h->n; i++) maxRow = std::max(maxRow, h->h_row_ptr[i + 1] - h->h_row_ptr[i]);
     const int rc = learner_attach_mesh(L, (size_t)h->n, maxRow);
@@ -1459,6 +1487,7 @@ int tg_learner_attach(tg_handle* h, tg_learner* L, int32_t mode) {
 }
 
 int tg_field_o1(tg_handle* h, int32_t count, const int32_t* nodes, double* out) {
+    DeviceScope dev_scope(h);
     if (!h || count < 0 || (count && (!nodes || !out))) return fail(h, TG_ERR_ARGUMENT, "tg_field_o1: bad argument");
     if (count == 0) return TG_OK;
     for (int32_t k = 0; k < count; k++)
@@ -1473,6 +1502,7 @@ int tg_field_o1(tg_handle* h, int32_t count, const int32_t* nodes, double* out) 
 }
 
 int tg_surface_init(tg_handle* h, int32_t vacuumId, int32_t* num) {
+    DeviceScope dev_scope(h);
     if (!h || vacuumId < 0 || vacuumId > 127 || h->types[vacuumId].id < 0)
         return fail(h, TG_ERR_ARGUMENT, "tg_surface_init: unknown vacuum id");
     h->vacuumId = vacuumId;
@@ -1488,6 +1518,7 @@ int tg_surface_init(tg_handle* h, int32_t vacuumId, int32_t* num) {
 int tg_surface_select(tg_handle* h, tg_select_info* info) { return tg_surface_select_mode(h, 0, 0.0f, info); }
 
 int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_select_info* info) {
+    DeviceScope dev_scope(h);
     if (!h || !info) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: null argument");
     if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: surface not initialised");
     if (mode < 0 || mode > 3) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: probability mode 0..3");
@@ -1552,6 +1583,7 @@ int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_sel
 }
 
 int tg_surface_pick(tg_handle* h, double u, int32_t* node, float* probability) {
+    DeviceScope dev_scope(h);
     if (!h || !node) return fail(h, TG_ERR_ARGUMENT, "tg_surface_pick: null argument");
     if (!h->selValid || h->sel.candidate < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_pick: no selection");
     // the smallest node T with sum_{surface i <= T} p_i >= u, by bisection
@@ -1592,6 +1624,7 @@ int tg_surface_pick(tg_handle* h, double u, int32_t* node, float* probability) {
 }
 
 int tg_cell_values(tg_handle* h, int32_t count, const int32_t* nodes, float* phi, float* field, float* force) {
+    DeviceScope dev_scope(h);
     if (!h || count < 0 || (!nodes && count != h->n))
         return fail(h, TG_ERR_ARGUMENT, "tg_cell_values: bad argument (nodes NULL needs count = N)");
     if (nodes)
@@ -1614,6 +1647,7 @@ int tg_cell_values(tg_handle* h, int32_t count, const int32_t* nodes, float* phi
 }
 
 int tg_surface_normals(tg_handle* h, int32_t count, const int32_t* nodes, float* normals) {
+    DeviceScope dev_scope(h);
     if (!h || count < 0 || (count && (!nodes || !normals))) return fail(h, TG_ERR_ARGUMENT, "tg_surface_normals: bad argument");
     if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_normals: surface not initialised");
     for (int32_t k = 0; k < count; k++)
@@ -1630,6 +1664,7 @@ int tg_surface_normals(tg_handle* h, int32_t count, const int32_t* nodes, float*
 
 int tg_surface_cells(tg_handle* h, int32_t mode, float temperature, int32_t capacity, int32_t* count, int32_t* cells,
                      float* probability) {
+    DeviceScope dev_scope(h);
     if (!h || !count || capacity < 0 || (capacity && (!cells || !probability)))
         return fail(h, TG_ERR_ARGUMENT, "tg_surface_cells: bad argument");
     *count = 0;
@@ -1666,6 +1701,7 @@ static std::string snapshot_name(const char* path, int32_t index) {
 }
 
 int tg_log_grid(tg_handle* h, const char* path, int32_t index, int32_t binary, const uint32_t* numbers) {
+    DeviceScope dev_scope(h);
     if (!h || !path) return fail(h, TG_ERR_ARGUMENT, "tg_log_grid: null argument");
     const int n = h->n;
     std::vector<float> phi(n), field(3 * (size_t)n), force(3 * (size_t)n);
@@ -1684,6 +1720,7 @@ int tg_log_grid(tg_handle* h, const char* path, int32_t index, int32_t binary, c
 
 int tg_log_surface(tg_handle* h, const char* path, int32_t index, int32_t binary, int32_t withNeighbours,
                    int32_t mode, float temperature, const uint32_t* numbers) {
+    DeviceScope dev_scope(h);
     if (!h || !path) return fail(h, TG_ERR_ARGUMENT, "tg_log_surface: null argument");
     const int n = h->n;
     int32_t nc = 0;
@@ -1729,6 +1766,7 @@ int tg_log_surface(tg_handle* h, const char* path, int32_t index, int32_t binary
 }
 
 int tg_get_surface(tg_handle* h, int32_t capacity, int32_t* nodes, float* ratios, int32_t* count) {
+    DeviceScope dev_scope(h);
     if (!h || !count) return fail(h, TG_ERR_ARGUMENT, "tg_get_surface: null argument");
     std::vector<int32_t> list(h->surfSlots);
     std::vector<float> rat(h->surfSlots);
@@ -1752,6 +1790,7 @@ int tg_get_surface(tg_handle* h, int32_t capacity, int32_t* nodes, float* ratios
 }
 
 int tg_surface_normal(tg_handle* h, int32_t node, float normal[3]) {
+    DeviceScope dev_scope(h);
     if (!h || node < 0 || node >= h->n || !normal) return fail(h, TG_ERR_ARGUMENT, "tg_surface_normal: bad argument");
     int rc = stage(h, h->stageF, 4);
     if (rc != TG_OK) return rc;
@@ -1875,6 +1914,7 @@ static int take_away_impl(tg_handle* h, int32_t node, int32_t capacity, int32_t*
 }
 
 int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached, int32_t* numDetached) {
+    DeviceScope dev_scope(h);
     if (!h || node < 0 || node >= h->n) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: bad node");
     if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_take_away: surface not initialised");
     const int rc = take_away_impl(h, node, capacity, detached, numDetached);
@@ -1883,6 +1923,7 @@ int tg_take_away(tg_handle* h, int32_t node, int32_t capacity, int32_t* detached
 }
 
 int tg_update_coordination(tg_handle* h) {
+    DeviceScope dev_scope(h);
     if (!h) return fail(h, TG_ERR_ARGUMENT, "tg_update_coordination: null handle");
     h->residValid = false;
     launch_update_coordination(h->dm(), h->typeScratch.p, h->stream);
@@ -1959,17 +2000,20 @@ static int trace_impl(tg_handle* h, int32_t nIons, const float* start, const flo
 
 int tg_trace(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
              const int32_t* guess, const tg_trace_opts* o, tg_impact* out) {
+    DeviceScope dev_scope(h);
     return trace_impl(h, nIons, start, vel, qm, guess, o, out, 0, nullptr, nullptr, "tg_trace");
 }
 
 int tg_trace_path(tg_handle* h, int32_t nIons, const float* start, const float* vel, const float* qm,
                   const int32_t* guess, const tg_trace_opts* o, int32_t cap, tg_impact* out, tg_path_point* points,
                   float* errors) {
+    DeviceScope dev_scope(h);
     if (cap <= 0) return fail(h, TG_ERR_ARGUMENT, "tg_trace_path: cap must be positive");
     return trace_impl(h, nIons, start, vel, qm, guess, o, out, cap, points, errors, "tg_trace_path");
 }
 
 int tg_potential_at(tg_handle* h, int32_t n, const float* xyz, const int32_t* guess, float* out) {
+    DeviceScope dev_scope(h);
     if (!h || n < 0 || (n && (!xyz || !out))) return fail(h, TG_ERR_ARGUMENT, "tg_potential_at: bad argument");
     if (n == 0) return TG_OK;
     if (!h->tet_v.p) return fail(h, TG_ERR_ARGUMENT, "tg_potential_at: mesh has no tetrahedra");
@@ -2248,6 +2292,7 @@ static bool path_opts_ok(const tg_event_opts* o) {
 }
 
 int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec) {
+    DeviceScope dev_scope(h);
     if (!h || !o || !rec) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: null argument");
     if (!path_opts_ok(o)) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: path_cap < 0 or path buffers missing");
     return run_event(h, o, eventIndex, rec, nullptr);
@@ -2255,6 +2300,7 @@ int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_ev
 
 int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int32_t count, tg_event_record* recs,
                   int32_t* done) {
+    DeviceScope dev_scope(h);
     if (!h || !o || count < 0 || (count && !recs)) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: bad argument");
     if (!path_opts_ok(o)) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: path_cap < 0 or path buffers missing");
     if (done) *done = 0;
@@ -2317,11 +2363,11 @@ static __device__ __align__(256) unsigned char g_field_scratch[kNoAllocBytes];
 std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
-// Device address of the scratch on the current device, looked up once per
-// device (the lookup may load this library's device image onto the device).
+// Device address of the scratch on the handle's device, looked up once per
+// device with that device current (the caller's DeviceScope makes it so; the
+// lookup may load this library's device image onto the device).
 int noalloc_scratch(tg_handle* h, unsigned char** out) {
-    int dev = -1;
-    CK(cudaGetDevice(&dev));
+    const int dev = h->device;
     if (dev < 0 || dev >= kNoAllocMaxDevices)
         return fail(h, TG_ERR_ARGUMENT, "tg_field_o1_noalloc: device ordinal beyond the 64 the scratch table covers");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
@@ -2339,6 +2385,7 @@ int noalloc_scratch(tg_handle* h, unsigned char** out) {
 extern "C" {
 
 int tg_field_o1_noalloc(tg_handle* h, int32_t count, const int32_t* nodes, double* out) {
+    DeviceScope dev_scope(h);
     if (!h || count < 0 || (count && (!nodes || !out)))
         return fail(h, TG_ERR_ARGUMENT, "tg_field_o1_noalloc: bad argument");
     if (count > TG_FIELD_O1_NOALLOC_MAX)

@@ -3,10 +3,51 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <exception>
+#include <mutex>
+#include <new>
 #include <thread>
 
 namespace tg_host {
+
+// Test hook (amg_inject_worker_failure): while set, one worker of every
+// threaded pass throws std::bad_alloc, as a failed allocation there would.
+static std::atomic<bool> g_fail_workers(false);
+
+void amg_inject_worker_failure(bool on) { g_fail_workers.store(on); }
+
 namespace {
+
+// Runs body(t) for t < T on T threads and joins every thread it started.  An
+// exception leaving a worker (std::bad_alloc from one of the per-thread
+// buffers, say) would call std::terminate; it is caught in the worker
+// instead and the first one is rethrown on the calling thread after the
+// joins.  If starting a thread throws, the threads already running are
+// joined before that error propagates.
+template <class F>
+void run_threads(int T, F body) {
+    std::mutex m;
+    std::exception_ptr first;
+    auto guarded = [&](int t) {
+        try {
+            if (g_fail_workers.load() && t == T - 1) throw std::bad_alloc();
+            body(t);
+        } catch (...) {
+            std::lock_guard<std::mutex> lock(m);
+            if (!first) first = std::current_exception();
+        }
+    };
+    std::vector<std::thread> pool;
+    try {
+        pool.reserve(T);
+        for (int t = 0; t < T; t++) pool.emplace_back(guarded, t);
+    } catch (...) {
+        for (auto& th : pool) th.join();
+        throw;
+    }
+    for (auto& th : pool) th.join();
+    if (first) std::rethrow_exception(first);
+}
 
 template <class F>
 void parallel_rows(int n, int threads, F f) {
@@ -14,14 +55,9 @@ void parallel_rows(int n, int threads, F f) {
         f(0, n, 0);
         return;
     }
-    std::vector<std::thread> pool;
     const int chunk = (n + threads - 1) / threads;
-    for (int t = 0; t < threads; t++) {
-        const int b = t * chunk, e = std::min(n, b + chunk);
-        if (b >= e) break;
-        pool.emplace_back(f, b, e, t);
-    }
-    for (auto& th : pool) th.join();
+    const int T = (n + chunk - 1) / chunk;
+    run_threads(T, [&](int t) { f(t * chunk, std::min(n, (t + 1) * chunk), t); });
 }
 
 // R = P^T.  Each thread takes a contiguous block of P's rows and writes its
@@ -249,9 +285,7 @@ AmgCsr galerkin(const AmgCsr& R, const AmgCsr& A, const AmgCsr& P, int threads) 
     if (T == 1) {
         work(0);
     } else {
-        std::vector<std::thread> pool;
-        for (int t = 0; t < T; t++) pool.emplace_back(work, t);
-        for (auto& th : pool) th.join();
+        run_threads(T, work);
     }
     AmgCsr Ac;
     Ac.rows = Ac.cols = nc;

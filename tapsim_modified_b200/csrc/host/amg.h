@@ -55,4 +55,9 @@ struct AmgOptions {
 // the error.
 std::string amg_build(AmgCsr&& A, const AmgOptions& opt, AmgHierarchy* out);
 
+// Test hook: while on, one worker thread of every threaded pass of the build
+// throws std::bad_alloc (an allocation failure inside a worker), which the
+// build must turn into an error on the calling thread.
+void amg_inject_worker_failure(bool on);
+
 }  // namespace tg_host

@@ -77,4 +77,6 @@ int tg_amg_host_matrix(const tg_amg_host* a, int32_t level, int32_t which, int32
 
 void tg_amg_host_destroy(tg_amg_host* a) { delete a; }
 
+void tg_amg_host_inject_worker_failure(int32_t on) { tg_host::amg_inject_worker_failure(on != 0); }
+
 }  // extern "C"

@@ -72,6 +72,7 @@ inline int roundup128(int n) { return (n + 127) / 128 * 128; }
 
 struct tg_learner {
     int hops = 6, cap = 4096, D = 32;
+    int device = -1;    // current at tg_learner_create; made current by every entry point
     float gain = 1.0f;  // multiplier of the prediction added in tg_solve
     std::string err;
     cudaStream_t stream = nullptr;
@@ -263,6 +264,8 @@ int build_graph(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, int* 
 
 // ---- hooks called by tg_solve (handle.cu) ----
 
+int learner_device(const tg_learner* L) { return L->device; }
+
 int learner_attach_mesh(tg_learner* L, size_t meshNodes, int maxRow) {
     if (maxRow > L->D)
         return lfail(L, TG_ERR_ARGUMENT, "learner: graph width " + std::to_string(L->D) +
@@ -332,6 +335,10 @@ int tg_learner_create(int32_t hops, int32_t max_nodes, int32_t ell_width, uint64
         ell_width > 256)
         return lfail(nullptr, TG_ERR_ARGUMENT, "tg_learner_create: bad argument");
     tg_learner* L = new tg_learner();
+    if (cudaGetDevice(&L->device) != cudaSuccess) {
+        delete L;
+        return lfail(nullptr, TG_ERR_CUDA, "tg_learner_create: no current CUDA device");
+    }
     L->hops = hops;
     L->cap = max_nodes;
     L->D = ell_width;
@@ -387,6 +394,7 @@ int tg_learner_create(int32_t hops, int32_t max_nodes, int32_t ell_width, uint64
 }
 
 void tg_learner_destroy(tg_learner* L) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L) return;
     if (L->stream) cudaStreamSynchronize(L->stream);
     L->P.release(); L->G.release(); L->M1.release(); L->M2.release(); L->Wb.release(); L->WTb.release();
@@ -405,12 +413,14 @@ const char* tg_learner_last_error(const tg_learner* L) { return L ? L->err.c_str
 int32_t tg_learner_num_params(void) { return kParams; }
 
 int tg_learner_set_gain(tg_learner* L, float gain) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L || !(gain >= 0.0f) || gain > 4.0f) return lfail(L, TG_ERR_ARGUMENT, "tg_learner_set_gain: gain in [0, 4]");
     L->gain = gain;
     return TG_OK;
 }
 
 int tg_learner_samples(const tg_learner* L, int32_t* count, int64_t* cells) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L) return lfail(nullptr, TG_ERR_ARGUMENT, "tg_learner_samples: null learner");
     if (count) *count = (int32_t)L->sLen.size();
     if (cells) *cells = L->sNodes;
@@ -418,6 +428,7 @@ int tg_learner_samples(const tg_learner* L, int32_t* count, int64_t* cells) {
 }
 
 int tg_learner_get_params(tg_learner* L, float* out) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L || !out) return lfail(L, TG_ERR_ARGUMENT, "tg_learner_get_params: null argument");
     LCK(cudaStreamSynchronize(L->stream));
     LCK(cudaMemcpy(out, L->P.p, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
@@ -425,6 +436,7 @@ int tg_learner_get_params(tg_learner* L, float* out) {
 }
 
 int tg_learner_set_params(tg_learner* L, const float* in) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L || !in) return lfail(L, TG_ERR_ARGUMENT, "tg_learner_set_params: null argument");
     LCK(cudaStreamSynchronize(L->stream));
     LCK(cudaMemcpy(L->P.p, in, sizeof(float) * kParams, cudaMemcpyHostToDevice));
@@ -434,6 +446,7 @@ int tg_learner_set_params(tg_learner* L, const float* in) {
 
 int tg_learner_get_sample(tg_learner* L, int32_t idx, int32_t* n, float* features, int32_t* ell_col, float* ell_w,
                           float* target) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L || idx < 0 || idx >= (int32_t)L->sLen.size() || !n)
         return lfail(L, TG_ERR_ARGUMENT, "tg_learner_get_sample: bad index");
     const int len = L->sLen[idx];
@@ -447,6 +460,7 @@ int tg_learner_get_sample(tg_learner* L, int32_t idx, int32_t* n, float* feature
 }
 
 int tg_learner_gradients(tg_learner* L, int32_t first, int32_t count, float* loss, float* grads, float* outputs) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L || first < 0 || count < 1 || first + count > (int32_t)L->sLen.size())
         return lfail(L, TG_ERR_ARGUMENT, "tg_learner_gradients: bad sample range");
     std::vector<int> idx;
@@ -466,6 +480,7 @@ int tg_learner_gradients(tg_learner* L, int32_t first, int32_t count, float* los
 
 int tg_learner_train(tg_learner* L, int32_t steps, int32_t batch, float lr, uint64_t seed, int32_t first,
                      int32_t count, float* mean_loss) {
+    ScopedDevice dev_scope(L ? L->device : -1);
     if (!L || steps < 0 || batch < 1 || !(lr > 0.0f)) return lfail(L, TG_ERR_ARGUMENT, "tg_learner_train: bad argument");
     const int total = (int)L->sLen.size();
     if (count <= 0) count = total - first;

@@ -9,6 +9,8 @@
 
 struct tg_learner;
 
+// the device the learner's buffers live on (current at tg_learner_create)
+int learner_device(const tg_learner* L);
 // sizes the per-mesh scratch (global -> graph index map); fails when the
 // graph width is below the mesh's longest row
 int learner_attach_mesh(tg_learner* L, size_t meshNodes, int maxRow);

@@ -342,3 +342,37 @@ def test_non_positive_diagonal_is_a_host_error():
     rc, h = _build(A)
     assert rc == N.TG_ERR_HOST
     assert not h.value
+
+
+def test_worker_allocation_failure_is_an_error():
+    """An allocation failure inside one of the build's worker threads comes
+    back from the C ABI as TG_ERR_HOST with its message, instead of ending
+    the process through std::terminate; every thread is joined, and the next
+    build (hook off) succeeds.  Run in a child process, so that a regression
+    (terminate) fails this test instead of ending the test session."""
+    import subprocess
+    import sys
+    import textwrap
+    from pathlib import Path
+    code = textwrap.dedent("""
+        import ctypes as C, sys
+        import numpy as np
+        sys.path.insert(0, %r)
+        sys.path.insert(0, %r)
+        import test_amg_host as T
+        from tapsim_modified_b200 import _native as N
+        L = N.lib()
+        A = T._poisson(m=14, seed=3)                 # 2,744 rows: threaded passes
+        L.tg_amg_host_inject_worker_failure(1)
+        rc, h = T._build(A)
+        msg = L.tg_last_error(None).decode()
+        L.tg_amg_host_inject_worker_failure(0)
+        assert rc == N.TG_ERR_HOST and not h.value, (rc, h.value)
+        assert "bad_alloc" in msg or "alloc" in msg, msg
+        rc, h = T._build(A)
+        assert rc == 0 and L.tg_amg_host_levels(h) >= 2
+        L.tg_amg_host_destroy(h)
+        print("ok")
+    """) % (str(Path(__file__).resolve().parent.parent), str(Path(__file__).resolve().parent))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), (r.returncode, r.stdout[-2000:], r.stderr[-2000:])
