@@ -121,19 +121,22 @@ def ncu_traffic_ratio(kernel: str):
     return float(m.group(1)) if m else None
 
 
-def reference_run(dump: Path, cfg: Path, n_events: int, threads: int) -> tuple[list[float], str]:
+def reference_run(dump: Path, cfg: Path, n_events: int, threads: int, ini: dict | None = None,
+                  label: str | None = None) -> tuple[list[float], str]:
     """The reference's own per-event path (oracle/_ref/ref_harness, built from
-    the reference sources) on the same mesh, resumed from a TAPSIM dump."""
+    the reference sources) on the same mesh, resumed from a TAPSIM dump;
+    per-event wall times.  ini: the evaporation options (default: the
+    reference's shipped defaults)."""
     harness = ROOT / "oracle" / "_ref" / "ref_harness"
     if not harness.exists():
         raise FileNotFoundError(harness)
     from tapsim_modified_b200.tapsim import INI_DEFAULTS
-    ini = dump.with_suffix(".ini")
+    ini_path = dump.with_suffix(".ini")
     # the reference's shipped defaults (tapsim.ini): local 3-hop relaxation
     # plus one global sweep per event, no refresh
-    ini.write_text("".join(f"{k} = {v}\n" for k, v in INI_DEFAULTS.items()))
+    ini_path.write_text("".join(f"{k} = {v}\n" for k, v in (ini or INI_DEFAULTS).items()))
     out = dump.with_suffix(".events")
-    cmd = [str(harness), "evap", str(cfg), "-", str(ini), str(n_events), str(out), "--dump", str(dump),
+    cmd = [str(harness), "evap", str(cfg), "-", str(ini_path), str(n_events), str(out), "--dump", str(dump),
            "--no-sync", "--no-init-relax", "--threads", str(threads)]
     subprocess.run(cmd, check=True, capture_output=True)
     walls = []
@@ -141,7 +144,7 @@ def reference_run(dump: Path, cfg: Path, n_events: int, threads: int) -> tuple[l
         if line.startswith("#"):
             continue
         walls.append(float(line.split()[-1]))
-    return walls, "reference TAPSim default ini: localRelax(shell 3) + 1 global sweep per event"
+    return walls, label or "reference TAPSim default ini: localRelax(shell 3) + 1 global sweep per event"
 
 
 def reduce_over_ranks(dist, maxed: list, summed: list, device: str):
@@ -198,8 +201,8 @@ def run_ours(args, rank: int, world: int, dist):
 
     def train_learner():
         """Learned near field: samples from events on a training tip of
-        another shape and seed (plain solver with the recycled far field),
-        trained on the device; the last tenth of the samples is held out."""
+        another shape and seed (plain solver), trained on the device; the
+        last tenth of the samples is held out."""
         t0 = time.perf_counter()
         tmesh = Mesh.from_tip(seed=101 + rank, **TIPS["train"])
         tgrid = Grid(tmesh)
@@ -207,8 +210,7 @@ def run_ours(args, rank: int, world: int, dist):
         learner = Learner(hops=6, max_cells=8192, ell_width=64, seed=7 + rank)
         learner.attach(tgrid, collect=True)
         tev = Evaporation(tgrid, opts, relax_mode=1,
-                          solve=solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, warm_start=1,
-                                           preconditioner=PRECOND))
+                          solve=solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, preconditioner=PRECOND))
         tev.run(args.train_events)
         learner.attach(tgrid)
         tgrid.close()
@@ -225,11 +227,12 @@ def run_ours(args, rank: int, world: int, dist):
                          "train_loss_last": last, "heldout_loss_untrained": before, "heldout_loss_trained": after,
                          "setup_s": time.perf_counter() - t0}
 
-    def run_arm(warm_start: int, learner=None):
+    def run_arm(name: str, warm_start: int, learner=None, inner_precision: int = 0, long_run: int = 0):
         """Mesh upload, initial relaxation, W warm-up and K timed events with
-        the given solve start; returns the timings and the event records."""
+        the given solve start (and long_run more events timed after them);
+        returns the timings and the event records.  The grid stays open."""
         sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4, warm_start=warm_start,
-                           preconditioner=PRECOND)
+                           preconditioner=PRECOND, inner_precision=inner_precision)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -242,54 +245,66 @@ def run_ours(args, rank: int, world: int, dist):
         if learner is not None:
             learner.attach(grid, predict=True)
         ev = Evaporation(grid, opts, relax_mode=1, solve=sopts)
-        ev.run(args.warmup)
-        # timed region: K events in one call of the public API (flights
-        # overlap the next event's relaxation); device time with CUDA events
-        # on the handle's stream, end-to-end time on the host clock around
-        # the call, which takes each event's options from host memory and
-        # returns its record to host memory
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        launches0 = L.tg_launch_count(grid._h)
-        torch.cuda.nvtx.range_push(f"timed_{('plain', 'warm', 'learned')[warm_start]}")
+        # the clock sampler runs from before the warm-up to the end of the
+        # long run, so that its 200 ms samples cover the timed events
         with ClockSampler(local) as clocks:
+            ev.run(args.warmup)
+            # timed region: K events in one call of the public API (flights
+            # overlap the next event's relaxation); device time with CUDA
+            # events on the handle's stream, end-to-end time on the host clock
+            # around the call, which takes each event's options from host
+            # memory and returns its record to host memory
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            launches0 = L.tg_launch_count(grid._h)
+            torch.cuda.nvtx.range_push(f"timed_{name}")
             t1 = time.perf_counter()
             N.check(L.tg_timer_start(grid._h), grid._h)
             ev.run(args.steps)
             ms = C.c_float()
             N.check(L.tg_timer_stop(grid._h, C.byref(ms)), grid._h)
             t_e2e = time.perf_counter() - t1
-        torch.cuda.nvtx.range_pop()
-        torch.cuda.synchronize()
-        launches = L.tg_launch_count(grid._h) - launches0
+            torch.cuda.nvtx.range_pop()
+            torch.cuda.synchronize()
+            launches = L.tg_launch_count(grid._h) - launches0
+            long_ms = None
+            if long_run:
+                N.check(L.tg_timer_start(grid._h), grid._h)
+                ev.run(long_run)
+                lm = C.c_float()
+                N.check(L.tg_timer_stop(grid._h, C.byref(lm)), grid._h)
+                long_ms = lm.value
         phi = grid.potentials()                 # device -> host result
         return {"grid": grid, "info0": info0, "dev_s": ms.value / 1e3, "t_e2e": t_e2e, "launches": launches,
-                "records": ev.records, "clocks": clocks, "phi": phi, "setup_s": setup_s}
+                "records": ev.records, "clocks": clocks, "phi": phi, "setup_s": setup_s, "long_ms": long_ms}
+
+    def iters(arm, first=None, last=None):
+        recs = arm["records"][args.warmup:][first:last]
+        return [r["relax_iterations"] for r in recs]
+
+    def seq_diff(a, b):
+        return next((k for k, (x, y) in enumerate(zip([r["node"] for r in a["records"]],
+                                                      [r["node"] for r in b["records"]])) if x != y), None)
 
     learner, learn_info = (None, None) if args.no_learned else train_learner()
-    plain = run_arm(0)
+    plain = run_arm("plain", 0)
     plain["grid"].close()
-    learned = None
-    if learner is not None:
-        learned = run_arm(2, learner)
-        learned["grid"].close()
-        learner.close()
-    # the headline arm: the recycled far field (warm_start 1); the plain and
-    # learned starts are timed on the same tip beside it
-    arm = run_arm(1)
+    recycled = run_arm("recycled", 1)
+    recycled["grid"].close()
+    fp64 = run_arm("fp64_inner", 0, inner_precision=1)
+    fp64["grid"].close()
+    # the headline arm: the learned warm start (warm_start 2), the metric's
+    # subject; without a learner the plain start
+    arm = run_arm("learned", 2, learner, long_run=args.long_events) if learner is not None \
+        else run_arm("plain_value", 0, long_run=args.long_events)
     grid, info0, dev_s, t_e2e, phi, clocks = (arm[k] for k in ("grid", "info0", "dev_s", "t_e2e", "phi", "clocks"))
     launches = arm["launches"]
     recs = arm["records"][args.warmup:]
-    iters = [r["relax_iterations"] for r in recs]
-    iters_plain = [r["relax_iterations"] for r in plain["records"][args.warmup:]]
     resid = max(r["rel_residual"] for r in recs + plain["records"][args.warmup:])
-    seq_w = [r["node"] for r in arm["records"]]
-    seq_p = [r["node"] for r in plain["records"]]
-    first_diff = next((k for k, (x, y) in enumerate(zip(seq_w, seq_p)) if x != y), None)
     # roofline of the dominant kernel (the multigrid's level-0 smoothing
     # pass, the largest share of the event's device time) on this mesh, and
-    # of the CG SpMV beside it
+    # of the CG SpMV and the FP64 residual beside it
     avg = C.c_float()
     nbytes = C.c_double()
     N.check(L.tg_bench_kernel(grid._h, 2, 50, C.byref(avg), C.byref(nbytes)), grid._h)
@@ -301,15 +316,21 @@ def run_ours(args, rank: int, world: int, dist):
     r_avg = C.c_float()
     r_bytes = C.c_double()
     N.check(L.tg_bench_kernel(grid._h, 1, 20, C.byref(r_avg), C.byref(r_bytes)), grid._h)
+    long_iters = [r["relax_iterations"] for r in arm["records"][args.warmup + args.steps:]]
+    grid.close()
+    if learner is not None:
+        learner.close()
+    precision = precision_errors(mesh, opts, args.precision_events) if args.precision_events > 0 else None
 
-    (dev_max, e2e_max, plain_max, lrn_max), (ev_total, ev_e2e_total) = reduce_over_ranks(
-        dist, [dev_s, t_e2e, plain["dev_s"], learned["dev_s"] if learned else 0.0],
-        [args.steps, args.steps], "cuda")
+    (dev_max, e2e_max, plain_max, rec_max, f64_max), (ev_total, ev_e2e_total) = reduce_over_ranks(
+        dist, [dev_s, t_e2e, plain["dev_s"], recycled["dev_s"], fp64["dev_s"]], [args.steps, args.steps], "cuda")
     if rank != 0:
         return None
 
     peak, peak_kind = measured_peak_hbm()
     traffic_ratio = ncu_traffic_ratio("k_amg_fine")
+    value_arm = "learned" if learner is not None else "plain"
+    windows = [long_iters[k:k + 50] for k in range(0, len(long_iters), 50)]
     out = {
         "metric": METRIC,
         "value": ev_total / dev_max,
@@ -328,27 +349,42 @@ def run_ours(args, rank: int, world: int, dist):
                         f"{TIPS[args.tip]['shank_length'] * 1e9:g} nm shank, "
                         f"{TIPS[args.tip]['half_angle_deg']:g} deg, vacuum to 1 um; {atoms} atoms, "
                         f"{mesh.num_nodes} cells per GPU; relax to rel. residual <= {REL_TOL:g} every event; "
-                        "solve started from the previous event's correction (recycled far field, warm_start 1)",
-            "value_arm": "recycled far field (warm_start 1); the plain start (warm_start 0) is in "
-                         "config.plain and the learned start (warm_start 2) in config.learned, timed on the same tip",
+                        + ("solve started from the learned warm start (warm_start 2)" if learner is not None
+                           else "plain start (no learner)"),
+            "value_arm": f"{value_arm}; the plain start (warm_start 0) is config.plain, the recycled correction "
+                         "(warm_start 1) config.recycled and the FP64 inner iterations config.fp64_inner, each "
+                         "timed on the same tip",
+            "learned_over_plain": (plain_max / dev_max) if learner is not None else None,
+            "recycled_over_plain": plain_max / rec_max,
             "events_per_gpu": args.steps,
             "plain": {"value": ev_total / plain_max, "ms_per_step": plain_max * 1e3 / args.steps,
-                      "solver_iterations_median": statistics.median(iters_plain),
+                      "solver_iterations_median": statistics.median(iters(plain)),
                       "start": "previous event's potentials (plain relaxation)"},
-            "learned": None if learned is None else dict(learn_info, **{
-                "value": ev_total / lrn_max, "ms_per_step": lrn_max * 1e3 / args.steps,
-                "solver_iterations_median": statistics.median(
-                    [r["relax_iterations"] for r in learned["records"][args.warmup:]]),
-                "sequence_first_difference": next((k for k, (x, y) in enumerate(zip(
-                    [r["node"] for r in learned["records"]], [r["node"] for r in plain["records"]])) if x != y), None),
-                "start": "recycled far field plus the network's near-field prediction (warm_start 2); training "
-                         "on the device outside the timed region"}),
-            "warm_over_plain": plain_max / dev_max,
-            "sequence": {"events": len(seq_w), "first_difference": first_diff,
-                         "note": "removed-node sequences of the warm-start and plain arms"},
+            "recycled": {"value": ev_total / rec_max, "ms_per_step": rec_max * 1e3 / args.steps,
+                         "solver_iterations_median": statistics.median(iters(recycled)),
+                         "sequence_first_difference": seq_diff(recycled, plain),
+                         "start": "plus the previous event's correction (warm_start 1)"},
+            "learned": None if learner is None else dict(learn_info, **{
+                "value": ev_total / dev_max, "ms_per_step": dev_max * 1e3 / args.steps,
+                "solver_iterations_median": statistics.median(iters(arm)),
+                "sequence_first_difference": seq_diff(arm, plain),
+                "start": "the network's near-field prediction on the plain start (warm_start 2); training on the "
+                         "device outside the timed region"}),
+            "fp64_inner": {"value": ev_total / f64_max, "ms_per_step": f64_max * 1e3 / args.steps,
+                           "solver_iterations_median": statistics.median(iters(fp64)),
+                           "sequence_first_difference": seq_diff(fp64, plain),
+                           "note": "FP64 couplings, vectors and recurrences in the inner CG (tg_solve_opts."
+                                   "inner_precision 1), FP32 V-cycle; same outer FP64 test"},
+            "fp64_error": precision,
+            "long_run": None if not args.long_events else {
+                "events": args.long_events, "arm": value_arm,
+                "value": args.long_events / (arm["long_ms"] / 1e3),
+                "solver_iterations_median_per_50": [statistics.median(w) for w in windows if w],
+                "note": "events after the K timed ones, in one call, device time with CUDA events; shows the "
+                        "rows that removals append (smoothed only until the hierarchy is rebuilt at 2% growth)"},
             "l2": "inputs larger than L2 (CSR working set ~GB)",
             "parallelism": f"independent tips, one per GPU (x{world})",
-            "solver_iterations_median": statistics.median(iters),
+            "solver_iterations_median": statistics.median(iters(arm)),
             "max_rel_residual": resid,
             "initial_solve": {"outer": info0.outer, "inner": info0.inner, "rel_residual": info0.rel_residual},
             "preconditioner": "smoothed-aggregation multigrid V(1,1)-cycle (tg_solve_opts.preconditioner 1)"
@@ -402,6 +438,151 @@ def run_ours(args, rank: int, world: int, dist):
             out["cpu_baseline"] = {"value": None, "unit": "events/s", "cores": os.cpu_count(), "kind": "reference",
                                    "sample": f"unavailable: {e}"}
     return out
+
+
+def precision_errors(mesh, opts, events: int) -> dict:
+    """Per-event errors of the FP32-inner solve against FP64 solves of the
+    same events (untimed).  Three grids of the tip run the same events in
+    lockstep, each relaxed by the defect-correction solve with:
+
+      fp32   FP32 inner iterations, rel. residual 1e-8 (the timed path)
+      fp64   FP64 inner iterations, rel. residual 1e-8
+      ref64  FP64 inner iterations, rel. residual 1e-12 (the FP64 reference)
+
+    After every event: max |phi - phi_ref64| over all cells, max |E - E_ref64|
+    of field_o1 over the surface cells (relative to the largest |E| there)
+    and the distance of the detector impacts (relative to the reference
+    impact's radius), for fp32 and fp64.  The comparison stops where a
+    removal sequence differs from ref64's (a near-tie)."""
+    import numpy as np
+
+    from tapsim_modified_b200.tapsim import Evaporation, Grid, solve_opts
+    setups = {"fp32": (REL_TOL, 0), "fp64": (REL_TOL, 1), "ref64": (1e-12, 1)}
+    grids, evs = {}, {}
+    for name, (tol, prec) in setups.items():
+        g = Grid(mesh)
+        g.solve(1e-12, 50, 50000, 1e-4, preconditioner=PRECOND, inner_precision=1)
+        grids[name] = g
+        evs[name] = Evaporation(g, opts, relax_mode=1,
+                                solve=solve_opts(rel_tol=tol, max_outer=50, max_inner=20000, preconditioner=PRECOND,
+                                                 inner_precision=prec))
+    rows = {"fp32": [], "fp64": []}
+    compared = 0
+    for _ in range(events):
+        rec = {k: evs[k].step() for k in setups}
+        if len({rec[k]["node"] for k in setups}) != 1:
+            break
+        compared += 1
+        phi = {k: grids[k].potentials() for k in setups}
+        surf, _ = grids["ref64"].surface()
+        field = {k: grids[k].field_o1(surf) for k in setups}
+        emax = float(np.linalg.norm(field["ref64"], axis=1).max())
+        ref_stop = np.array(rec["ref64"]["stop"])
+        for k in ("fp32", "fp64"):
+            rows[k].append((float(np.abs(phi[k] - phi["ref64"]).max()),
+                            float(np.linalg.norm(field[k] - field["ref64"], axis=1).max()) / emax,
+                            float(np.hypot(*(np.array(rec[k]["stop"])[:2] - ref_stop[:2])) / np.hypot(*ref_stop[:2]))))
+    for g in grids.values():
+        g.close()
+    out = {"events_compared": compared, "events_asked": events,
+           "reference": "FP64 inner iterations to rel. residual 1e-12, same events",
+           "columns": "max over the compared events of: max |dphi| [V] over all cells; max |dE| over the surface "
+                      "cells / max |E| there (field_o1); detector impact distance / impact radius"}
+    for k, v in rows.items():
+        if v:
+            out[k] = {"max_abs_dphi_V": max(r[0] for r in v), "max_rel_dE_surface": max(r[1] for r in v),
+                      "max_rel_dimpact": max(r[2] for r in v),
+                      "median_abs_dphi_V": statistics.median(r[0] for r in v)}
+    return out
+
+
+def merge_tip_stats(dist, events: int, wall_s: float, latencies_ms) -> dict:
+    """Whole-job figures of the many-tip run: events summed over ranks, the
+    slowest rank's wall time, and the per-event latency percentiles over the
+    events of every rank (gathered to every rank).  Without a process group
+    the values pass through."""
+    from tapsim_modified_b200.serving import latency_percentiles
+    lat = [float(x) for x in latencies_ms]
+    if dist:
+        parts = [None] * dist.get_world_size()
+        dist.all_gather_object(parts, (int(events), float(wall_s), lat))
+    else:
+        parts = [(int(events), float(wall_s), lat)]
+    total = sum(p[0] for p in parts)
+    wall = max(p[1] for p in parts)
+    merged = [x for p in parts for x in p[2]]
+    return {"events": total, "wall_s": wall, "events_per_s": total / wall if wall > 0 else None,
+            **latency_percentiles(merged), "latencies": len(merged)}
+
+
+def run_many_tips(args, rank: int, world: int, dist):
+    """Many-tip serving: args.tips seeded tips (cap radius U(4,12) nm, shank
+    U(10,30) nm, half angle U(0,15) deg), split over the ranks by the greedy
+    size-balanced partition; each round runs one event of every tip of the
+    rank (tg_run_tips: one host thread per tip's handle, the device work of
+    all tips overlapping on their streams).  W warm-up rounds, K timed
+    rounds; aggregate events/s and the p50/p99 per-event latency over all
+    ranks."""
+    import ctypes as C
+
+    import torch
+
+    from tapsim_modified_b200 import _native as N
+    from tapsim_modified_b200.serving import estimated_atoms, partition_tips, run_tips, tip_specs
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, Mesh, solve_opts
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    specs = tip_specs(args.tips)
+    sizes = [estimated_atoms(s) for s in specs]
+    mine = partition_tips(sizes, world)[rank]
+    t0 = time.perf_counter()
+    meshes = [Mesh.from_tip(**specs[k]) for k in mine]
+    t_mesh = time.perf_counter() - t0
+    opts = EvaporationOptions.from_ini(None)
+    sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4, preconditioner=PRECOND)
+    grids, evopts = [], []
+    t0 = time.perf_counter()
+    for m in meshes:
+        g = Grid(m)
+        g.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
+        ev = Evaporation(g, opts, relax_mode=1, solve=sopts)   # surface set and first selection
+        grids.append(g)
+        evopts.append(ev.opts)
+    t_setup = time.perf_counter() - t0
+    for w in range(args.warmup):
+        run_tips(grids, evopts, w + 1)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    lat = []
+    with ClockSampler(local) as clocks:
+        t1 = time.perf_counter()
+        for k in range(args.steps):
+            _, l, _ = run_tips(grids, evopts, args.warmup + k + 1)
+            lat.extend(l.tolist())
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t1
+    cells = sum(m.num_nodes for m in meshes)
+    for g in grids:
+        g.close()
+    stats = merge_tip_stats(dist, args.steps * len(mine), wall, lat)
+    if rank != 0:
+        return None
+    return {"metric": "many-tip serving: aggregate events/s and p50/p99 per-event latency, resid<=1e-8",
+            "value": stats["events_per_s"], "unit": "events/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": stats["wall_s"] * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64 residual/update + f32 inner CG, f64 flights",
+            "data": "synthetic (seeded bcc Fe [110] tips)",
+            "config": {"workload": f"{args.tips} tips, cap radius U(4,12) nm, shank U(10,30) nm, half angle "
+                                   "U(0,15) deg, vacuum to 1 um; a step is one event of every tip, each relaxed "
+                                   f"to rel. residual <= {REL_TOL:g}",
+                       "tips_rank0": len(mine), "cells_rank0": cells,
+                       "partition": "greedy size-balanced (largest first) over the ranks, no data-path exchange",
+                       "latency_ms": {"p50": stats["p50"], "p99": stats["p99"], "events": stats["latencies"]},
+                       "setup_s": {"meshes_rank0": t_mesh, "upload_and_initial_relaxation_rank0": t_setup},
+                       "wall_clock": "host clock around the K rounds, synchronised; max over ranks"},
+            "clocks": clocks.summary()}
 
 
 def hop_ball(row_ptr, col, site: int, hops: int):
@@ -499,23 +680,116 @@ def run_warm_bounds(args):
     return out
 
 
-def run_reference(args, rank: int, world: int):
-    if rank != 0:
-        return None
+def prepare_tip(args):
+    """Child-process step of the reference arm: builds the timed tip (seed
+    of rank 0), relaxes it on the device to rel. residual 1e-8 and writes
+    what the reference resumes from into args.prepare_tip: the configuration
+    (ref.cfg), a TAPSIM dump with the relaxed potentials (ref.dump), and
+    pairs.json, a seeded sample of neighbour pairs with this library's
+    couplings for the reference to check.  The reference arm's own process
+    never loads this library."""
     import numpy as np
 
-    mesh = build_mesh(args.tip, seed=1)
-    from tapsim_modified_b200.tapsim import Grid  # noqa: F401  (potentials come from the mesh presets)
+    from tapsim_modified_b200.tapsim import Grid
+    out = Path(args.prepare_tip)
+    mesh = build_mesh(args.tip, seed=tip_seed(0))
+    g = Grid(mesh)
+    g.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
+    phi = g.potentials()
+    g.close()
+    mesh.write_config(str(out / "ref.cfg"))
+    mesh.write_dump(str(out / "ref.dump"), phi.astype(np.float32))
+    a = mesh.arrays()
+    rp, col, cpl, typ = a["row_ptr"], a["col"], a["coupling"], a["type"]
+    types = a["types"]
+    rng = np.random.default_rng(5)
+    # pairs around the surface (an atom and a vacuum neighbour) and deeper
+    # in the vacuum, where the faces are large
+    atoms = np.nonzero(typ == 4)[0]
+    vac = np.nonzero(typ != 4)[0]
+    pairs = []
+    for surface, pool in ((True, atoms), (False, vac)):
+        taken = 0
+        for i in rng.choice(pool, size=min(len(pool), 4000), replace=False):
+            # an atom with a vacuum neighbour, or any vacuum cell's neighbour
+            cand = [q for q in range(rp[i], rp[i + 1]) if not surface or typ[col[q]] != typ[i]]
+            if not cand:
+                continue
+            q = int(rng.choice(cand))
+            j = int(col[q])
+            ti, tj = types[int(typ[i])], types[int(typ[j])]
+            if ti["neumann"] or tj["neumann"]:
+                continue
+            ei, ej = float(ti["epsilon"]), float(tj["epsilon"])
+            pairs.append({"i": int(i), "j": j, "coupling": float(cpl[q]), "eps_factor": 2 * ei * ej / (ei + ej)})
+            taken += 1
+            if taken == 100:
+                break
+    (out / "pairs.json").write_text(json.dumps({"cells": mesh.num_nodes, "atoms": int(len(atoms)), "pairs": pairs}))
+    return {"prepared": str(out), "cells": mesh.num_nodes}
+
+
+def reference_faces(dump: Path, pairs: list) -> dict:
+    """The reference's own coupling (computeCoupling, grid_3d.cpp:1392-1409:
+    eps factor * area(0.5 d) / d from get_voronoiFace + finiteArea) of each
+    sampled pair, against the coupling this library computed for the dump;
+    relative differences binned by face area (the reference forms lengths in
+    float, so atomic-scale faces carry float noise)."""
+    harness = ROOT / "oracle" / "_ref" / "ref_harness"
+    argv = [str(harness), "face", str(dump)]
+    for p in pairs:
+        argv += [str(p["i"]), str(p["j"])]
+    r = subprocess.run(argv, check=True, capture_output=True, text=True)
+    got = {}
+    for line in r.stdout.splitlines():
+        if line.startswith("pair"):
+            f = line.split()
+            got[(int(f[1]), int(f[2]))] = (float(f[8]), float(f[12]))  # areaHalf, d
+    bins = {"area >= 1e-18 m^2": [], "1e-19 <= area < 1e-18": [], "area < 1e-19": []}
+    for p in pairs:
+        area, d = got[(p["i"], p["j"])]
+        ref = p["eps_factor"] * area / d
+        rel = abs(p["coupling"] - ref) / max(abs(ref), 1e-300) if ref != 0.0 or p["coupling"] != 0.0 else 0.0
+        key = "area >= 1e-18 m^2" if area >= 1e-18 else ("1e-19 <= area < 1e-18" if area >= 1e-19 else "area < 1e-19")
+        bins[key].append(rel)
+    return {k: {"pairs": len(v), "max_rel_diff": max(v) if v else None,
+                "median_rel_diff": statistics.median(v) if v else None} for k, v in bins.items()}
+
+
+def run_reference(args, rank: int, world: int):
+    """The reference TAPSim (oracle/_ref/ref_harness, built from the
+    reference's own sources) on the timed tip, on the host cores.  A child
+    process prepares the tip with this library (mesh, relaxation to 1e-8 on
+    the device, TAPSIM dump); this process runs only the reference:
+
+      value          the reference's shipped default ini: localRelax (shell 3)
+                     plus one global sweep per event, no residual guarantee
+      converged_ini  REFRESH_RELAXATION_INTERVAL = 1, threshold 0: relaxation
+                     to the float fixed point after every event, the
+                     reference's nearest analogue of a residual target
+      couplings      the reference's own computeCoupling of sampled pairs
+                     against the couplings in the dump it resumes from"""
+    if rank != 0:
+        return None
+    from tapsim_modified_b200.tapsim import INI_DEFAULTS  # the ini keys only; no library load
+    threads = os.cpu_count() or 1
     with tempfile.TemporaryDirectory(prefix=".bench-", dir=str(ROOT)) as td:
-        dump = Path(td) / "ref.dump"
-        cfg = Path(td) / "ref.cfg"
-        mesh.write_dump(str(dump))
-        mesh.write_config(str(cfg))
-        threads = os.cpu_count() or 1
+        env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+        subprocess.run([sys.executable, str(ROOT / "bench.py"), "--prepare-tip", td, "--tip", args.tip], check=True,
+                       env=env)
+        dump, cfg = Path(td) / "ref.dump", Path(td) / "ref.cfg"
+        prep = json.loads((Path(td) / "pairs.json").read_text())
         walls, kind = reference_run(dump, cfg, args.warmup + args.steps, threads)
+        conv_ini = dict(INI_DEFAULTS)
+        conv_ini.update({"REFRESH_RELAXATION_INTERVAL": "1", "REFRESH_RELAXATION_ERROR_THRESHOLD": "0.0"})
+        conv_walls, conv_kind = reference_run(dump, cfg, args.converged_events, threads, ini=conv_ini,
+                                              label="reference TAPSim converged ini: relaxation to the float fixed "
+                                                    "point after every event (REFRESH_RELAXATION_INTERVAL 1, "
+                                                    "threshold 0)")
+        faces = reference_faces(dump, prep["pairs"])
     timed = walls[args.warmup:]
     per = sum(timed) / len(timed)
-    arrays = mesh.arrays()
+    conv_per = statistics.median(conv_walls)
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -530,8 +804,15 @@ def run_reference(args, rank: int, world: int):
         "vs_baseline": None,
         "dtype": "f32 storage, f64 accumulation (reference)",
         "data": "synthetic (same seeded tip as our arm)",
-        "config": {"workload": f"{args.tip}: {int((arrays['type'] == 4).sum())} atoms, {mesh.num_nodes} cells; "
-                               f"{kind}; no residual guarantee"},
+        "config": {"workload": f"{args.tip}: {prep['atoms']} atoms, {prep['cells']} cells; value: {kind} (no "
+                               f"residual guarantee); config.converged_ini: {conv_kind}",
+                   "converged_ini": {"value": 1.0 / conv_per, "events": len(conv_walls),
+                                     "ms_per_event_median": conv_per * 1e3},
+                   "couplings": faces,
+                   "resumed_from": "TAPSIM dump of the tip written by a child process with this library (mesh, "
+                                   "couplings, potentials relaxed to rel. residual 1e-8 on the device); resumed "
+                                   "with --no-sync, its couplings checked against the reference's computeCoupling "
+                                   "on sampled pairs (config.couplings)"},
         "cpu_baseline": {"value": 1.0 / per, "unit": "events/s", "cores": threads, "kind": "reference",
                          "sample": f"{len(timed)} events after {args.warmup} warm-up, {kind}"},
         "e2e": {"value": 1.0 / per, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -552,11 +833,23 @@ def main():
     ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
     ap.add_argument("--train-steps", type=int, default=600, help="Adam steps of the learned warm start")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
+    ap.add_argument("--long-events", type=int, default=200,
+                    help="events run and timed after the K timed ones on the headline arm")
+    ap.add_argument("--precision-events", type=int, default=20,
+                    help="events of the FP32-inner vs FP64 per-event error comparison (0: skip)")
+    ap.add_argument("--converged-events", type=int, default=3,
+                    help="events of the reference's converged ini timed beside its default ini (reference arm)")
+    ap.add_argument("--prepare-tip", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--tips", type=int, default=0,
+                    help="many-tip serving: this many seeded tips, one event of each per step (0: off)")
     ap.add_argument("--warm-bounds", action="store_true",
                     help="measure the iterations of exact and recycled starts instead of the events/s line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.prepare_tip:
+        log(json.dumps(prepare_tip(args)))
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     dist = None
@@ -567,6 +860,8 @@ def main():
         dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(minutes=20))
     if args.warm_bounds:
         out = run_warm_bounds(args) if rank == 0 else None
+    elif args.tips > 0:
+        out = run_many_tips(args, rank, world, dist)
     elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

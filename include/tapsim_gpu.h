@@ -117,7 +117,7 @@ int tg_local_relax(tg_handle* h, int32_t node, int32_t shell, double threshold, 
 typedef struct {
     double rel_tol;           /* e.g. 1e-8 */
     int32_t max_outer;        /* FP64 defect-correction steps */
-    int32_t max_inner;        /* FP32 iterations per step */
+    int32_t max_inner;        /* inner iterations per step */
     double inner_rtol;        /* inner relative reduction per step */
     /* Start of a solve that follows removals from a converged state:
      *   0  the current potentials (the previous event's solution; plain),
@@ -134,6 +134,14 @@ typedef struct {
      *      built on the host at the first solve that asks for it and again
      *      once removals have added 2% more cells to the system. */
     int32_t preconditioner;
+    /* Arithmetic of the inner iterations on the non-Neumann free cells:
+     *   0  FP32 (couplings, vectors and recurrences; the default),
+     *   1  FP64 couplings, vectors and recurrences, the multigrid V-cycle
+     *      still FP32 (needs preconditioner 1 and warm_start 0).  Its FP64
+     *      copy of the couplings is built at the first such solve.
+     * The residual test, its norm and the potential update are FP64 in both;
+     * the Neumann rows' inner iterations are FP32 in both. */
+    int32_t inner_precision;
 } tg_solve_opts;
 typedef struct {
     int32_t outer;            /* defect-correction steps taken */
@@ -253,6 +261,14 @@ typedef struct {
     int32_t integrator;         /* TRAJECTORY_INTEGRATOR_TYPE: 0 Euler, 1 Cash-Karp (the reference's default) */
     int32_t stepper;            /* TRAJECTORY_STEPPER_TYPE: 0 none, 1 error-restricted (default),
                                    2 geometry-restricted, 3 adaptive (trajectory_3d.cpp:358-532) */
+    /* Arithmetic of the Cash-Karp steps and of the error-restricted step
+     * control: 0 FP64 (default), 1 FP32 (as the reference integrates,
+     * trajectory_3d.cpp:583-676), 2 FP64 while the ion is within fp64_radius
+     * [m] of its start, where the field is steep, and FP32 beyond.  Point
+     * location and field interpolation are FP64 (exact orientation) in all
+     * three; the Euler integrator is FP64. */
+    int32_t precision;
+    double fp64_radius;
 } tg_trace_opts;
 typedef struct {
     float stop[3];              /* impact after extrapolation to the top plane [m] */
@@ -331,6 +347,17 @@ typedef struct {
     int32_t path_cap;
     tg_path_point* path_points;
     float* path_errors;
+    /* Forced removals (the reference harness's --force, for comparing a run
+     * with another one event by event past a near-tie): when force_nodes is
+     * not NULL, the k-th event of a call (k < force_count) removes
+     * force_nodes[k] instead of the chosen cell; later events choose as
+     * usual.  The cell must be on the surface (TG_ERR_ARGUMENT otherwise).
+     * The record's probability is then the forced cell's, while
+     * best_probability stays the chosen cell's: probability <
+     * best_probability marks an event where the forced cell was not this
+     * run's choice.  No counterpart in Process::evaporation. */
+    const int32_t* force_nodes;
+    int32_t force_count;
 } tg_event_opts;
 typedef struct {
     int32_t node;
@@ -358,6 +385,17 @@ int tg_run_event(tg_handle* h, const tg_event_opts* opts, int32_t event_index, t
  * the records before it are complete. */
 int tg_run_events(tg_handle* h, const tg_event_opts* opts, int32_t first_index, int32_t count,
                   tg_event_record* recs, int32_t* done);
+/* One event on each of `count` independent tips (many-tip serving; no
+ * counterpart in the reference, which evaporates one specimen per process):
+ * tg_run_events(handles[k], &opts[k], first_index, 1, &recs[k]) for every k,
+ * the handles driven concurrently from a pool of host threads (threads <= 0:
+ * one per handle up to the host's cores; each handle by one thread, so the
+ * one-thread-per-handle rule holds), their device work overlapping on the
+ * handles' own streams.  latency_ms[k]: the host wall time of tip k's event;
+ * status[k]: its return code.  Returns TG_OK when every tip's event ran, else
+ * the first failing code (TG_ERR_NO_SURFACE for a tip that has run out). */
+int tg_run_tips(tg_handle* const* handles, int32_t count, const tg_event_opts* opts, int32_t first_index,
+                tg_event_record* recs, float* latency_ms, int32_t* status, int32_t threads);
 
 /* ---- learned near-field warm start (no counterpart in the reference) -----
  * A message-passing network (an input layer and four message layers of
@@ -457,6 +495,10 @@ int tg_mesh_from_dump(const char* dump_file, const char* config_file, tg_mesh** 
 void tg_mesh_destroy(tg_mesh* m);
 /* Configuration::Table::temperature of the mesh's configuration [K] */
 float tg_mesh_temperature(const tg_mesh* m);
+/* Configuration::Table::operator[](name).id() (configuration.h): the id of
+ * the cell type with that name in the mesh's configuration, -1 if none
+ * (VACUUM_CELL_IDENTIFIER -> the vacuum id the event loop takes). */
+int32_t tg_mesh_type_id(const tg_mesh* m, const char* name);
 /* Fills a description whose pointers stay valid while the mesh lives. */
 int tg_mesh_describe(const tg_mesh* m, tg_mesh_desc* desc, int32_t* nnz);
 int tg_mesh_write_node_file(const tg_mesh* m, const char* path, int32_t binary);

@@ -41,7 +41,8 @@ class tg_mesh_desc(C.Structure):
 
 class tg_solve_opts(C.Structure):
     _fields_ = [("rel_tol", C.c_double), ("max_outer", C.c_int32), ("max_inner", C.c_int32),
-                ("inner_rtol", C.c_double), ("warm_start", C.c_int32), ("preconditioner", C.c_int32)]
+                ("inner_rtol", C.c_double), ("warm_start", C.c_int32), ("preconditioner", C.c_int32),
+                ("inner_precision", C.c_int32)]
 
 
 class tg_solve_info(C.Structure):
@@ -59,7 +60,8 @@ class tg_select_info(C.Structure):
 
 class tg_trace_opts(C.Structure):
     _fields_ = [("time_step", C.c_double), ("min_time_step", C.c_double), ("error_threshold", C.c_double),
-                ("max_steps", C.c_int32), ("stepper_limit", C.c_int32), ("walk_limit", C.c_int32), ("integrator", C.c_int32), ("stepper", C.c_int32)]
+                ("max_steps", C.c_int32), ("stepper_limit", C.c_int32), ("walk_limit", C.c_int32), ("integrator", C.c_int32), ("stepper", C.c_int32),
+                ("precision", C.c_int32), ("fp64_radius", C.c_double)]
 
 
 class tg_impact(C.Structure):
@@ -96,7 +98,8 @@ class tg_event_opts(C.Structure):
                 ("solve", tg_solve_opts), ("trace", tg_trace_opts), ("trace_enabled", C.c_int32),
                 ("normal_enabled", C.c_int32), ("prob_mode", C.c_int32), ("choice_mode", C.c_int32),
                 ("temperature", C.c_float), ("rng_seed", C.c_uint32), ("initial_velocity", C.c_int32),
-                ("path_cap", C.c_int32), ("path_points", C.c_void_p), ("path_errors", C.c_void_p)]
+                ("path_cap", C.c_int32), ("path_points", C.c_void_p), ("path_errors", C.c_void_p),
+                ("force_nodes", C.c_void_p), ("force_count", C.c_int32)]
 
 
 class tg_event_record(C.Structure):
@@ -159,6 +162,7 @@ SIGNATURES = {
     "tg_potential_at": (C.c_int, [_P, _I, _P, _P, _P]),
     "tg_run_event": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, C.POINTER(tg_event_record)]),
     "tg_run_events": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, _I, _P, C.POINTER(C.c_int32)]),
+    "tg_run_tips": (C.c_int, [_P, _I, _P, _I, _P, _P, _P, _I]),
     "tg_timer_start": (C.c_int, [_P]),
     "tg_timer_stop": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "tg_launch_count": (C.c_int64, [_P]),
@@ -188,6 +192,7 @@ SIGNATURES = {
     "tg_mesh_from_dump": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_P)]),
     "tg_mesh_destroy": (None, [_P]),
     "tg_mesh_temperature": (C.c_float, [_P]),
+    "tg_mesh_type_id": (C.c_int32, [_P, C.c_char_p]),
     "tg_mesh_describe": (C.c_int, [_P, C.POINTER(tg_mesh_desc), C.POINTER(_I)]),
     "tg_mesh_write_node_file": (C.c_int, [_P, C.c_char_p, _I]),
     "tg_mesh_write_config": (C.c_int, [_P, C.c_char_p]),

@@ -16,6 +16,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libtapsim_b200.so"
+PROGRAM = PKG / "tapsim_b200"
+HOST_PROGRAM = "host/tapsim_b200.cpp"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", "g++")
@@ -62,6 +64,12 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), *map(str, objs),
               "-Xcompiler", "-pthread", "-lpthread"])
+    # the C++ host program over the C ABI (evaporation / resumption
+    # commands), linked against the in-tree library
+    src = CSRC / HOST_PROGRAM
+    if force or _stale(PROGRAM, src, [ROOT / "include" / "tapsim_gpu.h", LIB]):
+        _run([CXX, "-O2", "-std=c++17", "-o", str(PROGRAM), str(src), f"-L{PKG}", "-ltapsim_b200",
+              "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

@@ -198,16 +198,130 @@ __global__ void k_vcg_warm_residual(VSys v, int slices, double* acc) {
 }
 
 // r of the Neumann rows += sum over V neighbours ceff_ij x_j
-__global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int count, float* rN) {
+// (x from the FP64 vector when x64 is given)
+__global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int count, float* rN,
+                                     const double* x64) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const int i = rows[t];
     float s = 0.0f;
     for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
         const int sl = v.slot_of[m.col[q]];
-        if (sl >= 0) s += m.ceff32[q] * v.x[sl];
+        if (sl >= 0) s += m.ceff32[q] * (x64 ? (float)x64[sl] : v.x[sl]);
     }
     rN[i] += s;
+}
+
+// ---- FP64 inner iterations (tg_solve_opts.inner_precision 1) ----
+// The same single-reduction PCG with its operator (FP64 couplings and
+// diagonal at the SELL positions of the FP32 ones), vectors and recurrences
+// in FP64.  The multigrid V-cycle stays FP32: it reads r rounded to float
+// (written beside r64 by init and update) and returns u in FP32, which the
+// FP64 recurrences take exactly.
+
+// val64 and d64 from the FP64 couplings the rows see (ceff64) and the FP64
+// diagonals, through the global-entry -> SELL-position map; the padding
+// entries keep the zeros they were cleared to
+__global__ void k_vcg64_derive(DevMesh m, VSys v, int nnz) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += stride) {
+        const int p = v.vpos[q];
+        if (p >= 0) v.val64[p] = m.ceff64[q];
+    }
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s <= v.capacity; s += stride) {
+        const int i = s < v.capacity ? v.node_of[s] : -1;
+        v.d64[s] = i >= 0 ? m.diag64[i] : 1.0;
+    }
+}
+
+// r64 = the kept FP64 residual of the slot's node (0 for padding), r = its
+// float copy for the V-cycle, x64 = p64 = s64 = 0, rho_0 = r.r
+__global__ void k_vcg64_init(VSys v, int slots, const double* __restrict__ rnode) {
+    double rr = 0.0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
+        const int i = v.node_of[s];
+        const double r = i >= 0 ? rnode[i] : 0.0;
+        v.r64[s] = r;
+        v.r[s] = (float)r;
+        v.x64[s] = 0.0;
+        v.p64[s] = 0.0;
+        v.s64[s] = 0.0;
+        rr += r * r;
+    }
+    block_sum_atomic<kBlock>(rr, &v.scal[3]);
+}
+
+// w64 = A64 u over SELL-32 slices; delta = w.u -> scal[4*it+1], gamma = r.u
+// -> scal[4*it]
+__global__ void k_vcg64_spmv(VSys v, int slices, int it, double target) {
+    if (cg_done(v.scal, it, target)) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    double dl = 0.0, gl = 0.0;
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
+        const int base = v.slice_start[warp];
+        const int width = v.slice_width[warp];
+        const int s = warp * 32 + lane;
+        const int* __restrict__ col = v.col + base + lane;
+        const double* __restrict__ val = v.val64 + base + lane;
+        const float* __restrict__ uu = v.u;
+        double acc = 0.0;
+        int k = 0;
+        for (; k + 8 <= width; k += 8) {
+            int c[8];
+            double a[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                c[j] = __ldcs(col + 32 * (k + j));
+                a[j] = __ldcs(val + 32 * (k + j));
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc += a[j] * (double)__ldg(uu + c[j]);
+        }
+        for (; k < width; k++) acc += __ldcs(val + 32 * k) * (double)__ldg(uu + __ldcs(col + 32 * k));
+        const double u = (double)v.u[s];
+        const double w = v.d64[s] * u - acc;
+        v.w64[s] = w;
+        dl += w * u;
+        gl += v.r64[s] * u;
+    }
+    block_sum2_atomic<kBlock>(dl, gl, &v.scal[4 * it + 1], &v.scal[4 * it]);
+}
+
+// p64 = u + beta p64, s64 = w64 + beta s64, x64 += alpha p64,
+// r64 -= alpha s64 (and its float copy), rho_{it+1} = r.r
+__global__ void k_vcg64_update(VSys v, int slots, int it, double target) {
+    if (cg_done(v.scal, it, target)) return;
+    double alpha, beta;
+    cg_coeffs(v.scal, it, &alpha, &beta);
+    if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[4 * it + 2] = alpha;
+    double rr = 0.0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
+        const double p = (double)v.u[s] + beta * v.p64[s];
+        const double sv = v.w64[s] + beta * v.s64[s];
+        v.p64[s] = p;
+        v.s64[s] = sv;
+        v.x64[s] += alpha * p;
+        const double r = v.r64[s] - alpha * sv;
+        v.r64[s] = r;
+        v.r[s] = (float)r;
+        rr += r * r;
+    }
+    block_sum_atomic<kBlock>(rr, &v.scal[4 * (it + 1) + 3]);
+}
+
+// phi64[node] += x64[slot] (hist[slot] += x64[slot] when recording); clears
+// the slot's vectors
+__global__ void k_vcg64_apply(DevMesh m, VSys v, int slots, int record) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots) return;
+    const int i = v.node_of[s];
+    if (i >= 0) {
+        m.phi64[i] += v.x64[s];
+        if (record) v.hist[s] += (float)v.x64[s];
+    }
+    v.x64[s] = v.r64[s] = v.p64[s] = v.s64[s] = v.w64[s] = 0.0;
+    v.x[s] = v.r[s] = v.u[s] = v.w[s] = v.p[s] = v.sv[s] = 0.0f;
 }
 
 // FP64 residual of the V rows, sum r^2 into *acc; with bacc also the
@@ -292,9 +406,15 @@ __device__ __forceinline__ void vsys_set_row_sum(VSys v, int s) {
     v.g[s] = (float)((double)v.d[s] - sum);
 }
 
-__device__ __forceinline__ void vsys_set_val(VSys v, int p, float a) {
+__device__ __forceinline__ void vsys_set_val(VSys v, int p, float a, double a64) {
     v.val[p] = a;
     v.val16[p] = __float2bfloat16_rn(a);
+    if (v.val64) v.val64[p] = a64;
+}
+
+__device__ __forceinline__ void vsys_set_diag(const DevMesh& m, VSys v, int s, int i) {
+    v.d[s] = m.diag32[i];
+    if (v.d64) v.d64[s] = m.diag64[i];
 }
 
 // Appends the row of a node that has just become a non-Neumann free cell
@@ -310,7 +430,7 @@ __device__ void vsys_add_row(const DevMesh& m, VSys v, int i) {
         } else {
             v.slot_of[i] = s;
             v.node_of[s] = i;
-            v.d[s] = m.diag32[i];
+            vsys_set_diag(m, v, s, i);
         }
     }
     s = __shfl_sync(0xffffffffu, s, 0);
@@ -333,13 +453,13 @@ __device__ void vsys_add_row(const DevMesh& m, VSys v, int i) {
             }
             const int sj = v.slot_of[j];
             v.col[base + 32 * k] = sj >= 0 ? sj : v.capacity;
-            vsys_set_val(v, base + 32 * k, m.ceff32[q]);
+            vsys_set_val(v, base + 32 * k, m.ceff32[q], m.ceff64[q]);
             v.vpos[q] = base + 32 * k;
             k++;
         }
         for (; k < width; k++) {
             v.col[base + 32 * k] = v.capacity;
-            vsys_set_val(v, base + 32 * k, 0.0f);
+            vsys_set_val(v, base + 32 * k, 0.0f, 0.0);
         }
         vsys_set_row_sum(v, s);
     }
@@ -352,9 +472,9 @@ __device__ void vsys_add_row(const DevMesh& m, VSys v, int i) {
         const int p = v.vpos[m.rev[q]];
         if (p >= 0) {
             v.col[p] = s;
-            vsys_set_val(v, p, m.ceff32[m.rev[q]]);
+            vsys_set_val(v, p, m.ceff32[m.rev[q]], m.ceff64[m.rev[q]]);
         }
-        v.d[sj] = m.diag32[j];
+        vsys_set_diag(m, v, sj, j);
         vsys_set_row_sum(v, sj);
     }
     __syncwarp();
@@ -373,15 +493,15 @@ __global__ void k_vsys_refresh(DevMesh m, VSys v, const int32_t* nodes, int coun
     for (int k = 0; k < count; k++) {
         const int i = nodes[k];
         const int si = v.slot_of[i];
-        if (si >= 0 && lane == 0) v.d[si] = m.diag32[i];
+        if (si >= 0 && lane == 0) vsys_set_diag(m, v, si, i);
         for (int q = m.row_ptr[i] + lane; q < m.row_ptr[i + 1]; q += 32) {
-            if (si >= 0 && v.vpos[q] >= 0) vsys_set_val(v, v.vpos[q], m.ceff32[q]);
+            if (si >= 0 && v.vpos[q] >= 0) vsys_set_val(v, v.vpos[q], m.ceff32[q], m.ceff64[q]);
             const int j = m.col[q];
             const int sj = v.slot_of[j];
             if (sj < 0) continue;
             const int p = v.vpos[m.rev[q]];
-            if (p >= 0) vsys_set_val(v, p, m.ceff32[m.rev[q]]);
-            v.d[sj] = m.diag32[j];
+            if (p >= 0) vsys_set_val(v, p, m.ceff32[m.rev[q]], m.ceff64[m.rev[q]]);
+            vsys_set_diag(m, v, sj, j);
             vsys_set_row_sum(v, sj);
         }
         __syncwarp();
@@ -449,8 +569,28 @@ void launch_vcg_warm_residual(const VSys& v, int slots, double* acc, cudaStream_
     }
 }
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
-                               cudaStream_t s) {
-    if (count > 0) { count_launch(); k_vcg_couple_neumann<<<blocks(count), kBlock, 0, s>>>(m, v, rows, count, rN); }
+                               cudaStream_t s, bool fromX64) {
+    if (count > 0) {
+        count_launch();
+        k_vcg_couple_neumann<<<blocks(count), kBlock, 0, s>>>(m, v, rows, count, rN, fromX64 ? v.x64 : nullptr);
+    }
+}
+void launch_vcg64_derive(const DevMesh& m, const VSys& v, int nnz, cudaStream_t s) {
+    count_launch();
+    k_vcg64_derive<<<4096, kBlock, 0, s>>>(m, v, nnz);
+}
+void launch_vcg64_init(const VSys& v, int slots, const double* rnode, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg64_init<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, rnode); }
+}
+void launch_vcg64_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s) {
+    const int slices = (slots + 31) / 32;
+    if (slices > 0) { count_launch(); k_vcg64_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, it, target); }
+}
+void launch_vcg64_update(const VSys& v, int slots, int it, double target, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg64_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, it, target); }
+}
+void launch_vcg64_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg64_apply<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, record ? 1 : 0); }
 }
 void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, int count, double* acc, double* bacc,
                          cudaStream_t s, double* r64, double* b64) {

@@ -486,15 +486,18 @@ __device__ __forceinline__ void path_error(const TraceParams& tp, int slot) {
     for (int j = 0; j < 6; j++) e[j] = sqrtf(e[j] * e[j] + e[6 + j] * e[6 + j]);
 }
 
-// One ion from x0 (velocity v0, charge/mass k) into *out; with kPath its
-// path and error estimate go to slot `slot` of tp's path buffers (a
-// separate instantiation, so that the flights without a path keep their
-// registers).
-template <bool kPath>
-__device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k, int guessTet, const TraceParams& tp,
-                                          unsigned rot, int slot, ImpactOut* out) {
-    // Cash-Karp tableau; the stage loops are unrolled so that every index is
-    // a compile-time constant and the stage vectors stay in registers
+// One Cash-Karp trial step (o5_integrator, trajectory_3d.cpp:583-676) of
+// length dt from (x, v), its arithmetic in R: FP64, or FP32 as the reference
+// integrates.  The state enters and leaves in double (rounded to R on the
+// way in, so in FP32 it is the float state); the points of the stages are
+// located and their fields interpolated as in FP64, then rounded to R.
+// *rel: the largest relative error of a position or velocity component (as
+// errorRestricted_stepper forms it, trajectory_3d.cpp:366-387).  Returns
+// false when a walk exceeded its bound.
+template <typename R>
+__device__ __forceinline__ bool ck_trial(const DevMesh& m, TetCache& fc, const TraceParams& tp, unsigned& rot, int& cur,
+                                         V3 x, V3 v, double k, double dt, V3* nxo, V3* nvo, V3* exo, V3* evo,
+                                         double* relo) {
     constexpr double B[6][5] = {{0, 0, 0, 0, 0},
                                 {1.0 / 5.0, 0, 0, 0, 0},
                                 {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
@@ -503,7 +506,78 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                                 {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
     constexpr double C5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
     constexpr double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
+    const R xx = (R)x.x, xy = (R)x.y, xz = (R)x.z, vx = (R)v.x, vy = (R)v.y, vz = (R)v.z;
+    const R kk = (R)k, h = (R)dt;
+    R dx[6][3], dv[6][3];
+    bool walkOk = true;
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        R px = xx, py = xy, pz = xz, qx = vx, qy = vy, qz = vz;
+#pragma unroll
+        for (int j = 0; j < s; j++) {
+            const R b = (R)B[s][j];
+            px += b * dx[j][0]; py += b * dx[j][1]; pz += b * dx[j][2];
+            qx += b * dv[j][0]; qy += b * dv[j][1]; qz += b * dv[j][2];
+        }
+        V3 E;
+        walkOk &= fast_field(m, fc, V3{(double)px, (double)py, (double)pz}, cur, tp.walk_limit, rot, &E, &cur);
+        dv[s][0] = (R)E.x * kk * h; dv[s][1] = (R)E.y * kk * h; dv[s][2] = (R)E.z * kk * h;
+        dx[s][0] = qx * h; dx[s][1] = qy * h; dx[s][2] = qz * h;
+    }
+    R nx[3] = {xx, xy, xz}, nv[3] = {vx, vy, vz}, ex[3] = {0, 0, 0}, ev[3] = {0, 0, 0};
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        const R c5 = (R)C5[s], dc = (R)(C5[s] - C4[s]);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            nx[c] += c5 * dx[s][c];
+            nv[c] += c5 * dv[s][c];
+            ex[c] += dc * dx[s][c];
+            ev[c] += dc * dv[s][c];
+        }
+    }
+    R rel = 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (nx[c] != (R)0) rel = fmax(rel, fabs(ex[c] / nx[c]));
+        if (nv[c] != (R)0) rel = fmax(rel, fabs(ev[c] / nv[c]));
+    }
+    *nxo = V3{(double)nx[0], (double)nx[1], (double)nx[2]};
+    *nvo = V3{(double)nv[0], (double)nv[1], (double)nv[2]};
+    *exo = V3{(double)ex[0], (double)ex[1], (double)ex[2]};
+    *evo = V3{(double)ev[0], (double)ev[1], (double)ev[2]};
+    *relo = (double)rel;
+    return walkOk;
+}
 
+// errorRestricted_stepper's rule (trajectory_3d.cpp:396-421) in R: accept
+// when rel is below the threshold or the step is at its floor, and adjust
+// dt by (tol / rel)^(1/4) with the safety factor 0.9, growing by at most
+// 1.1 and shrinking by at least 0.9.  Returns true to accept.
+template <typename R>
+__device__ __forceinline__ bool error_rule(double relIn, const TraceParams& tp, double* dtIo) {
+    const R rel = (R)relIn, tol = (R)tp.tol;
+    R dt = (R)*dtIo;
+    const bool accept = rel < tol || dt == (R)tp.dt_min;
+    if (!accept || rel != (R)0) {
+        const R tmp = dt * (R)pow(tol / rel, (R)0.25) * (R)0.9;
+        if (accept) dt = tmp < dt ? dt * (R)1.1 : tmp;
+        else dt = tmp > dt ? dt * (R)0.9 : tmp;
+    }
+    *dtIo = (double)dt;
+    return accept;
+}
+
+// One ion from x0 (velocity v0, charge/mass k) into *out; with kPath its
+// path and error estimate go to slot `slot` of tp's path buffers (a
+// separate instantiation, so that the flights without a path keep their
+// registers).
+// kPrec: the arithmetic of the Cash-Karp steps (TraceParams::precision),
+// fixed per instantiation so that each kernel holds only its own registers.
+template <bool kPath, int kPrec>
+__device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k, int guessTet, const TraceParams& tp,
+                                          unsigned rot, int slot, ImpactOut* out) {
+    const V3 x0 = x;
     ImpactOut res;
     TetCache fc;
     fc.a.t = -1;
@@ -543,8 +617,17 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
             bool accepted = false;
             bool located = false;  // the accepted trial point is already located (steppers 2, 3)
             int nt = -1;
+            // FP32 arithmetic for this step: always with precision 1, and
+            // with precision 2 once the ion is beyond fp64_radius of its start
+            const double ddx = x.x - x0.x, ddy = x.y - x0.y, ddz = x.z - x0.z;
+            const bool lo = kPrec != 0 && tp.integrator == 1 &&
+                            (kPrec == 1 || ddx * ddx + ddy * ddy + ddz * ddz > tp.fp64_radius2);
             for (int tries = 0; tries < tp.stepper_limit; tries++) {
-                if (dt < tp.dt_min) dt = tp.dt_min;
+                if (lo) {
+                    if ((float)dt < (float)tp.dt_min) dt = (double)(float)tp.dt_min;
+                } else if (dt < tp.dt_min) {
+                    dt = tp.dt_min;
+                }
                 used = dt;
                 if (tp.integrator == 0) {
                     // o1_integrator (trajectory_3d.cpp:560-581): Euler; the
@@ -563,39 +646,14 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                     }
                     continue;
                 }
-                V3 dxs[6], dvs[6];
-                bool walkOk = true;
-#pragma unroll
-                for (int s = 0; s < 6; s++) {
-                    V3 ps = x, vs = v;
-#pragma unroll
-                    for (int j = 0; j < s; j++) {
-                        ps.x += B[s][j] * dxs[j].x; ps.y += B[s][j] * dxs[j].y; ps.z += B[s][j] * dxs[j].z;
-                        vs.x += B[s][j] * dvs[j].x; vs.y += B[s][j] * dvs[j].y; vs.z += B[s][j] * dvs[j].z;
-                    }
-                    V3 E;
-                    walkOk &= fast_field(m, fc, ps, cur, tp.walk_limit, rot, &E, &cur);
-                    dvs[s] = V3{E.x * k * dt, E.y * k * dt, E.z * k * dt};
-                    dxs[s] = V3{vs.x * dt, vs.y * dt, vs.z * dt};
-                }
+                V3 ex, evv;
+                double rel;
+                bool walkOk;
+                if (kPrec == 1) walkOk = ck_trial<float>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel);
+                else if (kPrec == 0) walkOk = ck_trial<double>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel);
+                else walkOk = lo ? ck_trial<float>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel)
+                                 : ck_trial<double>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel);
                 if (!walkOk) atomicOr(m.status, S_WALK_LIMIT);
-                nx = x; nv = v;
-                V3 ex{0, 0, 0}, evv{0, 0, 0};
-#pragma unroll
-                for (int s = 0; s < 6; s++) {
-                    nx.x += C5[s] * dxs[s].x; nx.y += C5[s] * dxs[s].y; nx.z += C5[s] * dxs[s].z;
-                    nv.x += C5[s] * dvs[s].x; nv.y += C5[s] * dvs[s].y; nv.z += C5[s] * dvs[s].z;
-                    const double dc = C5[s] - C4[s];
-                    ex.x += dc * dxs[s].x; ex.y += dc * dxs[s].y; ex.z += dc * dxs[s].z;
-                    evv.x += dc * dvs[s].x; evv.y += dc * dvs[s].y; evv.z += dc * dvs[s].z;
-                }
-                double rel = 0.0;
-                if (nx.x != 0.0) rel = fmax(rel, fabs(ex.x / nx.x));
-                if (nx.y != 0.0) rel = fmax(rel, fabs(ex.y / nx.y));
-                if (nx.z != 0.0) rel = fmax(rel, fabs(ex.z / nx.z));
-                if (nv.x != 0.0) rel = fmax(rel, fabs(evv.x / nv.x));
-                if (nv.y != 0.0) rel = fmax(rel, fabs(evv.y / nv.y));
-                if (nv.z != 0.0) rel = fmax(rel, fabs(evv.z / nv.z));
                 if (kPath) path_trial_error(tp, slot, ex, evv);
                 if (tp.stepper != 1) {
                     const int verdict = stepper_verdict(m, fc, tp, nx, tet, cur, rot, rel, &dt, &nt, &located);
@@ -605,16 +663,11 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                     }
                     continue;
                 }
-                if (rel < tp.tol || dt == tp.dt_min) {
-                    if (rel != 0.0) {
-                        const double tmp = dt * pow(tp.tol / rel, 0.25) * 0.9;
-                        if (tmp < dt) dt *= 1.1; else dt = tmp;
-                    }
+                if (kPrec == 0 ? error_rule<double>(rel, tp, &dt)
+                               : (lo ? error_rule<float>(rel, tp, &dt) : error_rule<double>(rel, tp, &dt))) {
                     accepted = true;
                     break;
                 }
-                const double tmp = dt * pow(tp.tol / rel, 0.25) * 0.9;
-                if (tmp > dt) dt *= 0.9; else dt = tmp;
             }
             if (!accepted) {
                 status = 2;  // STEPPER_LIMIT_PASSED
@@ -636,20 +689,21 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                 path_error(tp, slot);
                 path_point(tp, slot, res.steps, time + used, nx, nv, nt);
             }
+            const double tnext = lo ? (double)((float)time + (float)used) : time + used;
             if (nt < 0) {
                 // left the mesh: the previous point is the last inside it
                 res.last_tet = tet;
                 res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
                 x = nx;
                 v = nv;
-                time += used;
+                time = tnext;
                 tet = -1;
                 status = 5;  // SYSTEM_LIMIT_PASSED
                 break;
             }
             x = nx;
             v = nv;
-            time += used;
+            time = tnext;
             tet = nt;
             cur = nt;
         }
@@ -690,22 +744,22 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
     *out = res;
 }
 
-template <bool kPath>
+template <bool kPath, int kPrec>
 __global__ void k_trace(DevMesh m, int nIons, const float* start, const float* vel, const float* qm,
                         const int32_t* guess, TraceParams tp, ImpactOut* out) {
     const int ion = blockIdx.x * blockDim.x + threadIdx.x;
     if (ion >= nIons) return;
     const V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
     const V3 v = vel ? V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]} : V3{0, 0, 0};
-    trace_ion<kPath>(m, x, v, qm[ion], guess ? guess[ion] : 0, tp, (unsigned)ion * 7u, ion, out + ion);
+    trace_ion<kPath, kPrec>(m, x, v, qm[ion], guess ? guess[ion] : 0, tp, (unsigned)ion * 7u, ion, out + ion);
 }
 
 // A single ion from rest, its start passed by value (no staging copy)
-template <bool kPath>
+template <bool kPath, int kPrec>
 __global__ void k_trace_one(DevMesh m, float x, float y, float z, float vx, float vy, float vz, float qm, int guess,
                             TraceParams tp, ImpactOut* out) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    trace_ion<kPath>(m, V3{x, y, z}, V3{vx, vy, vz}, qm, guess, tp, 0u, 0, out);
+    trace_ion<kPath, kPrec>(m, V3{x, y, z}, V3{vx, vy, vz}, qm, guess, tp, 0u, 0, out);
 }
 
 __global__ void k_potential_at(DevMesh m, int n, const float* xyz, const int32_t* guess, int limit, float* out) {
@@ -725,8 +779,13 @@ void launch_trace(const DevMesh& m, int nIons, const float* start, const float* 
     if (nIons <= 0) return;
     count_launch();
     const int blocks = (nIons + kBlock - 1) / kBlock;
-    if (tp.path) k_trace<true><<<blocks, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out);
-    else k_trace<false><<<blocks, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out);
+    auto go = [&](auto kernel) { kernel<<<blocks, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); };
+    const int prec = tp.precision == 1 ? 1 : (tp.precision == 2 ? 2 : 0);
+    if (tp.path) {
+        if (prec == 0) go(k_trace<true, 0>); else if (prec == 1) go(k_trace<true, 1>); else go(k_trace<true, 2>);
+    } else {
+        if (prec == 0) go(k_trace<false, 0>); else if (prec == 1) go(k_trace<false, 1>); else go(k_trace<false, 2>);
+    }
 }
 void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s) {
     if (m.ntets > 0) { count_launch(); k_pack_tets<<<(m.ntets + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, pack); }
@@ -742,8 +801,16 @@ void launch_vertex_fields(const DevMesh& m, cudaStream_t s, const int32_t* cells
 void launch_trace_one(const DevMesh& m, const float start[3], const float vel[3], float qm, int guess, TraceParams tp,
                       ImpactOut* out, cudaStream_t s) {
     count_launch();
-    if (tp.path) k_trace_one<true><<<1, 32, 0, s>>>(m, start[0], start[1], start[2], vel[0], vel[1], vel[2], qm, guess, tp, out);
-    else k_trace_one<false><<<1, 32, 0, s>>>(m, start[0], start[1], start[2], vel[0], vel[1], vel[2], qm, guess, tp, out);
+    auto go = [&](auto kernel) {
+        kernel<<<1, 32, 0, s>>>(m, start[0], start[1], start[2], vel[0], vel[1], vel[2], qm, guess, tp, out);
+    };
+    const int prec = tp.precision == 1 ? 1 : (tp.precision == 2 ? 2 : 0);
+    if (tp.path) {
+        if (prec == 0) go(k_trace_one<true, 0>); else if (prec == 1) go(k_trace_one<true, 1>); else go(k_trace_one<true, 2>);
+    } else {
+        if (prec == 0) go(k_trace_one<false, 0>); else if (prec == 1) go(k_trace_one<false, 1>);
+        else go(k_trace_one<false, 2>);
+    }
 }
 void launch_potential_at(const DevMesh& m, int n, const float* xyz, const int32_t* guess, int walkLimit, float* out,
                          cudaStream_t s) {

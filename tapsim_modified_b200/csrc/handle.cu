@@ -12,6 +12,7 @@
 #include <deque>
 #include <limits>
 #include <mutex>
+#include <thread>
 
 #include <stdlib.h>
 #include <exception>
@@ -146,6 +147,10 @@ struct tg_handle {
     DBuf<float> vVal, vVec;  // vVec: d, x, r, u, w, p, sv, hist, each capacity+1
     DBuf<__nv_bfloat16> vVal16;  // vVal rounded to bf16 (multigrid smoothing pass)
     DBuf<float> vG;              // row sums of the V rows (capacity+1)
+    // FP64 inner iterations: couplings at the SELL positions and the vectors
+    // d64, x64, r64, p64, s64, w64 (each capacity+1), allocated at the first
+    // solve with inner_precision 1
+    DBuf<double> vVal64, vVec64;
     DBuf<double> vScal;
     DBuf<double> vfield;     // vertex fields of the current flight call
     DBuf<float> tetpack;     // packed tetrahedra for the flights
@@ -224,6 +229,16 @@ struct tg_handle {
         v.scal = vScal.p;
         v.count = vCount.p;
         v.capacity = vCapacity;
+        v.val64 = vVal64.p;
+        v.d64 = v.x64 = v.r64 = v.p64 = v.s64 = v.w64 = nullptr;
+        if (vVec64.p) {
+            v.d64 = vVec64.p;
+            v.x64 = vVec64.p + stride;
+            v.r64 = vVec64.p + 2 * stride;
+            v.p64 = vVec64.p + 3 * stride;
+            v.s64 = vVec64.p + 4 * stride;
+            v.w64 = vVec64.p + 5 * stride;
+        }
         return v;
     }
 
@@ -856,7 +871,7 @@ void tg_destroy(tg_handle* h) {
     h->normalBuf.release();
     h->vSlotOf.release(); h->vNodeOf.release(); h->vSliceStart.release(); h->vSliceWidth.release();
     h->vCol.release(); h->vPos.release(); h->vCount.release(); h->vVal.release(); h->vVec.release();
-    h->vVal16.release(); h->vG.release();
+    h->vVal16.release(); h->vG.release(); h->vVal64.release(); h->vVec64.release();
     h->vScal.release(); h->vfield.release(); h->tetpack.release();
     for (int r = 0; r < tg_handle::kRing; r++) {
         if (h->ringStream[r]) {
@@ -1279,15 +1294,23 @@ static int amg_setup(tg_handle* h, double* seconds) {
 // of its start value or maxIter is reached.  r (slot order) must hold
 // the right-hand side; x receives the correction.  amg: the multigrid
 // V-cycle as the preconditioner instead of the diagonal.
-static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersOut) {
+// fp64: the FP64 iterations (multigrid only), their right-hand side taken
+// from the kept FP64 residuals by node.
+static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersOut, bool fp64 = false) {
     const size_t need = 4 * (size_t)(maxIter + 2);
     if (h->vScal.n < need) CK(h->vScal.alloc(need));
     VSys v = h->vs();
     const int slots = h->vActive;
     CK(cudaMemsetAsync(h->vScal.p, 0, sizeof(double) * need, h->stream));
-    launch_vcg_init(v, slots, !amg, h->stream);
-    if (amg) launch_amg_vcycle(v, slots, h->amg, 0, -1.0, h->stream);
-    launch_vcg_spmv(v, slots, 0, -1.0, amg, h->stream);
+    if (fp64) {
+        launch_vcg64_init(v, slots, h->resid.p, h->stream);
+        launch_amg_vcycle(v, slots, h->amg, 0, -1.0, h->stream);
+        launch_vcg64_spmv(v, slots, 0, -1.0, h->stream);
+    } else {
+        launch_vcg_init(v, slots, !amg, h->stream);
+        if (amg) launch_amg_vcycle(v, slots, h->amg, 0, -1.0, h->stream);
+        launch_vcg_spmv(v, slots, 0, -1.0, amg, h->stream);
+    }
     // stop on the 2-norm of the residual (rho = r.r), the norm the outer
     // FP64 test uses: rho_it <= rtol^2 rho_0, tested by the kernels
     // themselves, so the iterations queue before rho_0 is read back
@@ -1302,6 +1325,12 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
         const int start = it;
         const int end = std::min(maxIter, it + batch);
         for (; it < end; it++) {
+            if (fp64) {
+                launch_vcg64_update(v, slots, it, rel2, h->stream);
+                launch_amg_vcycle(v, slots, h->amg, it + 1, rel2, h->stream);
+                launch_vcg64_spmv(v, slots, it + 1, rel2, h->stream);
+                continue;
+            }
             launch_vcg_update(v, slots, it, rel2, !amg, h->stream);
             if (amg) launch_amg_vcycle(v, slots, h->amg, it + 1, rel2, h->stream);
             launch_vcg_spmv(v, slots, it + 1, rel2, amg, h->stream);
@@ -1334,6 +1363,10 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
 int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     DeviceScope dev_scope(h);
     if (!h || !o) return fail(h, TG_ERR_ARGUMENT, "tg_solve: null argument");
+    if (o->inner_precision < 0 || o->inner_precision > 1)
+        return fail(h, TG_ERR_ARGUMENT, "tg_solve: inner_precision 0 (FP32) or 1 (FP64)");
+    if (o->inner_precision == 1 && (o->preconditioner != 1 || o->warm_start != 0))
+        return fail(h, TG_ERR_ARGUMENT, "tg_solve: FP64 inner iterations take the multigrid preconditioner and a plain start");
     int rc = TG_OK;
     DevMesh m = h->dm();
     // ||b||^2 comes with the first residual of every solve (from a full pass
@@ -1384,6 +1417,23 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     const bool amg = o->preconditioner == 1;
     if (o->preconditioner < 0 || o->preconditioner > 1)
         return fail(h, TG_ERR_ARGUMENT, "tg_solve: preconditioner 0 (Jacobi) or 1 (multigrid)");
+    const bool fp64 = o->inner_precision == 1;
+    if (fp64 && h->vActive > 0 && !h->vVec64.p) {
+        // first FP64 solve: the FP64 copies of the V system's couplings and
+        // diagonals, kept in step by every later write of the FP32 ones
+        const size_t stored = h->vVal.n, stride = (size_t)h->vCapacity + 1;
+        cudaError_t e = h->vVal64.alloc(stored);
+        if (e == cudaSuccess) e = h->vVec64.alloc(6 * stride);
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->vVal64.p, 0, sizeof(double) * stored, h->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->vVec64.p, 0, sizeof(double) * 6 * stride, h->stream);
+        if (e != cudaSuccess) {
+            h->vVal64.release();
+            h->vVec64.release();
+            return cuda_check(h, e, "tg_solve: FP64 inner system");
+        }
+        vsys = h->vs();
+        launch_vcg64_derive(m, vsys, h->nnz, h->stream);
+    }
     // (re)build the hierarchy when there is none or removals have grown the
     // system by 2% since
     if (amg && (!h->amgReady || h->vActive > h->amgSlots + h->amgSlots / 50)) {
@@ -1438,11 +1488,11 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         const double rtol = std::min(0.5, std::max(o->inner_rtol, 0.3 * o->rel_tol / rel));
         int itV = 0, itN = 0;
         if (h->vActive > 0 && r2[0] > 0.0) {
-            rc = run_vcg(h, rtol, o->max_inner, amg, &itV);
+            rc = run_vcg(h, rtol, o->max_inner, amg, &itV, fp64);
             if (rc != TG_OK) return rc;
         }
         if (h->countAllN > 0) {
-            launch_vcg_couple_neumann(m, vsys, h->allN.p, h->countAllN, vN.r, h->stream);
+            launch_vcg_couple_neumann(m, vsys, h->allN.p, h->countAllN, vN.r, h->stream, fp64);
             // the Neumann rows' share of the global residual only has to fall
             // below 0.3 of the outer tolerance (the V rows' solve brings
             // theirs to about the same), whatever their own start
@@ -1452,7 +1502,8 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         }
         inf.inner += itV + itN;
         inf.inner_neumann += itN;
-        launch_vcg_apply(m, vsys, h->vActive, fromEvent, h->stream);
+        if (fp64) launch_vcg64_apply(m, vsys, h->vActive, fromEvent, h->stream);
+        else launch_vcg_apply(m, vsys, h->vActive, fromEvent, h->stream);
         launch_apply_correction(m, h->allN.p, h->countAllN, vN, h->stream);
     }
     h->selValid = false;
@@ -1944,6 +1995,8 @@ static TraceParams trace_params(const tg_handle* h, const tg_trace_opts* o) {
     tp.top_z = h->top_z;
     tp.integrator = o->integrator;
     tp.stepper = o->stepper;
+    tp.precision = o->precision;
+    tp.fp64_radius2 = o->fp64_radius * o->fp64_radius;
     return tp;
 }
 
@@ -1962,6 +2015,8 @@ static int trace_impl(tg_handle* h, int32_t nIons, const float* start, const flo
         (cap > 0 && nIons && (!points || !errors)))
         return fail(h, TG_ERR_ARGUMENT, std::string(what) + ": bad argument");
     if (!h->tet_v.p) return fail(h, TG_ERR_ARGUMENT, std::string(what) + ": mesh has no tetrahedra");
+    if (o->precision < 0 || o->precision > 2 || !(o->fp64_radius >= 0.0))
+        return fail(h, TG_ERR_ARGUMENT, std::string(what) + ": precision 0..2 and fp64_radius >= 0");
     if (nIons == 0) return TG_OK;
     if (guess)
         for (int32_t k = 0; k < nIons; k++)
@@ -2053,8 +2108,27 @@ static int ring_ready(tg_handle* h) {
     return TG_OK;
 }
 
-static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_event_record* rec,
-                     ImpactOut* asyncImpact) {
+// Probability of a surface cell in the last selection (score / sum in
+// float, as tg_surface_pick reports it); TG_ERR_ARGUMENT for a cell that is
+// not on the surface.
+static int surface_probability(tg_handle* h, int32_t node, float* probability) {
+    if (node < 0 || node >= h->n) return fail(h, TG_ERR_ARGUMENT, "forced removal: node out of range");
+    int32_t slot = -1;
+    CK(cudaMemcpyAsync(&h->pin->node[1], h->surfSlot.p + node, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    slot = h->pin->node[1];
+    if (slot < 0 || slot >= h->surfSlots)
+        return fail(h, TG_ERR_ARGUMENT, "forced removal: node " + std::to_string(node) + " is not on the surface");
+    float sc = 0.0f;
+    CK(cudaMemcpy(&sc, h->surfScore.p + slot, sizeof(float), cudaMemcpyDeviceToHost));
+    *probability = sc / (float)h->sel.score_sum;
+    return TG_OK;
+}
+
+// callIndex: the event's position within the calling tg_run_event(s) call,
+// which picks its forced removal (tg_event_opts.force_nodes)
+static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, int32_t callIndex,
+                     tg_event_record* rec, ImpactOut* asyncImpact) {
     if (h->vacuumId != o->vacuum_id) {
         int32_t ns;
         int rc = tg_surface_init(h, o->vacuum_id, &ns);
@@ -2062,6 +2136,8 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
     }
     if (o->prob_mode < 0 || o->prob_mode > 3 || o->choice_mode < 0 || o->choice_mode > 1)
         return fail(h, TG_ERR_ARGUMENT, "tg_run_event: probability mode 0..3, choice mode 0..1");
+    if (o->trace.precision < 0 || o->trace.precision > 2 || !(o->trace.fp64_radius >= 0.0))
+        return fail(h, TG_ERR_ARGUMENT, "tg_run_event: trace precision 0..2 and fp64_radius >= 0");
     int rc = TG_OK;
     if (!h->selValid || h->sel.prob_mode != o->prob_mode) {
         tg_select_info s;
@@ -2084,6 +2160,11 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, t
         int32_t r = 0;
         random_r(&h->rng, &r);
         rc = tg_surface_pick(h, (double)r / (double)RAND_MAX, &node, &probability);
+        if (rc != TG_OK) return rc;
+    }
+    if (o->force_nodes && callIndex < o->force_count) {
+        node = o->force_nodes[callIndex];
+        rc = surface_probability(h, node, &probability);
         if (rc != TG_OK) return rc;
     }
     rec->node = node;
@@ -2295,7 +2376,8 @@ int tg_run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, tg_ev
     DeviceScope dev_scope(h);
     if (!h || !o || !rec) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: null argument");
     if (!path_opts_ok(o)) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: path_cap < 0 or path buffers missing");
-    return run_event(h, o, eventIndex, rec, nullptr);
+    if (o->force_count < 0) return fail(h, TG_ERR_ARGUMENT, "tg_run_event: force_count < 0");
+    return run_event(h, o, eventIndex, 0, rec, nullptr);
 }
 
 int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int32_t count, tg_event_record* recs,
@@ -2303,6 +2385,7 @@ int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int3
     DeviceScope dev_scope(h);
     if (!h || !o || count < 0 || (count && !recs)) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: bad argument");
     if (!path_opts_ok(o)) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: path_cap < 0 or path buffers missing");
+    if (o->force_count < 0) return fail(h, TG_ERR_ARGUMENT, "tg_run_events: force_count < 0");
     if (done) *done = 0;
     int rc = stage(h, h->stageImpact, std::max(count, 1));
     if (rc == TG_OK && o->path_cap > 0 && o->trace_enabled) rc = stage_paths(h, std::max(count, 1), o->path_cap);
@@ -2310,7 +2393,7 @@ int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int3
     CK(cudaMemsetAsync(h->statusTrace.p, 0, sizeof(int), h->stream));
     int k = 0;
     for (; k < count; k++) {
-        rc = run_event(h, o, firstIndex + k, &recs[k], h->stageImpact.p + k);
+        rc = run_event(h, o, firstIndex + k, k, &recs[k], h->stageImpact.p + k);
         if (rc != TG_OK) break;
     }
     // every flight queued so far completes before the impacts are read
@@ -2336,6 +2419,48 @@ int tg_run_events(tg_handle* h, const tg_event_opts* o, int32_t firstIndex, int3
     }
     if (done) *done = k;
     return rc;
+}
+
+int tg_run_tips(tg_handle* const* handles, int32_t count, const tg_event_opts* opts, int32_t firstIndex,
+                tg_event_record* recs, float* latency_ms, int32_t* status, int32_t threads) {
+    if (count < 0 || (count && (!handles || !opts || !recs || !latency_ms || !status)))
+        return fail(nullptr, TG_ERR_ARGUMENT, "tg_run_tips: bad argument");
+    for (int32_t k = 0; k < count; k++) {
+        if (!handles[k]) return fail(nullptr, TG_ERR_ARGUMENT, "tg_run_tips: null handle");
+        for (int32_t j = 0; j < k; j++)
+            if (handles[j] == handles[k]) return fail(nullptr, TG_ERR_ARGUMENT, "tg_run_tips: a handle listed twice");
+    }
+    int T = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    T = std::max(1, std::min(T, (int)count));
+    // tip k goes to worker k % T: a handle is only ever driven by one thread
+    auto work = [&](int t) {
+        for (int32_t k = t; k < count; k += T) {
+            const auto t0 = std::chrono::steady_clock::now();
+            int32_t done = 0;
+            status[k] = tg_run_events(handles[k], &opts[k], firstIndex, 1, &recs[k], &done);
+            latency_ms[k] = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                                .count();
+        }
+    };
+    if (T == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> pool;
+        try {
+            pool.reserve(T);
+            for (int t = 0; t < T; t++) pool.emplace_back(work, t);
+        } catch (const std::exception& e) {
+            for (auto& th : pool) th.join();
+            return fail(nullptr, TG_ERR_HOST, std::string("tg_run_tips: starting host threads: ") + e.what());
+        }
+        for (auto& th : pool) th.join();
+    }
+    for (int32_t k = 0; k < count; k++)
+        if (status[k] != TG_OK) {
+            g_error = "tg_run_tips: tip " + std::to_string(k) + ": " + handles[k]->err;
+            return status[k];
+        }
+    return TG_OK;
 }
 
 }  // extern "C"

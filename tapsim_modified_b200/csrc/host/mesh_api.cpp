@@ -308,6 +308,11 @@ void tg_mesh_destroy(tg_mesh* m) { delete m; }
 
 float tg_mesh_temperature(const tg_mesh* m) { return m ? m->config.temperature : 0.0f; }
 
+int32_t tg_mesh_type_id(const tg_mesh* m, const char* name) {
+    if (!m || !name) return -1;
+    return m->config.id_of(name);
+}
+
 int tg_mesh_describe(const tg_mesh* m, tg_mesh_desc* d, int32_t* nnz) {
     if (!m || !d) return mesh_fail("tg_mesh_describe: null argument");
     std::memset(d, 0, sizeof(*d));

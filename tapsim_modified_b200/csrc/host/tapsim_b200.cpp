@@ -1,0 +1,311 @@
+// tapsim_b200: the evaporation loop of TAPSim (Process::evaporation,
+// tapsim/process.cpp:441-1124) as a C++ host program over the C ABI of
+// libtapsim_b200.so (include/tapsim_gpu.h).  The device runs steps I-VI of
+// every event (choice, removal, relaxation, fields, flight); this host keeps
+// the voltage queue and time scale (process.cpp:985-1036) in float, as the
+// reference does, and writes the results file with LogResults' layout.
+//
+// Command line, as the reference's (commands.cpp:280-577, 590-841):
+//   tapsim_b200 [options] evaporation iconfig inode [results]
+//   tapsim_b200 [options] evaporation --input-dump=? iconfig [results]
+//   tapsim_b200 [options] resumption idump [results]
+// Options taken from the reference: --ini-file=?, --threads=?, --write-ascii,
+// --write-binary, --no-file-output, --skip-relaxation, --event-limit=?,
+// --voltage-queue-size=?, --vacuum-identifier=?, --no-chunks, --chunk-size=?.
+// Options of this build: --relax-mode=solve|reference (solve: every event
+// relaxed to --rel-tol, 1e-8; reference: the ini's local/global/refresh
+// sweeps), --warm-start=0|1, --batch=? (events per library call).
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../../include/tapsim_gpu.h"
+
+namespace {
+
+// Process::EvaporationOptions keys with the defaults of makeIniList
+// (commands.cpp:1249-1325); the keys this program reads
+const std::map<std::string, std::string> kIniDefaults = {
+    {"RESULTS_FILENAME", "results_data"}, {"RESULTS_BINARY_OUTPUT", "0"}, {"RESULTS_CHUNK_SIZE", "10000"},
+    {"METHOD_EVAPORATION_PROBABILITY", "0"}, {"METHOD_EVAPORATION_CHOICE", "0"},
+    {"VACUUM_CELL_IDENTIFIER", "Vacuum"}, {"TRAJECTORY_INTEGRATOR_TYPE", "1"}, {"TRAJECTORY_STEPPER_TYPE", "1"},
+    {"TRAJECTORY_INITIAL_TIME_STEP", "1e-14"}, {"TRAJECTORY_MINIMUM_TIME_STEP", "1e-16"},
+    {"TRAJECTORY_ERROR_THRESHOLD", "1e-6"}, {"TRAJECTORY_NO_INITIAL_VELOCITY", "1"},
+    {"VOLTAGE_QUEUE_SIZE", "250"}, {"LOCAL_RELAXATION_ERROR_THRESHOLD", "1e-2"},
+    {"LOCAL_RELAXATION_SHELL_SIZE", "3"}, {"LOCAL_RELAXATION_CYCLE_SIZE", "5"}, {"LOCAL_RELAXATION_QUEUE_SIZE", "5"},
+    {"GLOBAL_RELAXATION_STEPS", "1"}, {"REFRESH_RELAXATION_INTERVAL", "0"},
+    {"REFRESH_RELAXATION_ERROR_THRESHOLD", "0.0"}, {"REFRESH_RELAXATION_CYCLE_SIZE", "100"},
+    {"REFRESH_RELAXATION_QUEUE_SIZE", "25"},
+};
+
+struct Args {
+    std::string command, config, nodes, dump, results, ini;
+    int threads = 0;
+    int binary = -1;          // -1: the ini's RESULTS_BINARY_OUTPUT
+    bool fileOutput = true;
+    bool skipRelaxation = false;
+    long eventLimit = -1;     // -1: until the surface is empty
+    int queueSize = -1;
+    std::string vacuum;
+    int chunkSize = -1;       // -1: the ini's; 0: one file
+    bool relaxReference = false;
+    double relTol = 1e-8;
+    int warmStart = 0;
+    int batch = 64;
+};
+
+[[noreturn]] void die(const std::string& msg) {
+    std::fprintf(stderr, "tapsim_b200: %s\n", msg.c_str());
+    std::exit(1);
+}
+
+void check(int rc, const tg_handle* h, const char* what) {
+    if (rc != TG_OK) die(std::string(what) + " failed (" + std::to_string(rc) + "): " + tg_last_error(h));
+}
+
+bool opt(const std::string& a, const char* name, std::string* value) {
+    const std::string p = std::string("--") + name + "=";
+    if (a.compare(0, p.size(), p) != 0) return false;
+    *value = a.substr(p.size());
+    return true;
+}
+
+Args parse(int argc, char** argv) {
+    Args a;
+    std::vector<std::string> pos;
+    for (int k = 1; k < argc; k++) {
+        const std::string s = argv[k];
+        std::string v;
+        if (opt(s, "ini-file", &v)) a.ini = v;
+        else if (opt(s, "threads", &v)) a.threads = std::atoi(v.c_str());
+        else if (s == "--write-ascii") a.binary = 0;
+        else if (s == "--write-binary") a.binary = 1;
+        else if (s == "--no-file-output") a.fileOutput = false;
+        else if (s == "--skip-relaxation") a.skipRelaxation = true;
+        else if (opt(s, "event-limit", &v)) a.eventLimit = std::atol(v.c_str());
+        else if (opt(s, "voltage-queue-size", &v)) a.queueSize = std::atoi(v.c_str());
+        else if (opt(s, "vacuum-identifier", &v)) a.vacuum = v;
+        else if (s == "--no-chunks") a.chunkSize = 0;
+        else if (opt(s, "chunk-size", &v)) a.chunkSize = std::atoi(v.c_str());
+        else if (opt(s, "input-dump", &v)) a.dump = v;
+        else if (opt(s, "relax-mode", &v)) {
+            if (v != "solve" && v != "reference") die("--relax-mode is solve or reference");
+            a.relaxReference = v == "reference";
+        } else if (opt(s, "rel-tol", &v)) a.relTol = std::atof(v.c_str());
+        else if (opt(s, "warm-start", &v)) a.warmStart = std::atoi(v.c_str());
+        else if (opt(s, "batch", &v)) a.batch = std::max(1, std::atoi(v.c_str()));
+        else if (s.compare(0, 2, "--") == 0) die("unknown or invalid argument in command line: \"" + s + "\"");
+        else pos.push_back(s);
+    }
+    if (pos.empty()) die("usage: tapsim_b200 [options] evaporation|resumption ...");
+    a.command = pos[0];
+    if (a.command == "evaporation") {
+        if (!a.dump.empty()) {
+            if (pos.size() < 2) die("missing arguments for processing in 'evaporation'-mode");
+            a.config = pos[1];
+            if (pos.size() > 2) a.results = pos[2];
+        } else {
+            if (pos.size() < 3) die("missing arguments for processing in 'evaporation'-mode");
+            a.config = pos[1];
+            a.nodes = pos[2];
+            if (pos.size() > 3) a.results = pos[3];
+        }
+    } else if (a.command == "resumption") {
+        if (pos.size() < 2) die("missing arguments for processing in 'resumption'-mode");
+        a.dump = pos[1];
+        if (pos.size() > 2) a.results = pos[2];
+    } else {
+        die("unknown command " + a.command);
+    }
+    return a;
+}
+
+std::map<std::string, std::string> read_ini(const std::string& path) {
+    std::map<std::string, std::string> ini = kIniDefaults;
+    if (path.empty()) return ini;
+    std::ifstream f(path);
+    if (!f) die("cannot read ini file " + path);
+    std::string line;
+    while (std::getline(f, line)) {
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.resize(hash);
+        const size_t eq = line.find('=');
+        if (eq == std::string::npos) continue;
+        auto trim = [](std::string s) {
+            const size_t b = s.find_first_not_of(" \t\r"), e = s.find_last_not_of(" \t\r");
+            return b == std::string::npos ? std::string() : s.substr(b, e - b + 1);
+        };
+        ini[trim(line.substr(0, eq))] = trim(line.substr(eq + 1));
+    }
+    return ini;
+}
+
+// MathVector3d<float>::length() in float
+float length3(const float v[3]) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    const Args a = parse(argc, argv);
+    const std::map<std::string, std::string> ini = read_ini(a.ini);
+    auto I = [&](const char* k) { return std::atoi(ini.at(k).c_str()); };
+    auto F = [&](const char* k) { return std::atof(ini.at(k).c_str()); };
+
+    // Process::initialization / readSystem: the mesh with its couplings
+    tg_mesh* mesh = nullptr;
+    int rc;
+    if (!a.dump.empty()) rc = tg_mesh_from_dump(a.dump.c_str(), a.config.empty() ? nullptr : a.config.c_str(), &mesh);
+    else rc = tg_mesh_from_files(a.nodes.c_str(), a.config.c_str(), a.threads, &mesh);
+    check(rc, nullptr, "reading the mesh");
+    tg_mesh_desc desc;
+    int32_t nnz = 0;
+    check(tg_mesh_describe(mesh, &desc, &nnz), nullptr, "tg_mesh_describe");
+    const int n = desc.num_nodes;
+    std::vector<uint32_t> numbers(n);
+    check(tg_mesh_numbers(mesh, numbers.data()), nullptr, "tg_mesh_numbers");
+    const std::string vacuumName = a.vacuum.empty() ? ini.at("VACUUM_CELL_IDENTIFIER") : a.vacuum;
+    const int vacuumId = tg_mesh_type_id(mesh, vacuumName.c_str());
+    if (vacuumId < 0) die("no cell type named " + vacuumName + " in the configuration");
+    std::map<int, tg_type> types;
+    for (int k = 0; k < desc.num_types; k++) types[desc.types[k].id] = desc.types[k];
+    tg_handle* h = nullptr;
+    check(tg_create(&desc, &h), nullptr, "tg_create");
+
+    tg_solve_opts solve{};
+    solve.rel_tol = a.relTol;
+    solve.max_outer = 50;
+    solve.max_inner = 20000;
+    solve.inner_rtol = 1e-4;
+    solve.warm_start = a.warmStart;
+    solve.preconditioner = 1;
+    // initial relaxation (Process::relaxation with the refresh parameters,
+    // commands.cpp:931-933), unless --skip-relaxation
+    if (!a.skipRelaxation) {
+        if (a.relaxReference) {
+            int64_t it = 0;
+            double dev = 0.0;
+            rc = tg_relax_threshold(h, F("REFRESH_RELAXATION_ERROR_THRESHOLD"), I("REFRESH_RELAXATION_CYCLE_SIZE"),
+                                    I("REFRESH_RELAXATION_QUEUE_SIZE"), 2000000, &it, &dev);
+            if (rc != TG_OK && rc != TG_ERR_RELAX_FAULT && rc != TG_ERR_ITERATION_CAP) check(rc, h, "relaxation");
+        } else {
+            tg_solve_opts s0 = solve;
+            s0.warm_start = 0;
+            tg_solve_info info;
+            check(tg_solve(h, &s0, &info), h, "relaxation");
+        }
+    }
+
+    tg_event_opts o{};
+    o.vacuum_id = vacuumId;
+    o.relax_mode = a.relaxReference ? 0 : 1;
+    o.local_threshold = F("LOCAL_RELAXATION_ERROR_THRESHOLD");
+    o.local_shell = I("LOCAL_RELAXATION_SHELL_SIZE");
+    o.local_cycle = I("LOCAL_RELAXATION_CYCLE_SIZE");
+    o.local_queue = I("LOCAL_RELAXATION_QUEUE_SIZE");
+    o.global_steps = I("GLOBAL_RELAXATION_STEPS");
+    o.refresh_interval = I("REFRESH_RELAXATION_INTERVAL");
+    o.refresh_threshold = F("REFRESH_RELAXATION_ERROR_THRESHOLD");
+    o.refresh_cycle = I("REFRESH_RELAXATION_CYCLE_SIZE");
+    o.refresh_queue = I("REFRESH_RELAXATION_QUEUE_SIZE");
+    o.refresh_max_sweeps = 2000000;
+    o.solve = solve;
+    o.trace.time_step = F("TRAJECTORY_INITIAL_TIME_STEP");
+    o.trace.min_time_step = F("TRAJECTORY_MINIMUM_TIME_STEP");
+    o.trace.error_threshold = F("TRAJECTORY_ERROR_THRESHOLD");
+    o.trace.max_steps = 100000;
+    o.trace.stepper_limit = 200;
+    o.trace.walk_limit = 100000;
+    o.trace.integrator = I("TRAJECTORY_INTEGRATOR_TYPE");
+    o.trace.stepper = I("TRAJECTORY_STEPPER_TYPE");
+    o.trace_enabled = 1;
+    o.normal_enabled = 1;
+    o.prob_mode = I("METHOD_EVAPORATION_PROBABILITY");
+    o.choice_mode = I("METHOD_EVAPORATION_CHOICE");
+    o.temperature = tg_mesh_temperature(mesh);
+    o.rng_seed = 99;  // std::srand(99) in main (tapsim.cpp:235)
+    o.initial_velocity = I("TRAJECTORY_NO_INITIAL_VELOCITY") ? 0 : 1;
+
+    // steps I-VI on the device, VI (voltage, time scale) and VII (results)
+    // here, one batch of events per library call
+    const size_t queueSize = a.queueSize >= 0 ? (size_t)a.queueSize : (size_t)I("VOLTAGE_QUEUE_SIZE");
+    std::deque<float> voltageQueue;
+    float voltageQueueSum = 0.0f;
+    std::vector<tg_result_row> rows;
+    std::vector<tg_event_record> recs((size_t)a.batch);
+    long events = 0;
+    for (;;) {
+        long want = a.batch;
+        if (a.eventLimit >= 0) want = std::min<long>(want, a.eventLimit - events);
+        if (want <= 0) break;
+        int32_t done = 0;
+        rc = tg_run_events(h, &o, (int32_t)(events + 1), (int32_t)want, recs.data(), &done);
+        if (rc != TG_OK && rc != TG_ERR_NO_SURFACE) check(rc, h, "tg_run_events");
+        for (int k = 0; k < done; k++) {
+            const tg_event_record& r = recs[k];
+            const tg_type& t = types.at(r.type_id);
+            float voltage, timeScale;
+            const float fb = length3(r.field_before);
+            if (r.impact.last_tet >= 0 && fb != 0.0f) {
+                float v = r.phi_before;
+                v -= r.impact.last_phi;
+                v *= t.evap_field;
+                v /= fb;
+                v /= r.scaling_reference;
+                voltageQueue.push_back(v);
+                voltageQueueSum += v;
+                while (voltageQueue.size() > queueSize) {
+                    voltageQueueSum -= voltageQueue.front();
+                    voltageQueue.pop_front();
+                }
+                voltage = voltageQueueSum / voltageQueue.size();
+                timeScale = r.phi_after;
+                timeScale -= r.impact.last_phi;
+                timeScale /= voltage;
+                timeScale = std::sqrt(timeScale);
+            } else {
+                voltage = fb == 0.0f ? 1.0f : 0.0f;
+                timeScale = 1.0f;
+            }
+            tg_result_row row{};
+            row.index = (uint32_t)(events + k + 1);
+            row.id = r.type_id;
+            row.number = numbers[r.node];
+            row.voltage = voltage;
+            for (int c = 0; c < 3; c++) {
+                row.start[c] = desc.xyz[3 * (size_t)r.node + c];
+                row.stop[c] = r.impact.stop[c];
+                row.field_before[c] = r.field_before[c];
+                row.field_after[c] = r.field_after[c];
+                row.normal[c] = r.normal[c];
+                row.apex[c] = r.apex[c];
+            }
+            row.tof = r.impact.stop_time * timeScale;
+            row.probability = r.probability;
+            row.potential_before = r.phi_before;
+            row.potential_after = r.phi_after;
+            rows.push_back(row);
+        }
+        events += done;
+        if (done < want) break;  // the surface ran out
+    }
+    std::printf("events %ld\n", events);
+    if (a.fileOutput) {
+        const std::string path = a.results.empty() ? ini.at("RESULTS_FILENAME") : a.results;
+        const int binary = a.binary >= 0 ? a.binary : I("RESULTS_BINARY_OUTPUT");
+        const int chunk = a.chunkSize >= 0 ? a.chunkSize : I("RESULTS_CHUNK_SIZE");
+        if (!path.empty())
+            check(tg_results_write(path.c_str(), binary, nullptr, (int32_t)rows.size(), rows.data(), chunk), nullptr,
+                  "tg_results_write");
+    }
+    tg_destroy(h);
+    tg_mesh_destroy(mesh);
+    return 0;
+}

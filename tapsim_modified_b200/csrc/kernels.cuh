@@ -94,6 +94,12 @@ struct VSys {
     double* scal;                 // gamma, delta, alpha per iteration
     int32_t* count;               // next free slot (device counter)
     int capacity;
+    // FP64 inner iterations (tg_solve_opts.inner_precision 1), allocated at
+    // the first solve that asks for them, null before: the couplings and the
+    // diagonal in FP64 at the same positions as val and d (kept in step by
+    // every write of those once allocated), and the CG vectors in FP64
+    double* val64;
+    double *d64, *x64, *r64, *p64, *s64, *w64;
 };
 // jacobi: the Jacobi preconditioner (u = r / d inside init / update);
 // otherwise u comes from launch_amg_vcycle and the SpMV adds gamma = r.u.
@@ -102,6 +108,15 @@ struct VSys {
 void launch_vcg_init(const VSys& v, int slots, bool jacobi, cudaStream_t s);
 void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withGamma, cudaStream_t s);
 void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s);
+// FP64 inner iterations with the multigrid preconditioner: the V-cycle runs
+// in FP32 on r rounded to float and its u enters the FP64 recurrences
+// exactly.  init64 takes the right-hand side from the FP64 residual by node
+// (the kept residuals of the first pass); apply64 adds x64 to the potentials.
+void launch_vcg64_derive(const DevMesh& m, const VSys& v, int nnz, cudaStream_t s);
+void launch_vcg64_init(const VSys& v, int slots, const double* rnode, cudaStream_t s);
+void launch_vcg64_spmv(const VSys& v, int slots, int it, double target, cudaStream_t s);
+void launch_vcg64_update(const VSys& v, int slots, int it, double target, cudaStream_t s);
+void launch_vcg64_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s);
 
 // ---- multigrid preconditioner (amg.cu) ----
 constexpr int kAmgMaxLevels = 12;
@@ -133,7 +148,7 @@ void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cu
 // r -= A hist on the V system (FP32), sum r^2 into *acc
 void launch_vcg_warm_residual(const VSys& v, int slots, double* acc, cudaStream_t s);
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
-                               cudaStream_t s);
+                               cudaStream_t s, bool fromX64 = false);
 // FP64 residual of the V rows (rows: their compact list, in node order)
 // into the V system's r; with bacc, also ||b||^2 of those rows.  With r64
 // (by node) each row's FP64 residual is kept, and with bacc and b64 its
@@ -233,6 +248,10 @@ struct TraceParams {
     float* path;
     float* path_err;
     int path_cap;
+    // arithmetic of the Cash-Karp steps: 0 FP64, 1 FP32 (as the reference),
+    // 2 FP64 within sqrt(fp64_radius2) of the start and FP32 beyond
+    int precision;
+    double fp64_radius2;
 };
 struct ImpactOut {
     float stop[3];

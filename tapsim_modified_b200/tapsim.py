@@ -140,18 +140,20 @@ def path_length(impact: N.tg_impact, cap: int) -> int:
 
 
 def trace_opts(time_step=1e-14, min_time_step=1e-16, error_threshold=1e-6, max_steps=100000, stepper_limit=200,
-               walk_limit=100000, integrator=1, stepper=1) -> N.tg_trace_opts:
+               walk_limit=100000, integrator=1, stepper=1, precision=0, fp64_radius=0.0) -> N.tg_trace_opts:
     """Trajectory options; integrator / stepper are TRAJECTORY_INTEGRATOR_TYPE
     (0 Euler, 1 Cash-Karp) and TRAJECTORY_STEPPER_TYPE (0 none, 1 error-
-    restricted, 2 geometry-restricted, 3 adaptive)."""
+    restricted, 2 geometry-restricted, 3 adaptive); precision 0 FP64, 1 FP32,
+    2 FP64 within fp64_radius [m] of the start and FP32 beyond."""
     return N.tg_trace_opts(time_step, min_time_step, error_threshold, max_steps, stepper_limit, walk_limit,
-                           integrator, stepper)
+                           integrator, stepper, precision, fp64_radius)
 
 
 def solve_opts(rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4, warm_start=0,
-               preconditioner=0) -> N.tg_solve_opts:
-    """preconditioner: 0 Jacobi, 1 multigrid (tg_solve_opts)."""
-    return N.tg_solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, preconditioner)
+               preconditioner=0, inner_precision=0) -> N.tg_solve_opts:
+    """preconditioner: 0 Jacobi, 1 multigrid; inner_precision: 0 FP32, 1 FP64
+    inner iterations (tg_solve_opts)."""
+    return N.tg_solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, preconditioner, inner_precision)
 
 
 class Grid:
@@ -199,9 +201,9 @@ class Grid:
         return rc, it.value, dev.value
 
     def solve(self, rel_tol=1e-8, max_outer=20, max_inner=4000, inner_rtol=1e-4, warm_start=0,
-              preconditioner=0) -> N.tg_solve_info:
+              preconditioner=0, inner_precision=0) -> N.tg_solve_info:
         info = N.tg_solve_info()
-        o = solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, preconditioner)
+        o = solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, preconditioner, inner_precision)
         self._ck(N.lib().tg_solve(self._h, C.byref(o), C.byref(info)))
         return info
 
@@ -649,15 +651,28 @@ class Evaporation:
             self._snapshot()
         return r
 
-    def run(self, count: int) -> list[dict]:
+    def run(self, count: int, force=None) -> list[dict]:
         """`count` events in one library call: each ion flight overlaps the
-        next event's removal and relaxation.  Same records as `step`."""
+        next event's removal and relaxation.  Same records as `step`.
+        force: node indices that the first len(force) events remove in place
+        of the chosen cells (tg_event_opts.force_nodes); a record whose
+        probability is below its best_probability removed a forced cell
+        that was not this run's choice."""
         out = []
+        forced = None if force is None else np.ascontiguousarray(force, np.int32)
+        done = 0
         while count > 0:
             # a batch ends where a snapshot is due
             k = min(count, self._events_to_snapshot())
             pts, err = self._path_buffers(k)
+            if forced is not None and done < len(forced):
+                self.opts.force_nodes = forced[done:].ctypes.data
+                self.opts.force_count = len(forced) - done
+            else:
+                self.opts.force_nodes = None
+                self.opts.force_count = 0
             recs = self.grid.run_events(self.opts, self.event + 1, k)
+            done += k
             for j, rec in enumerate(recs):
                 self.event += 1
                 r = self._record(rec, None if pts is None else (pts[j], err[j]))
@@ -671,23 +686,32 @@ class Evaporation:
     def _record(self, rec: N.tg_event_record, path=None) -> dict:
         """Step VI: voltage queue and time-of-flight scale (process.cpp:985-1036)."""
         imp = rec.impact
-        fb = math.sqrt(sum(float(x) ** 2 for x in rec.field_before))
+        # in float, operation by operation, as process.cpp:985-1036 does
+        f32 = np.float32
+        fbv = [f32(x) for x in rec.field_before]
+        fb = f32(np.sqrt(fbv[0] * fbv[0] + fbv[1] * fbv[1] + fbv[2] * fbv[2]))
         if imp.last_tet >= 0 and fb != 0.0:
-            v = (rec.phi_before - imp.last_phi) * self.evap_field[rec.type_id] / fb / rec.scaling_reference
+            v = f32(rec.phi_before) - f32(imp.last_phi)
+            v = v * f32(self.evap_field[rec.type_id])
+            v = v / fb
+            v = v / f32(rec.scaling_reference)
             self.voltage_queue.append(v)
-            self.voltage_sum += v
+            self.voltage_sum = f32(self.voltage_sum + v)
             while len(self.voltage_queue) > self.queue_size:
-                self.voltage_sum -= self.voltage_queue.popleft()
-            voltage = self.voltage_sum / len(self.voltage_queue)
-            ts = (rec.phi_after - imp.last_phi) / voltage
-            time_scale = math.sqrt(ts) if ts >= 0 else float("nan")
+                self.voltage_sum = f32(self.voltage_sum - self.voltage_queue.popleft())
+            voltage = f32(self.voltage_sum / f32(len(self.voltage_queue)))
+            ts = (f32(rec.phi_after) - f32(imp.last_phi)) / voltage
+            with np.errstate(invalid="ignore"):
+                time_scale = float(np.sqrt(f32(ts)))
+            voltage = float(voltage)
         else:
             voltage = 1.0 if fb == 0.0 else 0.0
             time_scale = 1.0
         return {
             "index": self.event, "node": rec.node, "id": rec.type_id, "number": int(self.numbers[rec.node]),
             "voltage": voltage,
-            "stop": tuple(imp.stop), "tof": imp.stop_time * time_scale, "probability": rec.probability,
+            "stop": tuple(imp.stop), "tof": float(np.float32(imp.stop_time) * np.float32(time_scale)),
+            "probability": rec.probability,
             "best": rec.best_ratio, "second": rec.second_ratio, "scaling_reference": rec.scaling_reference,
             "potentialBefore": rec.phi_before, "fieldBefore": tuple(rec.field_before),
             "potentialAfter": rec.phi_after, "fieldAfter": tuple(rec.field_after), "normal": tuple(rec.normal),

@@ -188,3 +188,31 @@ def test_path_of_a_start_outside_is_empty(solved):
     a, g, o = solved
     imps, paths, errs = g.trace_path(np.array([[0.0, 0.0, 10.0]]), QM_FE, 0, cap=16)
     assert imps[0].status == -1 and len(paths[0]) == 0 and np.all(errs[0] == 0.0)
+
+
+def test_fp32_and_mixed_flights_against_the_fp64_oracle(solved):
+    """precision 1 integrates in FP32 as the reference does (Cash-Karp steps
+    and error-restricted control in float), precision 2 in FP64 within
+    fp64_radius of the start and FP32 beyond.  Their impacts stay within the
+    bounds the FP64 flight keeps against the oracle; every ion reaches the
+    detector plane.  Out-of-range precisions are refused."""
+    from tapsim_modified_b200 import _native as N
+    a, g, o = solved
+    nodes, _ = g.surface()
+    starts = nodes[:: max(1, len(nodes) // 24)][:24]
+    H = float(a["xyz"][:, 2].max())
+    ref = [o.trace(a["xyz"][n], QM_FE, a["node_tet"][n]) for n in starts]
+    r_ref = np.array([np.hypot(r.stop[0], r.stop[1]) for r in ref])
+    for prec, radius in ((1, 0.0), (2, 5e-9)):
+        out = g.trace(a["xyz"][starts], QM_FE, a["node_tet"][starts], precision=prec, fp64_radius=radius)
+        d = np.array([np.hypot(out[k].stop[0] - ref[k].stop[0], out[k].stop[1] - ref[k].stop[1])
+                      for k in range(len(starts))]) / r_ref
+        print("precision", prec, "impact relative differences: median", np.median(d), "max", d.max())
+        for k in range(len(starts)):
+            assert out[k].status == ref[k].status == 5
+            assert abs(out[k].stop[2] - H) <= 1e-6 * H
+            assert abs(out[k].stop_time - ref[k].stop_time) <= 1e-2 * abs(ref[k].stop_time)
+        assert np.median(d) <= 1e-3
+        assert d.max() <= 2e-2
+    with pytest.raises(N.TapsimError):
+        g.trace(a["xyz"][starts[:1]], QM_FE, a["node_tet"][starts[0]], precision=3)

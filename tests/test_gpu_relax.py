@@ -99,3 +99,43 @@ def test_local_relax_keeps_dirichlet_and_converges(small_mesh):
         frontier = nxt - ring
         ring |= nxt
     assert set(changed.tolist()) <= ring
+
+
+def test_fp64_inner_iterations_match_oracle_and_fp32(small_mesh, ref_mesh, ref_events):
+    """inner_precision 1 (FP64 couplings, vectors and recurrences in the
+    inner CG, FP32 V-cycle): the initial solve and six events solved to
+    1e-10 agree with the oracle's potentials and with the FP32 inner solve,
+    and remove the same cells as the reference.  Options it does not take
+    are refused."""
+    from oracle import Oracle
+    from tapsim_modified_b200 import _native as N
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
+    a = small_mesh.arrays()
+    g = Grid(small_mesh)
+    info = g.solve(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1, inner_precision=1)
+    assert info.rel_residual <= 1e-10
+    o = Oracle(a)
+    o.solve(1e-12, 2_000_000, 1.9)
+    free = free_mask(a)
+    assert np.abs(g.potentials() - o.phi)[free].max() < 1e-7
+    with pytest.raises(N.TapsimError):
+        g.solve(rel_tol=1e-8, preconditioner=0, inner_precision=1)
+    with pytest.raises(N.TapsimError):
+        g.solve(rel_tol=1e-8, preconditioner=1, warm_start=1, inner_precision=1)
+    g.close()
+    from conftest import GOLDEN
+    opts = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
+    runs = {}
+    for prec in (0, 1):
+        g = Grid(ref_mesh)
+        g.solve(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1, inner_precision=prec)
+        ev = Evaporation(g, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, max_outer=50, max_inner=20000,
+                                                                   preconditioner=1, inner_precision=prec))
+        runs[prec] = (ev.run(6), g.potentials())
+        g.close()
+    (r32, phi32), (r64, phi64) = runs[0], runs[1]
+    assert [r["node"] for r in r32] == [r["node"] for r in r64] == [int(x) for x in ref_events[:6, 1]]
+    assert all(r["rel_residual"] <= 1e-10 for r in r32 + r64)
+    assert np.abs(phi32 - phi64).max() < 1e-8
+    for x, y in zip(r32, r64):
+        assert np.linalg.norm(np.subtract(x["stop"], y["stop"])) <= 1e-6 * np.linalg.norm(y["stop"])
