@@ -50,6 +50,12 @@ TIPS = {
     # about 3 GB on the device
     "prof": dict(cap_radius=12e-9, shank_length=30e-9, half_angle_deg=8.0, fine_shell=4e-9,
                  box_half_width=0.5e-6, box_height=1.0e-6),
+    # alloy tip with probe ions: bcc Fe-1.5 at.% Cu, r=10 nm cap on a 30 nm
+    # cylinder (about 1M atoms), Cu in precipitates at 2e24 m^-3 (lognormal
+    # radius clipped to 1-2 nm) and at random sites
+    "alloy10": dict(cap_radius=10e-9, shank_length=30e-9, half_angle_deg=0.0, fine_shell=4e-9,
+                    box_half_width=0.5e-6, box_height=1.0e-6, solute_fraction=0.015, precip_density=2e24,
+                    precip_rmin=1e-9, precip_rmax=2e-9),
     # training tip of the learned warm start: another shape and seed than the
     # timed tip (the network sees only neighbourhoods of removed atoms)
     "train": dict(cap_radius=10e-9, shank_length=20e-9, half_angle_deg=8.0, fine_shell=4e-9,
@@ -585,6 +591,99 @@ def run_many_tips(args, rank: int, world: int, dist):
             "clocks": clocks.summary()}
 
 
+def run_probe_ions(args):
+    """Alloy tip with probe ions: bcc Fe-1.5 at.% Cu, r = 10 nm cap on a 30 nm
+    shank (about 1M atoms), Cu in seeded spherical precipitates (lognormal
+    radius clipped to 1-2 nm, 2e24 m^-3) and the rest at random sites;
+    evaporation fields Fe 33 V/nm, Cu 30 V/nm.  Every event (relaxed to
+    1e-8) is followed by args.probe_ions probe ions launched in one kernel
+    from surface cells drawn uniformly (seeded per event) and traced to the
+    detector three times: in FP64, in FP32 (the reference's arithmetic) and
+    mixed (FP64 within 3 cap radii of the start, FP32 beyond).  Reports the
+    probe launches' ions/s and accepted steps/s (CUDA events on the handle's
+    stream) and the FP32 and mixed hit maps against the FP64 one."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from tapsim_modified_b200 import _native as N
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
+
+    torch.cuda.set_device(0)
+    L = N.lib()
+    mesh = build_mesh("alloy10", seed=tip_seed(0))
+    a = mesh.arrays()
+    cu = int((a["type"] == 5).sum())
+    atoms = int((a["type"] == 4).sum()) + cu
+    g = Grid(mesh)
+    g.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
+    opts = EvaporationOptions.from_ini(None)
+    ev = Evaporation(g, opts, relax_mode=1, solve=solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000,
+                                                            preconditioner=PRECOND))
+    qm = {k: v[0] / v[1] for k, v in ev.charge_mass.items()}
+    xyz, node_tet = a["xyz"], a["node_tet"]
+    fp64_radius = 3.0 * TIPS["alloy10"]["cap_radius"]
+    modes = {"fp64": dict(precision=0), "fp32": dict(precision=1), "mixed": dict(precision=2, fp64_radius=fp64_radius)}
+    ms = {k: 0.0 for k in modes}
+    steps = {k: 0 for k in modes}
+    dev = {k: [] for k in ("fp32", "mixed")}
+    status_ok = {k: 0 for k in modes}
+    ev_ms = 0.0
+    ions = 0
+    rng = np.random.default_rng(11)
+    ev.run(args.warmup)
+    for k in range(args.steps):
+        t = C.c_float()
+        N.check(L.tg_timer_start(g._h), g._h)
+        ev.run(1)
+        N.check(L.tg_timer_stop(g._h, C.byref(t)), g._h)
+        ev_ms += t.value
+        cells, _ = g.surface()
+        pick = rng.choice(cells, size=args.probe_ions, replace=len(cells) < args.probe_ions)
+        # ions from neighbouring sites follow neighbouring paths: ordered by
+        # azimuth and height, a warp's ions walk and step alike
+        order = np.lexsort((np.round(xyz[pick, 2] / 1e-9), np.arctan2(xyz[pick, 1], xyz[pick, 0])))
+        pick = pick[order]
+        q = np.array([qm[int(t_)] for t_ in a["type"][pick]], np.float32)
+        imp = {}
+        for name, kw in modes.items():
+            t = C.c_float()
+            N.check(L.tg_timer_start(g._h), g._h)
+            imp[name] = g.trace(xyz[pick], q, node_tet[pick], **kw)
+            N.check(L.tg_timer_stop(g._h, C.byref(t)), g._h)
+            ms[name] += t.value
+            steps[name] += sum(r.steps for r in imp[name])
+            status_ok[name] += sum(r.status == 5 for r in imp[name])
+        ions += len(pick)
+        ref = np.array([[r.stop[0], r.stop[1]] for r in imp["fp64"]], np.float64)
+        rad = np.hypot(ref[:, 0], ref[:, 1])
+        for name in dev:
+            got = np.array([[r.stop[0], r.stop[1]] for r in imp[name]], np.float64)
+            dev[name].extend((np.hypot(*(got - ref).T) / np.maximum(rad, 1e-30)).tolist())
+    g.close()
+    out = {"metric": "probe ions per event: ions/s of one launch of the event's probe ions (FP32), hit maps FP32 "
+                     "and mixed vs FP64",
+           "value": ions / (ms["fp32"] / 1e3), "unit": "ions/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": (ev_ms + ms["fp32"]) / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 flights (f64 point location)",
+           "data": "synthetic (seeded bcc Fe-1.5 at.% Cu tip)",
+           "config": {"workload": f"alloy10: bcc Fe-1.5 at.% Cu, r=10 nm cap, 30 nm shank, {atoms} atoms ({cu} Cu), "
+                                  f"{mesh.num_nodes} cells; per event: the event (rel. residual 1e-8) and "
+                                  f"{args.probe_ions} probe ions from uniformly drawn surface cells in one launch",
+                      "event_ms": ev_ms / args.steps,
+                      "probe": {name: {"ms_per_launch": ms[name] / args.steps, "ions_per_s": ions / (ms[name] / 1e3),
+                                       "steps_per_s": steps[name] / (ms[name] / 1e3),
+                                       "steps_per_ion": steps[name] / ions,
+                                       "reached_detector": status_ok[name] / ions} for name in modes},
+                      "hit_map_vs_fp64": {name: {"median_rel_impact_diff": float(np.median(v)),
+                                                 "p99_rel_impact_diff": float(np.percentile(v, 99)),
+                                                 "max_rel_impact_diff": float(np.max(v))} for name, v in dev.items()},
+                      "mixed_fp64_radius_m": fp64_radius,
+                      "note": "impact differences relative to the FP64 impact's radius on the detector plane"}}
+    return out
+
+
 def hop_ball(row_ptr, col, site: int, hops: int):
     """Cells within `hops` steps of `site` in the cell graph (site included)."""
     import numpy as np
@@ -840,6 +939,8 @@ def main():
     ap.add_argument("--converged-events", type=int, default=3,
                     help="events of the reference's converged ini timed beside its default ini (reference arm)")
     ap.add_argument("--prepare-tip", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--probe-ions", type=int, default=0,
+                    help="alloy tip: this many probe ions per event in one launch, FP32 / mixed / FP64 (0: off)")
     ap.add_argument("--tips", type=int, default=0,
                     help="many-tip serving: this many seeded tips, one event of each per step (0: off)")
     ap.add_argument("--warm-bounds", action="store_true",
@@ -862,6 +963,8 @@ def main():
         out = run_warm_bounds(args) if rank == 0 else None
     elif args.tips > 0:
         out = run_many_tips(args, rank, world, dist)
+    elif args.probe_ions > 0:
+        out = run_probe_ions(args) if rank == 0 else None
     elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

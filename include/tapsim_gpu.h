@@ -124,8 +124,10 @@ typedef struct {
      *   1  plus the previous event's correction on the non-Neumann free
      *      cells (the smooth far field of one removal changes little
      *      from one site to the next),
-     *   2  as 1, plus the prediction of an attached learner on the cells
-     *      around the removed atom (tg_learner_attach, mode bit 1).
+     *   2  0, plus the prediction of an attached learner on the free cells
+     *      around the removed atom (tg_learner_attach, mode bit 1); the
+     *      first residual is then updated in FP64 on those cells' rows and
+     *      their neighbours' instead of a pass over every row.
      * The solve always ends at rel_tol, whatever the start. */
     int32_t warm_start;
     /* Preconditioner of the inner iterations on the non-Neumann free cells:
@@ -155,6 +157,14 @@ typedef struct {
     double setup_seconds;     /* multigrid hierarchy built during this solve [s], 0 if none */
 } tg_solve_info;
 int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);
+/* The schedule of one level of the multigrid hierarchy (no counterpart in
+ * the reference): its rows, and the lanes per CSR row of its operator
+ * (levels smoothed with CSR rows) and of its restriction (every level but
+ * the coarsest), 0 where the level has none.  The hierarchy build times
+ * each lane-group size (2..32) on the level's own matrices and keeps the
+ * fastest; a_ms / r_ms are the kept launches' times [ms]. */
+int tg_amg_schedule(tg_handle* h, int32_t level, int32_t* rows, int32_t* a_lanes, int32_t* r_lanes, float* a_ms,
+                    float* r_ms);
 /* ||r||_2 / ||b||_2 of the current potentials (FP64). */
 int tg_residual(tg_handle* h, double* rel_residual);
 
@@ -400,12 +410,12 @@ int tg_run_tips(tg_handle* const* handles, int32_t count, const tg_event_opts* o
 /* ---- learned near-field warm start (no counterpart in the reference) -----
  * A message-passing network (an input layer and four message layers of
  * width 64, BF16 tensor-core GEMMs with FP32 accumulation) on the free cells
- * within `hops` steps of a removed atom predicts the part of the event's
- * correction that the recycled far field (warm_start 1) misses.  Samples are
- * (features right after the far-field start, converged correction) pairs
- * that tg_solve collects while a learner is attached in collect mode; the
- * network is trained on them on the device; tg_solve with warm_start 2 adds
- * its prediction before the CG.  The solve still ends at rel_tol. */
+ * within `hops` steps of a removed atom predicts the event's correction on
+ * those cells.  Samples are (features of the state right after the removal,
+ * converged correction) pairs that tg_solve collects while a learner is
+ * attached in collect mode; the network is trained on them on the device;
+ * tg_solve with warm_start 2 adds its prediction before the inner
+ * iterations.  The solve still ends at rel_tol. */
 typedef struct tg_learner tg_learner;
 int tg_learner_create(int32_t hops, int32_t max_cells, int32_t ell_width, uint64_t seed, tg_learner** out);
 void tg_learner_destroy(tg_learner* L);

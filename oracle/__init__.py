@@ -97,6 +97,12 @@ def lib():
                                      C.POINTER(orc_impact), C.c_int32, C.c_void_p, C.c_void_p]
         L.orc_potential_at.restype = C.c_double
         L.orc_potential_at.argtypes = [P, C.c_void_p, C.c_int32]
+        L.orc_local_set.restype = C.c_int32
+        L.orc_local_set.argtypes = [P, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
+        L.orc_local_solve.restype = C.c_int64
+        L.orc_local_solve.argtypes = [P, C.c_void_p, C.c_int32, C.c_double, C.c_int64]
+        L.orc_stagnated.restype = C.c_int32
+        L.orc_stagnated.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
         _lib = L
     return _lib
 
@@ -169,6 +175,18 @@ class Oracle:
 
     def relax(self, n: int) -> float:
         return self.L.orc_relax_cycles(C.byref(self.m), n)
+
+    def local_set(self, node: int, shell: int) -> np.ndarray:
+        """localRelax's cells (find_localNodes minus Dirichlet), ascending."""
+        out = np.empty(self.m.n, np.int32)
+        k = self.L.orc_local_set(C.byref(self.m), int(node), int(shell), _p(out), self.m.n)
+        return out[:k].copy()
+
+    def local_solve(self, cells: np.ndarray, tol: float = 1e-14, max_sweeps: int = 10_000_000) -> int:
+        """The fixed point of localRelax on `cells`, the rest held."""
+        c = np.ascontiguousarray(cells, np.int32)
+        return self.L.orc_local_solve(C.byref(self.m), _p(c), len(c), tol, max_sweeps)
+
 
     def field_o1(self, node: int) -> np.ndarray:
         out = np.zeros(3, np.float64)
@@ -250,3 +268,9 @@ class Oracle:
     def potential_at(self, p, tet_guess) -> float:
         s = np.ascontiguousarray(p, np.float64)
         return self.L.orc_potential_at(C.byref(self.m), _p(s), int(tet_guess))
+
+
+def stagnated(deviations, queue: int, cycle: int) -> bool:
+    """The RelaxationFault rule of relax(thr, cycle, queue) on a deviation history."""
+    d = np.ascontiguousarray(deviations, np.float64)
+    return bool(lib().orc_stagnated(_p(d), len(d), int(queue), int(cycle)))

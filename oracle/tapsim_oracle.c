@@ -71,6 +71,90 @@ int64_t orc_solve(orc_mesh* m, double tol, int64_t max_sweeps, double omega, dou
     return s;
 }
 
+/* Grid_3d::Table::find_localNodes (grid_3d.cpp:1284-1315) followed by the
+ * removal of Dirichlet cells that localRelax does (:707-721): the cells
+ * reached from `node` in 1..shell steps through the Delaunay neighbours,
+ * node itself only when a neighbour leads back to it (shell >= 2), minus
+ * the Dirichlet cells; written in ascending order (a std::set<int>).
+ * Returns the count (at most cap are written). */
+int32_t orc_local_set(const orc_mesh* m, int32_t node, int32_t shell, int32_t* out, int32_t cap) {
+    uint8_t* seen = calloc((size_t)m->n, 1);
+    int32_t* front = malloc(sizeof(int32_t) * (size_t)m->n);
+    int32_t* next = malloc(sizeof(int32_t) * (size_t)m->n);
+    int32_t nf = 1, total = 0;
+    front[0] = node;
+    for (int32_t h = 0; h < shell; h++) {
+        int32_t nn = 0;
+        for (int32_t f = 0; f < nf; f++)
+            for (int32_t q = m->row_ptr[front[f]]; q < m->row_ptr[front[f] + 1]; q++) {
+                const int32_t j = m->col[q];
+                if (seen[j]) continue;
+                seen[j] = 1;
+                next[nn++] = j;
+            }
+        int32_t* t = front;
+        front = next;
+        next = t;
+        nf = nn;
+    }
+    for (int32_t i = 0; i < m->n; i++)
+        if (seen[i] && !is_dirichlet(m, i)) {
+            if (total < cap) out[total] = i;
+            total++;
+        }
+    free(seen);
+    free(front);
+    free(next);
+    return total;
+}
+
+/* The fixed point of localRelax (grid_3d.cpp:722-795): the potentials of
+ * the listed cells that satisfy computePotential (:1317-1371) with every
+ * other cell held at its value; Gauss-Seidel over the list until a sweep
+ * changes no potential by more than tol.  Returns the sweeps, -1 on the cap. */
+int64_t orc_local_solve(orc_mesh* m, const int32_t* cells, int32_t count, double tol, int64_t max_sweeps) {
+    for (int64_t s = 1; s <= max_sweeps; s++) {
+        double dev = 0.0;
+        for (int32_t k = 0; k < count; k++) {
+            const int32_t i = cells[k];
+            double sum = 0.0, d = 0.0;
+            for (int32_t q = m->row_ptr[i]; q < m->row_ptr[i + 1]; q++) {
+                const double w = row_weight(m, i, q);
+                sum += w * m->phi[m->col[q]];
+                d += w;
+            }
+            const double v = (sum - m->q[i]) / d;
+            if (fabs(v - m->phi[i]) > dev) dev = fabs(v - m->phi[i]);
+            m->phi[i] = v;
+        }
+        if (dev <= tol) return s;
+    }
+    return -1;
+}
+
+/* The stagnation rule of Grid_3d::Table::relax(thr, cycle, queue) and
+ * localRelax (grid_3d.cpp:625-654): with a full queue of the last `queue`
+ * deviations, the least-squares slope of deviation over sweep index,
+ * sum (x - xm)(y - ym) / (queue (queue^2 - 1) cycle / 12); 1 when it is
+ * exactly zero (RelaxationFault), else 0 (also while the queue is short). */
+int32_t orc_stagnated(const double* dev, int32_t count, int32_t queue, int32_t cycle) {
+    if (queue <= 0 || count < queue) return 0;
+    const double* y = dev + count - queue;
+    const double xMean = (queue - 1) / 2.0f;
+    double yMean = 0.0;
+    for (int32_t k = 0; k < queue; k++) yMean += y[k];
+    yMean /= queue;
+    double num = 0.0;
+    for (int32_t k = 0; k < queue; k++) num += (k - xMean) * (y[k] - yMean);
+    double den = queue;
+    den *= queue;
+    den -= 1;
+    den *= queue;
+    den *= cycle;
+    den /= 12.0f;
+    return num / den == 0.0;
+}
+
 double orc_relax_cycles(orc_mesh* m, int32_t n) {
     double dev = 0.0;
     for (int k = 0; k < n; k++) dev = sweep(m, 1.0);

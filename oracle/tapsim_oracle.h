@@ -44,6 +44,16 @@ double orc_residual(const orc_mesh* m);
 int64_t orc_solve(orc_mesh* m, double tol, int64_t max_sweeps, double omega, double* rel_out);
 /* n reference-style sweeps (Gauss-Seidel, ascending order); returns max |delta| of the last */
 double orc_relax_cycles(orc_mesh* m, int32_t n);
+/* find_localNodes (grid_3d.cpp:1284-1315) minus the Dirichlet cells, as
+ * localRelax forms its set (:707-721), ascending; returns the count */
+int32_t orc_local_set(const orc_mesh* m, int32_t node, int32_t shell, int32_t* out, int32_t cap);
+/* the fixed point of localRelax on a cell list (every other cell held):
+ * Gauss-Seidel until a sweep moves no potential by more than tol; returns
+ * the sweeps, -1 on the cap */
+int64_t orc_local_solve(orc_mesh* m, const int32_t* cells, int32_t count, double tol, int64_t max_sweeps);
+/* the stagnation rule of relax(thr, cycle, queue) (grid_3d.cpp:625-654) on
+ * the last `queue` of `count` deviations: 1 for a zero slope */
+int32_t orc_stagnated(const double* dev, int32_t count, int32_t queue, int32_t cycle);
 /* Grid_3d::Table::field_o1; returns 0 when the 3x3 system is singular */
 int orc_field_o1(const orc_mesh* m, int32_t i, double E[3]);
 /* Grid_3d::Table::force (grid_3d.cpp:1201-1236) */

@@ -163,6 +163,8 @@ SIGNATURES = {
     "tg_run_event": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, C.POINTER(tg_event_record)]),
     "tg_run_events": (C.c_int, [_P, C.POINTER(tg_event_opts), _I, _I, _P, C.POINTER(C.c_int32)]),
     "tg_run_tips": (C.c_int, [_P, _I, _P, _I, _P, _P, _P, _I]),
+    "tg_amg_schedule": (C.c_int, [_P, _I, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "tg_timer_start": (C.c_int, [_P]),
     "tg_timer_stop": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "tg_launch_count": (C.c_int64, [_P]),

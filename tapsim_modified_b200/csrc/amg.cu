@@ -210,7 +210,66 @@ inline int grid_for(long long threads) {
     return (int)(b < cap ? (b > 0 ? b : 1) : cap);
 }
 
+// Mean time of `trials` launches of f() on s, after one warm-up launch.
+template <class F>
+float time_launches(F f, int trials, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    f();
+    cudaEventRecord(e0, s);
+    for (int k = 0; k < trials; k++) f();
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / trials;
+}
+
 }  // namespace
+
+int amg_tune_lanes(AmgDev& g, cudaStream_t s, float* aMs, float* rMs) {
+    static const int kCand[5] = {2, 4, 8, 16, 32};
+    constexpr int kTrials = 5;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return -1;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return -1;
+    }
+    const double* noScal = nullptr;  // target < 0: the kernels never read it
+    for (int l = 0; l + 1 < g.levels; l++) {
+        AmgDevLevel& L = g.lev[l];
+        AmgDevLevel& C = g.lev[l + 1];
+        // the restriction R_l: next level's rows, output into its b
+        float best = 1e30f;
+        for (int c : kCand) {
+            const float ms = time_launches(
+                [&] { launch_mv(c, C.n, L.r_ptr, L.r_col, L.r_val, l == 0 ? g.t0 : L.t, C.b, noScal, 0, -1.0, s); },
+                kTrials, s, e0, e1);
+            if (ms < best) {
+                best = ms;
+                L.r_lanes = c;
+            }
+        }
+        if (rMs) rMs[l] = best;
+        // the operator of level l + 1 when it is smoothed with CSR rows (not
+        // the coarsest, which the dense inverse solves)
+        if (l + 2 < g.levels) {
+            best = 1e30f;
+            for (int c : kCand) {
+                const float ms = time_launches(
+                    [&] { launch_csr(c, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, noScal, 0, -1.0, s); },
+                    kTrials, s, e0, e1);
+                if (ms < best) {
+                    best = ms;
+                    C.a_lanes = c;
+                }
+            }
+            if (aMs) aMs[l + 1] = best;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s) {
     const int slices = (slots + 31) / 32;

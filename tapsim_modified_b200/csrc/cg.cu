@@ -362,10 +362,14 @@ __global__ void k_vcg_residual(DevMesh m, VSys v, const int32_t* __restrict__ ro
 // passes compute them; the differences of their squares to the stored
 // values go into rsum (V rows, Neumann rows, b), and the FP32 right-hand
 // sides of the inner solves get the new values.
+// countDev (may be null): a device-side count that caps `count`, for a list
+// whose length only the device knows (the learned start's cells).
 __global__ void k_residual_rows(DevMesh m, VSys v, float* rN, const int32_t* __restrict__ flips, int count,
-                                int32_t* stamp, int epoch, double* r64, double* b64, double* rsum) {
+                                const int32_t* countDev, int32_t* stamp, int epoch, double* r64, double* b64,
+                                double* rsum) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (countDev && *countDev < count) count = *countDev;
     if (warp >= count) return;
     const int f = flips[warp];
     const int q0 = m.row_ptr[f], q1 = m.row_ptr[f + 1];
@@ -600,11 +604,11 @@ void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, i
     }
 }
 void launch_residual_rows(const DevMesh& m, const VSys& v, float* rN, const int32_t* flips, int count, int32_t* stamp,
-                          int epoch, double* r64, double* b64, double* rsum, cudaStream_t s) {
+                          int epoch, double* r64, double* b64, double* rsum, cudaStream_t s, const int32_t* countDev) {
     if (count > 0) {
         count_launch();
-        k_residual_rows<<<(count + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, s>>>(m, v, rN, flips, count, stamp,
-                                                                                     epoch, r64, b64, rsum);
+        k_residual_rows<<<(count + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, s>>>(m, v, rN, flips, count, countDev,
+                                                                                     stamp, epoch, r64, b64, rsum);
     }
 }
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s) {

@@ -147,6 +147,9 @@ struct tg_handle {
     DBuf<float> vVal, vVec;  // vVec: d, x, r, u, w, p, sv, hist, each capacity+1
     DBuf<__nv_bfloat16> vVal16;  // vVal rounded to bf16 (multigrid smoothing pass)
     DBuf<float> vG;              // row sums of the V rows (capacity+1)
+    // timings [ms] of the tuned lane groups of each level's operator and
+    // restriction (amg_tune_lanes), 0 where a level has none
+    float amgTunedA[tgd::kAmgMaxLevels] = {}, amgTunedR[tgd::kAmgMaxLevels] = {};
     // FP64 inner iterations: couplings at the SELL positions and the vectors
     // d64, x64, r64, p64, s64, w64 (each capacity+1), allocated at the first
     // solve with inner_precision 1
@@ -1273,6 +1276,12 @@ static int amg_setup_impl(tg_handle* h, double* seconds) {
         h->amg_release();
         return cuda_check(h, e, "multigrid upload");
     }
+    // the coarse levels' lane groups from timed trials on this hierarchy
+    for (int l = 0; l < tgd::kAmgMaxLevels; l++) h->amgTunedA[l] = h->amgTunedR[l] = 0.0f;
+    if (amg_tune_lanes(g, h->stream, h->amgTunedA, h->amgTunedR) != 0) {
+        h->amg_release();
+        return cuda_check(h, cudaGetLastError(), "multigrid schedule tuning");
+    }
     h->amg = g;
     h->amgReady = true;
     h->amgSlots = slots;
@@ -1379,14 +1388,15 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     // a solve right after removals from a converged state records its
     // correction; with warm_start it starts from the previous one
     const bool fromEvent = h->converged && h->removalsSinceSolve > 0;
-    const bool warm = fromEvent && h->histValid && (o->warm_start == 1 || o->warm_start == 2);
+    const bool warm = fromEvent && h->histValid && o->warm_start == 1;
     const bool learnPredict = fromEvent && h->learner && (h->learnMode & 2) && o->warm_start == 2 && h->lastSite >= 0;
     // the first residual after removals from a converged state: the rows the
     // removals touched, from the kept residuals of the potentials as they
-    // are; a warm start then takes A hist off the V rows (FP32) and the
-    // Neumann rows are recomputed.  The learned start changes potentials
-    // around the site as well and takes the full pass.
-    const bool incremental = h->residValid && fromEvent && !h->pendingOverflow && h->nPending > 0 && !learnPredict;
+    // are; a recycled start then takes A hist off the V rows (FP32) and the
+    // Neumann rows are recomputed.  The learned start changes the
+    // potentials of its graph's cells: their rows and their neighbours' are
+    // recomputed too (FP64), after the prediction.
+    const bool incremental = h->residValid && fromEvent && !h->pendingOverflow && h->nPending > 0;
     const int nPending = h->nPending;
     h->residValid = h->pendingOverflow = false;
     h->nPending = 0;
@@ -1405,12 +1415,25 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     }
     if (warm) launch_vcg_warm(m, vsys, h->vActive, 1.0f, h->stream);
     else if (fromEvent) CK(cudaMemsetAsync(vsys.hist, 0, sizeof(float) * ((size_t)h->vCapacity + 1), h->stream));
-    // learned near field on top of the recycled far field; sample collection
+    // learned near field on the plain start; sample collection
     const bool learnCollect = fromEvent && h->learner && (h->learnMode & 1) && h->lastSite >= 0;
     if (learnPredict || learnCollect) {
-        rc = learner_predict(h->learner, m, h->lastSite, vsys.slot_of, learnPredict ? vsys.hist : nullptr, h->stream,
-                             learnCollect);
+        rc = learner_predict(h->learner, m, h->lastSite, h->stream, learnCollect, learnPredict);
         if (rc != TG_OK) return fail(h, rc, std::string("tg_solve: ") + tg_learner_last_error(h->learner));
+        if (learnPredict && incremental) {
+            // the predicted cells' rows and their neighbours' from the new
+            // potentials, with a fresh stamp (the removals' pass above may
+            // have taken some of these rows before the prediction)
+            const int32_t *cells = nullptr, *cellCount = nullptr;
+            int cap = 0;
+            learner_graph_cells(h->learner, &cells, &cellCount, &cap);
+            if (++h->resEpoch == INT32_MAX) {
+                CK(cudaMemsetAsync(h->resStamp.p, 0, sizeof(int32_t) * (size_t)h->n, h->stream));
+                h->resEpoch = 1;
+            }
+            launch_residual_rows(m, vsys, vN.r, cells, cap, h->resStamp.p, h->resEpoch, rv, bv, h->rsum.p, h->stream,
+                                 cellCount);
+        }
     }
     h->converged = h->histValid = false;
     h->removalsSinceSolve = 0;
@@ -1515,6 +1538,23 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         if (rc != TG_OK) return fail(h, rc, std::string("tg_solve: ") + tg_learner_last_error(h->learner));
     }
     if (info) *info = inf;
+    return TG_OK;
+}
+
+int tg_amg_schedule(tg_handle* h, int32_t level, int32_t* rows, int32_t* a_lanes, int32_t* r_lanes, float* a_ms,
+                    float* r_ms) {
+    DeviceScope dev_scope(h);
+    if (!h) return fail(h, TG_ERR_ARGUMENT, "tg_amg_schedule: null handle");
+    if (!h->amgReady || level < 0 || level >= h->amg.levels)
+        return fail(h, TG_ERR_ARGUMENT, "tg_amg_schedule: no such multigrid level (built at the first multigrid solve)");
+    const tgd::AmgDevLevel& L = h->amg.lev[level];
+    if (rows) *rows = level == 0 ? h->amgSlots : L.n;
+    const bool csr = level >= 1 && level + 1 < h->amg.levels;
+    const bool restr = level + 1 < h->amg.levels;
+    if (a_lanes) *a_lanes = csr ? L.a_lanes : 0;
+    if (r_lanes) *r_lanes = restr ? L.r_lanes : 0;
+    if (a_ms) *a_ms = csr ? h->amgTunedA[level] : 0.0f;
+    if (r_ms) *r_ms = restr ? h->amgTunedR[level] : 0.0f;
     return TG_OK;
 }
 

@@ -137,6 +137,13 @@ struct AmgDev {
     float *y0, *t0;                         // level-0 work vectors (capacity + 1)
     const float* coarse_inv;                // dense inverse of the coarsest operator, row-major
 };
+// Autotuner of the coarse levels' schedules: for the restriction of every
+// level and the operator of every level smoothed by CSR rows, times each
+// lane-group size (2..32 lanes per row, 5 launches each after a warm-up,
+// CUDA events on s) and keeps the fastest in r_lanes / a_lanes.  aMs / rMs
+// (kAmgMaxLevels entries, may be null) receive the winners' times [ms].
+// Returns 0, or -1 on a CUDA error.
+int amg_tune_lanes(AmgDev& g, cudaStream_t s, float* aMs, float* rMs);
 // the level-0 smoothing pass t = b - A y alone (timing hook)
 void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s);
 // u = M^-1 r, one V(1,1)-cycle, for CG iteration `it`
@@ -161,7 +168,8 @@ void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, i
 // system's r and rN the new values.  stamp (by node) holds a value other
 // than epoch for every row
 void launch_residual_rows(const DevMesh& m, const VSys& v, float* rN, const int32_t* flips, int count, int32_t* stamp,
-                          int epoch, double* r64, double* b64, double* rsum, cudaStream_t s);
+                          int epoch, double* r64, double* b64, double* rsum, cudaStream_t s,
+                          const int32_t* countDev = nullptr);
 void launch_vsys_add_rows(const DevMesh& m, const VSys& v, const int32_t* nodes, int count, cudaStream_t s);
 // re-copies the couplings and diagonals that flips of the listed cells
 // changed into the V system (rows that existed before the flips)

@@ -2,10 +2,10 @@
 // samples the solver collects, and its inference inside tg_solve.
 //
 // A sample is one removal: the graph of free cells within `hops` steps of
-// the removed cell, 16 features per cell taken right after the recycled
-// far-field start is applied, and the target (phi_final - phi_start) / sigma
-// on the same cells, where phi_final is the potential the solve converged
-// to.  Training minimises the mean squared error over the cells of a batch
+// the removed cell, 16 features per cell taken from the state right after
+// the removal (the plain start), and the target (phi_final - phi_start) /
+// sigma on the same cells, where phi_final is the potential the solve
+// converged to.  Training minimises the mean squared error over the cells of a batch
 // of samples with Adam; forward and backward GEMMs run on the tensor cores
 // (mpnn.cu).  Inference adds sigma * y to the potentials (and to the
 // recorded correction) before the CG starts; the solve still ends at its
@@ -277,8 +277,13 @@ int learner_attach_mesh(tg_learner* L, size_t meshNodes, int maxRow) {
     return TG_OK;
 }
 
-int learner_predict(tg_learner* L, const DevMesh& m, int site, const int32_t* slotOf, float* hist, cudaStream_t s,
-                    bool collect) {
+void learner_graph_cells(const tg_learner* L, const int32_t** nodes, const int32_t** count, int* capacity) {
+    *nodes = L->nodes.p;
+    *count = L->count.p;
+    *capacity = L->cap;
+}
+
+int learner_predict(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, bool collect, bool predict) {
     const cudaStream_t own = L->stream;
     L->stream = s;
     L->collecting = collect;
@@ -297,10 +302,11 @@ int learner_predict(tg_learner* L, const DevMesh& m, int site, const int32_t* sl
             cudaMemcpyAsync(L->sCol.p + o * L->D, L->ellCol.p, sizeof(int32_t) * n * L->D, cudaMemcpyDeviceToDevice, s);
         }
     }
-    if (rc == TG_OK && hist != nullptr) {
+    if (rc == TG_OK && predict) {
         rc = forward(L, L->X.p, L->ellCol.p, L->ellW.p, n);
         if (rc == TG_OK)
-            launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, slotOf, hist, L->cap, s);
+            launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, nullptr, nullptr, L->cap,
+                                    s);
     }
     L->stream = own;
     if (rc == TG_OK && cudaGetLastError() != cudaSuccess) rc = lfail(L, TG_ERR_CUDA, "learner: launch");

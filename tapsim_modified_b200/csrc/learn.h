@@ -16,9 +16,12 @@ int learner_device(const tg_learner* L);
 int learner_attach_mesh(tg_learner* L, size_t meshNodes, int maxRow);
 // graph and features of `site` from the current state; with `collect` the
 // features are stored as a new sample (finished by learner_collect_end);
-// with `hist` the prediction is added to the potentials and to hist
-int learner_predict(tg_learner* L, const tgd::DevMesh& m, int site, const int32_t* slotOf, float* hist,
-                    cudaStream_t s, bool collect);
+// with `predict` the prediction is added to the potentials of the graph's
+// cells
+int learner_predict(tg_learner* L, const tgd::DevMesh& m, int site, cudaStream_t s, bool collect, bool predict);
+// the cells of the last graph (device list, its length on the device) and
+// the list's capacity: the cells whose potentials a prediction changed
+void learner_graph_cells(const tg_learner* L, const int32_t** nodes, const int32_t** count, int* capacity);
 // the target of the sample started by learner_predict, from the converged state
 int learner_collect_end(tg_learner* L, const tgd::DevMesh& m, cudaStream_t s);
 // drops a sample that learner_predict started

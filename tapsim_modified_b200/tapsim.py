@@ -207,6 +207,25 @@ class Grid:
         self._ck(N.lib().tg_solve(self._h, C.byref(o), C.byref(info)))
         return info
 
+    def amg_schedule(self) -> list[dict]:
+        """Per multigrid level: rows and the tuned lanes per CSR row of its
+        operator and restriction with their launch times (tg_amg_schedule)."""
+        out = []
+        level = 0
+        while True:
+            rows, al, rl = C.c_int32(), C.c_int32(), C.c_int32()
+            am, rm = C.c_float(), C.c_float()
+            rc = N.lib().tg_amg_schedule(self._h, level, C.byref(rows), C.byref(al), C.byref(rl), C.byref(am),
+                                         C.byref(rm))
+            if rc != N.TG_OK:
+                if level == 0:
+                    self._ck(rc)
+                break
+            out.append({"level": level, "rows": rows.value, "a_lanes": al.value, "r_lanes": rl.value,
+                        "a_ms": am.value, "r_ms": rm.value})
+            level += 1
+        return out
+
     def residual(self) -> float:
         r = C.c_double()
         self._ck(N.lib().tg_residual(self._h, C.byref(r)))

@@ -42,6 +42,11 @@ for them (logTrajectory.cpp:137-300, pushed as process.cpp:1048-1049 does):
 ref_traj_ascii.txt (one file) and ref_traj_bin.00000001 / .00000002
 (binary, chunk size 2).
 
+With `--default-ini` it runs 40 events with the reference's shipped default
+ini instead (localRelax of the 3-hop shell to 1e-2 V plus one global sweep
+per event, no refresh; process.cpp:851-893) after the same initial
+relaxation: ref_events_default.txt.
+
 With `--snapshots` it repeats the first event with Fe's DIELECTRICITY set
 to 5 (tip_eps5.cfg; --no-sync keeps the dump's couplings, so only the
 dielectric force changes) and keeps the snapshots that the reference's own
@@ -200,8 +205,32 @@ def snapshots():
     shutil.rmtree(tmp)
 
 
+def default_ini():
+    """40 events of the golden tip with the reference's shipped default ini
+    (local relaxation of the 3-hop shell to 1e-2 V plus one global sweep per
+    event, no refresh), one thread, after the initial relaxation to the float
+    fixed point: ref_events_default.txt."""
+    if not HARNESS.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    tmp = HERE / "_tmp"
+    tmp.mkdir(exist_ok=True)
+    with gzip.open(HERE / "ref_mesh.dump.gz", "rb") as f, open(tmp / "ref.dump", "wb") as g:
+        shutil.copyfileobj(f, g)
+    ini = dict(INI_DEFAULTS)
+    ini.update({"RESULTS_FILENAME": "", "TRAJECTORY_FILENAME": "", "GRID_FILENAME": "", "SURFACE_FILENAME": "",
+                "GEOMETRY_FILENAME": "", "DUMP_FILENAME": ""})
+    (tmp / "default.ini").write_text("".join(f"{k} = {v}\n" for k, v in ini.items()))
+    subprocess.run([str(HARNESS), "evap", str(HERE / "tip.cfg"), "-", str(tmp / "default.ini"), str(N_EVENTS),
+                    str(HERE / "ref_events_default.txt"), "--dump", str(tmp / "ref.dump"), "--threads", "1",
+                    "--init-relax", "0", "100", "25"], check=True, capture_output=True)
+    print("default ini ->", "ref_events_default.txt")
+    shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
-    if "--modes" in sys.argv:
+    if "--default-ini" in sys.argv:
+        default_ini()
+    elif "--modes" in sys.argv:
         modes()
     elif "--results" in sys.argv:
         results()

@@ -40,3 +40,33 @@ def test_multigrid_events_follow_reference(ref_mesh, ref_events):
         fb = np.array(r["fieldBefore"])
         assert np.linalg.norm(fb - row[8:11]) <= 1e-4 * np.linalg.norm(row[8:11])
     g.close()
+
+
+def test_tuned_schedules_of_the_hierarchy():
+    """The hierarchy build times every lane-group size of each coarse
+    operator and restriction on the device and keeps the fastest
+    (amg_tune_lanes): every level but the coarsest reports a restriction
+    schedule, every level smoothed with CSR rows an operator schedule, each a
+    power of two in 2..32 with a positive launch time; the solve converges
+    with them.  On the config-1 tip (307k cells) the hierarchy has at least
+    three levels."""
+    import sys
+    from conftest import GOLDEN as G
+    sys.path.insert(0, str(G))
+    from make_config1 import CONFIG1_TIP
+    from tapsim_modified_b200.tapsim import Grid, Mesh
+    g = Grid(Mesh.from_tip(**CONFIG1_TIP))
+    info = g.solve(rel_tol=1e-8, max_outer=50, max_inner=20000, preconditioner=1)
+    assert info.rel_residual <= 1e-8 and info.setup_seconds > 0
+    sched = g.amg_schedule()
+    print(sched)
+    assert len(sched) >= 3
+    assert sched[0]["rows"] > sched[1]["rows"] > sched[-1]["rows"]
+    for k, lv in enumerate(sched):
+        last = k == len(sched) - 1
+        assert (lv["r_lanes"] in (2, 4, 8, 16, 32) and lv["r_ms"] > 0) if not last else lv["r_lanes"] == 0
+        if 1 <= k < len(sched) - 1:
+            assert lv["a_lanes"] in (2, 4, 8, 16, 32) and lv["a_ms"] > 0
+        else:
+            assert lv["a_lanes"] == 0
+    g.close()

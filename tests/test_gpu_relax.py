@@ -139,3 +139,98 @@ def test_fp64_inner_iterations_match_oracle_and_fp32(small_mesh, ref_mesh, ref_e
     assert np.abs(phi32 - phi64).max() < 1e-8
     for x, y in zip(r32, r64):
         assert np.linalg.norm(np.subtract(x["stop"], y["stop"])) <= 1e-6 * np.linalg.norm(y["stop"])
+
+
+def _five_cell_handle():
+    """A hand-built system: one free cell coupled to four Dirichlet cells
+    (two at 1 V, two at 0 V) and nothing else, so that one sweep puts it at
+    its exact value (0.5 V) and every later sweep moves nothing."""
+    import ctypes as C
+    from tapsim_modified_b200 import _native as N
+    xyz = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0]], np.float32) * 1e-9
+    type_id = np.array([0, 1, 1, 2, 2], np.int8)
+    hull = np.zeros(5, np.uint8)
+    phi = np.array([0.0, 1.0, 1.0, 0.0, 0.0], np.float32)
+    row_ptr = np.array([0, 4, 5, 6, 7, 8], np.int32)
+    col = np.array([1, 2, 3, 4, 0, 0, 0, 0], np.int32)
+    cpl = np.ones(8, np.float64)
+    types = (N.tg_type * 3)()
+    for k, (dirichlet, p) in enumerate(((0, 0.0), (1, 1.0), (1, 0.0))):
+        types[k].id, types[k].epsilon, types[k].dirichlet, types[k].phi = k, 1.0, dirichlet, p
+        types[k].removable = 0
+    keep = (xyz, type_id, hull, phi, row_ptr, col, cpl, types)
+    d = N.tg_mesh_desc(num_nodes=5, xyz=xyz.ctypes.data, type_id=type_id.ctypes.data, hull=hull.ctypes.data,
+                       phi=phi.ctypes.data, row_ptr=row_ptr.ctypes.data, col=col.ctypes.data,
+                       coupling=cpl.ctypes.data, num_tets=0, num_types=3, types=types)
+    h = C.c_void_p()
+    N.check(N.lib().tg_create(C.byref(d), C.byref(h)))
+    return h, keep
+
+
+def test_stagnation_fault_on_a_built_case():
+    """The stagnation rule (grid_3d.cpp:625-654, RelaxationFault) fires, as
+    TG_ERR_RELAX_FAULT, once a full queue of deviations is flat: with the
+    threshold below any deviation the relaxation only ends that way.  The
+    free cell is exact after the first sweep (couplings of 1, so 0.5 V is
+    exact in FP64), so each cycle's deviation (its last sweep's largest
+    change) is 0: the queue of 3 is flat at the third cycle, where the rule
+    fires with two cycles of two sweeps counted (the count grows after the
+    test, as in the reference).  The same for localRelax on the cell's
+    shell-2 set."""
+    import ctypes as C
+    from oracle import stagnated
+    from tapsim_modified_b200 import _native as N
+    h, keep = _five_cell_handle()
+    L = N.lib()
+    it, dev = C.c_int64(), C.c_double()
+    rc = L.tg_relax_threshold(h, -1.0, 2, 3, 1000, C.byref(it), C.byref(dev))
+    assert rc == N.TG_ERR_RELAX_FAULT, rc
+    assert it.value == 4 and dev.value == 0.0
+    assert stagnated([0.0, 0.0, 0.0], 3, 2) and not stagnated([0.0, 0.0], 3, 2)
+    phi = np.empty(5, np.float64)
+    N.check(L.tg_get_phi(h, N.ptr(phi)), h)
+    assert phi[0] == 0.5
+    # localRelax from the free cell: its shell-2 set is the cell itself
+    N.check(L.tg_set_phi(h, N.ptr(np.array([0.25, 1.0, 1.0, 0.0, 0.0]))), h)
+    rc = L.tg_local_relax(h, 0, 2, -1.0, 2, 3, C.byref(it), C.byref(dev))
+    assert rc == N.TG_ERR_RELAX_FAULT, rc
+    assert it.value == 4 and dev.value == 0.0
+    N.check(L.tg_get_phi(h, N.ptr(phi)), h)
+    assert phi[0] == 0.5
+    L.tg_destroy(h)
+
+
+def test_local_relax_reaches_the_oracle_fixed_point(ref_mesh):
+    """tg_local_relax after a removal, to a deviation of 1e-13 V, against the
+    oracle's fixed point of localRelax on find_localNodes' set minus the
+    Dirichlet cells (grid_3d.cpp:707-795, 1284-1315): the same potentials on
+    the set, and no cell outside it moves.  The device sweeps in colour
+    order and the reference in index order, but both converge to this one
+    fixed point (the local Dirichlet problem)."""
+    from oracle import Oracle
+    from tapsim_modified_b200.tapsim import Grid
+    a = ref_mesh.arrays()
+    g = Grid(ref_mesh)
+    g.solve(rel_tol=1e-10)
+    g.surface_init(0)
+    s = g.select()
+    o = Oracle(a)
+    o.phi[:] = g.potentials()
+    o.surface_init(0)
+    g.take_away(s.candidate)
+    o.take_away(s.candidate, 0)
+    before = g.potentials()
+    for shell in (3, 5):
+        g.set_potentials(before)
+        o.phi[:] = before
+        rc, it, dev = g.local_relax(s.candidate, shell, 1e-13, 5, 5)
+        assert rc == 0 and dev <= 1e-13
+        cells = o.local_set(s.candidate, shell)
+        assert o.local_solve(cells, 1e-14, 200_000) > 0
+        after = g.potentials()
+        inside = np.zeros(len(after), bool)
+        inside[cells] = True
+        assert np.array_equal(after[~inside], before[~inside])
+        assert np.abs(after[inside] - o.phi[inside]).max() < 1e-11
+        print("shell", shell, "cells", len(cells), "sweeps", it,
+              "max |dphi| vs oracle", np.abs(after[inside] - o.phi[inside]).max())

@@ -66,3 +66,36 @@ def test_event_sequence_fields_and_impacts_match_reference(ref_mesh, ref_events)
             assert abs(imp.stop[2] - row[20]) <= 1e-6 * row[20]
             # potential after removal
             assert abs(o.phi[node] - row[11]) < 2e-5
+
+
+def test_local_set_is_find_local_nodes_minus_dirichlet(ref_mesh):
+    """orc_local_set follows find_localNodes (grid_3d.cpp:1284-1315): the
+    shell-1 set holds the neighbours only, the start joins from shell 2 on,
+    Dirichlet cells are dropped, and each shell contains the smaller one."""
+    from oracle import Oracle
+    a = ref_mesh.arrays()
+    o = Oracle(a)
+    types = a["types"]
+    dirichlet = np.array([bool(types[int(t)]["dirichlet"]) for t in a["type"]])
+    rp, col = a["row_ptr"], a["col"]
+    node = int(np.nonzero(~dirichlet)[0][len(np.nonzero(~dirichlet)[0]) // 2])
+    s1 = o.local_set(node, 1)
+    nb = set(col[rp[node]:rp[node + 1]].tolist())
+    assert set(s1.tolist()) == {j for j in nb if not dirichlet[j]}
+    s2, s3 = o.local_set(node, 2), o.local_set(node, 3)
+    assert node in set(s2.tolist()) and set(s1) <= set(s2) <= set(s3)
+    assert not dirichlet[s3].any() and np.all(np.diff(s3) > 0)
+
+
+def test_stagnation_rule_matches_the_reference_formula():
+    """The slope test of relax(thr, cycle, queue): a flat history is a
+    fault, a decreasing one is not, a short queue never is, and a queue of
+    one never is either (its slope is 0 / 0, which is not equal to 0)."""
+    from oracle import stagnated
+    assert stagnated([1e-3, 1e-3, 1e-3], 3, 5)
+    assert stagnated([0.0, 0.0, 0.0], 3, 2)
+    assert not stagnated([3e-3, 2e-3, 1e-3], 3, 5)
+    assert not stagnated([1e-3, 1e-3], 3, 5)
+    assert not stagnated([0.5], 1, 5)
+    # symmetric values around the mean cancel exactly
+    assert stagnated([1.0, 2.0, 1.0], 3, 1)
