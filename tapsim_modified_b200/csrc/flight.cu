@@ -778,8 +778,14 @@ void launch_trace(const DevMesh& m, int nIons, const float* start, const float* 
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s) {
     if (nIons <= 0) return;
     count_launch();
-    const int blocks = (nIons + kBlock - 1) / kBlock;
-    auto go = [&](auto kernel) { kernel<<<blocks, kBlock, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); };
+    // a flight is a chain of dependent loads, one ion per thread: with one
+    // warp per block, a few thousand ions spread over all SMs instead of
+    // filling a quarter of them four warps deep
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int block = nIons <= 2 * 32 * sms ? 32 : kBlock;
+    const int blocks = (nIons + block - 1) / block;
+    auto go = [&](auto kernel) { kernel<<<blocks, block, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); };
     const int prec = tp.precision == 1 ? 1 : (tp.precision == 2 ? 2 : 0);
     if (tp.path) {
         if (prec == 0) go(k_trace<true, 0>); else if (prec == 1) go(k_trace<true, 1>); else go(k_trace<true, 2>);

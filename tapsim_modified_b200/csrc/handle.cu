@@ -1608,9 +1608,10 @@ int tg_surface_init(tg_handle* h, int32_t vacuumId, int32_t* num) {
 
 int tg_surface_select(tg_handle* h, tg_select_info* info) { return tg_surface_select_mode(h, 0, 0.0f, info); }
 
-int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_select_info* info) {
-    DeviceScope dev_scope(h);
-    if (!h || !info) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: null argument");
+// The selection's kernels and the copy of its keys and sums into pinned
+// memory, queued on the handle's stream; select_decode reads them once the
+// stream has been synchronised.
+static int select_launch(tg_handle* h, int32_t mode, float temperature) {
     if (h->vacuumId < 0) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: surface not initialised");
     if (mode < 0 || mode > 3) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: probability mode 0..3");
     if (mode == 1 && !(temperature > 0.0f))
@@ -1624,8 +1625,25 @@ int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_sel
     launch_surface_second(h->sf(), h->surfSlots, h->acc.p, h->keys.p, h->stream);
     CK(cudaMemcpyAsync(h->pin->keys, h->keys.p, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(h->pin->sums, h->acc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    int rc = sync_status(h, "tg_surface_select");
+    return TG_OK;
+}
+
+static int select_decode(tg_handle* h, int32_t mode, tg_select_info* info);
+
+int tg_surface_select_mode(tg_handle* h, int32_t mode, float temperature, tg_select_info* info) {
+    DeviceScope dev_scope(h);
+    if (!h || !info) return fail(h, TG_ERR_ARGUMENT, "tg_surface_select: null argument");
+    int rc = select_launch(h, mode, temperature);
     if (rc != TG_OK) return rc;
+    rc = sync_status(h, "tg_surface_select");
+    if (rc != TG_OK) return rc;
+    return select_decode(h, mode, info);
+}
+
+// The candidate, the runner-ups, the apex and the sums of the selection
+// select_launch queued, from pinned memory (the stream has been
+// synchronised since); sets the handle's selection.
+static int select_decode(tg_handle* h, int32_t mode, tg_select_info* info) {
     unsigned long long k[7];
     std::memcpy(k, h->pin->keys, sizeof(k));
     const double sums[2] = {h->pin->sums[0], h->pin->sums[1]};
@@ -2279,12 +2297,12 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, i
         rec->relax_iterations = si.inner;
         rec->rel_residual = si.rel_residual;
     }
-    // IV) fields, probabilities and the next candidate
-    {
-        tg_select_info s;
-        rc = tg_surface_select_mode(h, o->prob_mode, o->temperature, &s);
-        if (rc != TG_OK && rc != TG_ERR_NO_SURFACE) return rc;
-    }
+    // IV) fields, probabilities and the next candidate: queued here and
+    // decoded after the event's one synchronisation at its end (only the
+    // next event reads them)
+    rc = select_launch(h, o->prob_mode, o->temperature);
+    if (rc != TG_OK) return rc;
+    h->selValid = false;
     // V) ion flight of the removed atom, VI) state after removal
     if (o->trace_enabled) {
         const float start[3] = {h->h_xyz[3 * (size_t)node], h->h_xyz[3 * (size_t)node + 1], h->h_xyz[3 * (size_t)node + 2]};
@@ -2369,6 +2387,11 @@ static int run_event(tg_handle* h, const tg_event_opts* o, int32_t eventIndex, i
     if (o->normal_enabled) CK(cudaStreamWaitEvent(h->stream, h->evNormal, 0));
     rc = sync_status(h, "tg_run_event");
     if (rc != TG_OK) return rc;
+    {
+        tg_select_info next;
+        rc = select_decode(h, o->prob_mode, &next);
+        if (rc != TG_OK && rc != TG_ERR_NO_SURFACE) return rc;
+    }
     rec->phi_before = (float)pin->before[0];
     rec->phi_after = (float)pin->after[0];
     for (int k = 0; k < 3; k++) {
