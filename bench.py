@@ -181,6 +181,37 @@ def build_mesh(tip: str, seed: int):
     return m
 
 
+def train_learner(args, rank: int, opts):
+    """Learned near field: samples from events on a training tip of another
+    shape and seed (plain solver, one sample per event), trained on the
+    device by the project's own forward and backward kernels; the last tenth
+    of the samples is held out.  Returns the learner and a summary."""
+    from tapsim_modified_b200.tapsim import Evaporation, Grid, Learner, Mesh, solve_opts
+    t0 = time.perf_counter()
+    tmesh = Mesh.from_tip(seed=101 + rank, **TIPS["train"])
+    tgrid = Grid(tmesh)
+    tgrid.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
+    learner = Learner(hops=6, max_cells=8192, ell_width=64, seed=7 + rank)
+    learner.attach(tgrid, collect=True)
+    tev = Evaporation(tgrid, opts, relax_mode=1,
+                      solve=solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, preconditioner=PRECOND))
+    tev.run(args.train_events)
+    learner.attach(tgrid)
+    tgrid.close()
+    n, cells = learner.samples()
+    hold = max(1, n // 10)
+    train_n = n - hold
+    before = learner.gradients(train_n, hold)[0]
+    last = learner.train(args.train_steps, batch=8, lr=1e-3, seed=rank, first=0, count=train_n)
+    after = learner.gradients(train_n, hold)[0]
+    return learner, {"train_tip": f"train: r={TIPS['train']['cap_radius'] * 1e9:g} nm cap, "
+                                  f"{TIPS['train']['shank_length'] * 1e9:g} nm shank, seed {101 + rank}, "
+                                  f"{tmesh.num_nodes} cells",
+                     "samples": n, "cells_per_sample": cells / max(n, 1), "train_steps": args.train_steps,
+                     "train_loss_last": last, "heldout_loss_untrained": before, "heldout_loss_trained": after,
+                     "setup_s": time.perf_counter() - t0}
+
+
 def run_ours(args, rank: int, world: int, dist):
     import ctypes as C
 
@@ -204,34 +235,6 @@ def run_ours(args, rank: int, world: int, dist):
     atoms = int((arrays["type"] == 4).sum())
     h2d_bytes = sum(v.nbytes for k, v in arrays.items() if isinstance(v, np.ndarray))
     opts = EvaporationOptions.from_ini(None)
-
-    def train_learner():
-        """Learned near field: samples from events on a training tip of
-        another shape and seed (plain solver), trained on the device; the
-        last tenth of the samples is held out."""
-        t0 = time.perf_counter()
-        tmesh = Mesh.from_tip(seed=101 + rank, **TIPS["train"])
-        tgrid = Grid(tmesh)
-        tgrid.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
-        learner = Learner(hops=6, max_cells=8192, ell_width=64, seed=7 + rank)
-        learner.attach(tgrid, collect=True)
-        tev = Evaporation(tgrid, opts, relax_mode=1,
-                          solve=solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, preconditioner=PRECOND))
-        tev.run(args.train_events)
-        learner.attach(tgrid)
-        tgrid.close()
-        n, cells = learner.samples()
-        hold = max(1, n // 10)
-        train_n = n - hold
-        before = learner.gradients(train_n, hold)[0]
-        last = learner.train(args.train_steps, batch=8, lr=1e-3, seed=rank, first=0, count=train_n)
-        after = learner.gradients(train_n, hold)[0]
-        return learner, {"train_tip": f"train: r={TIPS['train']['cap_radius'] * 1e9:g} nm cap, "
-                                      f"{TIPS['train']['shank_length'] * 1e9:g} nm shank, seed {101 + rank}, "
-                                      f"{tmesh.num_nodes} cells",
-                         "samples": n, "cells_per_sample": cells / max(n, 1), "train_steps": args.train_steps,
-                         "train_loss_last": last, "heldout_loss_untrained": before, "heldout_loss_trained": after,
-                         "setup_s": time.perf_counter() - t0}
 
     def run_arm(name: str, warm_start: int, learner=None, inner_precision: int = 0, long_run: int = 0):
         """Mesh upload, initial relaxation, W warm-up and K timed events with
@@ -293,7 +296,7 @@ def run_ours(args, rank: int, world: int, dist):
         return next((k for k, (x, y) in enumerate(zip([r["node"] for r in a["records"]],
                                                       [r["node"] for r in b["records"]])) if x != y), None)
 
-    learner, learn_info = (None, None) if args.no_learned else train_learner()
+    learner, learn_info = (None, None) if args.no_learned else train_learner(args, rank, opts)
     plain = run_arm("plain", 0)
     plain["grid"].close()
     recycled = run_arm("recycled", 1)
@@ -535,7 +538,7 @@ def run_many_tips(args, rank: int, world: int, dist):
 
     from tapsim_modified_b200 import _native as N
     from tapsim_modified_b200.serving import estimated_atoms, partition_tips, run_tips, tip_specs
-    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, Mesh, solve_opts
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, Learner, Mesh, solve_opts
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -546,12 +549,21 @@ def run_many_tips(args, rank: int, world: int, dist):
     meshes = [Mesh.from_tip(**specs[k]) for k in mine]
     t_mesh = time.perf_counter() - t0
     opts = EvaporationOptions.from_ini(None)
-    sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4, preconditioner=PRECOND)
-    grids, evopts = [], []
+    # the learned warm start: one network trained once, a copy of it per tip
+    # (a learner's graph buffers serve one handle at a time)
+    trained, learn_info = (None, None) if args.no_learned else train_learner(args, rank, opts)
+    sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4,
+                       warm_start=0 if trained is None else 2, preconditioner=PRECOND)
+    grids, evopts, learners = [], [], []
     t0 = time.perf_counter()
     for m in meshes:
         g = Grid(m)
         g.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
+        if trained is not None:
+            lr = Learner(hops=6, max_cells=8192, ell_width=64, seed=7)
+            lr.set_params(trained.params())
+            lr.attach(g, predict=True)
+            learners.append(lr)
         ev = Evaporation(g, opts, relax_mode=1, solve=sopts)   # surface set and first selection
         grids.append(g)
         evopts.append(ev.opts)
@@ -572,6 +584,10 @@ def run_many_tips(args, rank: int, world: int, dist):
     cells = sum(m.num_nodes for m in meshes)
     for g in grids:
         g.close()
+    for lr in learners:
+        lr.close()
+    if trained is not None:
+        trained.close()
     stats = merge_tip_stats(dist, args.steps * len(mine), wall, lat)
     if rank != 0:
         return None
@@ -586,6 +602,9 @@ def run_many_tips(args, rank: int, world: int, dist):
                        "tips_rank0": len(mine), "cells_rank0": cells,
                        "partition": "greedy size-balanced (largest first) over the ranks, no data-path exchange",
                        "latency_ms": {"p50": stats["p50"], "p99": stats["p99"], "events": stats["latencies"]},
+                       "start": "learned warm start (warm_start 2), one trained network copied to every tip"
+                                if learn_info else "plain start",
+                       "learner": learn_info,
                        "setup_s": {"meshes_rank0": t_mesh, "upload_and_initial_relaxation_rank0": t_setup},
                        "wall_clock": "host clock around the K rounds, synchronised; max over ranks"},
             "clocks": clocks.summary()}
