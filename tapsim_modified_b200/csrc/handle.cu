@@ -1127,26 +1127,31 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     CK(cudaMemsetAsync(scal.p, 0, sizeof(double) * need, h->stream));
     launch_cg_init(m, rows, count, v, h->stream);
     // stop on the 2-norm of the residual (r.r at scal[3it+2]), the norm the
-    // outer FP64 test uses
-    double rr0 = 0.0;
-    CK(cudaMemcpyAsync(&rr0, scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    const double target = std::max(rr0 * rtol * rtol, absTarget2);
+    // outer FP64 test uses: r.r <= max(rtol^2 r.r_0, absTarget2), tested by
+    // the kernels themselves, so the iterations queue before r.r_0 is read
+    const double rel2 = rtol * rtol;
     int it = 0;
     // iterations queued before the first read: one more than the last solve
     // of this system took, then small batches
     int& last = which == 0 ? h->lastItersCgV : h->lastItersCgN;
     int batch = std::min(16, std::max(2, last + 1));
-    double sb[3 * 16];
-    while (it < maxIter && rr0 > target) {
+    double sb[3 * 16], s0[3];
+    while (it < maxIter) {
         const int start = it;
         const int end = std::min(maxIter, it + batch);
-        for (; it < end; it++) launch_cg_iter(m, rows, count, v, it, target, h->stream);
+        for (; it < end; it++) launch_cg_iter(m, rows, count, v, it, rel2, absTarget2, h->stream);
         // r.r after j iterations sits at scal[3j+2]; the kernels of later
         // iterations of the batch returned early once it met the target
+        CK(cudaMemcpyAsync(s0, scal.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaMemcpyAsync(sb, scal.p + 3 * (size_t)(start + 1), sizeof(double) * 3 * (end - start),
                            cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
+        const double target = std::max(s0[2] * rel2, absTarget2);
+        if (!(s0[2] > target)) {
+            // nothing to do: every queued iteration returned at once
+            it = 0;
+            break;
+        }
         bool done = false;
         for (int j = start + 1; j <= end && !done; j++)
             if (sb[3 * (j - start - 1) + 2] <= target) {

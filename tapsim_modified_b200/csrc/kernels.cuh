@@ -194,8 +194,9 @@ struct CGVectors {
     double* scal;  // [3*(max_iter+2)] accumulators: rz, pAp per iteration
 };
 void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s);
-// one CG iteration; all of it is skipped once scal[3it] (r.z) <= target
-void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double target,
+// one CG iteration; all of it is skipped once r.r (scal[3it+2]) <=
+// max(rel2 * r.r at the start (scal[2]), abs2)
+void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double rel2, double abs2,
                     cudaStream_t s);
 // the SpMV kernel of one CG iteration on its own (timing hook)
 void launch_cg_spmv_only(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s);

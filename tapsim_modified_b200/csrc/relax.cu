@@ -107,10 +107,20 @@ __global__ void k_cg_init(DevMesh m, const int32_t* __restrict__ rows, int count
     block_sum_atomic<kBlock>(rr, &v.scal[2]);
 }
 
+// The target of r.r: rel2 times its start value (scal[2]), and at least
+// abs2; an iteration whose r.r (scal[3it+2]) meets it is done (rel2 < 0:
+// never).  Formed on
+// the device, so that iterations queue before the host has read r.r.
+__device__ __forceinline__ bool cg_met(const double* scal, int it, double rel2, double abs2) {
+    if (rel2 < 0.0) return false;  // never (launch_cg_spmv_only)
+    return scal[3 * it + 2] <= fmax(rel2 * scal[2], abs2);
+}
+
 // ap = A p on the rows (A = diag - offdiag), pAp -> scal[3it+1]; all three
-// kernels of an iteration are skipped once r.r (scal[3it+2]) <= target
-__global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
-    if (v.scal[3 * it + 2] <= target) return;
+// kernels of an iteration are skipped once it is done (cg_met)
+__global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double rel2,
+                          double abs2) {
+    if (cg_met(v.scal, it, rel2, abs2)) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double pap = 0.0;
     if (t < count) {
@@ -127,9 +137,10 @@ __global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count
 }
 
 // x += a p, r -= a ap, z = r/diag, rz_next -> scal[3(it+1)], r.r -> scal[3(it+1)+2]
-__global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
+__global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double rel2,
+                            double abs2) {
     const double rz = v.scal[3 * it];
-    if (v.scal[3 * it + 2] <= target) return;
+    if (cg_met(v.scal, it, rel2, abs2)) return;
     const double pap = v.scal[3 * it + 1];
     const float alpha = pap > 0.0 ? (float)(rz / pap) : 0.0f;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -149,9 +160,10 @@ __global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int cou
 }
 
 // p = z + beta p
-__global__ void k_cg_pupdate(const int32_t* __restrict__ rows, int count, CGVectors v, int it, double target) {
+__global__ void k_cg_pupdate(const int32_t* __restrict__ rows, int count, CGVectors v, int it, double rel2,
+                             double abs2) {
     const double rz = v.scal[3 * it];
-    if (v.scal[3 * it + 2] <= target) return;
+    if (cg_met(v.scal, it, rel2, abs2)) return;
     const double rzn = v.scal[3 * (it + 1)];
     const float beta = (float)(rzn / rz);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -296,15 +308,15 @@ void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc,
 void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
     if (count > 0) { count_launch(); k_cg_init<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v); }
 }
-void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double target,
+void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double rel2, double abs2,
                     cudaStream_t s) {
     if (count <= 0) return;
-    { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target); }
-    { count_launch(); k_cg_update<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, target); }
-    { count_launch(); k_cg_pupdate<<<blocks(count), kBlock, 0, s>>>(rows, count, v, it, target); }
+    { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, rel2, abs2); }
+    { count_launch(); k_cg_update<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, rel2, abs2); }
+    { count_launch(); k_cg_pupdate<<<blocks(count), kBlock, 0, s>>>(rows, count, v, it, rel2, abs2); }
 }
 void launch_cg_spmv_only(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
-    if (count > 0) { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, 0, -1.0); }
+    if (count > 0) { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, 0, -1.0, -1.0); }
 }
 void launch_add_coupled(const DevMesh& m, const int32_t* rows, int count, const float* xV, float* r, cudaStream_t s) {
     if (count > 0) { count_launch(); k_add_coupled<<<blocks(count), kBlock, 0, s>>>(m, rows, count, xV, r); }
