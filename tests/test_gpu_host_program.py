@@ -43,7 +43,8 @@ def test_host_program_matches_python_host(golden_dump, ref_mesh, ref_events, tmp
         assert int(row[0]) == rec["index"] == k + 1
         assert int(row[1]) == rec["id"]
         assert int(row[2]) == rec["number"] == int(numbers[int(ref_events[k, 1])])
-        assert np.allclose(row[4:7], xyz[rec["node"]], rtol=0, atol=0)
+        # the ASCII results file holds about seven significant digits
+        assert np.allclose(row[4:7], xyz[rec["node"]], rtol=1e-6, atol=1e-20)
         # the two hosts run separate solves to 1e-8 on the same device: the
         # float record fields agree to the solve's accuracy
         py = np.array([rec["voltage"], *rec["stop"], rec["tof"], rec["probability"], rec["potentialBefore"],
