@@ -160,9 +160,11 @@ int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);
 /* The schedule of one level of the multigrid hierarchy (no counterpart in
  * the reference): its rows, and the lanes per CSR row of its operator
  * (levels smoothed with CSR rows) and of its restriction (every level but
- * the coarsest), 0 where the level has none.  The hierarchy build times
- * each lane-group size (2..32) on the level's own matrices and keeps the
- * fastest; a_ms / r_ms are the kept launches' times [ms]. */
+ * the coarsest), 0 where the level has none; for level 0, a_lanes is the
+ * number of coupling loads each lane of the SELL-32 smoothing pass issues
+ * ahead of their gathers (4, 8 or 16).  The hierarchy build times each
+ * candidate on the level's own matrices and keeps the fastest; a_ms / r_ms
+ * are the kept launches' times [ms]. */
 int tg_amg_schedule(tg_handle* h, int32_t level, int32_t* rows, int32_t* a_lanes, int32_t* r_lanes, float* a_ms,
                     float* r_ms);
 /* ||r||_2 / ||b||_2 of the current potentials (FP64). */

@@ -45,6 +45,9 @@ __global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, co
 // all, so it is spectrally within a fraction of a percent of it; the
 // smoothing steps divide by the FP32 diagonal d on both sides of the cycle,
 // which keeps the preconditioner symmetric.
+// U: the column/value loads a lane issues ahead of their gathers (the bytes
+// a warp keeps in flight), chosen per hierarchy by timed trials.
+template <int U>
 __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, float* out, int mode,
                            const double* scal, int it, double target) {
     if (done(scal, it, target)) return;
@@ -58,16 +61,16 @@ __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, f
         const __nv_bfloat16* __restrict__ val = v.val16 + base + lane;
         float acc = 0.0f, sum = 0.0f;
         int k = 0;
-        for (; k + 8 <= width; k += 8) {
-            int c[8];
-            float a[8];
+        for (; k + U <= width; k += U) {
+            int c[U];
+            float a[U];
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
+            for (int j = 0; j < U; j++) {
                 c[j] = __ldcs(col + 32 * (k + j));
                 a[j] = __bfloat162float(__ldcs(val + 32 * (k + j)));
             }
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
+            for (int j = 0; j < U; j++) {
                 acc += a[j] * __ldg(y + c[j]);
                 sum += a[j];
             }
@@ -171,6 +174,16 @@ __global__ void k_amg_dense(int n, const float* inv, const float* b, float* x, c
 // loop then makes one pass)
 inline unsigned grid_full(long long threads) { return (unsigned)((threads + kBlock - 1) / kBlock); }
 
+// the level-0 pass with the hierarchy's load depth (AmgDev::fine_unroll)
+void launch_fine(int U, const VSys& v, int slices, const float* b, const float* y, float* out, int mode,
+                 const double* scal, int it, double target, cudaStream_t s) {
+    count_launch();
+    const unsigned grid = grid_full((long long)slices * 32);
+    if (U == 4) k_amg_fine<4><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, scal, it, target);
+    else if (U == 16) k_amg_fine<16><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, scal, it, target);
+    else k_amg_fine<8><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, scal, it, target);
+}
+
 // a group of L threads for every row
 inline unsigned grid_rows(int n, int L) { return (unsigned)(((long long)n * L + kBlock - 1) / kBlock); }
 
@@ -225,7 +238,7 @@ float time_launches(F f, int trials, cudaStream_t s, cudaEvent_t e0, cudaEvent_t
 
 }  // namespace
 
-int amg_tune_lanes(AmgDev& g, cudaStream_t s, float* aMs, float* rMs) {
+int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* aMs, float* rMs, float* fineMs) {
     static const int kCand[5] = {2, 4, 8, 16, 32};
     constexpr int kTrials = 5;
     cudaEvent_t e0, e1;
@@ -235,6 +248,20 @@ int amg_tune_lanes(AmgDev& g, cudaStream_t s, float* aMs, float* rMs) {
         return -1;
     }
     const double* noScal = nullptr;  // target < 0: the kernels never read it
+    // the level-0 smoothing pass: loads in flight per lane
+    {
+        const int slices = (slots + 31) / 32;
+        float best = 1e30f;
+        for (int U : {4, 8, 16}) {
+            const float ms = time_launches(
+                [&] { launch_fine(U, v, slices, v.r, g.y0, g.t0, 0, noScal, 0, -1.0, s); }, kTrials, s, e0, e1);
+            if (ms < best) {
+                best = ms;
+                g.fine_unroll = U;
+            }
+        }
+        if (fineMs) *fineMs = best;
+    }
     for (int l = 0; l + 1 < g.levels; l++) {
         AmgDevLevel& L = g.lev[l];
         AmgDevLevel& C = g.lev[l + 1];
@@ -273,8 +300,7 @@ int amg_tune_lanes(AmgDev& g, cudaStream_t s, float* aMs, float* rMs) {
 
 void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s) {
     const int slices = (slots + 31) / 32;
-    count_launch();
-    k_amg_fine<<<grid_full((long long)slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, g.t0, 0, v.scal, 0, -1.0);
+    launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, v.scal, 0, -1.0, s);
 }
 
 void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s) {
@@ -284,9 +310,7 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
     count_launch();
     k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.r, v.d, g.y0, scal, it, target);
     if (g.levels > 1) {
-        count_launch();
-        k_amg_fine<<<grid_full(slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, g.t0, 0, scal, it,
-                                                                         target);
+        launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, scal, it, target, s);
         // down: restrict, smooth, residual
         for (int l = 0; l + 1 < g.levels; l++) {
             const AmgDevLevel& L = g.lev[l];
@@ -311,18 +335,14 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
             count_launch();
             k_amg_prolong<<<grid_for(L.n), kBlock, 0, s>>>(L.n, L.p_ptr, L.p_col, L.p_val, C.x, y, scal, it, target);
             if (l == 0) {
-                count_launch();
-                k_amg_fine<<<grid_full(slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, v.u, 1, scal, it,
-                                                                                 target);
+                launch_fine(g.fine_unroll, v, slices, v.r, g.y0, v.u, 1, scal, it, target, s);
             } else {
                 launch_csr(L.a_lanes, L.n, L.a_ptr, L.a_col, L.a_val, L.diag, L.b, L.y, L.x, 1, scal, it, target, s);
             }
         }
     } else {
         // a single level: Jacobi twice (y, then the post-smoothing step)
-        count_launch();
-        k_amg_fine<<<grid_full(slices * 32), kBlock, 0, s>>>(v, slices, v.r, g.y0, v.u, 1, scal, it,
-                                                                         target);
+        launch_fine(g.fine_unroll, v, slices, v.r, g.y0, v.u, 1, scal, it, target, s);
     }
 }
 

@@ -150,6 +150,7 @@ struct tg_handle {
     // timings [ms] of the tuned lane groups of each level's operator and
     // restriction (amg_tune_lanes), 0 where a level has none
     float amgTunedA[tgd::kAmgMaxLevels] = {}, amgTunedR[tgd::kAmgMaxLevels] = {};
+    float amgTunedFine = 0.0f;  // and of the level-0 pass
     // FP64 inner iterations: couplings at the SELL positions and the vectors
     // d64, x64, r64, p64, s64, w64 (each capacity+1), allocated at the first
     // solve with inner_precision 1
@@ -1283,7 +1284,8 @@ static int amg_setup_impl(tg_handle* h, double* seconds) {
     }
     // the coarse levels' lane groups from timed trials on this hierarchy
     for (int l = 0; l < tgd::kAmgMaxLevels; l++) h->amgTunedA[l] = h->amgTunedR[l] = 0.0f;
-    if (amg_tune_lanes(g, h->stream, h->amgTunedA, h->amgTunedR) != 0) {
+    g.fine_unroll = 8;
+    if (amg_tune_lanes(g, h->vs(), slots, h->stream, h->amgTunedA, h->amgTunedR, &h->amgTunedFine) != 0) {
         h->amg_release();
         return cuda_check(h, cudaGetLastError(), "multigrid schedule tuning");
     }
@@ -1556,9 +1558,10 @@ int tg_amg_schedule(tg_handle* h, int32_t level, int32_t* rows, int32_t* a_lanes
     if (rows) *rows = level == 0 ? h->amgSlots : L.n;
     const bool csr = level >= 1 && level + 1 < h->amg.levels;
     const bool restr = level + 1 < h->amg.levels;
-    if (a_lanes) *a_lanes = csr ? L.a_lanes : 0;
+    // level 0: the loads per lane of its smoothing pass in place of lanes
+    if (a_lanes) *a_lanes = csr ? L.a_lanes : (level == 0 ? h->amg.fine_unroll : 0);
     if (r_lanes) *r_lanes = restr ? L.r_lanes : 0;
-    if (a_ms) *a_ms = csr ? h->amgTunedA[level] : 0.0f;
+    if (a_ms) *a_ms = csr ? h->amgTunedA[level] : (level == 0 ? h->amgTunedFine : 0.0f);
     if (r_ms) *r_ms = restr ? h->amgTunedR[level] : 0.0f;
     return TG_OK;
 }

@@ -44,8 +44,9 @@ def test_multigrid_events_follow_reference(ref_mesh, ref_events):
 
 def test_tuned_schedules_of_the_hierarchy():
     """The hierarchy build times every lane-group size of each coarse
-    operator and restriction on the device and keeps the fastest
-    (amg_tune_lanes): every level but the coarsest reports a restriction
+    operator and restriction, and the load depth of the level-0 pass, on the
+    device and keeps the fastest (amg_tune_lanes): every level but the
+    coarsest reports a restriction
     schedule, every level smoothed with CSR rows an operator schedule, each a
     power of two in 2..32 with a positive launch time; the solve converges
     with them.  On the config-1 tip (307k cells) the hierarchy has at least
@@ -65,7 +66,9 @@ def test_tuned_schedules_of_the_hierarchy():
     for k, lv in enumerate(sched):
         last = k == len(sched) - 1
         assert (lv["r_lanes"] in (2, 4, 8, 16, 32) and lv["r_ms"] > 0) if not last else lv["r_lanes"] == 0
-        if 1 <= k < len(sched) - 1:
+        if k == 0:
+            assert lv["a_lanes"] in (4, 8, 16) and lv["a_ms"] > 0   # the level-0 pass's load depth
+        elif k < len(sched) - 1:
             assert lv["a_lanes"] in (2, 4, 8, 16, 32) and lv["a_ms"] > 0
         else:
             assert lv["a_lanes"] == 0
