@@ -191,7 +191,7 @@ def train_learner(args, rank: int, opts):
     tmesh = Mesh.from_tip(seed=101 + rank, **TIPS["train"])
     tgrid = Grid(tmesh)
     tgrid.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
-    learner = Learner(hops=6, max_cells=8192, ell_width=64, seed=7 + rank)
+    learner = Learner(hops=6, max_cells=2048, ell_width=64, seed=7 + rank)
     learner.attach(tgrid, collect=True)
     tev = Evaporation(tgrid, opts, relax_mode=1,
                       solve=solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, preconditioner=PRECOND))
@@ -560,7 +560,7 @@ def run_many_tips(args, rank: int, world: int, dist):
         g = Grid(m)
         g.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
         if trained is not None:
-            lr = Learner(hops=6, max_cells=8192, ell_width=64, seed=7)
+            lr = Learner(hops=6, max_cells=2048, ell_width=64, seed=7)
             lr.set_params(trained.params())
             lr.attach(g, predict=True)
             learners.append(lr)

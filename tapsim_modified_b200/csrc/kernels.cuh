@@ -299,11 +299,14 @@ void launch_ball_reset(const int32_t* nodes, const int32_t* count, int32_t* loca
 void launch_ball_features(const DevMesh& m, int site, int hops, int D, const int32_t* nodes, const int8_t* level,
                           const int32_t* count, const int32_t* localOf, float* scale, float* X, int32_t* ellCol,
                           float* ellW, double* phiStart, int cap, cudaStream_t s);
-void launch_input_bf16(const float* X, int n, int npad, void* Z, void* ZT, cudaStream_t s);
+// nDev (may be null): a device-side row count that caps n
+void launch_input_bf16(const float* X, int n, int npad, void* Z, void* ZT, cudaStream_t s,
+                       const int32_t* nDev = nullptr);
 void launch_bias_act(const float* C, const float* b, const float* hPrev, float* u, float* h, int npad, cudaStream_t s);
 void launch_message_concat(const float* h, const int32_t* ellCol, const float* ellW, int D, int n, int npad, void* Z,
-                           void* ZT, cudaStream_t s);
-void launch_readout(const float* h, const float* w, const float* b, int n, float* y, cudaStream_t s);
+                           void* ZT, cudaStream_t s, const int32_t* nDev = nullptr);
+void launch_readout(const float* h, const float* w, const float* b, int n, float* y, cudaStream_t s,
+                    const int32_t* nDev = nullptr);
 void launch_loss(const float* y, const float* tgt, int n, float invCount, float* dy, float* loss, cudaStream_t s);
 void launch_readout_back(const float* h, const float* dy, const float* w, int n, int npad, float* gw, float* gb,
                          float* dh, cudaStream_t s);

@@ -175,21 +175,24 @@ int gemm(tg_learner* L, const void* A, const void* B, float* C, int M, int N, in
     return TG_OK;
 }
 
-// Forward pass over n rows (features X, ELL col/w); the readout lands in L->y
-int forward(tg_learner* L, const float* X, const int32_t* col, const float* w, int n) {
+// Forward pass over n rows (features X, ELL col/w); the readout lands in L->y.
+// nDev (may be null): the row count on the device, at most n; the rows
+// beyond it enter the GEMMs as zeros, so that n (the graph's capacity) sizes
+// the launches without the host reading the count.
+int forward(tg_learner* L, const float* X, const int32_t* col, const float* w, int n, const int32_t* nDev = nullptr) {
     const int npad = roundup128(std::max(n, 1));
     int rc = ensure_rows(L, npad);
     if (rc != TG_OK) return rc;
     cudaStream_t s = L->stream;
-    launch_input_bf16(X, n, npad, L->Zl(0), L->ZTl(0), s);
+    launch_input_bf16(X, n, npad, L->Zl(0), L->ZTl(0), s, nDev);
     if ((rc = gemm(L, L->Zl(0), L->WTbl(0), L->C.p, npad, kHid, kCat)) != TG_OK) return rc;
     launch_bias_act(L->C.p, L->bl(0), nullptr, L->Ul(0), L->Hl(0), npad, s);
     for (int l = 1; l < kLayers; l++) {
-        launch_message_concat(L->Hl(l - 1), col, w, L->D, n, npad, L->Zl(l), L->ZTl(l), s);
+        launch_message_concat(L->Hl(l - 1), col, w, L->D, n, npad, L->Zl(l), L->ZTl(l), s, nDev);
         if ((rc = gemm(L, L->Zl(l), L->WTbl(l), L->C.p, npad, kHid, kCat)) != TG_OK) return rc;
         launch_bias_act(L->C.p, L->bl(l), L->Hl(l - 1), L->Ul(l), L->Hl(l), npad, s);
     }
-    launch_readout(L->Hl(kLayers - 1), L->wout(), L->bout(), n, L->y.p, s);
+    launch_readout(L->Hl(kLayers - 1), L->wout(), L->bout(), n, L->y.p, s, nDev);
     LCK(cudaGetLastError());
     return TG_OK;
 }
@@ -246,13 +249,16 @@ int stage_batch(tg_learner* L, const std::vector<int>& idx, int* rowsOut) {
     return TG_OK;
 }
 
-// Builds the graph of `site` from the current state on stream s; returns its size
+// Builds the graph of `site` from the current state on stream s; with nOut
+// its size is read back (a synchronisation), otherwise it stays on the
+// device (L->count)
 int build_graph(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, int* nOut) {
     if ((size_t)m.n != L->meshNodes) return lfail(L, TG_ERR_ARGUMENT, "learner: attached to another mesh");
     launch_ball_bfs(m, site, L->hops, L->cap, L->nodes.p, L->level.p, L->count.p, L->localOf.p, s);
     launch_ball_features(m, site, L->hops, L->D, L->nodes.p, L->level.p, L->count.p, L->localOf.p, L->scale.p, L->X.p,
                          L->ellCol.p, L->ellW.p, L->collecting ? L->phiStart.p : nullptr, L->cap, s);
     launch_ball_reset(L->nodes.p, L->count.p, L->localOf.p, L->cap, s);
+    if (!nOut) return TG_OK;
     int n = 0;
     LCK(cudaMemcpyAsync(&n, L->count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     LCK(cudaStreamSynchronize(s));
@@ -287,8 +293,10 @@ int learner_predict(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, b
     const cudaStream_t own = L->stream;
     L->stream = s;
     L->collecting = collect;
+    // the graph's size is read back only to store a sample; a prediction
+    // alone runs over the graph's capacity with the size on the device
     int n = 0;
-    int rc = build_graph(L, m, site, s, &n);
+    int rc = build_graph(L, m, site, s, collect ? &n : nullptr);
     if (rc == TG_OK && collect) {
         // the sample's features are the state before any prediction; the
         // stream is idle here (build_graph synchronised it)
@@ -303,7 +311,8 @@ int learner_predict(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, b
         }
     }
     if (rc == TG_OK && predict) {
-        rc = forward(L, L->X.p, L->ellCol.p, L->ellW.p, n);
+        rc = collect ? forward(L, L->X.p, L->ellCol.p, L->ellW.p, n)
+                     : forward(L, L->X.p, L->ellCol.p, L->ellW.p, L->cap, L->count.p);
         if (rc == TG_OK)
             launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, nullptr, nullptr, L->cap,
                                     s);

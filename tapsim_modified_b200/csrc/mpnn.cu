@@ -297,9 +297,12 @@ __global__ void k_ball_features(DevMesh m, int site, int hops, int D, const int3
 
 // BF16 input block: features in columns 0..15, zeros to 128; also the
 // transposed copy (column-major) for the weight gradient
-__global__ void k_input_bf16(const float* X, int n, int npad, __nv_bfloat16* Z, __nv_bfloat16* ZT) {
+// nDev (may be null): the graph's row count on the device, which caps n
+__global__ void k_input_bf16(const float* X, int n, const int32_t* nDev, int npad, __nv_bfloat16* Z,
+                             __nv_bfloat16* ZT) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= npad * kCat) return;
+    if (nDev && *nDev < n) n = *nDev;
     const int i = t / kCat, f = t % kCat;
     const float v = (i < n && f < kFeat) ? X[(size_t)i * kFeat + f] : 0.0f;
     const __nv_bfloat16 b = __float2bfloat16_rn(v);
@@ -317,10 +320,11 @@ __global__ void k_bias_act(const float* C, const float* b, const float* hPrev, f
 }
 
 // z = [h, A h] in BF16 (row-major and transposed)
-__global__ void k_message_concat(const float* h, const int32_t* ellCol, const float* ellW, int D, int n, int npad,
-                                 __nv_bfloat16* Z, __nv_bfloat16* ZT) {
+__global__ void k_message_concat(const float* h, const int32_t* ellCol, const float* ellW, int D, int n,
+                                 const int32_t* nDev, int npad, __nv_bfloat16* Z, __nv_bfloat16* ZT) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= npad * kHid) return;
+    if (nDev && *nDev < n) n = *nDev;
     const int i = t / kHid, f = t % kHid;
     float hv = 0.0f, mv = 0.0f;
     if (i < n) {
@@ -338,8 +342,9 @@ __global__ void k_message_concat(const float* h, const int32_t* ellCol, const fl
     ZT[(size_t)(kHid + f) * npad + i] = mbv;
 }
 
-__global__ void k_readout(const float* h, const float* w, const float* b, int n, float* y) {
+__global__ void k_readout(const float* h, const float* w, const float* b, int n, const int32_t* nDev, float* y) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (nDev && *nDev < n) n = *nDev;
     if (i >= n) return;
     float s = b[0];
     for (int f = 0; f < kHid; f++) s += h[(size_t)i * kHid + f] * w[f];
@@ -502,9 +507,9 @@ void launch_ball_features(const DevMesh& m, int site, int hops, int D, const int
     k_ball_features<<<nblk(cap), 256, 0, s>>>(m, site, hops, D, nodes, level, count, localOf, scale, X, ellCol, ellW,
                                                phiStart);
 }
-void launch_input_bf16(const float* X, int n, int npad, void* Z, void* ZT, cudaStream_t s) {
+void launch_input_bf16(const float* X, int n, int npad, void* Z, void* ZT, cudaStream_t s, const int32_t* nDev) {
     count_launch();
-    k_input_bf16<<<nblk((long long)npad * kCat), 256, 0, s>>>(X, n, npad, static_cast<__nv_bfloat16*>(Z),
+    k_input_bf16<<<nblk((long long)npad * kCat), 256, 0, s>>>(X, n, nDev, npad, static_cast<__nv_bfloat16*>(Z),
                                                                 static_cast<__nv_bfloat16*>(ZT));
 }
 void launch_bias_act(const float* C, const float* b, const float* hPrev, float* u, float* h, int npad,
@@ -513,15 +518,16 @@ void launch_bias_act(const float* C, const float* b, const float* hPrev, float* 
     k_bias_act<<<nblk((long long)npad * kHid), 256, 0, s>>>(C, b, hPrev, u, h, npad);
 }
 void launch_message_concat(const float* h, const int32_t* ellCol, const float* ellW, int D, int n, int npad, void* Z,
-                           void* ZT, cudaStream_t s) {
+                           void* ZT, cudaStream_t s, const int32_t* nDev) {
     count_launch();
-    k_message_concat<<<nblk((long long)npad * kHid), 256, 0, s>>>(h, ellCol, ellW, D, n, npad,
+    k_message_concat<<<nblk((long long)npad * kHid), 256, 0, s>>>(h, ellCol, ellW, D, n, nDev, npad,
                                                                     static_cast<__nv_bfloat16*>(Z),
                                                                     static_cast<__nv_bfloat16*>(ZT));
 }
-void launch_readout(const float* h, const float* w, const float* b, int n, float* y, cudaStream_t s) {
+void launch_readout(const float* h, const float* w, const float* b, int n, float* y, cudaStream_t s,
+                    const int32_t* nDev) {
     count_launch();
-    k_readout<<<nblk(n), 256, 0, s>>>(h, w, b, n, y);
+    k_readout<<<nblk(n), 256, 0, s>>>(h, w, b, n, nDev, y);
 }
 void launch_loss(const float* y, const float* tgt, int n, float invCount, float* dy, float* loss, cudaStream_t s) {
     count_launch();
