@@ -124,10 +124,11 @@ typedef struct {
      *   1  plus the previous event's correction on the non-Neumann free
      *      cells (the smooth far field of one removal changes little
      *      from one site to the next),
-     *   2  0, plus the prediction of an attached learner on the free cells
-     *      around the removed atom (tg_learner_attach, mode bit 1); the
-     *      first residual is then updated in FP64 on those cells' rows and
-     *      their neighbours' instead of a pass over every row.
+     *   2  as 1, plus the prediction of an attached learner on the free
+     *      cells around the removed atom (tg_learner_attach, mode bit 1),
+     *      which also joins the recorded correction; the first residual is
+     *      updated in FP64 on those cells' rows and their neighbours'
+     *      instead of a pass over every row.
      * The solve always ends at rel_tol, whatever the start. */
     int32_t warm_start;
     /* Preconditioner of the inner iterations on the non-Neumann free cells:
@@ -412,12 +413,14 @@ int tg_run_tips(tg_handle* const* handles, int32_t count, const tg_event_opts* o
 /* ---- learned near-field warm start (no counterpart in the reference) -----
  * A message-passing network (an input layer and four message layers of
  * width 64, BF16 tensor-core GEMMs with FP32 accumulation) on the free cells
- * within `hops` steps of a removed atom predicts the event's correction on
- * those cells.  Samples are (features of the state right after the removal,
- * converged correction) pairs that tg_solve collects while a learner is
- * attached in collect mode; the network is trained on them on the device;
- * tg_solve with warm_start 2 adds its prediction before the inner
- * iterations.  The solve still ends at rel_tol. */
+ * within `hops` steps of a removed atom predicts the part of the event's
+ * correction on those cells that the start leaves (the recycled far field
+ * of warm_start 1, or the plain start).  Samples are (features of the state
+ * the solve starts from, converged correction) pairs that tg_solve collects
+ * while a learner is attached in collect mode; the network is trained on
+ * them on the device; tg_solve with warm_start 2 adds its prediction on top
+ * of the recycled far field before the inner iterations.  The solve still
+ * ends at rel_tol. */
 typedef struct tg_learner tg_learner;
 int tg_learner_create(int32_t hops, int32_t max_cells, int32_t ell_width, uint64_t seed, tg_learner** out);
 void tg_learner_destroy(tg_learner* L);

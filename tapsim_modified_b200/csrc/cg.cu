@@ -197,6 +197,16 @@ __global__ void k_vcg_warm_residual(VSys v, int slices, double* acc) {
     block_sum_atomic<kBlock>(r2, acc);
 }
 
+// sum of r^2 over the V slots into *acc
+__global__ void k_vcg_rnorm(VSys v, int slots, double* acc) {
+    double r2 = 0.0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
+        const double r = v.r[s];
+        r2 += r * r;
+    }
+    block_sum_atomic<kBlock>(r2, acc);
+}
+
 // r of the Neumann rows += sum over V neighbours ceff_ij x_j
 // (x from the FP64 vector when x64 is given)
 __global__ void k_vcg_couple_neumann(DevMesh m, VSys v, const int32_t* rows, int count, float* rN,
@@ -564,6 +574,9 @@ void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, c
 }
 void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s) {
     if (slots > 0) { count_launch(); k_vcg_warm<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, alpha); }
+}
+void launch_vcg_rnorm(const VSys& v, int slots, double* acc, cudaStream_t s) {
+    if (slots > 0) { count_launch(); k_vcg_rnorm<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, acc); }
 }
 void launch_vcg_warm_residual(const VSys& v, int slots, double* acc, cudaStream_t s) {
     const int slices = (slots + 31) / 32;

@@ -1395,14 +1395,14 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     // a solve right after removals from a converged state records its
     // correction; with warm_start it starts from the previous one
     const bool fromEvent = h->converged && h->removalsSinceSolve > 0;
-    const bool warm = fromEvent && h->histValid && o->warm_start == 1;
+    const bool warm = fromEvent && h->histValid && (o->warm_start == 1 || o->warm_start == 2);
     const bool learnPredict = fromEvent && h->learner && (h->learnMode & 2) && o->warm_start == 2 && h->lastSite >= 0;
     // the first residual after removals from a converged state: the rows the
     // removals touched, from the kept residuals of the potentials as they
     // are; a recycled start then takes A hist off the V rows (FP32) and the
-    // Neumann rows are recomputed.  The learned start changes the
+    // Neumann rows are recomputed.  The learned start then changes the
     // potentials of its graph's cells: their rows and their neighbours' are
-    // recomputed too (FP64), after the prediction.
+    // recomputed in FP64 after the prediction, and the sums formed again.
     const bool incremental = h->residValid && fromEvent && !h->pendingOverflow && h->nPending > 0;
     const int nPending = h->nPending;
     h->residValid = h->pendingOverflow = false;
@@ -1422,10 +1422,19 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     }
     if (warm) launch_vcg_warm(m, vsys, h->vActive, 1.0f, h->stream);
     else if (fromEvent) CK(cudaMemsetAsync(vsys.hist, 0, sizeof(float) * ((size_t)h->vCapacity + 1), h->stream));
-    // learned near field on the plain start; sample collection
+    // learned near field on top of the recycled far field (or the plain start
+    // while there is no history); sample collection.  With a recycled start,
+    // its FP32 first residual (r -= A hist) is taken before the prediction,
+    // so that the predicted cells' rows can then be recomputed in FP64.
     const bool learnCollect = fromEvent && h->learner && (h->learnMode & 1) && h->lastSite >= 0;
+    const bool warmFirst = learnPredict && incremental && warm;
+    if (warmFirst) {
+        CK(cudaMemsetAsync(h->rsum.p, 0, 2 * sizeof(double), h->stream));
+        launch_vcg_warm_residual(vsys, h->vActive, h->rsum.p, h->stream);
+    }
     if (learnPredict || learnCollect) {
-        rc = learner_predict(h->learner, m, h->lastSite, h->stream, learnCollect, learnPredict);
+        rc = learner_predict(h->learner, m, h->lastSite, h->stream, learnCollect, learnPredict, vsys.slot_of,
+                             fromEvent ? vsys.hist : nullptr);
         if (rc != TG_OK) return fail(h, rc, std::string("tg_solve: ") + tg_learner_last_error(h->learner));
         if (learnPredict && incremental) {
             // the predicted cells' rows and their neighbours' from the new
@@ -1440,6 +1449,13 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
             }
             launch_residual_rows(m, vsys, vN.r, cells, cap, h->resStamp.p, h->resEpoch, rv, bv, h->rsum.p, h->stream,
                                  cellCount);
+            if (warmFirst) {
+                // the V rows' sum of squares from their FP32 residuals as
+                // they now are, and the Neumann rows in full
+                CK(cudaMemsetAsync(h->rsum.p, 0, 2 * sizeof(double), h->stream));
+                launch_vcg_rnorm(vsys, h->vActive, h->rsum.p, h->stream);
+                launch_residual(m, h->allN.p, h->countAllN, vN.r, h->rsum.p + 1, h->stream, nullptr, rv, nullptr);
+            }
         }
     }
     h->converged = h->histValid = false;
@@ -1472,7 +1488,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
     }
     for (int outer = 0;; outer++) {
         if (outer == 0 && incremental) {
-            if (warm) {
+            if (warm && !warmFirst) {
                 CK(cudaMemsetAsync(h->rsum.p, 0, 2 * sizeof(double), h->stream));
                 launch_vcg_warm_residual(vsys, h->vActive, h->rsum.p, h->stream);
                 launch_residual(m, h->allN.p, h->countAllN, vN.r, h->rsum.p + 1, h->stream, nullptr, rv, nullptr);

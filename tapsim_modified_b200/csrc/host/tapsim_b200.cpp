@@ -14,7 +14,8 @@
 // --voltage-queue-size=?, --vacuum-identifier=?, --no-chunks, --chunk-size=?.
 // Options of this build: --relax-mode=solve|reference (solve: every event
 // relaxed to --rel-tol, 1e-8; reference: the ini's local/global/refresh
-// sweeps), --warm-start=0|1, --batch=? (events per library call).
+// sweeps), --warm-start=0|1, --batch=? (events per library call),
+// --records=? (every event's record as the library returned it, raw).
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -60,6 +61,7 @@ struct Args {
     double relTol = 1e-8;
     int warmStart = 0;
     int batch = 64;
+    std::string records;      // --records: every event's tg_event_record, raw, in order
 };
 
 [[noreturn]] void die(const std::string& msg) {
@@ -102,6 +104,7 @@ Args parse(int argc, char** argv) {
         } else if (opt(s, "rel-tol", &v)) a.relTol = std::atof(v.c_str());
         else if (opt(s, "warm-start", &v)) a.warmStart = std::atoi(v.c_str());
         else if (opt(s, "batch", &v)) a.batch = std::max(1, std::atoi(v.c_str()));
+        else if (opt(s, "records", &v)) a.records = v;
         else if (s.compare(0, 2, "--") == 0) die("unknown or invalid argument in command line: \"" + s + "\"");
         else pos.push_back(s);
     }
@@ -240,6 +243,8 @@ int main(int argc, char** argv) {
     float voltageQueueSum = 0.0f;
     std::vector<tg_result_row> rows;
     std::vector<tg_event_record> recs((size_t)a.batch);
+    FILE* rawOut = a.records.empty() ? nullptr : std::fopen(a.records.c_str(), "wb");
+    if (!a.records.empty() && !rawOut) die("cannot write " + a.records);
     long events = 0;
     for (;;) {
         long want = a.batch;
@@ -248,6 +253,7 @@ int main(int argc, char** argv) {
         int32_t done = 0;
         rc = tg_run_events(h, &o, (int32_t)(events + 1), (int32_t)want, recs.data(), &done);
         if (rc != TG_OK && rc != TG_ERR_NO_SURFACE) check(rc, h, "tg_run_events");
+        if (rawOut && done > 0) std::fwrite(recs.data(), sizeof(tg_event_record), (size_t)done, rawOut);
         for (int k = 0; k < done; k++) {
             const tg_event_record& r = recs[k];
             const tg_type& t = types.at(r.type_id);
@@ -296,6 +302,7 @@ int main(int argc, char** argv) {
         events += done;
         if (done < want) break;  // the surface ran out
     }
+    if (rawOut) std::fclose(rawOut);
     std::printf("events %ld\n", events);
     if (a.fileOutput) {
         const std::string path = a.results.empty() ? ini.at("RESULTS_FILENAME") : a.results;

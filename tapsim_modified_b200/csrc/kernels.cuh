@@ -155,6 +155,8 @@ void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, c
 // warm start: hist *= alpha, phi64 += hist on the V rows
 void launch_vcg_warm(const DevMesh& m, const VSys& v, int slots, float alpha, cudaStream_t s);
 // r -= A hist on the V system (FP32), sum r^2 into *acc
+// sum of r^2 over the V slots into *acc (the FP32 right-hand side as it is)
+void launch_vcg_rnorm(const VSys& v, int slots, double* acc, cudaStream_t s);
 void launch_vcg_warm_residual(const VSys& v, int slots, double* acc, cudaStream_t s);
 void launch_vcg_couple_neumann(const DevMesh& m, const VSys& v, const int32_t* rows, int count, float* rN,
                                cudaStream_t s, bool fromX64 = false);

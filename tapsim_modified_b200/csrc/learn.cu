@@ -2,10 +2,10 @@
 // samples the solver collects, and its inference inside tg_solve.
 //
 // A sample is one removal: the graph of free cells within `hops` steps of
-// the removed cell, 16 features per cell taken from the state right after
-// the removal (the plain start), and the target (phi_final - phi_start) /
-// sigma on the same cells, where phi_final is the potential the solve
-// converged to.  Training minimises the mean squared error over the cells of a batch
+// the removed cell, 16 features per cell taken from the state the solve
+// starts from (after the removal and, with a recycled start, the previous
+// event's correction), and the target (phi_final - phi_start) / sigma on the
+// same cells, where phi_final is the potential the solve converged to.  Training minimises the mean squared error over the cells of a batch
 // of samples with Adam; forward and backward GEMMs run on the tensor cores
 // (mpnn.cu).  Inference adds sigma * y to the potentials (and to the
 // recorded correction) before the CG starts; the solve still ends at its
@@ -289,7 +289,8 @@ void learner_graph_cells(const tg_learner* L, const int32_t** nodes, const int32
     *capacity = L->cap;
 }
 
-int learner_predict(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, bool collect, bool predict) {
+int learner_predict(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, bool collect, bool predict,
+                    const int32_t* slotOf, float* hist) {
     const cudaStream_t own = L->stream;
     L->stream = s;
     L->collecting = collect;
@@ -314,8 +315,7 @@ int learner_predict(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, b
         rc = collect ? forward(L, L->X.p, L->ellCol.p, L->ellW.p, n)
                      : forward(L, L->X.p, L->ellCol.p, L->ellW.p, L->cap, L->count.p);
         if (rc == TG_OK)
-            launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, nullptr, nullptr, L->cap,
-                                    s);
+            launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, slotOf, hist, L->cap, s);
     }
     L->stream = own;
     if (rc == TG_OK && cudaGetLastError() != cudaSuccess) rc = lfail(L, TG_ERR_CUDA, "learner: launch");

@@ -17,8 +17,10 @@ int learner_attach_mesh(tg_learner* L, size_t meshNodes, int maxRow);
 // graph and features of `site` from the current state; with `collect` the
 // features are stored as a new sample (finished by learner_collect_end);
 // with `predict` the prediction is added to the potentials of the graph's
-// cells
-int learner_predict(tg_learner* L, const tgd::DevMesh& m, int site, cudaStream_t s, bool collect, bool predict);
+// cells, and with `hist` also to the recorded correction of their V slots
+// (slotOf: node -> slot), so that the next event recycles all of it
+int learner_predict(tg_learner* L, const tgd::DevMesh& m, int site, cudaStream_t s, bool collect, bool predict,
+                    const int32_t* slotOf, float* hist);
 // the cells of the last graph (device list, its length on the device) and
 // the list's capacity: the cells whose potentials a prediction changed
 void learner_graph_cells(const tg_learner* L, const int32_t** nodes, const int32_t** count, int* capacity);

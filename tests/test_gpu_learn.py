@@ -19,7 +19,7 @@ def collected(ref_mesh):
     L = Learner(hops=6, max_cells=4096, ell_width=64, seed=3)
     L.attach(g, collect=True)
     opts = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
-    ev = Evaporation(g, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, preconditioner=1))
+    ev = Evaporation(g, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, warm_start=1, preconditioner=1))
     recs = ev.run(EVENTS)
     L.attach(g)  # detach
     return g, L, recs
@@ -70,10 +70,11 @@ def test_training_fits(collected):
 
 def test_learned_start_keeps_sequence_and_saves_iterations(ref_mesh):
     """Trained on the removals of another tip (another seed of the same
-    generator), the network's near-field prediction as the start of each
-    event's solve (warm_start 2, multigrid preconditioner) removes the same
-    cells as the plain start, ends at the same tolerance, and needs fewer
-    inner iterations over the golden tip's events."""
+    generator), the network's near-field prediction on top of the recycled
+    far field as the start of each event's solve (warm_start 2, multigrid
+    preconditioner) removes the same cells as the plain start, ends at the
+    same tolerance, and needs fewer inner iterations over the golden tip's
+    events than the plain start."""
     from conftest import SMALL_TIP
     from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, Learner, Mesh, solve_opts
     opts = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
@@ -82,7 +83,7 @@ def test_learned_start_keeps_sequence_and_saves_iterations(ref_mesh):
     tg.solve(rel_tol=1e-10, preconditioner=1)
     L = Learner(hops=6, max_cells=4096, ell_width=64, seed=5)
     L.attach(tg, collect=True)
-    Evaporation(tg, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, preconditioner=1)).run(120)
+    Evaporation(tg, opts, relax_mode=1, solve=solve_opts(rel_tol=1e-10, warm_start=1, preconditioner=1)).run(120)
     L.attach(tg)
     tg.close()
     n, _ = L.samples()
@@ -92,7 +93,7 @@ def test_learned_start_keeps_sequence_and_saves_iterations(ref_mesh):
     after = L.gradients(n - hold, hold)[0]
     print("held-out loss before", before, "after", after)
     runs = {}
-    for ws in (0, 2):
+    for ws in (0, 1, 2):
         g = Grid(ref_mesh)
         g.solve(rel_tol=1e-10, preconditioner=1)
         if ws == 2:
@@ -102,11 +103,12 @@ def test_learned_start_keeps_sequence_and_saves_iterations(ref_mesh):
         if ws == 2:
             L.attach(g)
         g.close()
-    plain, learned = runs[0], runs[2]
-    assert [r["node"] for r in learned] == [r["node"] for r in plain]
-    assert all(r["rel_residual"] <= 1e-10 for r in plain + learned)
+    plain, recycled, learned = runs[0], runs[1], runs[2]
+    assert [r["node"] for r in learned] == [r["node"] for r in plain] == [r["node"] for r in recycled]
+    assert all(r["rel_residual"] <= 1e-10 for r in plain + recycled + learned)
     it_p = sum(r["relax_iterations"] for r in plain[1:])
+    it_r = sum(r["relax_iterations"] for r in recycled[1:])
     it_l = sum(r["relax_iterations"] for r in learned[1:])
-    print("inner iterations over", len(plain) - 1, "events: plain", it_p, "learned", it_l)
+    print("inner iterations over", len(plain) - 1, "events: plain", it_p, "recycled", it_r, "learned", it_l)
     assert after < before
     assert it_l < it_p
