@@ -780,7 +780,7 @@ def run_warm_bounds(args):
                 t0 = time.perf_counter()
                 bi = B.solve(REL_TOL, 50, 20000, 1e-4, warm_start=0, preconditioner=PRECOND)
                 rows[s].append((bi.inner, time.perf_counter() - t0, bi.initial_rel_residual, int(b6.sum()),
-                                int(b12.sum())))
+                                int(b12.sum()), bi.inner - bi.inner_neumann))
         B.set_potentials(phi_post)
         d_prev = d
     out = {"impl": "warm_bounds", "workload": args.tip, "cells": mesh.num_nodes, "events": len(plain_path),
@@ -789,6 +789,7 @@ def run_warm_bounds(args):
                                 "solve_ms_median": 1e3 * statistics.median(x[1] for x in plain_path)},
            "starts": {s: {"inner_median": statistics.median(r[0] for r in v),
                           "inner_mean": statistics.mean(r[0] for r in v),
+                          "v_system_iterations_mean": statistics.mean(r[5] for r in v),
                           "solve_ms_median": 1e3 * statistics.median(r[1] for r in v),
                           "initial_rel_residual_median": statistics.median(r[2] for r in v)}
                       for s, v in rows.items()},
