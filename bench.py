@@ -548,7 +548,11 @@ def run_many_tips(args, rank: int, world: int, dist):
     sizes = [estimated_atoms(s) for s in specs]
     mine = partition_tips(sizes, world)[rank]
     t0 = time.perf_counter()
-    meshes = [Mesh.from_tip(**specs[k]) for k in mine]
+    # independent tips: built side by side, one host thread each (the
+    # library call releases the interpreter lock)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(mine), os.cpu_count() or 1))) as pool:
+        meshes = list(pool.map(lambda k: Mesh.from_tip(threads=1, **specs[k]), mine))
     t_mesh = time.perf_counter() - t0
     opts = EvaporationOptions.from_ini(None)
     # the learned warm start: one network trained once, a copy of it per tip
