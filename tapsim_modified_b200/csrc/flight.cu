@@ -10,6 +10,8 @@
 // geometry_3d.cpp:916-980); the tetrahedron comes from a visibility walk
 // (findTetrahedron, geometry_3d.cpp:988-1044) whose start face rotates
 // instead of being drawn with rand().
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace tgd {
@@ -744,11 +746,17 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
     *out = res;
 }
 
+// perWarp: the ions each warp carries (its first perWarp lanes; the rest
+// return at once).  A flight is a chain of dependent loads whose branches
+// (walk lengths, rejected steps) differ from ion to ion, so a warp runs its
+// lanes' flights largely one after another: few ions per warp over every
+// warp the SMs can hold beats full warps on a fraction of them.
 template <bool kPath, int kPrec>
-__global__ void k_trace(DevMesh m, int nIons, const float* start, const float* vel, const float* qm,
+__global__ void k_trace(DevMesh m, int nIons, int perWarp, const float* start, const float* vel, const float* qm,
                         const int32_t* guess, TraceParams tp, ImpactOut* out) {
-    const int ion = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ion >= nIons) return;
+    const int lane = threadIdx.x & 31;
+    const int ion = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * perWarp + lane;
+    if (lane >= perWarp || ion >= nIons) return;
     const V3 x{start[3 * ion], start[3 * ion + 1], start[3 * ion + 2]};
     const V3 v = vel ? V3{vel[3 * ion], vel[3 * ion + 1], vel[3 * ion + 2]} : V3{0, 0, 0};
     trace_ion<kPath, kPrec>(m, x, v, qm[ion], guess ? guess[ion] : 0, tp, (unsigned)ion * 7u, ion, out + ion);
@@ -778,14 +786,18 @@ void launch_trace(const DevMesh& m, int nIons, const float* start, const float* 
                   const int32_t* guess, TraceParams tp, ImpactOut* out, cudaStream_t s) {
     if (nIons <= 0) return;
     count_launch();
-    // a flight is a chain of dependent loads, one ion per thread: with one
-    // warp per block, a few thousand ions spread over all SMs instead of
-    // filling a quarter of them four warps deep
+    // ions per warp: as few as fill every warp slot the SMs hold at this
+    // kernel's register count (one wave), one warp per block
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int block = nIons <= 2 * 32 * sms ? 32 : kBlock;
-    const int blocks = (nIons + block - 1) / block;
-    auto go = [&](auto kernel) { kernel<<<blocks, block, 0, s>>>(m, nIons, start, vel, qm, guess, tp, out); };
+    auto go = [&](auto kernel) {
+        int perSM = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, 32, 0) != cudaSuccess || perSM < 1) perSM = 1;
+        const long long slots = (long long)perSM * sms;
+        const int perWarp = (int)std::min<long long>(32, std::max<long long>(1, (nIons + slots - 1) / slots));
+        const int warps = (nIons + perWarp - 1) / perWarp;
+        kernel<<<warps, 32, 0, s>>>(m, nIons, perWarp, start, vel, qm, guess, tp, out);
+    };
     const int prec = tp.precision == 1 ? 1 : (tp.precision == 2 ? 2 : 0);
     if (tp.path) {
         if (prec == 0) go(k_trace<true, 0>); else if (prec == 1) go(k_trace<true, 1>); else go(k_trace<true, 2>);
