@@ -426,8 +426,14 @@ int tg_learner_create(int32_t hops, int32_t max_cells, int32_t ell_width, uint64
 void tg_learner_destroy(tg_learner* L);
 const char* tg_learner_last_error(const tg_learner* L);
 int32_t tg_learner_num_params(void);
-/* multiplier of the prediction that warm_start 2 adds (default 1) */
+/* multiplier of the prediction that warm_start 2 adds (default 1; 0: no
+ * prediction, the sweeps below alone) */
 int tg_learner_set_gain(tg_learner* L, float gain);
+/* damped Jacobi sweeps (weight 0.8) over the graph's cells after the
+ * prediction, every other cell held (computePotential's update); they
+ * remove the prediction's high-frequency error.  Default 0; graphs of at
+ * most 4096 cells. */
+int tg_learner_set_refine(tg_learner* L, int32_t sweeps);
 /* mode: 0 detach, bit 0 collect samples, bit 1 predict (for warm_start 2).
  * The learner's graph width must hold the mesh's longest row. */
 int tg_learner_attach(tg_handle* h, tg_learner* L, int32_t mode);

@@ -181,6 +181,7 @@ SIGNATURES = {
     "tg_learner_last_error": (C.c_char_p, [_P]),
     "tg_learner_num_params": (C.c_int32, []),
     "tg_learner_set_gain": (C.c_int, [_P, C.c_float]),
+    "tg_learner_set_refine": (C.c_int, [_P, _I]),
     "tg_learner_attach": (C.c_int, [_P, _P, _I]),
     "tg_learner_samples": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "tg_learner_get_params": (C.c_int, [_P, _P]),

@@ -318,6 +318,10 @@ void launch_message_back(const float* dh, const float* dz, const int32_t* ellCol
 void launch_adam(float* p, const float* g, float* m1, float* m2, int count, float lr, float b1, float b2, float eps,
                  float c1, float c2, cudaStream_t s);
 void launch_weights_bf16(const float* W, void* Wb, void* WTb, cudaStream_t s);
+// damped Jacobi sweeps on the graph's cells (at most 4096), the rest held;
+// the change joins hist (V slots) when given
+void launch_local_refine(const DevMesh& m, const int32_t* nodes, const int32_t* count, int cap, int sweeps,
+                         float omega, const int32_t* slotOf, float* hist, cudaStream_t s);
 void launch_apply_prediction(const DevMesh& m, const int32_t* nodes, const int32_t* count, const float* y,
                              const float* scale, float gain, const int32_t* slotOf, float* hist, int cap,
                              cudaStream_t s);

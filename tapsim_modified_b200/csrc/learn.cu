@@ -74,6 +74,7 @@ struct tg_learner {
     int hops = 6, cap = 4096, D = 32;
     int device = -1;    // current at tg_learner_create; made current by every entry point
     float gain = 1.0f;  // multiplier of the prediction added in tg_solve
+    int refine = 0;     // damped Jacobi sweeps over the graph's cells after the prediction
     std::string err;
     cudaStream_t stream = nullptr;
     // parameters, gradients, Adam moments (FP32), BF16 weight copies
@@ -312,10 +313,15 @@ int learner_predict(tg_learner* L, const DevMesh& m, int site, cudaStream_t s, b
         }
     }
     if (rc == TG_OK && predict) {
-        rc = collect ? forward(L, L->X.p, L->ellCol.p, L->ellW.p, n)
-                     : forward(L, L->X.p, L->ellCol.p, L->ellW.p, L->cap, L->count.p);
-        if (rc == TG_OK)
-            launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, slotOf, hist, L->cap, s);
+        // gain 0: no prediction, the sweeps alone (to isolate the network)
+        if (L->gain > 0.0f) {
+            rc = collect ? forward(L, L->X.p, L->ellCol.p, L->ellW.p, n)
+                         : forward(L, L->X.p, L->ellCol.p, L->ellW.p, L->cap, L->count.p);
+            if (rc == TG_OK)
+                launch_apply_prediction(m, L->nodes.p, L->count.p, L->y.p, L->scale.p, L->gain, slotOf, hist, L->cap,
+                                        s);
+        }
+        if (rc == TG_OK) launch_local_refine(m, L->nodes.p, L->count.p, L->cap, L->refine, 0.8f, slotOf, hist, s);
     }
     L->stream = own;
     if (rc == TG_OK && cudaGetLastError() != cudaSuccess) rc = lfail(L, TG_ERR_CUDA, "learner: launch");
@@ -426,6 +432,15 @@ void tg_learner_destroy(tg_learner* L) {
 const char* tg_learner_last_error(const tg_learner* L) { return L ? L->err.c_str() : ""; }
 
 int32_t tg_learner_num_params(void) { return kParams; }
+
+int tg_learner_set_refine(tg_learner* L, int32_t sweeps) {
+    ScopedDevice dev_scope(L ? L->device : -1);
+    if (!L || sweeps < 0 || sweeps > 256) return lfail(L, TG_ERR_ARGUMENT, "tg_learner_set_refine: sweeps in [0, 256]");
+    if (sweeps > 0 && L->cap > 4096)
+        return lfail(L, TG_ERR_ARGUMENT, "tg_learner_set_refine: the sweeps take graphs of at most 4096 cells");
+    L->refine = sweeps;
+    return TG_OK;
+}
 
 int tg_learner_set_gain(tg_learner* L, float gain) {
     ScopedDevice dev_scope(L ? L->device : -1);

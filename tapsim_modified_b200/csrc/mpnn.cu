@@ -448,6 +448,43 @@ __global__ void k_apply_prediction(DevMesh m, const int32_t* nodes, const int32_
     }
 }
 
+// Damped Jacobi sweeps over the graph's cells after the prediction, every
+// other cell held: phi_i += omega ((sum_j ceff_ij phi_j - q_i) / diag_i -
+// phi_i) (computePotential's update, grid_3d.cpp:1317-1371).  One CTA: each
+// sweep computes every cell's new value from the old ones, then writes them
+// (the same result for any thread count).  The change joins the recorded
+// correction of the cells' V slots when hist is given.  The graph has at
+// most cap <= kRefineMax cells.
+constexpr int kRefineMax = 4096;
+__global__ void __launch_bounds__(1024) k_local_refine(DevMesh m, const int32_t* nodes, const int32_t* count,
+                                                       int cap, int sweeps, float omega, const int32_t* slotOf,
+                                                       float* hist) {
+    extern __shared__ double refineShared[];  // start[cap], next[cap]
+    double* start = refineShared;
+    double* next = refineShared + cap;
+    const int n = min(*count, cap);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) start[t] = m.phi64[nodes[t]];
+    __syncthreads();
+    for (int sw = 0; sw < sweeps; sw++) {
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            const int i = nodes[t];
+            const double d = m.diag64[i];
+            double sum = 0.0;
+            for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) sum += m.ceff64[q] * m.phi64[m.col[q]];
+            const double pi = m.phi64[i];
+            next[t] = d > 0.0 ? pi + (double)omega * ((sum - m.q64[i]) / d - pi) : pi;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < n; t += blockDim.x) m.phi64[nodes[t]] = next[t];
+        __syncthreads();
+    }
+    if (hist)
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            const int sl = slotOf[nodes[t]];
+            if (sl >= 0) hist[sl] += (float)(m.phi64[nodes[t]] - start[t]);
+        }
+}
+
 // training target: (phi_final - phi_start) / sigma
 __global__ void k_collect_target(DevMesh m, const int32_t* nodes, const int32_t* count, const double* phiStart,
                                  const float* scale, float* tgt) {
@@ -563,6 +600,19 @@ void launch_apply_prediction(const DevMesh& m, const int32_t* nodes, const int32
                              cudaStream_t s) {
     count_launch();
     k_apply_prediction<<<nblk(cap), 256, 0, s>>>(m, nodes, count, y, scale, gain, slotOf, hist);
+}
+void launch_local_refine(const DevMesh& m, const int32_t* nodes, const int32_t* count, int cap, int sweeps,
+                         float omega, const int32_t* slotOf, float* hist, cudaStream_t s) {
+    if (sweeps <= 0 || cap <= 0 || cap > kRefineMax) return;
+    static bool opted = false;
+    if (!opted) {
+        cudaFuncSetAttribute(k_local_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * sizeof(double) * kRefineMax));
+        opted = true;
+    }
+    count_launch();
+    k_local_refine<<<1, 1024, 2 * sizeof(double) * (size_t)cap, s>>>(m, nodes, count, cap, sweeps, omega, slotOf,
+                                                                     hist);
 }
 void launch_collect_target(const DevMesh& m, const int32_t* nodes, const int32_t* count, const double* phiStart,
                            const float* scale, float* tgt, int cap, cudaStream_t s) {

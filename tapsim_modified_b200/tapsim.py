@@ -431,8 +431,13 @@ class Learner:
         grid._ck(N.lib().tg_learner_attach(grid._h, self._h if mode else None, mode))
 
     def set_gain(self, gain: float):
-        """Multiplier of the prediction that warm_start=2 adds (default 1)."""
+        """Multiplier of the prediction that warm_start=2 adds (default 1;
+        0: no prediction, the refinement sweeps alone)."""
         self._ck(N.lib().tg_learner_set_gain(self._h, gain))
+
+    def set_refine(self, sweeps: int):
+        """Damped Jacobi sweeps over the prediction's cells after it (tg_learner_set_refine)."""
+        self._ck(N.lib().tg_learner_set_refine(self._h, sweeps))
 
     def samples(self) -> tuple[int, int]:
         n, cells = C.c_int32(), C.c_int64()
