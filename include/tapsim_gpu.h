@@ -163,9 +163,10 @@ int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);
  * (levels smoothed with CSR rows) and of its restriction (every level but
  * the coarsest), 0 where the level has none; for level 0, a_lanes is the
  * number of coupling loads each lane of the SELL-32 smoothing pass issues
- * ahead of their gathers (4, 8 or 16).  The hierarchy build times each
- * candidate on the level's own matrices and keeps the fastest; a_ms / r_ms
- * are the kept launches' times [ms]. */
+ * ahead of their gathers (4, 8 or 16).  The hierarchy build chooses them
+ * one at a time, from a row-length rule, by timing whole V-cycles with
+ * each candidate, and keeps a change that takes 3% off the cycle; a_ms /
+ * r_ms are the kept kernels' own launch times [ms]. */
 int tg_amg_schedule(tg_handle* h, int32_t level, int32_t* rows, int32_t* a_lanes, int32_t* r_lanes, float* a_ms,
                     float* r_ms);
 /* ||r||_2 / ||b||_2 of the current potentials (FP64). */

@@ -138,13 +138,14 @@ struct AmgDev {
     const float* coarse_inv;                // dense inverse of the coarsest operator, row-major
     int fine_unroll;                        // level-0 pass: loads per lane ahead of their gathers (4, 8, 16)
 };
-// Autotuner of the hierarchy's schedules, by timed trials (5 launches each
-// after a warm-up, CUDA events on s) on the hierarchy's own matrices: the
-// level-0 pass's loads per lane (4, 8, 16; fine_unroll), and for the
-// restriction of every level and the operator of every level smoothed by
-// CSR rows the lane-group size (2..32 lanes per row; r_lanes / a_lanes).
+// Autotuner of the hierarchy's schedules: the level-0 pass's loads per
+// lane (4, 8, 16; fine_unroll), and for the restriction of every level and
+// the operator of every level smoothed by CSR rows the lane-group size
+// (2..32 lanes per row; r_lanes / a_lanes), chosen one at a time from the
+// row-length rule's schedule by timing whole V-cycles (the least of three
+// batches of three, CUDA events on s), a change kept when it takes 3% off.
 // aMs / rMs (kAmgMaxLevels entries) and fineMs (may be null) receive the
-// winners' times [ms].  Returns 0, or -1 on a CUDA error.
+// kept kernels' own times [ms].  Returns 0, or -1 on a CUDA error.
 int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* aMs, float* rMs, float* fineMs);
 // the level-0 smoothing pass t = b - A y alone (timing hook)
 void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s);

@@ -43,9 +43,9 @@ def test_multigrid_events_follow_reference(ref_mesh, ref_events):
 
 
 def test_tuned_schedules_of_the_hierarchy():
-    """The hierarchy build times every lane-group size of each coarse
-    operator and restriction, and the load depth of the level-0 pass, on the
-    device and keeps the fastest (amg_tune_lanes): every level but the
+    """The hierarchy build chooses the lane-group size of each coarse
+    operator and restriction, and the load depth of the level-0 pass, by
+    timing whole V-cycles on the device (amg_tune_lanes): every level but the
     coarsest reports a restriction
     schedule, every level smoothed with CSR rows an operator schedule, each a
     power of two in 2..32 with a positive launch time; the solve converges
