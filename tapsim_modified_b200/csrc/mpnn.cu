@@ -176,6 +176,11 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
 // ---------------------------------------------------------------------------
 constexpr int kFeat = 16, kHid = 64, kCat = 128;
 
+// Breadth-first search from `site` over the free cells, `hops` levels, one
+// CTA: each warp takes a frontier cell and its lanes its neighbours, which
+// claim their cell with an atomic on localOf (-1 -> -2), so a level costs
+// one round of loads instead of one per neighbour.  The list order follows
+// the claims (it varies from run to run; nothing downstream depends on it).
 __global__ void k_ball_bfs(DevMesh m, int site, int hops, int cap, int32_t* nodes, int8_t* level, int32_t* count,
                            int32_t* localOf) {
     __shared__ int lvlStart, lvlEnd, total;
@@ -188,11 +193,13 @@ __global__ void k_ball_bfs(DevMesh m, int site, int hops, int cap, int32_t* node
         total = 1;
     }
     __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int L = 0; L < hops; L++) {
         const int s0 = lvlStart, s1 = lvlEnd;
-        for (int t = s0 + (int)threadIdx.x; t < s1; t += blockDim.x) {
+        for (int t = s0 + warp; t < s1; t += nwarps) {
             const int u = nodes[t];
-            for (int q = m.row_ptr[u]; q < m.row_ptr[u + 1]; q++) {
+            const int q1 = m.row_ptr[u + 1];
+            for (int q = m.row_ptr[u] + lane; q < q1; q += 32) {
                 const int j = m.col[q];
                 if (m.flags[j] & F_DIRICHLET) continue;
                 if (atomicCAS(&localOf[j], -1, -2) != -1) continue;
@@ -245,12 +252,15 @@ __global__ void k_site_scale(DevMesh m, int site, float* scale) {
     scale[1] = nbs > 0 ? (float)(dist / nbs) : 1.0f;
 }
 
-// features, ELL rows and (for sample collection) the start potentials
+// features, ELL rows and (for sample collection) the start potentials; one
+// warp per cell, its lanes over the cell's neighbours (warp sums, and the
+// ELL row compacted in CSR order by ballots)
 __global__ void k_ball_features(DevMesh m, int site, int hops, int D, const int32_t* nodes, const int8_t* level,
                                 const int32_t* count, const int32_t* localOf, const float* scale, float* X,
                                 int32_t* ellCol, float* ellW, double* phiStart) {
     const int n = *count;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (t >= n) return;
     const int g = nodes[t];
     const double sigma = scale[0], ell = scale[1];
@@ -258,25 +268,41 @@ __global__ void k_ball_features(DevMesh m, int site, int hops, int D, const int3
     const double dx = m.xyz[3 * g] - xs, dy = m.xyz[3 * g + 1] - ys, dz = m.xyz[3 * g + 2] - zs;
     const double dist = sqrt(dx * dx + dy * dy + dz * dz);
     double sum = 0.0, fixedC = 0.0, allC = 0.0;
-    int k = 0;
+    int k = 0;  // ELL entries written so far (the same in every lane)
     const double dg = m.diag64[g];
-    for (int q = m.row_ptr[g]; q < m.row_ptr[g + 1]; q++) {
-        const int j = m.col[q];
-        const double c = m.ceff64[q];
-        sum += c * m.phi64[j];
-        allC += m.c64[q];
-        if (m.flags[j] & F_DIRICHLET) fixedC += m.c64[q];
-        const int lj = localOf[j];
-        if (lj >= 0 && lj < n && k < D && c != 0.0) {
-            ellCol[(size_t)t * D + k] = lj;
-            ellW[(size_t)t * D + k] = dg > 0.0 ? (float)(c / dg) : 0.0f;
-            k++;
+    const int q0 = m.row_ptr[g], q1 = m.row_ptr[g + 1];
+    for (int base = q0; base < q1; base += 32) {
+        const int q = base + lane;
+        int lj = -1;
+        double c = 0.0;
+        if (q < q1) {
+            const int j = m.col[q];
+            c = m.ceff64[q];
+            sum += c * m.phi64[j];
+            const double c64 = m.c64[q];
+            allC += c64;
+            if (m.flags[j] & F_DIRICHLET) fixedC += c64;
+            lj = localOf[j];
         }
+        const bool take = q < q1 && lj >= 0 && lj < n && c != 0.0;
+        const unsigned mask = __ballot_sync(0xffffffffu, take);
+        const int at = k + __popc(mask & ((1u << lane) - 1u));
+        if (take && at < D) {
+            ellCol[(size_t)t * D + at] = lj;
+            ellW[(size_t)t * D + at] = dg > 0.0 ? (float)(c / dg) : 0.0f;
+        }
+        k = min(D, k + __popc(mask));
     }
-    for (; k < D; k++) {
-        ellCol[(size_t)t * D + k] = -1;
-        ellW[(size_t)t * D + k] = 0.0f;
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        allC += __shfl_xor_sync(0xffffffffu, allC, o);
+        fixedC += __shfl_xor_sync(0xffffffffu, fixedC, o);
     }
+    for (int e = k + lane; e < D; e += 32) {
+        ellCol[(size_t)t * D + e] = -1;
+        ellW[(size_t)t * D + e] = 0.0f;
+    }
+    if (lane != 0) return;
     const double r = sum - dg * m.phi64[g] - m.q64[g];
     float* x = X + (size_t)t * kFeat;
     x[0] = (float)(dx / ell);
@@ -541,7 +567,8 @@ void launch_ball_features(const DevMesh& m, int site, int hops, int D, const int
     count_launch();
     k_site_scale<<<1, 32, 0, s>>>(m, site, scale);
     count_launch();
-    k_ball_features<<<nblk(cap), 256, 0, s>>>(m, site, hops, D, nodes, level, count, localOf, scale, X, ellCol, ellW,
+    k_ball_features<<<nblk((long long)cap * 32), 256, 0, s>>>(m, site, hops, D, nodes, level, count, localOf, scale, X,
+                                                               ellCol, ellW,
                                                phiStart);
 }
 void launch_input_bf16(const float* X, int n, int npad, void* Z, void* ZT, cudaStream_t s, const int32_t* nDev) {
