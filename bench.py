@@ -191,7 +191,8 @@ def train_learner(args, rank: int, opts):
     tmesh = Mesh.from_tip(seed=101 + rank, **TIPS["train"])
     tgrid = Grid(tmesh)
     tgrid.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
-    learner = Learner(hops=6, max_cells=2048, ell_width=64, seed=7 + rank)
+    learner = Learner(hops=6, max_cells=1024, ell_width=64, seed=7 + rank)
+    learner.set_refine(args.refine)
     learner.attach(tgrid, collect=True)
     # samples of the state the learned start sees: the recycled far field
     tev = Evaporation(tgrid, opts, relax_mode=1,
@@ -566,8 +567,9 @@ def run_many_tips(args, rank: int, world: int, dist):
         g = Grid(m)
         g.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
         if trained is not None:
-            lr = Learner(hops=6, max_cells=2048, ell_width=64, seed=7)
+            lr = Learner(hops=6, max_cells=1024, ell_width=64, seed=7)
             lr.set_params(trained.params())
+            lr.set_refine(args.refine)
             lr.attach(g, predict=True)
             learners.append(lr)
         ev = Evaporation(g, opts, relax_mode=1, solve=sopts)   # surface set and first selection
@@ -958,6 +960,8 @@ def main():
     ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
     ap.add_argument("--train-steps", type=int, default=600, help="Adam steps of the learned warm start")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
+    ap.add_argument("--refine", type=int, default=8,
+                    help="damped Jacobi sweeps over the learned start's cells after its prediction")
     ap.add_argument("--long-events", type=int, default=200,
                     help="events run and timed after the K timed ones on the headline arm")
     ap.add_argument("--precision-events", type=int, default=20,
