@@ -250,6 +250,7 @@ def run_ours(args, rank: int, world: int, dist):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         grid = Grid(mesh)                       # host -> device upload of the mesh
+        grid.set_launch_mode(args.launch_mode)
         # initial relaxation; builds the multigrid hierarchy
         info0 = grid.solve(REL_TOL, 50, 50000, 1e-4, preconditioner=PRECOND)
         torch.cuda.synchronize()
@@ -401,6 +402,8 @@ def run_ours(args, rank: int, world: int, dist):
             "initial_solve": {"outer": info0.outer, "inner": info0.inner, "rel_residual": info0.rel_residual},
             "preconditioner": "smoothed-aggregation multigrid V(1,1)-cycle (tg_solve_opts.preconditioner 1)"
                               if PRECOND == 1 else "Jacobi",
+            "launch_mode": ("each multigrid CG iteration replayed from one captured CUDA graph" if args.launch_mode == 1
+                            else "every kernel launched from the host"),
             "setup": {"seconds": arm["setup_s"], "multigrid_hierarchy_s": info0.setup_seconds,
                       "mesh_h2d_bytes": h2d_bytes,
                       "note": "mesh upload (tg_create), multigrid hierarchy and initial relaxation, once per tip"},
@@ -960,6 +963,8 @@ def main():
     ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
     ap.add_argument("--train-steps", type=int, default=600, help="Adam steps of the learned warm start")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
+    ap.add_argument("--launch-mode", type=int, default=1, choices=(0, 1),
+                    help="1: the multigrid CG iterations replay a captured CUDA graph; 0: kernel by kernel")
     ap.add_argument("--refine", type=int, default=8,
                     help="damped Jacobi sweeps over the learned start's cells after its prediction")
     ap.add_argument("--long-events", type=int, default=200,

@@ -459,8 +459,15 @@ int tg_learner_train(tg_learner* L, int32_t steps, int32_t batch, float lr, uint
 /* CUDA events on the handle's stream around a region of calls. */
 int tg_timer_start(tg_handle* h);
 int tg_timer_stop(tg_handle* h, float* elapsed_ms);
-/* Kernels this handle has launched since creation. */
+/* Kernels launched in this process so far (every handle; the kernels of a
+ * replayed CUDA graph count at each replay). */
 int64_t tg_launch_count(const tg_handle* h);
+/* How the multigrid solve's FP32 CG iterations reach the device: 1 (the
+ * default) replays one iteration (update, V-cycle, SpMV) captured as a CUDA
+ * graph, whose kernels read the iteration index, target and slot count from
+ * device memory; 0 launches each kernel from the host.  Both run the same
+ * kernels on the same data. */
+int tg_set_launch_mode(tg_handle* h, int32_t mode);
 /* Times `iters` back-to-back launches of one hot kernel on the handle's
  * stream with CUDA events: 0 = FP32 CG SpMV over the non-Neumann free rows,
  * 1 = FP64 residual over all free rows, 2 = the multigrid's level-0
@@ -511,6 +518,32 @@ void tg_tip_params_default(tg_tip_params* p);
 int tg_mesh_from_tip(const tg_tip_params* p, int32_t threads, tg_mesh** out);
 /* Node file + config (meshgen output / File_Io::readGeomGrid input). */
 int tg_mesh_from_files(const char* node_file, const char* config_file, int32_t threads, tg_mesh** out);
+/* MeshGen's role for an arbitrary sample (meshgen/meshgen.cpp:2506-3986,
+ * replacing `meshgen sample out`): reads the sample node file (meshgen's
+ * readSample input, :197-360: the node-file layout with ids), places graded
+ * vacuum around it by the distance to its nearest atom (level 0 at the
+ * sample's median nearest-neighbour spacing h0 out to fine_shell, no nearer
+ * than exclusion * h0 to an atom; coarser levels by `coarsen` every
+ * layers_per_level layers), the box faces z = 0 (bottom marker), z =
+ * box_height (top) and |x|, |y| = box_half_width (sides, with every edge and
+ * corner node, :3855-3892), appends the sample last (:3908) and builds the
+ * Delaunay mesh and Voronoi couplings.  The sample must lie above z = 0 and
+ * fit into the box with its fine shell.  config_file NULL takes meshgen's
+ * configuration template (writeConfig, :491-595: top and sides Dirichlet
+ * 0 V, bottom Neumann, sample ids removable Dirichlet 1000 V with mass and
+ * evaporation field 0, which an evaporation run needs filled in);
+ * tg_mesh_write_config writes it out.  threads <= 0: all host cores.
+ * Deterministic in seed, whatever the thread count. */
+typedef struct {
+    double box_half_width, box_height, fine_shell, exclusion;
+    int32_t layers_per_level;
+    double coarsen, max_spacing;
+    int32_t vacuum_id, top_id, bottom_id, sides_id;
+    uint64_t seed;
+} tg_sample_params;
+void tg_sample_params_default(tg_sample_params* p);
+int tg_mesh_from_sample(const char* sample_file, const char* config_file, const tg_sample_params* p, int32_t threads,
+                        tg_mesh** out);
 /* TAPSIM dump (File_Io::readSystem); keeps the dump's float couplings.
  * config_file may be NULL to use the dump's own table. */
 int tg_mesh_from_dump(const char* dump_file, const char* config_file, tg_mesh** out);

@@ -120,6 +120,13 @@ class tg_tip_params(C.Structure):
                 ("precip_sigma", C.c_double), ("seed", C.c_uint64)]
 
 
+class tg_sample_params(C.Structure):
+    _fields_ = [("box_half_width", C.c_double), ("box_height", C.c_double), ("fine_shell", C.c_double),
+                ("exclusion", C.c_double), ("layers_per_level", C.c_int32), ("coarsen", C.c_double),
+                ("max_spacing", C.c_double), ("vacuum_id", C.c_int32), ("top_id", C.c_int32),
+                ("bottom_id", C.c_int32), ("sides_id", C.c_int32), ("seed", C.c_uint64)]
+
+
 # every symbol include/tapsim_gpu.h declares, with its ctypes signature
 _P = C.c_void_p
 _I = C.c_int32
@@ -168,6 +175,7 @@ SIGNATURES = {
     "tg_timer_start": (C.c_int, [_P]),
     "tg_timer_stop": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "tg_launch_count": (C.c_int64, [_P]),
+    "tg_set_launch_mode": (C.c_int, [_P, _I]),
     "tg_bench_kernel": (C.c_int, [_P, _I, _I, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
     "tg_gemm_bf16": (C.c_int, [_P, _P, _P, _I, _I, _I]),
     "tg_amg_host_build": (C.c_int, [_I, _P, _P, _P, C.POINTER(C.c_void_p)]),
@@ -192,6 +200,8 @@ SIGNATURES = {
     "tg_tip_params_default": (None, [C.POINTER(tg_tip_params)]),
     "tg_mesh_from_tip": (C.c_int, [C.POINTER(tg_tip_params), _I, C.POINTER(_P)]),
     "tg_mesh_from_files": (C.c_int, [C.c_char_p, C.c_char_p, _I, C.POINTER(_P)]),
+    "tg_sample_params_default": (None, [C.POINTER(tg_sample_params)]),
+    "tg_mesh_from_sample": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(tg_sample_params), _I, C.POINTER(_P)]),
     "tg_mesh_from_dump": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_P)]),
     "tg_mesh_destroy": (None, [_P]),
     "tg_mesh_temperature": (C.c_float, [_P]),

@@ -24,9 +24,9 @@ CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["relax.cu", "cg.cu", "amg.cu", "surface.cu", "flight.cu", "mpnn.cu", "learn.cu", "handle.cu"]
-CPP_SOURCES = ["host/tipgen.cpp", "host/delaunay.cpp", "host/voronoi.cpp", "host/formats.cpp", "host/mesh_api.cpp",
+CPP_SOURCES = ["host/tipgen.cpp", "host/samplegen.cpp", "host/delaunay.cpp", "host/voronoi.cpp", "host/formats.cpp", "host/mesh_api.cpp",
                "host/amg.cpp", "host/amg_api.cpp"]
-HEADERS = ["device_common.cuh", "kernels.cuh", "host/tipgen.h", "host/delaunay.h", "host/voronoi.h",
+HEADERS = ["device_common.cuh", "kernels.cuh", "host/tipgen.h", "host/samplegen.h", "host/delaunay.h", "host/voronoi.h",
            "host/formats.h", "host/predicates.h", "host/amg.h"]
 
 

@@ -25,15 +25,10 @@ constexpr int kBlock = 256;
 // 7.3M-cell tip where 2/3 took 27
 constexpr float kSmooth = 0.9f;
 
-// the CG iteration has converged: rho_it <= rel2 * rho_0 (rel2 < 0: never)
-__device__ __forceinline__ bool done(const double* scal, int it, double rel2) {
-    return rel2 >= 0.0 && scal[4 * it + 3] <= rel2 * scal[3];
-}
-
-// y = w b / d
-__global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, const double* scal, int it,
-                             double target) {
-    if (done(scal, it, target)) return;
+// y = w b / d over n rows (at most *countDev when given)
+__global__ void k_amg_jacobi(int n, const int32_t* countDev, const float* b, const float* d, float* y, Gate gate) {
+    if (gate.done()) return;
+    if (countDev) n = min(n, (*countDev + 31) & ~31);  // whole slices, padding rows included
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         y[i] = kSmooth * b[i] / d[i];
 }
@@ -48,9 +43,9 @@ __global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, co
 // U: the column/value loads a lane issues ahead of their gathers (the bytes
 // a warp keeps in flight), chosen per hierarchy by timed trials.
 template <int U>
-__global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, float* out, int mode,
-                           const double* scal, int it, double target) {
-    if (done(scal, it, target)) return;
+__global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, float* out, int mode, Gate gate) {
+    if (gate.done()) return;
+    slices = min(slices, (*v.count + 31) / 32);  // the slots in use
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
@@ -119,9 +114,8 @@ __device__ __forceinline__ float row_dot(const int32_t* ptr, const int32_t* col,
 // mode 0: t = b - A y; mode 1: x = y + w (b - A y) / diag
 template <int L>
 __global__ void k_amg_csr(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* diag,
-                          const float* b, const float* y, float* out, int mode, const double* scal, int it,
-                          double target) {
-    if (done(scal, it, target)) return;
+                          const float* b, const float* y, float* out, int mode, Gate gate) {
+    if (gate.done()) return;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = gid % L;
     const int row = min(gid / L, n - 1);  // whole groups stay active for the shuffles
@@ -135,8 +129,8 @@ __global__ void k_amg_csr(int n, const int32_t* ptr, const int32_t* col, const f
 // out = M y for a CSR matrix (restriction R t)
 template <int L>
 __global__ void k_amg_mv(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* y, float* out,
-                         const double* scal, int it, double target) {
-    if (done(scal, it, target)) return;
+                         Gate gate) {
+    if (gate.done()) return;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = gid % L;
     const int row = min(gid / L, n - 1);
@@ -146,8 +140,8 @@ __global__ void k_amg_mv(int n, const int32_t* ptr, const int32_t* col, const fl
 
 // y += P x' (prolongation, a few entries per row), one thread per row
 __global__ void k_amg_prolong(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* xc,
-                              float* y, const double* scal, int it, double target) {
-    if (done(scal, it, target)) return;
+                              float* y, Gate gate) {
+    if (gate.done()) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float acc = 0.0f;
         for (int q = ptr[i]; q < ptr[i + 1]; q++) acc += val[q] * __ldg(xc + col[q]);
@@ -156,9 +150,8 @@ __global__ void k_amg_prolong(int n, const int32_t* ptr, const int32_t* col, con
 }
 
 // x = C^-1 b with the coarsest level's dense inverse (row-major), one warp per row
-__global__ void k_amg_dense(int n, const float* inv, const float* b, float* x, const double* scal, int it,
-                            double target) {
-    if (done(scal, it, target)) return;
+__global__ void k_amg_dense(int n, const float* inv, const float* b, float* x, Gate gate) {
+    if (gate.done()) return;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
@@ -175,13 +168,13 @@ __global__ void k_amg_dense(int n, const float* inv, const float* b, float* x, c
 inline unsigned grid_full(long long threads) { return (unsigned)((threads + kBlock - 1) / kBlock); }
 
 // the level-0 pass with the hierarchy's load depth (AmgDev::fine_unroll)
-void launch_fine(int U, const VSys& v, int slices, const float* b, const float* y, float* out, int mode,
-                 const double* scal, int it, double target, cudaStream_t s) {
+void launch_fine(int U, const VSys& v, int slices, const float* b, const float* y, float* out, int mode, Gate gate,
+                 cudaStream_t s) {
     count_launch();
     const unsigned grid = grid_full((long long)slices * 32);
-    if (U == 4) k_amg_fine<4><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, scal, it, target);
-    else if (U == 16) k_amg_fine<16><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, scal, it, target);
-    else k_amg_fine<8><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, scal, it, target);
+    if (U == 4) k_amg_fine<4><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
+    else if (U == 16) k_amg_fine<16><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
+    else k_amg_fine<8><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
 }
 
 // a group of L threads for every row
@@ -189,36 +182,34 @@ inline unsigned grid_rows(int n, int L) { return (unsigned)(((long long)n * L + 
 
 // the lane-group kernels for L = 2 .. 32
 void launch_csr(int L, int n, const int32_t* ptr, const int32_t* col, const float* val, const float* diag,
-                const float* b, const float* y, float* out, int mode, const double* scal, int it, double target,
-                cudaStream_t s) {
+                const float* b, const float* y, float* out, int mode, Gate gate, cudaStream_t s) {
     count_launch();
     switch (L) {
-        case 2: k_amg_csr<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
-        case 4: k_amg_csr<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
-        case 8: k_amg_csr<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
-        case 16: k_amg_csr<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
-        default: k_amg_csr<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, scal, it, target); break;
+        case 2: k_amg_csr<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, gate); break;
+        case 4: k_amg_csr<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, gate); break;
+        case 8: k_amg_csr<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, gate); break;
+        case 16: k_amg_csr<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, gate); break;
+        default: k_amg_csr<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, diag, b, y, out, mode, gate); break;
     }
 }
 void launch_mv(int L, int n, const int32_t* ptr, const int32_t* col, const float* val, const float* y, float* out,
-               const double* scal, int it, double target, cudaStream_t s) {
+               Gate gate, cudaStream_t s) {
     count_launch();
     switch (L) {
-        case 2: k_amg_mv<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
-        case 4: k_amg_mv<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
-        case 8: k_amg_mv<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
-        case 16: k_amg_mv<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
-        default: k_amg_mv<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, y, out, scal, it, target); break;
+        case 2: k_amg_mv<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
+        case 4: k_amg_mv<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
+        case 8: k_amg_mv<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
+        case 16: k_amg_mv<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
+        default: k_amg_mv<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
     }
 }
 
 inline int grid_for(long long threads) {
-    static int cap = 0;
-    if (cap == 0) {
+    static const int cap = [] {  // initialised once, also under concurrent host threads
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cap = 16 * (sms > 0 ? sms : 148);
-    }
+        return 16 * (sms > 0 ? sms : 148);
+    }();
     const long long b = (threads + kBlock - 1) / kBlock;
     return (int)(b < cap ? (b > 0 ? b : 1) : cap);
 }
@@ -283,10 +274,9 @@ int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* a
         if (l + 2 < g.levels) tryChoice(&g.lev[l + 1].a_lanes, kCand, 5);
     }
     // the kept kernels' own times, for the record
-    const double* noScal = nullptr;  // target < 0: the kernels never read it
     if (fineMs) {
         const int slices = (slots + 31) / 32;
-        *fineMs = time_launches([&] { launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, noScal, 0, -1.0, s); },
+        *fineMs = time_launches([&] { launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, open_gate(), s); },
                                 kTrials, s, e0, e1);
     }
     for (int l = 0; l + 1 < g.levels; l++) {
@@ -294,11 +284,11 @@ int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* a
         AmgDevLevel& C = g.lev[l + 1];
         if (rMs)
             rMs[l] = time_launches(
-                [&] { launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, l == 0 ? g.t0 : L.t, C.b, noScal, 0, -1.0, s); },
+                [&] { launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, l == 0 ? g.t0 : L.t, C.b, open_gate(), s); },
                 kTrials, s, e0, e1);
         if (aMs && l + 2 < g.levels)
             aMs[l + 1] = time_launches(
-                [&] { launch_csr(C.a_lanes, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, noScal, 0, -1.0, s); },
+                [&] { launch_csr(C.a_lanes, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, open_gate(), s); },
                 kTrials, s, e0, e1);
     }
     cudaEventDestroy(e0);
@@ -308,31 +298,30 @@ int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* a
 
 void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s) {
     const int slices = (slots + 31) / 32;
-    launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, v.scal, 0, -1.0, s);
+    launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, open_gate(), s);
 }
 
 void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s) {
-    const double* scal = v.scal;
-    // level 0: b = r, output u
+    const Gate gate = make_gate(v, it, target);
+    // level 0: b = r, output u (its rows: at most the slots in use)
     const int slices = (slots + 31) / 32;
     count_launch();
-    k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.r, v.d, g.y0, scal, it, target);
+    k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.count, v.r, v.d, g.y0, gate);
     if (g.levels > 1) {
-        launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, scal, it, target, s);
+        launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, gate, s);
         // down: restrict, smooth, residual
         for (int l = 0; l + 1 < g.levels; l++) {
             const AmgDevLevel& L = g.lev[l];
             const AmgDevLevel& C = g.lev[l + 1];
             const float* t = l == 0 ? g.t0 : L.t;
-            launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, scal, it, target, s);
+            launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, gate, s);
             if (l + 1 == g.levels - 1) {
                 count_launch();
-                k_amg_dense<<<grid_for((long long)C.n * 32), kBlock, 0, s>>>(C.n, g.coarse_inv, C.b, C.x, scal, it,
-                                                                             target);
+                k_amg_dense<<<grid_for((long long)C.n * 32), kBlock, 0, s>>>(C.n, g.coarse_inv, C.b, C.x, gate);
             } else {
                 count_launch();
-                k_amg_jacobi<<<grid_for(C.n), kBlock, 0, s>>>(C.n, C.b, C.diag, C.y, scal, it, target);
-                launch_csr(C.a_lanes, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, scal, it, target, s);
+                k_amg_jacobi<<<grid_for(C.n), kBlock, 0, s>>>(C.n, nullptr, C.b, C.diag, C.y, gate);
+                launch_csr(C.a_lanes, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, gate, s);
             }
         }
         // up: prolong, post-smooth
@@ -341,16 +330,16 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
             const AmgDevLevel& C = g.lev[l + 1];
             float* y = l == 0 ? g.y0 : L.y;
             count_launch();
-            k_amg_prolong<<<grid_for(L.n), kBlock, 0, s>>>(L.n, L.p_ptr, L.p_col, L.p_val, C.x, y, scal, it, target);
+            k_amg_prolong<<<grid_for(L.n), kBlock, 0, s>>>(L.n, L.p_ptr, L.p_col, L.p_val, C.x, y, gate);
             if (l == 0) {
-                launch_fine(g.fine_unroll, v, slices, v.r, g.y0, v.u, 1, scal, it, target, s);
+                launch_fine(g.fine_unroll, v, slices, v.r, g.y0, v.u, 1, gate, s);
             } else {
-                launch_csr(L.a_lanes, L.n, L.a_ptr, L.a_col, L.a_val, L.diag, L.b, L.y, L.x, 1, scal, it, target, s);
+                launch_csr(L.a_lanes, L.n, L.a_ptr, L.a_col, L.a_val, L.diag, L.b, L.y, L.x, 1, gate, s);
             }
         }
     } else {
         // a single level: Jacobi twice (y, then the post-smoothing step)
-        launch_fine(g.fine_unroll, v, slices, v.r, g.y0, v.u, 1, scal, it, target, s);
+        launch_fine(g.fine_unroll, v, slices, v.r, g.y0, v.u, 1, gate, s);
     }
 }
 

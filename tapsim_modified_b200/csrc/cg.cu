@@ -68,8 +68,10 @@ __global__ void k_vcg_init(VSys v, int slots, int jacobi) {
 // w = A u over SELL-32 slices; delta -> scal[4*it+1] (it = iteration whose
 // u this is), and with withGamma gamma = r.u -> scal[4*it]; skipped once
 // iteration it has converged (cg_done)
-__global__ void k_vcg_spmv(VSys v, int slices, int it, double target, int withGamma) {
-    if (it >= 0 && cg_done(v.scal, it, target)) return;
+__global__ void k_vcg_spmv(VSys v, int slices, Gate gate, int withGamma) {
+    if (gate.done()) return;
+    const int it = gate.iter();
+    slices = min(slices, (*v.count + 31) / 32);  // the slots in use
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     double dl = 0.0, gl = 0.0;
@@ -103,7 +105,7 @@ __global__ void k_vcg_spmv(VSys v, int slices, int it, double target, int withGa
         dl += (double)w * (double)u;
         if (withGamma) gl += (double)v.r[s] * (double)u;
     }
-    const int at = 4 * (it < 0 ? 0 : it);
+    const int at = 4 * it;
     if (withGamma) block_sum2_atomic<kBlock>(dl, gl, &v.scal[at + 1], &v.scal[at]);
     else block_sum_atomic<kBlock>(dl, &v.scal[at + 1]);
 }
@@ -111,8 +113,10 @@ __global__ void k_vcg_spmv(VSys v, int slices, int it, double target, int withGa
 // p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s,
 // rho_{it+1} = r.r; with the Jacobi preconditioner also u = r / d and
 // gamma_{it+1} = r.u
-__global__ void k_vcg_update(VSys v, int slots, int it, double target, int jacobi) {
-    if (cg_done(v.scal, it, target)) return;
+__global__ void k_vcg_update(VSys v, int slots, Gate gate, int jacobi) {
+    if (gate.done()) return;
+    const int it = gate.iter();
+    slots = min(slots, (*v.count + 31) & ~31);  // the slots in use, in whole slices
     double alpha, beta;
     cg_coeffs(v.scal, it, &alpha, &beta);
     if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[4 * it + 2] = alpha;
@@ -135,6 +139,13 @@ __global__ void k_vcg_update(VSys v, int slots, int it, double target, int jacob
     }
     block_sum2_atomic<kBlock>(g, rr, &v.scal[4 * (it + 1)], &v.scal[4 * (it + 1) + 3]);
 }
+
+// the replayed CG iterations' counter and target
+__global__ void k_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2) {
+    *iter = 0;
+    *rel2Dev = rel2;
+}
+__global__ void k_vcg_replay_step(int32_t* iter) { *iter += 1; }
 
 // phi64[node] += x[slot] (and hist[slot] += x[slot] when recording);
 // clears the slot's vectors
@@ -334,34 +345,21 @@ __global__ void k_vcg64_apply(DevMesh m, VSys v, int slots, int record) {
     v.x[s] = v.r[s] = v.u[s] = v.w[s] = v.p[s] = v.sv[s] = 0.0f;
 }
 
-// FP64 residual of the V rows, sum r^2 into *acc; with bacc also the
-// squared norm of the Dirichlet part b_i = sum over Dirichlet neighbours
-// c_ij phi_j - q_i into *bacc (k_bnorm's value, from the same pass over the
-// row).  The rows are walked in node order (the compact list, whose CSR rows
-// neighbouring threads then read from neighbouring memory) and each result
-// is written to its slot; padding slots keep r = 0.
-__global__ void k_vcg_residual(DevMesh m, VSys v, const int32_t* __restrict__ rows, int count, double* acc,
-                               double* bacc, double* r64, double* b64) {
-    double r2 = 0.0, b2 = 0.0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-        const int i = rows[t];
-        double sum = 0.0, sb = 0.0;
-        for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
-            const int j = m.col[q];
-            const double c = m.ceff64[q] * m.phi64[j];
-            sum += c;
-            if (bacc && (m.flags[j] & F_DIRICHLET)) sb += c;
-        }
-        const double r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
-        const double b = sb - m.q64[i];
-        b2 += b * b;
-        v.r[v.slot_of[i]] = (float)r;
-        if (r64) r64[i] = r;
-        if (b64) b64[i] = b;
-        r2 += r * r;
+// One row's FP64 residual r and Dirichlet part b, summed as the full pass
+// (k_residual, relax.cu) sums them: in CSR order, products and sums
+// unfused, so that a value kept from a full pass and one recomputed here
+// agree to the bit when the row is unchanged.
+__device__ void resid_row(const DevMesh& m, int i, double& r, double& b) {
+    double s = 0.0, sb = 0.0;
+    for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
+        const int j = m.col[q];
+        const double c = __dmul_rn(m.ceff64[q], m.phi64[j]);
+        s = __dadd_rn(s, c);
+        if (m.flags[j] & F_DIRICHLET) sb = __dadd_rn(sb, c);
     }
-    if (bacc) block_sum2_atomic<kBlock>(r2, b2, acc, bacc);
-    else block_sum_atomic<kBlock>(r2, acc);
+    const double qi = m.q64[i];
+    r = __dsub_rn(__dsub_rn(s, __dmul_rn(m.diag64[i], m.phi64[i])), qi);
+    b = __dsub_rn(sb, qi);
 }
 
 // Residuals of the rows that removals have changed since the last full
@@ -387,15 +385,8 @@ __global__ void k_residual_rows(DevMesh m, VSys v, float* rN, const int32_t* __r
         const int i = k < 0 ? f : m.col[q0 + k];
         if (m.flags[i] & F_DIRICHLET) continue;
         if (atomicExch(stamp + i, epoch) == epoch) continue;
-        double sum = 0.0, sb = 0.0;
-        for (int q = m.row_ptr[i]; q < m.row_ptr[i + 1]; q++) {
-            const int j = m.col[q];
-            const double c = m.ceff64[q] * m.phi64[j];
-            sum += c;
-            if (m.flags[j] & F_DIRICHLET) sb += c;
-        }
-        const double r = sum - m.diag64[i] * m.phi64[i] - m.q64[i];
-        const double b = sb - m.q64[i];
+        double r, b;
+        resid_row(m, i, r, b);
         const double r0 = r64[i], b0 = b64[i];
         r64[i] = r;
         b64[i] = b;
@@ -541,12 +532,11 @@ inline int blocks(int n) { return (n + kBlock - 1) / kBlock; }
 // of one per 256 rows.  The SpMV keeps one warp per slice over the full
 // grid: slices differ in width, and many small blocks balance them.
 inline int reduce_blocks(int n) {
-    static int cap = 0;
-    if (cap == 0) {
+    static const int cap = [] {  // initialised once, also under concurrent host threads
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cap = 8 * (sms > 0 ? sms : 148);
-    }
+        return 8 * (sms > 0 ? sms : 148);
+    }();
     const int b = blocks(n);
     return b < cap ? b : cap;
 }
@@ -560,14 +550,22 @@ void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withG
     const int slices = (slots + 31) / 32;
     if (slices > 0) {
         count_launch();
-        k_vcg_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, it, target, withGamma ? 1 : 0);
+        k_vcg_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, make_gate(v, it, target), withGamma ? 1 : 0);
     }
 }
 void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s) {
     if (slots > 0) {
         count_launch();
-        k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, it, target, jacobi ? 1 : 0);
+        k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, make_gate(v, it, target), jacobi ? 1 : 0);
     }
+}
+void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, cudaStream_t s) {
+    count_launch();
+    k_vcg_replay_begin<<<1, 1, 0, s>>>(iter, rel2Dev, rel2);
+}
+void launch_vcg_replay_step(int32_t* iter, cudaStream_t s) {
+    count_launch();
+    k_vcg_replay_step<<<1, 1, 0, s>>>(iter);
 }
 void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s) {
     if (slots > 0) { count_launch(); k_vcg_apply<<<blocks(slots), kBlock, 0, s>>>(m, v, slots, record ? 1 : 0); }
@@ -611,10 +609,9 @@ void launch_vcg64_apply(const DevMesh& m, const VSys& v, int slots, bool record,
 }
 void launch_vcg_residual(const DevMesh& m, const VSys& v, const int32_t* rows, int count, double* acc, double* bacc,
                          cudaStream_t s, double* r64, double* b64) {
-    if (count > 0) {
-        count_launch();
-        k_vcg_residual<<<reduce_blocks(count), kBlock, 0, s>>>(m, v, rows, count, acc, bacc, r64, bacc ? b64 : nullptr);
-    }
+    // the residual pass of relax.cu, writing each row's float residual to
+    // its slot of the V system
+    launch_residual(m, rows, count, v.r, acc, s, bacc, r64, b64, v.slot_of);
 }
 void launch_residual_rows(const DevMesh& m, const VSys& v, float* rN, const int32_t* flips, int count, int32_t* stamp,
                           int epoch, double* r64, double* b64, double* rsum, cudaStream_t s, const int32_t* countDev) {

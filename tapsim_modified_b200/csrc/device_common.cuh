@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace tgd {
 
 // Makes device dev current for a scope (dev < 0: leaves the current device
@@ -145,5 +147,22 @@ __device__ __forceinline__ void block_max_atomic_u64(unsigned long long v, unsig
     }
     __syncthreads();
 }
+
+// Runs f() (a cudaError_t-returning setup such as cudaFuncSetAttribute,
+// which holds per device) the first time it is reached with each current
+// device 0..63; `done` is the caller's bit set of devices already set up.
+// Concurrent first calls may both run f, which must be idempotent.
+template <class F>
+inline cudaError_t once_per_device(std::atomic<uint64_t>& done, F f) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = dev >= 0 && dev < 64 ? (1ull << dev) : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = f();
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+    return e;
+}
+
 
 }  // namespace tgd

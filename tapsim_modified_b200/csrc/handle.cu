@@ -58,7 +58,13 @@ void set_process_error(const std::string& msg) { g_error = msg; }
 
 namespace tgd {
 static std::atomic<long long> g_launches(0);
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// while a thread captures a CUDA graph, its launches are counted here (they
+// run when the graph is replayed, which counts them then)
+static thread_local long long* t_captured = nullptr;
+void count_launch() {
+    if (t_captured) ++*t_captured;
+    else g_launches.fetch_add(1, std::memory_order_relaxed);
+}
 long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace tgd
 
@@ -191,6 +197,19 @@ struct tg_handle {
     DBuf<uint8_t> snapFlags;
     DBuf<int8_t> snapType;
     DBuf<float> normalBuf;
+    // One CG iteration of the multigrid solve (update, V-cycle, SpMV and the
+    // step of the device iteration counter) captured as a CUDA graph and
+    // replayed once per iteration: its kernels take the iteration index,
+    // target and slot count from device memory (VSys::iter, rel2, count).
+    // Captured again when the V system's or the hierarchy's device state
+    // (pointers, schedules) differs from the one it was captured with.
+    int launchMode = 1;                  // 1: replay the graph; 0: launch each kernel
+    cudaStream_t captureStream = nullptr;
+    cudaGraphExec_t iterExec = nullptr;
+    DBuf<int32_t> iterDev;               // [1] the replayed iterations' counter
+    DBuf<double> rel2Dev;                // [1] their relative target
+    std::vector<uint64_t> iterKey;       // the device state it was captured with
+    long long iterNodes = 0;             // kernels in one replay
     int lastItersJacobi = 16, lastItersAmg = 4;  // iterations of the last inner solves
     int lastItersCgV = 16, lastItersCgN = 16;
 
@@ -211,7 +230,7 @@ struct tg_handle {
     }
 
     VSys vs() {
-        VSys v;
+        VSys v{};
         v.slot_of = vSlotOf.p;
         v.node_of = vNodeOf.p;
         v.slice_start = vSliceStart.p;
@@ -243,6 +262,8 @@ struct tg_handle {
             v.s64 = vVec64.p + 4 * stride;
             v.w64 = vVec64.p + 5 * stride;
         }
+        v.iter = nullptr;
+        v.rel2 = nullptr;
         return v;
     }
 
@@ -868,6 +889,10 @@ void tg_destroy(tg_handle* h) {
         cudaStreamSynchronize(h->auxStream);
         cudaStreamDestroy(h->auxStream);
     }
+    if (h->iterExec) cudaGraphExecDestroy(h->iterExec);
+    if (h->captureStream) cudaStreamDestroy(h->captureStream);
+    h->iterDev.release();
+    h->rel2Dev.release();
     if (h->evSnap) cudaEventDestroy(h->evSnap);
     if (h->evNormal) cudaEventDestroy(h->evNormal);
     h->snapFlags.release();
@@ -911,6 +936,12 @@ int tg_timer_stop(tg_handle* h, float* ms) {
 }
 
 int64_t tg_launch_count(const tg_handle*) { return (int64_t)launches_so_far(); }
+
+int tg_set_launch_mode(tg_handle* h, int32_t mode) {
+    if (!h || mode < 0 || mode > 1) return fail(h, TG_ERR_ARGUMENT, "tg_set_launch_mode: mode 0 or 1");
+    h->launchMode = mode;
+    return TG_OK;
+}
 
 int tg_bench_kernel(tg_handle* h, int32_t which, int32_t iters, float* avg_ms, double* bytes) {
     DeviceScope dev_scope(h);
@@ -1312,6 +1343,62 @@ static int amg_setup(tg_handle* h, double* seconds) {
 // V-cycle as the preconditioner instead of the diagonal.
 // fp64: the FP64 iterations (multigrid only), their right-hand side taken
 // from the kept FP64 residuals by node.
+// Every pointer, size and schedule that the replayed iteration's kernels
+// take as parameters, field by field.
+static std::vector<uint64_t> iteration_key(const VSys& v, const AmgDev& g, int capacity) {
+    std::vector<uint64_t> k;
+    auto p = [&](const void* q) { k.push_back((uint64_t)(uintptr_t)q); };
+    auto i = [&](long long x) { k.push_back((uint64_t)x); };
+    p(v.slot_of); p(v.node_of); p(v.slice_start); p(v.slice_width); p(v.col); p(v.val); p(v.val16); p(v.g);
+    p(v.vpos); p(v.d); p(v.x); p(v.r); p(v.u); p(v.w); p(v.p); p(v.sv); p(v.hist); p(v.scal); p(v.count);
+    p(v.iter); p(v.rel2); i(v.capacity); i(capacity);
+    i(g.levels); p(g.y0); p(g.t0); p(g.coarse_inv); i(g.fine_unroll);
+    for (int l = 0; l < g.levels && l < kAmgMaxLevels; l++) {
+        const AmgDevLevel& L = g.lev[l];
+        i(L.n); i(L.a_lanes); i(L.r_lanes);
+        p(L.a_ptr); p(L.a_col); p(L.a_val); p(L.diag); p(L.p_ptr); p(L.p_col); p(L.p_val);
+        p(L.r_ptr); p(L.r_col); p(L.r_val); p(L.b); p(L.y); p(L.x); p(L.t);
+    }
+    return k;
+}
+
+// The replayed CG iteration of the multigrid solve for the V system as it
+// is now (captured anew when its device state changed); vg: the VSys whose
+// kernels read the iteration index, target and slot count on the device.
+static int iteration_graph(tg_handle* h, const VSys& vg) {
+    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vCapacity);
+    if (h->iterExec && key == h->iterKey) return TG_OK;
+    if (h->iterExec) {
+        CK(cudaGraphExecDestroy(h->iterExec));
+        h->iterExec = nullptr;
+    }
+    if (!h->captureStream) CK(cudaStreamCreateWithFlags(&h->captureStream, cudaStreamNonBlocking));
+    // grids for every slot the V system can hold; the kernels stop at the
+    // slots in use (*count)
+    const int cap = h->vCapacity;
+    long long nodes = 0;
+    t_captured = &nodes;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->captureStream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        launch_vcg_update(vg, cap, 0, -1.0, false, h->captureStream);
+        launch_amg_vcycle(vg, cap, h->amg, 1, -1.0, h->captureStream);
+        launch_vcg_spmv(vg, cap, 1, -1.0, true, h->captureStream);
+        launch_vcg_replay_step(h->iterDev.p, h->captureStream);
+        e = cudaStreamEndCapture(h->captureStream, &graph);
+    }
+    t_captured = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->iterExec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        h->iterExec = nullptr;
+        return cuda_check(h, e, "tg_solve: CG iteration graph");
+    }
+    h->iterNodes = nodes;
+    h->iterKey.swap(key);
+    return TG_OK;
+}
+
 static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersOut, bool fp64 = false) {
     const size_t need = 4 * (size_t)(maxIter + 2);
     if (h->vScal.n < need) CK(h->vScal.alloc(need));
@@ -1331,6 +1418,18 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
     // FP64 test uses: rho_it <= rtol^2 rho_0, tested by the kernels
     // themselves, so the iterations queue before rho_0 is read back
     const double rel2 = rtol * rtol;
+    // the multigrid FP32 iterations replay one captured iteration
+    const bool replay = amg && !fp64 && h->launchMode == 1 && slots > 0;
+    if (replay) {
+        if (!h->iterDev.p) CK(h->iterDev.alloc(1));
+        if (!h->rel2Dev.p) CK(h->rel2Dev.alloc(1));
+        VSys vg = v;
+        vg.iter = h->iterDev.p;
+        vg.rel2 = h->rel2Dev.p;
+        const int rc = iteration_graph(h, vg);
+        if (rc != TG_OK) return rc;
+        launch_vcg_replay_begin(h->iterDev.p, h->rel2Dev.p, rel2, h->stream);
+    }
     int it = 0;
     // iterations queued before the first read: about as many as the last
     // solve took; then small batches
@@ -1345,6 +1444,11 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
                 launch_vcg64_update(v, slots, it, rel2, h->stream);
                 launch_amg_vcycle(v, slots, h->amg, it + 1, rel2, h->stream);
                 launch_vcg64_spmv(v, slots, it + 1, rel2, h->stream);
+                continue;
+            }
+            if (replay) {
+                CK(cudaGraphLaunch(h->iterExec, h->stream));
+                g_launches.fetch_add(h->iterNodes, std::memory_order_relaxed);
                 continue;
             }
             launch_vcg_update(v, slots, it, rel2, !amg, h->stream);

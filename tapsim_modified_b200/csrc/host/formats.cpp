@@ -77,6 +77,7 @@ std::string read_node_file(const std::string& path, NodeFile* out) {
     out->xyz.assign(3 * n, 0.0f);
     out->id.assign(n, -1);
     out->number.assign(n, 0);
+    out->has_numbers = withNumbers != 0;
     out->phi.assign(withPotentials ? n : 0, 0.0f);
     for (long i = 0; i < n; i++) {
         if (ascii) {

@@ -21,7 +21,8 @@ namespace tg_host {
 struct NodeFile {
     std::vector<float> xyz;
     std::vector<short> id;
-    std::vector<uint32_t> number;  // empty when the file carries no numbers
+    std::vector<uint32_t> number;  // read, or assigned as readGeomGrid does
+    bool has_numbers = false;      // the file carries numbers
     std::vector<float> phi;        // empty when the file carries no potentials
 };
 

@@ -12,6 +12,7 @@
 #include "../../../include/tapsim_gpu.h"
 #include "delaunay.h"
 #include "formats.h"
+#include "samplegen.h"
 #include "tipgen.h"
 #include "voronoi.h"
 
@@ -138,9 +139,124 @@ ConfigTable default_tip_config() {
     return ct;
 }
 
+// The configuration template meshgen writes beside its node file
+// (writeConfig, meshgen/meshgen.cpp:491-595): vacuum; top and sides
+// Dirichlet at 0 V; bottom Neumann; every other id in the node set a
+// removable Dirichlet cell at 1000 V and charge state 1, whose mass and
+// evaporation field (left for the user to fill in there) are 0 here.
+ConfigTable sample_config_template(const SampleParams& sp, const std::vector<short>& ids) {
+    ConfigTable ct;
+    auto add = [&](int id, const char* name, bool rem, bool neu, bool dir, float phi, short q, float energy) {
+        CellType t;
+        t.id = id;
+        t.name = name;
+        t.removable = rem;
+        t.neumann = neu;
+        t.dirichlet = dir;
+        t.phi = phi;
+        t.evap_charge = q;
+        t.evap_energy = energy;
+        ct.types[id] = t;
+    };
+    add(sp.vacuum_id, "Vacuum", false, false, false, 0.0f, 0, 0.0f);
+    add(sp.top_id, "Top", false, false, true, 0.0f, 0, 0.0f);
+    add(sp.bottom_id, "Bottom", false, true, false, 1000.0f, 0, 0.0f);
+    add(sp.sides_id, "Sides", false, false, true, 0.0f, 0, 0.0f);
+    for (short id : ids)
+        if (!ct.types.count(id)) add(id, "Sample", true, false, true, 1000.0f, 1, 1.0f);
+    return ct;
+}
+
 }  // namespace
 
 extern "C" {
+
+void tg_sample_params_default(tg_sample_params* p) {
+    SampleParams d;
+    p->box_half_width = d.box_half_width;
+    p->box_height = d.box_height;
+    p->fine_shell = d.fine_shell;
+    p->exclusion = d.exclusion;
+    p->layers_per_level = d.layers_per_level;
+    p->coarsen = d.coarsen;
+    p->max_spacing = d.max_spacing;
+    p->vacuum_id = d.vacuum_id;
+    p->top_id = d.top_id;
+    p->bottom_id = d.bottom_id;
+    p->sides_id = d.sides_id;
+    p->seed = d.seed;
+}
+
+int tg_mesh_from_sample(const char* sampleFile, const char* configFile, const tg_sample_params* p, int32_t threads,
+                        tg_mesh** out) {
+    if (!sampleFile || !p || !out) return mesh_fail("tg_mesh_from_sample: null argument");
+    NodeFile nf;
+    std::string err = read_node_file(sampleFile, &nf);
+    if (!err.empty()) return mesh_fail(err);
+    SampleParams sp;
+    sp.box_half_width = p->box_half_width;
+    sp.box_height = p->box_height;
+    sp.fine_shell = p->fine_shell;
+    sp.exclusion = p->exclusion;
+    sp.layers_per_level = p->layers_per_level;
+    sp.coarsen = p->coarsen;
+    sp.max_spacing = p->max_spacing;
+    sp.vacuum_id = p->vacuum_id;
+    sp.top_id = p->top_id;
+    sp.bottom_id = p->bottom_id;
+    sp.sides_id = p->sides_id;
+    sp.seed = p->seed;
+    const int nThreads = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    SampleMesh sm;
+    err = generate_sample_mesh(nf.xyz, nf.id, sp, nThreads, &sm);
+    if (!err.empty()) return mesh_fail(err);
+    tg_mesh* m = new tg_mesh();
+    if (configFile) {
+        err = read_config(configFile, &m->config);
+        if (!err.empty()) {
+            delete m;
+            return mesh_fail(err);
+        }
+    } else {
+        m->config = sample_config_template(sp, nf.id);
+    }
+    fill_types(m);
+    const int n = (int)sm.id.size();
+    const int nGen = n - sm.num_sample;
+    m->xyz.swap(sm.xyz);
+    m->type.resize(n);
+    m->phi.resize(n);
+    m->number.resize(n);
+    // numbers as readGeomGrid gives them to meshgen's output
+    // (file_io.cpp:975-1000): the sample keeps the numbers its file carries
+    // and the generated nodes before it count on from the largest; without
+    // numbers in the file every node is numbered in node order
+    uint32_t next = 1;
+    if (nf.has_numbers)
+        for (uint32_t v : nf.number) next = std::max(next, v + 1);
+    for (int i = 0; i < n; i++) {
+        if (sm.id[i] < -128 || sm.id[i] > 127) {
+            delete m;
+            return mesh_fail("tg_mesh_from_sample: type id outside -128..127");
+        }
+        m->type[i] = (int8_t)sm.id[i];
+        auto it = m->config.types.find(m->type[i]);
+        if (it == m->config.types.end()) {
+            delete m;
+            return mesh_fail("tg_mesh_from_sample: node type missing from the configuration");
+        }
+        const bool sample = i >= nGen;
+        m->phi[i] = sample && !nf.phi.empty() ? nf.phi[i - nGen] : it->second.phi;
+        m->number[i] = !nf.has_numbers ? (uint32_t)(i + 1) : sample ? nf.number[i - nGen] : next++;
+    }
+    const int rc = build_from_points(m, nThreads, sp.seed);
+    if (rc != TG_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return TG_OK;
+}
 
 void tg_tip_params_default(tg_tip_params* p) {
     TipParams d;

@@ -18,6 +18,25 @@
 
 namespace tg_host {
 
+// SplitMix64 finaliser (the point jitter of the generated meshes)
+inline uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Uniform in [0,1) from a hash of (seed, a, b, c, d, e).
+inline double hash_unit(uint64_t seed, int64_t a, int64_t b, int64_t c, int64_t d, int64_t e) {
+    uint64_t h = mix64(seed);
+    h = mix64(h ^ (uint64_t)a);
+    h = mix64(h ^ (uint64_t)b);
+    h = mix64(h ^ (uint64_t)c);
+    h = mix64(h ^ (uint64_t)d);
+    h = mix64(h ^ (uint64_t)e);
+    return (double)(h >> 11) * (1.0 / 9007199254740992.0);
+}
+
 struct TipParams {
     double lattice_a = 0.2866e-9;      // bcc lattice constant [m]
     double cap_radius = 5e-9;          // R [m]

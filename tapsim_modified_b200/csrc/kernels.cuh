@@ -100,7 +100,34 @@ struct VSys {
     // every write of those once allocated), and the CG vectors in FP64
     double* val64;
     double *d64, *x64, *r64, *p64, *s64, *w64;
+    // CG iterations replayed from a CUDA graph: the iteration index counts
+    // from the device counter *iter and the relative target is *rel2 (both
+    // null when the host launches each iteration with its own values); the
+    // iteration kernels take their rows up to *count rounded up to whole
+    // slices, the host's count of the slots in use
+    const int32_t* iter;
+    const double* rel2;
 };
+// Early exit of the kernels of CG iteration `it` (cg.cu, amg.cu): they do
+// nothing once rho_it <= rel2 * rho_0 (rel2 < 0: never), so that
+// iterations queue before the host has seen rho_0.  With itBase the index
+// is it + *itBase, and with rel2Dev the target is *rel2Dev (an iteration
+// replayed from a CUDA graph).
+struct Gate {
+    const double* scal;
+    int it;
+    double rel2;
+    const int32_t* itBase;
+    const double* rel2Dev;
+    __device__ __forceinline__ int iter() const { return itBase ? it + *itBase : it; }
+    __device__ __forceinline__ bool done() const {
+        const double t = rel2Dev ? *rel2Dev : rel2;
+        return t >= 0.0 && scal[4 * iter() + 3] <= t * scal[3];
+    }
+};
+inline Gate make_gate(const VSys& v, int it, double rel2) { return Gate{v.scal, it, rel2, v.iter, v.rel2}; }
+// a gate that never closes (timing and setup launches)
+inline Gate open_gate() { return Gate{nullptr, 0, -1.0, nullptr, nullptr}; }
 // jacobi: the Jacobi preconditioner (u = r / d inside init / update);
 // otherwise u comes from launch_amg_vcycle and the SpMV adds gamma = r.u.
 // `target` of the iteration kernels (and of the V-cycle) is relative: they
@@ -108,6 +135,10 @@ struct VSys {
 void launch_vcg_init(const VSys& v, int slots, bool jacobi, cudaStream_t s);
 void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withGamma, cudaStream_t s);
 void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s);
+// the counter and target of iterations replayed from a CUDA graph: set to
+// 0 and rel2 before the first replay, stepped by 1 at the end of each
+void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, cudaStream_t s);
+void launch_vcg_replay_step(int32_t* iter, cudaStream_t s);
 // FP64 inner iterations with the multigrid preconditioner: the V-cycle runs
 // in FP32 on r rounded to float and its u enters the FP64 recurrences
 // exactly.  init64 takes the right-hand side from the FP64 residual by node
@@ -189,8 +220,10 @@ void launch_sweep64(const DevMesh& m, const int32_t* rows, int count, double* ma
 // stores r as float into r32
 // with bacc, also the squared norm of the rows' Dirichlet part (as
 // launch_bnorm) into *bacc
+// slotOf (may be null): r32 is indexed by slotOf[i] instead of i
 void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r32, double* acc, cudaStream_t s,
-                     double* bacc = nullptr, double* r64 = nullptr, double* b64 = nullptr);
+                     double* bacc = nullptr, double* r64 = nullptr, double* b64 = nullptr,
+                     const int32_t* slotOf = nullptr);
 // b_i = sum over Dirichlet neighbours c_ij phi_j - q_i; sum b^2 into *acc
 void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s);
 // FP32 conjugate gradients on the rows of one list (Jacobi preconditioner)

@@ -534,14 +534,14 @@ bool gemm_shape_ok(int M, int N, int K) { return M > 0 && M % 128 == 0 && (N == 
 
 cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int* status,
                              cudaStream_t s) {
-    static bool attrSet = false;
-    if (!attrSet) {
-        cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_gemm_bf16<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
-        if (e != cudaSuccess) return e;
-        attrSet = true;
-    }
+    static std::atomic<uint64_t> attrSet{0};
+    cudaError_t e = once_per_device(attrSet, [] {
+        cudaError_t r = cudaFuncSetAttribute(k_gemm_bf16<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(k_gemm_bf16<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        return r;
+    });
+    if (e != cudaSuccess) return e;
     const auto* a = static_cast<const __nv_bfloat16*>(A);
     const auto* b = static_cast<const __nv_bfloat16*>(B);
     count_launch();
@@ -631,12 +631,11 @@ void launch_apply_prediction(const DevMesh& m, const int32_t* nodes, const int32
 void launch_local_refine(const DevMesh& m, const int32_t* nodes, const int32_t* count, int cap, int sweeps,
                          float omega, const int32_t* slotOf, float* hist, cudaStream_t s) {
     if (sweeps <= 0 || cap <= 0 || cap > kRefineMax) return;
-    static bool opted = false;
-    if (!opted) {
-        cudaFuncSetAttribute(k_local_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(2 * sizeof(double) * kRefineMax));
-        opted = true;
-    }
+    static std::atomic<uint64_t> opted{0};
+    once_per_device(opted, [] {
+        return cudaFuncSetAttribute(k_local_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(2 * sizeof(double) * kRefineMax));
+    });
     count_launch();
     k_local_refine<<<1, 1024, 2 * sizeof(double) * (size_t)cap, s>>>(m, nodes, count, cap, sweeps, omega, slotOf,
                                                                      hist);

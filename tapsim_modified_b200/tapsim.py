@@ -55,6 +55,29 @@ class Mesh:
         N.check(N.lib().tg_mesh_from_files(str(node_file).encode(), str(config_file).encode(), threads, C.byref(h)))
         return cls(h)
 
+    @staticmethod
+    def sample_params(**kw) -> N.tg_sample_params:
+        p = N.tg_sample_params()
+        N.lib().tg_sample_params_default(C.byref(p))
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise KeyError(k)
+            setattr(p, k, v)
+        return p
+
+    @classmethod
+    def from_sample(cls, sample_file: str, config_file: str | None = None, threads: int = 0, **kw) -> "Mesh":
+        """MeshGen's role (meshgen/meshgen.cpp:2506-3986): graded vacuum and
+        the box's marked boundary nodes around the sample in a node file, the
+        sample appended last, then the Delaunay mesh and couplings.  Without
+        config_file the mesh takes meshgen's configuration template
+        (tg_mesh_from_sample)."""
+        h = C.c_void_p()
+        cfg = str(config_file).encode() if config_file else None
+        N.check(N.lib().tg_mesh_from_sample(str(sample_file).encode(), cfg, C.byref(cls.sample_params(**kw)), threads,
+                                            C.byref(h)))
+        return cls(h)
+
     @classmethod
     def from_dump(cls, dump_file: str, config_file: str | None = None) -> "Mesh":
         h = C.c_void_p()
@@ -206,6 +229,11 @@ class Grid:
         o = solve_opts(rel_tol, max_outer, max_inner, inner_rtol, warm_start, preconditioner, inner_precision)
         self._ck(N.lib().tg_solve(self._h, C.byref(o), C.byref(info)))
         return info
+
+    def set_launch_mode(self, mode: int):
+        """1: the multigrid solve replays one captured CG iteration (a CUDA
+        graph); 0: it launches every kernel (tg_set_launch_mode)."""
+        N.check(N.lib().tg_set_launch_mode(self._h, int(mode)), self._h)
 
     def amg_schedule(self) -> list[dict]:
         """Per multigrid level: rows and the tuned lanes per CSR row of its

@@ -73,3 +73,34 @@ def test_tuned_schedules_of_the_hierarchy():
         else:
             assert lv["a_lanes"] == 0
     g.close()
+
+
+def test_replayed_iterations_match_launched_ones(ref_mesh, ref_events):
+    """The multigrid solve's CG iterations replayed from a captured CUDA graph
+    (the default) and launched kernel by kernel give the same events: the
+    same removals, residuals at the tolerance and potentials equal to the
+    solves' own accuracy; the graph's kernels count once per replay."""
+    from tapsim_modified_b200 import _native as N
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
+    out = {}
+    for mode in (0, 1):
+        g = Grid(ref_mesh)
+        g.set_launch_mode(mode)
+        g.solve(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1)
+        ev = Evaporation(g, EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini")), relax_mode=1,
+                         solve=solve_opts(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1,
+                                          warm_start=1))
+        n0 = N.lib().tg_launch_count(g._h)
+        recs = ev.run(12)
+        launches = N.lib().tg_launch_count(g._h) - n0
+        out[mode] = ([r["node"] for r in recs], [r["rel_residual"] for r in recs], g.potentials(), launches)
+        g.close()
+    (n0_, r0, phi0, l0), (n1, r1, phi1, l1) = out[0], out[1]
+    print("launches over 12 events: kernel by kernel", l0, "replayed", l1)
+    assert n0_ == n1 == [int(x) for x in ref_events[:12, 1]]
+    assert max(r0 + r1) <= 1e-10
+    assert np.abs(phi1 - phi0).max() <= 1e-8 * np.abs(phi0).max()
+    # the same kernels run either way (the replay adds one counter step per
+    # iteration and a start per solve; early-exiting kernels count in both)
+    assert 0.8 * l0 <= l1 <= 1.3 * l0
+
