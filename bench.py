@@ -243,7 +243,8 @@ def run_ours(args, rank: int, world: int, dist):
         """Mesh upload, initial relaxation, W warm-up and K timed events with
         the given solve start (and long_run more events timed after them);
         returns the timings and the event records.  The grid stays open."""
-        sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4, warm_start=warm_start,
+        sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=args.inner_rtol,
+                           warm_start=warm_start,
                            preconditioner=PRECOND, inner_precision=inner_precision)
         if dist:
             dist.barrier()
@@ -402,6 +403,7 @@ def run_ours(args, rank: int, world: int, dist):
             "initial_solve": {"outer": info0.outer, "inner": info0.inner, "rel_residual": info0.rel_residual},
             "preconditioner": "smoothed-aggregation multigrid V(1,1)-cycle (tg_solve_opts.preconditioner 1)"
                               if PRECOND == 1 else "Jacobi",
+            "inner_rtol": args.inner_rtol,
             "launch_mode": ("each multigrid CG iteration replayed from one captured CUDA graph" if args.launch_mode == 1
                             else "every kernel launched from the host"),
             "setup": {"seconds": arm["setup_s"], "multigrid_hierarchy_s": info0.setup_seconds,
@@ -562,7 +564,7 @@ def run_many_tips(args, rank: int, world: int, dist):
     # the learned warm start: one network trained once, a copy of it per tip
     # (a learner's graph buffers serve one handle at a time)
     trained, learn_info = (None, None) if args.no_learned else train_learner(args, rank, opts)
-    sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=1e-4,
+    sopts = solve_opts(rel_tol=REL_TOL, max_outer=50, max_inner=20000, inner_rtol=args.inner_rtol,
                        warm_start=0 if trained is None else 2, preconditioner=PRECOND)
     grids, evopts, learners = [], [], []
     t0 = time.perf_counter()
@@ -963,6 +965,8 @@ def main():
     ap.add_argument("--train-events", type=int, default=300, help="events collected for the learned warm start")
     ap.add_argument("--train-steps", type=int, default=600, help="Adam steps of the learned warm start")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
+    ap.add_argument("--inner-rtol", type=float, default=1e-4,
+                    help="the inner solves' least relative reduction per FP64 defect-correction step")
     ap.add_argument("--launch-mode", type=int, default=1, choices=(0, 1),
                     help="1: the multigrid CG iterations replay a captured CUDA graph; 0: kernel by kernel")
     ap.add_argument("--refine", type=int, default=8,

@@ -464,9 +464,10 @@ int tg_timer_stop(tg_handle* h, float* elapsed_ms);
 int64_t tg_launch_count(const tg_handle* h);
 /* How the multigrid solve's FP32 CG iterations reach the device: 1 (the
  * default) replays one iteration (update, V-cycle, SpMV) captured as a CUDA
- * graph, whose kernels read the iteration index, target and slot count from
- * device memory; 0 launches each kernel from the host.  Both run the same
- * kernels on the same data. */
+ * graph, whose kernels read the iteration index and target from device
+ * memory (captured again when the hierarchy or the slots in use change);
+ * 0 launches each kernel from the host.  Both run the same kernels on the
+ * same data. */
 int tg_set_launch_mode(tg_handle* h, int32_t mode);
 /* Times `iters` back-to-back launches of one hot kernel on the handle's
  * stream with CUDA events: 0 = FP32 CG SpMV over the non-Neumann free rows,

@@ -25,10 +25,9 @@ constexpr int kBlock = 256;
 // 7.3M-cell tip where 2/3 took 27
 constexpr float kSmooth = 0.9f;
 
-// y = w b / d over n rows (at most *countDev when given)
-__global__ void k_amg_jacobi(int n, const int32_t* countDev, const float* b, const float* d, float* y, Gate gate) {
+// y = w b / d
+__global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, Gate gate) {
     if (gate.done()) return;
-    if (countDev) n = min(n, (*countDev + 31) & ~31);  // whole slices, padding rows included
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         y[i] = kSmooth * b[i] / d[i];
 }
@@ -45,7 +44,6 @@ __global__ void k_amg_jacobi(int n, const int32_t* countDev, const float* b, con
 template <int U>
 __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, float* out, int mode, Gate gate) {
     if (gate.done()) return;
-    slices = min(slices, (*v.count + 31) / 32);  // the slots in use
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
@@ -303,10 +301,10 @@ void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStr
 
 void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s) {
     const Gate gate = make_gate(v, it, target);
-    // level 0: b = r, output u (its rows: at most the slots in use)
+    // level 0: b = r, output u
     const int slices = (slots + 31) / 32;
     count_launch();
-    k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.count, v.r, v.d, g.y0, gate);
+    k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.r, v.d, g.y0, gate);
     if (g.levels > 1) {
         launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, gate, s);
         // down: restrict, smooth, residual
@@ -320,7 +318,7 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
                 k_amg_dense<<<grid_for((long long)C.n * 32), kBlock, 0, s>>>(C.n, g.coarse_inv, C.b, C.x, gate);
             } else {
                 count_launch();
-                k_amg_jacobi<<<grid_for(C.n), kBlock, 0, s>>>(C.n, nullptr, C.b, C.diag, C.y, gate);
+                k_amg_jacobi<<<grid_for(C.n), kBlock, 0, s>>>(C.n, C.b, C.diag, C.y, gate);
                 launch_csr(C.a_lanes, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, gate, s);
             }
         }

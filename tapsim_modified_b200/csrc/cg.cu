@@ -71,7 +71,6 @@ __global__ void k_vcg_init(VSys v, int slots, int jacobi) {
 __global__ void k_vcg_spmv(VSys v, int slices, Gate gate, int withGamma) {
     if (gate.done()) return;
     const int it = gate.iter();
-    slices = min(slices, (*v.count + 31) / 32);  // the slots in use
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     double dl = 0.0, gl = 0.0;
@@ -116,7 +115,6 @@ __global__ void k_vcg_spmv(VSys v, int slices, Gate gate, int withGamma) {
 __global__ void k_vcg_update(VSys v, int slots, Gate gate, int jacobi) {
     if (gate.done()) return;
     const int it = gate.iter();
-    slots = min(slots, (*v.count + 31) & ~31);  // the slots in use, in whole slices
     double alpha, beta;
     cg_coeffs(v.scal, it, &alpha, &beta);
     if (blockIdx.x == 0 && threadIdx.x == 0) v.scal[4 * it + 2] = alpha;

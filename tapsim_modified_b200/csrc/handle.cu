@@ -199,10 +199,10 @@ struct tg_handle {
     DBuf<float> normalBuf;
     // One CG iteration of the multigrid solve (update, V-cycle, SpMV and the
     // step of the device iteration counter) captured as a CUDA graph and
-    // replayed once per iteration: its kernels take the iteration index,
-    // target and slot count from device memory (VSys::iter, rel2, count).
-    // Captured again when the V system's or the hierarchy's device state
-    // (pointers, schedules) differs from the one it was captured with.
+    // replayed once per iteration: its kernels take the iteration index and
+    // target from device memory (VSys::iter, rel2).  Captured again when the
+    // V system's or the hierarchy's device state (pointers, schedules) or
+    // the slots in use differ from the ones it was captured with.
     int launchMode = 1;                  // 1: replay the graph; 0: launch each kernel
     cudaStream_t captureStream = nullptr;
     cudaGraphExec_t iterExec = nullptr;
@@ -1345,13 +1345,13 @@ static int amg_setup(tg_handle* h, double* seconds) {
 // from the kept FP64 residuals by node.
 // Every pointer, size and schedule that the replayed iteration's kernels
 // take as parameters, field by field.
-static std::vector<uint64_t> iteration_key(const VSys& v, const AmgDev& g, int capacity) {
+static std::vector<uint64_t> iteration_key(const VSys& v, const AmgDev& g, int slots) {
     std::vector<uint64_t> k;
     auto p = [&](const void* q) { k.push_back((uint64_t)(uintptr_t)q); };
     auto i = [&](long long x) { k.push_back((uint64_t)x); };
     p(v.slot_of); p(v.node_of); p(v.slice_start); p(v.slice_width); p(v.col); p(v.val); p(v.val16); p(v.g);
     p(v.vpos); p(v.d); p(v.x); p(v.r); p(v.u); p(v.w); p(v.p); p(v.sv); p(v.hist); p(v.scal); p(v.count);
-    p(v.iter); p(v.rel2); i(v.capacity); i(capacity);
+    p(v.iter); p(v.rel2); i(v.capacity); i(slots);
     i(g.levels); p(g.y0); p(g.t0); p(g.coarse_inv); i(g.fine_unroll);
     for (int l = 0; l < g.levels && l < kAmgMaxLevels; l++) {
         const AmgDevLevel& L = g.lev[l];
@@ -1363,19 +1363,18 @@ static std::vector<uint64_t> iteration_key(const VSys& v, const AmgDev& g, int c
 }
 
 // The replayed CG iteration of the multigrid solve for the V system as it
-// is now (captured anew when its device state changed); vg: the VSys whose
-// kernels read the iteration index, target and slot count on the device.
+// is now: captured anew when its device state or its slots in use changed
+// (removals append rows, a new slice of 32 every 32 rows); vg: the VSys
+// whose kernels read the iteration index and target on the device.
 static int iteration_graph(tg_handle* h, const VSys& vg) {
-    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vCapacity);
+    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vActive);
     if (h->iterExec && key == h->iterKey) return TG_OK;
     if (h->iterExec) {
         CK(cudaGraphExecDestroy(h->iterExec));
         h->iterExec = nullptr;
     }
     if (!h->captureStream) CK(cudaStreamCreateWithFlags(&h->captureStream, cudaStreamNonBlocking));
-    // grids for every slot the V system can hold; the kernels stop at the
-    // slots in use (*count)
-    const int cap = h->vCapacity;
+    const int cap = h->vActive;
     long long nodes = 0;
     t_captured = &nodes;
     cudaGraph_t graph = nullptr;

@@ -102,9 +102,7 @@ struct VSys {
     double *d64, *x64, *r64, *p64, *s64, *w64;
     // CG iterations replayed from a CUDA graph: the iteration index counts
     // from the device counter *iter and the relative target is *rel2 (both
-    // null when the host launches each iteration with its own values); the
-    // iteration kernels take their rows up to *count rounded up to whole
-    // slices, the host's count of the slots in use
+    // null when the host launches each iteration with its own values)
     const int32_t* iter;
     const double* rel2;
 };

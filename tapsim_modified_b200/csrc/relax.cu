@@ -10,8 +10,6 @@
 //   other rows:    the same sums skipping Neumann neighbours
 // The skip is folded into ceff (0 for a Neumann neighbour of a non-Neumann
 // row), so every free row is phi_i = (sum_j ceff_ij phi_j - q_i) / diag_i.
-#include <climits>
-
 #include "kernels.cuh"
 
 namespace tgd {
@@ -50,67 +48,31 @@ __global__ void k_sweep64(DevMesh m, const int32_t* __restrict__ rows, int count
 }
 
 // FP64 residual r_i = sum_j ceff_ij phi_j - diag_i phi_i - q_i of a row
-// list, sum r^2 into *acc; one thread per row, a warp for 32 consecutive
-// rows of the list.  The list runs in node order, so a warp's rows occupy
-// one span of the CSR arrays: the warp first copies that span's columns and
-// couplings into shared memory with coalesced loads (kResidStage entries at
-// most; a longer or scattered span, such as rows appended by removals,
-// reads in place), then each thread sums its own row from there, in CSR
-// order with unfused products and sums (resid_row, which the incremental
-// residuals repeat bit for bit), gathering the potentials.
+// list, sum r^2 into *acc; one thread per row, the row's entries in CSR
+// order with unfused products and sums (resid_row in cg.cu repeats them for
+// the incremental residuals, bit for bit).  One thread per row keeps a
+// row's whole chain of loads in flight per thread; groups of lanes per row,
+// or a warp staging its rows' span in shared memory first, measured slower
+// on the 7.3M-cell tip (2.4 and 3.0 TB/s against 4.1).
 // r32 (may be null) gets r as float, at slotOf[i] when slotOf is given (the
 // V system's slot) and at i otherwise; r64 and b64 (may be null) keep r and
 // the Dirichlet part by node.  With bacc, also the squared norm of the rows'
 // Dirichlet part b_i = sum over Dirichlet neighbours ceff_ij phi_j - q_i
 // (k_bnorm's value) from the same pass.
-constexpr int kResidWarps = 4;
-constexpr int kResidStage = 576;
-__global__ void __launch_bounds__(32 * kResidWarps) k_residual(DevMesh m, const int32_t* __restrict__ rows, int count,
-                                                               float* r32, const int32_t* __restrict__ slotOf,
-                                                               double* acc, double* bacc, double* r64, double* b64) {
-    __shared__ int32_t sCol[kResidWarps][kResidStage];
-    __shared__ double sVal[kResidWarps][kResidStage];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int t = (blockIdx.x * kResidWarps + w) * 32 + lane;
-    const bool live = t < count;
+__global__ void k_residual(DevMesh m, const int32_t* __restrict__ rows, int count, float* r32,
+                           const int32_t* __restrict__ slotOf, double* acc, double* bacc, double* r64, double* b64) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const bool withB = bacc != nullptr;  // uniform over the grid
-    int i = 0, lo = 0, hi = 0;
-    if (live) {
-        i = rows[t];
-        lo = m.row_ptr[i];
-        hi = m.row_ptr[i + 1];
-    }
-    const int base = __reduce_min_sync(0xffffffffu, live ? lo : INT_MAX);
-    const int end = __reduce_max_sync(0xffffffffu, live ? hi : INT_MIN);
-    const bool staged = end >= base && end - base <= kResidStage;  // uniform over the warp
-    if (staged) {
-        for (int k = lane; k < end - base; k += 32) {
-            sCol[w][k] = m.col[base + k];
-            sVal[w][k] = m.ceff64[base + k];
-        }
-        __syncwarp();
-    }
     double r2 = 0.0, b2 = 0.0;
-    if (live) {
+    if (t < count) {
+        const int i = rows[t];
+        const int q0 = m.row_ptr[i], q1 = m.row_ptr[i + 1];
         double s = 0.0, sb = 0.0;
-        if (staged) {
-            const int32_t* cs = sCol[w] - base;
-            const double* vs = sVal[w] - base;
-#pragma unroll 4
-            for (int q = lo; q < hi; q++) {
-                const int j = cs[q];
-                const double c = __dmul_rn(vs[q], m.phi64[j]);
-                s = __dadd_rn(s, c);
-                if (withB && (m.flags[j] & F_DIRICHLET)) sb = __dadd_rn(sb, c);
-            }
-        } else {
-#pragma unroll 4
-            for (int q = lo; q < hi; q++) {
-                const int j = m.col[q];
-                const double c = __dmul_rn(m.ceff64[q], m.phi64[j]);
-                s = __dadd_rn(s, c);
-                if (withB && (m.flags[j] & F_DIRICHLET)) sb = __dadd_rn(sb, c);
-            }
+        for (int q = q0; q < q1; q++) {
+            const int j = m.col[q];
+            const double c = __dmul_rn(m.ceff64[q], m.phi64[j]);
+            s = __dadd_rn(s, c);
+            if (withB && (m.flags[j] & F_DIRICHLET)) sb = __dadd_rn(sb, c);
         }
         const double qi = m.q64[i];
         const double r = __dsub_rn(__dsub_rn(s, __dmul_rn(m.diag64[i], m.phi64[i])), qi);
@@ -121,8 +83,8 @@ __global__ void __launch_bounds__(32 * kResidWarps) k_residual(DevMesh m, const 
         r2 = r * r;
         b2 = b * b;
     }
-    if (withB) block_sum2_atomic<32 * kResidWarps>(r2, b2, acc, bacc);
-    else block_sum_atomic<32 * kResidWarps>(r2, acc);
+    if (withB) block_sum2_atomic<kBlock>(r2, b2, acc, bacc);
+    else block_sum_atomic<kBlock>(r2, acc);
 }
 
 __global__ void k_bnorm(DevMesh m, const int32_t* __restrict__ rows, int count, double* acc) {
@@ -352,8 +314,7 @@ void launch_residual(const DevMesh& m, const int32_t* rows, int count, float* r3
     if (count <= 0) return;
     count_launch();
     b64 = bacc ? b64 : nullptr;
-    const int perBlock = 32 * kResidWarps;
-    k_residual<<<(count + perBlock - 1) / perBlock, perBlock, 0, s>>>(m, rows, count, r32, slotOf, acc, bacc, r64, b64);
+    k_residual<<<blocks(count), kBlock, 0, s>>>(m, rows, count, r32, slotOf, acc, bacc, r64, b64);
 }
 void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc, cudaStream_t s) {
     if (count > 0) { count_launch(); k_bnorm<<<blocks(count), kBlock, 0, s>>>(m, rows, count, acc); }
