@@ -210,6 +210,12 @@ struct tg_handle {
     DBuf<double> rel2Dev;                // [1] their relative target
     std::vector<uint64_t> iterKey;       // the device state it was captured with
     long long iterNodes = 0;             // kernels in one replay
+    // the same for the node-space CG iterations of either row list (run_cg)
+    cudaGraphExec_t cgExec[2] = {nullptr, nullptr};
+    std::vector<uint64_t> cgKey[2];
+    long long cgNodes[2] = {0, 0};
+    DBuf<int32_t> cgIterDev;             // [1] their counter
+    DBuf<double> cgTgtDev;               // [2] their targets rel2, abs2
     int lastItersJacobi = 16, lastItersAmg = 4;  // iterations of the last inner solves
     int lastItersCgV = 16, lastItersCgN = 16;
 
@@ -359,7 +365,7 @@ struct tg_handle {
         return s;
     }
     CGVectors cg(int which) {
-        CGVectors v;
+        CGVectors v{};
         float* base = cgbuf.p + (size_t)which * 5 * n;
         v.x = base;
         v.r = base + (size_t)n;
@@ -890,6 +896,10 @@ void tg_destroy(tg_handle* h) {
         cudaStreamDestroy(h->auxStream);
     }
     if (h->iterExec) cudaGraphExecDestroy(h->iterExec);
+    for (int w = 0; w < 2; w++)
+        if (h->cgExec[w]) cudaGraphExecDestroy(h->cgExec[w]);
+    h->cgIterDev.release();
+    h->cgTgtDev.release();
     if (h->captureStream) cudaStreamDestroy(h->captureStream);
     h->iterDev.release();
     h->rel2Dev.release();
@@ -1146,6 +1156,104 @@ int tg_residual(tg_handle* h, double* rel) {
 // absTarget2: a floor under the target of r.r (0: none), for a system whose
 // part of the global residual only has to fall below a share of the outer
 // tolerance
+}  // extern "C"
+
+// Every pointer, size and schedule that the replayed iteration's kernels
+// take as parameters, field by field.
+static std::vector<uint64_t> iteration_key(const VSys& v, const AmgDev& g, int slots) {
+    std::vector<uint64_t> k;
+    auto p = [&](const void* q) { k.push_back((uint64_t)(uintptr_t)q); };
+    auto i = [&](long long x) { k.push_back((uint64_t)x); };
+    p(v.slot_of); p(v.node_of); p(v.slice_start); p(v.slice_width); p(v.col); p(v.val); p(v.val16); p(v.g);
+    p(v.vpos); p(v.d); p(v.x); p(v.r); p(v.u); p(v.w); p(v.p); p(v.sv); p(v.hist); p(v.scal); p(v.count);
+    p(v.iter); p(v.rel2); i(v.capacity); i(slots);
+    i(g.levels); p(g.y0); p(g.t0); p(g.coarse_inv); i(g.fine_unroll);
+    for (int l = 0; l < g.levels && l < kAmgMaxLevels; l++) {
+        const AmgDevLevel& L = g.lev[l];
+        i(L.n); i(L.a_lanes); i(L.r_lanes);
+        p(L.a_ptr); p(L.a_col); p(L.a_val); p(L.diag); p(L.p_ptr); p(L.p_col); p(L.p_val);
+        p(L.r_ptr); p(L.r_col); p(L.r_val); p(L.b); p(L.y); p(L.x); p(L.t);
+    }
+    return k;
+}
+
+// Captures body(stream) into *exec (replacing the one there) on the
+// handle's capture stream; *nodes gets the kernels it launched.
+template <class F>
+static cudaError_t capture_graph(tg_handle* h, F body, cudaGraphExec_t* exec, long long* nodes) {
+    if (*exec) {
+        cudaError_t e = cudaGraphExecDestroy(*exec);
+        *exec = nullptr;
+        if (e != cudaSuccess) return e;
+    }
+    if (!h->captureStream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&h->captureStream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+    }
+    long long count = 0;
+    t_captured = &count;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->captureStream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        body(h->captureStream);
+        e = cudaStreamEndCapture(h->captureStream, &graph);
+    }
+    t_captured = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) *exec = nullptr;
+    *nodes = count;
+    return e;
+}
+
+// The replayed CG iteration of the multigrid solve for the V system as it
+// is now: captured anew when its device state or its slots in use changed
+// (removals append rows, a new slice of 32 every 32 rows); vg: the VSys
+// whose kernels read the iteration index and target on the device.
+static int iteration_graph(tg_handle* h, const VSys& vg) {
+    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vActive);
+    if (h->iterExec && key == h->iterKey) return TG_OK;
+    const int slots = h->vActive;
+    const cudaError_t e = capture_graph(
+        h,
+        [&](cudaStream_t cs) {
+            launch_vcg_update(vg, slots, 0, -1.0, false, cs);
+            launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs);
+            launch_vcg_spmv(vg, slots, 1, -1.0, true, cs);
+            launch_vcg_replay_step(h->iterDev.p, cs);
+        },
+        &h->iterExec, &h->iterNodes);
+    if (e != cudaSuccess) return cuda_check(h, e, "tg_solve: CG iteration graph");
+    h->iterKey.swap(key);
+    return TG_OK;
+}
+
+// The replayed iteration of the node-space CG on one row list (which: 0 or
+// 1), captured anew when its rows or vectors changed.
+static int cg_iteration_graph(tg_handle* h, int which, const DevMesh& m, const int32_t* rows, int count,
+                              const CGVectors& vg) {
+    std::vector<uint64_t> key;
+    for (const void* q : {(const void*)m.row_ptr, (const void*)m.col, (const void*)m.ceff32, (const void*)m.diag32,
+                          (const void*)rows, (const void*)vg.x, (const void*)vg.r, (const void*)vg.z,
+                          (const void*)vg.p, (const void*)vg.ap, (const void*)vg.scal, (const void*)vg.iter,
+                          (const void*)vg.tgt})
+        key.push_back((uint64_t)(uintptr_t)q);
+    key.push_back((uint64_t)count);
+    if (h->cgExec[which] && key == h->cgKey[which]) return TG_OK;
+    const cudaError_t e = capture_graph(
+        h,
+        [&](cudaStream_t cs) {
+            launch_cg_iter(m, rows, count, vg, 0, -1.0, -1.0, cs);
+            launch_cg_replay_step(h->cgIterDev.p, cs);
+        },
+        &h->cgExec[which], &h->cgNodes[which]);
+    if (e != cudaSuccess) return cuda_check(h, e, "tg_solve: node-space CG iteration graph");
+    h->cgKey[which].swap(key);
+    return TG_OK;
+}
+
+extern "C" {
+
 static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, double rtol, int maxIter, int* itersOut,
                   double absTarget2 = 0.0) {
     DevMesh m = h->dm();
@@ -1162,6 +1270,18 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     // outer FP64 test uses: r.r <= max(rtol^2 r.r_0, absTarget2), tested by
     // the kernels themselves, so the iterations queue before r.r_0 is read
     const double rel2 = rtol * rtol;
+    // the iterations replay one captured iteration
+    const bool replay = h->launchMode == 1 && count > 0;
+    if (replay) {
+        if (!h->cgIterDev.p) CK(h->cgIterDev.alloc(1));
+        if (!h->cgTgtDev.p) CK(h->cgTgtDev.alloc(2));
+        CGVectors vg = v;
+        vg.iter = h->cgIterDev.p;
+        vg.tgt = h->cgTgtDev.p;
+        const int rc = cg_iteration_graph(h, which, m, rows, count, vg);
+        if (rc != TG_OK) return rc;
+        launch_cg_replay_begin(h->cgIterDev.p, h->cgTgtDev.p, rel2, absTarget2, h->stream);
+    }
     int it = 0;
     // iterations queued before the first read: one more than the last solve
     // of this system took, then small batches
@@ -1171,7 +1291,14 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     while (it < maxIter) {
         const int start = it;
         const int end = std::min(maxIter, it + batch);
-        for (; it < end; it++) launch_cg_iter(m, rows, count, v, it, rel2, absTarget2, h->stream);
+        for (; it < end; it++) {
+            if (replay) {
+                CK(cudaGraphLaunch(h->cgExec[which], h->stream));
+                g_launches.fetch_add(h->cgNodes[which], std::memory_order_relaxed);
+                continue;
+            }
+            launch_cg_iter(m, rows, count, v, it, rel2, absTarget2, h->stream);
+        }
         // r.r after j iterations sits at scal[3j+2]; the kernels of later
         // iterations of the batch returned early once it met the target
         CK(cudaMemcpyAsync(s0, scal.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
@@ -1343,61 +1470,6 @@ static int amg_setup(tg_handle* h, double* seconds) {
 // V-cycle as the preconditioner instead of the diagonal.
 // fp64: the FP64 iterations (multigrid only), their right-hand side taken
 // from the kept FP64 residuals by node.
-// Every pointer, size and schedule that the replayed iteration's kernels
-// take as parameters, field by field.
-static std::vector<uint64_t> iteration_key(const VSys& v, const AmgDev& g, int slots) {
-    std::vector<uint64_t> k;
-    auto p = [&](const void* q) { k.push_back((uint64_t)(uintptr_t)q); };
-    auto i = [&](long long x) { k.push_back((uint64_t)x); };
-    p(v.slot_of); p(v.node_of); p(v.slice_start); p(v.slice_width); p(v.col); p(v.val); p(v.val16); p(v.g);
-    p(v.vpos); p(v.d); p(v.x); p(v.r); p(v.u); p(v.w); p(v.p); p(v.sv); p(v.hist); p(v.scal); p(v.count);
-    p(v.iter); p(v.rel2); i(v.capacity); i(slots);
-    i(g.levels); p(g.y0); p(g.t0); p(g.coarse_inv); i(g.fine_unroll);
-    for (int l = 0; l < g.levels && l < kAmgMaxLevels; l++) {
-        const AmgDevLevel& L = g.lev[l];
-        i(L.n); i(L.a_lanes); i(L.r_lanes);
-        p(L.a_ptr); p(L.a_col); p(L.a_val); p(L.diag); p(L.p_ptr); p(L.p_col); p(L.p_val);
-        p(L.r_ptr); p(L.r_col); p(L.r_val); p(L.b); p(L.y); p(L.x); p(L.t);
-    }
-    return k;
-}
-
-// The replayed CG iteration of the multigrid solve for the V system as it
-// is now: captured anew when its device state or its slots in use changed
-// (removals append rows, a new slice of 32 every 32 rows); vg: the VSys
-// whose kernels read the iteration index and target on the device.
-static int iteration_graph(tg_handle* h, const VSys& vg) {
-    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vActive);
-    if (h->iterExec && key == h->iterKey) return TG_OK;
-    if (h->iterExec) {
-        CK(cudaGraphExecDestroy(h->iterExec));
-        h->iterExec = nullptr;
-    }
-    if (!h->captureStream) CK(cudaStreamCreateWithFlags(&h->captureStream, cudaStreamNonBlocking));
-    const int cap = h->vActive;
-    long long nodes = 0;
-    t_captured = &nodes;
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(h->captureStream, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        launch_vcg_update(vg, cap, 0, -1.0, false, h->captureStream);
-        launch_amg_vcycle(vg, cap, h->amg, 1, -1.0, h->captureStream);
-        launch_vcg_spmv(vg, cap, 1, -1.0, true, h->captureStream);
-        launch_vcg_replay_step(h->iterDev.p, h->captureStream);
-        e = cudaStreamEndCapture(h->captureStream, &graph);
-    }
-    t_captured = nullptr;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->iterExec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-        h->iterExec = nullptr;
-        return cuda_check(h, e, "tg_solve: CG iteration graph");
-    }
-    h->iterNodes = nodes;
-    h->iterKey.swap(key);
-    return TG_OK;
-}
-
 static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersOut, bool fp64 = false) {
     const size_t need = 4 * (size_t)(maxIter + 2);
     if (h->vScal.n < need) CK(h->vScal.alloc(need));

@@ -228,8 +228,17 @@ void launch_bnorm(const DevMesh& m, const int32_t* rows, int count, double* acc,
 struct CGVectors {
     float *x, *r, *z, *p, *ap;
     double* scal;  // [3*(max_iter+2)] accumulators: rz, pAp per iteration
+    // iterations replayed from a CUDA graph: the index counts from the
+    // device counter *iter and the targets (rel2, abs2) are tgt[0], tgt[1]
+    // (both null when the host launches each iteration with its own values)
+    const int32_t* iter;
+    const double* tgt;
 };
 void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s);
+// the counter and targets of node-space CG iterations replayed from a CUDA
+// graph: set to 0, rel2 and abs2 before the first replay; the step adds 1
+void launch_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2, cudaStream_t s);
+void launch_cg_replay_step(int32_t* iter, cudaStream_t s);
 // one CG iteration; all of it is skipped once r.r (scal[3it+2]) <=
 // max(rel2 * r.r at the start (scal[2]), abs2)
 void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors v, int it, double rel2, double abs2,

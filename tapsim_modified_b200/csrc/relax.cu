@@ -130,10 +130,21 @@ __device__ __forceinline__ bool cg_met(const double* scal, int it, double rel2, 
     return scal[3 * it + 2] <= fmax(rel2 * scal[2], abs2);
 }
 
+// an iteration replayed from a CUDA graph takes its index and targets from
+// device memory (CGVectors::iter, tgt)
+__device__ __forceinline__ void cg_replayed(const CGVectors& v, int& it, double& rel2, double& abs2) {
+    if (v.iter) {
+        it += *v.iter;
+        rel2 = v.tgt[0];
+        abs2 = v.tgt[1];
+    }
+}
+
 // ap = A p on the rows (A = diag - offdiag), pAp -> scal[3it+1]; all three
 // kernels of an iteration are skipped once it is done (cg_met)
 __global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double rel2,
                           double abs2) {
+    cg_replayed(v, it, rel2, abs2);
     if (cg_met(v.scal, it, rel2, abs2)) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double pap = 0.0;
@@ -153,6 +164,7 @@ __global__ void k_cg_spmv(DevMesh m, const int32_t* __restrict__ rows, int count
 // x += a p, r -= a ap, z = r/diag, rz_next -> scal[3(it+1)], r.r -> scal[3(it+1)+2]
 __global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int count, CGVectors v, int it, double rel2,
                             double abs2) {
+    cg_replayed(v, it, rel2, abs2);
     const double rz = v.scal[3 * it];
     if (cg_met(v.scal, it, rel2, abs2)) return;
     const double pap = v.scal[3 * it + 1];
@@ -176,6 +188,7 @@ __global__ void k_cg_update(DevMesh m, const int32_t* __restrict__ rows, int cou
 // p = z + beta p
 __global__ void k_cg_pupdate(const int32_t* __restrict__ rows, int count, CGVectors v, int it, double rel2,
                              double abs2) {
+    cg_replayed(v, it, rel2, abs2);
     const double rz = v.scal[3 * it];
     if (cg_met(v.scal, it, rel2, abs2)) return;
     const double rzn = v.scal[3 * (it + 1)];
@@ -186,6 +199,13 @@ __global__ void k_cg_pupdate(const int32_t* __restrict__ rows, int count, CGVect
         v.p[i] = v.z[i] + beta * v.p[i];
     }
 }
+
+__global__ void k_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2) {
+    *iter = 0;
+    tgt[0] = rel2;
+    tgt[1] = abs2;
+}
+__global__ void k_cg_replay_step(int32_t* iter) { *iter += 1; }
 
 __global__ void k_add_coupled(DevMesh m, const int32_t* __restrict__ rows, int count, const float* xV, float* r) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -328,6 +348,14 @@ void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors 
     { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, rel2, abs2); }
     { count_launch(); k_cg_update<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, rel2, abs2); }
     { count_launch(); k_cg_pupdate<<<blocks(count), kBlock, 0, s>>>(rows, count, v, it, rel2, abs2); }
+}
+void launch_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2, cudaStream_t s) {
+    count_launch();
+    k_cg_replay_begin<<<1, 1, 0, s>>>(iter, tgt, rel2, abs2);
+}
+void launch_cg_replay_step(int32_t* iter, cudaStream_t s) {
+    count_launch();
+    k_cg_replay_step<<<1, 1, 0, s>>>(iter);
 }
 void launch_cg_spmv_only(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s) {
     if (count > 0) { count_launch(); k_cg_spmv<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, 0, -1.0, -1.0); }
