@@ -314,6 +314,11 @@ def run_ours(args, rank: int, world: int, dist):
         else run_arm("plain_value", 0, long_run=args.long_events)
     grid, info0, dev_s, t_e2e, phi, clocks = (arm[k] for k in ("grid", "info0", "dev_s", "t_e2e", "phi", "clocks"))
     launches = arm["launches"]
+    # the autotuned schedule of the value arm's hierarchy: per level its rows,
+    # lanes per CSR row (level 0: the smoothing pass's load depth, 1000+ for
+    # the pipelined kernel) and the kept launches' times
+    schedule = [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in lv.items()} for lv in grid.amg_schedule()] \
+        if PRECOND == 1 else None
     recs = arm["records"][args.warmup:]
     resid = max(r["rel_residual"] for r in recs + plain["records"][args.warmup:])
     # roofline of the dominant kernel (the multigrid's level-0 smoothing
@@ -403,6 +408,7 @@ def run_ours(args, rank: int, world: int, dist):
             "initial_solve": {"outer": info0.outer, "inner": info0.inner, "rel_residual": info0.rel_residual},
             "preconditioner": "smoothed-aggregation multigrid V(1,1)-cycle (tg_solve_opts.preconditioner 1)"
                               if PRECOND == 1 else "Jacobi",
+            "multigrid_schedule": schedule,
             "inner_rtol": args.inner_rtol,
             "launch_mode": ("each multigrid CG iteration replayed from one captured CUDA graph" if args.launch_mode == 1
                             else "every kernel launched from the host"),

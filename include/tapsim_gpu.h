@@ -163,7 +163,9 @@ int tg_solve(tg_handle* h, const tg_solve_opts* opts, tg_solve_info* info);
  * (levels smoothed with CSR rows) and of its restriction (every level but
  * the coarsest), 0 where the level has none; for level 0, a_lanes is the
  * number of coupling loads each lane of the SELL-32 smoothing pass issues
- * ahead of their gathers (4, 8 or 16).  The hierarchy build chooses them
+ * ahead of their gathers (4, 8 or 16; 1004 or 1008 for the software-
+ * pipelined pass, which loads the next 4 or 8 while it gathers the current
+ * ones).  The hierarchy build chooses them
  * one at a time, from a row-length rule, by timing whole V-cycles with
  * each candidate, and keeps a change that takes 3% off the cycle; a_ms /
  * r_ms are the kept kernels' own launch times [ms]. */

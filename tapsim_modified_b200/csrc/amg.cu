@@ -79,6 +79,68 @@ __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, f
     }
 }
 
+// The level-0 pass software-pipelined: a lane loads the columns and values
+// of its next U entries before it gathers the y of the current U, so that
+// the next round's loads from DRAM wait out the current round's gathers
+// (chosen per hierarchy against k_amg_fine by timed trials).
+template <int U>
+__global__ void k_amg_fine_pipe(VSys v, int slices, const float* b, const float* y, float* out, int mode,
+                                Gate gate) {
+    if (gate.done()) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < slices; warp += warps) {
+        const int base = v.slice_start[warp];
+        const int width = v.slice_width[warp];
+        const int s = warp * 32 + lane;
+        const int* __restrict__ col = v.col + base + lane;
+        const __nv_bfloat16* __restrict__ val = v.val16 + base + lane;
+        float acc = 0.0f, sum = 0.0f;
+        const int rounds = width / U;
+        int c[U];
+        float a[U];
+        if (rounds > 0) {
+#pragma unroll
+            for (int j = 0; j < U; j++) {
+                c[j] = __ldcs(col + 32 * j);
+                a[j] = __bfloat162float(__ldcs(val + 32 * j));
+            }
+        }
+        for (int r = 0; r < rounds; r++) {
+            int cn[U];
+            float an[U];
+            const bool more = r + 1 < rounds;
+            if (more) {
+#pragma unroll
+                for (int j = 0; j < U; j++) {
+                    cn[j] = __ldcs(col + 32 * ((r + 1) * U + j));
+                    an[j] = __bfloat162float(__ldcs(val + 32 * ((r + 1) * U + j)));
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < U; j++) {
+                acc += a[j] * __ldg(y + c[j]);
+                sum += a[j];
+            }
+            if (more) {
+#pragma unroll
+                for (int j = 0; j < U; j++) {
+                    c[j] = cn[j];
+                    a[j] = an[j];
+                }
+            }
+        }
+        for (int k = rounds * U; k < width; k++) {
+            const float a1 = __bfloat162float(__ldcs(val + 32 * k));
+            acc += a1 * __ldg(y + __ldcs(col + 32 * k));
+            sum += a1;
+        }
+        const float ys = y[s];
+        const float t = b[s] - ((v.g[s] + sum) * ys - acc);
+        out[s] = mode == 0 ? t : ys + kSmooth * t / v.d[s];
+    }
+}
+
 // Rows of the coarse operators and of the restrictions hold tens to a few
 // hundred entries: a group of L lanes per row (L from the matrix's mean row
 // length, AmgDevLevel::a_lanes / r_lanes), one row per group, a grid with a
@@ -165,12 +227,15 @@ __global__ void k_amg_dense(int n, const float* inv, const float* b, float* x, G
 // loop then makes one pass)
 inline unsigned grid_full(long long threads) { return (unsigned)((threads + kBlock - 1) / kBlock); }
 
-// the level-0 pass with the hierarchy's load depth (AmgDev::fine_unroll)
+// the level-0 pass with the hierarchy's load depth (AmgDev::fine_unroll;
+// plus kFinePipe: the software-pipelined kernel)
 void launch_fine(int U, const VSys& v, int slices, const float* b, const float* y, float* out, int mode, Gate gate,
                  cudaStream_t s) {
     count_launch();
     const unsigned grid = grid_full((long long)slices * 32);
-    if (U == 4) k_amg_fine<4><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
+    if (U == kFinePipe + 4) k_amg_fine_pipe<4><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
+    else if (U == kFinePipe + 8) k_amg_fine_pipe<8><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
+    else if (U == 4) k_amg_fine<4><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
     else if (U == 16) k_amg_fine<16><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
     else k_amg_fine<8><<<grid, kBlock, 0, s>>>(v, slices, b, y, out, mode, gate);
 }
@@ -265,8 +330,8 @@ int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* a
         }
         *knob = chosen;
     };
-    static const int kUnroll[3] = {4, 8, 16};
-    tryChoice(&g.fine_unroll, kUnroll, 3);
+    static const int kUnroll[5] = {4, 8, 16, kFinePipe + 4, kFinePipe + 8};
+    tryChoice(&g.fine_unroll, kUnroll, 5);
     for (int l = 0; l + 1 < g.levels; l++) {
         tryChoice(&g.lev[l].r_lanes, kCand, 5);
         if (l + 2 < g.levels) tryChoice(&g.lev[l + 1].a_lanes, kCand, 5);

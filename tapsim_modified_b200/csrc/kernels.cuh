@@ -160,15 +160,18 @@ struct AmgDevLevel {
     float *b, *y, *x, *t;                   // right-hand side, work, result, residual (levels >= 1)
     int a_lanes, r_lanes;                   // lanes per row of the operator and of the restriction (2..32)
 };
+constexpr int kFinePipe = 1000;             // AmgDev::fine_unroll offset of the pipelined level-0 pass
 struct AmgDev {
     int levels;                             // including level 0 (the V system) and the coarsest
     AmgDevLevel lev[kAmgMaxLevels];
     float *y0, *t0;                         // level-0 work vectors (capacity + 1)
     const float* coarse_inv;                // dense inverse of the coarsest operator, row-major
-    int fine_unroll;                        // level-0 pass: loads per lane ahead of their gathers (4, 8, 16)
+    int fine_unroll;                        // level-0 pass: loads per lane ahead of their gathers (4, 8, 16),
+                                            // plus kFinePipe for the software-pipelined kernel (4, 8)
 };
 // Autotuner of the hierarchy's schedules: the level-0 pass's loads per
-// lane (4, 8, 16; fine_unroll), and for the restriction of every level and
+// lane (4, 8, 16, or the pipelined kernel with 4 or 8; fine_unroll), and
+// for the restriction of every level and
 // the operator of every level smoothed by CSR rows the lane-group size
 // (2..32 lanes per row; r_lanes / a_lanes), chosen one at a time from the
 // row-length rule's schedule by timing whole V-cycles (the least of three
