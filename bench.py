@@ -410,8 +410,10 @@ def run_ours(args, rank: int, world: int, dist):
                               if PRECOND == 1 else "Jacobi",
             "multigrid_schedule": schedule,
             "inner_rtol": args.inner_rtol,
-            "launch_mode": ("each multigrid CG iteration replayed from one captured CUDA graph" if args.launch_mode == 1
-                            else "every kernel launched from the host"),
+            "launch_mode": {0: "every kernel launched from the host",
+                            1: "each multigrid CG iteration replayed from one captured CUDA graph",
+                            2: "the replayed CG iteration inside a device-side loop, one launch per inner solve"}
+                           [args.launch_mode],
             "setup": {"seconds": arm["setup_s"], "multigrid_hierarchy_s": info0.setup_seconds,
                       "mesh_h2d_bytes": h2d_bytes,
                       "note": "mesh upload (tg_create), multigrid hierarchy and initial relaxation, once per tip"},
@@ -973,8 +975,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
     ap.add_argument("--inner-rtol", type=float, default=1e-4,
                     help="the inner solves' least relative reduction per FP64 defect-correction step")
-    ap.add_argument("--launch-mode", type=int, default=1, choices=(0, 1),
-                    help="1: the multigrid CG iterations replay a captured CUDA graph; 0: kernel by kernel")
+    ap.add_argument("--launch-mode", type=int, default=1, choices=(0, 1, 2),
+                    help="1: the multigrid CG iterations replay a captured CUDA graph; 0: kernel by kernel; "
+                         "2: the replayed iteration inside a device-side loop")
     ap.add_argument("--refine", type=int, default=8,
                     help="damped Jacobi sweeps over the learned start's cells after its prediction")
     ap.add_argument("--long-events", type=int, default=200,

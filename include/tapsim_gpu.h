@@ -467,9 +467,14 @@ int64_t tg_launch_count(const tg_handle* h);
 /* How the multigrid solve's FP32 CG iterations reach the device: 1 (the
  * default) replays one iteration (update, V-cycle, SpMV) captured as a CUDA
  * graph, whose kernels read the iteration index and target from device
- * memory (captured again when the hierarchy or the slots in use change);
- * 0 launches each kernel from the host.  Both run the same kernels on the
- * same data. */
+ * memory (captured again when the hierarchy or the slots in use change),
+ * the host reading rho back between batches of replays; 2 replays it
+ * inside a device-side loop (a while-conditional graph node whose last
+ * kernel stops it at the target or the iteration cap), one launch per
+ * inner solve, its iteration count read with the solve's next residual;
+ * 0 launches each kernel from the host.  All run the same kernels on the
+ * same data; the node-space CG of the Neumann rows replays its iteration
+ * in modes 1 and 2. */
 int tg_set_launch_mode(tg_handle* h, int32_t mode);
 /* Times `iters` back-to-back launches of one hot kernel on the handle's
  * stream with CUDA events: 0 = FP32 CG SpMV over the non-Neumann free rows,

@@ -139,11 +139,26 @@ __global__ void k_vcg_update(VSys v, int slots, Gate gate, int jacobi) {
 }
 
 // the replayed CG iterations' counter and target
-__global__ void k_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2) {
+__global__ void k_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, int maxIter) {
     *iter = 0;
-    *rel2Dev = rel2;
+    rel2Dev[0] = rel2;
+    rel2Dev[1] = (double)maxIter;
 }
 __global__ void k_vcg_replay_step(int32_t* iter) { *iter += 1; }
+
+// The condition of the device-side loop around the replayed iteration: go
+// on while fewer than the cap (rel2Dev[1]) have run and rho_k > rel2 rho_0;
+// a NaN stops it.  *done gets the iterations the solve took (0 when rho_0
+// is 0, as the host loop counts them).  The counter steps once per body, so
+// the loop ends after the cap at the latest.
+__global__ void k_vcg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal,
+                                const double* rel2Dev, int32_t* done) {
+    const int k = *iter;
+    const double rho0 = scal[3];
+    const bool more = k < (int)rel2Dev[1] && rho0 > 0.0 && scal[4 * k + 3] > rel2Dev[0] * rho0;
+    *done = rho0 > 0.0 ? k : 0;
+    cudaGraphSetConditional(loop, more ? 1u : 0u);
+}
 
 // phi64[node] += x[slot] (and hist[slot] += x[slot] when recording);
 // clears the slot's vectors
@@ -557,9 +572,14 @@ void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jac
         k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, make_gate(v, it, target), jacobi ? 1 : 0);
     }
 }
-void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, cudaStream_t s) {
+void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, int maxIter, cudaStream_t s) {
     count_launch();
-    k_vcg_replay_begin<<<1, 1, 0, s>>>(iter, rel2Dev, rel2);
+    k_vcg_replay_begin<<<1, 1, 0, s>>>(iter, rel2Dev, rel2, maxIter);
+}
+void launch_vcg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal,
+                          const double* rel2Dev, int32_t* done, cudaStream_t s) {
+    count_launch();
+    k_vcg_loop_cond<<<1, 1, 0, s>>>(loop, iter, scal, rel2Dev, done);
 }
 void launch_vcg_replay_step(int32_t* iter, cudaStream_t s) {
     count_launch();

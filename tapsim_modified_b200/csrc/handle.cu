@@ -187,6 +187,7 @@ struct tg_handle {
         int32_t pending[4096];  // cells flipped since the last solve
         int32_t activated[4096];  // cells a removal adds to fieldCells
         int32_t status[4];        // the device status word, read with each sync
+        int32_t loopIters[4];     // the looped solve's iterations, read with the next sync
     };
     Pinned* pin = nullptr;
     int vNext = 0;            // host mirror of the V system's slot counter
@@ -207,7 +208,14 @@ struct tg_handle {
     cudaStream_t captureStream = nullptr;
     cudaGraphExec_t iterExec = nullptr;
     DBuf<int32_t> iterDev;               // [1] the replayed iterations' counter
-    DBuf<double> rel2Dev;                // [1] their relative target
+    DBuf<double> rel2Dev;                // [2] their relative target and iteration cap
+    // launch mode 2: the replayed iteration inside a device-side loop (a
+    // while-conditional graph node), one launch per inner solve; its count
+    // of iterations reaches the host with the solve's next read
+    cudaGraphExec_t loopExec = nullptr;
+    std::vector<uint64_t> loopKey;
+    DBuf<int32_t> loopDone;              // [1] iterations of the last looped solve
+    long long loopNodes = 0;             // kernels per iteration of the loop
     std::vector<uint64_t> iterKey;       // the device state it was captured with
     long long iterNodes = 0;             // kernels in one replay
     // the same for the node-space CG iterations of either row list (run_cg)
@@ -896,6 +904,8 @@ void tg_destroy(tg_handle* h) {
         cudaStreamDestroy(h->auxStream);
     }
     if (h->iterExec) cudaGraphExecDestroy(h->iterExec);
+    if (h->loopExec) cudaGraphExecDestroy(h->loopExec);
+    h->loopDone.release();
     for (int w = 0; w < 2; w++)
         if (h->cgExec[w]) cudaGraphExecDestroy(h->cgExec[w]);
     h->cgIterDev.release();
@@ -948,7 +958,7 @@ int tg_timer_stop(tg_handle* h, float* ms) {
 int64_t tg_launch_count(const tg_handle*) { return (int64_t)launches_so_far(); }
 
 int tg_set_launch_mode(tg_handle* h, int32_t mode) {
-    if (!h || mode < 0 || mode > 1) return fail(h, TG_ERR_ARGUMENT, "tg_set_launch_mode: mode 0 or 1");
+    if (!h || mode < 0 || mode > 2) return fail(h, TG_ERR_ARGUMENT, "tg_set_launch_mode: mode 0, 1 or 2");
     h->launchMode = mode;
     return TG_OK;
 }
@@ -1228,6 +1238,63 @@ static int iteration_graph(tg_handle* h, const VSys& vg) {
     return TG_OK;
 }
 
+// Launch mode 2: the replayed iteration inside a while-conditional graph
+// node.  The loop's body is the iteration (update, V-cycle, SpMV, counter
+// step) and k_vcg_loop_cond, which sets the node's condition from the
+// device counter and rho; the counter steps once per body, so the loop ends
+// by the iteration cap.  Captured anew with the iteration graph's key.
+static int iteration_loop_graph(tg_handle* h, const VSys& vg) {
+    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vActive);
+    key.push_back((uint64_t)(uintptr_t)h->loopDone.p);
+    if (h->loopExec && key == h->loopKey) return TG_OK;
+    if (h->loopExec) {
+        CK(cudaGraphExecDestroy(h->loopExec));
+        h->loopExec = nullptr;
+    }
+    if (!h->captureStream) CK(cudaStreamCreateWithFlags(&h->captureStream, cudaStreamNonBlocking));
+    const int slots = h->vActive;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    cudaGraphConditionalHandle loop{};
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams params{};
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) {
+        params.type = cudaGraphNodeTypeConditional;
+        params.conditional.handle = loop;
+        params.conditional.type = cudaGraphCondTypeWhile;
+        params.conditional.size = 1;
+        e = cudaGraphAddNode(&node, graph, nullptr, 0, &params);
+    }
+    long long nodes = 0;
+    if (e == cudaSuccess) {
+        cudaGraph_t body = params.conditional.phGraph_out[0];
+        t_captured = &nodes;
+        e = cudaStreamBeginCaptureToGraph(h->captureStream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaStream_t cs = h->captureStream;
+            launch_vcg_update(vg, slots, 0, -1.0, false, cs);
+            launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs);
+            launch_vcg_spmv(vg, slots, 1, -1.0, true, cs);
+            launch_vcg_replay_step(h->iterDev.p, cs);
+            launch_vcg_loop_cond(loop, h->iterDev.p, vg.scal, h->rel2Dev.p, h->loopDone.p, cs);
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(cs, &captured);
+        }
+        t_captured = nullptr;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->loopExec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        h->loopExec = nullptr;
+        return cuda_check(h, e, "tg_solve: CG iteration loop graph");
+    }
+    h->loopNodes = nodes;  // kernels per iteration of the loop
+    h->loopKey.swap(key);
+    return TG_OK;
+}
+
 // The replayed iteration of the node-space CG on one row list (which: 0 or
 // 1), captured anew when its rows or vectors changed.
 static int cg_iteration_graph(tg_handle* h, int which, const DevMesh& m, const int32_t* rows, int count,
@@ -1271,7 +1338,7 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     // the kernels themselves, so the iterations queue before r.r_0 is read
     const double rel2 = rtol * rtol;
     // the iterations replay one captured iteration
-    const bool replay = h->launchMode == 1 && count > 0;
+    const bool replay = h->launchMode >= 1 && count > 0;
     if (replay) {
         if (!h->cgIterDev.p) CK(h->cgIterDev.alloc(1));
         if (!h->cgTgtDev.p) CK(h->cgTgtDev.alloc(2));
@@ -1490,16 +1557,25 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
     // themselves, so the iterations queue before rho_0 is read back
     const double rel2 = rtol * rtol;
     // the multigrid FP32 iterations replay one captured iteration
-    const bool replay = amg && !fp64 && h->launchMode == 1 && slots > 0;
+    const bool replay = amg && !fp64 && h->launchMode >= 1 && slots > 0;
     if (replay) {
         if (!h->iterDev.p) CK(h->iterDev.alloc(1));
-        if (!h->rel2Dev.p) CK(h->rel2Dev.alloc(1));
+        if (!h->rel2Dev.p) CK(h->rel2Dev.alloc(2));
         VSys vg = v;
         vg.iter = h->iterDev.p;
         vg.rel2 = h->rel2Dev.p;
-        const int rc = iteration_graph(h, vg);
+        if (h->launchMode == 2 && !h->loopDone.p) CK(h->loopDone.alloc(1));
+        const int rc = h->launchMode == 2 ? iteration_loop_graph(h, vg) : iteration_graph(h, vg);
         if (rc != TG_OK) return rc;
-        launch_vcg_replay_begin(h->iterDev.p, h->rel2Dev.p, rel2, h->stream);
+        launch_vcg_replay_begin(h->iterDev.p, h->rel2Dev.p, rel2, maxIter, h->stream);
+        if (h->launchMode == 2) {
+            // the whole solve in one launch: the loop stops itself
+            CK(cudaGraphLaunch(h->loopExec, h->stream));
+            CK(cudaMemcpyAsync(&h->pin->loopIters[0], h->loopDone.p, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               h->stream));
+            *itersOut = -1;  // pending: pin->loopIters[0] after the next sync
+            return TG_OK;
+        }
     }
     int it = 0;
     // iterations queued before the first read: about as many as the last
@@ -1661,6 +1737,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         rc = amg_setup(h, &inf.setup_seconds);
         if (rc != TG_OK) return rc;
     }
+    bool loopPending = false;  // a looped inner solve whose count is still on its way
     for (int outer = 0;; outer++) {
         if (outer == 0 && incremental) {
             if (warm && !warmFirst) {
@@ -1683,6 +1760,14 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         CK(cudaMemcpyAsync(r2, h->rsum.p, sizeof(double) * (needB ? 3 : 2), cudaMemcpyDeviceToHost, h->stream));
         rc = sync_status(h, "tg_solve residual");
         if (rc != TG_OK) return rc;
+        if (loopPending) {
+            // the looped inner solve's iterations came back with this read
+            const int k = h->pin->loopIters[0];
+            inf.inner += k;
+            g_launches.fetch_add(h->loopNodes * k, std::memory_order_relaxed);
+            h->lastItersAmg = k;
+            loopPending = false;
+        }
         // sums kept across removals can round to a little below zero
         r2[0] = std::max(r2[0], 0.0);
         r2[1] = std::max(r2[1], 0.0);
@@ -1720,6 +1805,10 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
             const double floorN = 0.3 * o->rel_tol;
             rc = run_cg(h, 1, h->allN.p, h->countAllN, rtol, o->max_inner, &itN, floorN * floorN * h->bnorm2);
             if (rc != TG_OK) return rc;
+        }
+        if (itV < 0) {
+            loopPending = true;
+            itV = 0;
         }
         inf.inner += itV + itN;
         inf.inner_neumann += itN;

@@ -133,9 +133,14 @@ inline Gate open_gate() { return Gate{nullptr, 0, -1.0, nullptr, nullptr}; }
 void launch_vcg_init(const VSys& v, int slots, bool jacobi, cudaStream_t s);
 void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withGamma, cudaStream_t s);
 void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s);
-// the counter and target of iterations replayed from a CUDA graph: set to
-// 0 and rel2 before the first replay, stepped by 1 at the end of each
-void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, cudaStream_t s);
+// the counter, target and cap of iterations replayed from a CUDA graph:
+// set to 0, rel2 and maxIter before the first replay, stepped by 1 at the
+// end of each
+void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, int maxIter, cudaStream_t s);
+// the condition kernel of the device-side loop around the replayed
+// iteration (the last node of the loop's body); *done: the iterations run
+void launch_vcg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal,
+                          const double* rel2Dev, int32_t* done, cudaStream_t s);
 void launch_vcg_replay_step(int32_t* iter, cudaStream_t s);
 // FP64 inner iterations with the multigrid preconditioner: the V-cycle runs
 // in FP32 on r rounded to float and its u enters the FP64 recurrences

@@ -77,13 +77,14 @@ def test_tuned_schedules_of_the_hierarchy():
 
 def test_replayed_iterations_match_launched_ones(ref_mesh, ref_events):
     """The multigrid solve's CG iterations replayed from a captured CUDA graph
-    (the default) and launched kernel by kernel give the same events: the
+    (the default), launched kernel by kernel, and replayed inside a
+    device-side loop (one launch per inner solve) give the same events: the
     same removals, residuals at the tolerance and potentials equal to the
     solves' own accuracy; the graph's kernels count once per replay."""
     from tapsim_modified_b200 import _native as N
     from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
     out = {}
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         g = Grid(ref_mesh)
         g.set_launch_mode(mode)
         g.solve(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1)
@@ -95,12 +96,14 @@ def test_replayed_iterations_match_launched_ones(ref_mesh, ref_events):
         launches = N.lib().tg_launch_count(g._h) - n0
         out[mode] = ([r["node"] for r in recs], [r["rel_residual"] for r in recs], g.potentials(), launches)
         g.close()
-    (n0_, r0, phi0, l0), (n1, r1, phi1, l1) = out[0], out[1]
-    print("launches over 12 events: kernel by kernel", l0, "replayed", l1)
-    assert n0_ == n1 == [int(x) for x in ref_events[:12, 1]]
-    assert max(r0 + r1) <= 1e-10
+    (n0_, r0, phi0, l0), (n1, r1, phi1, l1), (n2, r2, phi2, l2) = out[0], out[1], out[2]
+    print("launches over 12 events: kernel by kernel", l0, "replayed", l1, "in a device-side loop", l2)
+    assert n0_ == n1 == n2 == [int(x) for x in ref_events[:12, 1]]
+    assert max(r0 + r1 + r2) <= 1e-10
     assert np.abs(phi1 - phi0).max() <= 1e-8 * np.abs(phi0).max()
+    assert np.abs(phi2 - phi0).max() <= 1e-8 * np.abs(phi0).max()
     # the same kernels run either way (the replay adds one counter step per
-    # iteration and a start per solve; early-exiting kernels count in both)
-    assert 0.8 * l0 <= l1 <= 1.3 * l0
+    # iteration and a start per solve, the loop a condition kernel; the
+    # host-driven modes also count the early-exiting kernels of a batch)
+    assert 0.6 * l0 <= l1 <= 1.3 * l0 and 0.6 * l0 <= l2 <= 1.3 * l0
 
