@@ -975,7 +975,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned arm")
     ap.add_argument("--inner-rtol", type=float, default=1e-4,
                     help="the inner solves' least relative reduction per FP64 defect-correction step")
-    ap.add_argument("--launch-mode", type=int, default=1, choices=(0, 1, 2),
+    ap.add_argument("--launch-mode", type=int, default=2, choices=(0, 1, 2),
                     help="1: the multigrid CG iterations replay a captured CUDA graph; 0: kernel by kernel; "
                          "2: the replayed iteration inside a device-side loop")
     ap.add_argument("--refine", type=int, default=8,

@@ -464,12 +464,12 @@ int tg_timer_stop(tg_handle* h, float* elapsed_ms);
 /* Kernels launched in this process so far (every handle; the kernels of a
  * replayed CUDA graph count at each replay). */
 int64_t tg_launch_count(const tg_handle* h);
-/* How the multigrid solve's FP32 CG iterations reach the device: 1 (the
- * default) replays one iteration (update, V-cycle, SpMV) captured as a CUDA
+/* How the multigrid solve's FP32 CG iterations reach the device: 1
+ * replays one iteration (update, V-cycle, SpMV) captured as a CUDA
  * graph, whose kernels read the iteration index and target from device
  * memory (captured again when the hierarchy or the slots in use change),
- * the host reading rho back between batches of replays; 2 replays it
- * inside a device-side loop (a while-conditional graph node whose last
+ * the host reading rho back between batches of replays; 2 (the default)
+ * replays it inside a device-side loop (a while-conditional graph node whose last
  * kernel stops it at the target or the iteration cap), one launch per
  * inner solve, its iteration count read with the solve's next residual;
  * 0 launches each kernel from the host.  All run the same kernels on the

@@ -204,7 +204,7 @@ struct tg_handle {
     // target from device memory (VSys::iter, rel2).  Captured again when the
     // V system's or the hierarchy's device state (pointers, schedules) or
     // the slots in use differ from the ones it was captured with.
-    int launchMode = 1;                  // 1: replay the graph; 0: launch each kernel
+    int launchMode = 2;                  // 2: the replayed graph in a device-side loop; 1: replay; 0: launch each kernel
     cudaStream_t captureStream = nullptr;
     cudaGraphExec_t iterExec = nullptr;
     DBuf<int32_t> iterDev;               // [1] the replayed iterations' counter

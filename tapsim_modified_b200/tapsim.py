@@ -231,8 +231,10 @@ class Grid:
         return info
 
     def set_launch_mode(self, mode: int):
-        """1: the multigrid solve replays one captured CG iteration (a CUDA
-        graph); 0: it launches every kernel (tg_set_launch_mode)."""
+        """2 (the default): the multigrid solve replays one captured CG
+        iteration (a CUDA graph) inside a device-side loop; 1: replays it
+        from the host in batches; 0: launches every kernel
+        (tg_set_launch_mode)."""
         N.check(N.lib().tg_set_launch_mode(self._h, int(mode)), self._h)
 
     def amg_schedule(self) -> list[dict]:
