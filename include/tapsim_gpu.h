@@ -473,8 +473,8 @@ int64_t tg_launch_count(const tg_handle* h);
  * kernel stops it at the target or the iteration cap), one launch per
  * inner solve, its iteration count read with the solve's next residual;
  * 0 launches each kernel from the host.  All run the same kernels on the
- * same data; the node-space CG of the Neumann rows follows the same mode
- * (replayed in batches in 1, in its own device-side loop in 2). */
+ * same data; the node-space CG of the Neumann rows replays its iteration
+ * in modes 1 and 2. */
 int tg_set_launch_mode(tg_handle* h, int32_t mode);
 /* Times `iters` back-to-back launches of one hot kernel on the handle's
  * stream with CUDA events: 0 = FP32 CG SpMV over the non-Neumann free rows,

@@ -223,12 +223,7 @@ struct tg_handle {
     std::vector<uint64_t> cgKey[2];
     long long cgNodes[2] = {0, 0};
     DBuf<int32_t> cgIterDev;             // [1] their counter
-    DBuf<double> cgTgtDev;               // [3] their targets rel2, abs2 and iteration cap
-    // launch mode 2 for the node-space CG (as loopExec for the V system)
-    cudaGraphExec_t cgLoopExec[2] = {nullptr, nullptr};
-    std::vector<uint64_t> cgLoopKey[2];
-    long long cgLoopNodes[2] = {0, 0};
-    DBuf<int32_t> cgLoopDone;            // [2] iterations of the last looped solve of each list
+    DBuf<double> cgTgtDev;               // [2] their targets rel2, abs2
     int lastItersJacobi = 16, lastItersAmg = 4;  // iterations of the last inner solves
     int lastItersCgV = 16, lastItersCgN = 16;
 
@@ -913,9 +908,6 @@ void tg_destroy(tg_handle* h) {
     h->loopDone.release();
     for (int w = 0; w < 2; w++)
         if (h->cgExec[w]) cudaGraphExecDestroy(h->cgExec[w]);
-    for (int w = 0; w < 2; w++)
-        if (h->cgLoopExec[w]) cudaGraphExecDestroy(h->cgLoopExec[w]);
-    h->cgLoopDone.release();
     h->cgIterDev.release();
     h->cgTgtDev.release();
     if (h->captureStream) cudaStreamDestroy(h->captureStream);
@@ -1246,20 +1238,21 @@ static int iteration_graph(tg_handle* h, const VSys& vg) {
     return TG_OK;
 }
 
-// A graph of one while-conditional node whose body body(stream, loop)
-// captures (its last kernel sets the condition through `loop`), into *exec
-// (replacing the one there); *nodes gets the body's kernels.
-template <class F>
-static cudaError_t capture_loop_graph(tg_handle* h, F body, cudaGraphExec_t* exec, long long* nodes) {
-    if (*exec) {
-        cudaError_t e = cudaGraphExecDestroy(*exec);
-        *exec = nullptr;
-        if (e != cudaSuccess) return e;
+// Launch mode 2: the replayed iteration inside a while-conditional graph
+// node.  The loop's body is the iteration (update, V-cycle, SpMV, counter
+// step) and k_vcg_loop_cond, which sets the node's condition from the
+// device counter and rho; the counter steps once per body, so the loop ends
+// by the iteration cap.  Captured anew with the iteration graph's key.
+static int iteration_loop_graph(tg_handle* h, const VSys& vg) {
+    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vActive);
+    key.push_back((uint64_t)(uintptr_t)h->loopDone.p);
+    if (h->loopExec && key == h->loopKey) return TG_OK;
+    if (h->loopExec) {
+        CK(cudaGraphExecDestroy(h->loopExec));
+        h->loopExec = nullptr;
     }
-    if (!h->captureStream) {
-        cudaError_t e = cudaStreamCreateWithFlags(&h->captureStream, cudaStreamNonBlocking);
-        if (e != cudaSuccess) return e;
-    }
+    if (!h->captureStream) CK(cudaStreamCreateWithFlags(&h->captureStream, cudaStreamNonBlocking));
+    const int slots = h->vActive;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaGraphCreate(&graph, 0);
     cudaGraphConditionalHandle loop{};
@@ -1273,46 +1266,31 @@ static cudaError_t capture_loop_graph(tg_handle* h, F body, cudaGraphExec_t* exe
         params.conditional.size = 1;
         e = cudaGraphAddNode(&node, graph, nullptr, 0, &params);
     }
-    long long count = 0;
+    long long nodes = 0;
     if (e == cudaSuccess) {
-        t_captured = &count;
-        e = cudaStreamBeginCaptureToGraph(h->captureStream, params.conditional.phGraph_out[0], nullptr, nullptr, 0,
+        cudaGraph_t body = params.conditional.phGraph_out[0];
+        t_captured = &nodes;
+        e = cudaStreamBeginCaptureToGraph(h->captureStream, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            body(h->captureStream, loop);
-            cudaGraph_t captured = nullptr;
-            e = cudaStreamEndCapture(h->captureStream, &captured);
-        }
-        t_captured = nullptr;
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    if (e != cudaSuccess) *exec = nullptr;
-    *nodes = count;
-    return e;
-}
-
-// Launch mode 2: the replayed iteration inside a while-conditional graph
-// node.  The loop's body is the iteration (update, V-cycle, SpMV, counter
-// step) and k_vcg_loop_cond, which sets the node's condition from the
-// device counter and rho; the counter steps once per body, so the loop ends
-// by the iteration cap.  Captured anew with the iteration graph's key.
-static int iteration_loop_graph(tg_handle* h, const VSys& vg) {
-    std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vActive);
-    key.push_back((uint64_t)(uintptr_t)h->loopDone.p);
-    if (h->loopExec && key == h->loopKey) return TG_OK;
-    const int slots = h->vActive;
-    const cudaError_t e = capture_loop_graph(
-        h,
-        [&](cudaStream_t cs, cudaGraphConditionalHandle loop) {
+            cudaStream_t cs = h->captureStream;
             launch_vcg_update(vg, slots, 0, -1.0, false, cs);
             launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs);
             launch_vcg_spmv(vg, slots, 1, -1.0, true, cs);
             launch_vcg_replay_step(h->iterDev.p, cs);
             launch_vcg_loop_cond(loop, h->iterDev.p, vg.scal, h->rel2Dev.p, h->loopDone.p, cs);
-        },
-        &h->loopExec, &h->loopNodes);
-    if (e != cudaSuccess) return cuda_check(h, e, "tg_solve: CG iteration loop graph");
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(cs, &captured);
+        }
+        t_captured = nullptr;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->loopExec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        h->loopExec = nullptr;
+        return cuda_check(h, e, "tg_solve: CG iteration loop graph");
+    }
+    h->loopNodes = nodes;  // kernels per iteration of the loop
     h->loopKey.swap(key);
     return TG_OK;
 }
@@ -1341,32 +1319,6 @@ static int cg_iteration_graph(tg_handle* h, int which, const DevMesh& m, const i
     return TG_OK;
 }
 
-// Launch mode 2 for the node-space CG: its replayed iteration and
-// k_cg_loop_cond inside a while-conditional graph node.
-static int cg_loop_graph(tg_handle* h, int which, const DevMesh& m, const int32_t* rows, int count,
-                         const CGVectors& vg) {
-    std::vector<uint64_t> key;
-    for (const void* q : {(const void*)m.row_ptr, (const void*)m.col, (const void*)m.ceff32, (const void*)m.diag32,
-                          (const void*)rows, (const void*)vg.x, (const void*)vg.r, (const void*)vg.z,
-                          (const void*)vg.p, (const void*)vg.ap, (const void*)vg.scal, (const void*)vg.iter,
-                          (const void*)vg.tgt, (const void*)h->cgLoopDone.p})
-        key.push_back((uint64_t)(uintptr_t)q);
-    key.push_back((uint64_t)count);
-    if (h->cgLoopExec[which] && key == h->cgLoopKey[which]) return TG_OK;
-    int32_t* done = h->cgLoopDone.p + which;
-    const cudaError_t e = capture_loop_graph(
-        h,
-        [&](cudaStream_t cs, cudaGraphConditionalHandle loop) {
-            launch_cg_iter(m, rows, count, vg, 0, -1.0, -1.0, cs);
-            launch_cg_replay_step(h->cgIterDev.p, cs);
-            launch_cg_loop_cond(loop, h->cgIterDev.p, vg.scal, vg.tgt, done, cs);
-        },
-        &h->cgLoopExec[which], &h->cgLoopNodes[which]);
-    if (e != cudaSuccess) return cuda_check(h, e, "tg_solve: node-space CG loop graph");
-    h->cgLoopKey[which].swap(key);
-    return TG_OK;
-}
-
 extern "C" {
 
 static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, double rtol, int maxIter, int* itersOut,
@@ -1389,23 +1341,13 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
     const bool replay = h->launchMode >= 1 && count > 0;
     if (replay) {
         if (!h->cgIterDev.p) CK(h->cgIterDev.alloc(1));
-        if (!h->cgTgtDev.p) CK(h->cgTgtDev.alloc(3));
-        if (h->launchMode == 2 && !h->cgLoopDone.p) CK(h->cgLoopDone.alloc(2));
+        if (!h->cgTgtDev.p) CK(h->cgTgtDev.alloc(2));
         CGVectors vg = v;
         vg.iter = h->cgIterDev.p;
         vg.tgt = h->cgTgtDev.p;
-        const int rc = h->launchMode == 2 ? cg_loop_graph(h, which, m, rows, count, vg)
-                                          : cg_iteration_graph(h, which, m, rows, count, vg);
+        const int rc = cg_iteration_graph(h, which, m, rows, count, vg);
         if (rc != TG_OK) return rc;
-        launch_cg_replay_begin(h->cgIterDev.p, h->cgTgtDev.p, rel2, absTarget2, maxIter, h->stream);
-        if (h->launchMode == 2) {
-            // the whole solve in one launch: the loop stops itself
-            CK(cudaGraphLaunch(h->cgLoopExec[which], h->stream));
-            CK(cudaMemcpyAsync(&h->pin->loopIters[1 + which], h->cgLoopDone.p + which, sizeof(int32_t),
-                               cudaMemcpyDeviceToHost, h->stream));
-            *itersOut = -1;  // pending: pin->loopIters[1 + which] after the next sync
-            return TG_OK;
-        }
+        launch_cg_replay_begin(h->cgIterDev.p, h->cgTgtDev.p, rel2, absTarget2, h->stream);
     }
     int it = 0;
     // iterations queued before the first read: one more than the last solve
@@ -1795,8 +1737,7 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         rc = amg_setup(h, &inf.setup_seconds);
         if (rc != TG_OK) return rc;
     }
-    bool loopPending = false;   // a looped inner solve whose count is still on its way
-    bool loopPendingN = false;  // the same for the Neumann rows
+    bool loopPending = false;  // a looped inner solve whose count is still on its way
     for (int outer = 0;; outer++) {
         if (outer == 0 && incremental) {
             if (warm && !warmFirst) {
@@ -1826,14 +1767,6 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
             g_launches.fetch_add(h->loopNodes * k, std::memory_order_relaxed);
             h->lastItersAmg = k;
             loopPending = false;
-        }
-        if (loopPendingN) {
-            const int k = h->pin->loopIters[2];
-            inf.inner += k;
-            inf.inner_neumann += k;
-            g_launches.fetch_add(h->cgLoopNodes[1] * k, std::memory_order_relaxed);
-            h->lastItersCgN = k;
-            loopPendingN = false;
         }
         // sums kept across removals can round to a little below zero
         r2[0] = std::max(r2[0], 0.0);
@@ -1876,10 +1809,6 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         if (itV < 0) {
             loopPending = true;
             itV = 0;
-        }
-        if (itN < 0) {
-            loopPendingN = true;
-            itN = 0;
         }
         inf.inner += itV + itN;
         inf.inner_neumann += itN;

@@ -243,14 +243,9 @@ struct CGVectors {
     const double* tgt;
 };
 void launch_cg_init(const DevMesh& m, const int32_t* rows, int count, CGVectors v, cudaStream_t s);
-// the counter, targets and cap of node-space CG iterations replayed from a
-// CUDA graph: set to 0, rel2, abs2 and maxIter before the first replay; the
-// step adds 1
-void launch_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2, int maxIter, cudaStream_t s);
-// the condition kernel of the device-side loop around the replayed
-// node-space CG iteration; *done: the iterations run
-void launch_cg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal, const double* tgt,
-                         int32_t* done, cudaStream_t s);
+// the counter and targets of node-space CG iterations replayed from a CUDA
+// graph: set to 0, rel2 and abs2 before the first replay; the step adds 1
+void launch_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2, cudaStream_t s);
 void launch_cg_replay_step(int32_t* iter, cudaStream_t s);
 // one CG iteration; all of it is skipped once r.r (scal[3it+2]) <=
 // max(rel2 * r.r at the start (scal[2]), abs2)

@@ -200,29 +200,12 @@ __global__ void k_cg_pupdate(const int32_t* __restrict__ rows, int count, CGVect
     }
 }
 
-__global__ void k_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2, int maxIter) {
+__global__ void k_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2) {
     *iter = 0;
     tgt[0] = rel2;
     tgt[1] = abs2;
-    tgt[2] = (double)maxIter;
 }
 __global__ void k_cg_replay_step(int32_t* iter) { *iter += 1; }
-
-// The condition of the device-side loop around the replayed node-space CG
-// iteration: go on while fewer than the cap (tgt[2]) have run and
-// r.r > max(rel2 r.r_0, abs2); a NaN stops it.  *done gets the iterations
-// the solve took (0 when r.r_0 met the target already, as the host loop
-// counts them).  The counter steps once per body, so the loop ends by the
-// cap at the latest.
-__global__ void k_cg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal,
-                               const double* tgt, int32_t* done) {
-    const int k = *iter;
-    const double target = fmax(tgt[0] * scal[2], tgt[1]);
-    const bool started = scal[2] > target;
-    const bool more = started && k < (int)tgt[2] && scal[3 * k + 2] > target;
-    *done = started ? k : 0;
-    cudaGraphSetConditional(loop, more ? 1u : 0u);
-}
 
 __global__ void k_add_coupled(DevMesh m, const int32_t* __restrict__ rows, int count, const float* xV, float* r) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -366,14 +349,9 @@ void launch_cg_iter(const DevMesh& m, const int32_t* rows, int count, CGVectors 
     { count_launch(); k_cg_update<<<blocks(count), kBlock, 0, s>>>(m, rows, count, v, it, rel2, abs2); }
     { count_launch(); k_cg_pupdate<<<blocks(count), kBlock, 0, s>>>(rows, count, v, it, rel2, abs2); }
 }
-void launch_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2, int maxIter, cudaStream_t s) {
+void launch_cg_replay_begin(int32_t* iter, double* tgt, double rel2, double abs2, cudaStream_t s) {
     count_launch();
-    k_cg_replay_begin<<<1, 1, 0, s>>>(iter, tgt, rel2, abs2, maxIter);
-}
-void launch_cg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal, const double* tgt,
-                         int32_t* done, cudaStream_t s) {
-    count_launch();
-    k_cg_loop_cond<<<1, 1, 0, s>>>(loop, iter, scal, tgt, done);
+    k_cg_replay_begin<<<1, 1, 0, s>>>(iter, tgt, rel2, abs2);
 }
 void launch_cg_replay_step(int32_t* iter, cudaStream_t s) {
     count_launch();
