@@ -9,6 +9,11 @@
 //   tapsim_b200 [options] evaporation iconfig inode [results]
 //   tapsim_b200 [options] evaporation --input-dump=? iconfig [results]
 //   tapsim_b200 [options] resumption idump [results]
+//   tapsim_b200 [options] meshgen isample onodes   (meshgen's role,
+//     meshgen/meshgen.cpp:2506-3986: graded vacuum and the marked box around
+//     the sample node file; --create-config-template=? writes meshgen's
+//     configuration template, --box-half-width=?, --box-height=?,
+//     --fine-shell=? [m] size the box, --write-ascii the node file)
 // Options taken from the reference: --ini-file=?, --threads=?, --write-ascii,
 // --write-binary, --no-file-output, --skip-relaxation, --event-limit=?,
 // --voltage-queue-size=?, --vacuum-identifier=?, --no-chunks, --chunk-size=?.
@@ -62,6 +67,8 @@ struct Args {
     int warmStart = 0;
     int batch = 64;
     std::string records;      // --records: every event's tg_event_record, raw, in order
+    std::string sample, configTemplate;  // meshgen
+    double boxHalfWidth = -1.0, boxHeight = -1.0, fineShell = -1.0;
 };
 
 [[noreturn]] void die(const std::string& msg) {
@@ -105,10 +112,14 @@ Args parse(int argc, char** argv) {
         else if (opt(s, "warm-start", &v)) a.warmStart = std::atoi(v.c_str());
         else if (opt(s, "batch", &v)) a.batch = std::max(1, std::atoi(v.c_str()));
         else if (opt(s, "records", &v)) a.records = v;
+        else if (opt(s, "create-config-template", &v)) a.configTemplate = v;
+        else if (opt(s, "box-half-width", &v)) a.boxHalfWidth = std::atof(v.c_str());
+        else if (opt(s, "box-height", &v)) a.boxHeight = std::atof(v.c_str());
+        else if (opt(s, "fine-shell", &v)) a.fineShell = std::atof(v.c_str());
         else if (s.compare(0, 2, "--") == 0) die("unknown or invalid argument in command line: \"" + s + "\"");
         else pos.push_back(s);
     }
-    if (pos.empty()) die("usage: tapsim_b200 [options] evaporation|resumption ...");
+    if (pos.empty()) die("usage: tapsim_b200 [options] evaporation|resumption|meshgen ...");
     a.command = pos[0];
     if (a.command == "evaporation") {
         if (!a.dump.empty()) {
@@ -125,6 +136,10 @@ Args parse(int argc, char** argv) {
         if (pos.size() < 2) die("missing arguments for processing in 'resumption'-mode");
         a.dump = pos[1];
         if (pos.size() > 2) a.results = pos[2];
+    } else if (a.command == "meshgen") {
+        if (pos.size() < 3) die("missing arguments for 'meshgen': isample onodes");
+        a.sample = pos[1];
+        a.nodes = pos[2];
     } else {
         die("unknown command " + a.command);
     }
@@ -156,8 +171,31 @@ float length3(const float v[3]) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v
 
 }  // namespace
 
+// meshgen's role: the sample's vacuum mesh, written as a node file (binary
+// unless --write-ascii, as meshgen's ASCII_OUTPUT_MODE 0) and, with
+// --create-config-template, the configuration template beside it
+int meshgen(const Args& a) {
+    tg_sample_params p;
+    tg_sample_params_default(&p);
+    if (a.boxHalfWidth > 0.0) p.box_half_width = a.boxHalfWidth;
+    if (a.boxHeight > 0.0) p.box_height = a.boxHeight;
+    if (a.fineShell > 0.0) p.fine_shell = a.fineShell;
+    tg_mesh* mesh = nullptr;
+    check(tg_mesh_from_sample(a.sample.c_str(), nullptr, &p, a.threads, &mesh), nullptr, "meshing the sample");
+    check(tg_mesh_write_node_file(mesh, a.nodes.c_str(), a.binary == 0 ? 0 : 1), nullptr, "writing the node file");
+    if (!a.configTemplate.empty())
+        check(tg_mesh_write_config(mesh, a.configTemplate.c_str()), nullptr, "writing the configuration template");
+    tg_mesh_desc desc;
+    int32_t nnz = 0;
+    check(tg_mesh_describe(mesh, &desc, &nnz), nullptr, "tg_mesh_describe");
+    std::printf("meshgen: %d nodes, %d couplings, %d tetrahedra\n", desc.num_nodes, nnz, desc.num_tets);
+    tg_mesh_destroy(mesh);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     const Args a = parse(argc, argv);
+    if (a.command == "meshgen") return meshgen(a);
     const std::map<std::string, std::string> ini = read_ini(a.ini);
     auto I = [&](const char* k) { return std::atoi(ini.at(k).c_str()); };
     auto F = [&](const char* k) { return std::atof(ini.at(k).c_str()); };

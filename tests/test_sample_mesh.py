@@ -170,3 +170,29 @@ def test_apex_fields_match_the_tip_mesh(tip_and_sample):
     print("apex field magnitudes (tip mesh)", fields[0][:5], "relative differences: median", np.median(rel),
           "max", rel.max())
     assert np.median(rel) <= 0.05 and rel.max() <= 0.15
+
+
+def test_host_program_meshgen(tip_and_sample, tmp_path):
+    """`tapsim_b200 meshgen isample onodes` (meshgen's command line) writes the
+    node file and the configuration template of the same mesh that
+    tg_mesh_from_sample builds, and the evaporation path reads them back
+    (tg_mesh_from_files) to the same nodes."""
+    import subprocess
+
+    from conftest import ROOT
+    from tapsim_modified_b200.tapsim import Mesh
+    program = ROOT / "tapsim_modified_b200" / "tapsim_b200"
+    if not program.exists():
+        pytest.skip("the host program is built by __graft_entry__.build()")
+    _, _, _, path, _, _ = tip_and_sample
+    nodes, cfg = tmp_path / "mesh.nodes", tmp_path / "mesh.cfg"
+    r = subprocess.run([str(program), f"--box-half-width={BOX['box_half_width']}", f"--box-height={BOX['box_height']}",
+                        f"--fine-shell={SMALL_TIP['fine_shell']}", f"--create-config-template={cfg}", "meshgen",
+                        str(path), str(nodes)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "meshgen:" in r.stdout
+    direct = Mesh.from_sample(str(path), fine_shell=SMALL_TIP["fine_shell"], **BOX).arrays()
+    back = Mesh.from_files(str(nodes), str(cfg)).arrays()
+    for k in ("xyz", "type", "row_ptr", "col"):
+        assert np.array_equal(direct[k], back[k]), k
+    assert back["types"].keys() == direct["types"].keys()
