@@ -176,7 +176,6 @@ struct tg_handle {
         double sums[4];
         double r2[4];
         double sb[4 * 17];
-        double sbN[3 * 17];   // the node-space CG's scal[0..2] and a batch of iterations
         double before[4];     // phi and field_o1 of the removed cell before removal
         double after[4];      // and after
         float normal[4];
@@ -207,10 +206,6 @@ struct tg_handle {
     // the slots in use differ from the ones it was captured with.
     int launchMode = 2;                  // 2: the replayed graph in a device-side loop; 1: replay; 0: launch each kernel
     cudaStream_t captureStream = nullptr;
-    // the Neumann rows' inner solve runs on its own stream beside the V
-    // rows' correction and the next residual of the V rows
-    cudaStream_t nStream = nullptr;
-    cudaEvent_t evCoupled = nullptr, evNDone = nullptr;
     cudaGraphExec_t iterExec = nullptr;
     DBuf<int32_t> iterDev;               // [1] the replayed iterations' counter
     DBuf<double> rel2Dev;                // [2] their relative target and iteration cap
@@ -916,12 +911,6 @@ void tg_destroy(tg_handle* h) {
     h->cgIterDev.release();
     h->cgTgtDev.release();
     if (h->captureStream) cudaStreamDestroy(h->captureStream);
-    if (h->nStream) {
-        cudaStreamSynchronize(h->nStream);
-        cudaStreamDestroy(h->nStream);
-    }
-    if (h->evCoupled) cudaEventDestroy(h->evCoupled);
-    if (h->evNDone) cudaEventDestroy(h->evNDone);
     h->iterDev.release();
     h->rel2Dev.release();
     if (h->evSnap) cudaEventDestroy(h->evSnap);
@@ -1333,9 +1322,7 @@ static int cg_iteration_graph(tg_handle* h, int which, const DevMesh& m, const i
 extern "C" {
 
 static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, double rtol, int maxIter, int* itersOut,
-                  double absTarget2 = 0.0, cudaStream_t stream = nullptr) {
-    // the solve's stream: the handle's unless given
-    const cudaStream_t st = stream ? stream : h->stream;
+                  double absTarget2 = 0.0) {
     DevMesh m = h->dm();
     CGVectors v = h->cg(which);
     DBuf<double>& scal = which == 0 ? h->scalV : h->scalN;
@@ -1344,8 +1331,8 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
         CK(scal.alloc(need));
         v = h->cg(which);
     }
-    CK(cudaMemsetAsync(scal.p, 0, sizeof(double) * need, st));
-    launch_cg_init(m, rows, count, v, st);
+    CK(cudaMemsetAsync(scal.p, 0, sizeof(double) * need, h->stream));
+    launch_cg_init(m, rows, count, v, h->stream);
     // stop on the 2-norm of the residual (r.r at scal[3it+2]), the norm the
     // outer FP64 test uses: r.r <= max(rtol^2 r.r_0, absTarget2), tested by
     // the kernels themselves, so the iterations queue before r.r_0 is read
@@ -1360,32 +1347,31 @@ static int run_cg(tg_handle* h, int which, const int32_t* rows, int count, doubl
         vg.tgt = h->cgTgtDev.p;
         const int rc = cg_iteration_graph(h, which, m, rows, count, vg);
         if (rc != TG_OK) return rc;
-        launch_cg_replay_begin(h->cgIterDev.p, h->cgTgtDev.p, rel2, absTarget2, st);
+        launch_cg_replay_begin(h->cgIterDev.p, h->cgTgtDev.p, rel2, absTarget2, h->stream);
     }
     int it = 0;
     // iterations queued before the first read: one more than the last solve
     // of this system took, then small batches
     int& last = which == 0 ? h->lastItersCgV : h->lastItersCgN;
     int batch = std::min(16, std::max(2, last + 1));
-    double* s0 = h->pin->sbN;        // scal[0..2], then the batch's iterations
-    double* sb = h->pin->sbN + 3;
+    double sb[3 * 16], s0[3];
     while (it < maxIter) {
         const int start = it;
         const int end = std::min(maxIter, it + batch);
         for (; it < end; it++) {
             if (replay) {
-                CK(cudaGraphLaunch(h->cgExec[which], st));
+                CK(cudaGraphLaunch(h->cgExec[which], h->stream));
                 g_launches.fetch_add(h->cgNodes[which], std::memory_order_relaxed);
                 continue;
             }
-            launch_cg_iter(m, rows, count, v, it, rel2, absTarget2, st);
+            launch_cg_iter(m, rows, count, v, it, rel2, absTarget2, h->stream);
         }
         // r.r after j iterations sits at scal[3j+2]; the kernels of later
         // iterations of the batch returned early once it met the target
-        CK(cudaMemcpyAsync(s0, scal.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(s0, scal.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaMemcpyAsync(sb, scal.p + 3 * (size_t)(start + 1), sizeof(double) * 3 * (end - start),
-                           cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+                           cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
         const double target = std::max(s0[2] * rel2, absTarget2);
         if (!(s0[2] > target)) {
             // nothing to do: every queued iteration returned at once
@@ -1752,16 +1738,6 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         if (rc != TG_OK) return rc;
     }
     bool loopPending = false;  // a looped inner solve whose count is still on its way
-    // the next outer step's V-row residual was queued beside the Neumann
-    // rows' solve (the Neumann potentials do not enter the V rows' residual)
-    bool vResidualQueued = false;
-    if (h->countAllN > 0 && !h->nStream) {
-        int leastPriority = 0, greatestPriority = 0;
-        CK(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
-        CK(cudaStreamCreateWithPriority(&h->nStream, cudaStreamNonBlocking, greatestPriority));
-        CK(cudaEventCreateWithFlags(&h->evCoupled, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&h->evNDone, cudaEventDisableTiming));
-    }
     for (int outer = 0;; outer++) {
         if (outer == 0 && incremental) {
             if (warm && !warmFirst) {
@@ -1774,12 +1750,9 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
             // a full pass; the first one also takes the Dirichlet parts, so
             // that the kept values describe the rows as they are
             if (outer == 0) needB = true;
-            if (!vResidualQueued) {
-                CK(cudaMemsetAsync(h->rsum.p, 0, (needB ? 3 : 2) * sizeof(double), h->stream));
-                launch_vcg_residual(m, vsys, h->allV.p, h->countAllV, h->rsum.p, needB ? h->rsum.p + 2 : nullptr,
-                                    h->stream, rv, bv);
-            }
-            vResidualQueued = false;
+            CK(cudaMemsetAsync(h->rsum.p, 0, (needB ? 3 : 2) * sizeof(double), h->stream));
+            launch_vcg_residual(m, vsys, h->allV.p, h->countAllV, h->rsum.p, needB ? h->rsum.p + 2 : nullptr,
+                                h->stream, rv, bv);
             launch_residual(m, h->allN.p, h->countAllN, vN.r, h->rsum.p + 1, h->stream,
                             needB ? h->rsum.p + 2 : nullptr, rv, bv);
         }
@@ -1825,31 +1798,13 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
             if (rc != TG_OK) return rc;
         }
         if (h->countAllN > 0) {
-            // the Neumann rows' right-hand side takes the V rows' correction
-            // (before the correction is applied, which clears it)
             launch_vcg_couple_neumann(m, vsys, h->allN.p, h->countAllN, vN.r, h->stream, fp64);
-            CK(cudaEventRecord(h->evCoupled, h->stream));
-            CK(cudaStreamWaitEvent(h->nStream, h->evCoupled, 0));
-        }
-        if (fp64) launch_vcg64_apply(m, vsys, h->vActive, fromEvent, h->stream);
-        else launch_vcg_apply(m, vsys, h->vActive, fromEvent, h->stream);
-        // the next outer step's V-row residual, on the handle's stream beside
-        // the Neumann rows' solve on their own
-        CK(cudaMemsetAsync(h->rsum.p, 0, (needB ? 3 : 2) * sizeof(double), h->stream));
-        launch_vcg_residual(m, vsys, h->allV.p, h->countAllV, h->rsum.p, needB ? h->rsum.p + 2 : nullptr, h->stream,
-                            rv, bv);
-        vResidualQueued = true;
-        if (h->countAllN > 0) {
             // the Neumann rows' share of the global residual only has to fall
             // below 0.3 of the outer tolerance (the V rows' solve brings
             // theirs to about the same), whatever their own start
             const double floorN = 0.3 * o->rel_tol;
-            rc = run_cg(h, 1, h->allN.p, h->countAllN, rtol, o->max_inner, &itN, floorN * floorN * h->bnorm2,
-                        h->nStream);
+            rc = run_cg(h, 1, h->allN.p, h->countAllN, rtol, o->max_inner, &itN, floorN * floorN * h->bnorm2);
             if (rc != TG_OK) return rc;
-            launch_apply_correction(m, h->allN.p, h->countAllN, vN, h->nStream);
-            CK(cudaEventRecord(h->evNDone, h->nStream));
-            CK(cudaStreamWaitEvent(h->stream, h->evNDone, 0));
         }
         if (itV < 0) {
             loopPending = true;
@@ -1857,6 +1812,9 @@ int tg_solve(tg_handle* h, const tg_solve_opts* o, tg_solve_info* info) {
         }
         inf.inner += itV + itN;
         inf.inner_neumann += itN;
+        if (fp64) launch_vcg64_apply(m, vsys, h->vActive, fromEvent, h->stream);
+        else launch_vcg_apply(m, vsys, h->vActive, fromEvent, h->stream);
+        launch_apply_correction(m, h->allN.p, h->countAllN, vN, h->stream);
     }
     h->selValid = false;
     h->converged = true;
