@@ -196,3 +196,36 @@ def test_host_program_meshgen(tip_and_sample, tmp_path):
     for k in ("xyz", "type", "row_ptr", "col"):
         assert np.array_equal(direct[k], back[k]), k
     assert back["types"].keys() == direct["types"].keys()
+
+
+@pytest.mark.gpu
+def test_events_run_on_the_sample_mesh(tip_and_sample):
+    """The event loop on the sample's own vacuum mesh: every event removes a
+    surface atom of the specimen, relaxes to the tolerance and sends its ion
+    to the detector, and its first removals are the tip mesh's first ones
+    (the same specimen, the same surface; measured: the same eight atoms,
+    one of them taken earlier)."""
+    from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
+    from conftest import GOLDEN
+    tip, a, atoms, path, _, cfg = tip_and_sample
+    m = sample_mesh(path, cfg)
+    b = m.arrays()
+    n_s = int(atoms.sum())
+    first = len(b["type"]) - n_s
+    opts = EvaporationOptions.from_ini(str(GOLDEN / "oracle.ini"))
+    sopts = solve_opts(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1)
+    removed = {}
+    for name, mesh, offset in (("tip", tip, None), ("sample", m, first)):
+        g = Grid(mesh)
+        g.solve(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1)
+        recs = Evaporation(g, opts, relax_mode=1, solve=sopts).run(8)
+        g.close()
+        assert all(r["status"] == 5 and r["rel_residual"] <= 1e-10 for r in recs), name
+        if offset is None:
+            s_tip = np.flatnonzero(atoms)
+            removed[name] = [int(np.searchsorted(s_tip, r["node"])) for r in recs]
+        else:
+            assert all(r["node"] >= offset for r in recs)       # a specimen atom
+            removed[name] = [r["node"] - offset for r in recs]
+    print("first removals (sample index): tip mesh", removed["tip"], "sample mesh", removed["sample"])
+    assert len(set(removed["tip"]) & set(removed["sample"])) >= 6
