@@ -641,7 +641,9 @@ def run_probe_ions(args):
     detector three times: in FP64, in FP32 (the reference's arithmetic) and
     mixed (FP64 within 3 cap radii of the start, FP32 beyond).  Reports the
     probe launches' ions/s and accepted steps/s (CUDA events on the handle's
-    stream) and the FP32 and mixed hit maps against the FP64 one."""
+    stream), the integrator's trials per ion (accepted and rejected; a warp
+    waits for its slowest ion), and the FP32 and mixed hit maps against the
+    FP64 one."""
     import ctypes as C
 
     import numpy as np
@@ -667,6 +669,7 @@ def run_probe_ions(args):
     modes = {"fp64": dict(precision=0), "fp32": dict(precision=1), "mixed": dict(precision=2, fp64_radius=fp64_radius)}
     ms = {k: 0.0 for k in modes}
     steps = {k: 0 for k in modes}
+    trials = {k: [] for k in modes}   # integrator trials (accepted and rejected) per ion
     dev = {k: [] for k in ("fp32", "mixed")}
     status_ok = {k: 0 for k in modes}
     ev_ms = 0.0
@@ -694,6 +697,7 @@ def run_probe_ions(args):
             N.check(L.tg_timer_stop(g._h, C.byref(t)), g._h)
             ms[name] += t.value
             steps[name] += sum(r.steps for r in imp[name])
+            trials[name].extend(r.trials for r in imp[name])
             status_ok[name] += sum(r.status == 5 for r in imp[name])
         ions += len(pick)
         ref = np.array([[r.stop[0], r.stop[1]] for r in imp["fp64"]], np.float64)
@@ -715,6 +719,9 @@ def run_probe_ions(args):
                       "probe": {name: {"ms_per_launch": ms[name] / args.steps, "ions_per_s": ions / (ms[name] / 1e3),
                                        "steps_per_s": steps[name] / (ms[name] / 1e3),
                                        "steps_per_ion": steps[name] / ions,
+                                       "trials_per_ion": {"mean": float(np.mean(trials[name])),
+                                                          "p99": float(np.percentile(trials[name], 99)),
+                                                          "max": int(np.max(trials[name]))},
                                        "reached_detector": status_ok[name] / ions} for name in modes},
                       "hit_map_vs_fp64": {name: {"median_rel_impact_diff": float(np.median(v)),
                                                  "p99_rel_impact_diff": float(np.percentile(v, 99)),

@@ -294,6 +294,7 @@ typedef struct {
     float last_phi;             /* Grid_3d::potential at last_pos [V] */
     int32_t steps;              /* accepted steps */
     int32_t status;             /* TG_TRAJ_* */
+    int32_t trials;             /* integrator trial steps, accepted and rejected */
 } tg_impact;
 /* Trajectory_3d::init/integrate/extrapolate (trajectory_3d.cpp:99-209,
  * 303-332) with o5_integrator (Cash-Karp, :583-676) and

@@ -66,7 +66,8 @@ class tg_trace_opts(C.Structure):
 
 class tg_impact(C.Structure):
     _fields_ = [("stop", C.c_float * 3), ("stop_time", C.c_float), ("last_pos", C.c_float * 3),
-                ("last_tet", C.c_int32), ("last_phi", C.c_float), ("steps", C.c_int32), ("status", C.c_int32)]
+                ("last_tet", C.c_int32), ("last_phi", C.c_float), ("steps", C.c_int32), ("status", C.c_int32),
+                ("trials", C.c_int32)]
 
 
 class tg_path_point(C.Structure):

@@ -587,6 +587,7 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
     double time = 0.0;
     int tet = locate(m, x, guessTet, tp.walk_limit, rot);
     res.steps = 0;
+    res.trials = 0;
     res.last_tet = tet;
     res.last_pos[0] = (float)x.x; res.last_pos[1] = (float)x.y; res.last_pos[2] = (float)x.z;
     res.last_phi = 0.0f;
@@ -625,6 +626,7 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
             const bool lo = kPrec != 0 && tp.integrator == 1 &&
                             (kPrec == 1 || ddx * ddx + ddy * ddy + ddz * ddz > tp.fp64_radius2);
             for (int tries = 0; tries < tp.stepper_limit; tries++) {
+                res.trials++;
                 if (lo) {
                     if ((float)dt < (float)tp.dt_min) dt = (double)(float)tp.dt_min;
                 } else if (dt < tp.dt_min) {

@@ -323,6 +323,7 @@ struct ImpactOut {
     float last_phi;
     int32_t steps;
     int32_t status;
+    int32_t trials;  // integrator trial steps, accepted and rejected
 };
 // packed tetrahedron records (32 words each) from tet_v, tet_n and xyz
 void launch_pack_tets(const DevMesh& m, float* pack, cudaStream_t s);
