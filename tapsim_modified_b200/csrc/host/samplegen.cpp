@@ -158,6 +158,11 @@ struct Builder {
     double W, H, h0;
     double bmin[3], bmax[3];  // the sample's bounding box
     std::vector<double> levelSpacing, levelOuter;
+    // atoms per cell of a grid with cells of fine_shell over the bounding
+    // box (one cell of margin): a point whose 27 cells hold no atom lies
+    // farther than the fine shell from the sample
+    std::vector<uint8_t> occ;
+    int64_t occN[3] = {0, 0, 0};
     SampleMesh mesh;
 
     Builder(const SampleParams& params, const KdTree& t, int nThreads, const std::vector<float>& xyz)
@@ -193,6 +198,28 @@ struct Builder {
         }
         levelOuter.back() = 1e300;
         mesh.spacing = h0;
+        for (int a = 0; a < 3; a++) occN[a] = (int64_t)std::ceil((bmax[a] - bmin[a]) / S) + 3;
+        occ.assign((size_t)(occN[0] * occN[1] * occN[2]), 0);
+        for (size_t k = 0; k < xyz.size(); k += 3) {
+            int64_t c[3];
+            for (int a = 0; a < 3; a++) c[a] = occ_cell(xyz[k + a], a);
+            occ[(size_t)((c[0] * occN[1] + c[1]) * occN[2] + c[2])] = 1;
+        }
+    }
+
+    int64_t occ_cell(double v, int a) const { return (int64_t)std::floor((v - (bmin[a] - p.fine_shell)) / p.fine_shell); }
+    // false when no atom lies within fine_shell of q (its 27 cells are empty)
+    bool atom_in_reach(double x, double y, double z) const {
+        const double q[3] = {x, y, z};
+        int64_t c[3];
+        for (int a = 0; a < 3; a++) c[a] = occ_cell(q[a], a);
+        for (int64_t i = c[0] - 1; i <= c[0] + 1; i++)
+            for (int64_t j = c[1] - 1; j <= c[1] + 1; j++)
+                for (int64_t k = c[2] - 1; k <= c[2] + 1; k++) {
+                    if (i < 0 || j < 0 || k < 0 || i >= occN[0] || j >= occN[1] || k >= occN[2]) continue;
+                    if (occ[(size_t)((i * occN[1] + j) * occN[2] + k)]) return true;
+                }
+        return false;
     }
 
     // median nearest-neighbour distance over up to 4096 evenly spaced atoms
@@ -315,6 +342,10 @@ struct Builder {
                         if (q[0] <= -W + m || q[0] >= W - m || q[1] <= -W + m || q[1] >= W - m || q[2] <= m ||
                             q[2] >= H - m)
                             return;
+                        // cheap tests first (the merge below would reject
+                        // these too): a site of an earlier generation there
+                        // already, or no atom within the fine shell
+                        if (site_near(q, 0.5 * h0) || !atom_in_reach(q[0], q[1], q[2])) return;
                         const double d = std::sqrt(tree.nearest2(q));
                         if (d < std::max(excl, 0.5 * h0) || d > S) return;
                         out.insert(out.end(), q, q + 3);
@@ -378,12 +409,14 @@ struct Builder {
                     const double m = 0.2 * h;
                     if (x <= -W + m || x >= W - m || y <= -W + m || y >= W - m || z <= m || z >= H - m) continue;
                     if (box_distance(x, y, z) > dOut) continue;
+                    if (k == 0) {
+                        // level 0 ends at the fine shell, and the lattice's
+                        // sites fill it in a crystal: two cheap tests first
+                        const double q[3] = {x, y, z};
+                        if (!atom_in_reach(x, y, z) || site_near(q, excl)) continue;
+                    }
                     const double d = distance(x, y, z);
                     if (d <= dIn || d > dOut || d < excl) continue;
-                    if (k == 0) {
-                        const double q[3] = {x, y, z};
-                        if (site_near(q, excl)) continue;
-                    }
                     out.push_back((float)x);
                     out.push_back((float)y);
                     out.push_back((float)z);
