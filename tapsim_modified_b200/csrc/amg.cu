@@ -39,6 +39,31 @@ __global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, Ga
 // all, so it is spectrally within a fraction of a percent of it; the
 // smoothing steps divide by the FP32 diagonal d on both sides of the cycle,
 // which keeps the preconditioner symmetric.
+// The entries k..width-1 (fewer than U) of a lane's row as one round: every
+// column and value load is issued before the first gather, so that a slice's
+// remainder costs one round trip, not one per entry.  The sums take the
+// entries in the same order as a loop over them would.
+template <int U>
+__device__ __forceinline__ void fine_last_round(const int* __restrict__ col, const __nv_bfloat16* __restrict__ val,
+                                                const float* __restrict__ y, int k, int width, float& acc,
+                                                float& sum) {
+    if (k >= width) return;
+    int c[U];
+    float a[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+        const bool in = k + j < width;
+        c[j] = in ? __ldcs(col + 32 * (k + j)) : 0;
+        a[j] = in ? __bfloat162float(__ldcs(val + 32 * (k + j))) : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++)
+        if (k + j < width) {
+            acc += a[j] * __ldg(y + c[j]);
+            sum += a[j];
+        }
+}
+
 // U: the column/value loads a lane issues ahead of their gathers (the bytes
 // a warp keeps in flight), chosen per hierarchy by timed trials.
 template <int U>
@@ -68,11 +93,7 @@ __global__ void k_amg_fine(VSys v, int slices, const float* b, const float* y, f
                 sum += a[j];
             }
         }
-        for (; k < width; k++) {
-            const float a = __bfloat162float(__ldcs(val + 32 * k));
-            acc += a * __ldg(y + __ldcs(col + 32 * k));
-            sum += a;
-        }
+        fine_last_round<U>(col, val, y, k, width, acc, sum);
         const float ys = y[s];
         const float t = b[s] - ((v.g[s] + sum) * ys - acc);
         out[s] = mode == 0 ? t : ys + kSmooth * t / v.d[s];
@@ -130,11 +151,7 @@ __global__ void k_amg_fine_pipe(VSys v, int slices, const float* b, const float*
                 }
             }
         }
-        for (int k = rounds * U; k < width; k++) {
-            const float a1 = __bfloat162float(__ldcs(val + 32 * k));
-            acc += a1 * __ldg(y + __ldcs(col + 32 * k));
-            sum += a1;
-        }
+        fine_last_round<U>(col, val, y, rounds * U, width, acc, sum);
         const float ys = y[s];
         const float t = b[s] - ((v.g[s] + sum) * ys - acc);
         out[s] = mode == 0 ? t : ys + kSmooth * t / v.d[s];

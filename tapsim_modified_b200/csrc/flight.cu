@@ -321,10 +321,11 @@ __device__ __forceinline__ bool beyond(const DevMesh& m, const TetSlot& S, int k
 }
 
 // findTetrahedron through the cache: on return c.a holds p's tetrahedron
-// (result 0), or -1 when p is outside the mesh, -2 when the walk exceeded
-// its bound.  The faces are tested in an order rotating from walk step to
+// (result 0; *found, when given, p's barycentric coordinates in it), or -1
+// when p is outside the mesh, -2 when the walk exceeded its bound.  The faces are tested in an order rotating from walk step to
 // walk step; the walk leaves through the first face p lies beyond.
-__device__ __forceinline__ int locate_cached(const DevMesh& m, TetCache& c, V3 p, int t, int limit, unsigned& rot) {
+__device__ __forceinline__ int locate_cached(const DevMesh& m, TetCache& c, V3 p, int t, int limit, unsigned& rot,
+                                             Bary* found = nullptr) {
     if (t < 0) return -1;
     for (int step = 0; step < limit; step++) {
         cache_tet(m, c, t);
@@ -345,7 +346,10 @@ __device__ __forceinline__ int locate_cached(const DevMesh& m, TetCache& c, V3 p
                 }
             }
         }
-        if (!moved) return 0;
+        if (!moved) {
+            if (found) *found = b;
+            return 0;
+        }
         if (next < 0) return -1;
         t = next;
     }
@@ -358,7 +362,8 @@ __device__ __forceinline__ int locate_cached(const DevMesh& m, TetCache& c, V3 p
 __device__ __forceinline__ bool fast_field(const DevMesh& m, TetCache& c, V3 p, int guess, int limit, unsigned& rot, V3* E,
                            int* located) {
     *E = V3{0, 0, 0};
-    const int sl = locate_cached(m, c, p, guess, limit, rot);
+    Bary b;  // the walk's last coordinates: p's in the tetrahedron it found
+    const int sl = locate_cached(m, c, p, guess, limit, rot, &b);
     if (sl == -2) return false;
     if (sl < 0) return true;
     TetSlot& S = c.a;
@@ -372,7 +377,6 @@ __device__ __forceinline__ bool fast_field(const DevMesh& m, TetCache& c, V3 p, 
     }
     double w0 = 0.25, w1 = 0.25, w2 = 0.25, w3 = 0.25;
     if (S.vol6 != 0.0f) {
-        const Bary b = lambdas(S, p);
         w0 = fabs(b.l0);
         w1 = fabs(b.l1);
         w2 = fabs(b.l2);
@@ -495,34 +499,65 @@ __device__ __forceinline__ void path_error(const TraceParams& tp, int slot) {
 // located and their fields interpolated as in FP64, then rounded to R.
 // *rel: the largest relative error of a position or velocity component (as
 // errorRestricted_stepper forms it, trajectory_3d.cpp:366-387).  Returns
-// false when a walk exceeded its bound.
+// false when a walk exceeded its bound.  s0: the first stage's field, kept
+// across the trials of a step.
+// The stages run as a loop that is not unrolled, the tableau's rows read from
+// constant memory: the kernel then holds one copy of the point location and
+// interpolation in its hot loop instead of six.  A flight is a long chain of
+// dependent steps on few warps per SM, and the unrolled body stalled on
+// instruction fetch more than on anything else; the arithmetic, and so every
+// result, is the same.
+__constant__ double kCashKarpB[6][5] = {{0, 0, 0, 0, 0},
+                                        {1.0 / 5.0, 0, 0, 0, 0},
+                                        {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
+                                        {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0, 0, 0},
+                                        {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0, 0},
+                                        {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0,
+                                         253.0 / 4096.0}};
+// The first stage's field of the current state.  Every trial of a step
+// evaluates its first stage at the same point, so a retried trial (after the
+// stepper shrank dt) takes the field from here and starts its next walk from
+// the tetrahedron it was found in.  The tetrahedron holding a point does not
+// depend on where a walk to it starts (short of a point on a shared face,
+// where both sides interpolate the same field), so the flights are those of
+// the recomputation; on 4096 probe ions in each precision they were
+// identical bit for bit.
+struct Stage0 {
+    V3 E;
+    int tet;
+    bool have;
+};
 template <typename R>
 __device__ __forceinline__ bool ck_trial(const DevMesh& m, TetCache& fc, const TraceParams& tp, unsigned& rot, int& cur,
                                          V3 x, V3 v, double k, double dt, V3* nxo, V3* nvo, V3* exo, V3* evo,
-                                         double* relo) {
-    constexpr double B[6][5] = {{0, 0, 0, 0, 0},
-                                {1.0 / 5.0, 0, 0, 0, 0},
-                                {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
-                                {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0, 0, 0},
-                                {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0, 0},
-                                {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+                                         double* relo, Stage0& s0) {
     constexpr double C5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
     constexpr double C4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
     const R xx = (R)x.x, xy = (R)x.y, xz = (R)x.z, vx = (R)v.x, vy = (R)v.y, vz = (R)v.z;
     const R kk = (R)k, h = (R)dt;
     R dx[6][3], dv[6][3];
     bool walkOk = true;
-#pragma unroll
+#pragma unroll 1
     for (int s = 0; s < 6; s++) {
         R px = xx, py = xy, pz = xz, qx = vx, qy = vy, qz = vz;
-#pragma unroll
+#pragma unroll 1
         for (int j = 0; j < s; j++) {
-            const R b = (R)B[s][j];
+            const R b = (R)kCashKarpB[s][j];
             px += b * dx[j][0]; py += b * dx[j][1]; pz += b * dx[j][2];
             qx += b * dv[j][0]; qy += b * dv[j][1]; qz += b * dv[j][2];
         }
         V3 E;
-        walkOk &= fast_field(m, fc, V3{(double)px, (double)py, (double)pz}, cur, tp.walk_limit, rot, &E, &cur);
+        if (s == 0 && s0.have) {
+            E = s0.E;
+            cur = s0.tet;
+        } else {
+            walkOk &= fast_field(m, fc, V3{(double)px, (double)py, (double)pz}, cur, tp.walk_limit, rot, &E, &cur);
+            if (s == 0) {
+                s0.E = E;
+                s0.tet = cur;
+                s0.have = true;
+            }
+        }
         dv[s][0] = (R)E.x * kk * h; dv[s][1] = (R)E.y * kk * h; dv[s][2] = (R)E.z * kk * h;
         dx[s][0] = qx * h; dx[s][1] = qy * h; dx[s][2] = qz * h;
     }
@@ -625,6 +660,8 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
             const double ddx = x.x - x0.x, ddy = x.y - x0.y, ddz = x.z - x0.z;
             const bool lo = kPrec != 0 && tp.integrator == 1 &&
                             (kPrec == 1 || ddx * ddx + ddy * ddy + ddz * ddz > tp.fp64_radius2);
+            Stage0 s0;
+            s0.have = false;
             for (int tries = 0; tries < tp.stepper_limit; tries++) {
                 res.trials++;
                 if (lo) {
@@ -653,10 +690,10 @@ __device__ __forceinline__ void trace_ion(const DevMesh& m, V3 x, V3 v, double k
                 V3 ex, evv;
                 double rel;
                 bool walkOk;
-                if (kPrec == 1) walkOk = ck_trial<float>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel);
-                else if (kPrec == 0) walkOk = ck_trial<double>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel);
-                else walkOk = lo ? ck_trial<float>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel)
-                                 : ck_trial<double>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel);
+                if (kPrec == 1) walkOk = ck_trial<float>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel, s0);
+                else if (kPrec == 0) walkOk = ck_trial<double>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel, s0);
+                else walkOk = lo ? ck_trial<float>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel, s0)
+                                 : ck_trial<double>(m, fc, tp, rot, cur, x, v, k, dt, &nx, &nv, &ex, &evv, &rel, s0);
                 if (!walkOk) atomicOr(m.status, S_WALK_LIMIT);
                 if (kPath) path_trial_error(tp, slot, ex, evv);
                 if (tp.stepper != 1) {
