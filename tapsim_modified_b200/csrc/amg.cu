@@ -23,7 +23,7 @@ constexpr int kBlock = 256;
 // diagonally dominant matrices) and the cycle stays symmetric positive
 // definite; 0.9 took 21 CG iterations to 1e-8 on the 3.2M-row system of the
 // 7.3M-cell tip where 2/3 took 27
-constexpr float kSmooth = 0.9f;
+constexpr float kSmooth = kAmgSmooth;
 
 // y = w b / d
 __global__ void k_amg_jacobi(int n, const float* b, const float* d, float* y, Gate gate) {
@@ -203,16 +203,21 @@ __global__ void k_amg_csr(int n, const int32_t* ptr, const int32_t* col, const f
     }
 }
 
-// out = M y for a CSR matrix (restriction R t)
+// out = M y for a CSR matrix (restriction R t); with diag, also the coarse
+// level's pre-smoothing step ysm = w out / diag (the Jacobi step of the level
+// it restricts to, in the same arithmetic as k_amg_jacobi)
 template <int L>
 __global__ void k_amg_mv(int n, const int32_t* ptr, const int32_t* col, const float* val, const float* y, float* out,
-                         Gate gate) {
+                         const float* diag, float* ysm, Gate gate) {
     if (gate.done()) return;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = gid % L;
     const int row = min(gid / L, n - 1);
     const float acc = row_dot<L>(ptr, col, val, y, row, lane);
-    if (lane == 0 && gid / L < n) out[row] = acc;
+    if (lane == 0 && gid / L < n) {
+        out[row] = acc;
+        if (diag) ysm[row] = kSmooth * acc / diag[row];
+    }
 }
 
 // y += P x' (prolongation, a few entries per row), one thread per row
@@ -273,14 +278,14 @@ void launch_csr(int L, int n, const int32_t* ptr, const int32_t* col, const floa
     }
 }
 void launch_mv(int L, int n, const int32_t* ptr, const int32_t* col, const float* val, const float* y, float* out,
-               Gate gate, cudaStream_t s) {
+               Gate gate, cudaStream_t s, const float* diag = nullptr, float* ysm = nullptr) {
     count_launch();
     switch (L) {
-        case 2: k_amg_mv<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
-        case 4: k_amg_mv<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
-        case 8: k_amg_mv<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
-        case 16: k_amg_mv<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
-        default: k_amg_mv<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, y, out, gate); break;
+        case 2: k_amg_mv<2><<<grid_rows(n, 2), kBlock, 0, s>>>(n, ptr, col, val, y, out, diag, ysm, gate); break;
+        case 4: k_amg_mv<4><<<grid_rows(n, 4), kBlock, 0, s>>>(n, ptr, col, val, y, out, diag, ysm, gate); break;
+        case 8: k_amg_mv<8><<<grid_rows(n, 8), kBlock, 0, s>>>(n, ptr, col, val, y, out, diag, ysm, gate); break;
+        case 16: k_amg_mv<16><<<grid_rows(n, 16), kBlock, 0, s>>>(n, ptr, col, val, y, out, diag, ysm, gate); break;
+        default: k_amg_mv<32><<<grid_rows(n, 32), kBlock, 0, s>>>(n, ptr, col, val, y, out, diag, ysm, gate); break;
     }
 }
 
@@ -364,7 +369,11 @@ int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* a
         AmgDevLevel& C = g.lev[l + 1];
         if (rMs)
             rMs[l] = time_launches(
-                [&] { launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, l == 0 ? g.t0 : L.t, C.b, open_gate(), s); },
+                [&] {
+                    const bool last = l + 2 == g.levels;  // C is the coarsest level (dense solve)
+                    launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, l == 0 ? g.t0 : L.t, C.b, open_gate(), s,
+                              last ? nullptr : C.diag, last ? nullptr : C.y);
+                },
                 kTrials, s, e0, e1);
         if (aMs && l + 2 < g.levels)
             aMs[l + 1] = time_launches(
@@ -381,12 +390,15 @@ void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStr
     launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, open_gate(), s);
 }
 
-void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s) {
+void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s,
+                       bool y0Ready) {
     const Gate gate = make_gate(v, it, target);
     // level 0: b = r, output u
     const int slices = (slots + 31) / 32;
-    count_launch();
-    k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.r, v.d, g.y0, gate);
+    if (!y0Ready) {
+        count_launch();
+        k_amg_jacobi<<<grid_for(slots), kBlock, 0, s>>>(slots, v.r, v.d, g.y0, gate);
+    }
     if (g.levels > 1) {
         launch_fine(g.fine_unroll, v, slices, v.r, g.y0, g.t0, 0, gate, s);
         // down: restrict, smooth, residual
@@ -394,13 +406,13 @@ void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double
             const AmgDevLevel& L = g.lev[l];
             const AmgDevLevel& C = g.lev[l + 1];
             const float* t = l == 0 ? g.t0 : L.t;
-            launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, gate, s);
             if (l + 1 == g.levels - 1) {
+                launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, gate, s);
                 count_launch();
                 k_amg_dense<<<grid_for((long long)C.n * 32), kBlock, 0, s>>>(C.n, g.coarse_inv, C.b, C.x, gate);
             } else {
-                count_launch();
-                k_amg_jacobi<<<grid_for(C.n), kBlock, 0, s>>>(C.n, C.b, C.diag, C.y, gate);
+                // the restriction also takes the coarse level's pre-smoothing step
+                launch_mv(L.r_lanes, C.n, L.r_ptr, L.r_col, L.r_val, t, C.b, gate, s, C.diag, C.y);
                 launch_csr(C.a_lanes, C.n, C.a_ptr, C.a_col, C.a_val, C.diag, C.b, C.y, C.t, 0, gate, s);
             }
         }

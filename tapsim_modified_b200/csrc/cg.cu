@@ -111,8 +111,9 @@ __global__ void k_vcg_spmv(VSys v, int slices, Gate gate, int withGamma) {
 
 // p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s,
 // rho_{it+1} = r.r; with the Jacobi preconditioner also u = r / d and
-// gamma_{it+1} = r.u
-__global__ void k_vcg_update(VSys v, int slots, Gate gate, int jacobi) {
+// gamma_{it+1} = r.u; with smoothY (the multigrid one) the V-cycle's first
+// step smoothY = w r / d, one launch fewer per iteration
+__global__ void k_vcg_update(VSys v, int slots, Gate gate, int jacobi, float* smoothY) {
     if (gate.done()) return;
     const int it = gate.iter();
     double alpha, beta;
@@ -132,6 +133,8 @@ __global__ void k_vcg_update(VSys v, int slots, Gate gate, int jacobi) {
             const float u = r / v.d[s];
             v.u[s] = u;
             g += (double)r * (double)u;
+        } else if (smoothY) {
+            smoothY[s] = kAmgSmooth * r / v.d[s];  // as k_amg_jacobi computes it
         }
         rr += (double)r * (double)r;
     }
@@ -566,10 +569,12 @@ void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withG
         k_vcg_spmv<<<blocks(slices * 32), kBlock, 0, s>>>(v, slices, make_gate(v, it, target), withGamma ? 1 : 0);
     }
 }
-void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s) {
+void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s,
+                       float* smoothY) {
     if (slots > 0) {
         count_launch();
-        k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, make_gate(v, it, target), jacobi ? 1 : 0);
+        k_vcg_update<<<reduce_blocks(slots), kBlock, 0, s>>>(v, slots, make_gate(v, it, target), jacobi ? 1 : 0,
+                                                             jacobi ? nullptr : smoothY);
     }
 }
 void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, int maxIter, cudaStream_t s) {

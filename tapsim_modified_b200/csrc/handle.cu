@@ -1227,8 +1227,8 @@ static int iteration_graph(tg_handle* h, const VSys& vg) {
     const cudaError_t e = capture_graph(
         h,
         [&](cudaStream_t cs) {
-            launch_vcg_update(vg, slots, 0, -1.0, false, cs);
-            launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs);
+            launch_vcg_update(vg, slots, 0, -1.0, false, cs, h->amg.y0);
+            launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs, true);
             launch_vcg_spmv(vg, slots, 1, -1.0, true, cs);
             launch_vcg_replay_step(h->iterDev.p, cs);
         },
@@ -1274,8 +1274,8 @@ static int iteration_loop_graph(tg_handle* h, const VSys& vg) {
                                           cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             cudaStream_t cs = h->captureStream;
-            launch_vcg_update(vg, slots, 0, -1.0, false, cs);
-            launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs);
+            launch_vcg_update(vg, slots, 0, -1.0, false, cs, h->amg.y0);
+            launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs, true);
             launch_vcg_spmv(vg, slots, 1, -1.0, true, cs);
             launch_vcg_replay_step(h->iterDev.p, cs);
             launch_vcg_loop_cond(loop, h->iterDev.p, vg.scal, h->rel2Dev.p, h->loopDone.p, cs);
@@ -1598,8 +1598,8 @@ static int run_vcg(tg_handle* h, double rtol, int maxIter, bool amg, int* itersO
                 g_launches.fetch_add(h->iterNodes, std::memory_order_relaxed);
                 continue;
             }
-            launch_vcg_update(v, slots, it, rel2, !amg, h->stream);
-            if (amg) launch_amg_vcycle(v, slots, h->amg, it + 1, rel2, h->stream);
+            launch_vcg_update(v, slots, it, rel2, !amg, h->stream, amg ? h->amg.y0 : nullptr);
+            if (amg) launch_amg_vcycle(v, slots, h->amg, it + 1, rel2, h->stream, true);
             launch_vcg_spmv(v, slots, it + 1, rel2, amg, h->stream);
         }
         // rho after j iterations sits at scal[4j+3]; the kernels of later

@@ -79,6 +79,9 @@ struct Surface {
 // Non-Neumann free rows in their own slot order, couplings in SELL-32
 // (cg.cu).  Vectors hold capacity+1 entries; entry `capacity` is the zero
 // slot that entries of non-free neighbours point at.
+// damped-Jacobi weight of the multigrid's smoothing steps (amg.cu)
+constexpr float kAmgSmooth = 0.9f;
+
 struct VSys {
     int32_t* slot_of;             // [n] node -> slot, -1
     int32_t* node_of;             // [capacity] slot -> node, -1 for padding
@@ -132,7 +135,10 @@ inline Gate open_gate() { return Gate{nullptr, 0, -1.0, nullptr, nullptr}; }
 // do nothing once rho_it <= target * rho_0; a negative target never skips
 void launch_vcg_init(const VSys& v, int slots, bool jacobi, cudaStream_t s);
 void launch_vcg_spmv(const VSys& v, int slots, int it, double target, bool withGamma, cudaStream_t s);
-void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s);
+// smoothY (multigrid preconditioner): also the V-cycle's first step,
+// smoothY = kAmgSmooth r / d, so that the cycle that follows skips it
+void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jacobi, cudaStream_t s,
+                       float* smoothY = nullptr);
 // the counter, target and cap of iterations replayed from a CUDA graph:
 // set to 0, rel2 and maxIter before the first replay, stepped by 1 at the
 // end of each
@@ -187,7 +193,9 @@ int amg_tune_lanes(AmgDev& g, const VSys& v, int slots, cudaStream_t s, float* a
 // the level-0 smoothing pass t = b - A y alone (timing hook)
 void launch_amg_fine_residual(const VSys& v, int slots, const AmgDev& g, cudaStream_t s);
 // u = M^-1 r, one V(1,1)-cycle, for CG iteration `it`
-void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s);
+// y0Ready: g.y0 already holds kAmgSmooth r / d (written by the CG update)
+void launch_amg_vcycle(const VSys& v, int slots, const AmgDev& g, int it, double target, cudaStream_t s,
+                       bool y0Ready = false);
 // phi64 += x on the V rows; with record, hist += x as well
 void launch_vcg_apply(const DevMesh& m, const VSys& v, int slots, bool record, cudaStream_t s);
 // warm start: hist *= alpha, phi64 += hist on the V rows
