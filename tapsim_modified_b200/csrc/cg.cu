@@ -149,14 +149,16 @@ __global__ void k_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, 
 }
 __global__ void k_vcg_replay_step(int32_t* iter) { *iter += 1; }
 
-// The condition of the device-side loop around the replayed iteration: go
-// on while fewer than the cap (rel2Dev[1]) have run and rho_k > rel2 rho_0;
-// a NaN stops it.  *done gets the iterations the solve took (0 when rho_0
-// is 0, as the host loop counts them).  The counter steps once per body, so
-// the loop ends after the cap at the latest.
-__global__ void k_vcg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal,
+// The end of a pass of the device-side loop around the replayed iteration:
+// the counter steps (the loop's counterpart of k_vcg_replay_step), then the
+// loop goes on while fewer than the cap (rel2Dev[1]) have run and rho_k >
+// rel2 rho_0; a NaN stops it.  *done gets the iterations the solve took (0
+// when rho_0 is 0, as the host loop counts them).  The counter steps once per
+// pass, so the loop ends after the cap at the latest.
+__global__ void k_vcg_loop_cond(cudaGraphConditionalHandle loop, int32_t* iter, const double* scal,
                                 const double* rel2Dev, int32_t* done) {
-    const int k = *iter;
+    const int k = *iter + 1;
+    *iter = k;
     const double rho0 = scal[3];
     const bool more = k < (int)rel2Dev[1] && rho0 > 0.0 && scal[4 * k + 3] > rel2Dev[0] * rho0;
     *done = rho0 > 0.0 ? k : 0;
@@ -581,7 +583,7 @@ void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, int ma
     count_launch();
     k_vcg_replay_begin<<<1, 1, 0, s>>>(iter, rel2Dev, rel2, maxIter);
 }
-void launch_vcg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal,
+void launch_vcg_loop_cond(cudaGraphConditionalHandle loop, int32_t* iter, const double* scal,
                           const double* rel2Dev, int32_t* done, cudaStream_t s) {
     count_launch();
     k_vcg_loop_cond<<<1, 1, 0, s>>>(loop, iter, scal, rel2Dev, done);

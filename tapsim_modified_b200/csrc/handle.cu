@@ -1239,10 +1239,10 @@ static int iteration_graph(tg_handle* h, const VSys& vg) {
 }
 
 // Launch mode 2: the replayed iteration inside a while-conditional graph
-// node.  The loop's body is the iteration (update, V-cycle, SpMV, counter
-// step) and k_vcg_loop_cond, which sets the node's condition from the
-// device counter and rho; the counter steps once per body, so the loop ends
-// by the iteration cap.  Captured anew with the iteration graph's key.
+// node.  The loop's body is the iteration (update, V-cycle, SpMV) and
+// k_vcg_loop_cond, which steps the device counter and sets the node's
+// condition from it and rho; the counter steps once per body, so the loop
+// ends by the iteration cap.  Captured anew with the iteration graph's key.
 static int iteration_loop_graph(tg_handle* h, const VSys& vg) {
     std::vector<uint64_t> key = iteration_key(vg, h->amg, h->vActive);
     key.push_back((uint64_t)(uintptr_t)h->loopDone.p);
@@ -1277,8 +1277,7 @@ static int iteration_loop_graph(tg_handle* h, const VSys& vg) {
             launch_vcg_update(vg, slots, 0, -1.0, false, cs, h->amg.y0);
             launch_amg_vcycle(vg, slots, h->amg, 1, -1.0, cs, true);
             launch_vcg_spmv(vg, slots, 1, -1.0, true, cs);
-            launch_vcg_replay_step(h->iterDev.p, cs);
-            launch_vcg_loop_cond(loop, h->iterDev.p, vg.scal, h->rel2Dev.p, h->loopDone.p, cs);
+            launch_vcg_loop_cond(loop, h->iterDev.p, vg.scal, h->rel2Dev.p, h->loopDone.p, cs);  // steps the counter
             cudaGraph_t captured = nullptr;
             e = cudaStreamEndCapture(cs, &captured);
         }

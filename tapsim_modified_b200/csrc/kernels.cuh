@@ -144,8 +144,9 @@ void launch_vcg_update(const VSys& v, int slots, int it, double target, bool jac
 // end of each
 void launch_vcg_replay_begin(int32_t* iter, double* rel2Dev, double rel2, int maxIter, cudaStream_t s);
 // the condition kernel of the device-side loop around the replayed
-// iteration (the last node of the loop's body); *done: the iterations run
-void launch_vcg_loop_cond(cudaGraphConditionalHandle loop, const int32_t* iter, const double* scal,
+// iteration (the last node of the loop's body): steps *iter, then sets the
+// loop's condition; *done: the iterations run
+void launch_vcg_loop_cond(cudaGraphConditionalHandle loop, int32_t* iter, const double* scal,
                           const double* rel2Dev, int32_t* done, cudaStream_t s);
 void launch_vcg_replay_step(int32_t* iter, cudaStream_t s);
 // FP64 inner iterations with the multigrid preconditioner: the V-cycle runs
