@@ -566,6 +566,10 @@ int32_t tg_mesh_type_id(const tg_mesh* m, const char* name);
 /* Fills a description whose pointers stay valid while the mesh lives. */
 int tg_mesh_describe(const tg_mesh* m, tg_mesh_desc* desc, int32_t* nnz);
 int tg_mesh_write_node_file(const tg_mesh* m, const char* path, int32_t binary);
+/* File_Io::writeGeomGrid (file_io.cpp:765-820) with numbers and potentials:
+ * the node file a relaxation leaves (tapsim.cpp:129-139), the potentials
+ * given (NULL: the mesh's own) as floats. */
+int tg_mesh_write_grid_nodes(const tg_mesh* m, const char* path, int32_t binary, const float* phi);
 int tg_mesh_write_config(const tg_mesh* m, const char* path);
 /* Writes a TAPSIM dump (File_Io::writeSystem layout) of the mesh with the
  * given potentials (NULL: the mesh's own). */

@@ -462,6 +462,20 @@ int tg_mesh_write_node_file(const tg_mesh* m, const char* path, int32_t binary) 
     return err.empty() ? TG_OK : mesh_fail(err);
 }
 
+int tg_mesh_write_grid_nodes(const tg_mesh* m, const char* path, int32_t binary, const float* phi) {
+    if (!m || !path) return mesh_fail("tg_mesh_write_grid_nodes: null argument");
+    const size_t n = m->type.size();
+    NodeFile nf;
+    nf.xyz = m->xyz;
+    nf.id.assign(m->type.begin(), m->type.end());
+    nf.number.resize(n);
+    for (size_t i = 0; i < n; i++) nf.number[i] = m->number.size() == n ? m->number[i] : (uint32_t)(i + 1);
+    const float* p = phi ? phi : m->phi.data();
+    nf.phi.assign(p, p + n);
+    const std::string err = write_node_file(path, nf, binary != 0);
+    return err.empty() ? TG_OK : mesh_fail(err);
+}
+
 int tg_mesh_write_config(const tg_mesh* m, const char* path) {
     if (!m || !path) return mesh_fail("tg_mesh_write_config: null argument");
     const std::string err = write_config_ascii(path, m->config);

@@ -5,7 +5,12 @@
 // the voltage queue and time scale (process.cpp:985-1036) in float, as the
 // reference does, and writes the results file with LogResults' layout.
 //
-// Command line, as the reference's (commands.cpp:280-577, 590-841):
+// Command line, as the reference's (commands.cpp:55-841):
+//   tapsim_b200 make-ini [filename]
+//   tapsim_b200 [options] relaxation iconfig inode [onode]
+//   tapsim_b200 [options] relaxation --read-dump=? oconfig onode
+//     (--write-dump=?, --threshold=?, --cycle-size=?, --queue-size=?,
+//     --init-potentials / --reset-potentials)
 //   tapsim_b200 [options] evaporation iconfig inode [results]
 //   tapsim_b200 [options] evaporation --input-dump=? iconfig [results]
 //   tapsim_b200 [options] resumption idump [results]
@@ -21,6 +26,7 @@
 // relaxed to --rel-tol, 1e-8; reference: the ini's local/global/refresh
 // sweeps), --warm-start=0|1, --batch=? (events per library call),
 // --records=? (every event's record as the library returned it, raw).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -37,20 +43,33 @@
 
 namespace {
 
-// Process::EvaporationOptions keys with the defaults of makeIniList
-// (commands.cpp:1249-1325); the keys this program reads
-const std::map<std::string, std::string> kIniDefaults = {
-    {"RESULTS_FILENAME", "results_data"}, {"RESULTS_BINARY_OUTPUT", "0"}, {"RESULTS_CHUNK_SIZE", "10000"},
-    {"METHOD_EVAPORATION_PROBABILITY", "0"}, {"METHOD_EVAPORATION_CHOICE", "0"},
-    {"VACUUM_CELL_IDENTIFIER", "Vacuum"}, {"TRAJECTORY_INTEGRATOR_TYPE", "1"}, {"TRAJECTORY_STEPPER_TYPE", "1"},
-    {"TRAJECTORY_INITIAL_TIME_STEP", "1e-14"}, {"TRAJECTORY_MINIMUM_TIME_STEP", "1e-16"},
-    {"TRAJECTORY_ERROR_THRESHOLD", "1e-6"}, {"TRAJECTORY_NO_INITIAL_VELOCITY", "1"},
-    {"VOLTAGE_QUEUE_SIZE", "250"}, {"LOCAL_RELAXATION_ERROR_THRESHOLD", "1e-2"},
-    {"LOCAL_RELAXATION_SHELL_SIZE", "3"}, {"LOCAL_RELAXATION_CYCLE_SIZE", "5"}, {"LOCAL_RELAXATION_QUEUE_SIZE", "5"},
-    {"GLOBAL_RELAXATION_STEPS", "1"}, {"REFRESH_RELAXATION_INTERVAL", "0"},
-    {"REFRESH_RELAXATION_ERROR_THRESHOLD", "0.0"}, {"REFRESH_RELAXATION_CYCLE_SIZE", "100"},
-    {"REFRESH_RELAXATION_QUEUE_SIZE", "25"},
+// The initialization file's keys and defaults in makeIniList's order
+// (commands.cpp:1249-1325), an empty key for each blank line; make-ini
+// writes them out, and every key a run reads defaults to them.
+const std::vector<std::pair<const char*, const char*>> kIniList = {
+    {"RESULTS_FILENAME", "results_data"}, {"RESULTS_BINARY_OUTPUT", "0"}, {"RESULTS_CHUNK_SIZE", "10000"}, {"", ""},
+    {"TRAJECTORY_FILENAME", "trajectory_data"}, {"TRAJECTORY_BINARY_OUTPUT", "1"}, {"TRAJECTORY_CHUNK_SIZE", "10000"},
+    {"", ""},
+    {"GRID_FILENAME", "grid_data"}, {"GRID_BINARY_OUTPUT", "1"}, {"GRID_INTERVAL", "2147483647"}, {"", ""},
+    {"SURFACE_FILENAME", "surface_data"}, {"SURFACE_BINARY_OUTPUT", "1"}, {"SURFACE_INTERVAL", "2147483647"}, {"", ""},
+    {"GEOMETRY_FILENAME", "geometry.dat"}, {"GEOMETRY_BINARY_OUTPUT", "1"}, {"GEOMETRY_CONTENTS", "0xff"}, {"", ""},
+    {"DUMP_FILENAME", "dump"}, {"DUMP_INTERVAL", "10000"}, {"", ""},
+    {"OUTPUT_DELAY_TIME", "60"}, {"", ""},
+    {"METHOD_EVAPORATION_PROBABILITY", "0"}, {"METHOD_EVAPORATION_CHOICE", "0"}, {"", ""},
+    {"VACUUM_CELL_IDENTIFIER", "Vacuum"}, {"", ""},
+    {"TRAJECTORY_INTEGRATOR_TYPE", "1"}, {"TRAJECTORY_STEPPER_TYPE", "1"}, {"TRAJECTORY_INITIAL_TIME_STEP", "1e-14"},
+    {"TRAJECTORY_MINIMUM_TIME_STEP", "1e-16"}, {"TRAJECTORY_ERROR_THRESHOLD", "1e-6"},
+    {"TRAJECTORY_NON_RANDOM_START_POSITION", "1"}, {"TRAJECTORY_NO_INITIAL_VELOCITY", "1"}, {"", ""},
+    {"VOLTAGE_QUEUE_SIZE", "250"}, {"", ""},
+    {"LOCAL_RELAXATION_ERROR_THRESHOLD", "1e-2"}, {"LOCAL_RELAXATION_SHELL_SIZE", "3"},
+    {"LOCAL_RELAXATION_CYCLE_SIZE", "5"}, {"LOCAL_RELAXATION_QUEUE_SIZE", "5"}, {"GLOBAL_RELAXATION_STEPS", "1"},
+    {"", ""},
+    {"REFRESH_RELAXATION_INTERVAL", "0"}, {"REFRESH_RELAXATION_ERROR_THRESHOLD", "0.0"},
+    {"REFRESH_RELAXATION_CYCLE_SIZE", "100"}, {"REFRESH_RELAXATION_QUEUE_SIZE", "25"}, {"", ""},
 };
+// the default initialization file (tapsim.cpp:64), read when present and
+// no --ini-file is given (commands.cpp:1038-1044)
+const char* kDefaultIni = "tapsim.ini";
 
 struct Args {
     std::string command, config, nodes, dump, results, ini;
@@ -68,6 +87,12 @@ struct Args {
     int batch = 64;
     std::string records;      // --records: every event's tg_event_record, raw, in order
     std::string sample, configTemplate;  // meshgen
+    std::string iniOut;                  // make-ini
+    // relaxation (RelaxationCommands, commands.cpp:861-894)
+    std::string readDump, writeDump, oconfig, onodes;
+    float threshold = 0.0f;
+    int cycleSize = 100, relaxQueue = 25;
+    bool resetPotentials = false;
     double boxHalfWidth = -1.0, boxHeight = -1.0, fineShell = -1.0;
 };
 
@@ -116,10 +141,16 @@ Args parse(int argc, char** argv) {
         else if (opt(s, "box-half-width", &v)) a.boxHalfWidth = std::atof(v.c_str());
         else if (opt(s, "box-height", &v)) a.boxHeight = std::atof(v.c_str());
         else if (opt(s, "fine-shell", &v)) a.fineShell = std::atof(v.c_str());
+        else if (opt(s, "read-dump", &v)) a.readDump = v;
+        else if (opt(s, "write-dump", &v)) a.writeDump = v;
+        else if (opt(s, "threshold", &v)) a.threshold = (float)std::atof(v.c_str());
+        else if (opt(s, "cycle-size", &v)) a.cycleSize = std::atoi(v.c_str());
+        else if (opt(s, "queue-size", &v)) a.relaxQueue = std::atoi(v.c_str());
+        else if (s == "--init-potentials" || s == "--reset-potentials") a.resetPotentials = true;
         else if (s.compare(0, 2, "--") == 0) die("unknown or invalid argument in command line: \"" + s + "\"");
         else pos.push_back(s);
     }
-    if (pos.empty()) die("usage: tapsim_b200 [options] evaporation|resumption|meshgen ...");
+    if (pos.empty()) die("usage: tapsim_b200 [options] make-ini|relaxation|evaporation|resumption|meshgen ...");
     a.command = pos[0];
     if (a.command == "evaporation") {
         if (!a.dump.empty()) {
@@ -136,6 +167,24 @@ Args parse(int argc, char** argv) {
         if (pos.size() < 2) die("missing arguments for processing in 'resumption'-mode");
         a.dump = pos[1];
         if (pos.size() > 2) a.results = pos[2];
+    } else if (a.command == "make-ini") {
+        // make-ini [filename] (commands.cpp:55-140)
+        if (pos.size() > 2) die("missing arguments for processing in 'make-ini'-mode");
+        a.iniOut = pos.size() > 1 ? pos[1] : kDefaultIni;
+    } else if (a.command == "relaxation") {
+        // relaxation iconfig inode [onode] | --read-dump=? oconfig onode
+        // (commands.cpp:142-277; iconfig inode alone writes the relaxed
+        // nodes over inode, as the reference does)
+        if (!a.readDump.empty()) {
+            if (pos.size() != 3) die("missing arguments for processing in 'relaxation'-mode");
+            a.oconfig = pos[1];
+            a.onodes = pos[2];
+        } else {
+            if (pos.size() != 3 && pos.size() != 4) die("missing arguments for processing in 'relaxation'-mode");
+            a.config = pos[1];
+            a.nodes = pos[2];
+            a.onodes = pos.size() == 4 ? pos[3] : pos[2];
+        }
     } else if (a.command == "meshgen") {
         if (pos.size() < 3) die("missing arguments for 'meshgen': isample onodes");
         a.sample = pos[1];
@@ -147,7 +196,9 @@ Args parse(int argc, char** argv) {
 }
 
 std::map<std::string, std::string> read_ini(const std::string& path) {
-    std::map<std::string, std::string> ini = kIniDefaults;
+    std::map<std::string, std::string> ini;
+    for (const auto& kv : kIniList)
+        if (kv.first[0]) ini[kv.first] = kv.second;
     if (path.empty()) return ini;
     std::ifstream f(path);
     if (!f) die("cannot read ini file " + path);
@@ -193,9 +244,107 @@ int meshgen(const Args& a) {
     return 0;
 }
 
+// make-ini (doMakeIni, tapsim.cpp:66-85): the default initialization file,
+// as File_Io::writeInitialization lays it out (file_io.cpp:96-112)
+int make_ini(const Args& a) {
+    std::ofstream f(a.iniOut, std::ios::trunc);
+    if (!f) die("cannot write " + a.iniOut);
+    for (const auto& kv : kIniList) {
+        if (kv.first[0]) f << kv.first << " = " << kv.second;
+        f << '\n';
+    }
+    if (!f) die("cannot write " + a.iniOut);
+    std::printf("make-ini: default initialization file \"%s\"\n", a.iniOut.c_str());
+    return 0;
+}
+
+// relaxation (doRelaxation, tapsim.cpp:87-148): the system from a dump or a
+// configuration and node file, its potentials reset at random on request,
+// relaxed, then the configuration (with --read-dump), the node file with
+// numbers and potentials, and a dump (--write-dump) written.  --relax-mode
+// as for evaporation: solve (default) relaxes to --rel-tol; reference runs
+// Grid_3d::Table::relax(threshold, cycle, queue) (Process::relaxation,
+// process.cpp:133-157), whose stagnation fault ends it without an error.
+int relaxation(const Args& a) {
+    tg_mesh* mesh = nullptr;
+    if (!a.readDump.empty()) check(tg_mesh_from_dump(a.readDump.c_str(), nullptr, &mesh), nullptr, "reading the dump");
+    else check(tg_mesh_from_files(a.nodes.c_str(), a.config.c_str(), a.threads, &mesh), nullptr, "reading the mesh");
+    tg_mesh_desc desc;
+    int32_t nnz = 0;
+    check(tg_mesh_describe(mesh, &desc, &nnz), nullptr, "tg_mesh_describe");
+    const int n = desc.num_nodes;
+    tg_handle* h = nullptr;
+    check(tg_create(&desc, &h), nullptr, "tg_create");
+    if (a.resetPotentials) {
+        // Grid_3d::Table::randomReset (grid_3d.cpp:811-848): free cells
+        // uniform in [min, max] of the types' potentials, in float, from
+        // the stream main() seeds with srand(99) (tapsim.cpp:235)
+        std::map<int, const tg_type*> types;
+        for (int k = 0; k < desc.num_types; k++) types[desc.types[k].id] = &desc.types[k];
+        if (types.empty()) die("relaxation: the configuration has no cell types");
+        float minPhi = types.begin()->second->phi, maxPhi = minPhi;
+        for (const auto& kv : types) {
+            minPhi = std::min(minPhi, kv.second->phi);
+            maxPhi = std::max(maxPhi, kv.second->phi);
+        }
+        std::srand(99);
+        std::vector<double> phi(n);
+        for (int i = 0; i < n; i++) {
+            const auto t = types.find(desc.type_id[i]);
+            if (t == types.end()) die("relaxation: a node of an unknown cell type");
+            float p;
+            if (t->second->dirichlet) {
+                p = t->second->phi;
+            } else {
+                p = (float)std::rand();
+                p /= (float)RAND_MAX;
+                p *= maxPhi - minPhi;
+                p += minPhi;
+            }
+            phi[i] = p;
+        }
+        check(tg_set_phi(h, phi.data()), h, "tg_set_phi");
+        std::printf("relaxation: potential values are reset\n");
+    }
+    if (a.relaxReference) {
+        int64_t it = 0;
+        double dev = 0.0;
+        const int rc = tg_relax_threshold(h, a.threshold, a.cycleSize, a.relaxQueue, 2000000, &it, &dev);
+        if (rc == TG_ERR_RELAX_FAULT || rc == TG_ERR_ITERATION_CAP)
+            std::printf("relaxation: numerical limit reached after %lld steps (deviation = %g)\n", (long long)it, dev);
+        else check(rc, h, "relaxation");
+        if (rc == TG_OK) std::printf("relaxation: %lld steps, deviation %g\n", (long long)it, dev);
+    } else {
+        tg_solve_opts so{};
+        so.rel_tol = a.relTol;
+        so.max_outer = 50;
+        so.max_inner = 20000;
+        so.inner_rtol = 1e-4;
+        so.warm_start = 0;
+        so.preconditioner = 1;
+        tg_solve_info info;
+        check(tg_solve(h, &so, &info), h, "relaxation");
+        std::printf("relaxation: relative residual %.3e after %d outer steps\n", info.rel_residual, info.outer);
+    }
+    std::vector<double> phi64(n);
+    check(tg_get_phi(h, phi64.data()), h, "tg_get_phi");
+    std::vector<float> phi(n);
+    for (int i = 0; i < n; i++) phi[i] = (float)phi64[i];
+    if (!a.oconfig.empty()) check(tg_mesh_write_config(mesh, a.oconfig.c_str()), nullptr, "writing the configuration");
+    if (!a.onodes.empty())
+        check(tg_mesh_write_grid_nodes(mesh, a.onodes.c_str(), 0, phi.data()), nullptr, "writing the node file");
+    if (!a.writeDump.empty()) check(tg_mesh_write_dump(mesh, a.writeDump.c_str(), phi.data()), nullptr, "writing the dump");
+    tg_destroy(h);
+    tg_mesh_destroy(mesh);
+    return 0;
+}
+
 int main(int argc, char** argv) {
-    const Args a = parse(argc, argv);
+    Args a = parse(argc, argv);
     if (a.command == "meshgen") return meshgen(a);
+    if (a.command == "make-ini") return make_ini(a);
+    if (a.command == "relaxation") return relaxation(a);
+    if (a.ini.empty() && std::ifstream(kDefaultIni).good()) a.ini = kDefaultIni;
     const std::map<std::string, std::string> ini = read_ini(a.ini);
     auto I = [&](const char* k) { return std::atoi(ini.at(k).c_str()); };
     auto F = [&](const char* k) { return std::atof(ini.at(k).c_str()); };

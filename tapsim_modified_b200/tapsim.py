@@ -148,6 +148,13 @@ class Mesh:
     def write_node_file(self, path: str, binary: bool = True):
         N.check(N.lib().tg_mesh_write_node_file(self._h, str(path).encode(), int(binary)))
 
+    def write_grid_nodes(self, path: str, phi: np.ndarray | None = None, binary: bool = False):
+        """File_Io::writeGeomGrid (file_io.cpp:765-820): the node file with
+        numbers and potentials (phi: float potentials, None: the mesh's own),
+        as a relaxation writes it (ASCII by default, tapsim.cpp:129-139)."""
+        p = None if phi is None else np.ascontiguousarray(phi, np.float32)
+        N.check(N.lib().tg_mesh_write_grid_nodes(self._h, str(path).encode(), int(binary), N.ptr(p)))
+
     def write_config(self, path: str):
         N.check(N.lib().tg_mesh_write_config(self._h, str(path).encode()))
 

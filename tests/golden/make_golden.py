@@ -47,6 +47,13 @@ ini instead (localRelax of the 3-hop shell to 1e-2 V plus one global sweep
 per event, no refresh; process.cpp:851-893) after the same initial
 relaxation: ref_events_default.txt.
 
+With `--commands` it runs two more of the reference's own `tapsim` modes
+(tapsim.cpp:66-148): `make-ini` (the default initialization file,
+ref_tapsim.ini) and `relaxation tip.cfg tip.nodes` with its defaults
+(threshold 0, cycles of 100, a queue of 25), keeping the relaxed node file
+it writes (ASCII, numbers and potentials; file_io.cpp:765-820), gzipped:
+ref_relaxed_nodes.txt.gz.
+
 With `--snapshots` it repeats the first event with Fe's DIELECTRICITY set
 to 5 (tip_eps5.cfg; --no-sync keeps the dump's couplings, so only the
 dielectric force changes) and keeps the snapshots that the reference's own
@@ -227,8 +234,26 @@ def default_ini():
     shutil.rmtree(tmp)
 
 
+def commands():
+    """The reference's make-ini and relaxation modes (see the docstring)."""
+    tapsim = ROOT / "oracle" / "_ref" / "tapsim"
+    if not tapsim.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    tmp = HERE / "_tmp"
+    tmp.mkdir(exist_ok=True)
+    subprocess.run([str(tapsim), "make-ini", str(HERE / "ref_tapsim.ini")], check=True, capture_output=True, cwd=tmp)
+    subprocess.run([str(tapsim), "relaxation", str(HERE / "tip.cfg"), str(HERE / "tip.nodes"), str(tmp / "relaxed.nodes")],
+                   check=True, capture_output=True, cwd=tmp)
+    with open(tmp / "relaxed.nodes", "rb") as f, gzip.open(HERE / "ref_relaxed_nodes.txt.gz", "wb", compresslevel=9) as g:
+        shutil.copyfileobj(f, g)
+    print("commands ->", "ref_tapsim.ini", "ref_relaxed_nodes.txt.gz")
+    shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
-    if "--default-ini" in sys.argv:
+    if "--commands" in sys.argv:
+        commands()
+    elif "--default-ini" in sys.argv:
         default_ini()
     elif "--modes" in sys.argv:
         modes()
