@@ -574,6 +574,11 @@ int tg_mesh_write_config(const tg_mesh* m, const char* path);
 /* Writes a TAPSIM dump (File_Io::writeSystem layout) of the mesh with the
  * given potentials (NULL: the mesh's own). */
 int tg_mesh_write_dump(const tg_mesh* m, const char* path, const float* phi);
+/* The event index a dump holds (LAST_INDEX, File_Io::readSystem's index,
+ * file_io.cpp:1027-1062) for a mesh read from one, else 0; a resumption
+ * numbers its events on from it (tapsim.cpp:206-225), and
+ * tg_mesh_write_dump writes it back. */
+uint32_t tg_mesh_dump_index(const tg_mesh* m);
 /* Grid_3d::Node::number of every node: the unique numbers of the node file
  * or dump (File_Io::readGeomGrid numbering, file_io.cpp:975-1000), index + 1
  * for a generated tip.  numbers_out: [N]. */

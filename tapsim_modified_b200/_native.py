@@ -210,6 +210,7 @@ SIGNATURES = {
     "tg_mesh_describe": (C.c_int, [_P, C.POINTER(tg_mesh_desc), C.POINTER(_I)]),
     "tg_mesh_write_node_file": (C.c_int, [_P, C.c_char_p, _I]),
     "tg_mesh_write_grid_nodes": (C.c_int, [_P, C.c_char_p, _I, _P]),
+    "tg_mesh_dump_index": (C.c_uint32, [_P]),
     "tg_mesh_write_config": (C.c_int, [_P, C.c_char_p]),
     "tg_mesh_write_dump": (C.c_int, [_P, C.c_char_p, _P]),
 }

@@ -31,6 +31,7 @@ struct tg_mesh {
     ConfigTable config;
     std::vector<tg_type> types;
     bool has_geom = false;
+    uint32_t dump_index = 0;  // LAST_INDEX of the dump the mesh was read from
 };
 
 namespace tgapi {
@@ -383,6 +384,7 @@ int tg_mesh_from_dump(const char* dumpFile, const char* configFile, tg_mesh** ou
     m->number.swap(d.number);
     // Grid_3d::Table::potential(i) reads phi[(phiSwitch + 1) % 2] (grid_3d.h:184)
     m->phi = ((d.phi_switch + 1) % 2) ? d.phi1 : d.phi0;
+    m->dump_index = d.last_index;
     m->row_ptr.swap(d.row_ptr);
     m->col.swap(d.col);
     m->coupling.assign(d.coupling.begin(), d.coupling.end());
@@ -482,6 +484,8 @@ int tg_mesh_write_config(const tg_mesh* m, const char* path) {
     return err.empty() ? TG_OK : mesh_fail(err);
 }
 
+uint32_t tg_mesh_dump_index(const tg_mesh* m) { return m ? m->dump_index : 0u; }
+
 int tg_mesh_numbers(const tg_mesh* m, uint32_t* out) {
     if (!m || !out) return mesh_fail("tg_mesh_numbers: null argument");
     const size_t n = m->type.size();
@@ -564,6 +568,7 @@ int tg_surface_log_write(const char* path, int32_t binary, int32_t nCells, const
 int tg_mesh_write_dump(const tg_mesh* m, const char* path, const float* phi) {
     if (!m || !path) return mesh_fail("tg_mesh_write_dump: null argument");
     Dump d;
+    d.last_index = m->dump_index;  // File_Io::writeSystem with the index read (tapsim.cpp:141-145)
     d.config = m->config;
     const int n = (int)m->type.size();
     for (int k = 0; k < 3; k++) {

@@ -20,8 +20,17 @@
 //     configuration template, --box-half-width=?, --box-height=?,
 //     --fine-shell=? [m] size the box, --write-ascii the node file)
 // Options taken from the reference: --ini-file=?, --threads=?, --write-ascii,
-// --write-binary, --no-file-output, --skip-relaxation, --event-limit=?,
-// --voltage-queue-size=?, --vacuum-identifier=?, --no-chunks, --chunk-size=?.
+// --write-binary, --no-file-output, --skip-relaxation, --init-potentials,
+// --reset-potentials, --threshold=?, --cycle-size=?, --queue-size=? (the
+// initial relaxation), --event-limit=?, --last-event=?, --shrink-limit=?,
+// --voltage-queue-size=? (--voltage-queue-limit=?), --vacuum-identifier=?,
+// --no-chunks, --chunk-size=?, --trajectory-error-threshold=?,
+// --evap-threshold=?, --evap-shell-size=?, --evap-cycle-size=?,
+// --evap-queue-size=?, --evap-global-cycles=?, --refresh-interval=?,
+// --refresh-threshold=?, --refresh-cycle-size=?, --refresh-queue-size=?;
+// --no-trajectories, --no-grids, --no-surfaces and --no-dump are accepted
+// (this program writes the results file only), and the options that ask
+// for those files are refused.
 // Options of this build: --relax-mode=solve|reference (solve: every event
 // relaxed to --rel-tol, 1e-8; reference: the ini's local/global/refresh
 // sweeps), --warm-start=0|1, --batch=? (events per library call),
@@ -90,9 +99,15 @@ struct Args {
     std::string iniOut;                  // make-ini
     // relaxation (RelaxationCommands, commands.cpp:861-894)
     std::string readDump, writeDump, oconfig, onodes;
-    float threshold = 0.0f;
-    int cycleSize = 100, relaxQueue = 25;
+    // the initial relaxation of evaporation (Grid_3d::Table::relax), -1: the
+    // ini's refresh parameters (commands.cpp:929-933); relaxation's own
+    // defaults are 0, 100 and 25 (commands.cpp:876-894)
+    float threshold = -1.0f;
+    int cycleSize = -1, relaxQueue = -1;
     bool resetPotentials = false;
+    std::map<std::string, std::string> iniOverrides;  // command-line values of ini keys
+    long lastEvent = -1;       // resumption: the index before the first event (-1: the dump's)
+    float shrinkLimit = -1.0f; // stop once the apex sank this far [m] (-1: never)
     double boxHalfWidth = -1.0, boxHeight = -1.0, fineShell = -1.0;
 };
 
@@ -125,7 +140,7 @@ Args parse(int argc, char** argv) {
         else if (s == "--no-file-output") a.fileOutput = false;
         else if (s == "--skip-relaxation") a.skipRelaxation = true;
         else if (opt(s, "event-limit", &v)) a.eventLimit = std::atol(v.c_str());
-        else if (opt(s, "voltage-queue-size", &v)) a.queueSize = std::atoi(v.c_str());
+        else if (opt(s, "voltage-queue-size", &v) || opt(s, "voltage-queue-limit", &v)) a.queueSize = std::atoi(v.c_str());
         else if (opt(s, "vacuum-identifier", &v)) a.vacuum = v;
         else if (s == "--no-chunks") a.chunkSize = 0;
         else if (opt(s, "chunk-size", &v)) a.chunkSize = std::atoi(v.c_str());
@@ -147,6 +162,30 @@ Args parse(int argc, char** argv) {
         else if (opt(s, "cycle-size", &v)) a.cycleSize = std::atoi(v.c_str());
         else if (opt(s, "queue-size", &v)) a.relaxQueue = std::atoi(v.c_str());
         else if (s == "--init-potentials" || s == "--reset-potentials") a.resetPotentials = true;
+        // evaporation and resumption (commands.cpp:280-841): ini values
+        else if (opt(s, "evap-threshold", &v)) a.iniOverrides["LOCAL_RELAXATION_ERROR_THRESHOLD"] = v;
+        else if (opt(s, "evap-shell-size", &v)) a.iniOverrides["LOCAL_RELAXATION_SHELL_SIZE"] = v;
+        else if (opt(s, "evap-cycle-size", &v)) a.iniOverrides["LOCAL_RELAXATION_CYCLE_SIZE"] = v;
+        else if (opt(s, "evap-queue-size", &v)) {
+            // the reference's handler falls through into --evap-global-cycles
+            // (commands.cpp:511-516), so the value sets both
+            a.iniOverrides["LOCAL_RELAXATION_QUEUE_SIZE"] = v;
+            a.iniOverrides["GLOBAL_RELAXATION_STEPS"] = v;
+        } else if (opt(s, "evap-global-cycles", &v)) a.iniOverrides["GLOBAL_RELAXATION_STEPS"] = v;
+        else if (opt(s, "refresh-interval", &v)) a.iniOverrides["REFRESH_RELAXATION_INTERVAL"] = v;
+        else if (opt(s, "refresh-threshold", &v)) a.iniOverrides["REFRESH_RELAXATION_ERROR_THRESHOLD"] = v;
+        else if (opt(s, "refresh-cycle-size", &v)) a.iniOverrides["REFRESH_RELAXATION_CYCLE_SIZE"] = v;
+        else if (opt(s, "refresh-queue-size", &v)) a.iniOverrides["REFRESH_RELAXATION_QUEUE_SIZE"] = v;
+        else if (opt(s, "trajectory-error-threshold", &v)) a.iniOverrides["TRAJECTORY_ERROR_THRESHOLD"] = v;
+        else if (opt(s, "shrink-limit", &v)) a.shrinkLimit = (float)std::atof(v.c_str());
+        else if (opt(s, "last-event", &v)) a.lastEvent = std::atol(v.c_str());
+        // outputs this program does not write: asking for none is accepted
+        else if (s == "--no-trajectories" || s == "--no-grids" || s == "--no-surfaces" || s == "--no-dump") {
+        } else if (opt(s, "write-trajectories", &v) || opt(s, "write-grids", &v) || opt(s, "write-surfaces", &v) ||
+                   opt(s, "snapshot-interval", &v) || opt(s, "dump-interval", &v)) {
+            die("\"" + s + "\": tapsim_b200 writes the results file only (the Python host's Evaporation writes "
+                "trajectories and grid and surface snapshots)");
+        }
         else if (s.compare(0, 2, "--") == 0) die("unknown or invalid argument in command line: \"" + s + "\"");
         else pos.push_back(s);
     }
@@ -258,6 +297,39 @@ int make_ini(const Args& a) {
     return 0;
 }
 
+// Grid_3d::Table::randomReset (grid_3d.cpp:811-848): free cells uniform in
+// [min, max] of the types' potentials, in float, from the stream main()
+// seeds with srand(99) (tapsim.cpp:235); Dirichlet cells at their type's
+void random_reset(tg_handle* h, const tg_mesh_desc& desc) {
+    const int n = desc.num_nodes;
+    std::map<int, const tg_type*> types;
+    for (int k = 0; k < desc.num_types; k++) types[desc.types[k].id] = &desc.types[k];
+    if (types.empty()) die("the configuration has no cell types");
+    float minPhi = types.begin()->second->phi, maxPhi = minPhi;
+    for (const auto& kv : types) {
+        minPhi = std::min(minPhi, kv.second->phi);
+        maxPhi = std::max(maxPhi, kv.second->phi);
+    }
+    std::srand(99);
+    std::vector<double> phi(n);
+    for (int i = 0; i < n; i++) {
+        const auto t = types.find(desc.type_id[i]);
+        if (t == types.end()) die("a node of an unknown cell type");
+        float p;
+        if (t->second->dirichlet) {
+            p = t->second->phi;
+        } else {
+            p = (float)std::rand();
+            p /= (float)RAND_MAX;
+            p *= maxPhi - minPhi;
+            p += minPhi;
+        }
+        phi[i] = p;
+    }
+    check(tg_set_phi(h, phi.data()), h, "tg_set_phi");
+    std::printf("potential values are reset\n");
+}
+
 // relaxation (doRelaxation, tapsim.cpp:87-148): the system from a dump or a
 // configuration and node file, its potentials reset at random on request,
 // relaxed, then the configuration (with --read-dump), the node file with
@@ -275,41 +347,12 @@ int relaxation(const Args& a) {
     const int n = desc.num_nodes;
     tg_handle* h = nullptr;
     check(tg_create(&desc, &h), nullptr, "tg_create");
-    if (a.resetPotentials) {
-        // Grid_3d::Table::randomReset (grid_3d.cpp:811-848): free cells
-        // uniform in [min, max] of the types' potentials, in float, from
-        // the stream main() seeds with srand(99) (tapsim.cpp:235)
-        std::map<int, const tg_type*> types;
-        for (int k = 0; k < desc.num_types; k++) types[desc.types[k].id] = &desc.types[k];
-        if (types.empty()) die("relaxation: the configuration has no cell types");
-        float minPhi = types.begin()->second->phi, maxPhi = minPhi;
-        for (const auto& kv : types) {
-            minPhi = std::min(minPhi, kv.second->phi);
-            maxPhi = std::max(maxPhi, kv.second->phi);
-        }
-        std::srand(99);
-        std::vector<double> phi(n);
-        for (int i = 0; i < n; i++) {
-            const auto t = types.find(desc.type_id[i]);
-            if (t == types.end()) die("relaxation: a node of an unknown cell type");
-            float p;
-            if (t->second->dirichlet) {
-                p = t->second->phi;
-            } else {
-                p = (float)std::rand();
-                p /= (float)RAND_MAX;
-                p *= maxPhi - minPhi;
-                p += minPhi;
-            }
-            phi[i] = p;
-        }
-        check(tg_set_phi(h, phi.data()), h, "tg_set_phi");
-        std::printf("relaxation: potential values are reset\n");
-    }
+    if (a.resetPotentials) random_reset(h, desc);
     if (a.relaxReference) {
         int64_t it = 0;
         double dev = 0.0;
-        const int rc = tg_relax_threshold(h, a.threshold, a.cycleSize, a.relaxQueue, 2000000, &it, &dev);
+        const int rc = tg_relax_threshold(h, a.threshold >= 0.0f ? a.threshold : 0.0f, a.cycleSize >= 0 ? a.cycleSize : 100,
+                                          a.relaxQueue >= 0 ? a.relaxQueue : 25, 2000000, &it, &dev);
         if (rc == TG_ERR_RELAX_FAULT || rc == TG_ERR_ITERATION_CAP)
             std::printf("relaxation: numerical limit reached after %lld steps (deviation = %g)\n", (long long)it, dev);
         else check(rc, h, "relaxation");
@@ -345,7 +388,9 @@ int main(int argc, char** argv) {
     if (a.command == "make-ini") return make_ini(a);
     if (a.command == "relaxation") return relaxation(a);
     if (a.ini.empty() && std::ifstream(kDefaultIni).good()) a.ini = kDefaultIni;
-    const std::map<std::string, std::string> ini = read_ini(a.ini);
+    if (!a.writeDump.empty()) die("--write-dump: tapsim_b200 writes no dumps during an evaporation");
+    std::map<std::string, std::string> ini = read_ini(a.ini);
+    for (const auto& kv : a.iniOverrides) ini[kv.first] = kv.second;
     auto I = [&](const char* k) { return std::atoi(ini.at(k).c_str()); };
     auto F = [&](const char* k) { return std::atof(ini.at(k).c_str()); };
 
@@ -366,8 +411,12 @@ int main(int argc, char** argv) {
     if (vacuumId < 0) die("no cell type named " + vacuumName + " in the configuration");
     std::map<int, tg_type> types;
     for (int k = 0; k < desc.num_types; k++) types[desc.types[k].id] = desc.types[k];
+    // the index before the first event: 0 for an evaporation, the dump's
+    // (or --last-event) for a resumption (tapsim.cpp:206-225)
+    const long initEvent = a.command == "resumption" ? (a.lastEvent >= 0 ? a.lastEvent : (long)tg_mesh_dump_index(mesh)) : 0;
     tg_handle* h = nullptr;
     check(tg_create(&desc, &h), nullptr, "tg_create");
+    if (a.resetPotentials) random_reset(h, desc);
 
     tg_solve_opts solve{};
     solve.rel_tol = a.relTol;
@@ -382,8 +431,10 @@ int main(int argc, char** argv) {
         if (a.relaxReference) {
             int64_t it = 0;
             double dev = 0.0;
-            rc = tg_relax_threshold(h, F("REFRESH_RELAXATION_ERROR_THRESHOLD"), I("REFRESH_RELAXATION_CYCLE_SIZE"),
-                                    I("REFRESH_RELAXATION_QUEUE_SIZE"), 2000000, &it, &dev);
+            rc = tg_relax_threshold(h, a.threshold >= 0.0f ? a.threshold : F("REFRESH_RELAXATION_ERROR_THRESHOLD"),
+                                    a.cycleSize >= 0 ? a.cycleSize : I("REFRESH_RELAXATION_CYCLE_SIZE"),
+                                    a.relaxQueue >= 0 ? a.relaxQueue : I("REFRESH_RELAXATION_QUEUE_SIZE"), 2000000,
+                                    &it, &dev);
             if (rc != TG_OK && rc != TG_ERR_RELAX_FAULT && rc != TG_ERR_ITERATION_CAP) check(rc, h, "relaxation");
         } else {
             tg_solve_opts s0 = solve;
@@ -433,14 +484,17 @@ int main(int argc, char** argv) {
     FILE* rawOut = a.records.empty() ? nullptr : std::fopen(a.records.c_str(), "wb");
     if (!a.records.empty() && !rawOut) die("cannot write " + a.records);
     long events = 0;
+    float initApexZ = 0.0f;
+    bool shrunk = false;
     for (;;) {
         long want = a.batch;
         if (a.eventLimit >= 0) want = std::min<long>(want, a.eventLimit - events);
         if (want <= 0) break;
         int32_t done = 0;
-        rc = tg_run_events(h, &o, (int32_t)(events + 1), (int32_t)want, recs.data(), &done);
+        // the refresh schedule tests (initial index + event index) % interval
+        // (process.cpp:876), the event index counting on from the initial one
+        rc = tg_run_events(h, &o, (int32_t)(initEvent + initEvent + events + 1), (int32_t)want, recs.data(), &done);
         if (rc != TG_OK && rc != TG_ERR_NO_SURFACE) check(rc, h, "tg_run_events");
-        if (rawOut && done > 0) std::fwrite(recs.data(), sizeof(tg_event_record), (size_t)done, rawOut);
         for (int k = 0; k < done; k++) {
             const tg_event_record& r = recs[k];
             const tg_type& t = types.at(r.type_id);
@@ -468,7 +522,7 @@ int main(int argc, char** argv) {
                 timeScale = 1.0f;
             }
             tg_result_row row{};
-            row.index = (uint32_t)(events + k + 1);
+            row.index = (uint32_t)(initEvent + events + k + 1);
             row.id = r.type_id;
             row.number = numbers[r.node];
             row.voltage = voltage;
@@ -485,9 +539,18 @@ int main(int argc, char** argv) {
             row.potential_before = r.phi_before;
             row.potential_after = r.phi_after;
             rows.push_back(row);
+            if (events + k == 0) initApexZ = r.apex[2];
+            // --shrink-limit: the run ends after the event whose apex lies
+            // that far below the first one's (process.cpp:1108)
+            if (a.shrinkLimit >= 0.0f && initApexZ - r.apex[2] >= a.shrinkLimit) {
+                shrunk = true;
+                done = k + 1;
+                break;
+            }
         }
+        if (rawOut && done > 0) std::fwrite(recs.data(), sizeof(tg_event_record), (size_t)done, rawOut);
         events += done;
-        if (done < want) break;  // the surface ran out
+        if (shrunk || done < want) break;  // shrunk, or the surface ran out
     }
     if (rawOut) std::fclose(rawOut);
     std::printf("events %ld\n", events);

@@ -148,6 +148,11 @@ class Mesh:
     def write_node_file(self, path: str, binary: bool = True):
         N.check(N.lib().tg_mesh_write_node_file(self._h, str(path).encode(), int(binary)))
 
+    @property
+    def dump_index(self) -> int:
+        """LAST_INDEX of the dump the mesh was read from (0 otherwise)."""
+        return int(N.lib().tg_mesh_dump_index(self._h))
+
     def write_grid_nodes(self, path: str, phi: np.ndarray | None = None, binary: bool = False):
         """File_Io::writeGeomGrid (file_io.cpp:765-820): the node file with
         numbers and potentials (phi: float potentials, None: the mesh's own),

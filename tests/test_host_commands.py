@@ -1,7 +1,9 @@
-"""The host program's make-ini and relaxation modes (tapsim_b200,
-csrc/host/tapsim_b200.cpp) against the reference's own `tapsim make-ini` and
-`tapsim relaxation` outputs (tests/golden/make_golden.py --commands;
-tapsim.cpp:66-148, commands.cpp:55-277)."""
+"""The host program's command line (tapsim_b200, csrc/host/tapsim_b200.cpp):
+its make-ini and relaxation modes against the reference's own `tapsim
+make-ini` and `tapsim relaxation` outputs (tests/golden/make_golden.py
+--commands; tapsim.cpp:66-148, commands.cpp:55-277), the reference's
+evaporation and resumption options (commands.cpp:280-841), and the dump's
+event index a resumption counts on from."""
 import gzip
 import subprocess
 
@@ -104,3 +106,44 @@ def test_relaxation_matches_the_reference(golden_dump, ref_mesh, ref_phi0, tmp_p
     _, rows2 = read_node_lines(nodes2.read_text())
     phi2 = np.array([float(x[5]) for x in rows2])
     assert np.abs(phi2 - phi_ref)[free].max() < 1e-4
+
+
+@pytest.mark.parametrize("opt", ["--write-trajectories=t", "--write-grids=g", "--write-surfaces=s",
+                                 "--snapshot-interval=5", "--dump-interval=5"])
+def test_evaporation_refuses_outputs_it_does_not_write(opt, tmp_path):
+    r = run([opt, "evaporation", tmp_path / "a.cfg", tmp_path / "a.nodes"], tmp_path)
+    assert r.returncode == 1
+    assert "results file only" in r.stderr
+
+
+def test_evaporation_takes_the_reference_options(tmp_path):
+    """Every evaporation/resumption option of the reference parses; the run
+    then fails where the mesh is read (before any device call)."""
+    opts = ["--skip-relaxation", "--init-potentials", "--reset-potentials", "--threshold=0", "--cycle-size=100",
+            "--queue-size=25", "--no-trajectories", "--no-grids", "--no-surfaces", "--no-dump", "--no-chunks",
+            "--chunk-size=10", "--vacuum-identifier=Vacuum", "--trajectory-error-threshold=1e-6",
+            "--shrink-limit=1e-9", "--event-limit=5", "--voltage-queue-limit=250", "--voltage-queue-size=250",
+            "--evap-threshold=1e-2", "--evap-shell-size=3", "--evap-cycle-size=5", "--evap-queue-size=5",
+            "--evap-global-cycles=1", "--refresh-interval=0", "--refresh-threshold=0", "--refresh-cycle-size=100",
+            "--refresh-queue-size=25", "--last-event=3", "--write-ascii", "--write-binary", "--no-file-output",
+            "--threads=2"]
+    r = run([*opts, "evaporation", tmp_path / "none.cfg", tmp_path / "none.nodes"], tmp_path)
+    assert r.returncode == 1
+    assert "reading the mesh" in r.stderr, r.stderr
+    r = run(["--write-dump=d", "evaporation", tmp_path / "none.cfg", tmp_path / "none.nodes"], tmp_path)
+    assert r.returncode == 1 and "--write-dump" in r.stderr
+
+
+def test_dump_index_is_kept(golden_dump, tmp_path):
+    """A dump's LAST_INDEX reads into the mesh (a resumption numbers its
+    events on from it) and is written back with the dump."""
+    from tapsim_modified_b200.tapsim import Mesh
+    data = golden_dump.read_bytes()
+    assert data.startswith(b"TAPSIM DUMP INFORMATION\nLAST_INDEX 0\n")
+    src = tmp_path / "indexed.dump"
+    src.write_bytes(data.replace(b"LAST_INDEX 0\n", b"LAST_INDEX 37\n", 1))
+    assert Mesh.from_dump(str(golden_dump), None).dump_index == 0
+    m = Mesh.from_dump(str(src), None)
+    assert m.dump_index == 37
+    m.write_dump(str(tmp_path / "back.dump"))
+    assert Mesh.from_dump(str(tmp_path / "back.dump"), None).dump_index == 37
