@@ -728,7 +728,8 @@ def run_probe_ions(args):
                                                  "p99_rel_impact_diff": float(np.percentile(v, 99)),
                                                  "max_rel_impact_diff": float(np.max(v))} for name, v in dev.items()},
                       "mixed_fp64_radius_m": fp64_radius,
-                      "value_arm": "mixed, the north star's precision split: the all-FP32 launch lasts as long as its "
+                      "value_arm": "mixed, FP64 where the field is steep near the start and FP32 beyond: the all-FP32 "
+                                   "launch lasts as long as its "
                                    "slowest ion, whose float step control near the tip takes several times the "
                                    "trials of any FP64 one (probe.fp32.trials_per_ion.max)",
                       "note": "impact differences relative to the FP64 impact's radius on the detector plane"}}
