@@ -49,14 +49,14 @@ def test_tuned_schedules_of_the_hierarchy():
     coarsest reports a restriction
     schedule, every level smoothed with CSR rows an operator schedule, each a
     power of two in 2..32 with a positive launch time; the solve converges
-    with them.  On the config-1 tip (307k cells) the hierarchy has at least
+    with them.  On the r = 5 nm tip (307k cells) the hierarchy has at least
     three levels."""
     import sys
     from conftest import GOLDEN as G
     sys.path.insert(0, str(G))
-    from make_config1 import CONFIG1_TIP
+    from make_tip5 import TIP5
     from tapsim_modified_b200.tapsim import Grid, Mesh
-    g = Grid(Mesh.from_tip(**CONFIG1_TIP))
+    g = Grid(Mesh.from_tip(**TIP5))
     info = g.solve(rel_tol=1e-8, max_outer=50, max_inner=20000, preconditioner=1)
     assert info.rel_residual <= 1e-8 and info.setup_seconds > 0
     sched = g.amg_schedule()

@@ -26,7 +26,7 @@ def test_tip_specs_are_seeded_and_in_range():
     assert atoms.min() > 2e4 and atoms.max() < 2e6
 
 
-def test_estimated_atoms_of_the_config1_tip():
+def test_estimated_atoms_of_the_5nm_tip():
     """A 5 nm cap on a 10 nm cylinder: the generator places 88,859 atoms."""
     from tapsim_modified_b200.serving import estimated_atoms
     est = estimated_atoms(dict(cap_radius=5e-9, shank_length=10e-9, half_angle_deg=0.0))

@@ -1,8 +1,8 @@
-"""Config 1 against the reference TAPSim built from source.
+"""The r = 5 nm, 307k-cell tip against the reference TAPSim built from source.
 
 Tip: bcc Fe [110], r = 5 nm hemispherical cap on a 10 nm cylindrical shank,
 vacuum coarsened out to a counter-electrode at 1 um: 88,859 atoms, 306,982
-cells.  tests/golden/make_config1.py ran the reference on this tip's node
+cells.  tests/golden/make_tip5.py ran the reference on this tip's node
 file: its own TetGen mesh and fastSync couplings, relaxation to its float
 fixed point, then 200 events with the converged ini (REFRESH_RELAXATION_
 INTERVAL = 1, threshold 0, one thread; process.cpp:680-1109, 876-894).  The
@@ -24,7 +24,7 @@ import pytest
 from conftest import GOLDEN
 
 sys.path.insert(0, str(GOLDEN))
-from make_config1 import CONFIG1_TIP  # noqa: E402
+from make_tip5 import TIP5  # noqa: E402
 
 NEAR_TIE = 1e-3   # relative probability gap below which two choices may differ
 # Detector impacts, as a fraction of the hit map's radius (the largest
@@ -40,25 +40,25 @@ IMPACT_MEDIAN = 5e-4
 
 
 def _events():
-    with gzip.open(GOLDEN / "config1_events.txt.gz", "rt") as f:
+    with gzip.open(GOLDEN / "tip5_events.txt.gz", "rt") as f:
         return np.loadtxt(f)
 
 
 @pytest.fixture(scope="module")
-def config1_mesh():
+def tip5_mesh():
     from tapsim_modified_b200.tapsim import Mesh
-    return Mesh.from_tip(**CONFIG1_TIP)
+    return Mesh.from_tip(**TIP5)
 
 
-def test_generator_writes_the_fixture_nodes(config1_mesh, tmp_path):
+def test_generator_writes_the_fixture_nodes(tip5_mesh, tmp_path):
     """The seeded generator still writes the node file the reference ran on
     (bit for bit), so the committed reference events describe this tip."""
-    p = tmp_path / "config1.nodes"
-    config1_mesh.write_node_file(str(p), binary=True)
-    want = (GOLDEN / "config1_nodes.sha256").read_text().split()[0]
+    p = tmp_path / "tip5.nodes"
+    tip5_mesh.write_node_file(str(p), binary=True)
+    want = (GOLDEN / "tip5_nodes.sha256").read_text().split()[0]
     assert hashlib.sha256(p.read_bytes()).hexdigest() == want
-    a = config1_mesh.arrays()
-    assert config1_mesh.num_nodes == 306982 and int((a["type"] == 4).sum()) == 88859
+    a = tip5_mesh.arrays()
+    assert tip5_mesh.num_nodes == 306982 and int((a["type"] == 4).sum()) == 88859
 
 
 def test_reference_log_is_whole():
@@ -69,14 +69,14 @@ def test_reference_log_is_whole():
 
 
 @pytest.mark.gpu
-def test_config1_sequence_fields_impacts(config1_mesh):
+def test_tip5_sequence_fields_impacts(tip5_mesh):
     from tapsim_modified_b200.tapsim import EvaporationOptions, Evaporation, Grid, solve_opts
     ev_ref = _events()
-    with gzip.open(GOLDEN / "config1_phi0.bin.gz") as f:
+    with gzip.open(GOLDEN / "tip5_phi0.bin.gz") as f:
         phi0 = np.frombuffer(f.read(), np.float32).astype(np.float64)
-    a = config1_mesh.arrays()
+    a = tip5_mesh.arrays()
     free = np.array([not a["types"][int(t)]["dirichlet"] for t in a["type"]])
-    g = Grid(config1_mesh)
+    g = Grid(tip5_mesh)
     g.solve(rel_tol=1e-10, max_outer=50, max_inner=20000, preconditioner=1)
     dphi0 = float(np.abs(g.potentials() - phi0)[free].max())
     print("initial relaxation: max |phi - phi_ref| over free cells", dphi0, "V")
