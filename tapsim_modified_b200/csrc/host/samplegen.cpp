@@ -30,6 +30,15 @@ class KdTree {
         for (int k = 0; k < n; k++)
             for (int a = 0; a < 3; a++) p_[3 * (size_t)k + a] = xyz[3 * (size_t)idx[k] + a];
         index_.swap(idx);
+        for (int a = 0; a < 3; a++) {
+            lo_[a] = 1e300;
+            hi_[a] = -1e300;
+        }
+        for (int k = 0; k < n; k++)
+            for (int a = 0; a < 3; a++) {
+                lo_[a] = std::min(lo_[a], p_[3 * (size_t)k + a]);
+                hi_[a] = std::max(hi_[a], p_[3 * (size_t)k + a]);
+            }
     }
     // the original indices of the points within sqrt(r2) of q, ascending
     void within(const double q[3], double r2, std::vector<int>& out) const {
@@ -43,7 +52,7 @@ class KdTree {
     // squared distance from q to the nearest point other than tree position `skip`
     double nearest2(const double q[3], int skip = -1) const {
         double best = 1e300;
-        query(0, size(), q, skip, best);
+        if (size() > 0) query(0, size(), q, skip, best, lo_, hi_);
         return best;
     }
     const double* point(int k) const { return &p_[3 * (size_t)k]; }
@@ -52,6 +61,7 @@ class KdTree {
     std::vector<double> p_;
     std::vector<int8_t> axis_;
     std::vector<int> index_;
+    double lo_[3], hi_[3];  // the points' bounding box
 
     void collect(int lo, int hi, const double q[3], double r2, std::vector<int>& out) const {
         while (hi > lo) {
@@ -91,28 +101,43 @@ class KdTree {
         }
     }
 
-    void query(int lo, int hi, const double q[3], int skip, double& best) const {
-        while (hi > lo) {
-            const int mid = lo + (hi - lo) / 2;
-            const double* p = point(mid);
-            if (mid != skip) {
-                const double dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
-                best = std::min(best, dx * dx + dy * dy + dz * dz);
-            }
-            if (hi - lo == 1) return;
-            const int a = axis_[mid];
-            const double diff = q[a] - p[a];
-            // the side of the split that holds q first, the other only if the
-            // split plane is nearer than the best point so far
-            if (diff < 0.0) {
-                query(lo, mid, q, skip, best);
-                if (diff * diff >= best) return;
-                lo = mid + 1;
-            } else {
-                query(mid + 1, hi, q, skip, best);
-                if (diff * diff >= best) return;
-                hi = mid;
-            }
+    // Nearest-point search over tree positions [lo, hi), whose points lie in
+    // the box [blo, bhi].  A subtree is skipped when its box lies at least
+    // the best distance so far from q: a point r inside has |q_a - r_a| >=
+    // the box's gap on every axis, in floating point too, so its squared
+    // distance is no smaller and the result is the exact minimum.  Far from
+    // the points (the coarse vacuum levels) the box test prunes what the
+    // split planes alone cannot.
+    void query(int lo, int hi, const double q[3], int skip, double& best, const double blo[3],
+               const double bhi[3]) const {
+        if (hi <= lo) return;
+        double box = 0.0;
+        for (int a = 0; a < 3; a++) {
+            const double e = q[a] < blo[a] ? blo[a] - q[a] : (q[a] > bhi[a] ? q[a] - bhi[a] : 0.0);
+            box += e * e;
+        }
+        if (box >= best) return;
+        const int mid = lo + (hi - lo) / 2;
+        const double* p = point(mid);
+        if (mid != skip) {
+            const double dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+            best = std::min(best, dx * dx + dy * dy + dz * dz);
+        }
+        if (hi - lo == 1) return;
+        const int a = axis_[mid];
+        // the children: [lo, mid) below the split value, [mid+1, hi) above
+        double lhi[3] = {bhi[0], bhi[1], bhi[2]}, rlo[3] = {blo[0], blo[1], blo[2]};
+        lhi[a] = p[a];
+        rlo[a] = p[a];
+        const double diff = q[a] - p[a];
+        // the side that holds q first, the other only if the split plane is
+        // nearer than the best point so far
+        if (diff < 0.0) {
+            query(lo, mid, q, skip, best, blo, lhi);
+            if (diff * diff < best) query(mid + 1, hi, q, skip, best, rlo, bhi);
+        } else {
+            query(mid + 1, hi, q, skip, best, rlo, bhi);
+            if (diff * diff < best) query(lo, mid, q, skip, best, blo, lhi);
         }
     }
 };
