@@ -287,12 +287,25 @@ struct Builder {
     static uint64_t cell_key(int64_t i, int64_t j, int64_t k) {
         return ((uint64_t)(i & 0x1FFFFF) << 42) | ((uint64_t)(j & 0x1FFFFF) << 21) | (uint64_t)(k & 0x1FFFFF);
     }
+    // The cells, of the 3 x 3 x 3 around q's, that can hold a point within r
+    // of q: on each axis those that [q - r, q + r] reaches (widened by a
+    // hair for rounding).  Any such point lies in them, so a scan of them
+    // finds what a scan of all 27 does.
+    void cell_range(const double q[3], double r, int64_t lo[3], int64_t hi[3]) const {
+        const double m = 1e-9 * h0;
+        for (int a = 0; a < 3; a++) {
+            const int64_t c = cell(q[a]);
+            lo[a] = std::max(c - 1, (int64_t)std::floor((q[a] - r - m) / h0));
+            hi[a] = std::min(c + 1, (int64_t)std::floor((q[a] + r + m) / h0));
+        }
+    }
     // a lattice site within r (<= h0) of q
     bool site_near(const double q[3], double r) const {
-        const int64_t ci = cell(q[0]), cj = cell(q[1]), ck = cell(q[2]);
-        for (int64_t i = ci - 1; i <= ci + 1; i++)
-            for (int64_t j = cj - 1; j <= cj + 1; j++)
-                for (int64_t k = ck - 1; k <= ck + 1; k++) {
+        int64_t lo[3], hi[3];
+        cell_range(q, r, lo, hi);
+        for (int64_t i = lo[0]; i <= hi[0]; i++)
+            for (int64_t j = lo[1]; j <= hi[1]; j++)
+                for (int64_t k = lo[2]; k <= hi[2]; k++) {
                     auto it = siteCells.find(cell_key(i, j, k));
                     if (it == siteCells.end()) continue;
                     for (int s : it->second) {
@@ -303,13 +316,15 @@ struct Builder {
                 }
         return false;
     }
-    // the lattice sites within r (<= h0) of q, ascending
+    // the lattice sites within r of q in the 3 x 3 x 3 cells around q's (all
+    // of them for r <= h0), ascending
     void sites_within(const double q[3], double r, std::vector<int>& out) const {
         out.clear();
-        const int64_t ci = cell(q[0]), cj = cell(q[1]), ck = cell(q[2]);
-        for (int64_t i = ci - 1; i <= ci + 1; i++)
-            for (int64_t j = cj - 1; j <= cj + 1; j++)
-                for (int64_t k = ck - 1; k <= ck + 1; k++) {
+        int64_t lo[3], hi[3];
+        cell_range(q, r, lo, hi);
+        for (int64_t i = lo[0]; i <= hi[0]; i++)
+            for (int64_t j = lo[1]; j <= hi[1]; j++)
+                for (int64_t k = lo[2]; k <= hi[2]; k++) {
                     auto it = siteCells.find(cell_key(i, j, k));
                     if (it == siteCells.end()) continue;
                     for (int s : it->second) {
